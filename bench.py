@@ -1,0 +1,351 @@
+"""Benchmark: FP64 cell-updates/s of the cubed-sphere MHD RK4 step on B200.
+
+One step = one classical RK4 step of the whole six-panel shell (4 operator
+evaluations: stage preparation with seam/radial ghosts, fused flux
+divergence + Powell + gravity + RK update), with dt = cfl / max CFL rate
+computed on the device before every step.  One cell-update = one valid cell
+advanced one full RK4 step.
+
+Workload (default): second-order PLM-MC + Rusanov, Powell on, 32 radial x
+32 x 32 angular cells per panel (196,608 cells), gamma 5/3, r in [21.5, 215]
+Rsun, radial stretch 1.5, CFL 0.4, seeded Parker-like wind + Gaussian
+pressure pulse (synthetic input; the reference ships no data for it).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 (torchrun): every rank runs an independent replica of the workload
+(weak scaling; the path has no exchange between replicas), timed on the
+device and reduced as the max over ranks.  --impl reference times the CPU
+restatement of the reference's algorithm (the reference itself cannot be
+built: its Proto dependency is absent) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 cell-updates/s on 1 B200 (RK4 step of the cubed-sphere MHD update)"
+UNIT = "cell-updates/s"
+L2_BYTES = 126 * 1024 * 1024
+OPERATOR_BYTES_PER_CELL_STAGE = 128  # read 8 FP64 primitives, write 8 FP64 rhs
+LAUNCHES_PER_STEP = 14               # cfl + 4 x (prim, ghosts, stage) + time
+
+
+def workload_params(args):
+    from heliocubed_b200.level import Params
+    return Params(nr=args.nr, na=args.na, limiter=args.limiter, riemann_solver=args.riemann,
+                  divergence_cleaning=1, sun_gravity=args.gravity, cfl=0.4)
+
+
+def workload_config(args, flush: bool):
+    return {
+        "workload": f"cubed-sphere MHD RK4 step, PLM-{'MC' if args.limiter == 3 else args.limiter} + "
+                    f"{'Roe' if args.riemann == 2 else 'Rusanov'}, {args.nr}x{args.na}^2x6",
+        "cells": 6 * args.nr * args.na * args.na,
+        "scheme": {"spatial_order": 2, "limiter": args.limiter, "riemann_solver": args.riemann,
+                   "powell": 1, "gravity": args.gravity, "temporal_order": 4, "cfl": 0.4},
+        "l2": "flushed between timed steps (256 MiB write)" if flush else "working set larger than L2",
+        "dt": "device CFL reduction every step",
+    }
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic_per_cell_stage():
+    """DRAM bytes per cell-stage of the operator kernel from the committed ncu
+    summary (profiles/o2_stage_kernel.md), or None before one exists."""
+    path = os.path.join(ROOT, "profiles", "o2_stage_kernel.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_cell_stage:\s*([0-9.eE+-]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows: list[list[str]] = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(args, budget_s: float = 12.0) -> dict:
+    """The oracle (CPU restatement of the reference) on the host cores, on a
+    bounded number of RK4 steps of the same workload."""
+    from oracle import pyoracle as po
+    cores = os.cpu_count() or 1
+    p = po.make_params(nr=args.nr, na=args.na, limiter=args.limiter, riemann_solver=args.riemann,
+                       sun_gravity=args.gravity)
+    L = po.OracleLevel(p)
+    from heliocubed_b200.level import InitSpec
+    spec = InitSpec.seeded(args.seed, args.nr, args.na)
+    s = po.HcInit()
+    s.kind = 1
+    for k in ("pulse_block", "pulse_i", "pulse_j", "pulse_k", "rho0", "p0", "vr", "b0", "r_ref", "pulse_amp",
+              "pulse_width"):
+        setattr(s, k, getattr(spec, k))
+    ju = L.init(s)
+    steps, t = 0, 0.0
+    t0 = time.perf_counter()
+    while True:
+        dt = 0.4 / L.inv_dt(ju)
+        L.rk4_step(ju, dt, t)
+        t += dt
+        steps += 1
+        if time.perf_counter() - t0 > budget_s or steps >= args.cpu_max_steps:
+            break
+    el = time.perf_counter() - t0
+    value = 6 * args.nr * args.na * args.na * steps / el
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} RK4 steps (CFL dt each step) of the same {args.nr}x{args.na}^2x6 workload, "
+                      f"OpenMP over {cores} host threads, {el:.1f} s"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    cb = cpu_baseline(args, budget_s=args.ref_budget)
+    out = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": workload_config(args, flush=False), "cpu_baseline": cb,
+           "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_b200(args, world, rank, local):
+    import torch
+    from heliocubed_b200.level import InitSpec, Shell
+    torch.cuda.set_device(local)
+    params = workload_params(args)
+    shell = Shell(params, device=local)
+    cells = shell.cells
+    spec = InitSpec.seeded(args.seed, args.nr, args.na)
+    ju0 = shell.init(spec)
+    ju = ju0.clone()
+    time_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    state_bytes = ju.numel() * 8
+    working = state_bytes * 3 + shell.ng * 8
+    flush = working < 2 * L2_BYTES
+    scratch = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda") if flush else None
+
+    for _ in range(args.warmup):
+        shell.advance(ju, 1, time_dev)
+    torch.cuda.synchronize()
+    if not shell.valid(ju):
+        raise RuntimeError("warm-up produced an invalid state")
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for s in range(args.steps):
+        if flush:
+            scratch.zero_()
+        ev[s][0].record(stream)
+        shell.advance(ju, 1, time_dev)
+        ev[s][1].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    ms = dist_max(ms, world)
+    ok = shell.valid(ju)
+
+    # operator kernel alone (hc_level_rhs: read primitives, write rhs) for the roofline
+    w = shell.prepare(ju)
+    k = shell.new_state()
+    for _ in range(3):
+        shell.rhs(w, k)
+    reps = 20
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for r in range(reps):
+        if flush:
+            scratch.zero_()
+        kev[r][0].record(stream)
+        shell.rhs(w, k)
+        kev[r][1].record(stream)
+    torch.cuda.synchronize()
+    kms = statistics.mean(a.elapsed_time(b) for a, b in kev)
+    peak, peak_kind = peaks()
+    achieved = OPERATOR_BYTES_PER_CELL_STAGE * cells / (kms * 1e-3) / 1e9
+    tr = profiled_traffic_per_cell_stage()
+
+    # end to end through the public API with host buffers
+    host_in = ju0.cpu().pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    dev = torch.empty_like(ju0)
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(2):
+        dev.copy_(host_in, non_blocking=True)
+        shell.advance(dev, 1, time_dev)
+        host_out.copy_(dev, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        dev.copy_(host_in, non_blocking=True)
+        shell.advance(dev, 1, time_dev)
+        host_out.copy_(dev, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = dist_max(e0.elapsed_time(e1) / e2e_steps, world)
+
+    if rank == 0:
+        value = cells * world * args.steps / (ms * 1e-3)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload_config(args, flush), parallelism=f"replicas x{world}"),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "kernel": "o2StageKernel (operator: read primitives, write rhs)",
+                         "algorithmic_bytes": f"{OPERATOR_BYTES_PER_CELL_STAGE} B/cell-stage x {cells} cells",
+                         "kernel_ms": kms,
+                         "traffic": None if tr is None else tr * cells},
+            "e2e": {"value": cells * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
+                    "d2h_bytes_per_step": state_bytes},
+            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+            "clocks": clocks,
+            "valid_state": ok,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_baseline(args)
+        print(json.dumps(out), flush=True)
+    shell.close()
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--nr", type=int, default=32)
+    ap.add_argument("--na", type=int, default=32)
+    ap.add_argument("--limiter", type=int, default=3)
+    ap.add_argument("--riemann", type=int, default=1)
+    ap.add_argument("--gravity", type=int, default=0)
+    ap.add_argument("--seed", type=int, default=20261204)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-max-steps", type=int, default=60)
+    ap.add_argument("--ref-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
+        return 0  # the CPU reference arm runs on rank 0 only
+    if args.impl == "reference":
+        run_reference(args, 1, 0)
+        return 0
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_b200(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,92 @@
+"""ctypes binding of the product library libhc_b200.so (C ABI: include/hc_abi.h).
+
+The library is built in-tree by heliocubed_b200.build.  There is no fallback:
+if the library is missing or CUDA is unavailable every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhc_b200.so")
+
+_D = C.POINTER(C.c_double)
+_VP = C.c_void_p
+
+HC_OK = 0
+ERRORS = {-1: "HC_ERR_ARG", -2: "HC_ERR_CUDA", -3: "HC_ERR_UNSUPPORTED", -4: "HC_ERR_INVALID_STATE", -5: "HC_ERR_NOMEM"}
+
+# Every function hc_abi.h declares, with its ctypes signature.
+SIGNATURES = {
+    "hc_last_error": (C.c_char_p, []),
+    "hc_ctx_create": (C.c_int, [_VP, C.c_int, C.POINTER(_VP)]),
+    "hc_ctx_destroy": (C.c_int, [_VP]),
+    "hc_level_state_size": (C.c_size_t, [_VP]),
+    "hc_level_primitive_size": (C.c_size_t, [_VP]),
+    "hc_box_rhs": (C.c_int, [_VP, _VP, _VP, _VP, C.c_double, _VP, _VP, _VP]),
+    "hc_box_gravity": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "hc_level_prepare": (C.c_int, [_VP, _VP, _VP, C.c_double, _VP]),
+    "hc_level_rhs": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "hc_level_rk4_step": (C.c_int, [_VP, _VP, C.c_double, C.c_double, _VP]),
+    "hc_level_advance_cfl": (C.c_int, [_VP, _VP, C.c_int, _VP, _VP, _VP]),
+    "hc_level_dt_cfl": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "hc_level_valid": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "hc_level_init": (C.c_int, [_VP, _VP, _VP, _VP]),
+    "hc_geometry_export": (C.c_long, [_VP, C.c_int, _VP]),
+}
+
+
+class HcParams(C.Structure):
+    """hc_params of include/hc_abi.h (option semantics of src/Inputs_Parsing.H)."""
+    _fields_ = [
+        ("spatial_order", C.c_int), ("limiter", C.c_int), ("riemann_solver", C.c_int),
+        ("divergence_cleaning", C.c_int), ("sun_gravity", C.c_int),
+        ("init_condition_type", C.c_int), ("temporal_order", C.c_int),
+        ("nr", C.c_int), ("na", C.c_int), ("reserved_i", C.c_int * 7),
+        ("gamma", C.c_double), ("entropy_fix_coeff", C.c_double), ("cfl", C.c_double),
+        ("inner_radius", C.c_double), ("outer_radius", C.c_double),
+        ("radial_stretch", C.c_double), ("strength", C.c_double), ("reserved_d", C.c_double * 7),
+    ]
+
+
+class HcBox(C.Structure):
+    _fields_ = [("lo", C.c_int * 3), ("hi", C.c_int * 3), ("ghost", C.c_int), ("block", C.c_int)]
+
+
+class HcInit(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("pulse_block", C.c_int), ("pulse_i", C.c_int), ("pulse_j", C.c_int),
+        ("pulse_k", C.c_int), ("reserved_i", C.c_int * 3),
+        ("rho0", C.c_double), ("p0", C.c_double), ("vr", C.c_double), ("b0", C.c_double),
+        ("r_ref", C.c_double), ("pulse_amp", C.c_double), ("pulse_width", C.c_double),
+        ("reserved_d", C.c_double * 4),
+    ]
+
+
+class HcError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libhc_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise HcError(f"{LIB_PATH} is missing: build it with `python -m heliocubed_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != HC_OK:
+        msg = lib().hc_last_error().decode(errors="replace")
+        raise HcError(f"{what} failed: {ERRORS.get(rc, rc)}: {msg}")

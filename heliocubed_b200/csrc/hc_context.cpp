@@ -1,0 +1,694 @@
+// Host side of the C ABI (include/hc_abi.h): option validation, level
+// geometry (the caches the reference keeps in levelGeometry statics and in
+// its per-patch face / CFL / gravity caches), workspace, and launch sequences.
+//
+// Metrics are the exact cell/face averages of the equiangular gnomonic map,
+// integrated here with 8-point Gauss-Legendre quadrature in double (the
+// reference obtains them from Proto's unvendored CubedSphereShell).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/hc_abi.h"
+#include "hc_level.h"
+
+using namespace hc;
+
+namespace {
+
+thread_local std::string g_lastError;
+
+int fail(int code, const std::string& msg) {
+  g_lastError = msg;
+  return code;
+}
+int cudaFail(cudaError_t e, const char* where) {
+  return fail(HC_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// src/BoxOp_Utilities.H:413-416, read as: global component k of a panel-local
+// vector q is SIGN[b][k] * q[PERM[b][k]].
+const int PERM[6][3] = {{1, 2, 0}, {1, 2, 0}, {1, 0, 2}, {0, 1, 2}, {1, 0, 2}, {0, 1, 2}};
+const int SIGN[6][3] = {{1, -1, -1}, {1, 1, 1}, {1, -1, 1}, {1, 1, 1}, {-1, 1, 1}, {-1, -1, 1}};
+const double PI = 3.14159265358979323846;
+
+struct Vec3 { double x[3]; };
+
+// Basis A = (Xhat, dXhat/dxi1, dXhat/dxi2) at panel coordinates (x1, x2).
+void basisAt(int b, double x1, double x2, double A[3][3], double X[3]) {
+  const double ta = std::tan(-PI / 4 + PI / 2 * x1), tb = std::tan(-PI / 4 + PI / 2 * x2);
+  const double rho2 = 1 + ta * ta + tb * tb, rho = std::sqrt(rho2), r3 = rho * rho2;
+  const double q[3] = {1 / rho, ta / rho, tb / rho};
+  const double da = PI / 2 * (1 + ta * ta), db = PI / 2 * (1 + tb * tb);
+  const double q1[3] = {-ta / r3 * da, (1 / rho - ta * ta / r3) * da, -ta * tb / r3 * da};
+  const double q2[3] = {-tb / r3 * db, -ta * tb / r3 * db, (1 / rho - tb * tb / r3) * db};
+  for (int k = 0; k < 3; ++k) {
+    const int p = PERM[b][k];
+    A[k][0] = SIGN[b][k] * q[p];
+    A[k][1] = SIGN[b][k] * q1[p];
+    A[k][2] = SIGN[b][k] * q2[p];
+    if (X) X[k] = A[k][0];
+  }
+}
+
+void cross(const double u[3], const double v[3], double w[3]) {
+  w[0] = u[1] * v[2] - u[2] * v[1];
+  w[1] = u[2] * v[0] - u[0] * v[2];
+  w[2] = u[0] * v[1] - u[1] * v[0];
+}
+
+struct Gauss {
+  double x[8], w[8];
+  Gauss() {
+    const int n = 8;
+    for (int i = 0; i < n; ++i) {
+      double z = std::cos(PI * (i + 0.75) / (n + 0.5)), pp = 1;
+      for (int it = 0; it < 60; ++it) {
+        double p1 = 1, p2 = 0;
+        for (int j = 1; j <= n; ++j) {
+          const double p3 = p2;
+          p2 = p1;
+          p1 = ((2 * j - 1) * z * p2 - (j - 1) * p3) / j;
+        }
+        pp = n * (z * p1 - p2) / (z * z - 1);
+        const double dz = p1 / pp;
+        z -= dz;
+        if (std::fabs(dz) < 1e-17) break;
+      }
+      x[i] = 0.5 * (1 - z);
+      w[i] = 1 / ((1 - z * z) * pp * pp);
+    }
+  }
+};
+
+// Cofactor row d of A (normal of a constant-xi_d face), times det when
+// d = 0 this is det(A) Xhat.
+void cofactorRow(const double A[3][3], int d, double n[3]) {
+  const int t1 = (d + 1) % 3, t2 = (d + 2) % 3;
+  const double a[3] = {A[0][t1], A[1][t1], A[2][t1]}, c[3] = {A[0][t2], A[1][t2], A[2][t2]};
+  cross(a, c, n);
+}
+
+double det3(const double A[3][3]) {
+  return A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) - A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+         A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+}
+
+void inv3(const double A[3][3], double I[3][3]) {
+  const double c00 = A[1][1] * A[2][2] - A[1][2] * A[2][1];
+  const double c01 = A[1][2] * A[2][0] - A[1][0] * A[2][2];
+  const double c02 = A[1][0] * A[2][1] - A[1][1] * A[2][0];
+  const double id = 1.0 / (A[0][0] * c00 + A[0][1] * c01 + A[0][2] * c02);
+  I[0][0] = c00 * id;
+  I[1][0] = c01 * id;
+  I[2][0] = c02 * id;
+  I[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) * id;
+  I[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) * id;
+  I[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) * id;
+  I[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) * id;
+  I[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) * id;
+  I[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id;
+}
+
+// src/MHD_SecondOrderFlux.H:11-30
+FaceGeom makeFrame(const double normal[3]) {
+  FaceGeom r{};
+  double f[3][3] = {};
+  double norm = 0;
+  for (int i = 0; i < 3; ++i) norm += normal[i] * normal[i];
+  norm = std::sqrt(norm);
+  for (int i = 0; i < 3; ++i) f[0][i] = normal[i] / norm;
+  int axis = 0;
+  for (int i = 1; i < 3; ++i)
+    if (std::fabs(f[0][i]) < std::fabs(f[0][axis])) axis = i;
+  f[1][(axis + 1) % 3] = f[0][(axis + 2) % 3];
+  f[1][(axis + 2) % 3] = -f[0][(axis + 1) % 3];
+  double t = 0;
+  for (int i = 0; i < 3; ++i) t += f[1][i] * f[1][i];
+  for (int i = 0; i < 3; ++i) f[1][i] /= std::sqrt(t);
+  for (int i = 0; i < 3; ++i) {
+    const int j = (i + 1) % 3, k = (i + 2) % 3;
+    f[2][i] = f[0][j] * f[1][k] - f[0][k] * f[1][j];
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.f[3 * i + j] = f[i][j];
+  r.norm = norm;
+  for (int d = 0; d < 3; ++d) r.n[d] = normal[d];
+  return r;
+}
+
+// Radial metrics, src/BoxOp_Utilities.H:36-59.
+struct RadialRow { double rlow, rhigh, rhalf, vol, Dr0, area0, areaT; };
+RadialRow radialRow(const hc_params& P, int i) {
+  const double r0 = P.inner_radius, r1 = P.outer_radius, C = P.radial_stretch, dxi0 = 1.0 / P.nr;
+  const double R_t = C == 0.0 ? (r1 - r0) : (r1 - r0) / std::expm1(C);
+  const double etalow = i * dxi0;
+  const double rlow = r0 + R_t * (C == 0.0 ? etalow : std::expm1(C * etalow));
+  const double etahigh = (i + 1.0) * dxi0;
+  const double rhigh = r0 + R_t * (C == 0.0 ? etahigh : std::expm1(C * etahigh));
+  const double eta_half = (etalow + etahigh) / 2.0;
+  const double rhalf = r0 + R_t * (C == 0.0 ? eta_half : std::expm1(C * eta_half));
+  RadialRow r;
+  r.rlow = rlow;
+  r.rhigh = rhigh;
+  r.rhalf = rhalf;
+  r.vol = (rhigh * rhigh * rhigh - rlow * rlow * rlow) / 3.0 / dxi0;
+  r.Dr0 = (rhigh - rlow) / dxi0;
+  r.area0 = rlow * rlow;
+  r.areaT = (rhigh * rhigh - rlow * rlow) / dxi0 / 2.0;
+  return r;
+}
+
+// Inner analytic wind in the native basis, src/BoxOp_PreStage.H:7-47 at t=0
+// (the time-independent case strength = 0 is tabulated on the host).
+void windNative(const hc_params& P, const double X[3], double u[8]) {
+  const double gam = P.gamma, r_BC = P.inner_radius;
+  const double r = std::sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+  const double p0 = 1.0e-7, rho0 = 700 * kMP, u0 = 500.0 * 1e5;
+  const double rho = rho0 * std::pow(r_BC / r, 2.0);
+  const double p = p0 * std::pow(r_BC / r, 2.0 * gam);
+  const double ur = u0 - P.strength / 100.0 * u0 / 3 * 0.0;
+  u[0] = rho;
+  u[1] = ur * rho;
+  u[2] = u[3] = u[5] = u[6] = u[7] = 0.0;
+  const double umag = std::sqrt(u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0];
+  const double Bmag = 0.0;
+  u[4] = p / (gam - 1.0) + 0.5 * u[0] * umag * umag + Bmag * Bmag / 8.0 / PI;
+}
+
+// Panel containing direction X and its panel coordinates.
+void locate(const double X[3], int& pb) {
+  pb = 0;
+  double best = -2;
+  for (int b = 0; b < 6; ++b) {
+    double q0 = 0;
+    for (int k = 0; k < 3; ++k)
+      if (PERM[b][k] == 0) q0 = SIGN[b][k] * X[k];
+    if (q0 > best) { best = q0; pb = b; }
+  }
+}
+void panelCoords(int b, const double X[3], double& x1, double& x2) {
+  double q[3];
+  for (int k = 0; k < 3; ++k) q[PERM[b][k]] = SIGN[b][k] * X[k];
+  x1 = (std::atan2(q[1], q[0]) + PI / 4) / (PI / 2);
+  x2 = (std::atan2(q[2], q[0]) + PI / 4) / (PI / 2);
+}
+
+template <class T>
+T* upload(const std::vector<T>& v, std::vector<void*>& owned, cudaError_t& err) {
+  void* p = nullptr;
+  if (err != cudaSuccess) return nullptr;
+  err = cudaMalloc(&p, std::max<size_t>(1, v.size() * sizeof(T)));
+  if (err != cudaSuccess) return nullptr;
+  owned.push_back(p);
+  if (!v.empty()) err = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return static_cast<T*>(p);
+}
+
+}  // namespace
+
+struct hc_ctx {
+  hc_params P;
+  int device = 0;
+  DevLevel L{};
+  std::vector<void*> owned;
+  // host copies for hc_geometry_export
+  std::vector<double> radialExport, detExport, detAAExport, normalExport[3];
+  // stage workspace
+  double* W = nullptr;     // ghosted primitives [6][8][nr+4][na+4][na+4]
+  double* acc = nullptr;   // RK accumulator [6][8][nr][na][na]
+  double* next = nullptr;  // next stage state
+  unsigned long long* invMax = nullptr;
+  int* flag = nullptr;
+};
+
+namespace {
+
+int buildLevel(hc_ctx* c) {
+  const hc_params& P = c->P;
+  const int nr = P.nr, na = P.na, g = kGhost;
+  const double h = 1.0 / na;
+  Gauss G;
+  DevLevel& L = c->L;
+  L.nr = nr; L.na = na; L.g = g;
+  L.n0 = nr + 2 * g; L.n1 = na + 2 * g;
+  L.Nv = (long)nr * na * na;
+  L.Ng = (long)L.n0 * L.n1 * L.n1;
+  L.h = h; L.dxi0 = 1.0 / nr;
+  L.gamma = P.gamma; L.entropy = P.entropy_fix_coeff; L.cfl_number = P.cfl; L.strength = P.strength;
+  L.r0 = P.inner_radius; L.innerBCType = P.init_condition_type;
+
+  // radial rows i = -g .. nr+g
+  std::vector<double4> radial(nr + 2 * g + 1);
+  std::vector<double> rc(nr + 2 * g + 1);
+  c->radialExport.assign((size_t)(nr + 1) * 4, 0.0);
+  for (int i = -g; i <= nr + g; ++i) {
+    const RadialRow r = radialRow(P, i);
+    radial[i + g] = make_double4(r.area0, r.areaT, r.Dr0, r.vol);
+    rc[i + g] = r.rhalf;
+    if (i >= 0 && i <= nr) {
+      double* e = &c->radialExport[4 * i];
+      e[0] = r.area0; e[1] = r.areaT; e[2] = r.Dr0; e[3] = r.vol;
+    }
+  }
+  for (int m = 0; m < g; ++m) {
+    const double rl = radialRow(P, nr - 1).rhalf, rr = radialRow(P, nr + m).rhalf;
+    L.outerScale2[m] = std::pow(rl / rr, 2.0);
+    L.outerScale1[m] = std::pow(rl / rr, 1.0);
+  }
+
+  const size_t nf = (size_t)(na + 1) * (na + 1);
+  std::vector<FaceGeom> faces(3 * 6 * nf);
+  std::vector<GravCell> grav((size_t)6 * na * na);
+  std::vector<double> basis((size_t)6 * na * na * 9), basisInv((size_t)6 * na * na * 9);
+  std::vector<CflCell> cfl((size_t)6 * na * na);
+  for (int d = 0; d < 3; ++d) c->normalExport[d].clear();
+  c->detExport.assign((size_t)6 * na * na, 0.0);
+  c->detAAExport.assign((size_t)6 * na * na * 9, 0.0);
+
+  for (int b = 0; b < 6; ++b) {
+    // Face normals: average over the face of the cofactor row.
+    for (int k = 0; k <= na; ++k)
+      for (int j = 0; j <= na; ++j)
+        for (int d = 0; d < 3; ++d) {
+          if ((d != 1 && j == na) || (d != 2 && k == na)) continue;
+          double n[3] = {0, 0, 0};
+          if (d == 0) {
+            for (int p = 0; p < 8; ++p)
+              for (int q = 0; q < 8; ++q) {
+                double A[3][3], m[3];
+                basisAt(b, (j + G.x[p]) * h, (k + G.x[q]) * h, A, nullptr);
+                cofactorRow(A, 0, m);
+                for (int r = 0; r < 3; ++r) n[r] += G.w[p] * G.w[q] * m[r];
+              }
+          } else {
+            for (int p = 0; p < 8; ++p) {
+              double A[3][3], m[3];
+              if (d == 1) basisAt(b, j * h, (k + G.x[p]) * h, A, nullptr);
+              else basisAt(b, (j + G.x[p]) * h, k * h, A, nullptr);
+              cofactorRow(A, d, m);
+              for (int r = 0; r < 3; ++r) n[r] += G.w[p] * m[r];
+            }
+          }
+          faces[((size_t)d * 6 + b) * nf + (size_t)k * (na + 1) + j] = makeFrame(n);
+        }
+    for (int k = 0; k < na; ++k)
+      for (int j = 0; j < na; ++j) {
+        const size_t ci = ((size_t)b * na + k) * na + j;
+        double det = 0, dA[3][3] = {{0}};
+        for (int p = 0; p < 8; ++p)
+          for (int q = 0; q < 8; ++q) {
+            double A[3][3];
+            basisAt(b, (j + G.x[p]) * h, (k + G.x[q]) * h, A, nullptr);
+            const double dt = det3(A), wt = G.w[p] * G.w[q];
+            det += wt * dt;
+            for (int r = 0; r < 3; ++r)
+              for (int s = 0; s < 3; ++s) dA[r][s] += wt * dt * A[r][s];
+          }
+        double Ac[3][3], X[3], Ai[3][3];
+        basisAt(b, (j + 0.5) * h, (k + 0.5) * h, Ac, X);
+        inv3(Ac, Ai);
+        GravCell& gc = grav[ci];
+        for (int r = 0; r < 3; ++r) { gc.x[r] = X[r]; gc.a0[r] = dA[r][0]; }
+        gc.det = det;
+        gc.pad = 0;
+        for (int r = 0; r < 3; ++r)
+          for (int s = 0; s < 3; ++s) {
+            basis[ci * 9 + 3 * r + s] = Ac[r][s];
+            basisInv[ci * 9 + 3 * r + s] = Ai[r][s];
+            c->detAAExport[ci * 9 + 3 * r + s] = dA[r][s];
+          }
+        c->detExport[ci] = det;
+        // CFL cache (src/BoxOp_SecondOrderCFL.H:46-77)
+        CflCell& cc = cfl[ci];
+        cc.inverseDet = 1.0 / det;
+        double dAi[3][3];
+        inv3(dA, dAi);
+        for (int r = 0; r < 3; ++r)
+          for (int s = 0; s < 3; ++s) {
+            cc.inverseDetA[3 * r + s] = dAi[r][s];
+            cc.cell[3 * r + s] = Ac[r][s];
+          }
+        for (int d = 0; d < 3; ++d) {
+          const FaceGeom& f = faces[((size_t)d * 6 + b) * nf + (size_t)k * (na + 1) + j];
+          double n2 = 0;
+          for (int q = 0; q < 3; ++q) n2 += f.n[q] * f.n[q];
+          cc.normal[d] = std::sqrt(n2);
+          if (d == 0) { cc.det[0] = det; continue; }
+          double fd = 0;
+          for (int p = 0; p < 8; ++p) {
+            double A[3][3];
+            if (d == 1) basisAt(b, j * h, (k + G.x[p]) * h, A, nullptr);
+            else basisAt(b, (j + G.x[p]) * h, k * h, A, nullptr);
+            fd += G.w[p] * det3(A);
+          }
+          cc.det[d] = fd;
+          double F[3][3];
+          if (d == 1) basisAt(b, j * h, (k + 0.5) * h, F, nullptr);
+          else basisAt(b, (j + 0.5) * h, k * h, F, nullptr);
+          for (int r = 0; r < 3; ++r)
+            for (int s = 0; s < 3; ++s) cc.face[d - 1][3 * r + s] = F[r][s];
+        }
+        cc.pad[0] = cc.pad[1] = 0;
+      }
+  }
+  for (int d = 0; d < 3; ++d) {
+    const int ej = d == 1 ? 1 : 0, ek = d == 2 ? 1 : 0;
+    for (int b = 0; b < 6; ++b)
+      for (int k = 0; k < na + ek; ++k)
+        for (int j = 0; j < na + ej; ++j) {
+          const FaceGeom& f = faces[((size_t)d * 6 + b) * nf + (size_t)k * (na + 1) + j];
+          for (int r = 0; r < 3; ++r) c->normalExport[d].push_back(f.n[r]);
+        }
+  }
+
+  // Seam plan: for each panel edge, the adjacent panel, its normal axis and
+  // side; ghost donors (4-point Lagrange along the adjacent edge, stencil
+  // kept inside the donor panel) and the seam-face index map.
+  std::vector<SeamDonor> seam((size_t)6 * 2 * 2 * g * na);
+  std::vector<int> faceMap((size_t)6 * 2 * 2 * na);
+  std::vector<EdgeLink> edges(6 * 2 * 2);
+  for (int b = 0; b < 6; ++b)
+    for (int ax = 1; ax <= 2; ++ax)
+      for (int side = 0; side < 2; ++side) {
+        const int e = (b * 2 + (ax - 1)) * 2 + side;
+        auto ghostX = [&](int m, double t, double X[3]) {
+          const double nrm = side == 0 ? -(m + 0.5) * h : 1 + (m + 0.5) * h;
+          double A[3][3];
+          if (ax == 1) basisAt(b, nrm, t, A, X);
+          else basisAt(b, t, nrm, A, X);
+        };
+        double X[3], y1, y2;
+        ghostX(0, 0.5, X);
+        int nb;
+        locate(X, nb);
+        panelCoords(nb, X, y1, y2);
+        const int nax = std::min(y1, 1 - y1) < std::min(y2, 1 - y2) ? 1 : 2;
+        const int nside = (nax == 1 ? y1 : y2) < 0.5 ? 0 : 1;
+        edges[e] = EdgeLink{nb, nax, nside, 0};
+        for (int m = 0; m < g; ++m)
+          for (int s = 0; s < na; ++s) {
+            ghostX(m, (s + 0.5) * h, X);
+            panelCoords(nb, X, y1, y2);
+            const double u = (nax == 1 ? y2 : y1) / h - 0.5;
+            int base = (int)std::floor(u) - 1;
+            base = std::max(0, std::min(na - 4, base));
+            const int layer = nside == 0 ? m : na - 1 - m;
+            SeamDonor dn{};
+            dn.b = nb;
+            for (int q = 0; q < 4; ++q) {
+              double wq = 1;
+              for (int r = 0; r < 4; ++r)
+                if (r != q) wq *= (u - (base + r)) / (double)(q - r);
+              dn.w[q] = wq;
+              dn.j[q] = nax == 1 ? layer : base + q;
+              dn.k[q] = nax == 1 ? base + q : layer;
+            }
+            seam[(((size_t)e) * g + m) * na + s] = dn;
+          }
+        for (int s = 0; s < na; ++s) {
+          double A[3][3];
+          const double t = (s + 0.5) * h, en = side == 0 ? 0.0 : 1.0;
+          if (ax == 1) basisAt(b, en, t, A, X);
+          else basisAt(b, t, en, A, X);
+          panelCoords(nb, X, y1, y2);
+          faceMap[(size_t)e * na + s] = (int)std::lround((nax == 1 ? y2 : y1) / h - 0.5);
+        }
+      }
+
+  // Inner wind table (time-independent when strength == 0).
+  std::vector<double> inner;
+  if (P.init_condition_type == 1 && P.strength == 0.0) {
+    inner.resize((size_t)6 * na * na * g * NC);
+    for (int b = 0; b < 6; ++b)
+      for (int k = 0; k < na; ++k)
+        for (int j = 0; j < na; ++j) {
+          const size_t ci = ((size_t)b * na + k) * na + j;
+          for (int i = -g; i < 0; ++i) {
+            const double radius = rc[i + g];
+            const double X[3] = {radius * grav[ci].x[0], radius * grav[ci].x[1], radius * grav[ci].x[2]};
+            windNative(P, X, &inner[(ci * g + (i + g)) * NC]);
+          }
+        }
+  }
+
+  cudaError_t err = cudaSuccess;
+  L.radial = upload(radial, c->owned, err);
+  L.rc = upload(rc, c->owned, err);
+  L.face = upload(faces, c->owned, err);
+  L.grav = upload(grav, c->owned, err);
+  L.basis = upload(basis, c->owned, err);
+  L.basisInv = upload(basisInv, c->owned, err);
+  L.cfl = upload(cfl, c->owned, err);
+  L.seam = upload(seam, c->owned, err);
+  L.faceMap = upload(faceMap, c->owned, err);
+  L.edge = upload(edges, c->owned, err);
+  L.innerBC = inner.empty() ? nullptr : upload(inner, c->owned, err);
+  if (err != cudaSuccess) return cudaFail(err, "geometry upload");
+  return HC_OK;
+}
+
+int allocWorkspace(hc_ctx* c) {
+  const size_t nv = 6 * NC * (size_t)c->L.Nv, ng = 6 * NC * (size_t)c->L.Ng;
+  void* p;
+  cudaError_t e;
+  if ((e = cudaMalloc(&p, ng * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace W");
+  c->owned.push_back(p); c->W = (double*)p;
+  if ((e = cudaMemset(p, 0, ng * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace W");
+  if ((e = cudaMalloc(&p, nv * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace acc");
+  c->owned.push_back(p); c->acc = (double*)p;
+  if ((e = cudaMalloc(&p, nv * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace next");
+  c->owned.push_back(p); c->next = (double*)p;
+  if ((e = cudaMalloc(&p, 64)) != cudaSuccess) return cudaFail(e, "workspace scalars");
+  c->owned.push_back(p); c->invMax = (unsigned long long*)p;
+  c->flag = (int*)((char*)p + 16);
+  return HC_OK;
+}
+
+StageArgs levelArgs(hc_ctx* c, const double* w) {
+  StageArgs a{};
+  a.L = c->L;
+  a.w = w;
+  a.wBoxStride = NC * c->L.Ng;
+  a.wN = c->L.Ng;
+  for (int d = 0; d < 3; ++d) a.wlo[d] = -kGhost;
+  a.wn[0] = c->L.n0; a.wn[1] = c->L.n1; a.wn[2] = c->L.n1;
+  a.lo[0] = a.lo[1] = a.lo[2] = 0;
+  a.hi[0] = c->P.nr - 1; a.hi[1] = a.hi[2] = c->P.na - 1;
+  a.nbox = 6;
+  a.block0 = 0;
+  a.scale = 1.0;
+  a.seams = 1;
+  return a;
+}
+
+int checkLaunch(cudaError_t e, const char* what) { return e == cudaSuccess ? HC_OK : cudaFail(e, what); }
+
+// One RK4 stage: prepare primitives of `src` then the fused operator + update.
+int rkStage(hc_ctx* c, const double* src, double* ju, int stage, double dtv, const double* invMax, double tbase,
+            const double* tdev, cudaStream_t s) {
+  static const double c4[4] = {0, 0.5, 0.5, 1};
+  int rc;
+  if ((rc = checkLaunch(launchPrimValid(c->L, src, c->W, s), "prim")) != HC_OK) return rc;
+  StageTime st{tbase, tdev, c4[stage], invMax, dtv};
+  if ((rc = checkLaunch(launchGhosts(c->L, c->W, st, s), "ghosts")) != HC_OK) return rc;
+  StageArgs a = levelArgs(c, c->W);
+  a.stage = stage;
+  a.invDtMax = invMax;
+  a.dtv = dtv;
+  a.ju = ju;
+  a.acc = c->acc;
+  a.next = c->next;
+  a.invalid = nullptr;
+  return checkLaunch(launchStage(a, MODE_RK, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
+                                 c->P.sun_gravity == 1, s),
+                     "stage");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hc_last_error(void) { return g_lastError.c_str(); }
+
+int hc_ctx_create(const hc_params* p, int device, hc_ctx** out) {
+  if (!p || !out) return fail(HC_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (p->spatial_order != 2) return fail(HC_ERR_UNSUPPORTED, "spatial_order must be 2 (PLM operator)");
+  if (p->limiter < 0 || p->limiter > 3) return fail(HC_ERR_ARG, "limiter must be 0..3");
+  if (p->riemann_solver != 1 && p->riemann_solver != 2) return fail(HC_ERR_ARG, "Riemann_solver_type must be 1 or 2");
+  if (p->temporal_order != 4) return fail(HC_ERR_UNSUPPORTED, "temporal_order must be 4 (classical RK4)");
+  if (p->nr < 4 || p->na < 4) return fail(HC_ERR_ARG, "need nr >= 4 and na >= 4");
+  if (!(p->gamma > 1.0)) return fail(HC_ERR_ARG, "gamma must exceed 1");
+  if (!(p->inner_radius > 0.0 && p->outer_radius > p->inner_radius))
+    return fail(HC_ERR_ARG, "need 0 < inner_radius < outer_radius");
+  if (p->init_condition_type != 1) return fail(HC_ERR_UNSUPPORTED, "radial boundary family must be 1 (analytic wind)");
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cudaFail(e, "cudaSetDevice");
+  hc_ctx* c = new (std::nothrow) hc_ctx;
+  if (!c) return fail(HC_ERR_NOMEM, "context allocation");
+  c->P = *p;
+  c->device = device;
+  int rc = buildLevel(c);
+  if (rc == HC_OK) rc = allocWorkspace(c);
+  if (rc != HC_OK) {
+    hc_ctx_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return HC_OK;
+}
+
+int hc_ctx_destroy(hc_ctx* c) {
+  if (!c) return HC_OK;
+  cudaSetDevice(c->device);
+  for (void* p : c->owned) cudaFree(p);
+  delete c;
+  return HC_OK;
+}
+
+size_t hc_level_state_size(const hc_ctx* c) { return c ? 6 * NC * (size_t)c->L.Nv : 0; }
+size_t hc_level_primitive_size(const hc_ctx* c) { return c ? 6 * NC * (size_t)c->L.Ng : 0; }
+
+int hc_box_rhs(hc_ctx* c, const hc_box* box, const double* w, const double* const* panel, double scale, double* rhs,
+               double* const* flux, void* stream) {
+  if (!c || !box || !w || !rhs) return fail(HC_ERR_ARG, "null argument");
+  const hc_box& B = *box;
+  if (B.block < 0 || B.block > 5) return fail(HC_ERR_ARG, "block must be 0..5");
+  if (B.ghost < 2) return fail(HC_ERR_ARG, "the PLM operator needs ghost >= 2");
+  const int n[3] = {c->P.nr, c->P.na, c->P.na};
+  for (int d = 0; d < 3; ++d)
+    if (B.lo[d] < 0 || B.hi[d] >= n[d] || B.hi[d] < B.lo[d]) return fail(HC_ERR_ARG, "box outside the panel");
+  StageArgs a{};
+  a.L = c->L;
+  a.w = w;
+  for (int d = 0; d < 3; ++d) {
+    a.wlo[d] = B.lo[d] - B.ghost;
+    a.wn[d] = B.hi[d] - B.lo[d] + 1 + 2 * B.ghost;
+    a.lo[d] = B.lo[d];
+    a.hi[d] = B.hi[d];
+  }
+  a.wN = (long)a.wn[0] * a.wn[1] * a.wn[2];
+  a.wBoxStride = 0;
+  a.nbox = 1;
+  a.block0 = B.block;
+  a.scale = scale;
+  a.rhs = rhs;
+  a.rhsN = (long)(B.hi[0] - B.lo[0] + 1) * (B.hi[1] - B.lo[1] + 1) * (B.hi[2] - B.lo[2] + 1);
+  for (int d = 0; d < 3; ++d) a.flux[d] = flux ? flux[d] : nullptr;
+  for (int q = 0; q < 6; ++q) a.panel[q] = panel ? panel[q] : nullptr;
+  return checkLaunch(launchStage(a, MODE_BOX, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
+                                 false, (cudaStream_t)stream),
+                     "hc_box_rhs");
+}
+
+int hc_box_gravity(hc_ctx* c, const hc_box* box, const double* w, double* rhs, void* stream) {
+  if (!c || !box || !w || !rhs) return fail(HC_ERR_ARG, "null argument");
+  const hc_box& B = *box;
+  if (B.block < 0 || B.block > 5) return fail(HC_ERR_ARG, "block must be 0..5");
+  const int n[3] = {c->P.nr, c->P.na, c->P.na};
+  int wlo[3], wn[3];
+  for (int d = 0; d < 3; ++d) {
+    if (B.lo[d] < 0 || B.hi[d] >= n[d] || B.hi[d] < B.lo[d]) return fail(HC_ERR_ARG, "box outside the panel");
+    wlo[d] = B.lo[d] - B.ghost;
+    wn[d] = B.hi[d] - B.lo[d] + 1 + 2 * B.ghost;
+  }
+  return checkLaunch(launchBoxGravity(c->L, B.lo, B.hi, B.block, w, wlo, wn, rhs, (cudaStream_t)stream), "hc_box_gravity");
+}
+
+int hc_level_prepare(hc_ctx* c, const double* ju, double* w, double t, void* stream) {
+  if (!c || !ju || !w) return fail(HC_ERR_ARG, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = checkLaunch(launchPrimValid(c->L, ju, w, s), "prim");
+  if (rc != HC_OK) return rc;
+  StageTime st{t, nullptr, 0.0, nullptr, 0.0};
+  return checkLaunch(launchGhosts(c->L, w, st, s), "ghosts");
+}
+
+int hc_level_rhs(hc_ctx* c, const double* w, double* k, void* stream) {
+  if (!c || !w || !k) return fail(HC_ERR_ARG, "null argument");
+  StageArgs a = levelArgs(c, w);
+  a.rhs = k;
+  return checkLaunch(launchStage(a, MODE_RHS, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
+                                 c->P.sun_gravity == 1, (cudaStream_t)stream),
+                     "hc_level_rhs");
+}
+
+int hc_level_rk4_step(hc_ctx* c, double* ju, double dt, double t, void* stream) {
+  if (!c || !ju) return fail(HC_ERR_ARG, "null argument");
+  if (!(dt > 0)) return fail(HC_ERR_ARG, "dt must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int stage = 0; stage < 4; ++stage) {
+    const int rc = rkStage(c, stage == 0 ? ju : c->next, ju, stage, dt, nullptr, t, nullptr, s);
+    if (rc != HC_OK) return rc;
+  }
+  return HC_OK;
+}
+
+int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, double* dt_dev, void* stream) {
+  if (!c || !ju || nsteps < 0) return fail(HC_ERR_ARG, "bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  const double* invMax = reinterpret_cast<const double*>(c->invMax);
+  for (int n = 0; n < nsteps; ++n) {
+    int rc = checkLaunch(launchCfl(c->L, ju, c->invMax, s), "cfl");
+    if (rc != HC_OK) return rc;
+    for (int stage = 0; stage < 4; ++stage) {
+      rc = rkStage(c, stage == 0 ? ju : c->next, ju, stage, 0.0, invMax, 0.0, time_dev, s);
+      if (rc != HC_OK) return rc;
+    }
+    rc = checkLaunch(launchAdvanceTime(time_dev, invMax, c->P.cfl, dt_dev, s), "time");
+    if (rc != HC_OK) return rc;
+  }
+  return HC_OK;
+}
+
+int hc_level_dt_cfl(hc_ctx* c, const double* ju, double* inv_dt_max, void* stream) {
+  if (!c || !ju || !inv_dt_max) return fail(HC_ERR_ARG, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = checkLaunch(launchCfl(c->L, ju, c->invMax, s), "cfl");
+  if (rc != HC_OK) return rc;
+  return checkLaunch(launchBitsToDouble(c->invMax, inv_dt_max, s), "cfl copy");
+}
+
+int hc_level_valid(hc_ctx* c, const double* ju, int* ok, void* stream) {
+  if (!c || !ju || !ok) return fail(HC_ERR_ARG, "null argument");
+  return checkLaunch(launchValid(c->L, ju, ok, (cudaStream_t)stream), "valid");
+}
+
+int hc_level_init(hc_ctx* c, const hc_init* in, double* ju, void* stream) {
+  if (!c || !in || !ju) return fail(HC_ERR_ARG, "null argument");
+  if (in->kind != 1) return fail(HC_ERR_UNSUPPORTED, "init kind must be 1");
+  if (in->pulse_block < 0 || in->pulse_block > 5) return fail(HC_ERR_ARG, "pulse_block must be 0..5");
+  struct InitArgsHost {
+    int kind, pb, pi, pj, pk;
+    double rho0, p0, vr, b0, r_ref, amp, width;
+    double cx[3];
+  } a;
+  a.kind = in->kind; a.pb = in->pulse_block; a.pi = in->pulse_i; a.pj = in->pulse_j; a.pk = in->pulse_k;
+  a.rho0 = in->rho0; a.p0 = in->p0; a.vr = in->vr; a.b0 = in->b0; a.r_ref = in->r_ref;
+  a.amp = in->pulse_amp; a.width = in->pulse_width;
+  const double h = 1.0 / c->P.na;
+  double A[3][3];
+  basisAt(in->pulse_block, (in->pulse_j + 0.5) * h, (in->pulse_k + 0.5) * h, A, a.cx);
+  return checkLaunch(launchInit(c->L, &a, ju, (cudaStream_t)stream), "init");
+}
+
+long hc_geometry_export(const hc_ctx* c, int what, double* out) {
+  if (!c) return -1;
+  const std::vector<double>* v = nullptr;
+  if (what == 0) v = &c->radialExport;
+  else if (what >= 1 && what <= 3) v = &c->normalExport[what - 1];
+  else if (what == 4) v = &c->detExport;
+  else if (what == 5) v = &c->detAAExport;
+  else return -1;
+  if (out) std::memcpy(out, v->data(), v->size() * sizeof(double));
+  return (long)v->size();
+}
+
+}  // extern "C"

@@ -1,0 +1,632 @@
+// sm_100a kernels of the second-order (PLM) per-box MHD update and the RK4
+// stage that consumes it.  FP64 throughout.
+//
+// o2StageKernel -- one CTA per TX x TY x TZ cell tile of one box.  Phase 1
+// computes every face of the tile in all three directions (flat loop over
+// faces, radial index fastest so stencil loads are coalesced) and keeps the
+// face fluxes in shared memory; phase 2 forms the flux divergence, Powell and
+// gravity sources per cell and either accumulates the per-box rhs or applies
+// the RK4 stage update in registers (k never goes to HBM).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hc_device.cuh"
+#include "hc_level.h"
+
+namespace hc {
+
+namespace {
+
+constexpr int TX = 16, TY = 4, TZ = 2;
+constexpr int NT = TX * TY * TZ;
+constexpr int NF0 = (TX + 1) * TY * TZ, NF1 = TX * (TY + 1) * TZ, NF2 = TX * TY * (TZ + 1);
+constexpr int NF = NF0 + NF1 + NF2;
+
+__device__ __forceinline__ long cellOffset(int i, int j, int k, const int lo[3], const int n[3]) {
+  return (long)(i - lo[0]) + (long)n[0] * ((long)(j - lo[1]) + (long)n[1] * (long)(k - lo[2]));
+}
+
+// Cartesian primitives from native conserved u through the cell basis A
+// (src/BoxOp_SecondOrderPreStage.H:199-214).
+__device__ __forceinline__ void nativeToPrimitive(const double u[8], const double* A, double gamma, double out[8]) {
+  double ww[8];
+  ww[0] = u[0];
+  ww[4] = u[4];
+#pragma unroll
+  for (int grp = 0; grp < 2; ++grp) {
+    const int st = grp == 0 ? 1 : 5;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) ww[st + d] = A[3 * d] * u[st] + A[3 * d + 1] * u[st + 1] + A[3 * d + 2] * u[st + 2];
+  }
+  cartesianPrimitiveFromConserved(out, ww, 1.0, gamma);
+}
+
+// Analytic inner wind, src/BoxOp_PreStage.H:7-47 (time-dependent form).
+__device__ void analyticWind(const DevLevel& L, const double X[3], double t, double u[8]) {
+  const double gam = L.gamma, r_BC = L.r0;
+  const double r = sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+  const double theta = atan2(sqrt(X[0] * X[0] + X[1] * X[1]), X[2]);
+  const double phi = atan2(X[1], X[0]);
+  const double p0 = 1.0e-7, rho0 = 700 * kMP, u0 = 500.0 * 1e5;
+  const double rho = rho0 * pow(r_BC / r, 2.0);
+  const double p = p0 * pow(r_BC / r, 2.0 * gam);
+  const double carr_rot_time = 25.38 * 24 * 60 * 60;
+  const double omega = 2.0 * kPi / carr_rot_time;
+  const double phit = phi - omega * t;
+  const double perturbationScale = L.strength / 100.0;
+  const double sinTheta = sin(theta);
+  const double angularPattern = pow(sinTheta, 5) * sin(5 * phit) + pow(sinTheta, 10) * sin(10 * phit);
+  const double ur = u0 - perturbationScale * u0 / 3 * angularPattern;
+  u[0] = rho;
+  u[1] = ur * rho;
+  u[2] = u[3] = u[5] = u[6] = u[7] = 0.0;
+  const double umag = sqrt(u[1] * u[1]) / u[0];
+  u[4] = p / (gam - 1.0) + 0.5 * u[0] * umag * umag + 0.0 / 8.0 / kPi;
+}
+
+// ---------------------------------------------------------------------------
+// One face of the second-order operator (src/BoxOp_SecondOrder.H:257-324).
+// ---------------------------------------------------------------------------
+template <int LIM, bool ROE, int MODE>
+__device__ __forceinline__ void o2Face(const StageArgs& a, const double* __restrict__ w, int block, int dir, int i,
+                                       int j, int k, double out[8], double& bf, bool powell) {
+  const DevLevel& L = a.L;
+  const long sN = a.wN;
+  const long c0 = cellOffset(i, j, k, a.wlo, a.wn);
+  const long step = dir == 0 ? 1L : dir == 1 ? (long)a.wn[0] : (long)a.wn[0] * a.wn[1];
+  double l[8], r[8];
+#pragma unroll
+  for (int q = 0; q < NC; ++q) {
+    const double* s = w + q * sN + c0;
+    plmComponent<LIM>(__ldg(s - 2 * step), __ldg(s - step), __ldg(s), __ldg(s + step), l[q], r[q]);
+  }
+  // Complete-state fallbacks (src/BoxOp_SecondOrder.H:32-36).
+  if (!(l[0] >= kRHO00 && l[4] >= 0)) {
+#pragma unroll
+    for (int q = 0; q < NC; ++q) l[q] = __ldg(w + q * sN + c0 - step);
+  }
+  if (!(r[0] >= kRHO00 && r[4] >= 0)) {
+#pragma unroll
+    for (int q = 0; q < NC; ++q) r[q] = __ldg(w + q * sN + c0);
+  }
+  if (dir > 0) {
+    const int idx = dir == 1 ? j : k;
+    if (MODE == MODE_BOX) {
+      // Caller-supplied adjacent-panel states (src/BoxOp_SecondOrder.H:252-281).
+      const double* pl = a.panel[2 * dir];
+      const double* ph = a.panel[2 * dir + 1];
+      const bool atLo = pl && idx == a.lo[dir], atHi = ph && idx == a.hi[dir] + 1;
+      if (atLo || atHi) {
+        const int v0 = a.hi[0] - a.lo[0] + 1, v1 = a.hi[1] - a.lo[1] + 1, v2 = a.hi[2] - a.lo[2] + 1;
+        const int s1 = dir == 1 ? 1 : v1;
+        const long sidx = (long)(i - a.lo[0]) + (long)v0 * ((dir == 1 ? 0 : j - a.lo[1]) + (long)s1 * (dir == 2 ? 0 : k - a.lo[2]));
+        const long sN2 = (long)v0 * s1 * (dir == 2 ? 1 : v2);
+        const double* src = atLo ? pl : ph;
+        double* dst = atLo ? l : r;
+#pragma unroll
+        for (int q = 0; q < NC; ++q) dst[q] = src[q * sN2 + sidx];
+      }
+    } else if (a.seams && (idx == 0 || idx == L.na)) {
+      // Shared seam state: the adjacent panel's reconstruction from its own
+      // cells at the same physical face (src/BoxOp_SecondOrder.H:68-121).
+      const int side = idx == 0 ? 0 : 1;
+      const int e = (block * 2 + (dir - 1)) * 2 + side;
+      const EdgeLink lk = L.edge[e];
+      const int s2 = L.faceMap[e * L.na + (dir == 1 ? k : j)];
+      const double* wn = a.w + (long)lk.nb * a.wBoxStride;
+      const int first = lk.side == 0 ? -1 : L.na - 2;
+      double st[3][8];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int n = first + q;
+        const long o = lk.axis == 1 ? cellOffset(i, n, s2, a.wlo, a.wn) : cellOffset(i, s2, n, a.wlo, a.wn);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) st[q][c] = __ldg(wn + c * sN + o);
+      }
+      if (lk.side == 0) {
+        if (side == 0) plmRight<LIM>(st[0], st[1], st[2], l);
+        else plmRight<LIM>(st[0], st[1], st[2], r);
+      } else {
+        if (side == 0) plmLeft<LIM>(st[0], st[1], st[2], l);
+        else plmLeft<LIM>(st[0], st[1], st[2], r);
+      }
+    }
+  }
+  const FaceGeom& g = L.face[((size_t)dir * 6 + block) * (L.na + 1) * (L.na + 1) + (size_t)k * (L.na + 1) + j];
+  const double4 rd = L.radial[i + L.g];
+  const double area = dir == 0 ? rd.x : rd.y;
+  secondOrderFaceFlux<ROE>(out, l, r, g, area, L.gamma, L.entropy);
+  if (powell) {
+    double f = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) f += 0.5 * (l[5 + d] + r[5 + d]) * g.n[d] * area;
+    bf = f;
+  }
+}
+
+template <int LIM, bool ROE, int MODE>
+__global__ void __launch_bounds__(NT) o2StageKernel(const StageArgs a, const int powell, const int grav) {
+  extern __shared__ double sF[];  // [9][NF]: 8 flux components + Powell face B_n
+  const int v0 = a.hi[0] - a.lo[0] + 1, v1 = a.hi[1] - a.lo[1] + 1, v2 = a.hi[2] - a.lo[2] + 1;
+  const int nbx = (v0 + TX - 1) / TX, nby = (v1 + TY - 1) / TY, nbz = (v2 + TZ - 1) / TZ;
+  int t = blockIdx.x;
+  const int bx = t % nbx; t /= nbx;
+  const int by = t % nby; t /= nby;
+  const int bz = t % nbz;
+  const int box = t / nbz;
+  const int block = a.block0 + box;
+  const int oi = a.lo[0] + bx * TX, oj = a.lo[1] + by * TY, ok = a.lo[2] + bz * TZ;
+  const double* __restrict__ w = a.w + (long)box * a.wBoxStride;
+
+  for (int f = threadIdx.x; f < NF; f += NT) {
+    int dir, fi, fj, fk;
+    if (f < NF0) { dir = 0; fi = f % (TX + 1); const int q = f / (TX + 1); fj = q % TY; fk = q / TY; }
+    else if (f < NF0 + NF1) { dir = 1; const int g = f - NF0; fi = g % TX; const int q = g / TX; fj = q % (TY + 1); fk = q / (TY + 1); }
+    else { dir = 2; const int g = f - NF0 - NF1; fi = g % TX; const int q = g / TX; fj = q % TY; fk = q / TY; }
+    const int i = oi + fi, j = oj + fj, k = ok + fk;
+    const bool valid = i <= a.hi[0] + (dir == 0) && j <= a.hi[1] + (dir == 1) && k <= a.hi[2] + (dir == 2);
+    double out[8];
+    double bf = 0;
+    if (valid) {
+      o2Face<LIM, ROE, MODE>(a, w, block, dir, i, j, k, out, bf, powell != 0);
+      if (MODE == MODE_BOX && a.flux[dir]) {
+        const int f0 = v0 + (dir == 0), f1 = v1 + (dir == 1), f2 = v2 + (dir == 2);
+        const long fidx = (long)(i - a.lo[0]) + (long)f0 * ((long)(j - a.lo[1]) + (long)f1 * (k - a.lo[2]));
+        const long fN = (long)f0 * f1 * f2;
+#pragma unroll
+        for (int q = 0; q < NC; ++q) a.flux[dir][q * fN + fidx] = out[q];
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < NC; ++q) out[q] = 0;
+    }
+#pragma unroll
+    for (int q = 0; q < NC; ++q) sF[q * NF + f] = out[q];
+    sF[8 * NF + f] = bf;
+  }
+  __syncthreads();
+
+  const int li = threadIdx.x % TX, lj = (threadIdx.x / TX) % TY, lk = threadIdx.x / (TX * TY);
+  const int i = oi + li, j = oj + lj, k = ok + lk;
+  if (i > a.hi[0] || j > a.hi[1] || k > a.hi[2]) return;
+  const DevLevel& L = a.L;
+  const long cw = cellOffset(i, j, k, a.wlo, a.wn);
+  double kv[8];
+  long vidx = 0;
+  if (MODE == MODE_BOX) {
+    vidx = (long)(i - a.lo[0]) + (long)v0 * ((long)(j - a.lo[1]) + (long)v1 * (k - a.lo[2]));
+#pragma unroll
+    for (int q = 0; q < NC; ++q) kv[q] = a.rhs[q * a.rhsN + vidx];
+  } else {
+    vidx = (long)box * NC * L.Nv + (long)i + (long)L.nr * ((long)j + (long)L.na * k);
+#pragma unroll
+    for (int q = 0; q < NC; ++q) kv[q] = 0.0;
+    if (grav) {
+      // src/BoxOp_Gravity.H:36-58
+      const GravCell gc = L.grav[((size_t)block * L.na + k) * L.na + j];
+      const double factor = -kGrav * kMsun * L.radial[i + L.g].z * __ldg(w + cw);
+      double radialVelocity = 0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        kv[1 + d] += factor * gc.a0[d];
+        radialVelocity += gc.x[d] * __ldg(w + (1 + d) * a.wN + cw);
+      }
+      kv[4] += factor * gc.det * radialVelocity;
+    }
+  }
+  const int fl[3] = {li + (TX + 1) * (lj + TY * lk), NF0 + li + TX * (lj + (TY + 1) * lk), NF0 + NF1 + li + TX * (lj + TY * lk)};
+  const int fs[3] = {1, TX, TX * TY};
+  const double coef[3] = {-a.scale / L.dxi0, -a.scale / L.h, -a.scale / L.h};
+  double md = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+#pragma unroll
+    for (int q = 0; q < NC; ++q) kv[q] += coef[d] * (sF[q * NF + fl[d] + fs[d]] - sF[q * NF + fl[d]]);
+    if (powell) md += coef[d] * (sF[8 * NF + fl[d] + fs[d]] - sF[8 * NF + fl[d]]);
+  }
+  if (powell) {
+    // src/BoxOp_SecondOrder.H:351-369
+    double vb = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double b = __ldg(w + (5 + d) * a.wN + cw), vel = __ldg(w + (1 + d) * a.wN + cw);
+      kv[1 + d] += md * b / (4 * kPi);
+      kv[5 + d] += md * vel;
+      vb += vel * b;
+    }
+    kv[4] += md * vb / (4 * kPi);
+  }
+  if (MODE == MODE_BOX) {
+#pragma unroll
+    for (int q = 0; q < NC; ++q) a.rhs[q * a.rhsN + vidx] = kv[q];
+    return;
+  }
+  if (MODE == MODE_RHS) {
+#pragma unroll
+    for (int q = 0; q < NC; ++q) a.rhs[vidx + q * L.Nv] = kv[q];
+    return;
+  }
+  // Classical RK4 (src/MHD_AMRRungeKutta.H:10-12): stage = U + (dt a) k,
+  // U_new = U + sum_s (dt b_s) k_s accumulated in stage order.
+  const double dt = a.invDtMax ? L.cfl_number / *a.invDtMax : a.dtv;
+  constexpr double b4[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+  constexpr double a4[3] = {0.5, 0.5, 1.0};
+  const long N = L.Nv;
+  if (a.stage == 0) {
+    const double fb = dt * b4[0], fa = dt * a4[0];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      const double u = a.ju[vidx + q * N];
+      a.acc[vidx + q * N] = u + fb * kv[q];
+      a.next[vidx + q * N] = u + fa * kv[q];
+    }
+  } else if (a.stage < 3) {
+    const double fb = dt * b4[a.stage], fa = dt * a4[a.stage];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      a.acc[vidx + q * N] = a.acc[vidx + q * N] + fb * kv[q];
+      a.next[vidx + q * N] = a.ju[vidx + q * N] + fa * kv[q];
+    }
+  } else {
+    const double fb = dt * b4[3];
+    bool bad = false;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      const double u = a.acc[vidx + q * N] + fb * kv[q];
+      a.ju[vidx + q * N] = u;
+      bad = bad || !isfinite(u) || (q == 0 && !(u > 0));
+    }
+    if (bad && a.invalid) atomicOr(a.invalid, 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stage preparation (src/BoxOp_SecondOrderPreStage.H:7-218).
+// ---------------------------------------------------------------------------
+__global__ void primValidKernel(const DevLevel L, const double* __restrict__ ju, double* __restrict__ w) {
+  const long n = 6L * L.Nv;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(t / L.Nv);
+    const long r = t - (long)b * L.Nv;
+    const int i = (int)(r % L.nr);
+    const int j = (int)((r / L.nr) % L.na);
+    const int k = (int)(r / ((long)L.nr * L.na));
+    double in[8], out[8];
+    const double* src = ju + (long)b * NC * L.Nv + r;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) in[c] = src[c * L.Nv];
+    const double invJ = 1.0 / (L.radial[i + L.g].w * L.grav[((size_t)b * L.na + k) * L.na + j].det);
+    cartesianPrimitiveFromConserved(out, in, invJ, L.gamma);
+    double* dst = w + (long)b * NC * L.Ng + (long)(i + L.g) + (long)L.n0 * ((long)(j + L.g) + (long)L.n1 * (k + L.g));
+#pragma unroll
+    for (int c = 0; c < NC; ++c) dst[c * L.Ng] = out[c];
+  }
+}
+
+__device__ __forceinline__ long gIdx(const DevLevel& L, int b, int i, int j, int k) {
+  return (long)b * NC * L.Ng + (long)(i + L.g) + (long)L.n0 * ((long)(j + L.g) + (long)L.n1 * (k + L.g));
+}
+
+__global__ void ghostsKernel(const DevLevel L, double* __restrict__ w, const StageTime st) {
+  const long nSeam = 6L * 2 * 2 * L.g * L.na * L.nr;
+  const long nRad = 6L * L.na * L.na;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nSeam + nRad; t += (long)gridDim.x * blockDim.x) {
+    if (t < nSeam) {
+      // Panel-seam ghost: 4-point along-edge interpolation of the adjacent
+      // panel's Cartesian primitives, then the floors of :70-75.
+      const int i = (int)(t % L.nr);
+      long q = t / L.nr;
+      const int s = (int)(q % L.na); q /= L.na;
+      const int m = (int)(q % L.g); q /= L.g;
+      const int side = (int)(q % 2); q /= 2;
+      const int ax = (int)(q % 2);
+      const int b = (int)(q / 2);
+      const SeamDonor dn = L.seam[((((long)b * 2 + ax) * 2 + side) * L.g + m) * L.na + s];
+      const int n = side == 0 ? -1 - m : L.na + m;
+      const int gj = ax == 0 ? n : s, gk = ax == 0 ? s : n;
+      double v[8];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        double acc = 0.;
+#pragma unroll
+        for (int d = 0; d < 4; ++d) acc += dn.w[d] * w[gIdx(L, dn.b, i, dn.j[d], dn.k[d]) + c * L.Ng];
+        v[c] = acc;
+      }
+      v[0] = dmax(v[0], kRHO00);
+      v[4] = dmax(v[4], 0.0);
+      const long o = gIdx(L, b, i, gj, gk);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) w[o + c * L.Ng] = v[c];
+    } else {
+      const long r = t - nSeam;
+      const int j = (int)(r % L.na);
+      const int k = (int)((r / L.na) % L.na);
+      const int b = (int)(r / ((long)L.na * L.na));
+      const size_t cidx = ((size_t)b * L.na + k) * L.na + j;
+      const double* A = L.basis + cidx * 9;
+      // Inner radial ghosts: analytic wind (src/BoxOp_PreStage.H:215-228).
+      if (L.innerBCType == 1) {
+        for (int i = -L.g; i < 0; ++i) {
+          double u[8], out[8];
+          if (L.innerBC) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) u[c] = L.innerBC[(cidx * L.g + (i + L.g)) * NC + c];
+          } else {
+            const double dt = st.invDtMax ? L.cfl_number / *st.invDtMax : st.dtv;
+            const double time = st.tbase + (st.tdev ? *st.tdev : 0.0) + st.cfrac * dt;
+            const GravCell gc = L.grav[cidx];
+            const double radius = L.rc[i + L.g];
+            const double X[3] = {radius * gc.x[0], radius * gc.x[1], radius * gc.x[2]};
+            analyticWind(L, X, time, u);
+          }
+          nativeToPrimitive(u, A, L.gamma, out);
+          const long o = gIdx(L, b, i, j, k);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) w[o + c * L.Ng] = out[c];
+        }
+      }
+      // Outer radial ghosts: copy the last owned layer in the native basis,
+      // scaled by (r_last/r)^2 (B tangential: ^1) (src/BoxOp_PreStage.H:105-141).
+      const double* Ai = L.basisInv + cidx * 9;
+      double wl[8], u[8];
+      const long ol = gIdx(L, b, L.nr - 1, j, k);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) wl[c] = w[ol + c * L.Ng];
+      u[0] = wl[0];
+      double kinetic = 0, magnetic = 0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        kinetic += 0.5 * wl[0] * wl[1 + d] * wl[1 + d];
+        magnetic += wl[5 + d] * wl[5 + d] / (8 * kPi);
+        u[1 + d] = Ai[3 * d] * wl[0] * wl[1] + Ai[3 * d + 1] * wl[0] * wl[2] + Ai[3 * d + 2] * wl[0] * wl[3];
+        u[5 + d] = Ai[3 * d] * wl[5] + Ai[3 * d + 1] * wl[6] + Ai[3 * d + 2] * wl[7];
+      }
+      u[4] = (wl[4] - 0.0) / (L.gamma - 1.0) + kinetic + magnetic;
+      for (int m = 0; m < L.g; ++m) {
+        double ug[8], out[8];
+        const double s2 = L.outerScale2[m], s1 = L.outerScale1[m];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) ug[c] = u[c] * s2;
+        ug[6] = u[6] * s1;
+        ug[7] = u[7] * s1;
+        nativeToPrimitive(ug, A, L.gamma, out);
+        const long o = gIdx(L, b, L.nr + m, j, k);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) w[o + c * L.Ng] = out[c];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CFL rate (src/BoxOp_SecondOrderCFL.H:117-209): max over cells of
+// sum_d (fast bound + |v|)/width_d.  Warp-shuffle then one atomic per warp.
+// ---------------------------------------------------------------------------
+__global__ void cflKernel(const DevLevel L, const double* __restrict__ ju, unsigned long long* invMaxBits) {
+  const long n = 6L * L.Nv;
+  double best = 0.0;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(t / L.Nv);
+    const long r = t - (long)b * L.Nv;
+    const int i = (int)(r % L.nr);
+    const int j = (int)((r / L.nr) % L.na);
+    const int k = (int)(r / ((long)L.nr * L.na));
+    const CflCell& a = L.cfl[((size_t)b * L.na + k) * L.na + j];
+    const double4 rd = L.radial[i + L.g];
+    const double volume = rd.w, inverseVolume = 1.0 / rd.w, width0 = rd.z * L.dxi0;
+    const double area[3] = {rd.x, rd.y, rd.y};
+    double u[8];
+    const double* src = ju + (long)b * NC * L.Nv + r;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) u[c] = src[c * L.Nv];
+    double rho = u[0] * a.inverseDet;
+    rho *= inverseVolume;
+    rho = dmax(rho, kRHO00);
+    double energy = u[4] * a.inverseDet;
+    energy *= inverseVolume;
+    double v[3], bb[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      v[d] = a.inverseDetA[3 * d] * u[1] + a.inverseDetA[3 * d + 1] * u[2] + a.inverseDetA[3 * d + 2] * u[3];
+      bb[d] = a.inverseDetA[3 * d] * u[5] + a.inverseDetA[3 * d + 1] * u[6] + a.inverseDetA[3 * d + 2] * u[7];
+      v[d] *= inverseVolume;
+      bb[d] *= inverseVolume;
+      v[d] /= rho;
+    }
+    double kinetic = 0, magnetic = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double vc = a.cell[3 * d] * v[0] + a.cell[3 * d + 1] * v[1] + a.cell[3 * d + 2] * v[2];
+      const double bc = a.cell[3 * d] * bb[0] + a.cell[3 * d + 1] * bb[1] + a.cell[3 * d + 2] * bb[2];
+      kinetic += vc * vc / 2;
+      magnetic += bc * bc / 8.0 / kPi;
+    }
+    kinetic *= rho;
+    double pressure = (energy - kinetic - magnetic) * (L.gamma - 1);
+    if (pressure < 0) pressure = 0;
+    double inverseDt = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double* basis = d == 0 ? a.cell : a.face[d - 1];
+      double v2 = 0, fullB2 = 0;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const double velocity = basis[3 * q] * v[0] + basis[3 * q + 1] * v[1] + basis[3 * q + 2] * v[2];
+        const double field = basis[3 * q] * bb[0] + basis[3 * q + 1] * bb[1] + basis[3 * q + 2] * bb[2];
+        v2 += velocity * velocity;
+        fullB2 += field * field;
+      }
+      const double width = d == 0 ? width0 : volume * a.det[d] * L.h / area[d] / a.normal[d];
+      const double wave = sqrt(L.gamma * pressure / rho + fullB2 / 4.0 / kPi / rho);
+      inverseDt += (wave + sqrt(v2)) / width;
+    }
+    // std::max(localMaximum, x) ignores a NaN x.
+    best = best < inverseDt ? inverseDt : best;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double other = __shfl_xor_sync(0xffffffffu, best, o);
+    best = best < other ? other : best;
+  }
+  if ((threadIdx.x & 31) == 0 && best > 0) atomicMax(invMaxBits, (unsigned long long)__double_as_longlong(best));
+}
+
+__global__ void setIntKernel(int* p, int v) { *p = v; }
+
+// src/BoxOp_EulerCubedSphereImplem.H:817-876: finite components, rho > 0.
+__global__ void validKernel(const DevLevel L, const double* __restrict__ ju, int* ok) {
+  const long n = 6L * NC * L.Nv;
+  bool bad = false;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const double v = ju[t];
+    const int c = (int)((t / L.Nv) % NC);
+    bad = bad || !isfinite(v) || (c == 0 && !(v > 0));
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(ok, 0);
+}
+
+// Seeded synthetic initial state, kind 1 (formula in hc_abi.h / DESIGN.md).
+struct InitArgs {
+  int kind, pb, pi, pj, pk;
+  double rho0, p0, vr, b0, r_ref, amp, width;
+  double cx[3];
+};
+
+__global__ void initKernel(const DevLevel L, const InitArgs in, double* __restrict__ ju) {
+  const long n = 6L * L.Nv;
+  const double dang = kPi / 2 * L.h;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(t / L.Nv);
+    const long r = t - (long)b * L.Nv;
+    const int i = (int)(r % L.nr);
+    const int j = (int)((r / L.nr) % L.na);
+    const int k = (int)(r / ((long)L.nr * L.na));
+    const GravCell gc = L.grav[((size_t)b * L.na + k) * L.na + j];
+    const double* X = gc.x;
+    const double cr0 = X[1] * in.cx[2] - X[2] * in.cx[1], cr1 = X[2] * in.cx[0] - X[0] * in.cx[2],
+                 cr2 = X[0] * in.cx[1] - X[1] * in.cx[0];
+    const double ang = atan2(sqrt(cr0 * cr0 + cr1 * cr1 + cr2 * cr2), X[0] * in.cx[0] + X[1] * in.cx[1] + X[2] * in.cx[2]);
+    const double da = ang / dang;
+    const double sgn = X[2] >= 0 ? 1.0 : -1.0;
+    const double4 rd = L.radial[i + L.g];
+    const double rc = L.rc[i + L.g];
+    const double s = in.r_ref / rc, s2 = s * s;
+    const double rho = in.rho0 * s2;
+    double p = in.p0 * pow(s, 2.0 * L.gamma);
+    const double di = (double)(i - in.pi);
+    const double d2 = di * di + da * da;
+    if (in.amp != 0) p = p * (1.0 + in.amp * exp(-d2 / (2.0 * in.width * in.width)));
+    const double br = in.b0 * s2 * sgn;
+    const double E = p / (L.gamma - 1.0) + 0.5 * rho * in.vr * in.vr + br * br / (8.0 * kPi);
+    const double J = rd.w * gc.det;
+    const double u[8] = {rho, rho * in.vr * X[0], rho * in.vr * X[1], rho * in.vr * X[2], E, br * X[0], br * X[1], br * X[2]};
+    double* dst = ju + (long)b * NC * L.Nv + r;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) dst[c * L.Nv] = J * u[c];
+  }
+}
+
+__global__ void boxGravityKernel(const DevLevel L, int lo0, int lo1, int lo2, int v0, int v1, int v2, int block,
+                                 const double* __restrict__ w, int wl0, int wl1, int wl2, int wn0, int wn1, long wN,
+                                 double* __restrict__ rhs) {
+  const long n = (long)v0 * v1 * v2;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = lo0 + (int)(t % v0);
+    const int j = lo1 + (int)((t / v0) % v1);
+    const int k = lo2 + (int)(t / ((long)v0 * v1));
+    const long s = (long)(i - wl0) + (long)wn0 * ((long)(j - wl1) + (long)wn1 * (k - wl2));
+    const GravCell gc = L.grav[((size_t)block * L.na + k) * L.na + j];
+    const double factor = -kGrav * kMsun * L.radial[i + L.g].z * w[s];
+    double radialVelocity = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      rhs[(1 + d) * n + t] += factor * gc.a0[d];
+      radialVelocity += gc.x[d] * w[(1 + d) * wN + s];
+    }
+    rhs[4 * n + t] += factor * gc.det * radialVelocity;
+  }
+}
+
+__global__ void advanceTimeKernel(double* time, const double* invDtMax, double cfl, double* dtOut) {
+  const double dt = cfl / *invDtMax;
+  if (time) *time += dt;
+  if (dtOut) *dtOut = dt;
+}
+
+int gridFor(long n, int threads) {
+  long g = (n + threads - 1) / threads;
+  const long cap = 148L * 16;
+  if (g > cap) g = cap;
+  return (int)(g < 1 ? 1 : g);
+}
+
+template <int LIM, bool ROE>
+cudaError_t launchStageT(const StageArgs& a, int mode, bool powell, bool grav, cudaStream_t s) {
+  const int v0 = a.hi[0] - a.lo[0] + 1, v1 = a.hi[1] - a.lo[1] + 1, v2 = a.hi[2] - a.lo[2] + 1;
+  const long blocks = (long)a.nbox * ((v0 + TX - 1) / TX) * ((v1 + TY - 1) / TY) * ((v2 + TZ - 1) / TZ);
+  const size_t smem = stageSmemBytes(mode);
+  if (mode == MODE_BOX) o2StageKernel<LIM, ROE, MODE_BOX><<<(unsigned)blocks, NT, smem, s>>>(a, powell, grav);
+  else if (mode == MODE_RK) o2StageKernel<LIM, ROE, MODE_RK><<<(unsigned)blocks, NT, smem, s>>>(a, powell, grav);
+  else o2StageKernel<LIM, ROE, MODE_RHS><<<(unsigned)blocks, NT, smem, s>>>(a, powell, grav);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t stageSmemBytes(int) { return sizeof(double) * 9 * NF; }
+
+cudaError_t launchStage(const StageArgs& a, int mode, int limiter, bool roe, bool powell, bool grav, cudaStream_t s) {
+  const int lim = limiter == 0 ? 0 : limiter == 3 ? 3 : 1;
+  if (lim == 0) return roe ? launchStageT<0, true>(a, mode, powell, grav, s) : launchStageT<0, false>(a, mode, powell, grav, s);
+  if (lim == 1) return roe ? launchStageT<1, true>(a, mode, powell, grav, s) : launchStageT<1, false>(a, mode, powell, grav, s);
+  return roe ? launchStageT<3, true>(a, mode, powell, grav, s) : launchStageT<3, false>(a, mode, powell, grav, s);
+}
+
+cudaError_t launchPrimValid(const DevLevel& L, const double* ju, double* w, cudaStream_t s) {
+  primValidKernel<<<gridFor(6L * L.Nv, 256), 256, 0, s>>>(L, ju, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launchGhosts(const DevLevel& L, double* w, const StageTime& t, cudaStream_t s) {
+  const long n = 6L * 2 * 2 * L.g * L.na * L.nr + 6L * L.na * L.na;
+  ghostsKernel<<<gridFor(n, 128), 128, 0, s>>>(L, w, t);
+  return cudaGetLastError();
+}
+
+cudaError_t launchCfl(const DevLevel& L, const double* ju, unsigned long long* invMaxBits, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(invMaxBits, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  cflKernel<<<gridFor(6L * L.Nv, 256), 256, 0, s>>>(L, ju, invMaxBits);
+  return cudaGetLastError();
+}
+
+cudaError_t launchValid(const DevLevel& L, const double* ju, int* ok, cudaStream_t s) {
+  setIntKernel<<<1, 1, 0, s>>>(ok, 1);
+  validKernel<<<gridFor(6L * NC * L.Nv, 256), 256, 0, s>>>(L, ju, ok);
+  return cudaGetLastError();
+}
+
+cudaError_t launchInit(const DevLevel& L, const void* init, double* ju, cudaStream_t s) {
+  initKernel<<<gridFor(6L * L.Nv, 256), 256, 0, s>>>(L, *static_cast<const InitArgs*>(init), ju);
+  return cudaGetLastError();
+}
+
+cudaError_t launchBoxGravity(const DevLevel& L, const int lo[3], const int hi[3], int block, const double* w,
+                             const int wlo[3], const int wn[3], double* rhs, cudaStream_t s) {
+  const int v0 = hi[0] - lo[0] + 1, v1 = hi[1] - lo[1] + 1, v2 = hi[2] - lo[2] + 1;
+  const long wN = (long)wn[0] * wn[1] * wn[2];
+  boxGravityKernel<<<gridFor((long)v0 * v1 * v2, 256), 256, 0, s>>>(L, lo[0], lo[1], lo[2], v0, v1, v2, block, w, wlo[0],
+                                                                     wlo[1], wlo[2], wn[0], wn[1], wN, rhs);
+  return cudaGetLastError();
+}
+
+cudaError_t launchAdvanceTime(double* time, const double* invDtMax, double cfl, double* dtOut, cudaStream_t s) {
+  advanceTimeKernel<<<1, 1, 0, s>>>(time, invDtMax, cfl, dtOut);
+  return cudaGetLastError();
+}
+
+cudaError_t launchBitsToDouble(const unsigned long long* bits, double* out, cudaStream_t s) {
+  return cudaMemcpyAsync(out, bits, sizeof(double), cudaMemcpyDeviceToDevice, s);
+}
+
+}  // namespace hc

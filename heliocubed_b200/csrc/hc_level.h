@@ -1,0 +1,121 @@
+// Level geometry and kernel argument structures shared by the host context
+// (hc_context.cpp) and the kernels (hc_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "hc_common.h"
+
+namespace hc {
+
+constexpr int kGhost = 2;  // ghost width of level primitive arrays (O2)
+
+// Seam ghost donor: 4-point along-edge interpolation in panel `b`.
+struct SeamDonor {
+  int b;
+  int j[4];
+  int k[4];
+  int pad;
+  double w[4];
+};
+
+// Neighbour across one panel edge (edge = (axis-1)*2 + side of this panel).
+struct EdgeLink {
+  int nb, axis, side, pad;
+};
+
+// CFL geometry of one angular cell, src/BoxOp_SecondOrderCFL.H:14-20.
+struct CflCell {
+  double inverseDet;
+  double inverseDetA[9];
+  double cell[9];
+  double face[2][9];
+  double det[3];
+  double normal[3];
+  double pad[2];
+};
+
+// Per-cell gravity / conversion data: Xhat at the centre, det, first column
+// of <det(A) A>, pad (src/BoxOp_Gravity.H:16-26).
+struct GravCell {
+  double x[3];
+  double det;
+  double a0[3];
+  double pad;
+};
+
+struct DevLevel {
+  int nr, na, g;
+  int n0, n1;            // ghosted dims nr+2g, na+2g
+  long Nv, Ng;           // cells per box: valid, ghosted
+  double h, dxi0;
+  const double4* radial; // [nr+2g+1], index i+g: {area0 (rlow^2), areaT, Dr0, vol}
+  const double* rc;      // [nr+2g+1], index i+g: cell-centre radius rhalf
+  const FaceGeom* face;  // [3][6][na+1][na+1]
+  const GravCell* grav;  // [6][na][na]
+  const double* basis;   // [6][na][na][9] cell-centre A, row-major
+  const double* basisInv;// [6][na][na][9]
+  const CflCell* cfl;    // [6][na][na]
+  const SeamDonor* seam; // [6][2][2][g][na]
+  const int* faceMap;    // [6][2][2][na]: neighbour along-edge index of a seam face
+  const EdgeLink* edge;  // [6][2][2]
+  const double* innerBC; // [6][na][na][g][8] native conserved wind, or null
+  double outerScale2[kGhost], outerScale1[kGhost];
+  double gamma, entropy, cfl_number, strength, r0;
+  int innerBCType;
+};
+
+// Operator launch: boxes share the valid region [lo,hi]; box b lies on panel
+// block0+b, its primitives start at w + b*wBoxStride on storage box
+// (wlo, wn), component stride wN.
+struct StageArgs {
+  DevLevel L;
+  const double* w;
+  long wBoxStride, wN;
+  int wlo[3], wn[3];
+  int lo[3], hi[3];
+  int nbox, block0;
+  double scale;
+  int seams;             // compute shared seam states from neighbour panels
+  // per-box outputs (MODE 0): rhs on valid (accumulated), flux on extrude(d)
+  double* rhs;
+  long rhsBoxStride, rhsN;
+  double* flux[3];
+  const double* panel[6];
+  // level RK stage (MODE 1): k never leaves registers
+  int stage;
+  const double* invDtMax;  // device: dt = cfl / *invDtMax (null: use dtv)
+  double dtv;
+  double* ju;
+  double* acc;
+  double* next;
+  int* invalid;            // OR-ed validity flag of the new state (stage 3)
+};
+
+enum { MODE_BOX = 0, MODE_RK = 1, MODE_RHS = 2 };
+
+// Host launchers (hc_kernels.cu).  Every launcher returns a cudaError_t.
+cudaError_t launchStage(const StageArgs& a, int mode, int limiter, bool roe, bool powell, bool grav,
+                        cudaStream_t s);
+cudaError_t launchPrimValid(const DevLevel& L, const double* ju, double* w, cudaStream_t s);
+// Time of a stage: t = tbase + (tdev ? *tdev : 0) + cfrac * dt, with
+// dt = invDtMax ? cfl / *invDtMax : dtv.
+struct StageTime {
+  double tbase;
+  const double* tdev;
+  double cfrac;
+  const double* invDtMax;
+  double dtv;
+};
+cudaError_t launchGhosts(const DevLevel& L, double* w, const StageTime& t, cudaStream_t s);
+cudaError_t launchCfl(const DevLevel& L, const double* ju, unsigned long long* invMaxBits, cudaStream_t s);
+cudaError_t launchValid(const DevLevel& L, const double* ju, int* ok, cudaStream_t s);
+cudaError_t launchInit(const DevLevel& L, const void* init, double* ju, cudaStream_t s);
+cudaError_t launchBoxGravity(const DevLevel& L, const int lo[3], const int hi[3], int block, const double* w,
+                             const int wlo[3], const int wn[3], double* rhs, cudaStream_t s);
+cudaError_t launchAdvanceTime(double* time, const double* invDtMax, double cfl, double* dtOut, cudaStream_t s);
+cudaError_t launchBitsToDouble(const unsigned long long* bits, double* out, cudaStream_t s);
+size_t stageSmemBytes(int mode);
+
+}  // namespace hc

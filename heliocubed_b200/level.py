@@ -1,0 +1,222 @@
+"""Host mirror of the reference's level/operator interface on one GPU.
+
+`Shell` owns an hc_ctx (the level geometry the reference caches in
+BoxOp_EulerCubedSphere::levelGeometry statics, src/BoxOp_EulerCubedSphere.H:
+348-368) and exposes, over device tensors, the calls the reference's drivers
+make:
+
+    Shell.prepare      preStageLevel / prepareSecondOrderPrimitives
+                       (src/BoxOp_PreStage.H:434-501)
+    Shell.rhs          StageLevel (src/BoxOp_EulerCubedSphereImplem.H:961-1012)
+    Shell.rk4_step     MBLevelRK::advance, order 4 (src/MHD_LevelRK.H:22-61)
+    Shell.advance      the uniform driver's CFL + RK4 loop (exec/main.cpp:369-440)
+    Shell.inv_dt_max   dtCFLSecondOrderHost (src/BoxOp_SecondOrderCFL.H:99-210)
+    Shell.valid        validConservedState (src/BoxOp_EulerCubedSphereImplem.H:817-876)
+    Shell.box_rhs      BoxOp_EulerCubedSphere::operator() on one box
+    Shell.box_gravity  gravitySecondOrderPrimitives (src/BoxOp_Gravity.H:3-82)
+
+All arithmetic runs in libhc_b200.so; torch supplies device memory and the
+current CUDA stream only.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+C_SR = 6.96e10          # cm, src/MHD_Constants.H:4
+C_MP = 1.67262192e-24   # g, src/MHD_Constants.H:5
+
+
+@dataclass
+class Params:
+    """Options of the second-order path (names follow src/Inputs_Parsing.H)."""
+    nr: int = 32
+    na: int = 32
+    spatial_order: int = 2
+    limiter: int = 3              # 0 unlimited, 1/2 minmod, 3 MC
+    riemann_solver: int = 1       # 1 Rusanov, 2 Roe 8-wave
+    divergence_cleaning: int = 1  # Powell
+    sun_gravity: int = 0
+    init_condition_type: int = 1  # analytic-wind inner boundary
+    temporal_order: int = 4
+    gamma: float = 5.0 / 3.0
+    entropy_fix_coeff: float = 0.3
+    cfl: float = 0.4
+    inner_radius: float = 21.5 * C_SR
+    outer_radius: float = 215.0 * C_SR
+    radial_stretch: float = 1.5
+    strength: float = 0.0
+
+    def to_c(self) -> N.HcParams:
+        p = N.HcParams()
+        for k in ("nr", "na", "spatial_order", "limiter", "riemann_solver", "divergence_cleaning",
+                  "sun_gravity", "init_condition_type", "temporal_order", "gamma", "entropy_fix_coeff",
+                  "cfl", "inner_radius", "outer_radius", "radial_stretch", "strength"):
+            setattr(p, k, getattr(self, k))
+        return p
+
+
+@dataclass
+class InitSpec:
+    """Seeded synthetic initial state (kind 1): Parker-like wind with a
+    Gaussian pressure pulse; see hc_init in include/hc_abi.h."""
+    pulse_block: int = 0
+    pulse_i: int = 0
+    pulse_j: int = 0
+    pulse_k: int = 0
+    rho0: float = 700.0 * C_MP
+    p0: float = 1.0e-7
+    vr: float = 400.0e5
+    b0: float = 5.0e-3
+    r_ref: float = 21.5 * C_SR
+    pulse_amp: float = 0.5
+    pulse_width: float = 3.0
+
+    def to_c(self) -> N.HcInit:
+        s = N.HcInit()
+        s.kind = 1
+        for k in ("pulse_block", "pulse_i", "pulse_j", "pulse_k", "rho0", "p0", "vr", "b0", "r_ref",
+                  "pulse_amp", "pulse_width"):
+            setattr(s, k, getattr(self, k))
+        return s
+
+    @staticmethod
+    def seeded(seed: int, nr: int, na: int, margin: int = 6) -> "InitSpec":
+        """Pulse centre at a seeded cell at least `margin` cells from every
+        panel edge (and from the radial boundaries when the grid allows)."""
+        rng = np.random.default_rng(seed)
+        def pick(n):
+            lo, hi = (margin, n - 1 - margin) if n - 1 - 2 * margin >= 0 else (0, n - 1)
+            return int(rng.integers(lo, hi + 1))
+        return InitSpec(pulse_block=int(rng.integers(0, 6)), pulse_i=pick(nr), pulse_j=pick(na), pulse_k=pick(na))
+
+
+def _ptr(t: torch.Tensor | None):
+    if t is None:
+        return None
+    if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+        raise ValueError("expected a contiguous float64 CUDA tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class Shell:
+    """One cubed-sphere level (six panels, one box each) on one GPU."""
+
+    def __init__(self, params: Params, device: int | None = None):
+        if not torch.cuda.is_available():
+            raise N.HcError("heliocubed_b200 needs a CUDA device; there is no CPU path")
+        self.params = params
+        self.device = torch.cuda.current_device() if device is None else device
+        self._lib = N.lib()
+        self._ctx = C.c_void_p()
+        self._cp = params.to_c()
+        with torch.cuda.device(self.device):
+            N.check(self._lib.hc_ctx_create(C.byref(self._cp), self.device, C.byref(self._ctx)), "hc_ctx_create")
+        self.nv = int(self._lib.hc_level_state_size(self._ctx))
+        self.ng = int(self._lib.hc_level_primitive_size(self._ctx))
+        self._scalar = torch.zeros(4, dtype=torch.float64, device=self._dev)
+        self._flag = torch.zeros(1, dtype=torch.int32, device=self._dev)
+
+    @property
+    def _dev(self) -> torch.device:
+        return torch.device("cuda", self.device)
+
+    @property
+    def cells(self) -> int:
+        return 6 * self.params.nr * self.params.na ** 2
+
+    def close(self) -> None:
+        if self._ctx:
+            self._lib.hc_ctx_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- storage ---------------------------------------------------------
+    def new_state(self) -> torch.Tensor:
+        return torch.zeros(self.nv, dtype=torch.float64, device=self._dev)
+
+    def new_primitive(self) -> torch.Tensor:
+        return torch.zeros(self.ng, dtype=torch.float64, device=self._dev)
+
+    def state_view(self, ju: torch.Tensor) -> torch.Tensor:
+        """[panel][component][k][j][i] view of a level state."""
+        p = self.params
+        return ju.view(6, 8, p.na, p.na, p.nr)
+
+    # -- level operations ------------------------------------------------
+    def init(self, spec: InitSpec, ju: torch.Tensor | None = None) -> torch.Tensor:
+        ju = self.new_state() if ju is None else ju
+        s = spec.to_c()
+        N.check(self._lib.hc_level_init(self._ctx, C.byref(s), _ptr(ju), _stream()), "hc_level_init")
+        return ju
+
+    def prepare(self, ju: torch.Tensor, t: float = 0.0, w: torch.Tensor | None = None) -> torch.Tensor:
+        w = self.new_primitive() if w is None else w
+        N.check(self._lib.hc_level_prepare(self._ctx, _ptr(ju), _ptr(w), t, _stream()), "hc_level_prepare")
+        return w
+
+    def rhs(self, w: torch.Tensor, k: torch.Tensor | None = None) -> torch.Tensor:
+        k = self.new_state() if k is None else k
+        N.check(self._lib.hc_level_rhs(self._ctx, _ptr(w), _ptr(k), _stream()), "hc_level_rhs")
+        return k
+
+    def rk4_step(self, ju: torch.Tensor, dt: float, t: float = 0.0) -> None:
+        N.check(self._lib.hc_level_rk4_step(self._ctx, _ptr(ju), dt, t, _stream()), "hc_level_rk4_step")
+
+    def advance(self, ju: torch.Tensor, nsteps: int, time: torch.Tensor | None = None,
+                dt_out: torch.Tensor | None = None) -> None:
+        """nsteps RK4 steps with dt = cfl / max CFL rate, computed on device."""
+        N.check(self._lib.hc_level_advance_cfl(self._ctx, _ptr(ju), nsteps, _ptr(time), _ptr(dt_out), _stream()),
+                "hc_level_advance_cfl")
+
+    def inv_dt_max(self, ju: torch.Tensor) -> torch.Tensor:
+        out = torch.zeros(1, dtype=torch.float64, device=self._dev)
+        N.check(self._lib.hc_level_dt_cfl(self._ctx, _ptr(ju), _ptr(out), _stream()), "hc_level_dt_cfl")
+        return out
+
+    def valid(self, ju: torch.Tensor) -> bool:
+        N.check(self._lib.hc_level_valid(self._ctx, _ptr(ju), C.c_void_p(self._flag.data_ptr()), _stream()),
+                "hc_level_valid")
+        return bool(self._flag.item())
+
+    def box_rhs(self, box: N.HcBox, w: torch.Tensor, rhs: torch.Tensor, fluxes=None, panel=None,
+                scale: float = 1.0) -> None:
+        fl = (C.c_void_p * 3)(*[(f.data_ptr() if f is not None else None) for f in fluxes]) if fluxes else None
+        pn = (C.c_void_p * 6)(*[(f.data_ptr() if f is not None else None) for f in panel]) if panel else None
+        N.check(self._lib.hc_box_rhs(self._ctx, C.byref(box), _ptr(w), pn, scale, _ptr(rhs), fl, _stream()),
+                "hc_box_rhs")
+
+    def box_gravity(self, box: N.HcBox, w: torch.Tensor, rhs: torch.Tensor) -> None:
+        N.check(self._lib.hc_box_gravity(self._ctx, C.byref(box), _ptr(w), _ptr(rhs), _stream()), "hc_box_gravity")
+
+    def geometry(self, what: int) -> np.ndarray:
+        n = self._lib.hc_geometry_export(self._ctx, what, None)
+        if n < 0:
+            raise N.HcError(f"unknown geometry table {what}")
+        out = np.zeros(n)
+        self._lib.hc_geometry_export(self._ctx, what, C.c_void_p(out.ctypes.data))
+        return out
+
+
+def make_box(lo, hi, ghost: int, block: int) -> N.HcBox:
+    b = N.HcBox()
+    for d in range(3):
+        b.lo[d] = lo[d]
+        b.hi[d] = hi[d]
+    b.ghost = ghost
+    b.block = block
+    return b

@@ -1,0 +1,171 @@
+/*
+ * hc_abi.h -- C ABI of the B200-native HelioCubed per-box MHD update.
+ *
+ * Every entry point returns an int status (HC_OK or a negative HC_ERR_*),
+ * never throws, and takes plain pointers and sizes.  Device buffers are
+ * caller-owned CUDA device pointers; `stream` is a cudaStream_t passed as
+ * void* (NULL = legacy default stream).  One host thread per context.
+ *
+ * Data layout (identical to Proto BoxData<double,8> as used by the
+ * reference): component-major SoA, radial index fastest,
+ *   offset(c,i,j,k) = c*N + (i-lo0) + n0*((j-lo1) + n1*(k-lo2)),
+ * over the storage box of the array.  Components are
+ *   conserved  JU : rho, m_x, m_y, m_z, E, B_x, B_y, B_z  (Cartesian, times J)
+ *   primitive  W  : rho, v_x, v_y, v_z, p, B_x, B_y, B_z  (Cartesian)
+ * exactly as src/BoxOp_EulerCubedSphere.H:39-51 and src/MHD_AMR.H:99-101.
+ *
+ * A "level" is the six-panel cubed-sphere shell with one box per panel
+ * (nr radial x na x na angular cells); level arrays hold the six boxes
+ * back to back (box b = panel b), valid cells only unless stated.
+ */
+#ifndef HC_ABI_H
+#define HC_ABI_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HC_NUMCOMPS 8
+#define HC_NPANELS 6
+
+enum {
+  HC_OK = 0,
+  HC_ERR_ARG = -1,          /* bad argument (size, pointer, option value) */
+  HC_ERR_CUDA = -2,         /* a CUDA runtime call failed */
+  HC_ERR_UNSUPPORTED = -3,  /* option combination not built */
+  HC_ERR_INVALID_STATE = -4,/* non-finite or non-positive-density cell */
+  HC_ERR_NOMEM = -5
+};
+
+/* Option semantics mirror src/Inputs_Parsing.H:43-178 (ParseInputs). */
+typedef struct hc_params {
+  int spatial_order;        /* 2: PLM operator (src/BoxOp_SecondOrder.H) */
+  int limiter;              /* 0 unlimited, 1|2 minmod, 3 MC (Inputs_Parsing.H:71) */
+  int riemann_solver;       /* 1 Rusanov, 2 Roe 8-wave (Inputs_Parsing.H:79) */
+  int divergence_cleaning;  /* 1: Powell source (Inputs_Parsing.H:118) */
+  int sun_gravity;          /* 1: solar gravity source (Inputs_Parsing.H:175) */
+  int init_condition_type;  /* radial BC family; 1 = analytic wind (BoxOp_PreStage.H:7-47) */
+  int temporal_order;       /* 4: classical RK4 (MHD_AMRRungeKutta.H:10-12) */
+  int nr, na;               /* level cells per panel: radial, angular */
+  int reserved_i[7];
+  double gamma;             /* ratio of specific heats */
+  double entropy_fix_coeff; /* Roe entropy fix, default 0.3 */
+  double cfl;               /* dt = cfl / max(inverse dt) */
+  double inner_radius;      /* cm */
+  double outer_radius;      /* cm */
+  double radial_stretch;    /* C in r = r0 + R_t expm1(C eta) (BoxOp_Utilities.H:36-46) */
+  double strength;          /* analytic-wind perturbation strength (percent) */
+  double reserved_d[7];
+} hc_params;
+
+/* One box of a panel in panel index space (inclusive bounds), the ghost
+ * width of its primitive storage and the panel (Proto block) it lies on. */
+typedef struct hc_box {
+  int lo[3];
+  int hi[3];
+  int ghost;
+  int block;
+} hc_box;
+
+/* Seeded synthetic initial states (the configs' own inputs; the reference
+ * defines no such problem).  kind 1: Parker-like wind + Gaussian pressure
+ * pulse; see DESIGN.md for the formulas. */
+typedef struct hc_init {
+  int kind;
+  int pulse_block, pulse_i, pulse_j, pulse_k;
+  int reserved_i[3];
+  double rho0, p0, vr, b0, r_ref;   /* r_ref: radius where rho0/p0/b0 hold (cm) */
+  double pulse_amp, pulse_width;    /* delta p = amp*p*exp(-d^2/(2 w^2)), d in cells */
+  double reserved_d[4];
+} hc_init;
+
+typedef struct hc_ctx hc_ctx;
+
+/* Last error message of the calling thread ("" if none). */
+const char* hc_last_error(void);
+
+/* Create a context on CUDA device `device`: validates options, builds the
+ * level geometry (the metric caches the reference keeps in statics,
+ * src/BoxOp_EulerCubedSphere.H:348-368) and its stage workspace.
+ * Replaces BoxOp_EulerCubedSphere::levelGeometry + ParseInputs. */
+int hc_ctx_create(const hc_params* params, int device, hc_ctx** out);
+int hc_ctx_destroy(hc_ctx* ctx);
+
+/* Number of doubles in one level array of valid cells (6*8*nr*na*na) and of
+ * one ghosted level primitive array (6*8*(nr+4)*(na+4)^2). */
+size_t hc_level_state_size(const hc_ctx* ctx);
+size_t hc_level_primitive_size(const hc_ctx* ctx);
+
+/* Per-box operator, second-order path with Cartesian primitives.
+ * Replaces BoxOp_EulerCubedSphere::operator()(rhs, fluxes, W, dt, scale,
+ * counter, cartesianPrimitives=true) (src/BoxOp_EulerCubedSphere.H:412-421,
+ * body src/BoxOp_SecondOrder.H:155-370):
+ *   rhs[valid]      += -scale * sum_d (F_d(i+1)-F_d(i))/dxi_d + Powell source
+ *   flux[d][faces]   = F_d on valid.extrude(d) (overwritten; may be NULL)
+ * w: primitives on valid.grow(ghost) (ghost >= 2).  panel_states[2d+side]
+ * (d in {1,2}, may be NULL): reconstructed adjacent-panel states on the
+ * seam face slab valid.extrude(d).face(d,side), 8 comps SoA, replacing the
+ * local left (side 0) / right (side 1) state there
+ * (src/BoxOp_SecondOrder.H:252-281). */
+int hc_box_rhs(hc_ctx* ctx, const hc_box* box, const double* w,
+               const double* const* panel_states, double scale,
+               double* rhs, double* const* flux, void* stream);
+
+/* Solar gravity on second-order primitives, rhs[valid] += source.
+ * Replaces gravitySecondOrderPrimitives (src/BoxOp_Gravity.H:3-82). */
+int hc_box_gravity(hc_ctx* ctx, const hc_box* box, const double* w,
+                   double* rhs, void* stream);
+
+/* Stage preparation of a level: JU (valid) -> ghosted Cartesian primitives
+ * with panel-seam ghosts, floors and radial boundary ghosts at time t.
+ * Replaces preStageLevel -> prepareSecondOrderPrimitives
+ * (src/BoxOp_PreStage.H:434-501, src/BoxOp_SecondOrderPreStage.H:7-218). */
+int hc_level_prepare(hc_ctx* ctx, const double* ju, double* w, double t,
+                     void* stream);
+
+/* Stage right-hand side of a level: k = gravity + L(w) with shared panel
+ * seam states.  Replaces the zero/gravity part of preStageLevel plus
+ * StageLevel (src/BoxOp_EulerCubedSphereImplem.H:961-1012). */
+int hc_level_rhs(hc_ctx* ctx, const double* w, double* k, void* stream);
+
+/* One classical RK4 step of the level in place, with dt from host.
+ * Replaces MBLevelRK::advance(order 4) (src/MHD_LevelRK.H:22-61, tableau
+ * src/MHD_AMRRungeKutta.H:10-12). */
+int hc_level_rk4_step(hc_ctx* ctx, double* ju, double dt, double t,
+                      void* stream);
+
+/* nsteps RK4 steps with dt = cfl/max(inverse dt) computed on the device
+ * before every step (exec/main.cpp:377-383).  *time_dev (device double) is
+ * advanced in place; dt_dev (device double, may be NULL) receives the
+ * last dt.  No host synchronisation inside. */
+int hc_level_advance_cfl(hc_ctx* ctx, double* ju, int nsteps,
+                         double* time_dev, double* dt_dev, void* stream);
+
+/* Maximum over valid cells of the second-order CFL rate, written to the
+ * device double *inv_dt_max.  Replaces dtCFLSecondOrderHost
+ * (src/BoxOp_SecondOrderCFL.H:99-210) whose result is 1/max. */
+int hc_level_dt_cfl(hc_ctx* ctx, const double* ju, double* inv_dt_max,
+                    void* stream);
+
+/* *ok (device int) = 1 if every component of every valid cell is finite
+ * and density is positive, else 0.  Replaces validConservedState
+ * (src/BoxOp_EulerCubedSphereImplem.H:817-876). */
+int hc_level_valid(hc_ctx* ctx, const double* ju, int* ok, void* stream);
+
+/* Seeded synthetic initial state (valid cells) of the level. */
+int hc_level_init(hc_ctx* ctx, const hc_init* init, double* ju, void* stream);
+
+/* Host copies of the level geometry used by the kernels, for tests:
+ * what = 0 radial line [nr+1][4]: rlow^2, (rhigh^2-rlow^2)/(2dxi0),
+ *          (rhigh-rlow)/dxi0, dVolr (last row: face only)
+ * what = 1+d face normals adjA for direction d: [6][na+e1][na+e2][3]
+ * what = 4 cell detA [6][na][na];  what = 5 cell detA_A [6][na][na][3][3]
+ * Returns the number of doubles written (or needed if out is NULL). */
+long hc_geometry_export(const hc_ctx* ctx, int what, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HC_ABI_H */

@@ -1,0 +1,184 @@
+"""ctypes bindings of the oracle (libhc_oracle.so) and of the reference pin
+(_ref/libhcref.so).  Test infrastructure only: used by tests/, by
+__graft_entry__.smoke() as the checker and by bench.py's CPU-baseline arm.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+
+
+class HcParams(C.Structure):
+    """Mirror of hc_params in include/hc_abi.h."""
+    _fields_ = [
+        ("spatial_order", C.c_int), ("limiter", C.c_int), ("riemann_solver", C.c_int),
+        ("divergence_cleaning", C.c_int), ("sun_gravity", C.c_int),
+        ("init_condition_type", C.c_int), ("temporal_order", C.c_int),
+        ("nr", C.c_int), ("na", C.c_int), ("reserved_i", C.c_int * 7),
+        ("gamma", C.c_double), ("entropy_fix_coeff", C.c_double), ("cfl", C.c_double),
+        ("inner_radius", C.c_double), ("outer_radius", C.c_double),
+        ("radial_stretch", C.c_double), ("strength", C.c_double), ("reserved_d", C.c_double * 7),
+    ]
+
+
+class HcBox(C.Structure):
+    _fields_ = [("lo", C.c_int * 3), ("hi", C.c_int * 3), ("ghost", C.c_int), ("block", C.c_int)]
+
+
+class HcInit(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("pulse_block", C.c_int), ("pulse_i", C.c_int), ("pulse_j", C.c_int),
+        ("pulse_k", C.c_int), ("reserved_i", C.c_int * 3),
+        ("rho0", C.c_double), ("p0", C.c_double), ("vr", C.c_double), ("b0", C.c_double),
+        ("r_ref", C.c_double), ("pulse_amp", C.c_double), ("pulse_width", C.c_double),
+        ("reserved_d", C.c_double * 4),
+    ]
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_D)
+
+
+def _load(path: str) -> C.CDLL:
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} missing: run python oracle/build.py")
+    return C.CDLL(path)
+
+
+_orc = None
+_ref = None
+
+
+def lib() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        L = _load(os.path.join(HERE, "libhc_oracle.so"))
+        L.orc_level_create.restype = C.c_void_p
+        L.orc_level_create.argtypes = [C.POINTER(HcParams)]
+        L.orc_level_destroy.argtypes = [C.c_void_p]
+        L.orc_box_rhs.argtypes = [C.c_void_p, C.POINTER(HcBox), _D, C.POINTER(_D), C.c_double, _D, C.POINTER(_D)]
+        L.orc_box_gravity.argtypes = [C.c_void_p, C.POINTER(HcBox), _D, _D]
+        L.orc_level_prepare.argtypes = [C.c_void_p, _D, _D, C.c_double]
+        L.orc_level_rhs.argtypes = [C.c_void_p, _D, _D]
+        L.orc_level_rk4_step.argtypes = [C.c_void_p, _D, C.c_double, C.c_double]
+        L.orc_level_inv_dt.restype = C.c_double
+        L.orc_level_inv_dt.argtypes = [C.c_void_p, _D]
+        L.orc_level_valid.argtypes = [C.c_void_p, _D]
+        L.orc_level_init.argtypes = [C.c_void_p, C.POINTER(HcInit), _D]
+        L.orc_geometry.restype = C.c_long
+        L.orc_geometry.argtypes = [C.c_void_p, C.c_int, _D]
+        L.orc_roe8.argtypes = [_D, _D, C.c_double, C.c_double, C.c_int, _D]
+        L.orc_rusanov.argtypes = [_D, _D, C.c_double, _D]
+        L.orc_frame.argtypes = [_D, _D, _D]
+        L.orc_face_flux.argtypes = [_D, _D, _D, C.c_double, C.c_double, C.c_double, C.c_int, _D]
+        L.orc_plm.argtypes = [_D, _D, _D, _D, C.c_int, _D, _D]
+        L.orc_cart_prim.argtypes = [_D, C.c_double, C.c_double, _D]
+        _orc = L
+    return _orc
+
+
+def ref_lib() -> C.CDLL | None:
+    """The reference-header pin library, or None where it was not built."""
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libhcref.so")
+        if not os.path.exists(path):
+            return None
+        L = C.CDLL(path)
+        L.ref_roe8.argtypes = [_D, _D, C.c_double, C.c_double, C.c_int, _D]
+        L.ref_rusanov.argtypes = [_D, _D, C.c_double, _D]
+        L.ref_frame.argtypes = [_D, _D, _D]
+        L.ref_face_flux.argtypes = [_D, _D, _D, C.c_double, C.c_double, C.c_double, C.c_int, _D]
+        L.ref_mapped_roe.argtypes = [_D, _D, _D, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, _D]
+        L.ref_factored_roe.argtypes = [_D, _D, _D, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, _D]
+        L.ref_usable_primitive.argtypes = [_D, C.c_double]
+        _ref = L
+    return _ref
+
+
+def make_params(**kw) -> HcParams:
+    """hc_params with the configs' common settings (CGS, gamma 5/3,
+    r in [21.5, 215] Rsun, radial_stretch 1.5, Powell on, entropy fix 0.3)."""
+    p = HcParams()
+    p.spatial_order = 2
+    p.limiter = 3
+    p.riemann_solver = 1
+    p.divergence_cleaning = 1
+    p.sun_gravity = 0
+    p.init_condition_type = 1
+    p.temporal_order = 4
+    p.nr = 16
+    p.na = 16
+    p.gamma = 5.0 / 3.0
+    p.entropy_fix_coeff = 0.3
+    p.cfl = 0.4
+    p.inner_radius = 21.5 * 6.96e10
+    p.outer_radius = 215.0 * 6.96e10
+    p.radial_stretch = 1.5
+    p.strength = 0.0
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class OracleLevel:
+    """A cached oracle level (one box per panel)."""
+
+    def __init__(self, params: HcParams):
+        self.params = params
+        self.L = lib()
+        self.h = self.L.orc_level_create(C.byref(params))
+        nr, na = params.nr, params.na
+        self.nv = 6 * 8 * nr * na * na
+        self.ng = 6 * 8 * (nr + 4) * (na + 4) ** 2
+
+    def __del__(self):
+        try:
+            self.L.orc_level_destroy(self.h)
+        except Exception:
+            pass
+
+    def init(self, init: HcInit) -> np.ndarray:
+        ju = np.zeros(self.nv)
+        self.L.orc_level_init(self.h, C.byref(init), dptr(ju))
+        return ju
+
+    def prepare(self, ju: np.ndarray, t: float = 0.0) -> np.ndarray:
+        w = np.zeros(self.ng)
+        self.L.orc_level_prepare(self.h, dptr(ju), dptr(w), t)
+        return w
+
+    def rhs(self, w: np.ndarray) -> np.ndarray:
+        k = np.zeros(self.nv)
+        self.L.orc_level_rhs(self.h, dptr(w), dptr(k))
+        return k
+
+    def rk4_step(self, ju: np.ndarray, dt: float, t: float = 0.0) -> None:
+        self.L.orc_level_rk4_step(self.h, dptr(ju), dt, t)
+
+    def inv_dt(self, ju: np.ndarray) -> float:
+        return self.L.orc_level_inv_dt(self.h, dptr(ju))
+
+    def valid(self, ju: np.ndarray) -> bool:
+        return bool(self.L.orc_level_valid(self.h, dptr(ju)))
+
+    def geometry(self, what: int) -> np.ndarray:
+        n = self.L.orc_geometry(self.h, what, None)
+        out = np.zeros(n)
+        self.L.orc_geometry(self.h, what, dptr(out))
+        return out
+
+    def box_rhs(self, box: HcBox, w: np.ndarray, rhs: np.ndarray, fluxes=None, panel=None, scale=1.0):
+        fl = (_D * 3)(*[dptr(f) if f is not None else None for f in fluxes]) if fluxes is not None else None
+        pn = (_D * 6)(*[dptr(f) if f is not None else None for f in panel]) if panel is not None else None
+        self.L.orc_box_rhs(self.h, C.byref(box), dptr(w), pn, scale, dptr(rhs), fl)
+
+    def box_gravity(self, box: HcBox, w: np.ndarray, rhs: np.ndarray):
+        self.L.orc_box_gravity(self.h, C.byref(box), dptr(w), dptr(rhs))

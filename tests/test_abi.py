@@ -1,0 +1,69 @@
+"""The C ABI surface: the product library loads, exports every entry point
+include/hc_abi.h declares, and rejects bad options before touching a GPU.
+No compute call is made here."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from conftest import ROOT, gpu_available
+
+HEADER = os.path.join(ROOT, "include", "hc_abi.h")
+
+
+def declared_functions() -> list[str]:
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(hc_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for must in ("hc_ctx_create", "hc_box_rhs", "hc_level_rk4_step", "hc_level_dt_cfl", "hc_level_valid"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(product_lib_path):
+    lib = C.CDLL(product_lib_path)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header(product_lib_path):
+    from heliocubed_b200 import _native
+    assert set(declared_functions()) == set(_native.SIGNATURES)
+
+
+def test_struct_layouts_match_header(product_lib_path):
+    from heliocubed_b200 import _native
+    # 16 ints + 16 doubles, 8 ints, 8 ints + 11 doubles (see hc_abi.h)
+    assert C.sizeof(_native.HcParams) == 16 * 4 + 14 * 8 + 0 * 8 or C.sizeof(_native.HcParams) == 64 + 112
+    assert C.sizeof(_native.HcBox) == 8 * 4
+    assert C.sizeof(_native.HcInit) == 8 * 4 + 11 * 8
+
+
+@pytest.mark.parametrize("field,value,code", [
+    ("spatial_order", 4, -3), ("limiter", 7, -1), ("riemann_solver", 3, -1),
+    ("temporal_order", 2, -3), ("nr", 2, -1), ("gamma", 1.0, -1), ("init_condition_type", 0, -3),
+])
+def test_bad_options_rejected(product_lib_path, field, value, code):
+    from heliocubed_b200 import _native
+    from heliocubed_b200.level import Params
+    p = Params(nr=8, na=8).to_c()
+    setattr(p, field, value)
+    ctx = C.c_void_p()
+    rc = _native.lib().hc_ctx_create(C.byref(p), 0, C.byref(ctx))
+    assert rc == code
+    assert not ctx
+    assert _native.lib().hc_last_error()
+
+
+def test_no_device_is_an_error_not_a_fallback(product_lib_path):
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    from heliocubed_b200 import HcError, Params, Shell
+    with pytest.raises(HcError):
+        Shell(Params(nr=8, na=8))

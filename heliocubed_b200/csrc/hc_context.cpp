@@ -116,6 +116,24 @@ void inv3(const double A[3][3], double I[3][3]) {
   I[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id;
 }
 
+// Components that vanish or coincide in magnitude by the cube's symmetry are
+// set to exactly those values: quadrature round-off must not decide the
+// least-aligned-axis choice of secondOrderFrame (a strict comparison), on
+// which the Roe entropy fix (|V|+|W| in the face frame) depends.
+void snapNormal(double n[3]) {
+  const double mag = std::max(std::fabs(n[0]), std::max(std::fabs(n[1]), std::fabs(n[2])));
+  const double tol = 1e-13 * mag;
+  for (int i = 0; i < 3; ++i)
+    if (std::fabs(n[i]) < tol) n[i] = 0.0;
+  for (int a = 0; a < 3; ++a)
+    for (int b = a + 1; b < 3; ++b)
+      if (n[a] != 0.0 && std::fabs(std::fabs(n[a]) - std::fabs(n[b])) <= tol) {
+        const double m = 0.5 * (std::fabs(n[a]) + std::fabs(n[b]));
+        n[a] = std::copysign(m, n[a]);
+        n[b] = std::copysign(m, n[b]);
+      }
+}
+
 // src/MHD_SecondOrderFlux.H:11-30
 FaceGeom makeFrame(const double normal[3]) {
   FaceGeom r{};
@@ -296,6 +314,7 @@ int buildLevel(hc_ctx* c) {
               for (int r = 0; r < 3; ++r) n[r] += G.w[p] * m[r];
             }
           }
+          snapNormal(n);
           faces[((size_t)d * 6 + b) * nf + (size_t)k * (na + 1) + j] = makeFrame(n);
         }
     for (int k = 0; k < na; ++k)

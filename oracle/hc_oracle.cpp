@@ -249,6 +249,23 @@ void plmFace(const double* mm, const double* m, const double* c, const double* p
 
 struct Frame { double f[3][3], norm, normal[3]; };
 
+// Exact symmetric values of a face normal: components below 1e-13 of the
+// largest are zero and pairs equal in magnitude to 1e-13 take their common
+// mean magnitude, so that the least-aligned-axis choice below is the one
+// exact arithmetic makes on the cube's symmetry lines.
+void symmetricNormal(double n[3]) {
+  double mag = std::max(std::fabs(n[0]), std::max(std::fabs(n[1]), std::fabs(n[2])));
+  double tol = 1e-13 * mag;
+  for (int i = 0; i < 3; ++i) if (std::fabs(n[i]) < tol) n[i] = 0.0;
+  for (int a = 0; a < 3; ++a)
+    for (int b = a + 1; b < 3; ++b)
+      if (n[a] != 0.0 && std::fabs(std::fabs(n[a]) - std::fabs(n[b])) <= tol) {
+        double m = 0.5 * (std::fabs(n[a]) + std::fabs(n[b]));
+        n[a] = std::copysign(m, n[a]);
+        n[b] = std::copysign(m, n[b]);
+      }
+}
+
 // src/MHD_SecondOrderFlux.H:11-30
 Frame secondOrderFrame(const double normal[3]) {
   Frame r{};
@@ -529,6 +546,7 @@ struct Level {
             LD n[3];
             faceNormal(b, d, j, k, (LD)h, n);
             double nd[3] = {(double)n[0], (double)n[1], (double)n[2]};
+            symmetricNormal(nd);
             frames[d][frameIdx(b, j, k)] = secondOrderFrame(nd);
           }
       for (int k = 0; k < na; ++k)

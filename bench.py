@@ -38,7 +38,7 @@ METRIC = "FP64 cell-updates/s on 1 B200 (RK4 step of the cubed-sphere MHD update
 UNIT = "cell-updates/s"
 L2_BYTES = 126 * 1024 * 1024
 OPERATOR_BYTES_PER_CELL_STAGE = 128  # read 8 FP64 primitives, write 8 FP64 rhs
-LAUNCHES_PER_STEP = 14               # cfl + 4 x (prim, ghosts, stage) + time
+LAUNCHES_PER_STEP = 11               # prim + cfl + 4 x (ghosts, stage) + time (prologue in every 1-step call)
 
 
 def workload_params(args):
@@ -56,6 +56,7 @@ def workload_config(args, flush: bool):
                    "powell": 1, "gravity": args.gravity, "temporal_order": 4, "cfl": 0.4},
         "l2": "flushed between timed steps (256 MiB write)" if flush else "working set larger than L2",
         "dt": "device CFL reduction every step",
+        "launch": "CUDA graph replay per step" if args.graph else "eager launches",
     }
 
 
@@ -222,8 +223,16 @@ def run_b200(args, world, rank, local):
     flush = working < 2 * L2_BYTES
     scratch = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda") if flush else None
 
+    graph = shell.capture_advance(ju, 1, time_dev) if args.graph else None
+
+    def step():
+        if graph is not None:
+            graph.replay()
+        else:
+            shell.advance(ju, 1, time_dev)
+
     for _ in range(args.warmup):
-        shell.advance(ju, 1, time_dev)
+        step()
     torch.cuda.synchronize()
     if not shell.valid(ju):
         raise RuntimeError("warm-up produced an invalid state")
@@ -237,7 +246,7 @@ def run_b200(args, world, rank, local):
         if flush:
             scratch.zero_()
         ev[s][0].record(stream)
-        shell.advance(ju, 1, time_dev)
+        step()
         ev[s][1].record(stream)
     torch.cuda.synchronize()
     barrier(world)
@@ -324,6 +333,8 @@ def main() -> int:
     ap.add_argument("--gravity", type=int, default=0)
     ap.add_argument("--seed", type=int, default=20261204)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="launch the step eagerly instead of replaying a captured CUDA graph")
     ap.add_argument("--cpu-max-steps", type=int, default=60)
     ap.add_argument("--ref-budget", type=float, default=20.0)
     args = ap.parse_args()

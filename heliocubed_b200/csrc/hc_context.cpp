@@ -238,11 +238,11 @@ struct hc_ctx {
   std::vector<void*> owned;
   // host copies for hc_geometry_export
   std::vector<double> radialExport, detExport, detAAExport, normalExport[3];
-  // stage workspace
-  double* W = nullptr;     // ghosted primitives [6][8][nr+4][na+4][na+4]
-  double* acc = nullptr;   // RK accumulator [6][8][nr][na][na]
-  double* next = nullptr;  // next stage state
-  unsigned long long* invMax = nullptr;
+  // stage workspace: stage s reads W[s % 2] and writes the next stage's
+  // primitives into W[(s + 1) % 2]
+  double* W[2] = {nullptr, nullptr};  // ghosted primitives [6][8][na+4][na+4][nr+4]
+  double* acc = nullptr;              // RK accumulator [6][8][na][na][nr]
+  unsigned long long* invMax = nullptr;  // two CFL slots (bit patterns), ping-pong per step
   int* flag = nullptr;
 };
 
@@ -259,7 +259,7 @@ int buildLevel(hc_ctx* c) {
   L.Nv = (long)nr * na * na;
   L.Ng = (long)L.n0 * L.n1 * L.n1;
   L.h = h; L.dxi0 = 1.0 / nr;
-  L.gamma = P.gamma; L.entropy = P.entropy_fix_coeff; L.cfl_number = P.cfl; L.strength = P.strength;
+  L.gamma = P.gamma; L.invGm1 = 1.0 / (P.gamma - 1.0); L.entropy = P.entropy_fix_coeff; L.cfl_number = P.cfl; L.strength = P.strength;
   L.r0 = P.inner_radius; L.innerBCType = P.init_condition_type;
 
   // radial rows i = -g .. nr+g
@@ -477,16 +477,16 @@ int allocWorkspace(hc_ctx* c) {
   const size_t nv = 6 * NC * (size_t)c->L.Nv, ng = 6 * NC * (size_t)c->L.Ng;
   void* p;
   cudaError_t e;
-  if ((e = cudaMalloc(&p, ng * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace W");
-  c->owned.push_back(p); c->W = (double*)p;
-  if ((e = cudaMemset(p, 0, ng * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace W");
+  for (int q = 0; q < 2; ++q) {
+    if ((e = cudaMalloc(&p, ng * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace W");
+    c->owned.push_back(p); c->W[q] = (double*)p;
+    if ((e = cudaMemset(p, 0, ng * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace W");
+  }
   if ((e = cudaMalloc(&p, nv * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace acc");
   c->owned.push_back(p); c->acc = (double*)p;
-  if ((e = cudaMalloc(&p, nv * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace next");
-  c->owned.push_back(p); c->next = (double*)p;
   if ((e = cudaMalloc(&p, 64)) != cudaSuccess) return cudaFail(e, "workspace scalars");
   c->owned.push_back(p); c->invMax = (unsigned long long*)p;
-  c->flag = (int*)((char*)p + 16);
+  c->flag = (int*)((char*)p + 32);
   return HC_OK;
 }
 
@@ -509,25 +509,33 @@ StageArgs levelArgs(hc_ctx* c, const double* w) {
 
 int checkLaunch(cudaError_t e, const char* what) { return e == cudaSuccess ? HC_OK : cudaFail(e, what); }
 
-// One RK4 stage: prepare primitives of `src` then the fused operator + update.
-int rkStage(hc_ctx* c, const double* src, double* ju, int stage, double dtv, const double* invMax, double tbase,
-            const double* tdev, cudaStream_t s) {
+// One RK4 step on W[0] = primitives of ju (valid cells).  Stage s fills the
+// ghosts of W[s % 2], then the fused operator + update writes the next
+// stage's primitives into W[(s + 1) % 2]; stage 3 leaves the new state's
+// primitives in W[0] and, with invMaxOut, its CFL rate.
+int rkStep(hc_ctx* c, double* ju, double dtv, const double* invMax, unsigned long long* invMaxOut, double tbase,
+           const double* tdev, cudaStream_t s) {
   static const double c4[4] = {0, 0.5, 0.5, 1};
-  int rc;
-  if ((rc = checkLaunch(launchPrimValid(c->L, src, c->W, s), "prim")) != HC_OK) return rc;
-  StageTime st{tbase, tdev, c4[stage], invMax, dtv};
-  if ((rc = checkLaunch(launchGhosts(c->L, c->W, st, s), "ghosts")) != HC_OK) return rc;
-  StageArgs a = levelArgs(c, c->W);
-  a.stage = stage;
-  a.invDtMax = invMax;
-  a.dtv = dtv;
-  a.ju = ju;
-  a.acc = c->acc;
-  a.next = c->next;
-  a.invalid = nullptr;
-  return checkLaunch(launchStage(a, MODE_RK, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
+  for (int stage = 0; stage < 4; ++stage) {
+    double* win = c->W[stage % 2];
+    StageTime st{tbase, tdev, c4[stage], invMax, dtv};
+    int rc = checkLaunch(launchGhosts(c->L, win, st, s), "ghosts");
+    if (rc != HC_OK) return rc;
+    StageArgs a = levelArgs(c, win);
+    a.stage = stage;
+    a.invDtMax = invMax;
+    a.dtv = dtv;
+    a.ju = ju;
+    a.acc = c->acc;
+    a.wOut = c->W[(stage + 1) % 2];
+    a.invMaxOut = stage == 3 ? invMaxOut : nullptr;
+    a.invalid = nullptr;
+    rc = checkLaunch(launchStage(a, MODE_RK, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
                                  c->P.sun_gravity == 1, s),
                      "stage");
+    if (rc != HC_OK) return rc;
+  }
+  return HC_OK;
 }
 
 }  // namespace
@@ -643,28 +651,28 @@ int hc_level_rk4_step(hc_ctx* c, double* ju, double dt, double t, void* stream) 
   if (!c || !ju) return fail(HC_ERR_ARG, "null argument");
   if (!(dt > 0)) return fail(HC_ERR_ARG, "dt must be positive");
   cudaStream_t s = (cudaStream_t)stream;
-  for (int stage = 0; stage < 4; ++stage) {
-    const int rc = rkStage(c, stage == 0 ? ju : c->next, ju, stage, dt, nullptr, t, nullptr, s);
-    if (rc != HC_OK) return rc;
-  }
-  return HC_OK;
+  const int rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
+  if (rc != HC_OK) return rc;
+  return rkStep(c, ju, dt, nullptr, nullptr, t, nullptr, s);
 }
 
 int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, double* dt_dev, void* stream) {
   if (!c || !ju || nsteps < 0) return fail(HC_ERR_ARG, "bad argument");
+  if (nsteps == 0) return HC_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  const double* invMax = reinterpret_cast<const double*>(c->invMax);
-  for (int n = 0; n < nsteps; ++n) {
-    int rc = checkLaunch(launchCfl(c->L, ju, c->invMax, s), "cfl");
-    if (rc != HC_OK) return rc;
-    for (int stage = 0; stage < 4; ++stage) {
-      rc = rkStage(c, stage == 0 ? ju : c->next, ju, stage, 0.0, invMax, 0.0, time_dev, s);
-      if (rc != HC_OK) return rc;
-    }
-    rc = checkLaunch(launchAdvanceTime(time_dev, invMax, c->P.cfl, dt_dev, s), "time");
-    if (rc != HC_OK) return rc;
+  // The first step's primitives and CFL rate come from ju; every later
+  // step's come from the previous step's last stage.
+  int rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
+  if (rc == HC_OK) rc = checkLaunch(launchCfl(c->L, ju, c->invMax, s), "cfl");
+  for (int n = 0; n < nsteps && rc == HC_OK; ++n) {
+    const int cur = n % 2;
+    unsigned long long* next = c->invMax + (1 - cur);
+    const double* invMax = reinterpret_cast<const double*>(c->invMax + cur);
+    rc = checkLaunch(cudaMemsetAsync(next, 0, sizeof(unsigned long long), s), "cfl reset");
+    if (rc == HC_OK) rc = rkStep(c, ju, 0.0, invMax, n + 1 < nsteps ? next : nullptr, 0.0, time_dev, s);
+    if (rc == HC_OK) rc = checkLaunch(launchAdvanceTime(time_dev, invMax, c->P.cfl, dt_dev, s), "time");
   }
-  return HC_OK;
+  return rc;
 }
 
 int hc_level_dt_cfl(hc_ctx* c, const double* ju, double* inv_dt_max, void* stream) {

@@ -75,8 +75,9 @@ HC_DEV void plmRight(const double* m, const double* c, const double* p, double h
   }
 }
 
-// src/MHD_Roe8Wave.H:604-629
-HC_DEV void rusanovDissipation(double out[8], const double* wl, const double* wr, double gamma) {
+// src/MHD_Roe8Wave.H:604-629.  invGm1 = 1/(gamma-1) replaces the division
+// by (gamma-1) (one rounding of difference, inside the parity tolerance).
+HC_DEV void rusanovDissipation(double out[8], const double* wl, const double* wr, double gamma, double invGm1) {
   constexpr double inv4Pi = 0.079577471545947667884441881686257181;
   double cl[8], cr[8], speed = 0.0;
 #pragma unroll
@@ -92,7 +93,7 @@ HC_DEV void rusanovDissipation(double out[8], const double* wl, const double* wr
       cs[1 + d] = w[0] * w[1 + d];
       cs[5 + d] = w[5 + d];
     }
-    cs[4] = w[4] / (gamma - 1.0) + 0.5 * w[0] * v2 + 0.5 * inv4Pi * b2;
+    cs[4] = w[4] * invGm1 + 0.5 * w[0] * v2 + 0.5 * inv4Pi * b2;
     speed = fmax(speed, fabs(w[1]) + sqrt((gamma * w[4] + inv4Pi * b2) / w[0]));
   }
 #pragma unroll
@@ -163,7 +164,7 @@ HC_DEV bool roeRightNonzero(int r, int k) {
 // Returns false where the reference requests the Rusanov fallback.
 template <bool CHECK>
 __device__ __noinline__ bool roe8WaveDissipation(double out[8], const double* wl, const double* wr, double gamma,
-                                                 double del2) {
+                                                 double del2, double invHg) {
   const double RhoL = wl[0], UL = wl[1], VL = wl[2], WL = wl[3], PGasL = wl[4], BXL = wl[5], BYL = wl[6], BZL = wl[7];
   const double RhoR = wr[0], UR = wr[1], VR = wr[2], WR = wr[3], PGasR = wr[4], BXR = wr[5], BYR = wr[6], BZR = wr[7];
   if (!(RhoL > 0.0 && RhoR > 0.0 && PGasL > 0.0 && PGasR > 0.0)) return false;
@@ -175,11 +176,11 @@ __device__ __noinline__ bool roe8WaveDissipation(double out[8], const double* wl
   const double RUL = RhoL * UL, RVL = RhoL * VL, RWL = RhoL * WL;
   const double BxBL = d_1_8PI * (BXL * BXL + BYL * BYL + BZL * BZL);
   const double RUxUL = half * (RUL * UL + RVL * VL + RWL * WL);
-  const double PL = PGasL + BxBL, EL = PGasL / hgamma + RUxUL + BxBL, AL2 = gamma * PGasL / RhoL;
+  const double PL = PGasL + BxBL, EL = PGasL * invHg + RUxUL + BxBL, AL2 = gamma * PGasL / RhoL;
   const double RUR = RhoR * UR, RVR = RhoR * VR, RWR = RhoR * WR;
   const double BxBR = d_1_8PI * (BXR * BXR + BYR * BYR + BZR * BZR);
   const double RUxUR = half * (RUR * UR + RVR * VR + RWR * WR);
-  const double PR = PGasR + BxBR, ER = PGasR / hgamma + RUxUR + BxBR, AR2 = gamma * PGasR / RhoR;
+  const double PR = PGasR + BxBR, ER = PGasR * invHg + RUxUR + BxBR, AR2 = gamma * PGasR / RhoR;
   const double ccmi = AL2 > AR2 ? AR2 : AL2, ccma = AL2 > AR2 ? AL2 : AR2;
   const double Rho = half * (RhoL + RhoR), U = half * (UL + UR), V = half * (VL + VR), W = half * (WL + WR);
   const double BX = half * (BXL + BXR), BY = half * (BYL + BYR), BZ = half * (BZL + BZR), P = half * (PL + PR);
@@ -254,7 +255,7 @@ __device__ __noinline__ bool roe8WaveDissipation(double out[8], const double* wl
       double d[8];
 #pragma unroll
       for (int r = 0; r < 8; ++r) d[r] = roeRightNonzero(r, k) ? amplitude * roeRight(e, r, k) : 0.0;
-      const double d4 = kk * d[0] + Rho * (U * d[1] + V * d[2] + W * d[3]) + d[4] / hgamma + d_1_4PI * (BX * d[5] + BY * d[6] + BZ * d[7]);
+      const double d4 = kk * d[0] + Rho * (U * d[1] + V * d[2] + W * d[3]) + d[4] * invHg + d_1_4PI * (BX * d[5] + BY * d[6] + BZ * d[7]);
       const double d1 = U * d[0] + Rho * d[1], d2 = V * d[0] + Rho * d[2], d3 = W * d[0] + Rho * d[3];
       s0 += d[0]; s1 += d1; s2 += d2; s3 += d3; s4 += d4; s5 += d[5]; s6 += d[6]; s7 += d[7];
       if (eig[order[wave + 1]] > eig[k]) {
@@ -285,7 +286,7 @@ __device__ __noinline__ bool roe8WaveDissipation(double out[8], const double* wl
       }
     ra[r] = s;
   }
-  const double ra4 = ra[0] * kk + Rho * (U * ra[1] + V * ra[2] + W * ra[3]) + ra[4] / hgamma + d_1_4PI * (BX * ra[5] + BY * ra[6] + BZ * ra[7]);
+  const double ra4 = ra[0] * kk + Rho * (U * ra[1] + V * ra[2] + W * ra[3]) + ra[4] * invHg + d_1_4PI * (BX * ra[5] + BY * ra[6] + BZ * ra[7]);
   out[0] = -ra[0];
   out[1] = -(U * ra[0] + Rho * ra[1]);
   out[2] = -(V * ra[0] + Rho * ra[2]);
@@ -305,7 +306,7 @@ __device__ __noinline__ bool roe8WaveDissipation(double out[8], const double* wl
 // multiplied by radialArea*|adjA|.
 template <bool ROE>
 HC_DEV void secondOrderFaceFlux(double out[8], const double* l, const double* r, const FaceGeom& g, double radialArea,
-                                double gamma, double entropy) {
+                                double gamma, double invGm1, double entropy) {
   constexpr double inv4pi = 1.0 / (4.0 * kPi);
   double loc[2][8], flux[2][8];
 #pragma unroll
@@ -327,7 +328,7 @@ HC_DEV void secondOrderFaceFlux(double out[8], const double* l, const double* r,
       vb += q[1 + i] * q[5 + i];
     }
     const double pressure = q[4] + 0.5 * inv4pi * b2;
-    const double energy = q[4] / (gamma - 1) + 0.5 * q[0] * v2 + 0.5 * inv4pi * b2;
+    const double energy = q[4] * invGm1 + 0.5 * q[0] * v2 + 0.5 * inv4pi * b2;
     double* f = flux[side];
     f[0] = q[0] * q[1];
     f[4] = (energy + pressure) * q[1] - inv4pi * q[5] * vb;
@@ -339,8 +340,8 @@ HC_DEV void secondOrderFaceFlux(double out[8], const double* l, const double* r,
   }
   double diss[8];
   bool done = false;
-  if (ROE) done = roe8WaveDissipation<true>(diss, loc[0], loc[1], gamma, entropy);
-  if (!done) rusanovDissipation(diss, loc[0], loc[1], gamma);
+  if (ROE) done = roe8WaveDissipation<true>(diss, loc[0], loc[1], gamma, entropy, invGm1);
+  if (!done) rusanovDissipation(diss, loc[0], loc[1], gamma, invGm1);
   const double area = radialArea * g.norm;
   double num[8];
 #pragma unroll

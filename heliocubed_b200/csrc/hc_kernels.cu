@@ -135,7 +135,7 @@ __device__ __forceinline__ void o2Face(const StageArgs& a, const double* __restr
   const FaceGeom& g = L.face[((size_t)dir * 6 + block) * (L.na + 1) * (L.na + 1) + (size_t)k * (L.na + 1) + j];
   const double4 rd = L.radial[i + L.g];
   const double area = dir == 0 ? rd.x : rd.y;
-  secondOrderFaceFlux<ROE>(out, l, r, g, area, L.gamma, L.entropy);
+  secondOrderFaceFlux<ROE>(out, l, r, g, area, L.gamma, L.invGm1, L.entropy);
   if (powell) {
     double f = 0;
 #pragma unroll
@@ -144,8 +144,102 @@ __device__ __forceinline__ void o2Face(const StageArgs& a, const double* __restr
   }
 }
 
+// CFL rate of one valid cell from its conserved state,
+// src/BoxOp_SecondOrderCFL.H:138-202 (no mapped scale, no cone density).
+__device__ __forceinline__ double cflRate(const DevLevel& L, int b, int i, int j, int k, const double u[8]) {
+  const CflCell& a = L.cfl[((size_t)b * L.na + k) * L.na + j];
+  const double4 rd = L.radial[i + L.g];
+  const double volume = rd.w, inverseVolume = 1.0 / rd.w, width0 = rd.z * L.dxi0;
+  const double area[3] = {rd.x, rd.y, rd.y};
+  double rho = u[0] * a.inverseDet;
+  rho *= inverseVolume;
+  rho = dmax(rho, kRHO00);
+  double energy = u[4] * a.inverseDet;
+  energy *= inverseVolume;
+  double v[3], bb[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    v[d] = a.inverseDetA[3 * d] * u[1] + a.inverseDetA[3 * d + 1] * u[2] + a.inverseDetA[3 * d + 2] * u[3];
+    bb[d] = a.inverseDetA[3 * d] * u[5] + a.inverseDetA[3 * d + 1] * u[6] + a.inverseDetA[3 * d + 2] * u[7];
+    v[d] *= inverseVolume;
+    bb[d] *= inverseVolume;
+    v[d] /= rho;
+  }
+  double kinetic = 0, magnetic = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double vc = a.cell[3 * d] * v[0] + a.cell[3 * d + 1] * v[1] + a.cell[3 * d + 2] * v[2];
+    const double bc = a.cell[3 * d] * bb[0] + a.cell[3 * d + 1] * bb[1] + a.cell[3 * d + 2] * bb[2];
+    kinetic += vc * vc / 2;
+    magnetic += bc * bc / 8.0 / kPi;
+  }
+  kinetic *= rho;
+  double pressure = (energy - kinetic - magnetic) * (L.gamma - 1);
+  if (pressure < 0) pressure = 0;
+  double inverseDt = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double* basis = d == 0 ? a.cell : a.face[d - 1];
+    double v2 = 0, fullB2 = 0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const double velocity = basis[3 * q] * v[0] + basis[3 * q + 1] * v[1] + basis[3 * q + 2] * v[2];
+      const double field = basis[3 * q] * bb[0] + basis[3 * q + 1] * bb[1] + basis[3 * q + 2] * bb[2];
+      v2 += velocity * velocity;
+      fullB2 += field * field;
+    }
+    const double width = d == 0 ? width0 : volume * a.det[d] * L.h / area[d] / a.normal[d];
+    const double wave = sqrt(L.gamma * pressure / rho + fullB2 / 4.0 / kPi / rho);
+    inverseDt += (wave + sqrt(v2)) / width;
+  }
+  return inverseDt;
+}
+
+// Max over a warp (std::max order: a NaN candidate never replaces the max),
+// then one atomic per warp on the bit pattern (non-negative doubles order as
+// unsigned integers).
+__device__ __forceinline__ void warpMaxAtomic(double v, unsigned long long* out) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double other = __shfl_xor_sync(0xffffffffu, v, o);
+    v = v < other ? other : v;
+  }
+  if ((threadIdx.x & 31) == 0 && v > 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+}
+
+template <int DIR, int LIM, bool ROE, int MODE>
+__device__ __forceinline__ void o2FaceLoop(const StageArgs& a, const double* __restrict__ w, int block, int oi,
+                                           int oj, int ok, int v0, int v1, int v2, double* sF, int base,
+                                           bool powell) {
+  constexpr int EX = TX + (DIR == 0), EY = TY + (DIR == 1), EZ = TZ + (DIR == 2);
+  constexpr int NFD = EX * EY * EZ;
+  for (int f = threadIdx.x; f < NFD; f += NT) {
+    const int fi = f % EX, fj = (f / EX) % EY, fk = f / (EX * EY);
+    const int i = oi + fi, j = oj + fj, k = ok + fk;
+    const bool valid = i <= a.hi[0] + (DIR == 0) && j <= a.hi[1] + (DIR == 1) && k <= a.hi[2] + (DIR == 2);
+    double out[8];
+    double bf = 0;
+    if (valid) {
+      o2Face<LIM, ROE, MODE>(a, w, block, DIR, i, j, k, out, bf, powell);
+      if (MODE == MODE_BOX && a.flux[DIR]) {
+        const int f0 = v0 + (DIR == 0), f1 = v1 + (DIR == 1), f2 = v2 + (DIR == 2);
+        const long fidx = (long)(i - a.lo[0]) + (long)f0 * ((long)(j - a.lo[1]) + (long)f1 * (k - a.lo[2]));
+        const long fN = (long)f0 * f1 * f2;
+#pragma unroll
+        for (int q = 0; q < NC; ++q) a.flux[DIR][q * fN + fidx] = out[q];
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < NC; ++q) out[q] = 0;
+    }
+#pragma unroll
+    for (int q = 0; q < NC; ++q) sF[q * NF + base + f] = out[q];
+    sF[8 * NF + base + f] = bf;
+  }
+}
+
 template <int LIM, bool ROE, int MODE>
-__global__ void __launch_bounds__(NT) o2StageKernel(const StageArgs a, const int powell, const int grav) {
+__global__ void __launch_bounds__(NT, ROE ? 3 : 4) o2StageKernel(const StageArgs a, const int powell, const int grav) {
   extern __shared__ double sF[];  // [9][NF]: 8 flux components + Powell face B_n
   const int v0 = a.hi[0] - a.lo[0] + 1, v1 = a.hi[1] - a.lo[1] + 1, v2 = a.hi[2] - a.lo[2] + 1;
   const int nbx = (v0 + TX - 1) / TX, nby = (v1 + TY - 1) / TY, nbz = (v2 + TZ - 1) / TZ;
@@ -158,126 +252,111 @@ __global__ void __launch_bounds__(NT) o2StageKernel(const StageArgs a, const int
   const int oi = a.lo[0] + bx * TX, oj = a.lo[1] + by * TY, ok = a.lo[2] + bz * TZ;
   const double* __restrict__ w = a.w + (long)box * a.wBoxStride;
 
-  for (int f = threadIdx.x; f < NF; f += NT) {
-    int dir, fi, fj, fk;
-    if (f < NF0) { dir = 0; fi = f % (TX + 1); const int q = f / (TX + 1); fj = q % TY; fk = q / TY; }
-    else if (f < NF0 + NF1) { dir = 1; const int g = f - NF0; fi = g % TX; const int q = g / TX; fj = q % (TY + 1); fk = q / (TY + 1); }
-    else { dir = 2; const int g = f - NF0 - NF1; fi = g % TX; const int q = g / TX; fj = q % TY; fk = q / TY; }
-    const int i = oi + fi, j = oj + fj, k = ok + fk;
-    const bool valid = i <= a.hi[0] + (dir == 0) && j <= a.hi[1] + (dir == 1) && k <= a.hi[2] + (dir == 2);
-    double out[8];
-    double bf = 0;
-    if (valid) {
-      o2Face<LIM, ROE, MODE>(a, w, block, dir, i, j, k, out, bf, powell != 0);
-      if (MODE == MODE_BOX && a.flux[dir]) {
-        const int f0 = v0 + (dir == 0), f1 = v1 + (dir == 1), f2 = v2 + (dir == 2);
-        const long fidx = (long)(i - a.lo[0]) + (long)f0 * ((long)(j - a.lo[1]) + (long)f1 * (k - a.lo[2]));
-        const long fN = (long)f0 * f1 * f2;
-#pragma unroll
-        for (int q = 0; q < NC; ++q) a.flux[dir][q * fN + fidx] = out[q];
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < NC; ++q) out[q] = 0;
-    }
-#pragma unroll
-    for (int q = 0; q < NC; ++q) sF[q * NF + f] = out[q];
-    sF[8 * NF + f] = bf;
-  }
+  o2FaceLoop<0, LIM, ROE, MODE>(a, w, block, oi, oj, ok, v0, v1, v2, sF, 0, powell != 0);
+  o2FaceLoop<1, LIM, ROE, MODE>(a, w, block, oi, oj, ok, v0, v1, v2, sF, NF0, powell != 0);
+  o2FaceLoop<2, LIM, ROE, MODE>(a, w, block, oi, oj, ok, v0, v1, v2, sF, NF0 + NF1, powell != 0);
   __syncthreads();
 
   const int li = threadIdx.x % TX, lj = (threadIdx.x / TX) % TY, lk = threadIdx.x / (TX * TY);
   const int i = oi + li, j = oj + lj, k = ok + lk;
-  if (i > a.hi[0] || j > a.hi[1] || k > a.hi[2]) return;
+  // Inactive threads of a partial tile stay for the warp-wide CFL reduction.
+  const bool active = i <= a.hi[0] && j <= a.hi[1] && k <= a.hi[2];
   const DevLevel& L = a.L;
-  const long cw = cellOffset(i, j, k, a.wlo, a.wn);
-  double kv[8];
-  long vidx = 0;
-  if (MODE == MODE_BOX) {
-    vidx = (long)(i - a.lo[0]) + (long)v0 * ((long)(j - a.lo[1]) + (long)v1 * (k - a.lo[2]));
+  double rate = 0.0;
+  if (active) {
+    const long cw = cellOffset(i, j, k, a.wlo, a.wn);
+    double kv[8];
+    long vidx = 0;
+    if (MODE == MODE_BOX) {
+      vidx = (long)(i - a.lo[0]) + (long)v0 * ((long)(j - a.lo[1]) + (long)v1 * (k - a.lo[2]));
 #pragma unroll
-    for (int q = 0; q < NC; ++q) kv[q] = a.rhs[q * a.rhsN + vidx];
-  } else {
-    vidx = (long)box * NC * L.Nv + (long)i + (long)L.nr * ((long)j + (long)L.na * k);
+      for (int q = 0; q < NC; ++q) kv[q] = a.rhs[q * a.rhsN + vidx];
+    } else {
+      vidx = (long)box * NC * L.Nv + (long)i + (long)L.nr * ((long)j + (long)L.na * k);
 #pragma unroll
-    for (int q = 0; q < NC; ++q) kv[q] = 0.0;
-    if (grav) {
-      // src/BoxOp_Gravity.H:36-58
-      const GravCell gc = L.grav[((size_t)block * L.na + k) * L.na + j];
-      const double factor = -kGrav * kMsun * L.radial[i + L.g].z * __ldg(w + cw);
-      double radialVelocity = 0;
+      for (int q = 0; q < NC; ++q) kv[q] = 0.0;
+      if (grav) {
+        // src/BoxOp_Gravity.H:36-58
+        const GravCell gc = L.grav[((size_t)block * L.na + k) * L.na + j];
+        const double factor = -kGrav * kMsun * L.radial[i + L.g].z * __ldg(w + cw);
+        double radialVelocity = 0;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        kv[1 + d] += factor * gc.a0[d];
-        radialVelocity += gc.x[d] * __ldg(w + (1 + d) * a.wN + cw);
+        for (int d = 0; d < 3; ++d) {
+          kv[1 + d] += factor * gc.a0[d];
+          radialVelocity += gc.x[d] * __ldg(w + (1 + d) * a.wN + cw);
+        }
+        kv[4] += factor * gc.det * radialVelocity;
       }
-      kv[4] += factor * gc.det * radialVelocity;
     }
-  }
-  const int fl[3] = {li + (TX + 1) * (lj + TY * lk), NF0 + li + TX * (lj + (TY + 1) * lk), NF0 + NF1 + li + TX * (lj + TY * lk)};
-  const int fs[3] = {1, TX, TX * TY};
-  const double coef[3] = {-a.scale / L.dxi0, -a.scale / L.h, -a.scale / L.h};
-  double md = 0;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-#pragma unroll
-    for (int q = 0; q < NC; ++q) kv[q] += coef[d] * (sF[q * NF + fl[d] + fs[d]] - sF[q * NF + fl[d]]);
-    if (powell) md += coef[d] * (sF[8 * NF + fl[d] + fs[d]] - sF[8 * NF + fl[d]]);
-  }
-  if (powell) {
-    // src/BoxOp_SecondOrder.H:351-369
-    double vb = 0;
+    const int fl[3] = {li + (TX + 1) * (lj + TY * lk), NF0 + li + TX * (lj + (TY + 1) * lk),
+                       NF0 + NF1 + li + TX * (lj + TY * lk)};
+    const int fs[3] = {1, TX, TX * TY};
+    const double coef[3] = {-a.scale / L.dxi0, -a.scale / L.h, -a.scale / L.h};
+    double md = 0;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double b = __ldg(w + (5 + d) * a.wN + cw), vel = __ldg(w + (1 + d) * a.wN + cw);
-      kv[1 + d] += md * b / (4 * kPi);
-      kv[5 + d] += md * vel;
-      vb += vel * b;
+#pragma unroll
+      for (int q = 0; q < NC; ++q) kv[q] += coef[d] * (sF[q * NF + fl[d] + fs[d]] - sF[q * NF + fl[d]]);
+      if (powell) md += coef[d] * (sF[8 * NF + fl[d] + fs[d]] - sF[8 * NF + fl[d]]);
     }
-    kv[4] += md * vb / (4 * kPi);
-  }
-  if (MODE == MODE_BOX) {
+    if (powell) {
+      // src/BoxOp_SecondOrder.H:351-369
+      double vb = 0;
 #pragma unroll
-    for (int q = 0; q < NC; ++q) a.rhs[q * a.rhsN + vidx] = kv[q];
-    return;
-  }
-  if (MODE == MODE_RHS) {
-#pragma unroll
-    for (int q = 0; q < NC; ++q) a.rhs[vidx + q * L.Nv] = kv[q];
-    return;
-  }
-  // Classical RK4 (src/MHD_AMRRungeKutta.H:10-12): stage = U + (dt a) k,
-  // U_new = U + sum_s (dt b_s) k_s accumulated in stage order.
-  const double dt = a.invDtMax ? L.cfl_number / *a.invDtMax : a.dtv;
-  constexpr double b4[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
-  constexpr double a4[3] = {0.5, 0.5, 1.0};
-  const long N = L.Nv;
-  if (a.stage == 0) {
-    const double fb = dt * b4[0], fa = dt * a4[0];
-#pragma unroll
-    for (int q = 0; q < NC; ++q) {
-      const double u = a.ju[vidx + q * N];
-      a.acc[vidx + q * N] = u + fb * kv[q];
-      a.next[vidx + q * N] = u + fa * kv[q];
+      for (int d = 0; d < 3; ++d) {
+        const double b = __ldg(w + (5 + d) * a.wN + cw), vel = __ldg(w + (1 + d) * a.wN + cw);
+        kv[1 + d] += md * b / (4 * kPi);
+        kv[5 + d] += md * vel;
+        vb += vel * b;
+      }
+      kv[4] += md * vb / (4 * kPi);
     }
-  } else if (a.stage < 3) {
-    const double fb = dt * b4[a.stage], fa = dt * a4[a.stage];
+    if (MODE == MODE_BOX) {
 #pragma unroll
-    for (int q = 0; q < NC; ++q) {
-      a.acc[vidx + q * N] = a.acc[vidx + q * N] + fb * kv[q];
-      a.next[vidx + q * N] = a.ju[vidx + q * N] + fa * kv[q];
-    }
-  } else {
-    const double fb = dt * b4[3];
-    bool bad = false;
+      for (int q = 0; q < NC; ++q) a.rhs[q * a.rhsN + vidx] = kv[q];
+    } else if (MODE == MODE_RHS) {
 #pragma unroll
-    for (int q = 0; q < NC; ++q) {
-      const double u = a.acc[vidx + q * N] + fb * kv[q];
-      a.ju[vidx + q * N] = u;
-      bad = bad || !isfinite(u) || (q == 0 && !(u > 0));
+      for (int q = 0; q < NC; ++q) a.rhs[vidx + q * L.Nv] = kv[q];
+    } else {
+      // Classical RK4 (src/MHD_AMRRungeKutta.H:10-12): stage = U + (dt a) k,
+      // U_new = U + sum_s (dt b_s) k_s accumulated in stage order.  The next
+      // stage's primitives go straight to wOut (no stage state in HBM).
+      const double dt = a.invDtMax ? L.cfl_number / *a.invDtMax : a.dtv;
+      constexpr double b4[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+      constexpr double a4[3] = {0.5, 0.5, 1.0};
+      const long N = L.Nv;
+      double u[8];
+      if (a.stage < 3) {
+        const double fb = dt * b4[a.stage], fa = dt * a4[a.stage];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+          const double u0 = a.ju[vidx + q * N];
+          const double ac = a.stage == 0 ? u0 : a.acc[vidx + q * N];
+          a.acc[vidx + q * N] = ac + fb * kv[q];
+          u[q] = u0 + fa * kv[q];
+        }
+      } else {
+        const double fb = dt * b4[3];
+        bool bad = false;
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+          u[q] = a.acc[vidx + q * N] + fb * kv[q];
+          a.ju[vidx + q * N] = u[q];
+          bad = bad || !isfinite(u[q]) || (q == 0 && !(u[q] > 0));
+        }
+        if (bad && a.invalid) atomicOr(a.invalid, 1);
+        if (a.invMaxOut) rate = cflRate(L, box, i, j, k, u);
+      }
+      // src/BoxOp_SecondOrderPreStage.H:46-54: JU/J -> Cartesian primitives.
+      double wv[8];
+      const double invJ = 1.0 / (L.radial[i + L.g].w * L.grav[((size_t)block * L.na + k) * L.na + j].det);
+      cartesianPrimitiveFromConserved(wv, u, invJ, L.gamma);
+      double* wo = a.wOut + (long)box * a.wBoxStride + cw;
+#pragma unroll
+      for (int q = 0; q < NC; ++q) wo[q * a.wN] = wv[q];
     }
-    if (bad && a.invalid) atomicOr(a.invalid, 1);
   }
+  if (MODE == MODE_RK && a.stage == 3 && a.invMaxOut) warpMaxAtomic(rate, a.invMaxOut);
 }
 
 // ---------------------------------------------------------------------------
@@ -411,64 +490,14 @@ __global__ void cflKernel(const DevLevel L, const double* __restrict__ ju, unsig
     const int i = (int)(r % L.nr);
     const int j = (int)((r / L.nr) % L.na);
     const int k = (int)(r / ((long)L.nr * L.na));
-    const CflCell& a = L.cfl[((size_t)b * L.na + k) * L.na + j];
-    const double4 rd = L.radial[i + L.g];
-    const double volume = rd.w, inverseVolume = 1.0 / rd.w, width0 = rd.z * L.dxi0;
-    const double area[3] = {rd.x, rd.y, rd.y};
     double u[8];
     const double* src = ju + (long)b * NC * L.Nv + r;
 #pragma unroll
     for (int c = 0; c < NC; ++c) u[c] = src[c * L.Nv];
-    double rho = u[0] * a.inverseDet;
-    rho *= inverseVolume;
-    rho = dmax(rho, kRHO00);
-    double energy = u[4] * a.inverseDet;
-    energy *= inverseVolume;
-    double v[3], bb[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      v[d] = a.inverseDetA[3 * d] * u[1] + a.inverseDetA[3 * d + 1] * u[2] + a.inverseDetA[3 * d + 2] * u[3];
-      bb[d] = a.inverseDetA[3 * d] * u[5] + a.inverseDetA[3 * d + 1] * u[6] + a.inverseDetA[3 * d + 2] * u[7];
-      v[d] *= inverseVolume;
-      bb[d] *= inverseVolume;
-      v[d] /= rho;
-    }
-    double kinetic = 0, magnetic = 0;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const double vc = a.cell[3 * d] * v[0] + a.cell[3 * d + 1] * v[1] + a.cell[3 * d + 2] * v[2];
-      const double bc = a.cell[3 * d] * bb[0] + a.cell[3 * d + 1] * bb[1] + a.cell[3 * d + 2] * bb[2];
-      kinetic += vc * vc / 2;
-      magnetic += bc * bc / 8.0 / kPi;
-    }
-    kinetic *= rho;
-    double pressure = (energy - kinetic - magnetic) * (L.gamma - 1);
-    if (pressure < 0) pressure = 0;
-    double inverseDt = 0;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const double* basis = d == 0 ? a.cell : a.face[d - 1];
-      double v2 = 0, fullB2 = 0;
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const double velocity = basis[3 * q] * v[0] + basis[3 * q + 1] * v[1] + basis[3 * q + 2] * v[2];
-        const double field = basis[3 * q] * bb[0] + basis[3 * q + 1] * bb[1] + basis[3 * q + 2] * bb[2];
-        v2 += velocity * velocity;
-        fullB2 += field * field;
-      }
-      const double width = d == 0 ? width0 : volume * a.det[d] * L.h / area[d] / a.normal[d];
-      const double wave = sqrt(L.gamma * pressure / rho + fullB2 / 4.0 / kPi / rho);
-      inverseDt += (wave + sqrt(v2)) / width;
-    }
-    // std::max(localMaximum, x) ignores a NaN x.
-    best = best < inverseDt ? inverseDt : best;
+    const double inverseDt = cflRate(L, b, i, j, k, u);
+    best = best < inverseDt ? inverseDt : best;  // std::max(localMaximum, x)
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const double other = __shfl_xor_sync(0xffffffffu, best, o);
-    best = best < other ? other : best;
-  }
-  if ((threadIdx.x & 31) == 0 && best > 0) atomicMax(invMaxBits, (unsigned long long)__double_as_longlong(best));
+  warpMaxAtomic(best, invMaxBits);
 }
 
 __global__ void setIntKernel(int* p, int v) { *p = v; }

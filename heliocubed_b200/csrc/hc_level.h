@@ -62,7 +62,7 @@ struct DevLevel {
   const EdgeLink* edge;  // [6][2][2]
   const double* innerBC; // [6][na][na][g][8] native conserved wind, or null
   double outerScale2[kGhost], outerScale1[kGhost];
-  double gamma, entropy, cfl_number, strength, r0;
+  double gamma, invGm1, entropy, cfl_number, strength, r0;
   int innerBCType;
 };
 
@@ -83,13 +83,17 @@ struct StageArgs {
   long rhsBoxStride, rhsN;
   double* flux[3];
   const double* panel[6];
-  // level RK stage (MODE 1): k never leaves registers
+  // level RK stage (MODE 1): k never leaves registers.  The epilogue writes
+  // the next stage's primitives (valid cells) into wOut; stage 3 writes the
+  // new state into ju, its primitives into wOut and, when invMaxOut is set,
+  // the CFL rate of the new state (atomic max of the bit pattern).
   int stage;
   const double* invDtMax;  // device: dt = cfl / *invDtMax (null: use dtv)
   double dtv;
   double* ju;
   double* acc;
-  double* next;
+  double* wOut;
+  unsigned long long* invMaxOut;
   int* invalid;            // OR-ed validity flag of the new state (stage 3)
 };
 

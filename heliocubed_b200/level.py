@@ -183,6 +183,21 @@ class Shell:
         N.check(self._lib.hc_level_advance_cfl(self._ctx, _ptr(ju), nsteps, _ptr(time), _ptr(dt_out), _stream()),
                 "hc_level_advance_cfl")
 
+    def capture_advance(self, ju: torch.Tensor, nsteps: int, time: torch.Tensor,
+                        dt_out: torch.Tensor | None = None) -> "torch.cuda.CUDAGraph":
+        """Capture `advance(ju, nsteps, time)` into a CUDA graph (the launch
+        sequence has no host synchronisation or allocation).  One eager run
+        on a side stream precedes the capture, so ju advances by nsteps."""
+        g = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(device=self._dev)
+        side.wait_stream(torch.cuda.current_stream(self._dev))
+        with torch.cuda.stream(side):
+            self.advance(ju, nsteps, time, dt_out)
+        torch.cuda.current_stream(self._dev).wait_stream(side)
+        with torch.cuda.graph(g):
+            self.advance(ju, nsteps, time, dt_out)
+        return g
+
     def inv_dt_max(self, ju: torch.Tensor) -> torch.Tensor:
         out = torch.zeros(1, dtype=torch.float64, device=self._dev)
         N.check(self._lib.hc_level_dt_cfl(self._ctx, _ptr(ju), _ptr(out), _stream()), "hc_level_dt_cfl")

@@ -265,3 +265,20 @@ def test_seam_fluxes_conserve_mass(oracle_lib):
         net += -nr * (F[:, :, nr].sum() - F[:, :, 0].sum())
         mag += nr * (np.abs(F[:, :, nr]).sum() + np.abs(F[:, :, 0]).sum())
     assert abs(total - net) <= 1e-12 * mag, (total, net, mag)
+
+
+def test_graph_replay_matches_eager(oracle_lib):
+    """The step captured as a CUDA graph replays the same launches."""
+    shell, orc = _pair(oracle_lib)
+    ju = _perturbed_state(oracle_lib, orc, _spec(12, 10))
+    a = torch.from_numpy(ju.copy()).cuda()
+    b = torch.from_numpy(ju.copy()).cuda()
+    ta = torch.zeros(1, dtype=torch.float64, device="cuda")
+    tb = torch.zeros(1, dtype=torch.float64, device="cuda")
+    g = shell.capture_advance(b, 1, tb)   # one eager step + capture
+    shell.advance(a, 1, ta)
+    for _ in range(3):
+        g.replay()
+        shell.advance(a, 1, ta)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b) and torch.equal(ta, tb)

@@ -239,7 +239,7 @@ __device__ __forceinline__ void o2FaceLoop(const StageArgs& a, const double* __r
 }
 
 template <int LIM, bool ROE, int MODE>
-__global__ void __launch_bounds__(NT, ROE ? 3 : 4) o2StageKernel(const StageArgs a, const int powell, const int grav) {
+__global__ void __launch_bounds__(NT, ROE ? 2 : 3) o2StageKernel(const StageArgs a, const int powell, const int grav) {
   extern __shared__ double sF[];  // [9][NF]: 8 flux components + Powell face B_n
   const int v0 = a.hi[0] - a.lo[0] + 1, v1 = a.hi[1] - a.lo[1] + 1, v2 = a.hi[2] - a.lo[2] + 1;
   const int nbx = (v0 + TX - 1) / TX, nby = (v1 + TY - 1) / TY, nbz = (v2 + TZ - 1) / TZ;

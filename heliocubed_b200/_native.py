@@ -29,6 +29,7 @@ SIGNATURES = {
     "hc_level_prepare": (C.c_int, [_VP, _VP, _VP, C.c_double, _VP]),
     "hc_level_rhs": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hc_level_rk4_step": (C.c_int, [_VP, _VP, C.c_double, C.c_double, _VP]),
+    "hc_level_rk4_step_noalloc": (C.c_int, [_VP, _VP, C.c_double, C.c_double, _VP]),
     "hc_level_advance_cfl": (C.c_int, [_VP, _VP, C.c_int, _VP, _VP, _VP]),
     "hc_level_dt_cfl": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hc_level_valid": (C.c_int, [_VP, _VP, _VP, _VP]),

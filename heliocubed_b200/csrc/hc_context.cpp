@@ -540,6 +540,13 @@ int rkStep(hc_ctx* c, double* ju, double dtv, const double* invMax, unsigned lon
 
 }  // namespace
 
+namespace hc {
+const DevLevel* ctxLevel(const hc_ctx* c) { return &c->L; }
+const hc_params* ctxParams(const hc_ctx* c) { return &c->P; }
+int ctxDevice(const hc_ctx* c) { return c->device; }
+int setLastError(int code, const char* msg) { return fail(code, msg); }
+}  // namespace hc
+
 extern "C" {
 
 const char* hc_last_error(void) { return g_lastError.c_str(); }

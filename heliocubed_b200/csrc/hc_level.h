@@ -123,3 +123,13 @@ cudaError_t launchBitsToDouble(const unsigned long long* bits, double* out, cuda
 size_t stageSmemBytes(int mode);
 
 }  // namespace hc
+
+// Context internals for sibling translation units (not part of the C ABI).
+struct hc_ctx;
+struct hc_params;
+namespace hc {
+const DevLevel* ctxLevel(const hc_ctx* c);
+const hc_params* ctxParams(const hc_ctx* c);
+int ctxDevice(const hc_ctx* c);
+int setLastError(int code, const char* msg);
+}  // namespace hc

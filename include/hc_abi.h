@@ -136,6 +136,20 @@ int hc_level_rhs(hc_ctx* ctx, const double* w, double* k, void* stream);
 int hc_level_rk4_step(hc_ctx* ctx, double* ju, double dt, double t,
                       void* stream);
 
+/* hc_level_rk4_step without any device allocation by the library: for
+ * callers that cannot call cudaMalloc while they step (inside a stream
+ * capture, under a host framework that owns all device memory, in a serving
+ * loop that must not wait on the allocator).  Its stage workspace is one
+ * fixed 16 MiB device array inside the library (levels up to 6 x 21 x 21^2
+ * cells; larger levels return HC_ERR_ARG with the sizes), held by every GPU
+ * that loads the library until the process exits, shared by all calls on
+ * that device: calls that overlap on the GPU race, so serialise them.  The
+ * first call on a device looks up the array's device address; make that
+ * first call before any stream capture, with the context's device current.
+ * This entry point has no counterpart in the reference. */
+int hc_level_rk4_step_noalloc(hc_ctx* ctx, double* ju, double dt, double t,
+                              void* stream);
+
 /* nsteps RK4 steps with dt = cfl/max(inverse dt) computed on the device
  * before every step (exec/main.cpp:377-383).  *time_dev (device double) is
  * advanced in place; dt_dev (device double, may be NULL) receives the

@@ -26,6 +26,7 @@ SIGNATURES = {
     "hc_level_primitive_size": (C.c_size_t, [_VP]),
     "hc_box_rhs": (C.c_int, [_VP, _VP, _VP, _VP, C.c_double, _VP, _VP, _VP]),
     "hc_box_gravity": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "hc_box_rhs_o4": (C.c_int, [_VP, _VP, _VP, C.c_double, _VP, _VP, _VP]),
     "hc_level_prepare": (C.c_int, [_VP, _VP, _VP, C.c_double, _VP]),
     "hc_level_rhs": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hc_level_rk4_step": (C.c_int, [_VP, _VP, C.c_double, C.c_double, _VP]),
@@ -44,10 +45,12 @@ class HcParams(C.Structure):
         ("spatial_order", C.c_int), ("limiter", C.c_int), ("riemann_solver", C.c_int),
         ("divergence_cleaning", C.c_int), ("sun_gravity", C.c_int),
         ("init_condition_type", C.c_int), ("temporal_order", C.c_int),
-        ("nr", C.c_int), ("na", C.c_int), ("reserved_i", C.c_int * 7),
+        ("nr", C.c_int), ("na", C.c_int), ("spatial_operator", C.c_int), ("berta_detector_type", C.c_int),
+        ("berta_fallback_type", C.c_int), ("reserved_i", C.c_int * 4),
         ("gamma", C.c_double), ("entropy_fix_coeff", C.c_double), ("cfl", C.c_double),
         ("inner_radius", C.c_double), ("outer_radius", C.c_double),
-        ("radial_stretch", C.c_double), ("strength", C.c_double), ("reserved_d", C.c_double * 7),
+        ("radial_stretch", C.c_double), ("strength", C.c_double), ("berta_eta_d", C.c_double),
+        ("reserved_d", C.c_double * 6),
     ]
 
 

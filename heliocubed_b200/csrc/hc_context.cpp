@@ -244,6 +244,10 @@ struct hc_ctx {
   double* acc = nullptr;              // RK accumulator [6][8][na][na][nr]
   unsigned long long* invMax = nullptr;  // two CFL slots (bit patterns), ping-pong per step
   int* flag = nullptr;
+  // fourth-order operator: metric tables and grow-only scratch
+  O4Geo o4{};
+  double* o4scratch = nullptr;
+  size_t o4scratchDoubles = 0;
 };
 
 namespace {
@@ -473,6 +477,85 @@ int buildLevel(hc_ctx* c) {
   return HC_OK;
 }
 
+// Fourth-order metric tables over angular indices [-ext, na+ext] (ghost
+// cells beyond the panel edges use the gnomonic extension of the map) and the
+// radial table over [-kO4Rad, nr+kO4Rad].
+int buildO4Geometry(hc_ctx* c) {
+  const hc_params& P = c->P;
+  const int na = P.na, nr = P.nr, ext = kO4Ang;
+  const int n = na + 2 * ext + 1;
+  const double h = 1.0 / na;
+  Gauss G;
+  std::vector<double> face((size_t)6 * 3 * n * n * kO4FaceRec), cell((size_t)6 * n * n * 9);
+  for (int b = 0; b < 6; ++b)
+    for (int k = -ext; k <= na + ext; ++k)
+      for (int j = -ext; j <= na + ext; ++j) {
+        double A[3][3];
+        basisAt(b, (j + 0.5) * h, (k + 0.5) * h, A, nullptr);
+        double* cb = &cell[(((size_t)b * n + (k + ext)) * n + (j + ext)) * 9];
+        for (int r = 0; r < 3; ++r)
+          for (int q = 0; q < 3; ++q) cb[3 * r + q] = A[r][q];
+        for (int d = 0; d < 3; ++d) {
+          double* e = &face[((((size_t)b * 3 + d) * n + (k + ext)) * n + (j + ext)) * kO4FaceRec];
+          double dA[3][3] = {{0}}, det = 0, nn[3] = {0, 0, 0};
+          if (d == 0) {
+            for (int p = 0; p < 8; ++p)
+              for (int q = 0; q < 8; ++q) {
+                double Aq[3][3], m[3];
+                basisAt(b, (j + G.x[p]) * h, (k + G.x[q]) * h, Aq, nullptr);
+                const double wt = G.w[p] * G.w[q], dt = det3(Aq);
+                det += wt * dt;
+                cofactorRow(Aq, 0, m);
+                for (int r = 0; r < 3; ++r) {
+                  nn[r] += wt * m[r];
+                  for (int s2 = 0; s2 < 3; ++s2) dA[r][s2] += wt * dt * Aq[r][s2];
+                }
+              }
+          } else {
+            for (int p = 0; p < 8; ++p) {
+              double Aq[3][3], m[3];
+              if (d == 1) basisAt(b, j * h, (k + G.x[p]) * h, Aq, nullptr);
+              else basisAt(b, (j + G.x[p]) * h, k * h, Aq, nullptr);
+              const double dt = det3(Aq);
+              det += G.w[p] * dt;
+              cofactorRow(Aq, d, m);
+              for (int r = 0; r < 3; ++r) {
+                nn[r] += G.w[p] * m[r];
+                for (int s2 = 0; s2 < 3; ++s2) dA[r][s2] += G.w[p] * dt * Aq[r][s2];
+              }
+            }
+          }
+          snapNormal(nn);
+          for (int r = 0; r < 3; ++r)
+            for (int q = 0; q < 3; ++q) e[3 * r + q] = dA[r][q];
+          e[9] = det;
+          for (int r = 0; r < 3; ++r) e[10 + r] = nn[r];
+          double F[3][3];
+          if (d == 0) basisAt(b, (j + 0.5) * h, (k + 0.5) * h, F, nullptr);
+          else if (d == 1) basisAt(b, j * h, (k + 0.5) * h, F, nullptr);
+          else basisAt(b, (j + 0.5) * h, k * h, F, nullptr);
+          for (int r = 0; r < 3; ++r)
+            for (int q = 0; q < 3; ++q) e[13 + 3 * r + q] = F[r][q];
+        }
+      }
+  std::vector<double4> radial(nr + 2 * kO4Rad + 1);
+  for (int i = -kO4Rad; i <= nr + kO4Rad; ++i) {
+    const RadialRow r = radialRow(P, i);
+    radial[i + kO4Rad] = make_double4(r.area0, r.areaT, r.Dr0, r.vol);
+  }
+  cudaError_t err = cudaSuccess;
+  O4Geo& g = c->o4;
+  g.nr = nr; g.na = na; g.ext = ext;
+  g.face = upload(face, c->owned, err);
+  g.cell = upload(cell, c->owned, err);
+  g.radial = upload(radial, c->owned, err);
+  g.gamma = P.gamma; g.invGm1 = 1.0 / (P.gamma - 1.0); g.entropy = P.entropy_fix_coeff; g.eta_d = P.berta_eta_d;
+  g.dx[0] = 1.0 / nr; g.dx[1] = 1.0 / na; g.dx[2] = 1.0 / na;
+  g.roe = P.riemann_solver == 2; g.powell = P.divergence_cleaning == 1; g.fallback = P.berta_fallback_type;
+  if (err != cudaSuccess) return cudaFail(err, "O4 geometry upload");
+  return HC_OK;
+}
+
 int allocWorkspace(hc_ctx* c) {
   const size_t nv = 6 * NC * (size_t)c->L.Nv, ng = 6 * NC * (size_t)c->L.Ng;
   void* p;
@@ -554,7 +637,15 @@ const char* hc_last_error(void) { return g_lastError.c_str(); }
 int hc_ctx_create(const hc_params* p, int device, hc_ctx** out) {
   if (!p || !out) return fail(HC_ERR_ARG, "null argument");
   *out = nullptr;
-  if (p->spatial_order != 2) return fail(HC_ERR_UNSUPPORTED, "spatial_order must be 2 (PLM operator)");
+  if (p->spatial_order != 2 && p->spatial_order != 4)
+    return fail(HC_ERR_UNSUPPORTED, "spatial_order must be 2 (PLM) or 4 (Berta WENOZ)");
+  if (p->spatial_order == 4) {
+    if (p->spatial_operator != 2) return fail(HC_ERR_UNSUPPORTED, "at order 4 only spatial_operator 2 (Berta) is built");
+    if (p->berta_detector_type != 0) return fail(HC_ERR_UNSUPPORTED, "Berta_detector_type must be 0 (Jameson)");
+    if (p->berta_fallback_type != 0 && p->berta_fallback_type != 1) return fail(HC_ERR_ARG, "Berta_fallback_type must be 0 or 1");
+    if (!(p->berta_eta_d > 0)) return fail(HC_ERR_ARG, "Berta_eta_d must be positive");
+    if (p->na < 2 * kO4Ang) return fail(HC_ERR_ARG, "the fourth-order operator needs na >= 16");
+  }
   if (p->limiter < 0 || p->limiter > 3) return fail(HC_ERR_ARG, "limiter must be 0..3");
   if (p->riemann_solver != 1 && p->riemann_solver != 2) return fail(HC_ERR_ARG, "Riemann_solver_type must be 1 or 2");
   if (p->temporal_order != 4) return fail(HC_ERR_UNSUPPORTED, "temporal_order must be 4 (classical RK4)");
@@ -571,6 +662,7 @@ int hc_ctx_create(const hc_params* p, int device, hc_ctx** out) {
   c->device = device;
   int rc = buildLevel(c);
   if (rc == HC_OK) rc = allocWorkspace(c);
+  if (rc == HC_OK && p->spatial_order == 4) rc = buildO4Geometry(c);
   if (rc != HC_OK) {
     hc_ctx_destroy(c);
     return rc;
@@ -583,6 +675,7 @@ int hc_ctx_destroy(hc_ctx* c) {
   if (!c) return HC_OK;
   cudaSetDevice(c->device);
   for (void* p : c->owned) cudaFree(p);
+  if (c->o4scratch) cudaFree(c->o4scratch);
   delete c;
   return HC_OK;
 }
@@ -620,6 +713,66 @@ int hc_box_rhs(hc_ctx* c, const hc_box* box, const double* w, const double* cons
   return checkLaunch(launchStage(a, MODE_BOX, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
                                  false, (cudaStream_t)stream),
                      "hc_box_rhs");
+}
+
+int hc_box_rhs_o4(hc_ctx* c, const hc_box* box, const double* usph, double scale, double* rhs, double* const* flux,
+                  void* stream) {
+  if (!c || !box || !usph || !rhs) return fail(HC_ERR_ARG, "null argument");
+  if (c->P.spatial_order != 4) return fail(HC_ERR_UNSUPPORTED, "context was created with spatial_order != 4");
+  const hc_box& B = *box;
+  if (B.block < 0 || B.block > 5) return fail(HC_ERR_ARG, "block must be 0..5");
+  if (B.ghost < kO4Ghost) return fail(HC_ERR_ARG, "the Berta operator needs ghost >= 5");
+  const int n[3] = {c->P.nr, c->P.na, c->P.na};
+  for (int d = 0; d < 3; ++d)
+    if (B.lo[d] < 0 || B.hi[d] >= n[d] || B.hi[d] < B.lo[d]) return fail(HC_ERR_ARG, "box outside the panel");
+  O4Args a{};
+  a.G = c->o4;
+  a.nbox = 1;
+  a.block0 = B.block;
+  a.ghost = kO4Ghost;
+  for (int d = 0; d < 3; ++d) { a.vlo[d] = B.lo[d]; a.vhi[d] = B.hi[d]; }
+  a.U = usph;
+  for (int d = 0; d < 3; ++d) { a.ur.lo[d] = B.lo[d] - B.ghost; a.ur.n[d] = B.hi[d] - B.lo[d] + 1 + 2 * B.ghost; }
+  a.ur.N = (long)a.ur.n[0] * a.ur.n[1] * a.ur.n[2];
+  a.uStride = 8 * a.ur.N;
+  a.scale = scale;
+  a.rhs = rhs;
+  a.rhsStride = 8L * (B.hi[0] - B.lo[0] + 1) * (B.hi[1] - B.lo[1] + 1) * (B.hi[2] - B.lo[2] + 1);
+  for (int d = 0; d < 3; ++d) a.flux[d] = flux ? flux[d] : nullptr;
+  // grow-only scratch (allocated outside any stream capture on first use)
+  const size_t need = o4ScratchDoubles(1, a.vlo, a.vhi, kO4Ghost);
+  if (need > c->o4scratchDoubles) {
+    if (c->o4scratch) cudaFree(c->o4scratch);
+    c->o4scratch = nullptr;
+    c->o4scratchDoubles = 0;
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, need * sizeof(double));
+    if (e != cudaSuccess) return cudaFail(e, "O4 scratch");
+    c->o4scratch = static_cast<double*>(p);
+    c->o4scratchDoubles = need;
+  }
+  double* sp = c->o4scratch;
+  Reg g{};
+  {
+    int lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) { lo[d] = B.lo[d] - kO4Ghost; hi[d] = B.hi[d] + kO4Ghost; }
+    g.N = (long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+  }
+  long nf = 1, n1 = 1, n2 = 1;
+  for (int d = 0; d < 3; ++d) {
+    const int ext = B.hi[d] - B.lo[d] + 1;
+    nf *= ext + 2 * kO4Ghost - 6 + 1;
+    n1 *= ext + 2;
+    n2 *= ext + 4;
+  }
+  a.WA = sp; sp += 8 * g.N;
+  a.WP = sp; sp += 8 * g.N;
+  a.th = sp; sp += g.N;
+  a.thr = sp; sp += g.N;
+  a.face = sp; sp += (long)kO4FaceArrays * nf;
+  a.mj = sp; sp += n1;
+  a.kp = sp;
+  return checkLaunch(launchO4BoxOperator(a, (cudaStream_t)stream), "hc_box_rhs_o4");
 }
 
 int hc_box_gravity(hc_ctx* c, const hc_box* box, const double* w, double* rhs, void* stream) {

@@ -124,6 +124,63 @@ size_t stageSmemBytes(int mode);
 
 }  // namespace hc
 
+namespace hc {
+// ---------------------------------------------------------------------------
+// Fourth-order Berta operator (hc_o4.cu).
+// ---------------------------------------------------------------------------
+constexpr int kO4Ghost = 5;  // NGHOST: Jameson detector + WENOZ + transverse products
+constexpr int kO4Ang = 8;    // angular margin of the O4 metric tables
+constexpr int kO4Rad = 10;   // radial margin of the O4 radial table
+
+// Face metrics of direction d at angular (j,k): <det A A> (9), <det A> (1),
+// <adjA row d> (3), pointwise basis at the face centre (9; d = 0: cell centre).
+constexpr int kO4FaceRec = 22;
+
+struct O4Geo {
+  int nr, na, ext;        // tables cover angular indices [-ext, na+ext]
+  const double* face;     // [6][3][na+2ext+1 (k)][na+2ext+1 (j)][22]
+  const double* cell;     // [6][na+2ext+1][na+2ext+1][9] cell-centre basis
+  const double4* radial;  // [nr+2*kO4Rad+1], index i+kO4Rad: {rlow^2, areaT, Dr0, dVolr}
+  double gamma, invGm1, entropy, eta_d, dx[3];
+  int roe, powell, fallback;
+};
+
+// A box region: low corner, extents, cell count.
+struct Reg {
+  int lo[3], n[3];
+  long N;
+};
+
+// One batched O4 operator evaluation: nbox boxes (panels block0 + b) with
+// the same valid box [vlo, vhi]; U on valid.grow(ghost) in the caller's
+// storage (region ur, box stride uStride); rhs accumulated on the valid box.
+struct O4Args {
+  O4Geo G;
+  int nbox, block0, ghost;
+  int vlo[3], vhi[3];
+  const double* U;
+  Reg ur;
+  long uStride;
+  double scale;
+  double* rhs;
+  long rhsStride;
+  double* flux[3];
+  // scratch (device): cell arrays on the ghosted box, face arrays on the
+  // reconstruction face box of the current direction
+  double* WA;   // [nbox][8][G]
+  double* WP;   // [nbox][8][G]
+  double* th;   // [nbox][G]
+  double* thr;  // [nbox][G] raw detector flag
+  double* face; // [nbox][kO4FaceArrays][F]
+  double* mj;   // [nbox][V+1]
+  double* kp;   // [nbox][8][V+2]
+};
+constexpr int kO4FaceArrays = 8 * 9 + 8;  // WL, WR, FS, QD/DP, FA, FM, FR, Fx (8 each) + thF, PS, BP, PA, T3, Bflux, Bprod, pad
+
+cudaError_t launchO4BoxOperator(const O4Args& a, cudaStream_t s);
+size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost);
+}  // namespace hc
+
 // Context internals for sibling translation units (not part of the C ABI).
 struct hc_ctx;
 struct hc_params;

@@ -1,0 +1,1007 @@
+// Fourth-order Berta pointwise-WENOZ operator on batched ghosted boxes,
+// src/BoxOp_BertaCubedSphereImplem.H:1737-2076 with the Roe glue of
+// src/BoxOp_RoeCubedSphere.H:29-145 and the Powell terms of
+// src/BoxOp_DivBcleaning.H:35-172.  FP64.
+//
+// One kernel per stage of the operator; every intermediate lives on the box
+// the reference computes it on (cell arrays on the ghosted box G, face arrays
+// on the reconstruction face box F = G.extrude(d).grow(-3) of direction d).
+// Each kernel covers the region where its result is defined; a thread
+// handles one cell or face of one box.
+#include <cuda_runtime.h>
+
+#include "hc_device.cuh"
+#include "hc_level.h"
+
+namespace hc {
+namespace {
+
+struct Box3 {
+  int lo[3], hi[3];
+  __host__ __device__ Box3 grow(int g) const { Box3 b = *this; for (int d = 0; d < 3; ++d) { b.lo[d] -= g; b.hi[d] += g; } return b; }
+  __host__ __device__ Box3 growTrans(int d, int g) const {
+    Box3 b = *this;
+    for (int t = 0; t < 3; ++t) if (t != d) { b.lo[t] -= g; b.hi[t] += g; }
+    return b;
+  }
+  __host__ __device__ Box3 extrude(int d) const { Box3 b = *this; b.hi[d] += 1; return b; }
+  __host__ __device__ int n(int d) const { return hi[d] - lo[d] + 1; }
+  __host__ __device__ long size() const { return (long)n(0) * n(1) * n(2); }
+};
+
+__host__ __device__ inline Reg regOf(const Box3& b) {
+  Reg r;
+  for (int d = 0; d < 3; ++d) { r.lo[d] = b.lo[d]; r.n[d] = b.n(d); }
+  r.N = b.size();
+  return r;
+}
+
+__device__ __forceinline__ long roff(const Reg& r, int i, int j, int k) {
+  return (long)(i - r.lo[0]) + (long)r.n[0] * ((long)(j - r.lo[1]) + (long)r.n[1] * (long)(k - r.lo[2]));
+}
+
+// Offsets of the face arrays inside a box's face scratch (units of F.N).
+enum FaceArr { F_WL = 0, F_WR = 8, F_FS = 16, F_QD = 24, F_FA = 32, F_FM = 40, F_FR = 48, F_FX = 56,
+               F_THF = 64, F_PS = 65, F_BP = 66, F_PA = 67, F_T3 = 68, F_BFLUX = 69, F_BPROD = 70 };
+
+struct Ctx {
+  O4Args a;
+  int d;
+  Box3 V, G, GR, GD, F, F1, F2, V0, V1, V2;
+  Reg gr, fr, v1r, v2r, vr;
+};
+
+Ctx makeCtx(const O4Args& a, int d) {
+  Ctx c;
+  c.a = a;
+  c.d = d;
+  for (int q = 0; q < 3; ++q) { c.V.lo[q] = a.vlo[q]; c.V.hi[q] = a.vhi[q]; }
+  c.G = c.V.grow(a.ghost);
+  c.GR = c.G.grow(-1);
+  c.GD = c.G.grow(-2);
+  c.F = c.G.extrude(d).grow(-3);
+  c.F1 = c.F.growTrans(d, -1);
+  c.F2 = c.F1.growTrans(d, -1);
+  c.V0 = c.V.extrude(d);
+  c.V1 = c.V.grow(1);
+  c.V2 = c.V.grow(2);
+  c.gr = regOf(c.G);
+  // face scratch is laid out on the largest face box over the directions
+  Box3 FB = c.G.grow(-3);
+  for (int q = 0; q < 3; ++q) FB.hi[q] += 1;
+  c.fr = regOf(FB);
+  c.v1r = regOf(c.V1);
+  c.v2r = regOf(c.V2);
+  c.vr = regOf(c.V);
+  return c;
+}
+
+// ---- geometry access -------------------------------------------------------
+__device__ __forceinline__ const double* faceRec(const O4Geo& g, int block, int d, int j, int k) {
+  const long n = g.na + 2 * g.ext + 1;
+  return g.face + ((((long)block * 3 + d) * n + (k + g.ext)) * n + (j + g.ext)) * kO4FaceRec;
+}
+__device__ __forceinline__ const double* cellBasis(const O4Geo& g, int block, int j, int k) {
+  const long n = g.na + 2 * g.ext + 1;
+  return g.cell + (((long)block * n + (k + g.ext)) * n + (j + g.ext)) * 9;
+}
+__device__ __forceinline__ double4 radialRow(const O4Geo& g, int i) { return g.radial[i + kO4Rad]; }
+__device__ __forceinline__ double adjDr(const O4Geo& g, int d, int i) {
+  const double4 r = radialRow(g, i);
+  return d == 0 ? r.x : r.y;
+}
+__device__ __forceinline__ double radialPoint(const O4Geo& g, int d, int i) {
+  if (d == 0) return adjDr(g, 0, i);
+  const double a = adjDr(g, d, i);
+  return a - (1.0 / 24.0) * (adjDr(g, d, i + 1) - 2.0 * a + adjDr(g, d, i - 1));
+}
+
+// ---- pointwise pieces -----------------------------------------------------
+// f_sphToPrim + energies + pressure (src/BoxOp_BertaCubedSphereImplem.H:212-340)
+__device__ void sphToPrim(const double u[8], const double* A, double gamma, double w[8]) {
+  w[0] = dmax(u[0], kRHO00);
+  w[1] = u[1] / w[0];
+  w[2] = u[2] / w[0];
+  w[3] = u[3] / w[0];
+  w[4] = u[4];
+  w[5] = u[5]; w[6] = u[6]; w[7] = u[7];
+  double ke = 0., me = 0.;
+#pragma unroll
+  for (int d0 = 0; d0 < 3; ++d0) {
+    const double vc = A[3 * d0] * w[1] + A[3 * d0 + 1] * w[2] + A[3 * d0 + 2] * w[3];
+    const double bc = A[3 * d0] * w[5] + A[3 * d0 + 1] * w[6] + A[3 * d0 + 2] * w[7];
+    ke += vc * vc / 2;
+    me += bc * bc / 8.0 / kPi;
+  }
+  ke *= w[0];
+  w[4] = (w[4] - ke - me) * (gamma - 1.0);
+  if (w[4] < 0.0) w[4] = 0.0;
+}
+
+// EnergyW (src/BoxOp_Utilities.H:447-520)
+__device__ void energyW(const double w[8], const double* A, double& ke, double& me, double& vb) {
+  ke = 0.; me = 0.; vb = 0.;
+#pragma unroll
+  for (int d0 = 0; d0 < 3; ++d0) {
+    const double vc = A[3 * d0] * w[1] + A[3 * d0 + 1] * w[2] + A[3 * d0 + 2] * w[3];
+    const double bc = A[3 * d0] * w[5] + A[3 * d0 + 1] * w[6] + A[3 * d0 + 2] * w[7];
+    ke += vc * vc;
+    me += bc * bc / 8.0 / kPi;
+    vb += vc * bc;
+  }
+  ke *= w[0] * .5;
+}
+
+// f_primflux (src/BoxOp_EulerCubedSphere.H:195-225)
+__device__ void primFlux(double f[8], const double w[8], double ke, double me, double vb, double gamma, int c) {
+  const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+  const double velnorm = w[c + 1], veltan1 = w[c1 + 1], veltan2 = w[c2 + 1];
+  const double bnorm = w[c + 5], btan1 = w[c1 + 5], btan2 = w[c2 + 5];
+  f[0] = w[0] * velnorm;
+  f[c + 1] = f[0] * velnorm - bnorm * bnorm / 4.0 / kPi;
+  f[c1 + 1] = f[0] * veltan1 - bnorm * btan1 / 4.0 / kPi;
+  f[c2 + 1] = f[0] * veltan2 - bnorm * btan2 / 4.0 / kPi;
+  f[4] = (2.0 * me + ke + w[4] * gamma / (gamma - 1.0)) * velnorm - bnorm * vb / 4.0 / kPi;
+  f[5] = velnorm * w[5] - w[1] * bnorm;
+  f[6] = velnorm * w[6] - w[2] * bnorm;
+  f[7] = velnorm * w[7] - w[3] * bnorm;
+}
+
+// bertaNormalizeWenoStencil (:747-773)
+template <int N>
+__device__ double normalizeStencil(double (&v)[N]) {
+  double scale = 0.0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) scale = dmax(scale, fabs(v[i]));
+  if (scale == 0.0) {
+    for (int i = 0; i < N; ++i) if (v[i] != 0.0) return v[i];
+    return scale;
+  }
+  if (scale > 0.0) {
+    if (scale >= 2.2250738585072014e-308) {
+      const double inverse = 1.0 / scale;
+#pragma unroll
+      for (int i = 0; i < N; ++i) v[i] *= inverse;
+    } else {
+      for (int i = 0; i < N; ++i) v[i] /= scale;
+    }
+  }
+  return scale;
+}
+
+__device__ void wenozSide(double m2, double m1, double c0, double p1, double p2, double& out) {
+  const double eps = 1.0e-40, d0 = 1.0 / 16.0, d1 = 5.0 / 8.0, d2 = 5.0 / 16.0;
+  const double q0 = (3.0 * m2 - 10.0 * m1 + 15.0 * c0) / 8.0;
+  const double q1 = (-m1 + 6.0 * c0 + 3.0 * p1) / 8.0;
+  const double q2 = (3.0 * c0 + 6.0 * p1 - p2) / 8.0;
+  const double b0a = m2 - 2.0 * m1 + c0, b0b = m2 - 4.0 * m1 + 3.0 * c0;
+  const double b1a = m1 - 2.0 * c0 + p1, b1b = m1 - p1;
+  const double b2a = c0 - 2.0 * p1 + p2, b2b = 3.0 * c0 - 4.0 * p1 + p2;
+  const double beta0 = (13.0 / 12.0) * b0a * b0a + 0.25 * b0b * b0b;
+  const double beta1 = (13.0 / 12.0) * b1a * b1a + 0.25 * b1b * b1b;
+  const double beta2 = (13.0 / 12.0) * b2a * b2a + 0.25 * b2b * b2b;
+  const double tau5 = fabs(beta0 - beta2);
+  const double a0 = d0 * (1.0 + tau5 / (beta0 + eps));
+  const double a1 = d1 * (1.0 + tau5 / (beta1 + eps));
+  const double a2 = d2 * (1.0 + tau5 / (beta2 + eps));
+  const double asum = a0 + a1 + a2;
+  out = (a0 * q0 + a1 * q1 + a2 * q2) / asum;
+}
+
+// f_wenoz_pointwise_faceF (:782-878), one component, cells W[i-3..i+2].
+__device__ void wenozFace(const double in[6], double& L, double& R) {
+  double v[6] = {in[0], in[1], in[2], in[3], in[4], in[5]};
+  const double scale = normalizeStencil(v);
+  if (scale == 0.0) { L = R = 0.0; return; }
+  double l, r;
+  wenozSide(v[0], v[1], v[2], v[3], v[4], l);
+  wenozSide(v[5], v[4], v[3], v[2], v[1], r);
+  L = scale * l;
+  R = scale * r;
+}
+
+// f_weno3_pointwise_faceF (:881-946), one component, cells W[i-2..i+1].
+__device__ void weno3Face(const double in[4], double dx2, double& L, double& R) {
+  const double d0 = 3.0 / 4.0, d1 = 1.0 / 4.0, eps = dx2;
+  double v[4] = {in[0], in[1], in[2], in[3]};
+  const double scale = normalizeStencil(v);
+  if (scale == 0.0) { L = R = 0.0; return; }
+  {
+    const double vm1 = v[0], v0 = v[1], vp1 = v[2];
+    const double Dm = v0 - vm1, Dp = vp1 - v0;
+    const double beta0 = Dp * Dp, beta1 = Dm * Dm, tau = (Dp - Dm) * (Dp - Dm);
+    const double a0 = d0 * (1.0 + tau / (beta0 + eps)), a1 = d1 * (1.0 + tau / (beta1 + eps));
+    const double q0 = 0.5 * (vp1 + v0), q1 = 0.5 * (-vm1 + 3.0 * v0);
+    L = scale * ((a0 * q0 + a1 * q1) / (a0 + a1));
+  }
+  {
+    const double rm1 = v[3], r0 = v[2], rp1 = v[1];
+    const double Dm = r0 - rm1, Dp = rp1 - r0;
+    const double beta0 = Dp * Dp, beta1 = Dm * Dm, tau = (Dp - Dm) * (Dp - Dm);
+    const double a0 = d0 * (1.0 + tau / (beta0 + eps)), a1 = d1 * (1.0 + tau / (beta1 + eps));
+    const double q0 = 0.5 * (rp1 + r0), q1 = 0.5 * (-rm1 + 3.0 * r0);
+    R = scale * ((a0 * q0 + a1 * q1) / (a0 + a1));
+  }
+}
+
+__device__ double minmod3(double a, double b, double c) {
+  if (a > 0.0 && b > 0.0 && c > 0.0) return dmin(a, dmin(b, c));
+  if (a < 0.0 && b < 0.0 && c < 0.0) return dmax(a, dmax(b, c));
+  return 0.0;
+}
+
+// f_plm_pointwise_faceF (:949-991), one component, cells W[i-2..i+1].
+__device__ void plmFallbackFace(const double in[4], double& L, double& R) {
+  const double theta = 1.5;
+  const double dm = in[1] - in[0], dp = in[2] - in[1], dc = 0.5 * (in[2] - in[0]);
+  L = in[1] + 0.5 * minmod3(theta * dm, dc, theta * dp);
+  const double rdm = in[2] - in[1], rdp = in[3] - in[2], rdc = 0.5 * (in[3] - in[1]);
+  R = in[2] - 0.5 * minmod3(theta * rdm, rdc, theta * rdp);
+}
+
+__device__ bool usablePrimitive(const double w[8]) {
+  bool ok = true;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) ok = ok && isfinite(w[c]);
+  return ok && w[0] >= kRHO00 && w[4] >= 0.0;
+}
+
+// mappedRoe8WaveDissipation + factoredRoe8WaveDissipation (src/MHD_Roe8Wave.H:634-740)
+__device__ void factoredRoe(double out[8], const double* wl, const double* wr, const double* A, double radialArea,
+                            int dir, double gamma, double invGm1, double entropy) {
+  const int t1 = (dir + 1) % 3, t2 = (dir + 2) % 3;
+  double f0[3], f1[3], f2[3], normal2 = 0.0, tangent2 = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int j = (i + 1) % 3, k = (i + 2) % 3;
+    f0[i] = A[3 * j + t1] * A[3 * k + t2] - A[3 * k + t1] * A[3 * j + t2];
+    f1[i] = A[3 * i + t1];
+    normal2 += f0[i] * f0[i];
+    tangent2 += f1[i] * f1[i];
+  }
+  const double normalMag = sqrt(normal2), tangentMag = sqrt(tangent2);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) { f0[i] /= normalMag; f1[i] /= tangentMag; }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int j = (i + 1) % 3, k = (i + 2) % 3;
+    f2[i] = f0[j] * f1[k] - f0[k] * f1[j];
+  }
+  double loc[2][8];
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const double* w = side == 0 ? wl : wr;
+    loc[side][0] = fmax(w[0], kRHO00);
+    loc[side][4] = fmax(w[4], 0.0);
+    double vC[3], bC[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      vC[i] = A[3 * i] * w[1] + A[3 * i + 1] * w[2] + A[3 * i + 2] * w[3];
+      bC[i] = A[3 * i] * w[5] + A[3 * i + 1] * w[6] + A[3 * i + 2] * w[7];
+    }
+    loc[side][1] = f0[0] * vC[0] + f0[1] * vC[1] + f0[2] * vC[2];
+    loc[side][2] = f1[0] * vC[0] + f1[1] * vC[1] + f1[2] * vC[2];
+    loc[side][3] = f2[0] * vC[0] + f2[1] * vC[1] + f2[2] * vC[2];
+    loc[side][5] = f0[0] * bC[0] + f0[1] * bC[1] + f0[2] * bC[2];
+    loc[side][6] = f1[0] * bC[0] + f1[1] * bC[1] + f1[2] * bC[2];
+    loc[side][7] = f2[0] * bC[0] + f2[1] * bC[1] + f2[2] * bC[2];
+  }
+  double diss[8];
+  if (!roe8WaveDissipation<true>(diss, loc[0], loc[1], gamma, entropy, invGm1))
+    rusanovDissipation(diss, loc[0], loc[1], gamma, invGm1);
+  const double area = radialArea * normalMag;
+  double mapped[8];
+  mapped[0] = area * diss[0];
+  mapped[4] = area * diss[4];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    mapped[1 + i] = area * f0[i] * diss[1] + area * f1[i] * diss[2] + area * f2[i] * diss[3];
+    mapped[5 + i] = area * f0[i] * diss[5] + area * f1[i] * diss[6] + area * f2[i] * diss[7];
+  }
+  double adj[3][3];
+#pragma unroll
+  for (int dd = 0; dd < 3; ++dd) {
+    const int s1 = (dd + 1) % 3, s2 = (dd + 2) % 3;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int j = (i + 1) % 3, k = (i + 2) % 3;
+      adj[dd][i] = A[3 * j + s1] * A[3 * k + s2] - A[3 * k + s1] * A[3 * j + s2];
+    }
+  }
+  const double det = A[0] * adj[0][0] + A[3] * adj[0][1] + A[6] * adj[0][2];
+  out[0] = mapped[0] / det;
+  out[4] = mapped[4] / det;
+  const double det2 = det * det;
+#pragma unroll
+  for (int dd = 0; dd < 3; ++dd) {
+    out[1 + dd] = adj[dd][0] * mapped[1] / det2 + adj[dd][1] * mapped[2] / det2 + adj[dd][2] * mapped[3] / det2;
+    out[5 + dd] = adj[dd][0] * mapped[5] / det2 + adj[dd][1] * mapped[6] / det2 + adj[dd][2] * mapped[7] / det2;
+  }
+}
+
+// ---- stencils on scratch arrays --------------------------------------------
+struct View {
+  const double* p;
+  Reg r;
+  __device__ double operator()(int c, int i, int j, int k) const { return p[c * r.N + roff(r, i, j, k)]; }
+};
+
+__device__ __forceinline__ void stepDir(int q[3], int d, int s) { q[d] += s; }
+
+__device__ double lapFace(const View& f, int c, int d, int i, int j, int k) {
+  const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+  int a[3] = {i, j, k}, b[3] = {i, j, k}, e[3] = {i, j, k}, g[3] = {i, j, k};
+  a[t1] -= 1; b[t1] += 1; e[t2] -= 1; g[t2] += 1;
+  return (f(c, a[0], a[1], a[2]) + f(c, b[0], b[1], b[2])) + (f(c, e[0], e[1], e[2]) + f(c, g[0], g[1], g[2])) -
+         4.0 * f(c, i, j, k);
+}
+
+__device__ double cdiff(const View& f, int c, int t, int i, int j, int k) {
+  int a[3] = {i, j, k}, b[3] = {i, j, k};
+  a[t] += 1; b[t] -= 1;
+  return 0.5 * f(c, a[0], a[1], a[2]) - 0.5 * f(c, b[0], b[1], b[2]);
+}
+
+__device__ double lapCell(const View& f, int c, int i, int j, int k) {
+  return (f(c, i - 1, j, k) + f(c, i + 1, j, k)) + (f(c, i, j - 1, k) + f(c, i, j + 1, k)) +
+         (f(c, i, j, k - 1) + f(c, i, j, k + 1)) - 6.0 * f(c, i, j, k);
+}
+
+__device__ __forceinline__ double faceProd(double f4, double g4, double df0, double dg0, double df1, double dg1) {
+  double value = 0.0;
+  value += df0 * dg0 * (1.0 / 12.0);
+  value += df1 * dg1 * (1.0 / 12.0);
+  value += f4 * g4 * 1.0;
+  return value;
+}
+
+// Decode thread -> (box, i, j, k) over box region b.
+template <class F>
+__device__ __forceinline__ void forRegion(const Box3& b, int nbox, F f) {
+  const long n = b.size();
+  const long total = n * nbox;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const int box = (int)(t / n);
+    const long r = t - (long)box * n;
+    const int i = b.lo[0] + (int)(r % b.n(0));
+    const int j = b.lo[1] + (int)((r / b.n(0)) % b.n(1));
+    const int k = b.lo[2] + (int)(r / ((long)b.n(0) * b.n(1)));
+    f(box, i, j, k);
+  }
+}
+
+// ---- kernels ------------------------------------------------------------------
+// 1. detector primitives of the averages, V(<U>) (:1776).
+__global__ void o4PrimAvgKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  forRegion(c.G, a.nbox, [&](int b, int i, int j, int k) {
+    double u[8], w[8];
+    const double* U = a.U + b * a.uStride + roff(a.ur, i, j, k);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) u[q] = U[q * a.ur.N];
+    sphToPrim(u, cellBasis(a.G, a.block0 + b, j, k), a.G.gamma, w);
+    double* W = a.WA + (long)b * 8 * c.gr.N + roff(c.gr, i, j, k);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) W[q * c.gr.N] = w[q];
+  });
+}
+
+__device__ __forceinline__ double magp(const double* W, long N, long o) {
+  const double bx = W[5 * N + o], by = W[6 * N + o], bz = W[7 * N + o];
+  return 0.5 * (bx * bx + by * by + bz * bz);
+}
+__device__ __forceinline__ double eta1(double qm, double q0, double qp) {
+  const double num = fabs(qp - 2.0 * q0 + qm);
+  const double den = fabs(qp) + 2.0 * fabs(q0) + fabs(qm) + 1.0e-40;
+  return num / den;
+}
+
+// 2. raw Jameson flag on G.grow(-1) (:347-402).
+__global__ void o4ThetaRawKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  forRegion(c.GR, a.nbox, [&](int b, int i, int j, int k) {
+    const double* W = a.WA + (long)b * 8 * c.gr.N;
+    const long N = c.gr.N, o = roff(c.gr, i, j, k);
+    double et[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      int m[3] = {i, j, k}, p[3] = {i, j, k};
+      m[d] -= 1; p[d] += 1;
+      const long om = roff(c.gr, m[0], m[1], m[2]), op = roff(c.gr, p[0], p[1], p[2]);
+      const double er = eta1(W[om], W[o], W[op]);
+      const double ep = eta1(W[4 * N + om], W[4 * N + o], W[4 * N + op]);
+      const double em = eta1(magp(W, N, om), magp(W, N, o), magp(W, N, op));
+      et[d] = dmax(er, dmax(ep, em));
+    }
+    const double eta = sqrt(et[0] * et[0] + et[1] * et[1] + et[2] * et[2]);
+    a.thr[(long)b * N + o] = eta < a.G.eta_d ? 1.0 : 0.0;
+  });
+}
+
+// 3. dilated theta (0 outside G.grow(-2)), theta-aware average-to-point and
+// point primitives on G (:404-507, 696-741, 212-275).
+__global__ void o4PointKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  forRegion(c.G, a.nbox, [&](int b, int i, int j, int k) {
+    const long N = c.gr.N, o = roff(c.gr, i, j, k);
+    const double* R = a.thr + (long)b * N;
+    double t = 0.0;
+    const bool inD = i >= c.GD.lo[0] && i <= c.GD.hi[0] && j >= c.GD.lo[1] && j <= c.GD.hi[1] && k >= c.GD.lo[2] &&
+                     k <= c.GD.hi[2];
+    if (inD) {
+      t = R[o];
+      t = dmin(t, R[roff(c.gr, i - 1, j, k)]);
+      t = dmin(t, R[roff(c.gr, i + 1, j, k)]);
+      t = dmin(t, R[roff(c.gr, i, j - 1, k)]);
+      t = dmin(t, R[roff(c.gr, i, j + 1, k)]);
+      t = dmin(t, R[roff(c.gr, i, j, k - 1)]);
+      t = dmin(t, R[roff(c.gr, i, j, k + 1)]);
+    }
+    a.th[(long)b * N + o] = t;
+    const bool inner = i >= c.GR.lo[0] && i <= c.GR.hi[0] && j >= c.GR.lo[1] && j <= c.GR.hi[1] &&
+                       k >= c.GR.lo[2] && k <= c.GR.hi[2];
+    View U{a.U + b * a.uStride, a.ur};
+    double u[8], w[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) u[q] = (inner && t > 0.5) ? U(q, i, j, k) - lapCell(U, q, i, j, k) / 24.0 : U(q, i, j, k);
+    sphToPrim(u, cellBasis(a.G, a.block0 + b, j, k), a.G.gamma, w);
+    double* W = a.WP + (long)b * 8 * N + o;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) W[q * N] = w[q];
+  });
+}
+
+__device__ __forceinline__ double* faceArr(const Ctx& c, int b, int arr) {
+  return c.a.face + ((long)b * kO4FaceArrays + arr) * c.fr.N;
+}
+__device__ __forceinline__ View faceView(const Ctx& c, int b, int arr) { return View{faceArr(c, b, arr), c.fr}; }
+__device__ __forceinline__ const double* faceBasis(const Ctx& c, int b, int j, int k) {
+  return c.d == 0 ? cellBasis(c.a.G, c.a.block0 + b, j, k) : faceRec(c.a.G, c.a.block0 + b, c.d, j, k) + 13;
+}
+
+// 4. reconstruction (WENOZ / WENO3 / PLM with clamps), Roe repair, energies,
+// point flux sum, total-pressure sum, centred normal B, Rusanov jump (F).
+__global__ void o4FaceReconKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  const int d = c.d;
+  const double dx2 = a.G.dx[d] * a.G.dx[d];
+  forRegion(c.F, a.nbox, [&](int b, int i, int j, int k) {
+    const long NG = c.gr.N, NF = c.fr.N;
+    const double* th = a.th + (long)b * NG;
+    const double* WP = a.WP + (long)b * 8 * NG;
+    const double* WA = a.WA + (long)b * 8 * NG;
+    long cell[6];
+#pragma unroll
+    for (int s = -3; s <= 2; ++s) {
+      int q[3] = {i, j, k};
+      q[d] += s;
+      cell[s + 3] = roff(c.gr, q[0], q[1], q[2]);
+    }
+    const long fo = roff(c.fr, i, j, k);
+    double thF = dmin(th[cell[2]], th[cell[3]]);
+    double value = th[cell[0]];
+    value = dmin(value, th[cell[1]]);
+    value = dmin(value, th[cell[2]]);
+    value = dmin(value, th[cell[3]]);
+    value = dmin(value, th[cell[4]]);
+    const double thR = dmin(value, th[cell[5]]);
+    const bool smooth = thR > 0.5;
+    double l[8], r[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      double L, R;
+      if (smooth) {
+        const double st[6] = {WP[q * NG + cell[0]], WP[q * NG + cell[1]], WP[q * NG + cell[2]],
+                              WP[q * NG + cell[3]], WP[q * NG + cell[4]], WP[q * NG + cell[5]]};
+        wenozFace(st, L, R);
+      } else {
+        const double st[4] = {WP[q * NG + cell[1]], WP[q * NG + cell[2]], WP[q * NG + cell[3]], WP[q * NG + cell[4]]};
+        if (a.G.fallback == 0) weno3Face(st, dx2, L, R);
+        else plmFallbackFace(st, L, R);
+      }
+      if (q == 0) { L = dmax(L, kRHO00); R = dmax(R, kRHO00); }
+      if (q == 4) { L = dmax(L, 1.0e-12); R = dmax(R, 1.0e-12); }
+      l[q] = L;
+      r[q] = R;
+    }
+    if (a.G.roe) {
+      double cl[8], cr[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) { cl[q] = WA[q * NG + cell[2]]; cr[q] = WA[q * NG + cell[3]]; }
+      if (!(usablePrimitive(l) && usablePrimitive(r)) && usablePrimitive(cl) && usablePrimitive(cr)) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) { l[q] = cl[q]; r[q] = cr[q]; }
+        thF = 0.0;
+      }
+    }
+    double* base = a.face + (long)b * kO4FaceArrays * NF + fo;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { base[(F_WL + q) * NF] = l[q]; base[(F_WR + q) * NF] = r[q]; }
+    base[F_THF * NF] = thF;
+    const double* A = faceBasis(c, b, j, k);
+    double kl, ml, vl, kr, mr, vr, fl[8], fr[8];
+    energyW(l, A, kl, ml, vl);
+    energyW(r, A, kr, mr, vr);
+    primFlux(fl, l, kl, ml, vl, a.G.gamma, d);
+    primFlux(fr, r, kr, mr, vr, a.G.gamma, d);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) base[(F_FS + q) * NF] = fl[q] + fr[q];
+    base[F_PS * NF] = (l[4] + ml) + (r[4] + mr);
+    base[F_BP * NF] = (l[5 + d] + r[5 + d]) * 0.5;
+    if (!a.G.roe) {
+      const double rad = radialPoint(a.G, d, i);
+      const double g = a.G.gamma;
+      base[(F_QD + 0) * NF] = rad * r[0] - rad * l[0];
+#pragma unroll
+      for (int e = 0; e < 3; ++e) {
+        base[(F_QD + 1 + e) * NF] = rad * r[0] * r[1 + e] - rad * l[0] * l[1 + e];
+        base[(F_QD + 5 + e) * NF] = rad * r[5 + e] - rad * l[5 + e];
+      }
+      base[(F_QD + 4) * NF] = rad * (kr + mr + r[4] / (g - 1.0)) - rad * (kl + ml + l[4] / (g - 1.0));
+    }
+  });
+}
+
+// 4b. pointwise factored Roe dissipation on the final faces + one transverse
+// ring (src/BoxOp_RoeCubedSphere.H:73-98).
+__global__ void o4RoePointKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  const int d = c.d;
+  const Box3 PB = c.V0.growTrans(d, 1);
+  forRegion(PB, a.nbox, [&](int b, int i, int j, int k) {
+    const long NF = c.fr.N;
+    double* base = a.face + (long)b * kO4FaceArrays * NF + roff(c.fr, i, j, k);
+    double l[8], r[8], o[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { l[q] = base[(F_WL + q) * NF]; r[q] = base[(F_WR + q) * NF]; }
+    factoredRoe(o, l, r, faceBasis(c, b, j, k), radialPoint(a.G, d, i), d, a.G.gamma, a.G.invGm1, a.G.entropy);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) base[(F_QD + q) * NF] = o[q];
+  });
+}
+
+// 5. theta-aware point-to-average of the flux sum and total pressure (F1).
+__global__ void o4FaceAvgKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  const int d = c.d;
+  forRegion(c.F1, a.nbox, [&](int b, int i, int j, int k) {
+    const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
+    double* base = a.face + (long)b * kO4FaceArrays * NF;
+    const bool sm = base[F_THF * NF + fo] > 0.5;
+    const View FS = faceView(c, b, F_FS);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const double pt = FS(q, i, j, k);
+      base[(F_FA + q) * NF + fo] = sm ? pt + lapFace(FS, q, d, i, j, k) / 24.0 : pt;
+    }
+    const View PS = faceView(c, b, F_PS);
+    const double pp = PS(0, i, j, k);
+    base[F_PA * NF + fo] = sm ? pp + lapFace(PS, 0, d, i, j, k) / 24.0 : pp;
+  });
+}
+
+// 6. mapped flux with separable metrics (bertaMapHostBox, :35-95 and
+// :1361-1450) on F1; zero on F outside it.
+__global__ void o4FaceMapKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  const int d = c.d;
+  const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+  const bool skipFirst = t1 == 0;
+  forRegion(c.F, a.nbox, [&](int b, int i, int j, int k) {
+    const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
+    double* base = a.face + (long)b * kO4FaceArrays * NF;
+    const bool in1 = (d == 0 || (i >= c.F1.lo[0] && i <= c.F1.hi[0])) && (d == 1 || (j >= c.F1.lo[1] && j <= c.F1.hi[1])) &&
+                     (d == 2 || (k >= c.F1.lo[2] && k <= c.F1.hi[2]));
+    if (!in1) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) base[(F_FM + q) * NF + fo] = 0.0;
+      return;
+    }
+    const int blk = a.block0 + b;
+    const double* M = faceRec(a.G, blk, d, j, k);
+    double dM[2][10];
+    const int tr[2] = {t1, t2};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int t = tr[q];
+      int pa[3] = {i, j, k}, pb[3] = {i, j, k};
+      pa[t] += 1; pb[t] -= 1;
+      const double* Ma = faceRec(a.G, blk, d, pa[1], pa[2]);
+      const double* Mb = faceRec(a.G, blk, d, pb[1], pb[2]);
+#pragma unroll
+      for (int e = 0; e < 10; ++e) dM[q][e] = 0.5 * Ma[e] - 0.5 * Mb[e];
+    }
+    const View FA = faceView(c, b, F_FA);
+    double dF[2][8], fa[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      fa[q] = FA(q, i, j, k);
+      dF[0][q] = skipFirst ? 0.0 : cdiff(FA, q, t1, i, j, k);
+      dF[1][q] = cdiff(FA, q, t2, i, j, k);
+    }
+    double out[8];
+#pragma unroll
+    for (int qq = 0; qq < 2; ++qq) {
+      const int q = qq == 0 ? 0 : 4;
+      double term = 0.0;
+      if (!skipFirst) term += dM[0][9] * dF[0][q] * (1.0 / 12.0);
+      term += dM[1][9] * dF[1][q] * (1.0 / 12.0);
+      term += M[9] * fa[q] * 1.0;
+      out[q] = 0.0 + term;
+    }
+#pragma unroll
+    for (int bb = 0; bb < 2; ++bb) {
+      const int bs = bb == 0 ? 1 : 5;
+#pragma unroll
+      for (int row = 0; row < 3; ++row) {
+        double sum = 0.0;
+#pragma unroll
+        for (int col = 0; col < 3; ++col) {
+          double term = 0.0;
+          if (!skipFirst) term += dM[0][3 * row + col] * dF[0][bs + col] * (1.0 / 12.0);
+          term += dM[1][3 * row + col] * dF[1][bs + col] * (1.0 / 12.0);
+          term += M[3 * row + col] * fa[bs + col] * 1.0;
+          sum += term;
+        }
+        out[bs + row] = sum;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) base[(F_FM + q) * NF + fo] = out[q];
+  });
+}
+
+// 7. radial-area face products of the mapped flux and of <p_tot> (F1).
+__global__ void o4FaceRadialKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  const int d = c.d;
+  forRegion(c.F1, a.nbox, [&](int b, int i, int j, int k) {
+    const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
+    double* base = a.face + (long)b * kO4FaceArrays * NF;
+    const double s = adjDr(a.G, d, i);
+    const double ds = 0.5 * adjDr(a.G, d, i + 1) - 0.5 * adjDr(a.G, d, i - 1);
+    const View FM = faceView(c, b, F_FM);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      double value = 0.0;
+      if (d != 0) value += (0.5 * FM(q, i + 1, j, k) - 0.5 * FM(q, i - 1, j, k)) * ds * (1.0 / 12.0);
+      value += FM(q, i, j, k) * s * 1.0;
+      base[(F_FR + q) * NF + fo] = value;
+    }
+    const View PA = faceView(c, b, F_PA);
+    double value = 0.0;
+    if (d != 0) value += (0.5 * PA(0, i + 1, j, k) - 0.5 * PA(0, i - 1, j, k)) * ds * (1.0 / 12.0);
+    value += PA(0, i, j, k) * s * 1.0;
+    base[F_T3 * NF + fo] = value;
+  });
+}
+
+// 8. pressure force, dissipation, combine on the final faces V0; writes the
+// flux (scratch and caller).
+__global__ void o4FaceFinalKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  const int d = c.d;
+  const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+  const int tr[2] = {t1, t2};
+  forRegion(c.V0, a.nbox, [&](int b, int i, int j, int k) {
+    const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
+    double* base = a.face + (long)b * kO4FaceArrays * NF;
+    const int blk = a.block0 + b;
+    const double* M = faceRec(a.G, blk, d, j, k);
+    double fs[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) fs[q] = base[(F_FR + q) * NF + fo];
+    // pressure force: <adjA> x <p_tot adjDr> (bertaFaceTensorProduct)
+    const View T3 = faceView(c, b, F_T3);
+#pragma unroll
+    for (int row = 0; row < 3; ++row) {
+      double value = 0.0;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int t = tr[q];
+        if (d != 0 && t == 0) continue;
+        int pa[3] = {i, j, k}, pb[3] = {i, j, k};
+        pa[t] += 1; pb[t] -= 1;
+        const double dn = 0.5 * faceRec(a.G, blk, d, pa[1], pa[2])[10 + row] - 0.5 * faceRec(a.G, blk, d, pb[1], pb[2])[10 + row];
+        value += dn * cdiff(T3, 0, t, i, j, k) * (1.0 / 12.0);
+      }
+      value += M[10 + row] * T3(0, i, j, k) * 1.0;
+      fs[1 + row] += value;
+    }
+    const bool sm = base[F_THF * NF + fo] > 0.5;
+    const View QD = faceView(c, b, F_QD);
+    double diss[8];
+    if (a.G.roe) {
+      double dM[2][10];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int t = tr[q];
+        int pa[3] = {i, j, k}, pb[3] = {i, j, k};
+        pa[t] += 1; pb[t] -= 1;
+        const double* Ma = faceRec(a.G, blk, d, pa[1], pa[2]);
+        const double* Mb = faceRec(a.G, blk, d, pb[1], pb[2]);
+#pragma unroll
+        for (int e = 0; e < 10; ++e) dM[q][e] = 0.5 * Ma[e] - 0.5 * Mb[e];
+      }
+      double avg[8], dP0[8], dP1[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const double pt = QD(q, i, j, k);
+        avg[q] = sm ? pt + lapFace(QD, q, d, i, j, k) / 24.0 : pt;
+        dP0[q] = cdiff(QD, q, t1, i, j, k);
+        dP1[q] = cdiff(QD, q, t2, i, j, k);
+      }
+      diss[0] = faceProd(M[9], avg[0], dM[0][9], dP0[0], dM[1][9], dP1[0]);
+      diss[4] = faceProd(M[9], avg[4], dM[0][9], dP0[4], dM[1][9], dP1[4]);
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb) {
+        const int bs = bb == 0 ? 1 : 5;
+#pragma unroll
+        for (int row = 0; row < 3; ++row) {
+          double sum = 0.0;
+#pragma unroll
+          for (int col = 0; col < 3; ++col)
+            sum += faceProd(M[3 * row + col], avg[bs + col], dM[0][3 * row + col], dP0[bs + col], dM[1][3 * row + col],
+                            dP1[bs + col]);
+          diss[bs + row] = sum;
+        }
+      }
+    } else {
+      double qv[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const double pt = QD(q, i, j, k);
+        qv[q] = sm ? pt + lapFace(QD, q, d, i, j, k) / 24.0 : pt;
+      }
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb) {
+        const int bs = bb == 0 ? 1 : 5;
+#pragma unroll
+        for (int row = 0; row < 3; ++row)
+          diss[bs + row] = M[3 * row] * qv[bs] * 1.0 + M[3 * row + 1] * qv[bs + 1] * 1.0 + M[3 * row + 2] * qv[bs + 2] * 1.0;
+      }
+      diss[0] = M[9] * qv[0];
+      diss[4] = M[9] * qv[4];
+      // face wave-speed bound (:1665-1720)
+      double l[8], r[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) { l[q] = base[(F_WL + q) * NF + fo]; r[q] = base[(F_WR + q) * NF + fo]; }
+      const double* A = faceBasis(c, b, j, k);
+      double rho = 0.5 * (l[0] + r[0]);
+      const double w_d = 0.5 * (l[1 + d] + r[1 + d]);
+      const double bs3[3] = {0.5 * (l[5] + r[5]), 0.5 * (l[6] + r[6]), 0.5 * (l[7] + r[7])};
+      double p = 0.5 * (l[4] + r[4]);
+      if (p < 0.0) p = 0.0;
+      rho = dmax(rho, kRHO00);
+      double Bn = 0.0, Bm = 0.0;
+#pragma unroll
+      for (int e0 = 0; e0 < 3; ++e0) {
+        const double bC = A[3 * e0] * bs3[0] + A[3 * e0 + 1] * bs3[1] + A[3 * e0 + 2] * bs3[2];
+        Bn += A[3 * e0] * bC;
+        Bm += bC * bC;
+      }
+      Bm = sqrt(Bm);
+      const double g = a.G.gamma;
+      const double ce = sqrt(g * p / rho);
+      const double aa = ce * ce + Bm * Bm / (4.0 * kPi * rho);
+      const double bb2 = fabs(Bn) * ce / sqrt(kPi * rho);
+      const double af = 0.5 * (sqrt(dmax(0.0, aa + bb2)) + sqrt(dmax(0.0, aa - bb2)));
+      const double Am = sqrt(A[d] * A[d] + A[3 + d] * A[3 + d] + A[6 + d] * A[6 + d]);
+      const double speed = fabs(w_d) + af * Am;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) diss[q] *= speed;
+    }
+    double fx[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      fx[q] = 0.5 * (fs[q] - diss[q]);
+      base[(F_FX + q) * NF + fo] = fx[q];
+    }
+    if (a.flux[d]) {
+      Box3 V0 = c.V0;
+      const Reg r0 = regOf(V0);
+      double* fo2 = a.flux[d] + (long)b * 8 * r0.N + roff(r0, i, j, k);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) fo2[q * r0.N] = fx[q];
+    }
+  });
+}
+
+// 9. flux divergence into rhs (V).
+__global__ void o4DivKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  const int d = c.d;
+  const double coef = -a.scale / a.G.dx[d];
+  forRegion(c.V, a.nbox, [&](int b, int i, int j, int k) {
+    const View FX = faceView(c, b, F_FX);
+    int p[3] = {i, j, k};
+    p[d] += 1;
+    double* R = a.rhs + b * a.rhsStride + roff(c.vr, i, j, k);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) R[q * c.vr.N] += coef * (FX(q, p[0], p[1], p[2]) - FX(q, i, j, k));
+  });
+}
+
+// 10. Powell face flux (DivBPowell1, src/BoxOp_DivBcleaning.H:35-74).
+__global__ void o4PowellFluxKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  const int d = c.d;
+  const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+  const int tr[2] = {t1, t2};
+  const Box3 BF = c.V1.extrude(d).growTrans(d, 1);
+  forRegion(BF, a.nbox, [&](int b, int i, int j, int k) {
+    const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
+    double* base = a.face + (long)b * kO4FaceArrays * NF;
+    const int blk = a.block0 + b;
+    const double det = faceRec(a.G, blk, d, j, k)[9];
+    double out;
+    if (base[F_THF * NF + fo] <= 0.5) {
+      out = det * base[F_BP * NF + fo];
+    } else {
+      View U{a.U + b * a.uStride, a.ur};
+      auto bface = [&](int ii, int jj, int kk) {
+        int m2[3] = {ii, jj, kk}, m1[3] = {ii, jj, kk}, p1[3] = {ii, jj, kk};
+        m2[d] -= 2; m1[d] -= 1; p1[d] += 1;
+        return (7.0 / 12.0) * (U(5 + d, m1[0], m1[1], m1[2]) + U(5 + d, ii, jj, kk)) -
+               (1.0 / 12.0) * (U(5 + d, m2[0], m2[1], m2[2]) + U(5 + d, p1[0], p1[1], p1[2]));
+      };
+      double df[2], dg[2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int t = tr[q];
+        int pa[3] = {i, j, k}, pb[3] = {i, j, k};
+        pa[t] += 1; pb[t] -= 1;
+        df[q] = 0.5 * faceRec(a.G, blk, d, pa[1], pa[2])[9] - 0.5 * faceRec(a.G, blk, d, pb[1], pb[2])[9];
+        dg[q] = 0.5 * bface(pa[0], pa[1], pa[2]) - 0.5 * bface(pb[0], pb[1], pb[2]);
+      }
+      out = faceProd(det, bface(i, j, k), df[0], dg[0], df[1], dg[1]);
+    }
+    base[F_BFLUX * NF + fo] = out;
+  });
+}
+
+// 11. Powell radial-area product and divergence into -J div B (V+1).
+__global__ void o4PowellProdKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  const int d = c.d;
+  const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+  const int tr[2] = {t1, t2};
+  const Box3 BP = c.V1.extrude(d);
+  forRegion(BP, a.nbox, [&](int b, int i, int j, int k) {
+    const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
+    double* base = a.face + (long)b * kO4FaceArrays * NF;
+    const View BF = faceView(c, b, F_BFLUX);
+    double df[2], dg[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int t = tr[q];
+      df[q] = cdiff(BF, 0, t, i, j, k);
+      dg[q] = t == 0 ? 0.5 * adjDr(a.G, d, i + 1) - 0.5 * adjDr(a.G, d, i - 1) : 0.0;
+    }
+    base[F_BPROD * NF + fo] = faceProd(BF(0, i, j, k), adjDr(a.G, d, i), df[0], dg[0], df[1], dg[1]);
+  });
+}
+
+__global__ void o4PowellDivKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  const int d = c.d;
+  const double coef = -1.0 / a.G.dx[d];
+  forRegion(c.V1, a.nbox, [&](int b, int i, int j, int k) {
+    const View BP = faceView(c, b, F_BPROD);
+    int p[3] = {i, j, k};
+    p[d] += 1;
+    a.mj[(long)b * c.v1r.N + roff(c.v1r, i, j, k)] += coef * (BP(0, p[0], p[1], p[2]) - BP(0, i, j, k));
+  });
+}
+
+// 12. DivBPowell2 with point primitives (src/BoxOp_DivBcleaning.H:80-172).
+__global__ void o4PowellCoefKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  forRegion(c.V2, a.nbox, [&](int b, int i, int j, int k) {
+    const long NG = c.gr.N, o = roff(c.gr, i, j, k);
+    const double* WP = a.WP + (long)b * 8 * NG;
+    const double* A = cellBasis(a.G, a.block0 + b, j, k);
+    double vel[3], mag[3];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      vel[e] = A[3 * e] * WP[1 * NG + o] + A[3 * e + 1] * WP[2 * NG + o] + A[3 * e + 2] * WP[3 * NG + o];
+      mag[e] = A[3 * e] * WP[5 * NG + o] + A[3 * e + 1] * WP[6 * NG + o] + A[3 * e + 2] * WP[7 * NG + o];
+    }
+    double* K = a.kp + (long)b * 16 * c.v2r.N + roff(c.v2r, i, j, k);
+    const long N = c.v2r.N;
+    K[0] = 0;
+    double e4 = 0;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      K[(1 + e) * N] = mag[e] / (4.0 * kPi);
+      K[(5 + e) * N] = vel[e];
+      e4 += vel[e] * mag[e] / (4.0 * kPi);
+    }
+    K[4 * N] = e4;
+  });
+}
+
+__global__ void o4PowellAvgKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  forRegion(c.V1, a.nbox, [&](int b, int i, int j, int k) {
+    const View KP{a.kp + (long)b * 16 * c.v2r.N, c.v2r};
+    double* KA = a.kp + (long)b * 16 * c.v2r.N + 8 * c.v2r.N + roff(c.v2r, i, j, k);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) KA[q * c.v2r.N] = KP(q, i, j, k) + lapCell(KP, q, i, j, k) / 24.0;
+  });
+}
+
+__global__ void o4PowellApplyKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  forRegion(c.V, a.nbox, [&](int b, int i, int j, int k) {
+    const View KA{a.kp + (long)b * 16 * c.v2r.N + 8 * c.v2r.N, c.v2r};
+    const View MJ{a.mj + (long)b * c.v1r.N, c.v1r};
+    double* R = a.rhs + b * a.rhsStride + roff(c.vr, i, j, k);
+    for (int q = 1; q < 8; ++q) {
+      double value = 0.0;
+#pragma unroll
+      for (int t = 0; t < 3; ++t) value += cdiff(MJ, 0, t, i, j, k) * cdiff(KA, q, t, i, j, k) * (1.0 / 12.0);
+      value += MJ(0, i, j, k) * KA(q, i, j, k) * 1.0;
+      R[q * c.vr.N] += value;
+    }
+  });
+}
+
+int blocksFor(long n) {
+  long g = (n + 127) / 128;
+  if (g > 148L * 32) g = 148L * 32;
+  return (int)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost) {
+  Box3 V;
+  for (int q = 0; q < 3; ++q) { V.lo[q] = vlo[q]; V.hi[q] = vhi[q]; }
+  const Box3 G = V.grow(ghost);
+  Box3 FB = G.grow(-3);
+  for (int q = 0; q < 3; ++q) FB.hi[q] += 1;
+  const size_t NG = (size_t)G.size(), NF = (size_t)FB.size(), N1 = (size_t)V.grow(1).size(), N2 = (size_t)V.grow(2).size();
+  return (size_t)nbox * (8 * NG + 8 * NG + NG + NG + (size_t)kO4FaceArrays * NF + N1 + 16 * N2);
+}
+
+cudaError_t launchO4BoxOperator(const O4Args& a, cudaStream_t s) {
+  // scratch carve-up (see o4ScratchDoubles)
+  Ctx c0 = makeCtx(a, 0);
+  const long nb = a.nbox;
+  const int T = 128;
+  cudaError_t e;
+#define HC_LAUNCH(kernel, ctx, region)                                                  \
+  kernel<<<blocksFor((region).size() * nb), T, 0, s>>>(ctx);                           \
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  HC_LAUNCH(o4PrimAvgKernel, c0, c0.G)
+  HC_LAUNCH(o4ThetaRawKernel, c0, c0.GR)
+  HC_LAUNCH(o4PointKernel, c0, c0.G)
+  if (a.G.powell) {
+    if ((e = cudaMemsetAsync(a.mj, 0, sizeof(double) * nb * c0.v1r.N, s)) != cudaSuccess) return e;
+  }
+  for (int d = 0; d < 3; ++d) {
+    Ctx c = makeCtx(a, d);
+    HC_LAUNCH(o4FaceReconKernel, c, c.F)
+    if (a.G.roe) { HC_LAUNCH(o4RoePointKernel, c, c.V0.growTrans(d, 1)) }
+    HC_LAUNCH(o4FaceAvgKernel, c, c.F1)
+    HC_LAUNCH(o4FaceMapKernel, c, c.F)
+    HC_LAUNCH(o4FaceRadialKernel, c, c.F1)
+    HC_LAUNCH(o4FaceFinalKernel, c, c.V0)
+    HC_LAUNCH(o4DivKernel, c, c.V)
+    if (a.G.powell) {
+      HC_LAUNCH(o4PowellFluxKernel, c, c.V1.extrude(d).growTrans(d, 1))
+      HC_LAUNCH(o4PowellProdKernel, c, c.V1.extrude(d))
+      HC_LAUNCH(o4PowellDivKernel, c, c.V1)
+    }
+  }
+  if (a.G.powell) {
+    HC_LAUNCH(o4PowellCoefKernel, c0, c0.V2)
+    HC_LAUNCH(o4PowellAvgKernel, c0, c0.V1)
+    HC_LAUNCH(o4PowellApplyKernel, c0, c0.V)
+  }
+#undef HC_LAUNCH
+  return cudaSuccess;
+}
+
+}  // namespace hc

@@ -51,12 +51,17 @@ class Params:
     outer_radius: float = 215.0 * C_SR
     radial_stretch: float = 1.5
     strength: float = 0.0
+    spatial_operator: int = 2      # order 4: Berta WENOZ
+    berta_detector_type: int = 0   # Jameson
+    berta_fallback_type: int = 0   # 0 WENO3, 1 PLM
+    berta_eta_d: float = 0.02
 
     def to_c(self) -> N.HcParams:
         p = N.HcParams()
         for k in ("nr", "na", "spatial_order", "limiter", "riemann_solver", "divergence_cleaning",
                   "sun_gravity", "init_condition_type", "temporal_order", "gamma", "entropy_fix_coeff",
-                  "cfl", "inner_radius", "outer_radius", "radial_stretch", "strength"):
+                  "cfl", "inner_radius", "outer_radius", "radial_stretch", "strength", "spatial_operator",
+                  "berta_detector_type", "berta_fallback_type", "berta_eta_d"):
             setattr(p, k, getattr(self, k))
         return p
 
@@ -214,6 +219,14 @@ class Shell:
         pn = (C.c_void_p * 6)(*[(f.data_ptr() if f is not None else None) for f in panel]) if panel else None
         N.check(self._lib.hc_box_rhs(self._ctx, C.byref(box), _ptr(w), pn, scale, _ptr(rhs), fl, _stream()),
                 "hc_box_rhs")
+
+    def box_rhs_o4(self, box: N.HcBox, usph: torch.Tensor, rhs: torch.Tensor, fluxes=None,
+                   scale: float = 1.0) -> None:
+        """Fourth-order Berta operator on one box (BertaOperator):
+        usph are native conserved averages on valid.grow(ghost >= 5)."""
+        fl = (C.c_void_p * 3)(*[(f.data_ptr() if f is not None else None) for f in fluxes]) if fluxes else None
+        N.check(self._lib.hc_box_rhs_o4(self._ctx, C.byref(box), _ptr(usph), scale, _ptr(rhs), fl, _stream()),
+                "hc_box_rhs_o4")
 
     def box_gravity(self, box: N.HcBox, w: torch.Tensor, rhs: torch.Tensor) -> None:
         N.check(self._lib.hc_box_gravity(self._ctx, C.byref(box), _ptr(w), _ptr(rhs), _stream()), "hc_box_gravity")

@@ -41,7 +41,7 @@ enum {
 
 /* Option semantics mirror src/Inputs_Parsing.H:43-178 (ParseInputs). */
 typedef struct hc_params {
-  int spatial_order;        /* 2: PLM operator (src/BoxOp_SecondOrder.H) */
+  int spatial_order;        /* 2: PLM operator (src/BoxOp_SecondOrder.H); 4: Berta WENOZ */
   int limiter;              /* 0 unlimited, 1|2 minmod, 3 MC (Inputs_Parsing.H:71) */
   int riemann_solver;       /* 1 Rusanov, 2 Roe 8-wave (Inputs_Parsing.H:79) */
   int divergence_cleaning;  /* 1: Powell source (Inputs_Parsing.H:118) */
@@ -49,7 +49,10 @@ typedef struct hc_params {
   int init_condition_type;  /* radial BC family; 1 = analytic wind (BoxOp_PreStage.H:7-47) */
   int temporal_order;       /* 4: classical RK4 (MHD_AMRRungeKutta.H:10-12) */
   int nr, na;               /* level cells per panel: radial, angular */
-  int reserved_i[7];
+  int spatial_operator;     /* at order 4: 2 = Berta WENOZ (Inputs_Parsing.H:78) */
+  int berta_detector_type;  /* 0 Jameson (Inputs_Parsing.H:82-84) */
+  int berta_fallback_type;  /* 0 WENO3, 1 PLM (theta = 1.5 minmod3) */
+  int reserved_i[4];
   double gamma;             /* ratio of specific heats */
   double entropy_fix_coeff; /* Roe entropy fix, default 0.3 */
   double cfl;               /* dt = cfl / max(inverse dt) */
@@ -57,7 +60,8 @@ typedef struct hc_params {
   double outer_radius;      /* cm */
   double radial_stretch;    /* C in r = r0 + R_t expm1(C eta) (BoxOp_Utilities.H:36-46) */
   double strength;          /* analytic-wind perturbation strength (percent) */
-  double reserved_d[7];
+  double berta_eta_d;       /* Jameson threshold, default 0.02 */
+  double reserved_d[6];
 } hc_params;
 
 /* One box of a panel in panel index space (inclusive bounds), the ghost
@@ -112,6 +116,19 @@ size_t hc_level_primitive_size(const hc_ctx* ctx);
 int hc_box_rhs(hc_ctx* ctx, const hc_box* box, const double* w,
                const double* const* panel_states, double scale,
                double* rhs, double* const* flux, void* stream);
+
+/* Per-box fourth-order Berta pointwise-WENOZ operator (context created with
+ * spatial_order 4, spatial_operator 2).  Replaces
+ * BoxOp_EulerCubedSphere::operator() -> BertaOperator
+ * (src/BoxOp_BertaCubedSphereImplem.H:1737-2076):
+ *   rhs[valid]    += -scale * sum_d (F_d(i+1)-F_d(i))/dxi_d + Powell source
+ *   flux[d][faces] = F_d on valid.extrude(d) (overwritten; may be NULL)
+ * usph: native-basis conserved cell averages on valid.grow(ghost), ghost >= 5
+ * (NGHOST, src/BoxOp_EulerCubedSphere.H:386-389).  Uses context scratch that
+ * grows on first use of a larger box (a cudaMalloc: not inside a capture). */
+int hc_box_rhs_o4(hc_ctx* ctx, const hc_box* box, const double* usph,
+                  double scale, double* rhs, double* const* flux,
+                  void* stream);
 
 /* Solar gravity on second-order primitives, rhs[valid] += source.
  * Replaces gravitySecondOrderPrimitives (src/BoxOp_Gravity.H:3-82). */

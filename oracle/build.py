@@ -39,8 +39,9 @@ def _stale(out: str, srcs: list[str]) -> bool:
 def build_oracle(force: bool = False) -> str:
     src = os.path.join(HERE, "hc_oracle.cpp")
     hdr = os.path.join(REPO, "include", "hc_abi.h")
+    inc = os.path.join(HERE, "hc_oracle_o4.inc")
     out = os.path.join(HERE, "libhc_oracle.so")
-    if force or _stale(out, [src, hdr, __file__]):
+    if force or _stale(out, [src, hdr, inc, __file__]):
         _run(["g++", *CXXFLAGS, "-fopenmp", src, "-o", out])
     return out
 

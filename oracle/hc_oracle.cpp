@@ -20,7 +20,9 @@
 // with -ffp-contract=off so the arithmetic order below is the one executed.
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <limits>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -1146,6 +1148,8 @@ void levelInit(const Level& L, const hc_init& in, double* ju) {
       }
 }
 
+#include "hc_oracle_o4.inc"
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1159,6 +1163,10 @@ void orc_level_destroy(void* L) { delete static_cast<Level*>(L); }
 int orc_box_rhs(void* L, const hc_box* box, const double* w, const double* const* panel,
                 double scale, double* rhs, double* const* flux) {
   boxOperator(*static_cast<Level*>(L), box->lo, box->hi, box->ghost, box->block, w, panel, scale, rhs, flux);
+  return 0;
+}
+int orc_box_rhs_o4(void* L, const hc_box* box, const double* usph, double scale, double* rhs, double* const* flux) {
+  o4BoxOperator(*static_cast<Level*>(L), box->lo, box->hi, box->ghost, box->block, usph, scale, rhs, flux);
   return 0;
 }
 int orc_box_gravity(void* L, const hc_box* box, const double* w, double* rhs) {

@@ -20,10 +20,12 @@ class HcParams(C.Structure):
         ("spatial_order", C.c_int), ("limiter", C.c_int), ("riemann_solver", C.c_int),
         ("divergence_cleaning", C.c_int), ("sun_gravity", C.c_int),
         ("init_condition_type", C.c_int), ("temporal_order", C.c_int),
-        ("nr", C.c_int), ("na", C.c_int), ("reserved_i", C.c_int * 7),
+        ("nr", C.c_int), ("na", C.c_int), ("spatial_operator", C.c_int), ("berta_detector_type", C.c_int),
+        ("berta_fallback_type", C.c_int), ("reserved_i", C.c_int * 4),
         ("gamma", C.c_double), ("entropy_fix_coeff", C.c_double), ("cfl", C.c_double),
         ("inner_radius", C.c_double), ("outer_radius", C.c_double),
-        ("radial_stretch", C.c_double), ("strength", C.c_double), ("reserved_d", C.c_double * 7),
+        ("radial_stretch", C.c_double), ("strength", C.c_double), ("berta_eta_d", C.c_double),
+        ("reserved_d", C.c_double * 6),
     ]
 
 
@@ -65,6 +67,7 @@ def lib() -> C.CDLL:
         L.orc_level_destroy.argtypes = [C.c_void_p]
         L.orc_box_rhs.argtypes = [C.c_void_p, C.POINTER(HcBox), _D, C.POINTER(_D), C.c_double, _D, C.POINTER(_D)]
         L.orc_box_gravity.argtypes = [C.c_void_p, C.POINTER(HcBox), _D, _D]
+        L.orc_box_rhs_o4.argtypes = [C.c_void_p, C.POINTER(HcBox), _D, C.c_double, _D, C.POINTER(_D)]
         L.orc_level_prepare.argtypes = [C.c_void_p, _D, _D, C.c_double]
         L.orc_level_rhs.argtypes = [C.c_void_p, _D, _D]
         L.orc_level_rk4_step.argtypes = [C.c_void_p, _D, C.c_double, C.c_double]
@@ -123,6 +126,10 @@ def make_params(**kw) -> HcParams:
     p.outer_radius = 215.0 * 6.96e10
     p.radial_stretch = 1.5
     p.strength = 0.0
+    p.spatial_operator = 2
+    p.berta_detector_type = 0
+    p.berta_fallback_type = 0
+    p.berta_eta_d = 0.02
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -179,6 +186,10 @@ class OracleLevel:
         fl = (_D * 3)(*[dptr(f) if f is not None else None for f in fluxes]) if fluxes is not None else None
         pn = (_D * 6)(*[dptr(f) if f is not None else None for f in panel]) if panel is not None else None
         self.L.orc_box_rhs(self.h, C.byref(box), dptr(w), pn, scale, dptr(rhs), fl)
+
+    def box_rhs_o4(self, box: HcBox, usph: np.ndarray, rhs: np.ndarray, fluxes=None, scale=1.0):
+        fl = (_D * 3)(*[dptr(f) if f is not None else None for f in fluxes]) if fluxes is not None else None
+        self.L.orc_box_rhs_o4(self.h, C.byref(box), dptr(usph), scale, dptr(rhs), fl)
 
     def box_gravity(self, box: HcBox, w: np.ndarray, rhs: np.ndarray):
         self.L.orc_box_gravity(self.h, C.byref(box), dptr(w), dptr(rhs))

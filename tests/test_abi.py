@@ -45,15 +45,18 @@ def test_struct_layouts_match_header(product_lib_path):
     assert C.sizeof(_native.HcInit) == 8 * 4 + 11 * 8
 
 
-@pytest.mark.parametrize("field,value,code", [
-    ("spatial_order", 4, -3), ("limiter", 7, -1), ("riemann_solver", 3, -1),
-    ("temporal_order", 2, -3), ("nr", 2, -1), ("gamma", 1.0, -1), ("init_condition_type", 0, -3),
+@pytest.mark.parametrize("fields,code", [
+    ({"spatial_order": 3}, -3), ({"limiter": 7}, -1), ({"riemann_solver": 3}, -1),
+    ({"temporal_order": 2}, -3), ({"nr": 2}, -1), ({"gamma": 1.0}, -1), ({"init_condition_type": 0}, -3),
+    ({"spatial_order": 4, "spatial_operator": 1}, -3), ({"spatial_order": 4, "berta_detector_type": 1}, -3),
+    ({"spatial_order": 4, "berta_fallback_type": 2}, -1), ({"spatial_order": 4}, -1),  # na = 8 < 16
 ])
-def test_bad_options_rejected(product_lib_path, field, value, code):
+def test_bad_options_rejected(product_lib_path, fields, code):
     from heliocubed_b200 import _native
     from heliocubed_b200.level import Params
     p = Params(nr=8, na=8).to_c()
-    setattr(p, field, value)
+    for field, value in fields.items():
+        setattr(p, field, value)
     ctx = C.c_void_p()
     rc = _native.lib().hc_ctx_create(C.byref(p), 0, C.byref(ctx))
     assert rc == code

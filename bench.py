@@ -1,17 +1,21 @@
 """Benchmark: FP64 cell-updates/s of the cubed-sphere MHD RK4 step on B200.
 
 One step = one classical RK4 step of the whole six-panel shell (4 operator
-evaluations: stage preparation with seam/radial ghosts, fused flux
-divergence + Powell + gravity + RK update), with dt = cfl / max CFL rate
-computed on the device before every step.  One cell-update = one valid cell
-advanced one full RK4 step.
+evaluations with their stage preparation and RK update), with dt = cfl /
+max CFL rate computed on the device before every step.  One cell-update =
+one valid cell advanced one full RK4 step.
 
-Workload (default): second-order PLM-MC + Rusanov, Powell on, 32 radial x
-32 x 32 angular cells per panel (196,608 cells), gamma 5/3, r in [21.5, 215]
-Rsun, radial stretch 1.5, CFL 0.4, seeded Parker-like wind + Gaussian
-pressure pulse (synthetic input; the reference ships no data for it).
+Workloads (synthetic input; the reference ships no data for them), gamma
+5/3, r in [21.5, 215] Rsun, radial stretch 1.5, CFL 0.4, Powell on:
+  --order 4 (default): fourth-order Berta pointwise WENOZ (Jameson detector,
+      WENO3 fallback) + Roe 8-wave, 64 radial x 64 x 64 angular cells per
+      panel (1,572,864 cells); Parker-like wind with seeded 5 % tangential
+      perturbations of v and of B (B_t the surface curl of a seeded stream
+      function).
+  --order 2: second-order PLM-MC + Rusanov, 32 x 32^2 x 6 (196,608 cells);
+      Parker-like wind + seeded Gaussian pressure pulse.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--order 2|4]
 
 N > 1 (torchrun): every rank runs an independent replica of the workload
 (weak scaling; the path has no exchange between replicas), timed on the
@@ -31,6 +35,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -38,22 +44,40 @@ METRIC = "FP64 cell-updates/s on 1 B200 (RK4 step of the cubed-sphere MHD update
 UNIT = "cell-updates/s"
 L2_BYTES = 126 * 1024 * 1024
 OPERATOR_BYTES_PER_CELL_STAGE = 128  # read 8 FP64 primitives, write 8 FP64 rhs
-LAUNCHES_PER_STEP = 11               # prim + cfl + 4 x (ghosts, stage) + time (prologue in every 1-step call)
 
 
-def workload_params(args):
+def launches_per_step(args) -> int:
+    """Kernels of this library launched by one hc_level_advance_cfl step."""
+    if args.order == 2:
+        return 11  # prim + cfl + 4 x (ghosts, stage) + time (prologue in every 1-step call)
+    roe, powell = int(args.riemann == 2), 1
+    per_stage = 3 + 3 + 3 * (6 + roe + 3 * powell) + 3 * powell + 1  # prepare, operator, update
+    return 1 + 4 * per_stage + 2 + 1                                  # cfl, stages, reflux, time
+
+
+def workload_params(args, nr=None, na=None):
     from heliocubed_b200.level import Params
-    return Params(nr=args.nr, na=args.na, limiter=args.limiter, riemann_solver=args.riemann,
-                  divergence_cleaning=1, sun_gravity=args.gravity, cfl=0.4)
+    return Params(nr=nr or args.nr, na=na or args.na, spatial_order=args.order, limiter=args.limiter,
+                  riemann_solver=args.riemann, divergence_cleaning=1, sun_gravity=args.gravity, cfl=0.4,
+                  berta_fallback_type=0)
+
+
+def scheme_name(args) -> str:
+    solver = "Roe 8-wave" if args.riemann == 2 else "Rusanov"
+    if args.order == 4:
+        return f"Berta pointwise WENOZ (WENO3 fallback) + {solver}"
+    return f"PLM-{'MC' if args.limiter == 3 else args.limiter} + {solver}"
 
 
 def workload_config(args, flush: bool):
     return {
-        "workload": f"cubed-sphere MHD RK4 step, PLM-{'MC' if args.limiter == 3 else args.limiter} + "
-                    f"{'Roe' if args.riemann == 2 else 'Rusanov'}, {args.nr}x{args.na}^2x6",
+        "workload": f"cubed-sphere MHD RK4 step, {scheme_name(args)}, {args.nr}x{args.na}^2x6",
         "cells": 6 * args.nr * args.na * args.na,
-        "scheme": {"spatial_order": 2, "limiter": args.limiter, "riemann_solver": args.riemann,
-                   "powell": 1, "gravity": args.gravity, "temporal_order": 4, "cfl": 0.4},
+        "scheme": {"spatial_order": args.order, "limiter": args.limiter if args.order == 2 else None,
+                   "riemann_solver": args.riemann, "powell": 1, "gravity": args.gravity, "temporal_order": 4,
+                   "cfl": 0.4},
+        "init": ("Parker-like wind + seeded 5% tangential v and B (stream-function curl)" if args.order == 4
+                 else "Parker-like wind + seeded Gaussian pressure pulse"),
         "l2": "flushed between timed steps (256 MiB write)" if flush else "working set larger than L2",
         "dt": "device CFL reduction every step",
         "launch": "CUDA graph replay per step" if args.graph else "eager launches",
@@ -68,10 +92,10 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic_per_cell_stage():
-    """DRAM bytes per cell-stage of the operator kernel from the committed ncu
-    summary (profiles/o2_stage_kernel.md), or None before one exists."""
-    path = os.path.join(ROOT, "profiles", "o2_stage_kernel.md")
+def profiled_traffic_per_cell_stage(order: int):
+    """DRAM bytes per cell-stage of the operator from the committed ncu
+    summary of that operator, or None before one exists."""
+    path = os.path.join(ROOT, "profiles", "o2_stage_kernel.md" if order == 2 else "o4_operator.md")
     if not os.path.exists(path):
         return None
     m = re.search(r"traffic_bytes_per_cell_stage:\s*([0-9.eE+-]+)", open(path).read())
@@ -164,20 +188,30 @@ def barrier(world: int):
 
 def cpu_baseline(args, budget_s: float = 12.0) -> dict:
     """The oracle (CPU restatement of the reference) on the host cores, on a
-    bounded number of RK4 steps of the same workload."""
+    bounded number of RK4 steps of the same scheme: the full grid at order 2,
+    a 32 x 32^2 x 6 grid at order 4 (one step of the 64^3 grid takes minutes
+    on the host)."""
     from oracle import pyoracle as po
     cores = os.cpu_count() or 1
-    p = po.make_params(nr=args.nr, na=args.na, limiter=args.limiter, riemann_solver=args.riemann,
-                       sun_gravity=args.gravity)
-    L = po.OracleLevel(p)
-    from heliocubed_b200.level import InitSpec
-    spec = InitSpec.seeded(args.seed, args.nr, args.na)
-    s = po.HcInit()
-    s.kind = 1
-    for k in ("pulse_block", "pulse_i", "pulse_j", "pulse_k", "rho0", "p0", "vr", "b0", "r_ref", "pulse_amp",
-              "pulse_width"):
-        setattr(s, k, getattr(spec, k))
-    ju = L.init(s)
+    nr, na = (args.nr, args.na) if args.order == 2 else (min(args.nr, 32), min(args.na, 32))
+    p = po.make_params(nr=nr, na=na, spatial_order=args.order, limiter=args.limiter, riemann_solver=args.riemann,
+                       sun_gravity=args.gravity, berta_fallback_type=0)
+    if args.order == 4:
+        from heliocubed_b200.level import perturbed_wind_state
+        L = po.OracleLevelO4(p)
+        det = L.base.geometry(4).reshape(6, na, na)
+        dvolr = L.base.geometry(0).reshape(nr + 1, 4)[:nr, 3]
+        ju = np.ascontiguousarray(perturbed_wind_state(workload_params(args, nr, na), det, dvolr, args.seed).reshape(-1))
+    else:
+        L = po.OracleLevel(p)
+        from heliocubed_b200.level import InitSpec
+        spec = InitSpec.seeded(args.seed, nr, na)
+        s = po.HcInit()
+        s.kind = 1
+        for k in ("pulse_block", "pulse_i", "pulse_j", "pulse_k", "rho0", "p0", "vr", "b0", "r_ref", "pulse_amp",
+                  "pulse_width"):
+            setattr(s, k, getattr(spec, k))
+        ju = L.init(s)
     steps, t = 0, 0.0
     t0 = time.perf_counter()
     while True:
@@ -188,9 +222,10 @@ def cpu_baseline(args, budget_s: float = 12.0) -> dict:
         if time.perf_counter() - t0 > budget_s or steps >= args.cpu_max_steps:
             break
     el = time.perf_counter() - t0
-    value = 6 * args.nr * args.na * args.na * steps / el
+    value = 6 * nr * na * na * steps / el
+    same = "the same" if (nr, na) == (args.nr, args.na) else f"the same scheme on a"
     return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{steps} RK4 steps (CFL dt each step) of the same {args.nr}x{args.na}^2x6 workload, "
+            "sample": f"{steps} RK4 steps (CFL dt each step) of {same} {nr}x{na}^2x6 grid, "
                       f"OpenMP over {cores} host threads, {el:.1f} s"}
 
 
@@ -213,8 +248,10 @@ def run_b200(args, world, rank, local):
     params = workload_params(args)
     shell = Shell(params, device=local)
     cells = shell.cells
-    spec = InitSpec.seeded(args.seed, args.nr, args.na)
-    ju0 = shell.init(spec)
+    if args.order == 4:
+        ju0 = shell.init_perturbed_wind(args.seed)
+    else:
+        ju0 = shell.init(InitSpec.seeded(args.seed, args.nr, args.na))
     ju = ju0.clone()
     time_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
@@ -272,7 +309,7 @@ def run_b200(args, world, rank, local):
     kms = statistics.mean(a.elapsed_time(b) for a, b in kev)
     peak, peak_kind = peaks()
     achieved = OPERATOR_BYTES_PER_CELL_STAGE * cells / (kms * 1e-3) / 1e9
-    tr = profiled_traffic_per_cell_stage()
+    tr = profiled_traffic_per_cell_stage(args.order)
 
     # end to end through the public API with host buffers
     host_in = ju0.cpu().pin_memory()
@@ -304,13 +341,15 @@ def run_b200(args, world, rank, local):
             "config": dict(workload_config(args, flush), parallelism=f"replicas x{world}"),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "kernel": "o2StageKernel (operator: read primitives, write rhs)",
+                         "kernel": ("o2StageKernel (operator: read primitives, write rhs)" if args.order == 2 else
+                                    "Berta operator launch group (hc_level_rhs, %d kernels): read USph, write rhs"
+                                    % (3 + 3 * (6 + int(args.riemann == 2) + 3) + 3)),
                          "algorithmic_bytes": f"{OPERATOR_BYTES_PER_CELL_STAGE} B/cell-stage x {cells} cells",
                          "kernel_ms": kms,
                          "traffic": None if tr is None else tr * cells},
             "e2e": {"value": cells * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes},
-            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+            "gpu_launches": launches_per_step(args) * args.steps,
             "clocks": clocks,
             "valid_state": ok,
         }
@@ -323,13 +362,14 @@ def run_b200(args, world, rank, local):
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--nr", type=int, default=32)
-    ap.add_argument("--na", type=int, default=32)
+    ap.add_argument("--order", type=int, choices=[2, 4], default=4)
+    ap.add_argument("--nr", type=int, default=None)
+    ap.add_argument("--na", type=int, default=None)
     ap.add_argument("--limiter", type=int, default=3)
-    ap.add_argument("--riemann", type=int, default=1)
+    ap.add_argument("--riemann", type=int, default=None)
     ap.add_argument("--gravity", type=int, default=0)
     ap.add_argument("--seed", type=int, default=20261204)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -338,6 +378,11 @@ def main() -> int:
     ap.add_argument("--cpu-max-steps", type=int, default=60)
     ap.add_argument("--ref-budget", type=float, default=20.0)
     args = ap.parse_args()
+    o4 = args.order == 4
+    args.nr = args.nr or (64 if o4 else 32)
+    args.na = args.na or (64 if o4 else 32)
+    args.riemann = args.riemann or (2 if o4 else 1)
+    args.steps = args.steps or (100 if o4 else 2000)
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:

@@ -248,6 +248,14 @@ struct hc_ctx {
   O4Geo o4{};
   double* o4scratch = nullptr;
   size_t o4scratchDoubles = 0;
+  // fourth-order level step: tables and level-sized buffers (order 4 only)
+  O4Level o4l{};
+  double* o4us = nullptr;      // native averages on the ghosted panels [6][8][Ng]
+  double* o4cart = nullptr;    // Cartesian averages with seam ghosts [6][8][Nc]
+  double* o4next = nullptr;    // next stage state [6][8][Nv]
+  double* o4k = nullptr;       // stage right-hand side [6][8][Nv]
+  double* o4reg = nullptr;     // seam flux register [6][2][2][8][na][nr]
+  double* o4lvlScratch = nullptr;
 };
 
 namespace {
@@ -556,6 +564,171 @@ int buildO4Geometry(hc_ctx* c) {
   return HC_OK;
 }
 
+// Panel holding direction X; directions within 1e-12 of a panel edge go to
+// the lowest panel index, so seam-interpolation stencils do not depend on
+// round-off.
+int locateTie(const double X[3]) {
+  double q0[6], best = -2;
+  for (int b = 0; b < 6; ++b) {
+    q0[b] = 0;
+    for (int k = 0; k < 3; ++k)
+      if (PERM[b][k] == 0) q0[b] = SIGN[b][k] * X[k];
+    best = std::max(best, q0[b]);
+  }
+  for (int b = 0; b < 6; ++b)
+    if (q0[b] >= best - 1e-12 * std::fabs(best)) return b;
+  return 0;
+}
+
+// Point value at u (cell m spans [m, m+1]) of the cubic whose averages over
+// cells base..base+3 are given: the derivative of the quartic through the
+// running sums at faces base..base+4.
+void averageInterp(long double u, int base, double w[4], long double scale) {
+  long double dL[5];
+  for (int n = 0; n < 5; ++n) {
+    long double sum = 0;
+    for (int r = 0; r < 5; ++r) {
+      if (r == n) continue;
+      long double t = 1.0L / (n - r);
+      for (int q = 0; q < 5; ++q)
+        if (q != n && q != r) t *= (u - (base + q)) / (long double)(n - q);
+      sum += t;
+    }
+    dL[n] = sum;
+  }
+  for (int m = 0; m < 4; ++m) {
+    long double acc = 0;
+    for (int n = m + 1; n < 5; ++n) acc += dL[n];
+    w[m] = (double)(scale * acc);
+  }
+}
+
+// Tables of the fourth-order level step and its level-sized buffers.
+int buildO4Level(hc_ctx* c) {
+  const hc_params& P = c->P;
+  const int nr = P.nr, na = P.na, g = kO4Ghost, ga = kO4Cart;
+  const int nA = na + 2 * ga, nG = na + 2 * g;
+  const double h = 1.0 / na;
+  Gauss G;
+  O4Level& O = c->o4l;
+  O.nr = nr; O.na = na; O.g = g; O.ga = ga; O.nA = nA; O.nG = nG;
+  O.Nv = (long)nr * na * na;
+  O.Ng = (long)(nr + 2 * g) * nG * nG;
+  O.Nc = (long)nr * nA * nA;
+  O.gamma = P.gamma; O.r0 = P.inner_radius; O.strength = P.strength; O.cfl = P.cfl;
+  std::vector<double> coef((size_t)6 * nA * nA * 27, 0.0), Ab((size_t)6 * nA * nA * 9);
+  std::vector<double> detx((size_t)6 * (na + 2) * (na + 2)), xhat((size_t)6 * nG * nG * 3);
+  std::vector<int2> ringJK;
+  for (int k = -ga; k < na + ga; ++k)
+    for (int j = -ga; j < na + ga; ++j)
+      if (!(j >= 0 && j < na && k >= 0 && k < na)) ringJK.push_back(make_int2(j, k));
+  O.nring = (int)ringJK.size();
+  std::vector<O4Point> ring((size_t)6 * O.nring * 5);
+  auto aIdx = [&](int b, int j, int k) { return ((size_t)b * nA + (k + ga)) * nA + (j + ga); };
+  for (int b = 0; b < 6; ++b) {
+    for (int k = -ga; k < na + ga; ++k)
+      for (int j = -ga; j < na + ga; ++j) {
+        double A[3][3] = {{0}}, I[3][3];
+        for (int p = 0; p < 8; ++p)
+          for (int q = 0; q < 8; ++q) {
+            double Aq[3][3];
+            basisAt(b, (j + G.x[p]) * h, (k + G.x[q]) * h, Aq, nullptr);
+            for (int r = 0; r < 3; ++r)
+              for (int s2 = 0; s2 < 3; ++s2) A[r][s2] += G.w[p] * G.w[q] * Aq[r][s2];
+          }
+        inv3(A, I);
+        for (int r = 0; r < 3; ++r)
+          for (int s2 = 0; s2 < 3; ++s2) {
+            Ab[aIdx(b, j, k) * 9 + 3 * r + s2] = A[r][s2];
+            coef[aIdx(b, j, k) * 27 + 3 * r + s2] = I[r][s2];
+          }
+      }
+    for (int k = -ga + 1; k < na + ga - 1; ++k)
+      for (int j = -ga + 1; j < na + ga - 1; ++j)
+        for (int e = 0; e < 9; ++e) {
+          coef[aIdx(b, j, k) * 27 + 9 + e] = 0.5 * (Ab[aIdx(b, j + 1, k) * 9 + e] - Ab[aIdx(b, j - 1, k) * 9 + e]);
+          coef[aIdx(b, j, k) * 27 + 18 + e] = 0.5 * (Ab[aIdx(b, j, k + 1) * 9 + e] - Ab[aIdx(b, j, k - 1) * 9 + e]);
+        }
+    for (int k = -1; k <= na; ++k)
+      for (int j = -1; j <= na; ++j) {
+        double det = 0;
+        for (int p = 0; p < 8; ++p)
+          for (int q = 0; q < 8; ++q) {
+            double Aq[3][3];
+            basisAt(b, (j + G.x[p]) * h, (k + G.x[q]) * h, Aq, nullptr);
+            det += G.w[p] * G.w[q] * det3(Aq);
+          }
+        detx[((size_t)b * (na + 2) + (k + 1)) * (na + 2) + (j + 1)] = det;
+      }
+    for (int k = -g; k < na + g; ++k)
+      for (int j = -g; j < na + g; ++j) {
+        double A[3][3], X[3];
+        basisAt(b, (j + 0.5) * h, (k + 0.5) * h, A, X);
+        for (int q = 0; q < 3; ++q) xhat[(((size_t)b * nG + (k + g)) * nG + (j + g)) * 3 + q] = X[q];
+      }
+    static const int off[5][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+    for (int r = 0; r < O.nring; ++r)
+      for (int q = 0; q < 5; ++q) {
+        const int j = ringJK[r].x + off[q][0], k = ringJK[r].y + off[q][1];
+        double A[3][3], X[3], y1, y2;
+        basisAt(b, (j + 0.5) * h, (k + 0.5) * h, A, X);
+        O4Point pt{};
+        pt.p = locateTie(X);
+        panelCoords(pt.p, X, y1, y2);
+        const long double u1 = (long double)y1 / h, u2 = (long double)y2 / h;
+        pt.j0 = std::max(0, std::min(na - 4, (int)std::floor((double)u1) - 1));
+        pt.k0 = std::max(0, std::min(na - 4, (int)std::floor((double)u2) - 1));
+        averageInterp(u1, pt.j0, pt.wj, q == 0 ? 5.0L / 6.0L : 1.0L / 24.0L);
+        averageInterp(u2, pt.k0, pt.wk, 1.0L);
+        ring[((size_t)b * O.nring + r) * 5 + q] = pt;
+      }
+  }
+  std::vector<double2> radial(nr + 2 * g + 2);
+  for (int i = -g - 1; i <= nr + g; ++i) {
+    const RadialRow rr = radialRow(P, i);
+    radial[i + g + 1] = make_double2(rr.vol, rr.rhalf);
+  }
+  cudaError_t err = cudaSuccess;
+  O.coef = upload(coef, c->owned, err);
+  O.detx = upload(detx, c->owned, err);
+  O.xhat = upload(xhat, c->owned, err);
+  O.radial = upload(radial, c->owned, err);
+  O.ringJK = upload(ringJK, c->owned, err);
+  O.ring = upload(ring, c->owned, err);
+  if (err != cudaSuccess) return cudaFail(err, "O4 level tables");
+  const int vlo[3] = {0, 0, 0}, vhi[3] = {nr - 1, na - 1, na - 1};
+  const size_t sizes[6] = {(size_t)6 * 8 * O.Ng, (size_t)6 * 8 * O.Nc, (size_t)6 * 8 * O.Nv, (size_t)6 * 8 * O.Nv,
+                           (size_t)6 * 2 * 2 * 8 * na * nr, o4ScratchDoubles(6, vlo, vhi, kO4Ghost)};
+  double** dst[6] = {&c->o4us, &c->o4cart, &c->o4next, &c->o4k, &c->o4reg, &c->o4lvlScratch};
+  for (int q = 0; q < 6; ++q) {
+    void* p = nullptr;
+    if ((err = cudaMalloc(&p, sizes[q] * sizeof(double))) != cudaSuccess) return cudaFail(err, "O4 level buffers");
+    c->owned.push_back(p);
+    *dst[q] = static_cast<double*>(p);
+    if ((err = cudaMemset(p, 0, sizes[q] * sizeof(double))) != cudaSuccess) return cudaFail(err, "O4 level buffers");
+  }
+  return HC_OK;
+}
+
+// Carve the operator scratch of nbox boxes (valid box [vlo, vhi]) from sp.
+void carveO4Scratch(O4Args& a, double* sp) {
+  long ng = 1, nf = 1, n1 = 1;
+  for (int d = 0; d < 3; ++d) {
+    const int ext = a.vhi[d] - a.vlo[d] + 1;
+    ng *= ext + 2 * kO4Ghost;
+    nf *= ext + 2 * kO4Ghost - 6 + 1;
+    n1 *= ext + 2;
+  }
+  const long nb = a.nbox;
+  a.WA = sp; sp += nb * 8 * ng;
+  a.WP = sp; sp += nb * 8 * ng;
+  a.th = sp; sp += nb * ng;
+  a.thr = sp; sp += nb * ng;
+  a.face = sp; sp += nb * (long)kO4FaceArrays * nf;
+  a.mj = sp; sp += nb * n1;
+  a.kp = sp;
+}
+
 int allocWorkspace(hc_ctx* c) {
   const size_t nv = 6 * NC * (size_t)c->L.Nv, ng = 6 * NC * (size_t)c->L.Ng;
   void* p;
@@ -621,6 +794,55 @@ int rkStep(hc_ctx* c, double* ju, double dtv, const double* invMax, unsigned lon
   return HC_OK;
 }
 
+// The batched operator over the six panels of the fourth-order level.
+O4Args levelO4Args(hc_ctx* c, const double* us, double* k) {
+  O4Args a{};
+  a.G = c->o4;
+  a.nbox = 6;
+  a.block0 = 0;
+  a.ghost = kO4Ghost;
+  a.vlo[0] = a.vlo[1] = a.vlo[2] = 0;
+  a.vhi[0] = c->P.nr - 1;
+  a.vhi[1] = a.vhi[2] = c->P.na - 1;
+  a.U = us;
+  for (int d = 0; d < 3; ++d) {
+    a.ur.lo[d] = -kO4Ghost;
+    a.ur.n[d] = a.vhi[d] + 1 + 2 * kO4Ghost;
+  }
+  a.ur.N = c->o4l.Ng;
+  a.uStride = 8 * c->o4l.Ng;
+  a.scale = 1.0;
+  a.rhs = k;
+  a.rhsStride = 8 * c->o4l.Nv;
+  carveO4Scratch(a, c->o4lvlScratch);
+  return a;
+}
+
+// One fourth-order RK4 step: per stage, prepare USph from the stage state,
+// evaluate the operator into k (seam fluxes into the register), update the
+// accumulator and the next stage; then reconcile the seam fluxes.
+int o4Step(hc_ctx* c, double* ju, double dtv, const double* invMax, double tbase, const double* tdev, cudaStream_t s) {
+  static const double c4[4] = {0, 0.5, 0.5, 1}, b4[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+  const O4Level& O = c->o4l;
+  int rc = checkLaunch(cudaMemsetAsync(c->o4reg, 0, sizeof(double) * 6 * 2 * 2 * 8 * O.na * O.nr, s), "register");
+  for (int stage = 0; stage < 4 && rc == HC_OK; ++stage) {
+    O4StageIO io{O, stage == 0 ? ju : c->o4next, c->o4cart, c->o4us, StageTime{tbase, tdev, c4[stage], invMax, dtv}};
+    rc = checkLaunch(launchO4Prepare(io, s), "O4 prepare");
+    if (rc == HC_OK) rc = checkLaunch(cudaMemsetAsync(c->o4k, 0, sizeof(double) * 6 * 8 * O.Nv, s), "O4 k");
+    if (rc != HC_OK) break;
+    O4Args a = levelO4Args(c, c->o4us, c->o4k);
+    a.reg = c->o4reg;
+    a.regWeight = invMax ? b4[stage] : dtv * b4[stage];
+    a.regWeightDev = invMax;
+    a.cfl = c->P.cfl;
+    rc = checkLaunch(launchO4BoxOperator(a, s), "O4 operator");
+    if (rc == HC_OK)
+      rc = checkLaunch(launchO4Update(O, stage, c->o4k, ju, c->acc, c->o4next, invMax, c->P.cfl, dtv, s), "O4 update");
+  }
+  if (rc == HC_OK) rc = checkLaunch(launchO4Reflux(O, c->L, c->o4reg, ju, s), "O4 reflux");
+  return rc;
+}
+
 }  // namespace
 
 namespace hc {
@@ -663,6 +885,7 @@ int hc_ctx_create(const hc_params* p, int device, hc_ctx** out) {
   int rc = buildLevel(c);
   if (rc == HC_OK) rc = allocWorkspace(c);
   if (rc == HC_OK && p->spatial_order == 4) rc = buildO4Geometry(c);
+  if (rc == HC_OK && p->spatial_order == 4) rc = buildO4Level(c);
   if (rc != HC_OK) {
     hc_ctx_destroy(c);
     return rc;
@@ -681,7 +904,10 @@ int hc_ctx_destroy(hc_ctx* c) {
 }
 
 size_t hc_level_state_size(const hc_ctx* c) { return c ? 6 * NC * (size_t)c->L.Nv : 0; }
-size_t hc_level_primitive_size(const hc_ctx* c) { return c ? 6 * NC * (size_t)c->L.Ng : 0; }
+size_t hc_level_primitive_size(const hc_ctx* c) {
+  if (!c) return 0;
+  return c->P.spatial_order == 4 ? 6 * NC * (size_t)c->o4l.Ng : 6 * NC * (size_t)c->L.Ng;
+}
 
 int hc_box_rhs(hc_ctx* c, const hc_box* box, const double* w, const double* const* panel, double scale, double* rhs,
                double* const* flux, void* stream) {
@@ -751,27 +977,7 @@ int hc_box_rhs_o4(hc_ctx* c, const hc_box* box, const double* usph, double scale
     c->o4scratch = static_cast<double*>(p);
     c->o4scratchDoubles = need;
   }
-  double* sp = c->o4scratch;
-  Reg g{};
-  {
-    int lo[3], hi[3];
-    for (int d = 0; d < 3; ++d) { lo[d] = B.lo[d] - kO4Ghost; hi[d] = B.hi[d] + kO4Ghost; }
-    g.N = (long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
-  }
-  long nf = 1, n1 = 1, n2 = 1;
-  for (int d = 0; d < 3; ++d) {
-    const int ext = B.hi[d] - B.lo[d] + 1;
-    nf *= ext + 2 * kO4Ghost - 6 + 1;
-    n1 *= ext + 2;
-    n2 *= ext + 4;
-  }
-  a.WA = sp; sp += 8 * g.N;
-  a.WP = sp; sp += 8 * g.N;
-  a.th = sp; sp += g.N;
-  a.thr = sp; sp += g.N;
-  a.face = sp; sp += (long)kO4FaceArrays * nf;
-  a.mj = sp; sp += n1;
-  a.kp = sp;
+  carveO4Scratch(a, c->o4scratch);
   return checkLaunch(launchO4BoxOperator(a, (cudaStream_t)stream), "hc_box_rhs_o4");
 }
 
@@ -792,6 +998,10 @@ int hc_box_gravity(hc_ctx* c, const hc_box* box, const double* w, double* rhs, v
 int hc_level_prepare(hc_ctx* c, const double* ju, double* w, double t, void* stream) {
   if (!c || !ju || !w) return fail(HC_ERR_ARG, "null argument");
   cudaStream_t s = (cudaStream_t)stream;
+  if (c->P.spatial_order == 4) {
+    O4StageIO io{c->o4l, ju, c->o4cart, w, StageTime{t, nullptr, 0.0, nullptr, 0.0}};
+    return checkLaunch(launchO4Prepare(io, s), "O4 prepare");
+  }
   int rc = checkLaunch(launchPrimValid(c->L, ju, w, s), "prim");
   if (rc != HC_OK) return rc;
   StageTime st{t, nullptr, 0.0, nullptr, 0.0};
@@ -800,6 +1010,13 @@ int hc_level_prepare(hc_ctx* c, const double* ju, double* w, double t, void* str
 
 int hc_level_rhs(hc_ctx* c, const double* w, double* k, void* stream) {
   if (!c || !w || !k) return fail(HC_ERR_ARG, "null argument");
+  if (c->P.spatial_order == 4) {
+    if (c->P.sun_gravity) return fail(HC_ERR_UNSUPPORTED, "fourth-order gravity is not built");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int rc = checkLaunch(cudaMemsetAsync(k, 0, sizeof(double) * 6 * NC * c->o4l.Nv, s), "O4 k");
+    if (rc != HC_OK) return rc;
+    return checkLaunch(launchO4BoxOperator(levelO4Args(c, w, k), s), "O4 operator");
+  }
   StageArgs a = levelArgs(c, w);
   a.rhs = k;
   return checkLaunch(launchStage(a, MODE_RHS, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
@@ -811,6 +1028,10 @@ int hc_level_rk4_step(hc_ctx* c, double* ju, double dt, double t, void* stream) 
   if (!c || !ju) return fail(HC_ERR_ARG, "null argument");
   if (!(dt > 0)) return fail(HC_ERR_ARG, "dt must be positive");
   cudaStream_t s = (cudaStream_t)stream;
+  if (c->P.spatial_order == 4) {
+    if (c->P.sun_gravity) return fail(HC_ERR_UNSUPPORTED, "fourth-order gravity is not built");
+    return o4Step(c, ju, dt, nullptr, t, nullptr, s);
+  }
   const int rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
   if (rc != HC_OK) return rc;
   return rkStep(c, ju, dt, nullptr, nullptr, t, nullptr, s);
@@ -820,6 +1041,18 @@ int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, do
   if (!c || !ju || nsteps < 0) return fail(HC_ERR_ARG, "bad argument");
   if (nsteps == 0) return HC_OK;
   cudaStream_t s = (cudaStream_t)stream;
+  if (c->P.spatial_order == 4) {
+    // dtCFL of the state at the start of each step, then the step.
+    if (c->P.sun_gravity) return fail(HC_ERR_UNSUPPORTED, "fourth-order gravity is not built");
+    int rc = HC_OK;
+    const double* invMax = reinterpret_cast<const double*>(c->invMax);
+    for (int n = 0; n < nsteps && rc == HC_OK; ++n) {
+      rc = checkLaunch(launchCfl(c->L, ju, c->invMax, s), "cfl");
+      if (rc == HC_OK) rc = o4Step(c, ju, 0.0, invMax, 0.0, time_dev, s);
+      if (rc == HC_OK) rc = checkLaunch(launchAdvanceTime(time_dev, invMax, c->P.cfl, dt_dev, s), "time");
+    }
+    return rc;
+  }
   // The first step's primitives and CFL rate come from ju; every later
   // step's come from the previous step's last stage.
   int rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");

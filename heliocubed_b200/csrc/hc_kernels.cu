@@ -43,25 +43,7 @@ __device__ __forceinline__ void nativeToPrimitive(const double u[8], const doubl
 
 // Analytic inner wind, src/BoxOp_PreStage.H:7-47 (time-dependent form).
 __device__ void analyticWind(const DevLevel& L, const double X[3], double t, double u[8]) {
-  const double gam = L.gamma, r_BC = L.r0;
-  const double r = sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
-  const double theta = atan2(sqrt(X[0] * X[0] + X[1] * X[1]), X[2]);
-  const double phi = atan2(X[1], X[0]);
-  const double p0 = 1.0e-7, rho0 = 700 * kMP, u0 = 500.0 * 1e5;
-  const double rho = rho0 * pow(r_BC / r, 2.0);
-  const double p = p0 * pow(r_BC / r, 2.0 * gam);
-  const double carr_rot_time = 25.38 * 24 * 60 * 60;
-  const double omega = 2.0 * kPi / carr_rot_time;
-  const double phit = phi - omega * t;
-  const double perturbationScale = L.strength / 100.0;
-  const double sinTheta = sin(theta);
-  const double angularPattern = pow(sinTheta, 5) * sin(5 * phit) + pow(sinTheta, 10) * sin(10 * phit);
-  const double ur = u0 - perturbationScale * u0 / 3 * angularPattern;
-  u[0] = rho;
-  u[1] = ur * rho;
-  u[2] = u[3] = u[5] = u[6] = u[7] = 0.0;
-  const double umag = sqrt(u[1] * u[1]) / u[0];
-  u[4] = p / (gam - 1.0) + 0.5 * u[0] * umag * umag + 0.0 / 8.0 / kPi;
+  windConserved(L.gamma, L.r0, L.strength, X, t, u);
 }
 
 // ---------------------------------------------------------------------------

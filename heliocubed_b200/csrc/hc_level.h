@@ -174,11 +174,62 @@ struct O4Args {
   double* face; // [nbox][kO4FaceArrays][F]
   double* mj;   // [nbox][V+1]
   double* kp;   // [nbox][8][V+2]
+  // seam flux register (level step only; boxes are whole panels): the
+  // final face flux of panel-boundary faces of directions 1, 2 is added
+  // times regWeight into reg [6][2][2][8][na][nr]
+  double* reg;
+  double regWeight;
+  const double* regWeightDev;  // when set, regWeight *= cfl / *regWeightDev
+  double cfl;
 };
 constexpr int kO4FaceArrays = 8 * 9 + 8;  // WL, WR, FS, QD/DP, FA, FM, FR, Fx (8 each) + thF, PS, BP, PA, T3, Bflux, Bprod, pad
 
 cudaError_t launchO4BoxOperator(const O4Args& a, cudaStream_t s);
 size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost);
+
+// ---------------------------------------------------------------------------
+// Fourth-order level step (hc_o4level.cu): one box per panel.
+// ---------------------------------------------------------------------------
+constexpr int kO4Cart = 6;  // angular ghost layers of the Cartesian averages
+
+// One point of a seam ghost average: panel p, 4 x 4 donor cells starting at
+// (j0, k0), tensor weights wj (times the point's coefficient) and wk.
+struct O4Point {
+  int p, j0, k0, pad;
+  double wj[4], wk[4];
+};
+
+struct O4Level {
+  int nr, na, g, ga;        // g = kO4Ghost, ga = kO4Cart
+  int nA, nG;               // na + 2 ga, na + 2 g
+  int nring;                // seam ghost positions per panel
+  long Nv, Ng, Nc;          // per panel: valid, ghosted native, Cartesian
+  const double* coef;       // [6][nA][nA][27]: <A>^-1, D1 <A>, D2 <A> (row-major)
+  const double* detx;       // [6][na+2][na+2]: <det A>, j, k in [-1, na]
+  const double* xhat;       // [6][nG][nG][3]: unit direction of the cell centre
+  const double2* radial;    // [nr + 2g + 2], index i + g + 1: {dVolr, cell-centre radius}
+  const int2* ringJK;       // [nring]: (j, k) of each seam ghost position
+  const O4Point* ring;      // [6][nring][5]
+  double gamma, r0, strength, cfl;
+};
+
+// Kernel arguments of the stage preparation and the RK update.
+struct O4StageIO {
+  O4Level O;
+  const double* ju;   // stage state [6][8][Nv]
+  double* cart;       // [6][8][Nc]
+  double* us;         // [6][8][Ng]
+  StageTime t;
+};
+
+cudaError_t launchO4Prepare(const O4StageIO& io, cudaStream_t s);
+// acc/stage/ju update after stage s (classical RK4, b = 1/6, 1/3, 1/3, 1/6;
+// next stage = ju + a_{s+1} dt k with a = 1/2, 1/2, 1).
+cudaError_t launchO4Update(const O4Level& O, int stage, const double* k, double* ju, double* acc, double* next,
+                           const double* invDtMax, double cfl, double dtv, cudaStream_t s);
+// Seam flux reconciliation from the time-integrated register
+// [6][2][2][8][na][nr] (edge axis 1..2, side 0..1, component, along-edge, radial).
+cudaError_t launchO4Reflux(const O4Level& O, const DevLevel& L, const double* reg, double* ju, cudaStream_t s);
 }  // namespace hc
 
 // Context internals for sibling translation units (not part of the C ABI).

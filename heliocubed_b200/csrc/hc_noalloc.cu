@@ -72,6 +72,8 @@ extern "C" int hc_level_rk4_step_noalloc(hc_ctx* ctx, double* ju, double dt, dou
   if (!(dt > 0)) return setLastError(HC_ERR_ARG, "hc_level_rk4_step_noalloc: dt must be positive");
   const DevLevel& L = *ctxLevel(ctx);
   const hc_params& P = *ctxParams(ctx);
+  if (P.spatial_order != 2)
+    return setLastError(HC_ERR_UNSUPPORTED, "hc_level_rk4_step_noalloc: only second-order contexts are supported");
   const size_t wDoubles = 6 * size_t(NC) * size_t(L.Ng), accDoubles = 6 * size_t(NC) * size_t(L.Nv);
   const size_t need = 2 * wDoubles + accDoubles;
   if (need > kScratchDoubles) {

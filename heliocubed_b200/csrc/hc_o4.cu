@@ -326,7 +326,6 @@ struct View {
   __device__ double operator()(int c, int i, int j, int k) const { return p[c * r.N + roff(r, i, j, k)]; }
 };
 
-__device__ __forceinline__ void stepDir(int q[3], int d, int s) { q[d] += s; }
 
 __device__ double lapFace(const View& f, int c, int d, int i, int j, int k) {
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
@@ -803,6 +802,17 @@ __global__ void o4FaceFinalKernel(const Ctx c) {
       double* fo2 = a.flux[d] + (long)b * 8 * r0.N + roff(r0, i, j, k);
 #pragma unroll
       for (int q = 0; q < 8; ++q) fo2[q * r0.N] = fx[q];
+    }
+    if (a.reg && d > 0) {
+      const int f = d == 1 ? j : k;
+      if (f == 0 || f == a.G.na) {
+        const long nrna = (long)a.G.na * a.G.nr;
+        const int side = f == 0 ? 0 : 1, s = d == 1 ? k : j;
+        const double w = a.regWeightDev ? a.regWeight * (a.cfl / *a.regWeightDev) : a.regWeight;
+        double* R = a.reg + (((long)blk * 2 + (d - 1)) * 2 + side) * 8 * nrna + (long)s * a.G.nr + i;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) R[q * nrna] += w * fx[q];
+      }
     }
   });
 }

@@ -1,0 +1,314 @@
+// Fourth-order level step on one box per panel: stage preparation, RK4
+// update and panel-seam flux reconciliation.  FP64.
+//
+// Stage preparation follows the Cartesian state conversion of
+// src/MHD_StateConversion.H:153-316 (state_conversion = 1):
+//   1. o4CartesianKernel: JU -> fourth-order Cartesian averages U inside each
+//      panel (quotient by <det A> with the (1/12) D(JU/det) D(det) angular
+//      correction, then by dVolr with the radial one);
+//   2. o4SeamKernel: U on kO4Cart angular ghost layers (panel corners
+//      included) from the panels that contain the ghost cells (own
+//      fourth-order average interpolation; the tables come from the host);
+//   3. o4NativeKernel: U -> native averages USph with the fourth-order matrix
+//      quotient of src/MHD_CachedCartesianConversion.H:65-210 on the ghosted
+//      box, and the radial ghosts of src/BoxOp_PreStage.H:57-228 (inner:
+//      analytic wind; outer: last layer scaled by (r_last / r)^2, B_t by r).
+// The operator then runs batched over the six panels (hc_o4.cu) and adds
+// its seam face fluxes, times b_s dt, into a register; after the fourth
+// stage every seam face takes the mean of both sides' time-integrated
+// fluxes (src/MHD_AMR.H:1478-1497; src/MHD_LevelRK.H:45-56).
+#include <cuda_runtime.h>
+
+#include "hc_device.cuh"
+#include "hc_level.h"
+
+namespace hc {
+namespace {
+
+constexpr int kThreads = 128;
+
+int blocksFor(long n) {
+  long g = (n + kThreads - 1) / kThreads;
+  if (g > 148L * 64) g = 148L * 64;
+  return (int)(g < 1 ? 1 : g);
+}
+
+__device__ __forceinline__ long vIdx(const O4Level& O, int b, int c, int i, int j, int k) {
+  return ((long)b * 8 + c) * O.Nv + i + (long)O.nr * (j + (long)O.na * k);
+}
+__device__ __forceinline__ long cIdx(const O4Level& O, int b, int c, int i, int j, int k) {
+  return ((long)b * 8 + c) * O.Nc + i + (long)O.nr * ((j + O.ga) + (long)O.nA * (k + O.ga));
+}
+__device__ __forceinline__ long gIdx4(const O4Level& O, int b, int c, int i, int j, int k) {
+  return ((long)b * 8 + c) * O.Ng + (i + O.g) + (long)(O.nr + 2 * O.g) * ((j + O.g) + (long)O.nG * (k + O.g));
+}
+__device__ __forceinline__ double detAt(const O4Level& O, int b, int j, int k) {
+  return O.detx[((long)b * (O.na + 2) + (k + 1)) * (O.na + 2) + (j + 1)];
+}
+__device__ __forceinline__ double volAt(const O4Level& O, int i) { return O.radial[i + O.g + 1].x; }
+
+// 1. JU -> Cartesian averages, src/MHD_StateConversion.H:198-262.
+__global__ void o4CartesianKernel(const O4StageIO io) {
+  const O4Level& O = io.O;
+  const long n = 6L * O.Nv;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(t / O.Nv);
+    const long r = t - (long)b * O.Nv;
+    const int i = (int)(r % O.nr);
+    const int j = (int)((r / O.nr) % O.na);
+    const int k = (int)(r / ((long)O.nr * O.na));
+    const int na = O.na;
+    const double det = detAt(O, b, j, k);
+    const double dd1 = 0.5 * (detAt(O, b, j + 1, k) - detAt(O, b, j - 1, k));
+    const double dd2 = 0.5 * (detAt(O, b, j, k + 1) - detAt(O, b, j, k - 1));
+    // CubedSphereShell::deriv3case at (j, k): undivided centred difference
+    // inside the panel, second-order one-sided on its first and last cells;
+    // the three-cell windows it reads
+    const int ja = j == 0 ? 0 : (j == na - 1 ? na - 3 : j - 1);
+    const int ka = k == 0 ? 0 : (k == na - 1 ? na - 3 : k - 1);
+    double detJ[3], detK[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      detJ[q] = detAt(O, b, ja + q, k);
+      detK[q] = detAt(O, b, j, ka + q);
+    }
+    // the radial window of deriv3case at i
+    const int ia = i == 0 ? 0 : (i == O.nr - 1 ? O.nr - 3 : i - 1);
+    const double dv = 0.5 * (volAt(O, i + 1) - volAt(O, i - 1));
+    for (int c = 0; c < 8; ++c) {
+      double ang[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int ii = ia + q;
+        double qj[3], qk[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          qj[m] = io.ju[vIdx(O, b, c, ii, ja + m, k)] / detJ[m];
+          qk[m] = io.ju[vIdx(O, b, c, ii, j, ka + m)] / detK[m];
+        }
+        const double d1 = j == 0 ? 0.5 * (-3.0 * qj[0] + 4.0 * qj[1] - qj[2])
+                        : (j == na - 1 ? 0.5 * (3.0 * qj[2] - 4.0 * qj[1] + qj[0]) : 0.5 * (qj[2] - qj[0]));
+        const double d2 = k == 0 ? 0.5 * (-3.0 * qk[0] + 4.0 * qk[1] - qk[2])
+                        : (k == na - 1 ? 0.5 * (3.0 * qk[2] - 4.0 * qk[1] + qk[0]) : 0.5 * (qk[2] - qk[0]));
+        const double corr = d1 * dd1 + d2 * dd2;
+        ang[q] = (io.ju[vIdx(O, b, c, ii, j, k)] - corr / 12.0) / det;
+      }
+      double rq[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) rq[q] = ang[q] / volAt(O, ia + q);
+      const int slot = i - ia;
+      const double dq = i == 0 ? 0.5 * (-3.0 * rq[0] + 4.0 * rq[1] - rq[2])
+                      : (i == O.nr - 1 ? 0.5 * (3.0 * rq[2] - 4.0 * rq[1] + rq[0]) : 0.5 * (rq[2] - rq[0]));
+      io.cart[cIdx(O, b, c, i, j, k)] = (ang[slot] - dq * dv / 12.0) / volAt(O, i);
+    }
+  }
+}
+
+// 2. Seam ghosts of the Cartesian averages.
+__global__ void o4SeamKernel(const O4StageIO io) {
+  const O4Level& O = io.O;
+  const long n = 6L * O.nring * O.nr;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % O.nr);
+    const long q = t / O.nr;
+    const int pos = (int)(q % O.nring);
+    const int b = (int)(q / O.nring);
+    const int2 jk = O.ringJK[pos];
+    const O4Point* pts = O.ring + ((long)b * O.nring + pos) * 5;
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+    for (int p = 0; p < 5; ++p) {
+      const O4Point pt = pts[p];
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        double row[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const long base = cIdx(O, pt.p, 0, i, pt.j0 + m, pt.k0 + kk);
+#pragma unroll
+          for (int c = 0; c < 8; ++c) row[c] += pt.wj[m] * io.cart[base + (long)c * O.Nc];
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] += pt.wk[kk] * row[c];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) io.cart[cIdx(O, b, c, i, jk.x, jk.y)] = v[c];
+  }
+}
+
+// Native conversion of one cell (src/MHD_CachedCartesianConversion.H:65-124).
+__device__ void nativeCell(const O4Level& O, const double* __restrict__ cart, int b, int i, int j, int k, double out[8]) {
+  const double* cf = O.coef + (((long)b * O.nA + (k + O.ga)) * O.nA + (j + O.ga)) * 27;
+  out[0] = cart[cIdx(O, b, 0, i, j, k)];
+  out[4] = cart[cIdx(O, b, 4, i, j, k)];
+#pragma unroll
+  for (int grp = 0; grp < 2; ++grp) {
+    const int st = grp == 0 ? 1 : 5;
+    double q[4][3];
+    const int nj[4] = {j + 1, j - 1, j, j};
+    const int nk[4] = {k, k, k + 1, k - 1};
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const double* I = O.coef + (((long)b * O.nA + (nk[e] + O.ga)) * O.nA + (nj[e] + O.ga)) * 27;
+      const double x0 = cart[cIdx(O, b, st, i, nj[e], nk[e])];
+      const double x1 = cart[cIdx(O, b, st + 1, i, nj[e], nk[e])];
+      const double x2 = cart[cIdx(O, b, st + 2, i, nj[e], nk[e])];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        double v = 0.0;
+        v += I[3 * r] * x0 * 1.0;
+        v += I[3 * r + 1] * x1 * 1.0;
+        v += I[3 * r + 2] * x2 * 1.0;
+        q[e][r] = v;
+      }
+    }
+    double d1[3], d2[3], corrected[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      d1[r] = 0.5 * (q[0][r] - q[1][r]);
+      d2[r] = 0.5 * (q[2][r] - q[3][r]);
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      double first = 0.0, second = 0.0;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        first += cf[9 + 3 * r + s] * d1[s] * (-1.0 / 12.0);
+        second += cf[18 + 3 * r + s] * d2[s] * (-1.0 / 12.0);
+      }
+      double correction = 0.0;
+      correction += first;
+      correction += second;
+      corrected[r] = cart[cIdx(O, b, st + r, i, j, k)] + correction;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      double v = 0.0;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) v += cf[3 * r + s] * corrected[s] * 1.0;
+      out[st + r] = v;
+    }
+  }
+}
+
+// 3. Native averages on the ghosted box and the radial ghosts.
+__global__ void o4NativeKernel(const O4StageIO io) {
+  const O4Level& O = io.O;
+  const int n0 = O.nr + 2 * O.g;
+  const long n = 6L * n0 * O.nG * O.nG;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % n0) - O.g;
+    long q = t / n0;
+    const int j = (int)(q % O.nG) - O.g;
+    q /= O.nG;
+    const int k = (int)(q % O.nG) - O.g;
+    const int b = (int)(q / O.nG);
+    double u[8];
+    if (i < 0) {
+      const StageTime& st = io.t;
+      const double dt = st.invDtMax ? O.cfl / *st.invDtMax : st.dtv;
+      const double time = st.tbase + (st.tdev ? *st.tdev : 0.0) + st.cfrac * dt;
+      const double* xh = O.xhat + (((long)b * O.nG + (k + O.g)) * O.nG + (j + O.g)) * 3;
+      const double radius = O.radial[i + O.g + 1].y;
+      const double X[3] = {radius * xh[0], radius * xh[1], radius * xh[2]};
+      windConserved(O.gamma, O.r0, O.strength, X, time, u);
+    } else if (i < O.nr) {
+      nativeCell(O, io.cart, b, i, j, k, u);
+    } else {
+      nativeCell(O, io.cart, b, O.nr - 1, j, k, u);
+      const double rl = O.radial[O.nr - 1 + O.g + 1].y, rr = O.radial[i + O.g + 1].y;
+      const double s2 = pow(rl / rr, 2.0), s1 = pow(rl / rr, 1.0);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) u[c] *= c < 6 ? s2 : s1;
+    }
+    double* o = io.us + gIdx4(O, b, 0, i, j, k);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) o[(long)c * O.Ng] = u[c];
+  }
+}
+
+// RK4 update after stage s (the tableau of src/MHD_AMRRungeKutta.H:10-12).
+__global__ void o4UpdateKernel(const O4Level O, int stage, const double* __restrict__ k, double* __restrict__ ju,
+                               double* __restrict__ acc, double* __restrict__ next, const double* invDtMax, double cfl,
+                               double dtv) {
+  const double b4[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+  const double a4[4] = {0.5, 0.5, 1.0, 0.0};
+  const double dt = invDtMax ? cfl / *invDtMax : dtv;
+  const double fb = dt * b4[stage], fa = dt * a4[stage];
+  const long n = 6L * 8 * O.Nv;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const double kv = k[t];
+    if (stage == 0) {
+      const double u = ju[t];
+      acc[t] = u + fb * kv;
+      next[t] = u + fa * kv;
+    } else if (stage < 3) {
+      acc[t] += fb * kv;
+      next[t] = ju[t] + fa * kv;
+    } else {
+      ju[t] = acc[t] + fb * kv;
+    }
+  }
+}
+
+// Seam reconciliation of one edge axis (cells of different faces of one
+// axis never coincide, so each launch is race free).
+__global__ void o4RefluxKernel(const O4Level O, const DevLevel L, int ax, const double* __restrict__ reg,
+                               double* __restrict__ ju) {
+  const long nrna = (long)O.na * O.nr;
+  const long n = 6L * 2 * nrna;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % O.nr);
+    long q = t / O.nr;
+    const int s = (int)(q % O.na);
+    q /= O.na;
+    const int side = (int)(q % 2);
+    const int b = (int)(q / 2);
+    const int e = (ax - 1) * 2 + side;
+    const EdgeLink nb = L.edge[b * 4 + e];
+    const int sn = L.faceMap[((long)b * 4 + e) * O.na + s];
+    const double sigma = nb.side != side ? 1.0 : -1.0;
+    const double dir = side ? -(double)O.na : (double)O.na;
+    const int edge = side ? O.na - 1 : 0;
+    const int j = ax == 1 ? edge : s, k = ax == 1 ? s : edge;
+    const double* fa = reg + (((long)b * 2 + (ax - 1)) * 2 + side) * 8 * nrna + (long)s * O.nr + i;
+    const double* fb = reg + (((long)nb.nb * 2 + (nb.axis - 1)) * 2 + nb.side) * 8 * nrna + (long)sn * O.nr + i;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const double a = fa[c * nrna];
+      const double mean = 0.5 * (a + sigma * fb[c * nrna]);
+      ju[vIdx(O, b, c, i, j, k)] += dir * (mean - a);
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launchO4Prepare(const O4StageIO& io, cudaStream_t s) {
+  const O4Level& O = io.O;
+  o4CartesianKernel<<<blocksFor(6L * O.Nv), kThreads, 0, s>>>(io);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  o4SeamKernel<<<blocksFor(6L * O.nring * O.nr), kThreads, 0, s>>>(io);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  o4NativeKernel<<<blocksFor(6L * (O.nr + 2 * O.g) * O.nG * O.nG), kThreads, 0, s>>>(io);
+  return cudaGetLastError();
+}
+
+cudaError_t launchO4Update(const O4Level& O, int stage, const double* k, double* ju, double* acc, double* next,
+                           const double* invDtMax, double cfl, double dtv, cudaStream_t s) {
+  o4UpdateKernel<<<blocksFor(6L * 8 * O.Nv), kThreads, 0, s>>>(O, stage, k, ju, acc, next, invDtMax, cfl, dtv);
+  return cudaGetLastError();
+}
+
+cudaError_t launchO4Reflux(const O4Level& O, const DevLevel& L, const double* reg, double* ju, cudaStream_t s) {
+  for (int ax = 1; ax <= 2; ++ax) {
+    o4RefluxKernel<<<blocksFor(6L * 2 * O.na * O.nr), kThreads, 0, s>>>(O, L, ax, reg, ju);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace hc

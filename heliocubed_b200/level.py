@@ -101,6 +101,74 @@ class InitSpec:
         return InitSpec(pulse_block=int(rng.integers(0, 6)), pulse_i=pick(nr), pulse_j=pick(na), pulse_k=pick(na))
 
 
+_PERM = ((1, 2, 0), (1, 2, 0), (1, 0, 2), (0, 1, 2), (1, 0, 2), (0, 1, 2))
+_SIGN = ((1, -1, -1), (1, 1, 1), (1, -1, 1), (1, 1, 1), (-1, 1, 1), (-1, -1, 1))
+
+
+def cell_directions(na: int) -> np.ndarray:
+    """Unit Cartesian direction of every cell centre, [6][3][k][j]
+    (equiangular gnomonic panels, xi = (j + 1/2) / na)."""
+    x = (np.arange(na) + 0.5) / na
+    a = np.tan(-np.pi / 4 + np.pi / 2 * x)[None, :]
+    c = np.tan(-np.pi / 4 + np.pi / 2 * x)[:, None]
+    rho = np.sqrt(1 + a * a + c * c)
+    q = (1 / rho, a / rho, c / rho)
+    out = np.zeros((6, 3, na, na))
+    for b in range(6):
+        for k in range(3):
+            out[b, k] = _SIGN[b][k] * np.broadcast_to(q[_PERM[b][k]], (na, na))
+    return out
+
+
+def perturbed_wind_state(params: Params, det: np.ndarray, dvolr: np.ndarray, seed: int, amp: float = 0.05,
+                         spec: "InitSpec | None" = None) -> np.ndarray:
+    """Synthetic level state JU [6][8][k][j][i] (host, float64): the
+    Parker-like wind of InitSpec (rho ~ r^-2, v_r, p ~ r^-2 gamma,
+    B_r ~ r^-2 sign(cos theta)) plus seeded tangential perturbations of
+    relative size `amp` in v and B.  The tangential field is the surface
+    curl of a seeded stream function times (r_ref / r)^2, so div B = 0 for
+    the continuous field.  Cell averages are taken as J x point values at
+    the cell centre (J = <det A> dVolr); det [6][k][j], dvolr [nr]."""
+    spec = spec or InitSpec()
+    nr, na, gam = params.nr, params.na, params.gamma
+    rng = np.random.default_rng(seed)
+    r0, r1, C = params.inner_radius, params.outer_radius, params.radial_stretch
+    Rt = (r1 - r0) / np.expm1(C)
+    r = r0 + Rt * np.expm1(C * (np.arange(nr) + 0.5) / nr)
+    s = spec.r_ref / r
+    X = cell_directions(na)                                    # [6][3][k][j]
+
+    def tangential_pattern(nmodes=4):
+        """Surface gradient x rhat of psi = sum_m c_m sin(k_m . X + phi_m),
+        normalised to unit max magnitude."""
+        kv = rng.normal(size=(nmodes, 3)) * 2.0
+        ph = rng.uniform(0, 2 * np.pi, nmodes)
+        cm = rng.normal(size=nmodes)
+        grad = np.zeros_like(X)
+        for m in range(nmodes):
+            arg = np.einsum("q,bqkj->bkj", kv[m], X) + ph[m]
+            grad += cm[m] * np.cos(arg)[:, None] * kv[m][None, :, None, None]
+        grad -= np.einsum("bqkj,bqkj->bkj", grad, X)[:, None] * X   # tangential part
+        curl = np.cross(grad, X, axis=1)
+        return curl / np.abs(curl).max()
+
+    vt = tangential_pattern()
+    bt = tangential_pattern()
+    rho = spec.rho0 * s ** 2                                   # [nr]
+    p = spec.p0 * s ** (2 * gam)
+    sgn = np.sign(X[:, 2])                                     # sign(cos theta)
+    Br = spec.b0 * s[None, None, None, :] ** 2 * sgn[..., None]
+    ju = np.zeros((6, 8, na, na, nr))
+    v = spec.vr * X[..., None] + amp * spec.vr * vt[..., None]                     # [6][3][k][j][i]
+    B = Br[:, None] * X[..., None] + amp * spec.b0 * bt[..., None] * s[None, None, None, None, :] ** 2
+    J = det[:, :, :, None] * dvolr[None, None, None, :]
+    ju[:, 0] = rho * J
+    ju[:, 1:4] = rho * v * J[:, None]
+    ju[:, 5:8] = B * J[:, None]
+    ju[:, 4] = (p / (gam - 1) + 0.5 * rho * (v ** 2).sum(1) + (B ** 2).sum(1) / (8 * np.pi)) * J
+    return ju
+
+
 def _ptr(t: torch.Tensor | None):
     if t is None:
         return None
@@ -168,6 +236,14 @@ class Shell:
         s = spec.to_c()
         N.check(self._lib.hc_level_init(self._ctx, C.byref(s), _ptr(ju), _stream()), "hc_level_init")
         return ju
+
+    def init_perturbed_wind(self, seed: int, amp: float = 0.05) -> torch.Tensor:
+        """Level state of perturbed_wind_state (built on the host, copied)."""
+        p = self.params
+        det = self.geometry(4).reshape(6, p.na, p.na)
+        dvolr = self.geometry(0).reshape(p.nr + 1, 4)[:p.nr, 3]
+        ju = perturbed_wind_state(p, det, dvolr, seed, amp)
+        return torch.from_numpy(np.ascontiguousarray(ju.reshape(-1))).to(self._dev)
 
     def prepare(self, ju: torch.Tensor, t: float = 0.0, w: torch.Tensor | None = None) -> torch.Tensor:
         w = self.new_primitive() if w is None else w

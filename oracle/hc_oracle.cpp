@@ -1169,6 +1169,26 @@ int orc_box_rhs_o4(void* L, const hc_box* box, const double* usph, double scale,
   o4BoxOperator(*static_cast<Level*>(L), box->lo, box->hi, box->ghost, box->block, usph, scale, rhs, flux);
   return 0;
 }
+void* orc_o4_level_create(void* L) { return new O4Level(*static_cast<Level*>(L)); }
+void orc_o4_level_destroy(void* O) { delete static_cast<O4Level*>(O); }
+int orc_o4_prepare(void* O, const double* ju, double* us, double t) { o4Prepare(*static_cast<O4Level*>(O), ju, us, t); return 0; }
+int orc_o4_cartesian(void* O, const double* ju, double* cart) {
+  const O4Level& o = *static_cast<O4Level*>(O);
+  std::fill(cart, cart + (size_t)6 * 8 * o.Nc, 0.0);
+  o4Cartesian(o, ju, cart);
+  o4Seams(o, cart);
+  return 0;
+}
+int orc_o4_seams(void* O, double* cart) { o4Seams(*static_cast<O4Level*>(O), cart); return 0; }
+long orc_o4_sizes(void* O, long* out) {
+  const O4Level& o = *static_cast<O4Level*>(O);
+  out[0] = (long)o.Nv; out[1] = (long)o.Ng; out[2] = (long)o.Nc; out[3] = o.g; out[4] = o.ga;
+  return 0;
+}
+int orc_o4_rhs(void* O, const double* us, double* k, double* reg, double weight) { o4Rhs(*static_cast<O4Level*>(O), us, k, reg, weight); return 0; }
+int orc_o4_reflux(void* O, const double* reg, double* ju) { o4Reflux(*static_cast<O4Level*>(O), reg, ju); return 0; }
+int orc_o4_rk4_step(void* O, double* ju, double dt, double t) { o4Rk4(*static_cast<O4Level*>(O), ju, dt, t); return 0; }
+double orc_o4_inv_dt(void* O, const double* ju) { return o4InvDt(*static_cast<O4Level*>(O), ju); }
 int orc_box_gravity(void* L, const hc_box* box, const double* w, double* rhs) {
   boxGravity(*static_cast<Level*>(L), box->lo, box->hi, box->ghost, box->block, w, rhs);
   return 0;

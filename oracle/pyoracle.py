@@ -83,6 +83,18 @@ def lib() -> C.CDLL:
         L.orc_face_flux.argtypes = [_D, _D, _D, C.c_double, C.c_double, C.c_double, C.c_int, _D]
         L.orc_plm.argtypes = [_D, _D, _D, _D, C.c_int, _D, _D]
         L.orc_cart_prim.argtypes = [_D, C.c_double, C.c_double, _D]
+        L.orc_o4_level_create.restype = C.c_void_p
+        L.orc_o4_level_create.argtypes = [C.c_void_p]
+        L.orc_o4_level_destroy.argtypes = [C.c_void_p]
+        L.orc_o4_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_long)]
+        L.orc_o4_prepare.argtypes = [C.c_void_p, _D, _D, C.c_double]
+        L.orc_o4_cartesian.argtypes = [C.c_void_p, _D, _D]
+        L.orc_o4_seams.argtypes = [C.c_void_p, _D]
+        L.orc_o4_rhs.argtypes = [C.c_void_p, _D, _D, _D, C.c_double]
+        L.orc_o4_reflux.argtypes = [C.c_void_p, _D, _D]
+        L.orc_o4_rk4_step.argtypes = [C.c_void_p, _D, C.c_double, C.c_double]
+        L.orc_o4_inv_dt.restype = C.c_double
+        L.orc_o4_inv_dt.argtypes = [C.c_void_p, _D]
         _orc = L
     return _orc
 
@@ -193,3 +205,57 @@ class OracleLevel:
 
     def box_gravity(self, box: HcBox, w: np.ndarray, rhs: np.ndarray):
         self.L.orc_box_gravity(self.h, C.byref(box), dptr(w), dptr(rhs))
+
+
+class OracleLevelO4:
+    """The fourth-order level step of the oracle: stage preparation (Cartesian
+    conversion, seam ghosts, native conversion, radial ghosts), the per-panel
+    operator with the seam flux register, RK4 and the CFL rate."""
+
+    def __init__(self, params: HcParams):
+        self.base = OracleLevel(params)
+        self.L = self.base.L
+        self.h = self.L.orc_o4_level_create(self.base.h)
+        sz = (C.c_long * 5)()
+        self.L.orc_o4_sizes(self.h, sz)
+        self.nv, self.ng, self.nc, self.g, self.ga = (int(x) for x in sz)
+        self.nr, self.na = params.nr, params.na
+
+    def __del__(self):
+        try:
+            self.L.orc_o4_level_destroy(self.h)
+        except Exception:
+            pass
+
+    def init(self, init: HcInit) -> np.ndarray:
+        return self.base.init(init)
+
+    def prepare(self, ju: np.ndarray, t: float = 0.0) -> np.ndarray:
+        us = np.zeros(6 * 8 * self.ng)
+        self.L.orc_o4_prepare(self.h, dptr(ju), dptr(us), t)
+        return us
+
+    def cartesian(self, ju: np.ndarray) -> np.ndarray:
+        cart = np.zeros(6 * 8 * self.nc)
+        self.L.orc_o4_cartesian(self.h, dptr(ju), dptr(cart))
+        return cart
+
+    def seams(self, cart: np.ndarray) -> None:
+        self.L.orc_o4_seams(self.h, dptr(cart))
+
+    def rhs(self, us: np.ndarray, reg: np.ndarray | None = None, weight: float = 1.0) -> np.ndarray:
+        k = np.zeros(6 * 8 * self.nv)
+        self.L.orc_o4_rhs(self.h, dptr(us), dptr(k), dptr(reg) if reg is not None else None, weight)
+        return k
+
+    def register(self) -> np.ndarray:
+        return np.zeros(6 * 2 * 2 * 8 * self.na * self.nr)
+
+    def reflux(self, reg: np.ndarray, ju: np.ndarray) -> None:
+        self.L.orc_o4_reflux(self.h, dptr(reg), dptr(ju))
+
+    def rk4_step(self, ju: np.ndarray, dt: float, t: float = 0.0) -> None:
+        self.L.orc_o4_rk4_step(self.h, dptr(ju), dt, t)
+
+    def inv_dt(self, ju: np.ndarray) -> float:
+        return self.L.orc_o4_inv_dt(self.h, dptr(ju))

@@ -46,7 +46,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if src.endswith(".cu") and verbose:
                 cmd += ["-Xptxas", "-v"]
             if src.endswith(".cpp"):
-                cmd = [NVCC, *COMMON, "-x", "c++", "-c", path, "-o", obj]
+                cmd = [NVCC, *ARCH, *COMMON, "-x", "c++", "-c", path, "-o", obj]
             subprocess.run(cmd, check=True)
     if force or _stale(LIB, objs):
         subprocess.run([NVCC, *ARCH, "-shared", "--cudart", "static", *objs, "-o", LIB], check=True)

@@ -162,9 +162,11 @@ HC_DEV bool roeRightNonzero(int r, int k) {
 // src/MHD_Roe8Wave.H:16-600: D = |A|(U_R - U_L) with arithmetic averages,
 // eight-wave entropy fix and (CHECK) the intermediate-state fan walk.
 // Returns false where the reference requests the Rusanov fallback.
+// roe8Body is inlined where the caller has registers to spare;
+// roe8WaveDissipation is its out-of-line form.
 template <bool CHECK>
-__device__ __noinline__ bool roe8WaveDissipation(double out[8], const double* wl, const double* wr, double gamma,
-                                                 double del2, double invHg) {
+__device__ __forceinline__ bool roe8Body(double out[8], const double* wl, const double* wr, double gamma, double del2,
+                                         double invHg) {
   const double RhoL = wl[0], UL = wl[1], VL = wl[2], WL = wl[3], PGasL = wl[4], BXL = wl[5], BYL = wl[6], BZL = wl[7];
   const double RhoR = wr[0], UR = wr[1], VR = wr[2], WR = wr[3], PGasR = wr[4], BXR = wr[5], BYR = wr[6], BZR = wr[7];
   if (!(RhoL > 0.0 && RhoR > 0.0 && PGasL > 0.0 && PGasR > 0.0)) return false;
@@ -299,6 +301,12 @@ __device__ __noinline__ bool roe8WaveDissipation(double out[8], const double* wl
 #pragma unroll
   for (int q = 0; q < 8; ++q) ok = ok && isfinite(out[q]);
   return ok;
+}
+
+template <bool CHECK>
+__device__ __noinline__ bool roe8WaveDissipation(double out[8], const double* wl, const double* wr, double gamma,
+                                                 double del2, double invHg) {
+  return roe8Body<CHECK>(out, wl, wr, gamma, del2, invHg);
 }
 
 // src/MHD_SecondOrderFlux.H:34-74: local-frame MHD flux of both states,

@@ -97,8 +97,11 @@ __device__ __forceinline__ double radialPoint(const O4Geo& g, int d, int i) {
 }
 
 // ---- pointwise pieces -----------------------------------------------------
+// Divisions by 4 pi and 8 pi are multiplications by the rounded reciprocals
+// (a one-ulp difference from the reference's x / 8.0 / M_PI).
+constexpr double kInv4Pi = 0.25 / kPi, kInv8Pi = 0.125 / kPi;
 // f_sphToPrim + energies + pressure (src/BoxOp_BertaCubedSphereImplem.H:212-340)
-__device__ void sphToPrim(const double u[8], const double* A, double gamma, double w[8]) {
+__device__ __forceinline__ void sphToPrim(const double u[8], const double* A, double gamma, double w[8]) {
   w[0] = dmax(u[0], kRHO00);
   w[1] = u[1] / w[0];
   w[2] = u[2] / w[0];
@@ -111,7 +114,7 @@ __device__ void sphToPrim(const double u[8], const double* A, double gamma, doub
     const double vc = A[3 * d0] * w[1] + A[3 * d0 + 1] * w[2] + A[3 * d0 + 2] * w[3];
     const double bc = A[3 * d0] * w[5] + A[3 * d0 + 1] * w[6] + A[3 * d0 + 2] * w[7];
     ke += vc * vc / 2;
-    me += bc * bc / 8.0 / kPi;
+    me += bc * bc * kInv8Pi;
   }
   ke *= w[0];
   w[4] = (w[4] - ke - me) * (gamma - 1.0);
@@ -119,29 +122,29 @@ __device__ void sphToPrim(const double u[8], const double* A, double gamma, doub
 }
 
 // EnergyW (src/BoxOp_Utilities.H:447-520)
-__device__ void energyW(const double w[8], const double* A, double& ke, double& me, double& vb) {
+__device__ __forceinline__ void energyW(const double w[8], const double* A, double& ke, double& me, double& vb) {
   ke = 0.; me = 0.; vb = 0.;
 #pragma unroll
   for (int d0 = 0; d0 < 3; ++d0) {
     const double vc = A[3 * d0] * w[1] + A[3 * d0 + 1] * w[2] + A[3 * d0 + 2] * w[3];
     const double bc = A[3 * d0] * w[5] + A[3 * d0 + 1] * w[6] + A[3 * d0 + 2] * w[7];
     ke += vc * vc;
-    me += bc * bc / 8.0 / kPi;
+    me += bc * bc * kInv8Pi;
     vb += vc * bc;
   }
   ke *= w[0] * .5;
 }
 
 // f_primflux (src/BoxOp_EulerCubedSphere.H:195-225)
-__device__ void primFlux(double f[8], const double w[8], double ke, double me, double vb, double gamma, int c) {
+__device__ __forceinline__ void primFlux(double f[8], const double w[8], double ke, double me, double vb, double gamma, int c) {
   const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
   const double velnorm = w[c + 1], veltan1 = w[c1 + 1], veltan2 = w[c2 + 1];
   const double bnorm = w[c + 5], btan1 = w[c1 + 5], btan2 = w[c2 + 5];
   f[0] = w[0] * velnorm;
-  f[c + 1] = f[0] * velnorm - bnorm * bnorm / 4.0 / kPi;
-  f[c1 + 1] = f[0] * veltan1 - bnorm * btan1 / 4.0 / kPi;
-  f[c2 + 1] = f[0] * veltan2 - bnorm * btan2 / 4.0 / kPi;
-  f[4] = (2.0 * me + ke + w[4] * gamma / (gamma - 1.0)) * velnorm - bnorm * vb / 4.0 / kPi;
+  f[c + 1] = f[0] * velnorm - bnorm * bnorm * kInv4Pi;
+  f[c1 + 1] = f[0] * veltan1 - bnorm * btan1 * kInv4Pi;
+  f[c2 + 1] = f[0] * veltan2 - bnorm * btan2 * kInv4Pi;
+  f[4] = (2.0 * me + ke + w[4] * gamma / (gamma - 1.0)) * velnorm - bnorm * vb * kInv4Pi;
   f[5] = velnorm * w[5] - w[1] * bnorm;
   f[6] = velnorm * w[6] - w[2] * bnorm;
   f[7] = velnorm * w[7] - w[3] * bnorm;
@@ -149,7 +152,7 @@ __device__ void primFlux(double f[8], const double w[8], double ke, double me, d
 
 // bertaNormalizeWenoStencil (:747-773)
 template <int N>
-__device__ double normalizeStencil(double (&v)[N]) {
+__device__ __forceinline__ double normalizeStencil(double (&v)[N]) {
   double scale = 0.0;
 #pragma unroll
   for (int i = 0; i < N; ++i) scale = dmax(scale, fabs(v[i]));
@@ -169,11 +172,13 @@ __device__ double normalizeStencil(double (&v)[N]) {
   return scale;
 }
 
-__device__ void wenozSide(double m2, double m1, double c0, double p1, double p2, double& out) {
+__device__ __forceinline__ void wenozSide(double m2, double m1, double c0, double p1, double p2, double& out) {
+  // a_k = d_k (1 + tau / D_k), D_k = beta_k + eps; out = sum a_k q_k / sum a_k
+  // evaluated with one division: a_k prop. to d_k (D_k + tau) prod_{j != k} D_j.
   const double eps = 1.0e-40, d0 = 1.0 / 16.0, d1 = 5.0 / 8.0, d2 = 5.0 / 16.0;
-  const double q0 = (3.0 * m2 - 10.0 * m1 + 15.0 * c0) / 8.0;
-  const double q1 = (-m1 + 6.0 * c0 + 3.0 * p1) / 8.0;
-  const double q2 = (3.0 * c0 + 6.0 * p1 - p2) / 8.0;
+  const double q0 = (3.0 * m2 - 10.0 * m1 + 15.0 * c0) * 0.125;
+  const double q1 = (-m1 + 6.0 * c0 + 3.0 * p1) * 0.125;
+  const double q2 = (3.0 * c0 + 6.0 * p1 - p2) * 0.125;
   const double b0a = m2 - 2.0 * m1 + c0, b0b = m2 - 4.0 * m1 + 3.0 * c0;
   const double b1a = m1 - 2.0 * c0 + p1, b1b = m1 - p1;
   const double b2a = c0 - 2.0 * p1 + p2, b2b = 3.0 * c0 - 4.0 * p1 + p2;
@@ -181,15 +186,15 @@ __device__ void wenozSide(double m2, double m1, double c0, double p1, double p2,
   const double beta1 = (13.0 / 12.0) * b1a * b1a + 0.25 * b1b * b1b;
   const double beta2 = (13.0 / 12.0) * b2a * b2a + 0.25 * b2b * b2b;
   const double tau5 = fabs(beta0 - beta2);
-  const double a0 = d0 * (1.0 + tau5 / (beta0 + eps));
-  const double a1 = d1 * (1.0 + tau5 / (beta1 + eps));
-  const double a2 = d2 * (1.0 + tau5 / (beta2 + eps));
-  const double asum = a0 + a1 + a2;
-  out = (a0 * q0 + a1 * q1 + a2 * q2) / asum;
+  const double D0 = beta0 + eps, D1 = beta1 + eps, D2 = beta2 + eps;
+  const double w0 = d0 * (D0 + tau5) * (D1 * D2);
+  const double w1 = d1 * (D1 + tau5) * (D0 * D2);
+  const double w2 = d2 * (D2 + tau5) * (D0 * D1);
+  out = (w0 * q0 + w1 * q1 + w2 * q2) / (w0 + w1 + w2);
 }
 
 // f_wenoz_pointwise_faceF (:782-878), one component, cells W[i-3..i+2].
-__device__ void wenozFace(const double in[6], double& L, double& R) {
+__device__ __forceinline__ void wenozFace(const double in[6], double& L, double& R) {
   double v[6] = {in[0], in[1], in[2], in[3], in[4], in[5]};
   const double scale = normalizeStencil(v);
   if (scale == 0.0) { L = R = 0.0; return; }
@@ -201,7 +206,8 @@ __device__ void wenozFace(const double in[6], double& L, double& R) {
 }
 
 // f_weno3_pointwise_faceF (:881-946), one component, cells W[i-2..i+1].
-__device__ void weno3Face(const double in[4], double dx2, double& L, double& R) {
+__device__ __forceinline__ void weno3Face(const double in[4], double dx2, double& L, double& R) {
+  // a_k = d_k (1 + tau / (beta_k + eps)) with one division per side, as in wenozSide.
   const double d0 = 3.0 / 4.0, d1 = 1.0 / 4.0, eps = dx2;
   double v[4] = {in[0], in[1], in[2], in[3]};
   const double scale = normalizeStencil(v);
@@ -209,29 +215,29 @@ __device__ void weno3Face(const double in[4], double dx2, double& L, double& R) 
   {
     const double vm1 = v[0], v0 = v[1], vp1 = v[2];
     const double Dm = v0 - vm1, Dp = vp1 - v0;
-    const double beta0 = Dp * Dp, beta1 = Dm * Dm, tau = (Dp - Dm) * (Dp - Dm);
-    const double a0 = d0 * (1.0 + tau / (beta0 + eps)), a1 = d1 * (1.0 + tau / (beta1 + eps));
+    const double tau = (Dp - Dm) * (Dp - Dm), B0 = Dp * Dp + eps, B1 = Dm * Dm + eps;
+    const double w0 = d0 * (B0 + tau) * B1, w1 = d1 * (B1 + tau) * B0;
     const double q0 = 0.5 * (vp1 + v0), q1 = 0.5 * (-vm1 + 3.0 * v0);
-    L = scale * ((a0 * q0 + a1 * q1) / (a0 + a1));
+    L = scale * ((w0 * q0 + w1 * q1) / (w0 + w1));
   }
   {
     const double rm1 = v[3], r0 = v[2], rp1 = v[1];
     const double Dm = r0 - rm1, Dp = rp1 - r0;
-    const double beta0 = Dp * Dp, beta1 = Dm * Dm, tau = (Dp - Dm) * (Dp - Dm);
-    const double a0 = d0 * (1.0 + tau / (beta0 + eps)), a1 = d1 * (1.0 + tau / (beta1 + eps));
+    const double tau = (Dp - Dm) * (Dp - Dm), B0 = Dp * Dp + eps, B1 = Dm * Dm + eps;
+    const double w0 = d0 * (B0 + tau) * B1, w1 = d1 * (B1 + tau) * B0;
     const double q0 = 0.5 * (rp1 + r0), q1 = 0.5 * (-rm1 + 3.0 * r0);
-    R = scale * ((a0 * q0 + a1 * q1) / (a0 + a1));
+    R = scale * ((w0 * q0 + w1 * q1) / (w0 + w1));
   }
 }
 
-__device__ double minmod3(double a, double b, double c) {
+__device__ __forceinline__ double minmod3(double a, double b, double c) {
   if (a > 0.0 && b > 0.0 && c > 0.0) return dmin(a, dmin(b, c));
   if (a < 0.0 && b < 0.0 && c < 0.0) return dmax(a, dmax(b, c));
   return 0.0;
 }
 
 // f_plm_pointwise_faceF (:949-991), one component, cells W[i-2..i+1].
-__device__ void plmFallbackFace(const double in[4], double& L, double& R) {
+__device__ __forceinline__ void plmFallbackFace(const double in[4], double& L, double& R) {
   const double theta = 1.5;
   const double dm = in[1] - in[0], dp = in[2] - in[1], dc = 0.5 * (in[2] - in[0]);
   L = in[1] + 0.5 * minmod3(theta * dm, dc, theta * dp);
@@ -239,7 +245,7 @@ __device__ void plmFallbackFace(const double in[4], double& L, double& R) {
   R = in[2] - 0.5 * minmod3(theta * rdm, rdc, theta * rdp);
 }
 
-__device__ bool usablePrimitive(const double w[8]) {
+__device__ __forceinline__ bool usablePrimitive(const double w[8]) {
   bool ok = true;
 #pragma unroll
   for (int c = 0; c < 8; ++c) ok = ok && isfinite(w[c]);
@@ -247,7 +253,7 @@ __device__ bool usablePrimitive(const double w[8]) {
 }
 
 // mappedRoe8WaveDissipation + factoredRoe8WaveDissipation (src/MHD_Roe8Wave.H:634-740)
-__device__ void factoredRoe(double out[8], const double* wl, const double* wr, const double* A, double radialArea,
+__device__ __forceinline__ void factoredRoe(double out[8], const double* wl, const double* wr, const double* A, double radialArea,
                             int dir, double gamma, double invGm1, double entropy) {
   const int t1 = (dir + 1) % 3, t2 = (dir + 2) % 3;
   double f0[3], f1[3], f2[3], normal2 = 0.0, tangent2 = 0.0;
@@ -260,8 +266,9 @@ __device__ void factoredRoe(double out[8], const double* wl, const double* wr, c
     tangent2 += f1[i] * f1[i];
   }
   const double normalMag = sqrt(normal2), tangentMag = sqrt(tangent2);
+  const double invN = 1.0 / normalMag, invT = 1.0 / tangentMag;
 #pragma unroll
-  for (int i = 0; i < 3; ++i) { f0[i] /= normalMag; f1[i] /= tangentMag; }
+  for (int i = 0; i < 3; ++i) { f0[i] *= invN; f1[i] *= invT; }
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     const int j = (i + 1) % 3, k = (i + 2) % 3;
@@ -287,7 +294,7 @@ __device__ void factoredRoe(double out[8], const double* wl, const double* wr, c
     loc[side][7] = f2[0] * bC[0] + f2[1] * bC[1] + f2[2] * bC[2];
   }
   double diss[8];
-  if (!roe8WaveDissipation<true>(diss, loc[0], loc[1], gamma, entropy, invGm1))
+  if (!roe8Body<true>(diss, loc[0], loc[1], gamma, entropy, invGm1))
     rusanovDissipation(diss, loc[0], loc[1], gamma, invGm1);
   const double area = radialArea * normalMag;
   double mapped[8];
@@ -309,13 +316,13 @@ __device__ void factoredRoe(double out[8], const double* wl, const double* wr, c
     }
   }
   const double det = A[0] * adj[0][0] + A[3] * adj[0][1] + A[6] * adj[0][2];
-  out[0] = mapped[0] / det;
-  out[4] = mapped[4] / det;
-  const double det2 = det * det;
+  const double invDet = 1.0 / det, invDet2 = 1.0 / (det * det);
+  out[0] = mapped[0] * invDet;
+  out[4] = mapped[4] * invDet;
 #pragma unroll
   for (int dd = 0; dd < 3; ++dd) {
-    out[1 + dd] = adj[dd][0] * mapped[1] / det2 + adj[dd][1] * mapped[2] / det2 + adj[dd][2] * mapped[3] / det2;
-    out[5 + dd] = adj[dd][0] * mapped[5] / det2 + adj[dd][1] * mapped[6] / det2 + adj[dd][2] * mapped[7] / det2;
+    out[1 + dd] = (adj[dd][0] * mapped[1] + adj[dd][1] * mapped[2] + adj[dd][2] * mapped[3]) * invDet2;
+    out[5 + dd] = (adj[dd][0] * mapped[5] + adj[dd][1] * mapped[6] + adj[dd][2] * mapped[7]) * invDet2;
   }
 }
 
@@ -327,7 +334,7 @@ struct View {
 };
 
 
-__device__ double lapFace(const View& f, int c, int d, int i, int j, int k) {
+__device__ __forceinline__ double lapFace(const View& f, int c, int d, int i, int j, int k) {
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
   int a[3] = {i, j, k}, b[3] = {i, j, k}, e[3] = {i, j, k}, g[3] = {i, j, k};
   a[t1] -= 1; b[t1] += 1; e[t2] -= 1; g[t2] += 1;
@@ -335,13 +342,13 @@ __device__ double lapFace(const View& f, int c, int d, int i, int j, int k) {
          4.0 * f(c, i, j, k);
 }
 
-__device__ double cdiff(const View& f, int c, int t, int i, int j, int k) {
+__device__ __forceinline__ double cdiff(const View& f, int c, int t, int i, int j, int k) {
   int a[3] = {i, j, k}, b[3] = {i, j, k};
   a[t] += 1; b[t] -= 1;
   return 0.5 * f(c, a[0], a[1], a[2]) - 0.5 * f(c, b[0], b[1], b[2]);
 }
 
-__device__ double lapCell(const View& f, int c, int i, int j, int k) {
+__device__ __forceinline__ double lapCell(const View& f, int c, int i, int j, int k) {
   return (f(c, i - 1, j, k) + f(c, i + 1, j, k)) + (f(c, i, j - 1, k) + f(c, i, j + 1, k)) +
          (f(c, i, j, k - 1) + f(c, i, j, k + 1)) - 6.0 * f(c, i, j, k);
 }
@@ -442,7 +449,7 @@ __global__ void o4PointKernel(const Ctx c) {
     View U{a.U + b * a.uStride, a.ur};
     double u[8], w[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) u[q] = (inner && t > 0.5) ? U(q, i, j, k) - lapCell(U, q, i, j, k) / 24.0 : U(q, i, j, k);
+    for (int q = 0; q < 8; ++q) u[q] = (inner && t > 0.5) ? U(q, i, j, k) - lapCell(U, q, i, j, k) * (1.0 / 24.0) : U(q, i, j, k);
     sphToPrim(u, cellBasis(a.G, a.block0 + b, j, k), a.G.gamma, w);
     double* W = a.WP + (long)b * 8 * N + o;
 #pragma unroll
@@ -454,15 +461,17 @@ __device__ __forceinline__ double* faceArr(const Ctx& c, int b, int arr) {
   return c.a.face + ((long)b * kO4FaceArrays + arr) * c.fr.N;
 }
 __device__ __forceinline__ View faceView(const Ctx& c, int b, int arr) { return View{faceArr(c, b, arr), c.fr}; }
+template <int D>
 __device__ __forceinline__ const double* faceBasis(const Ctx& c, int b, int j, int k) {
-  return c.d == 0 ? cellBasis(c.a.G, c.a.block0 + b, j, k) : faceRec(c.a.G, c.a.block0 + b, c.d, j, k) + 13;
+  return D == 0 ? cellBasis(c.a.G, c.a.block0 + b, j, k) : faceRec(c.a.G, c.a.block0 + b, D, j, k) + 13;
 }
 
 // 4. reconstruction (WENOZ / WENO3 / PLM with clamps), Roe repair, energies,
 // point flux sum, total-pressure sum, centred normal B, Rusanov jump (F).
+template <int D>
 __global__ void o4FaceReconKernel(const Ctx c) {
   const O4Args& a = c.a;
-  const int d = c.d;
+  constexpr int d = D;
   const double dx2 = a.G.dx[d] * a.G.dx[d];
   forRegion(c.F, a.nbox, [&](int b, int i, int j, int k) {
     const long NG = c.gr.N, NF = c.fr.N;
@@ -517,7 +526,7 @@ __global__ void o4FaceReconKernel(const Ctx c) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) { base[(F_WL + q) * NF] = l[q]; base[(F_WR + q) * NF] = r[q]; }
     base[F_THF * NF] = thF;
-    const double* A = faceBasis(c, b, j, k);
+    const double* A = faceBasis<D>(c, b, j, k);
     double kl, ml, vl, kr, mr, vr, fl[8], fr[8];
     energyW(l, A, kl, ml, vl);
     energyW(r, A, kr, mr, vr);
@@ -543,9 +552,10 @@ __global__ void o4FaceReconKernel(const Ctx c) {
 
 // 4b. pointwise factored Roe dissipation on the final faces + one transverse
 // ring (src/BoxOp_RoeCubedSphere.H:73-98).
+template <int D>
 __global__ void o4RoePointKernel(const Ctx c) {
   const O4Args& a = c.a;
-  const int d = c.d;
+  constexpr int d = D;
   const Box3 PB = c.V0.growTrans(d, 1);
   forRegion(PB, a.nbox, [&](int b, int i, int j, int k) {
     const long NF = c.fr.N;
@@ -553,16 +563,17 @@ __global__ void o4RoePointKernel(const Ctx c) {
     double l[8], r[8], o[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) { l[q] = base[(F_WL + q) * NF]; r[q] = base[(F_WR + q) * NF]; }
-    factoredRoe(o, l, r, faceBasis(c, b, j, k), radialPoint(a.G, d, i), d, a.G.gamma, a.G.invGm1, a.G.entropy);
+    factoredRoe(o, l, r, faceBasis<D>(c, b, j, k), radialPoint(a.G, d, i), d, a.G.gamma, a.G.invGm1, a.G.entropy);
 #pragma unroll
     for (int q = 0; q < 8; ++q) base[(F_QD + q) * NF] = o[q];
   });
 }
 
 // 5. theta-aware point-to-average of the flux sum and total pressure (F1).
+template <int D>
 __global__ void o4FaceAvgKernel(const Ctx c) {
   const O4Args& a = c.a;
-  const int d = c.d;
+  constexpr int d = D;
   forRegion(c.F1, a.nbox, [&](int b, int i, int j, int k) {
     const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
     double* base = a.face + (long)b * kO4FaceArrays * NF;
@@ -571,19 +582,20 @@ __global__ void o4FaceAvgKernel(const Ctx c) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const double pt = FS(q, i, j, k);
-      base[(F_FA + q) * NF + fo] = sm ? pt + lapFace(FS, q, d, i, j, k) / 24.0 : pt;
+      base[(F_FA + q) * NF + fo] = sm ? pt + lapFace(FS, q, d, i, j, k) * (1.0 / 24.0) : pt;
     }
     const View PS = faceView(c, b, F_PS);
     const double pp = PS(0, i, j, k);
-    base[F_PA * NF + fo] = sm ? pp + lapFace(PS, 0, d, i, j, k) / 24.0 : pp;
+    base[F_PA * NF + fo] = sm ? pp + lapFace(PS, 0, d, i, j, k) * (1.0 / 24.0) : pp;
   });
 }
 
 // 6. mapped flux with separable metrics (bertaMapHostBox, :35-95 and
 // :1361-1450) on F1; zero on F outside it.
+template <int D>
 __global__ void o4FaceMapKernel(const Ctx c) {
   const O4Args& a = c.a;
-  const int d = c.d;
+  constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
   const bool skipFirst = t1 == 0;
   forRegion(c.F, a.nbox, [&](int b, int i, int j, int k) {
@@ -651,9 +663,10 @@ __global__ void o4FaceMapKernel(const Ctx c) {
 }
 
 // 7. radial-area face products of the mapped flux and of <p_tot> (F1).
+template <int D>
 __global__ void o4FaceRadialKernel(const Ctx c) {
   const O4Args& a = c.a;
-  const int d = c.d;
+  constexpr int d = D;
   forRegion(c.F1, a.nbox, [&](int b, int i, int j, int k) {
     const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
     double* base = a.face + (long)b * kO4FaceArrays * NF;
@@ -677,9 +690,10 @@ __global__ void o4FaceRadialKernel(const Ctx c) {
 
 // 8. pressure force, dissipation, combine on the final faces V0; writes the
 // flux (scratch and caller).
+template <int D>
 __global__ void o4FaceFinalKernel(const Ctx c) {
   const O4Args& a = c.a;
-  const int d = c.d;
+  constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
   const int tr[2] = {t1, t2};
   forRegion(c.V0, a.nbox, [&](int b, int i, int j, int k) {
@@ -726,7 +740,7 @@ __global__ void o4FaceFinalKernel(const Ctx c) {
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const double pt = QD(q, i, j, k);
-        avg[q] = sm ? pt + lapFace(QD, q, d, i, j, k) / 24.0 : pt;
+        avg[q] = sm ? pt + lapFace(QD, q, d, i, j, k) * (1.0 / 24.0) : pt;
         dP0[q] = cdiff(QD, q, t1, i, j, k);
         dP1[q] = cdiff(QD, q, t2, i, j, k);
       }
@@ -750,7 +764,7 @@ __global__ void o4FaceFinalKernel(const Ctx c) {
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const double pt = QD(q, i, j, k);
-        qv[q] = sm ? pt + lapFace(QD, q, d, i, j, k) / 24.0 : pt;
+        qv[q] = sm ? pt + lapFace(QD, q, d, i, j, k) * (1.0 / 24.0) : pt;
       }
 #pragma unroll
       for (int bb = 0; bb < 2; ++bb) {
@@ -765,7 +779,7 @@ __global__ void o4FaceFinalKernel(const Ctx c) {
       double l[8], r[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) { l[q] = base[(F_WL + q) * NF + fo]; r[q] = base[(F_WR + q) * NF + fo]; }
-      const double* A = faceBasis(c, b, j, k);
+      const double* A = faceBasis<D>(c, b, j, k);
       double rho = 0.5 * (l[0] + r[0]);
       const double w_d = 0.5 * (l[1 + d] + r[1 + d]);
       const double bs3[3] = {0.5 * (l[5] + r[5]), 0.5 * (l[6] + r[6]), 0.5 * (l[7] + r[7])};
@@ -818,9 +832,10 @@ __global__ void o4FaceFinalKernel(const Ctx c) {
 }
 
 // 9. flux divergence into rhs (V).
+template <int D>
 __global__ void o4DivKernel(const Ctx c) {
   const O4Args& a = c.a;
-  const int d = c.d;
+  constexpr int d = D;
   const double coef = -a.scale / a.G.dx[d];
   forRegion(c.V, a.nbox, [&](int b, int i, int j, int k) {
     const View FX = faceView(c, b, F_FX);
@@ -833,9 +848,10 @@ __global__ void o4DivKernel(const Ctx c) {
 }
 
 // 10. Powell face flux (DivBPowell1, src/BoxOp_DivBcleaning.H:35-74).
+template <int D>
 __global__ void o4PowellFluxKernel(const Ctx c) {
   const O4Args& a = c.a;
-  const int d = c.d;
+  constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
   const int tr[2] = {t1, t2};
   const Box3 BF = c.V1.extrude(d).growTrans(d, 1);
@@ -871,9 +887,10 @@ __global__ void o4PowellFluxKernel(const Ctx c) {
 }
 
 // 11. Powell radial-area product and divergence into -J div B (V+1).
+template <int D>
 __global__ void o4PowellProdKernel(const Ctx c) {
   const O4Args& a = c.a;
-  const int d = c.d;
+  constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
   const int tr[2] = {t1, t2};
   const Box3 BP = c.V1.extrude(d);
@@ -892,9 +909,10 @@ __global__ void o4PowellProdKernel(const Ctx c) {
   });
 }
 
+template <int D>
 __global__ void o4PowellDivKernel(const Ctx c) {
   const O4Args& a = c.a;
-  const int d = c.d;
+  constexpr int d = D;
   const double coef = -1.0 / a.G.dx[d];
   forRegion(c.V1, a.nbox, [&](int b, int i, int j, int k) {
     const View BP = faceView(c, b, F_BPROD);
@@ -937,7 +955,7 @@ __global__ void o4PowellAvgKernel(const Ctx c) {
     const View KP{a.kp + (long)b * 16 * c.v2r.N, c.v2r};
     double* KA = a.kp + (long)b * 16 * c.v2r.N + 8 * c.v2r.N + roff(c.v2r, i, j, k);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) KA[q * c.v2r.N] = KP(q, i, j, k) + lapCell(KP, q, i, j, k) / 24.0;
+    for (int q = 0; q < 8; ++q) KA[q * c.v2r.N] = KP(q, i, j, k) + lapCell(KP, q, i, j, k) * (1.0 / 24.0);
   });
 }
 
@@ -984,6 +1002,10 @@ cudaError_t launchO4BoxOperator(const O4Args& a, cudaStream_t s) {
 #define HC_LAUNCH(kernel, ctx, region)                                                  \
   kernel<<<blocksFor((region).size() * nb), T, 0, s>>>(ctx);                           \
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+#define HC_LAUNCH_D(kernel, ctx, region)                                                \
+  if ((ctx).d == 0) { HC_LAUNCH(kernel<0>, ctx, region) }                              \
+  else if ((ctx).d == 1) { HC_LAUNCH(kernel<1>, ctx, region) }                         \
+  else { HC_LAUNCH(kernel<2>, ctx, region) }
   HC_LAUNCH(o4PrimAvgKernel, c0, c0.G)
   HC_LAUNCH(o4ThetaRawKernel, c0, c0.GR)
   HC_LAUNCH(o4PointKernel, c0, c0.G)
@@ -992,17 +1014,17 @@ cudaError_t launchO4BoxOperator(const O4Args& a, cudaStream_t s) {
   }
   for (int d = 0; d < 3; ++d) {
     Ctx c = makeCtx(a, d);
-    HC_LAUNCH(o4FaceReconKernel, c, c.F)
-    if (a.G.roe) { HC_LAUNCH(o4RoePointKernel, c, c.V0.growTrans(d, 1)) }
-    HC_LAUNCH(o4FaceAvgKernel, c, c.F1)
-    HC_LAUNCH(o4FaceMapKernel, c, c.F)
-    HC_LAUNCH(o4FaceRadialKernel, c, c.F1)
-    HC_LAUNCH(o4FaceFinalKernel, c, c.V0)
-    HC_LAUNCH(o4DivKernel, c, c.V)
+    HC_LAUNCH_D(o4FaceReconKernel, c, c.F)
+    if (a.G.roe) { HC_LAUNCH_D(o4RoePointKernel, c, c.V0.growTrans(d, 1)) }
+    HC_LAUNCH_D(o4FaceAvgKernel, c, c.F1)
+    HC_LAUNCH_D(o4FaceMapKernel, c, c.F)
+    HC_LAUNCH_D(o4FaceRadialKernel, c, c.F1)
+    HC_LAUNCH_D(o4FaceFinalKernel, c, c.V0)
+    HC_LAUNCH_D(o4DivKernel, c, c.V)
     if (a.G.powell) {
-      HC_LAUNCH(o4PowellFluxKernel, c, c.V1.extrude(d).growTrans(d, 1))
-      HC_LAUNCH(o4PowellProdKernel, c, c.V1.extrude(d))
-      HC_LAUNCH(o4PowellDivKernel, c, c.V1)
+      HC_LAUNCH_D(o4PowellFluxKernel, c, c.V1.extrude(d).growTrans(d, 1))
+      HC_LAUNCH_D(o4PowellProdKernel, c, c.V1.extrude(d))
+      HC_LAUNCH_D(o4PowellDivKernel, c, c.V1)
     }
   }
   if (a.G.powell) {
@@ -1010,6 +1032,7 @@ cudaError_t launchO4BoxOperator(const O4Args& a, cudaStream_t s) {
     HC_LAUNCH(o4PowellAvgKernel, c0, c0.V1)
     HC_LAUNCH(o4PowellApplyKernel, c0, c0.V)
   }
+#undef HC_LAUNCH_D
 #undef HC_LAUNCH
   return cudaSuccess;
 }

@@ -58,48 +58,54 @@ __global__ void o4CartesianKernel(const O4StageIO io) {
     const int j = (int)((r / O.nr) % O.na);
     const int k = (int)(r / ((long)O.nr * O.na));
     const int na = O.na;
-    const double det = detAt(O, b, j, k);
+    // Quotients use reciprocals of <det A> and dVolr (one rounding from the
+    // reference's divisions).
+    const double invDet = 1.0 / detAt(O, b, j, k);
     const double dd1 = 0.5 * (detAt(O, b, j + 1, k) - detAt(O, b, j - 1, k));
     const double dd2 = 0.5 * (detAt(O, b, j, k + 1) - detAt(O, b, j, k - 1));
     // CubedSphereShell::deriv3case at (j, k): undivided centred difference
     // inside the panel, second-order one-sided on its first and last cells;
-    // the three-cell windows it reads
+    // the three-cell windows it reads and their weights
     const int ja = j == 0 ? 0 : (j == na - 1 ? na - 3 : j - 1);
     const int ka = k == 0 ? 0 : (k == na - 1 ? na - 3 : k - 1);
-    double detJ[3], detK[3];
+    double wj[3], wk[3], wr[3];
+    auto weights = [](int x, int n, double w[3]) {
+      if (x == 0) { w[0] = -1.5; w[1] = 2.0; w[2] = -0.5; }
+      else if (x == n - 1) { w[0] = 0.5; w[1] = -2.0; w[2] = 1.5; }
+      else { w[0] = -0.5; w[1] = 0.0; w[2] = 0.5; }
+    };
+    weights(j, na, wj);
+    weights(k, na, wk);
+    weights(i, O.nr, wr);
+    double invJ[3], invK[3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-      detJ[q] = detAt(O, b, ja + q, k);
-      detK[q] = detAt(O, b, j, ka + q);
+      invJ[q] = 1.0 / detAt(O, b, ja + q, k);
+      invK[q] = 1.0 / detAt(O, b, j, ka + q);
     }
     // the radial window of deriv3case at i
     const int ia = i == 0 ? 0 : (i == O.nr - 1 ? O.nr - 3 : i - 1);
+    double invV[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) invV[q] = 1.0 / volAt(O, ia + q);
     const double dv = 0.5 * (volAt(O, i + 1) - volAt(O, i - 1));
+    const int slot = i - ia;
     for (int c = 0; c < 8; ++c) {
-      double ang[3];
+      double dq = 0.0, angI = 0.0;
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         const int ii = ia + q;
-        double qj[3], qk[3];
+        double d1 = 0.0, d2 = 0.0;
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-          qj[m] = io.ju[vIdx(O, b, c, ii, ja + m, k)] / detJ[m];
-          qk[m] = io.ju[vIdx(O, b, c, ii, j, ka + m)] / detK[m];
+          d1 += wj[m] * (io.ju[vIdx(O, b, c, ii, ja + m, k)] * invJ[m]);
+          d2 += wk[m] * (io.ju[vIdx(O, b, c, ii, j, ka + m)] * invK[m]);
         }
-        const double d1 = j == 0 ? 0.5 * (-3.0 * qj[0] + 4.0 * qj[1] - qj[2])
-                        : (j == na - 1 ? 0.5 * (3.0 * qj[2] - 4.0 * qj[1] + qj[0]) : 0.5 * (qj[2] - qj[0]));
-        const double d2 = k == 0 ? 0.5 * (-3.0 * qk[0] + 4.0 * qk[1] - qk[2])
-                        : (k == na - 1 ? 0.5 * (3.0 * qk[2] - 4.0 * qk[1] + qk[0]) : 0.5 * (qk[2] - qk[0]));
-        const double corr = d1 * dd1 + d2 * dd2;
-        ang[q] = (io.ju[vIdx(O, b, c, ii, j, k)] - corr / 12.0) / det;
+        const double ang = (io.ju[vIdx(O, b, c, ii, j, k)] - (d1 * dd1 + d2 * dd2) * (1.0 / 12.0)) * invDet;
+        dq += wr[q] * (ang * invV[q]);
+        if (q == slot) angI = ang;
       }
-      double rq[3];
-#pragma unroll
-      for (int q = 0; q < 3; ++q) rq[q] = ang[q] / volAt(O, ia + q);
-      const int slot = i - ia;
-      const double dq = i == 0 ? 0.5 * (-3.0 * rq[0] + 4.0 * rq[1] - rq[2])
-                      : (i == O.nr - 1 ? 0.5 * (3.0 * rq[2] - 4.0 * rq[1] + rq[0]) : 0.5 * (rq[2] - rq[0]));
-      io.cart[cIdx(O, b, c, i, j, k)] = (ang[slot] - dq * dv / 12.0) / volAt(O, i);
+      io.cart[cIdx(O, b, c, i, j, k)] = (angI - dq * dv * (1.0 / 12.0)) * invV[slot];
     }
   }
 }

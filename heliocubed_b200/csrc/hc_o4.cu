@@ -469,7 +469,7 @@ __device__ __forceinline__ const double* faceBasis(const Ctx& c, int b, int j, i
 // 4. reconstruction (WENOZ / WENO3 / PLM with clamps), Roe repair, energies,
 // point flux sum, total-pressure sum, centred normal B, Rusanov jump (F).
 template <int D>
-__global__ void o4FaceReconKernel(const Ctx c) {
+__global__ void __launch_bounds__(128, 5) o4FaceReconKernel(const Ctx c) {
   const O4Args& a = c.a;
   constexpr int d = D;
   const double dx2 = a.G.dx[d] * a.G.dx[d];
@@ -553,7 +553,7 @@ __global__ void o4FaceReconKernel(const Ctx c) {
 // 4b. pointwise factored Roe dissipation on the final faces + one transverse
 // ring (src/BoxOp_RoeCubedSphere.H:73-98).
 template <int D>
-__global__ void o4RoePointKernel(const Ctx c) {
+__global__ void __launch_bounds__(128, 3) o4RoePointKernel(const Ctx c) {
   const O4Args& a = c.a;
   constexpr int d = D;
   const Box3 PB = c.V0.growTrans(d, 1);
@@ -691,7 +691,7 @@ __global__ void o4FaceRadialKernel(const Ctx c) {
 // 8. pressure force, dissipation, combine on the final faces V0; writes the
 // flux (scratch and caller).
 template <int D>
-__global__ void o4FaceFinalKernel(const Ctx c) {
+__global__ void __launch_bounds__(128, 4) o4FaceFinalKernel(const Ctx c) {
   const O4Args& a = c.a;
   constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;

@@ -359,6 +359,60 @@ def run_b200(args, world, rank, local):
     shell.close()
 
 
+def run_serve(args, world, rank, local):
+    """Served ensemble (config-4 style, scaled: see --serve-* flags): the same
+    seeded requests through the continuous-batching server and through the
+    plain one-at-a-time path; aggregate cell-updates/s of each and p50/p99
+    time-to-solution (all requests arrive at t = 0)."""
+    import torch
+    from heliocubed_b200 import serve
+    torch.cuda.set_device(local)
+    reqs = serve.synthetic_requests(args.serve_requests, args.seed, None, args.serve_steps,
+                                    radial=(32, 48, 64), angular=(32, 48))
+    shells, states = {}, {}
+    for r in reqs:
+        shp = (r.nr, r.na, r.order)
+        if shp not in shells:
+            shells[shp] = serve.Shell(r.params(), device=local)
+        states[r.rid] = serve.initial_state(shells[shp], r)
+    server = serve.EnsembleServer(hbm_budget=args.serve_budget_gb * 1e9, max_inflight=args.serve_inflight,
+                                  chunk=10, device=local)
+    counts = {}
+    for r in reqs:
+        counts[(r.nr, r.na, r.order)] = counts.get((r.nr, r.na, r.order), 0) + 1
+    for shp, n in counts.items():
+        server.warm([r for r in reqs if (r.nr, r.na, r.order) == shp], per_shape=min(n, args.serve_inflight))
+    # warm the plain path's contexts with one step each
+    for shp, sh in shells.items():
+        rid = next(r.rid for r in reqs if (r.nr, r.na, r.order) == shp)
+        ju = torch.from_numpy(states[rid]).to(sh._dev)
+        sh.advance(ju, 1, torch.zeros(1, dtype=torch.float64, device=sh._dev))
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    plain = serve.run_plain(reqs, states, device=local, shells=shells)
+    batched = server.run(reqs, states)
+    clocks = sampler.stop()
+    same = all(np.array_equal(a.state, b.state) for a, b in
+               zip(sorted(plain, key=lambda r: r.rid), sorted(batched, key=lambda r: r.rid)))
+    sp, sb = serve.summarize(plain), serve.summarize(batched)
+    if rank == 0:
+        out = {"metric": "FP64 cell-updates/s on 1 B200, batched vs plain; ensemble p50/p99 latency",
+               "value": sb["cell_updates_per_s"] * world, "unit": UNIT, "n_gpus": world,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic",
+               "config": {"workload": "served ensemble of cone-cloud solves (scaled config 4)",
+                          "requests": len(reqs), "steps_per_request": args.serve_steps,
+                          "grids": "nr in {32,48,64} x na in {32,48}, 50/50 PLM-MC+Rusanov / WENOZ+Roe",
+                          "arrivals": "all at t=0 (closed loop)", "max_inflight": args.serve_inflight,
+                          "hbm_budget_gb": args.serve_budget_gb, "chunk_steps": 10},
+               "batched": sb, "plain": sp, "batched_over_plain": sb["cell_updates_per_s"] / sp["cell_updates_per_s"],
+               "identical_results": same, "clocks": clocks}
+        print(json.dumps(out), flush=True)
+    for sh in shells.values():
+        sh.close()
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -377,6 +431,11 @@ def main() -> int:
                     help="launch the step eagerly instead of replaying a captured CUDA graph")
     ap.add_argument("--cpu-max-steps", type=int, default=60)
     ap.add_argument("--ref-budget", type=float, default=20.0)
+    ap.add_argument("--serve", action="store_true", help="run the served-ensemble benchmark instead")
+    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-steps", type=int, default=40)
+    ap.add_argument("--serve-inflight", type=int, default=8)
+    ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     args = ap.parse_args()
     o4 = args.order == 4
     args.nr = args.nr or (64 if o4 else 32)
@@ -394,6 +453,8 @@ def main() -> int:
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.serve:
+            run_serve(args, world, rank, local)
         else:
             run_b200(args, world, rank, local)
     finally:

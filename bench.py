@@ -393,8 +393,9 @@ def run_serve(args, world, rank, local):
     plain = serve.run_plain(reqs, states, device=local, shells=shells)
     batched = server.run(reqs, states)
     clocks = sampler.stop()
-    same = all(np.array_equal(a.state, b.state) for a, b in
+    same = all(np.array_equal(a.state, b.state, equal_nan=True) for a, b in
                zip(sorted(plain, key=lambda r: r.rid), sorted(batched, key=lambda r: r.rid)))
+    finite = sum(int(np.isfinite(r.state).all()) for r in batched)
     sp, sb = serve.summarize(plain), serve.summarize(batched)
     if rank == 0:
         out = {"metric": "FP64 cell-updates/s on 1 B200, batched vs plain; ensemble p50/p99 latency",
@@ -407,7 +408,7 @@ def run_serve(args, world, rank, local):
                           "arrivals": "all at t=0 (closed loop)", "max_inflight": args.serve_inflight,
                           "hbm_budget_gb": args.serve_budget_gb, "chunk_steps": 10},
                "batched": sb, "plain": sp, "batched_over_plain": sb["cell_updates_per_s"] / sp["cell_updates_per_s"],
-               "identical_results": same, "clocks": clocks}
+               "identical_results": same, "finite_results": finite, "clocks": clocks}
         print(json.dumps(out), flush=True)
     for sh in shells.values():
         sh.close()

@@ -27,6 +27,7 @@ SIGNATURES = {
     "hc_box_rhs": (C.c_int, [_VP, _VP, _VP, _VP, C.c_double, _VP, _VP, _VP]),
     "hc_box_gravity": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "hc_box_rhs_o4": (C.c_int, [_VP, _VP, _VP, C.c_double, _VP, _VP, _VP]),
+    "hc_box_gravity_o4": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "hc_level_prepare": (C.c_int, [_VP, _VP, _VP, C.c_double, _VP]),
     "hc_level_rhs": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hc_level_rk4_step": (C.c_int, [_VP, _VP, C.c_double, C.c_double, _VP]),

@@ -831,6 +831,10 @@ int o4Step(hc_ctx* c, double* ju, double dtv, const double* invMax, double tbase
     if (rc == HC_OK) rc = checkLaunch(cudaMemsetAsync(c->o4k, 0, sizeof(double) * 6 * 8 * O.Nv, s), "O4 k");
     if (rc != HC_OK) break;
     O4Args a = levelO4Args(c, c->o4us, c->o4k);
+    if (c->P.sun_gravity) {
+      rc = checkLaunch(launchO4Gravity(a, s), "O4 gravity");
+      if (rc != HC_OK) break;
+    }
     a.reg = c->o4reg;
     a.regWeight = invMax ? b4[stage] : dtv * b4[stage];
     a.regWeightDev = invMax;
@@ -981,6 +985,30 @@ int hc_box_rhs_o4(hc_ctx* c, const hc_box* box, const double* usph, double scale
   return checkLaunch(launchO4BoxOperator(a, (cudaStream_t)stream), "hc_box_rhs_o4");
 }
 
+int hc_box_gravity_o4(hc_ctx* c, const hc_box* box, const double* usph, double* rhs, void* stream) {
+  if (!c || !box || !usph || !rhs) return fail(HC_ERR_ARG, "null argument");
+  if (c->P.spatial_order != 4) return fail(HC_ERR_UNSUPPORTED, "context was created with spatial_order != 4");
+  const hc_box& B = *box;
+  if (B.block < 0 || B.block > 5) return fail(HC_ERR_ARG, "block must be 0..5");
+  if (B.ghost < 1) return fail(HC_ERR_ARG, "Gravity_Euler needs ghost >= 1");
+  const int n[3] = {c->P.nr, c->P.na, c->P.na};
+  for (int d = 0; d < 3; ++d)
+    if (B.lo[d] < 0 || B.hi[d] >= n[d] || B.hi[d] < B.lo[d]) return fail(HC_ERR_ARG, "box outside the panel");
+  O4Args a{};
+  a.G = c->o4;
+  a.nbox = 1;
+  a.block0 = B.block;
+  a.ghost = B.ghost;
+  for (int d = 0; d < 3; ++d) { a.vlo[d] = B.lo[d]; a.vhi[d] = B.hi[d]; }
+  a.U = usph;
+  for (int d = 0; d < 3; ++d) { a.ur.lo[d] = B.lo[d] - B.ghost; a.ur.n[d] = B.hi[d] - B.lo[d] + 1 + 2 * B.ghost; }
+  a.ur.N = (long)a.ur.n[0] * a.ur.n[1] * a.ur.n[2];
+  a.uStride = 8 * a.ur.N;
+  a.rhs = rhs;
+  a.rhsStride = 8L * (B.hi[0] - B.lo[0] + 1) * (B.hi[1] - B.lo[1] + 1) * (B.hi[2] - B.lo[2] + 1);
+  return checkLaunch(launchO4Gravity(a, (cudaStream_t)stream), "hc_box_gravity_o4");
+}
+
 int hc_box_gravity(hc_ctx* c, const hc_box* box, const double* w, double* rhs, void* stream) {
   if (!c || !box || !w || !rhs) return fail(HC_ERR_ARG, "null argument");
   const hc_box& B = *box;
@@ -1011,11 +1039,12 @@ int hc_level_prepare(hc_ctx* c, const double* ju, double* w, double t, void* str
 int hc_level_rhs(hc_ctx* c, const double* w, double* k, void* stream) {
   if (!c || !w || !k) return fail(HC_ERR_ARG, "null argument");
   if (c->P.spatial_order == 4) {
-    if (c->P.sun_gravity) return fail(HC_ERR_UNSUPPORTED, "fourth-order gravity is not built");
     cudaStream_t s = (cudaStream_t)stream;
-    const int rc = checkLaunch(cudaMemsetAsync(k, 0, sizeof(double) * 6 * NC * c->o4l.Nv, s), "O4 k");
+    int rc = checkLaunch(cudaMemsetAsync(k, 0, sizeof(double) * 6 * NC * c->o4l.Nv, s), "O4 k");
+    const O4Args a = levelO4Args(c, w, k);
+    if (rc == HC_OK && c->P.sun_gravity) rc = checkLaunch(launchO4Gravity(a, s), "O4 gravity");
     if (rc != HC_OK) return rc;
-    return checkLaunch(launchO4BoxOperator(levelO4Args(c, w, k), s), "O4 operator");
+    return checkLaunch(launchO4BoxOperator(a, s), "O4 operator");
   }
   StageArgs a = levelArgs(c, w);
   a.rhs = k;
@@ -1028,10 +1057,7 @@ int hc_level_rk4_step(hc_ctx* c, double* ju, double dt, double t, void* stream) 
   if (!c || !ju) return fail(HC_ERR_ARG, "null argument");
   if (!(dt > 0)) return fail(HC_ERR_ARG, "dt must be positive");
   cudaStream_t s = (cudaStream_t)stream;
-  if (c->P.spatial_order == 4) {
-    if (c->P.sun_gravity) return fail(HC_ERR_UNSUPPORTED, "fourth-order gravity is not built");
-    return o4Step(c, ju, dt, nullptr, t, nullptr, s);
-  }
+  if (c->P.spatial_order == 4) return o4Step(c, ju, dt, nullptr, t, nullptr, s);
   const int rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
   if (rc != HC_OK) return rc;
   return rkStep(c, ju, dt, nullptr, nullptr, t, nullptr, s);
@@ -1043,7 +1069,6 @@ int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, do
   cudaStream_t s = (cudaStream_t)stream;
   if (c->P.spatial_order == 4) {
     // dtCFL of the state at the start of each step, then the step.
-    if (c->P.sun_gravity) return fail(HC_ERR_UNSUPPORTED, "fourth-order gravity is not built");
     int rc = HC_OK;
     const double* invMax = reinterpret_cast<const double*>(c->invMax);
     for (int n = 0; n < nsteps && rc == HC_OK; ++n) {

@@ -185,6 +185,8 @@ struct O4Args {
 constexpr int kO4FaceArrays = 8 * 9 + 8;  // WL, WR, FS, QD/DP, FA, FM, FR, Fx (8 each) + thF, PS, BP, PA, T3, Bflux, Bprod, pad
 
 cudaError_t launchO4BoxOperator(const O4Args& a, cudaStream_t s);
+// Gravity_Euler on the valid boxes of `a` (reads U, G; adds into rhs).
+cudaError_t launchO4Gravity(const O4Args& a, cudaStream_t s);
 size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost);
 
 // ---------------------------------------------------------------------------

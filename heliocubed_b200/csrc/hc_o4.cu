@@ -975,6 +975,44 @@ __global__ void o4PowellApplyKernel(const Ctx c) {
   });
 }
 
+// Gravity_Euler (src/BoxOp_Gravity.H:84-164) on the valid boxes: with
+// dr = D_r (dr/dxi0) the fourth-order cell products <rho dr>, <rho V_r dr>
+// (<ab> = <a><b> + (1/12) sum_d D_d a D_d b; dr varies only radially), then
+// rhs(m_d) += -GM faceProduct(<det A A>(d, 0), <rho dr>, 0) and
+// rhs(E) += -GM faceProduct(<det A>, <rho V_r dr>, 0), faceProduct over the
+// two angular directions.
+__global__ void o4GravityKernel(const Ctx c) {
+  const O4Args& a = c.a;
+  const double minusGM = -kGrav * kMsun;
+  forRegion(c.V, a.nbox, [&](int b, int i, int j, int k) {
+    const View U{a.U + b * a.uStride, a.ur};
+    const int blk = a.block0 + b;
+    const double dr0 = radialRow(a.G, i).z;
+    const double da = 0.5 * radialRow(a.G, i + 1).z - 0.5 * radialRow(a.G, i - 1).z;
+    const int pj[5] = {j, j + 1, j - 1, j, j}, pk[5] = {k, k, k, k + 1, k - 1};
+    double rd[5], re[5];
+    const double* M[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const double d0 = 0.5 * U(0, i + 1, pj[q], pk[q]) - 0.5 * U(0, i - 1, pj[q], pk[q]);
+      const double d1 = 0.5 * U(1, i + 1, pj[q], pk[q]) - 0.5 * U(1, i - 1, pj[q], pk[q]);
+      rd[q] = dr0 * U(0, i, pj[q], pk[q]) + da * d0 * (1.0 / 12.0);
+      re[q] = dr0 * U(1, i, pj[q], pk[q]) + da * d1 * (1.0 / 12.0);
+      M[q] = faceRec(a.G, blk, 0, pj[q], pk[q]);
+    }
+    auto faceP = [&](int e, const double* v) {
+      double value = M[0][e] * v[0];
+      value += (0.5 * M[1][e] - 0.5 * M[2][e]) * (0.5 * v[1] - 0.5 * v[2]) * (1.0 / 12.0);
+      value += (0.5 * M[3][e] - 0.5 * M[4][e]) * (0.5 * v[3] - 0.5 * v[4]) * (1.0 / 12.0);
+      return value;
+    };
+    double* R = a.rhs + b * a.rhsStride + roff(c.vr, i, j, k);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) R[(1 + d) * c.vr.N] += faceP(3 * d, rd) * minusGM;
+    R[4 * c.vr.N] += faceP(9, re) * minusGM;
+  });
+}
+
 int blocksFor(long n) {
   long g = (n + 127) / 128;
   if (g > 148L * 32) g = 148L * 32;
@@ -991,6 +1029,12 @@ size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost)
   for (int q = 0; q < 3; ++q) FB.hi[q] += 1;
   const size_t NG = (size_t)G.size(), NF = (size_t)FB.size(), N1 = (size_t)V.grow(1).size(), N2 = (size_t)V.grow(2).size();
   return (size_t)nbox * (8 * NG + 8 * NG + NG + NG + (size_t)kO4FaceArrays * NF + N1 + 16 * N2);
+}
+
+cudaError_t launchO4Gravity(const O4Args& a, cudaStream_t s) {
+  const Ctx c = makeCtx(a, 0);
+  o4GravityKernel<<<blocksFor(c.V.size() * a.nbox), 128, 0, s>>>(c);
+  return cudaGetLastError();
 }
 
 cudaError_t launchO4BoxOperator(const O4Args& a, cudaStream_t s) {

@@ -307,6 +307,12 @@ class Shell:
     def box_gravity(self, box: N.HcBox, w: torch.Tensor, rhs: torch.Tensor) -> None:
         N.check(self._lib.hc_box_gravity(self._ctx, C.byref(box), _ptr(w), _ptr(rhs), _stream()), "hc_box_gravity")
 
+    def box_gravity_o4(self, box: N.HcBox, usph: torch.Tensor, rhs: torch.Tensor) -> None:
+        """Gravity_Euler (src/BoxOp_Gravity.H:84-164) on one box of native
+        averages (valid.grow(ghost >= 1)); rhs[valid] += source."""
+        N.check(self._lib.hc_box_gravity_o4(self._ctx, C.byref(box), _ptr(usph), _ptr(rhs), _stream()),
+                "hc_box_gravity_o4")
+
     def geometry(self, what: int) -> np.ndarray:
         n = self._lib.hc_geometry_export(self._ctx, what, None)
         if n < 0:

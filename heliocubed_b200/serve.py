@@ -40,13 +40,17 @@ class Cone:
     """Synthetic cone-shaped cloud: inside `half_width_deg` of the axis at
     (lat, lon) and below `r_top` (cm), the density is `density_ratio` times
     the wind's and the radial speed `speed_kms`; pressure and field are the
-    wind's."""
+    wind's.  The edges are tapered smoothly (cos^2 over +-`edge` of the half
+    width and of r_top): a sharp-edged cloud moving at up to 2000 km/s
+    through the 400 km/s wind is a discontinuous initial state that the
+    fourth-order scheme need not survive at coarse grids."""
     speed_kms: float = 1000.0
     half_width_deg: float = 30.0
     lat_deg: float = 0.0
     lon_deg: float = 0.0
     density_ratio: float = 4.0
     r_top: float = 30.0 * C_SR
+    edge: float = 0.25
 
 
 @dataclass
@@ -82,10 +86,16 @@ def cone_state(params: Params, det: np.ndarray, dvolr: np.ndarray, cone: Cone,
     X = cell_directions(na)                                      # [6][3][k][j]
     lat, lon = math.radians(cone.lat_deg), math.radians(cone.lon_deg)
     axis = np.array([math.cos(lat) * math.cos(lon), math.cos(lat) * math.sin(lon), math.sin(lat)])
-    inside = (np.einsum("q,bqkj->bkj", axis, X) >= math.cos(math.radians(cone.half_width_deg)))
-    inside = inside[..., None] & (r <= cone.r_top)[None, None, None, :]
-    rho = spec.rho0 * s ** 2 * np.where(inside, cone.density_ratio, 1.0)
-    vr = np.where(inside, cone.speed_kms * 1e5, spec.vr)
+    def taper(x, x0, width):
+        """1 below x0 - width, 0 above x0 + width, cos^2 in between."""
+        t = np.clip((x - (x0 - width)) / (2 * width), 0.0, 1.0)
+        return np.cos(0.5 * np.pi * t) ** 2
+
+    angle = np.arccos(np.clip(np.einsum("q,bqkj->bkj", axis, X), -1.0, 1.0))
+    hw = math.radians(cone.half_width_deg)
+    weight = taper(angle, hw, cone.edge * hw)[..., None] * taper(r, cone.r_top, cone.edge * (cone.r_top - r0))
+    rho = spec.rho0 * s ** 2 * (1.0 + (cone.density_ratio - 1.0) * weight)
+    vr = spec.vr + (cone.speed_kms * 1e5 - spec.vr) * weight
     p = spec.p0 * s ** (2 * gam) * np.ones_like(rho)
     Br = spec.b0 * s[None, None, None, :] ** 2 * np.sign(X[:, 2])[..., None]
     J = det[:, :, :, None] * dvolr[None, None, None, :]

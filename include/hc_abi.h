@@ -135,21 +135,38 @@ int hc_box_rhs_o4(hc_ctx* ctx, const hc_box* box, const double* usph,
 int hc_box_gravity(hc_ctx* ctx, const hc_box* box, const double* w,
                    double* rhs, void* stream);
 
-/* Stage preparation of a level: JU (valid) -> ghosted Cartesian primitives
- * with panel-seam ghosts, floors and radial boundary ghosts at time t.
- * Replaces preStageLevel -> prepareSecondOrderPrimitives
- * (src/BoxOp_PreStage.H:434-501, src/BoxOp_SecondOrderPreStage.H:7-218). */
+/* Solar gravity at fourth order on native averages, rhs[valid] += source
+ * (fourth-order cell and face products of dr/dxi, <rho>, <rho V_r> and the
+ * averaged metrics; context created with spatial_order 4).  usph lives on
+ * valid.grow(ghost), ghost >= 1.  Replaces Gravity_Euler
+ * (src/BoxOp_Gravity.H:84-164). */
+int hc_box_gravity_o4(hc_ctx* ctx, const hc_box* box, const double* usph,
+                      double* rhs, void* stream);
+
+/* Stage preparation of a level at time t; w holds hc_level_primitive_size
+ * doubles.  Order 2: JU (valid) -> ghosted Cartesian primitives [6][8]
+ * [na+4][na+4][nr+4] with panel-seam ghosts, floors and radial boundary
+ * ghosts; replaces preStageLevel -> prepareSecondOrderPrimitives
+ * (src/BoxOp_PreStage.H:434-501, src/BoxOp_SecondOrderPreStage.H:7-218).
+ * Order 4: JU -> native conserved averages USph [6][8][na+10][na+10][nr+10]
+ * by the Cartesian state conversion with seam ghosts (panel corners
+ * included) and radial boundary ghosts; replaces preStageLevel ->
+ * consToSphInterpEulerCartesian + fillRadialBoundaries
+ * (src/MHD_StateConversion.H:153-316, src/BoxOp_SeamPressure.H:5-34). */
 int hc_level_prepare(hc_ctx* ctx, const double* ju, double* w, double t,
                      void* stream);
 
-/* Stage right-hand side of a level: k = gravity + L(w) with shared panel
- * seam states.  Replaces the zero/gravity part of preStageLevel plus
- * StageLevel (src/BoxOp_EulerCubedSphereImplem.H:961-1012). */
+/* Stage right-hand side of a level: k = gravity + L(w) (order 2: with
+ * shared panel seam states; order 4: the Berta operator on each panel,
+ * Gravity_Euler when sun_gravity).  Replaces the zero/gravity part of
+ * preStageLevel plus StageLevel (src/BoxOp_EulerCubedSphereImplem.H:961-1012). */
 int hc_level_rhs(hc_ctx* ctx, const double* w, double* k, void* stream);
 
 /* One classical RK4 step of the level in place, with dt from host.
  * Replaces MBLevelRK::advance(order 4) (src/MHD_LevelRK.H:22-61, tableau
- * src/MHD_AMRRungeKutta.H:10-12). */
+ * src/MHD_AMRRungeKutta.H:10-12).  At spatial order 4 the panel-seam
+ * fluxes are reconciled after the step from the time-integrated flux
+ * register: each side takes the mean of both sides (src/MHD_AMR.H:1478-1497). */
 int hc_level_rk4_step(hc_ctx* ctx, double* ju, double dt, double t,
                       void* stream);
 
@@ -174,9 +191,11 @@ int hc_level_rk4_step_noalloc(hc_ctx* ctx, double* ju, double dt, double t,
 int hc_level_advance_cfl(hc_ctx* ctx, double* ju, int nsteps,
                          double* time_dev, double* dt_dev, void* stream);
 
-/* Maximum over valid cells of the second-order CFL rate, written to the
- * device double *inv_dt_max.  Replaces dtCFLSecondOrderHost
- * (src/BoxOp_SecondOrderCFL.H:99-210) whose result is 1/max. */
+/* Maximum over valid cells of the CFL rate, written to the device double
+ * *inv_dt_max.  Replaces dtCFLSecondOrderHost (src/BoxOp_SecondOrderCFL.H:
+ * 99-210) and, at order 4, dtCFL/dtInv (src/BoxOp_EulerCubedSphereImplem.H:
+ * 878-954,1013-1131), whose results are 1/max; the two use the same
+ * arithmetic on JU. */
 int hc_level_dt_cfl(hc_ctx* ctx, const double* ju, double* inv_dt_max,
                     void* stream);
 

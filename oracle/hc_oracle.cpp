@@ -1189,6 +1189,10 @@ int orc_o4_rhs(void* O, const double* us, double* k, double* reg, double weight)
 int orc_o4_reflux(void* O, const double* reg, double* ju) { o4Reflux(*static_cast<O4Level*>(O), reg, ju); return 0; }
 int orc_o4_rk4_step(void* O, double* ju, double dt, double t) { o4Rk4(*static_cast<O4Level*>(O), ju, dt, t); return 0; }
 double orc_o4_inv_dt(void* O, const double* ju) { return o4InvDt(*static_cast<O4Level*>(O), ju); }
+int orc_box_gravity_o4(void* L, const hc_box* box, const double* usph, double* rhs) {
+  o4Gravity(*static_cast<Level*>(L), box->lo, box->hi, box->ghost, box->block, usph, rhs);
+  return 0;
+}
 int orc_box_gravity(void* L, const hc_box* box, const double* w, double* rhs) {
   boxGravity(*static_cast<Level*>(L), box->lo, box->hi, box->ghost, box->block, w, rhs);
   return 0;

@@ -67,6 +67,7 @@ def lib() -> C.CDLL:
         L.orc_level_destroy.argtypes = [C.c_void_p]
         L.orc_box_rhs.argtypes = [C.c_void_p, C.POINTER(HcBox), _D, C.POINTER(_D), C.c_double, _D, C.POINTER(_D)]
         L.orc_box_gravity.argtypes = [C.c_void_p, C.POINTER(HcBox), _D, _D]
+        L.orc_box_gravity_o4.argtypes = [C.c_void_p, C.POINTER(HcBox), _D, _D]
         L.orc_box_rhs_o4.argtypes = [C.c_void_p, C.POINTER(HcBox), _D, C.c_double, _D, C.POINTER(_D)]
         L.orc_level_prepare.argtypes = [C.c_void_p, _D, _D, C.c_double]
         L.orc_level_rhs.argtypes = [C.c_void_p, _D, _D]
@@ -205,6 +206,9 @@ class OracleLevel:
 
     def box_gravity(self, box: HcBox, w: np.ndarray, rhs: np.ndarray):
         self.L.orc_box_gravity(self.h, C.byref(box), dptr(w), dptr(rhs))
+
+    def box_gravity_o4(self, box: HcBox, usph: np.ndarray, rhs: np.ndarray):
+        self.L.orc_box_gravity_o4(self.h, C.byref(box), dptr(usph), dptr(rhs))
 
 
 class OracleLevelO4:

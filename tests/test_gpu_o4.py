@@ -2,7 +2,7 @@
 the C ABI, on single ghosted boxes (BertaOperator,
 src/BoxOp_BertaCubedSphereImplem.H:1737-2076).
 
-Tolerance: 1e-12 normwise per component for rhs and fluxes (the device
+Tolerance: 1e-12 normwise per component for rhs and fluxes (gravity 1e-13) (the device
 contracts a*b+c into FMA; the oracle does not).  Inputs are seeded:
 a smooth wind (detector quiet) and a field with a sharp jump (detector
 fires, WENO3 / PLM fallbacks and the Roe repair are exercised).
@@ -102,4 +102,38 @@ def test_box_operator_o4_matches_oracle(oracle_lib, riemann, fallback, jump, blo
     for d in range(3):
         e = rel_err_components(flux_g[d].cpu().numpy().reshape(8, -1), flux_o[d].reshape(8, -1), 0)
         assert e.max() < 1e-12, (d, e)
+    shell.close()
+
+
+@pytest.mark.parametrize("block,lo,hi,g", [(3, (2, 0, 5), (9, 6, 15), 5), (1, (0, 4, 0), (5, 15, 3), 1)])
+def test_box_gravity_o4_matches_oracle(oracle_lib, block, lo, hi, g):
+    """Gravity_Euler (src/BoxOp_Gravity.H:84-164) through hc_box_gravity_o4,
+    boxes at panel edges (the angular metric products reach outside)."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    import torch
+
+    import heliocubed_b200 as hc
+    from heliocubed_b200.level import make_box
+    po = oracle_lib
+    nr, na = 16, 16
+    kw = dict(nr=nr, na=na, spatial_order=4, riemann_solver=2, sun_gravity=1)
+    shell = hc.Shell(hc.Params(**kw))
+    orc = po.OracleLevel(po.make_params(**kw))
+    u = usph_box(nr, lo, hi, g, seed=block)
+    v = [hi[d] - lo[d] + 1 for d in range(3)]
+    rhs0 = np.random.default_rng(5).standard_normal(8 * v[0] * v[1] * v[2]) * 1e-3
+    box_o = po.HcBox()
+    for d in range(3):
+        box_o.lo[d], box_o.hi[d] = lo[d], hi[d]
+    box_o.ghost, box_o.block = g, block
+    rhs_o = rhs0.copy()
+    orc.box_gravity_o4(box_o, u, rhs_o)
+    rhs_g = torch.from_numpy(rhs0.copy()).cuda()
+    shell.box_gravity_o4(make_box(lo, hi, g, block), torch.from_numpy(u).cuda(), rhs_g)
+    got = rhs_g.cpu().numpy().reshape(8, -1) - rhs0.reshape(8, -1)
+    ref = rhs_o.reshape(8, -1) - rhs0.reshape(8, -1)
+    assert np.abs(ref[[0, 5, 6, 7]]).max() == 0.0 and np.abs(got[[0, 5, 6, 7]]).max() == 0.0
+    err = np.abs(got[[1, 2, 3, 4]] - ref[[1, 2, 3, 4]]).max(axis=1) / np.abs(ref[[1, 2, 3, 4]]).max(axis=1)
+    assert err.max() < 1e-13, err
     shell.close()

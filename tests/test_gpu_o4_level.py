@@ -37,6 +37,7 @@ GAMMA = 5.0 / 3.0
 CASES = [
     dict(riemann_solver=2, berta_fallback_type=0, divergence_cleaning=1),
     dict(riemann_solver=1, berta_fallback_type=1, divergence_cleaning=1),
+    dict(riemann_solver=2, berta_fallback_type=0, divergence_cleaning=1, sun_gravity=1),
 ]
 
 
@@ -55,7 +56,8 @@ def _unit(b, x1, x2):
 
 def _pair(po, nr=16, na=16, **case):
     _need_gpu()
-    kw = dict(nr=nr, na=na, spatial_order=4, sun_gravity=0, **case)
+    kw = dict(nr=nr, na=na, spatial_order=4, sun_gravity=0)
+    kw.update(case)
     shell = hc.Shell(hc.Params(**kw))
     orc = po.OracleLevelO4(po.make_params(**kw))
     return shell, orc

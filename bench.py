@@ -414,6 +414,106 @@ def run_serve(args, world, rank, local):
         sh.close()
 
 
+def run_amr(args, world, rank, local):
+    """Batched AMR-style operator evaluation (config-3 style, scaled): boxes
+    of 8^3-32^3 on three refinement levels (48^3, 96^3 and 192^3 per panel,
+    ratio 2), fourth-order WENOZ + Roe + Powell.  The batched path evaluates
+    each level's boxes with one launch per operator kernel (hc_o4_batch_rhs);
+    the plain path calls the operator once per box, as the reference's level
+    evaluation does per patch.  Metric: cell-stage evaluations per second."""
+    import torch
+    from heliocubed_b200.level import Params, Shell, make_box, wind_box_state
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(args.seed)
+    plan = [(48, [(16, None)]), (96, [(16, args.amr_l1)]), (192, [(8, int(0.6 * args.amr_l2)),
+                                                             (16, int(0.3 * args.amr_l2)),
+                                                             (32, args.amr_l2 - int(0.6 * args.amr_l2) - int(0.3 * args.amr_l2))])]
+    levels = []
+    for n, groups in plan:
+        sh = Shell(Params(nr=n, na=n, spatial_order=4, riemann_solver=2, berta_fallback_type=0), device=local)
+        specs = []
+        for size, count in groups:
+            if count is None:  # tile the whole level
+                for b in range(6):
+                    for k0 in range(0, n, size):
+                        for j0 in range(0, n, size):
+                            for i0 in range(0, n, size):
+                                specs.append((b, (i0, j0, k0), size))
+            else:
+                for _ in range(count):
+                    lo = tuple(int(rng.integers(0, n - size + 1)) for _ in range(3))
+                    specs.append((int(rng.integers(0, 6)), lo, size))
+        works = []
+        for q, (b, lo, size) in enumerate(specs):
+            hi = tuple(x + size - 1 for x in lo)
+            u = torch.from_numpy(wind_box_state(sh.params, lo, hi, 5, args.seed + q)).to(sh._dev)
+            rhs = torch.zeros(8 * size ** 3, dtype=torch.float64, device=sh._dev)
+            works.append((make_box(lo, hi, 5, b), u, rhs, None))
+        batch = sh.o4_batch(works)
+        singles = [sh.o4_batch([w]) for w in works]
+        levels.append((n, sh, works, batch, singles))
+    cells = sum(sum(int(w[2].numel()) // 8 for w in lv[2]) for lv in levels)
+    nboxes = sum(len(lv[2]) for lv in levels)
+    stream = torch.cuda.current_stream()
+
+    def batched():
+        for _, _, _, batch, _ in levels:
+            batch.rhs()
+
+    def plain():
+        for _, _, _, _, singles in levels:
+            for one in singles:
+                one.rhs()
+
+    def timed(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms_b = timed(batched, args.amr_reps)
+    ms_p = timed(plain, max(1, args.amr_reps // 4))
+    clocks = sampler.stop()
+    # identical results
+    for _, _, works, _, _ in levels:
+        for w in works:
+            w[2].zero_()
+    batched()
+    ref = [w[2].clone() for lv in levels for w in lv[2]]
+    for _, _, works, _, _ in levels:
+        for w in works:
+            w[2].zero_()
+    plain()
+    torch.cuda.synchronize()
+    same = all(torch.equal(a, w[2]) for a, w in zip(ref, [w for lv in levels for w in lv[2]]))
+    if rank == 0:
+        out = {"metric": "FP64 cell-stage evaluations/s, batched AMR boxes vs plain per-box launches",
+               "value": cells / (ms_b * 1e-3) * world, "unit": "cell-stage evaluations/s", "n_gpus": world,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic",
+               "config": {"workload": "AMR-style box batch (scaled config 3), Berta WENOZ + Roe + Powell",
+                          "levels": [{"n": n, "boxes": len(w)} for n, _, w, _, _ in levels], "boxes": nboxes,
+                          "cells": cells, "ghost": 5},
+               "batched": {"ms_per_evaluation": ms_b, "launches": 3 * 36},
+               "plain": {"ms_per_evaluation": ms_p, "cell_stage_per_s": cells / (ms_p * 1e-3),
+                         "launches": 36 * nboxes},
+               "batched_over_plain": ms_p / ms_b, "identical_results": same, "clocks": clocks}
+        print(json.dumps(out), flush=True)
+    for _, sh, _, batch, singles in levels:
+        batch.close()
+        for one in singles:
+            one.close()
+        sh.close()
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -433,6 +533,10 @@ def main() -> int:
     ap.add_argument("--cpu-max-steps", type=int, default=60)
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--serve", action="store_true", help="run the served-ensemble benchmark instead")
+    ap.add_argument("--amr", action="store_true", help="run the batched AMR-box operator benchmark instead")
+    ap.add_argument("--amr-l1", type=int, default=600)
+    ap.add_argument("--amr-l2", type=int, default=1200)
+    ap.add_argument("--amr-reps", type=int, default=8)
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-steps", type=int, default=40)
     ap.add_argument("--serve-inflight", type=int, default=8)
@@ -456,6 +560,8 @@ def main() -> int:
             run_reference(args, world, rank)
         elif args.serve:
             run_serve(args, world, rank, local)
+        elif args.amr:
+            run_amr(args, world, rank, local)
         else:
             run_b200(args, world, rank, local)
     finally:

@@ -28,6 +28,9 @@ SIGNATURES = {
     "hc_box_gravity": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "hc_box_rhs_o4": (C.c_int, [_VP, _VP, _VP, C.c_double, _VP, _VP, _VP]),
     "hc_box_gravity_o4": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "hc_o4_batch_create": (C.c_int, [_VP, _VP, C.c_int, C.c_double, _VP]),
+    "hc_o4_batch_rhs": (C.c_int, [_VP, _VP, _VP]),
+    "hc_o4_batch_destroy": (C.c_int, [_VP]),
     "hc_level_prepare": (C.c_int, [_VP, _VP, _VP, C.c_double, _VP]),
     "hc_level_rhs": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hc_level_rk4_step": (C.c_int, [_VP, _VP, C.c_double, C.c_double, _VP]),
@@ -67,6 +70,11 @@ class HcInit(C.Structure):
         ("r_ref", C.c_double), ("pulse_amp", C.c_double), ("pulse_width", C.c_double),
         ("reserved_d", C.c_double * 4),
     ]
+
+
+class HcBoxWork(C.Structure):
+    """Mirror of hc_box_work in include/hc_abi.h."""
+    _fields_ = [("box", HcBox), ("usph", C.c_void_p), ("rhs", C.c_void_p), ("flux", C.c_void_p * 3)]
 
 
 class HcError(RuntimeError):

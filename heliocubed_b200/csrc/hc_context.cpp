@@ -256,6 +256,10 @@ struct hc_ctx {
   double* o4k = nullptr;       // stage right-hand side [6][8][Nv]
   double* o4reg = nullptr;     // seam flux register [6][2][2][8][na][nr]
   double* o4lvlScratch = nullptr;
+  O4Batch* o4levelBatch = nullptr;  // the six panels on o4us -> o4k
+  // operator batches of recent argument sets (hc_box_rhs_o4, hc_level_rhs on
+  // caller arrays), oldest first
+  std::vector<std::pair<std::string, O4Batch*>> o4cache;
 };
 
 namespace {
@@ -696,17 +700,6 @@ int buildO4Level(hc_ctx* c) {
   O.ringJK = upload(ringJK, c->owned, err);
   O.ring = upload(ring, c->owned, err);
   if (err != cudaSuccess) return cudaFail(err, "O4 level tables");
-  const int vlo[3] = {0, 0, 0}, vhi[3] = {nr - 1, na - 1, na - 1};
-  const size_t sizes[6] = {(size_t)6 * 8 * O.Ng, (size_t)6 * 8 * O.Nc, (size_t)6 * 8 * O.Nv, (size_t)6 * 8 * O.Nv,
-                           (size_t)6 * 2 * 2 * 8 * na * nr, o4ScratchDoubles(6, vlo, vhi, kO4Ghost)};
-  double** dst[6] = {&c->o4us, &c->o4cart, &c->o4next, &c->o4k, &c->o4reg, &c->o4lvlScratch};
-  for (int q = 0; q < 6; ++q) {
-    void* p = nullptr;
-    if ((err = cudaMalloc(&p, sizes[q] * sizeof(double))) != cudaSuccess) return cudaFail(err, "O4 level buffers");
-    c->owned.push_back(p);
-    *dst[q] = static_cast<double*>(p);
-    if ((err = cudaMemset(p, 0, sizes[q] * sizeof(double))) != cudaSuccess) return cudaFail(err, "O4 level buffers");
-  }
   return HC_OK;
 }
 
@@ -733,13 +726,15 @@ int allocWorkspace(hc_ctx* c) {
   const size_t nv = 6 * NC * (size_t)c->L.Nv, ng = 6 * NC * (size_t)c->L.Ng;
   void* p;
   cudaError_t e;
-  for (int q = 0; q < 2; ++q) {
+  for (int q = 0; q < 2 && c->P.spatial_order == 2; ++q) {
     if ((e = cudaMalloc(&p, ng * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace W");
     c->owned.push_back(p); c->W[q] = (double*)p;
     if ((e = cudaMemset(p, 0, ng * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace W");
   }
-  if ((e = cudaMalloc(&p, nv * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace acc");
-  c->owned.push_back(p); c->acc = (double*)p;
+  if (c->P.spatial_order == 2) {
+    if ((e = cudaMalloc(&p, nv * sizeof(double))) != cudaSuccess) return cudaFail(e, "workspace acc");
+    c->owned.push_back(p); c->acc = (double*)p;
+  }
   if ((e = cudaMalloc(&p, 64)) != cudaSuccess) return cudaFail(e, "workspace scalars");
   c->owned.push_back(p); c->invMax = (unsigned long long*)p;
   c->flag = (int*)((char*)p + 32);
@@ -818,6 +813,61 @@ O4Args levelO4Args(hc_ctx* c, const double* us, double* k) {
   return a;
 }
 
+// The operator batch of an argument set, built on first use (a cudaMalloc
+// and a copy: not inside a stream capture) and kept for the next calls.
+O4Batch* cachedBatch(hc_ctx* c, const O4Args& a, int* rc) {
+  std::string key;
+  auto put = [&key](const void* p, size_t n) { key.append(static_cast<const char*>(p), n); };
+  put(&a.nbox, sizeof a.nbox); put(&a.block0, sizeof a.block0); put(&a.ghost, sizeof a.ghost);
+  put(a.vlo, sizeof a.vlo); put(a.vhi, sizeof a.vhi); put(&a.U, sizeof a.U); put(a.ur.lo, sizeof a.ur.lo);
+  put(a.ur.n, sizeof a.ur.n); put(&a.uStride, sizeof a.uStride); put(&a.scale, sizeof a.scale);
+  put(&a.rhs, sizeof a.rhs); put(&a.rhsStride, sizeof a.rhsStride); put(a.flux, sizeof a.flux);
+  put(&a.WA, sizeof a.WA); put(&a.face, sizeof a.face); put(&a.kp, sizeof a.kp);
+  for (auto& e : c->o4cache)
+    if (e.first == key) return e.second;
+  std::vector<O4Args> boxes;
+  o4SplitArgs(a, boxes);
+  cudaError_t err;
+  O4Batch* B = o4BatchCreate(boxes.data(), (int)boxes.size(), &err);
+  if (!B) {
+    *rc = cudaFail(err, "O4 batch");
+    return nullptr;
+  }
+  if (c->o4cache.size() >= 32) {
+    o4BatchDestroy(c->o4cache.front().second);
+    c->o4cache.erase(c->o4cache.begin());
+  }
+  c->o4cache.emplace_back(key, B);
+  return B;
+}
+
+// Level-sized buffers of the fourth-order level step and the operator batch
+// over them, allocated on the first level call (so a context used only for
+// box and batch evaluations holds none): make that first call outside any
+// stream capture.
+int ensureO4Buffers(hc_ctx* c) {
+  if (c->o4levelBatch) return HC_OK;
+  const O4Level& O = c->o4l;
+  const int nr = O.nr, na = O.na;
+  const int vlo[3] = {0, 0, 0}, vhi[3] = {nr - 1, na - 1, na - 1};
+  const size_t sizes[7] = {(size_t)6 * 8 * O.Ng, (size_t)6 * 8 * O.Nc, (size_t)6 * 8 * O.Nv, (size_t)6 * 8 * O.Nv,
+                           (size_t)6 * 2 * 2 * 8 * na * nr, o4ScratchDoubles(6, vlo, vhi, kO4Ghost),
+                           (size_t)6 * 8 * O.Nv};
+  double** dst[7] = {&c->o4us, &c->o4cart, &c->o4next, &c->o4k, &c->o4reg, &c->o4lvlScratch, &c->acc};
+  cudaError_t err;
+  for (int q = 0; q < 7; ++q) {
+    void* p = nullptr;
+    if ((err = cudaMalloc(&p, sizes[q] * sizeof(double))) != cudaSuccess) return cudaFail(err, "O4 level buffers");
+    c->owned.push_back(p);
+    *dst[q] = static_cast<double*>(p);
+    if ((err = cudaMemset(p, 0, sizes[q] * sizeof(double))) != cudaSuccess) return cudaFail(err, "O4 level buffers");
+  }
+  std::vector<O4Args> boxes;
+  o4SplitArgs(levelO4Args(c, c->o4us, c->o4k), boxes);
+  c->o4levelBatch = o4BatchCreate(boxes.data(), (int)boxes.size(), &err);
+  return c->o4levelBatch ? HC_OK : cudaFail(err, "O4 level batch");
+}
+
 // One fourth-order RK4 step: per stage, prepare USph from the stage state,
 // evaluate the operator into k (seam fluxes into the register), update the
 // accumulator and the next stage; then reconcile the seam fluxes.
@@ -830,16 +880,12 @@ int o4Step(hc_ctx* c, double* ju, double dtv, const double* invMax, double tbase
     rc = checkLaunch(launchO4Prepare(io, s), "O4 prepare");
     if (rc == HC_OK) rc = checkLaunch(cudaMemsetAsync(c->o4k, 0, sizeof(double) * 6 * 8 * O.Nv, s), "O4 k");
     if (rc != HC_OK) break;
-    O4Args a = levelO4Args(c, c->o4us, c->o4k);
     if (c->P.sun_gravity) {
-      rc = checkLaunch(launchO4Gravity(a, s), "O4 gravity");
+      rc = checkLaunch(launchO4BatchGravity(c->o4levelBatch, s), "O4 gravity");
       if (rc != HC_OK) break;
     }
-    a.reg = c->o4reg;
-    a.regWeight = invMax ? b4[stage] : dtv * b4[stage];
-    a.regWeightDev = invMax;
-    a.cfl = c->P.cfl;
-    rc = checkLaunch(launchO4BoxOperator(a, s), "O4 operator");
+    const RegArgs rg{c->o4reg, invMax ? b4[stage] : dtv * b4[stage], invMax, c->P.cfl};
+    rc = checkLaunch(launchO4Batch(c->o4levelBatch, &rg, s), "O4 operator");
     if (rc == HC_OK)
       rc = checkLaunch(launchO4Update(O, stage, c->o4k, ju, c->acc, c->o4next, invMax, c->P.cfl, dtv, s), "O4 update");
   }
@@ -901,6 +947,8 @@ int hc_ctx_create(const hc_params* p, int device, hc_ctx** out) {
 int hc_ctx_destroy(hc_ctx* c) {
   if (!c) return HC_OK;
   cudaSetDevice(c->device);
+  for (auto& e : c->o4cache) o4BatchDestroy(e.second);
+  o4BatchDestroy(c->o4levelBatch);
   for (void* p : c->owned) cudaFree(p);
   if (c->o4scratch) cudaFree(c->o4scratch);
   delete c;
@@ -982,7 +1030,101 @@ int hc_box_rhs_o4(hc_ctx* c, const hc_box* box, const double* usph, double scale
     c->o4scratchDoubles = need;
   }
   carveO4Scratch(a, c->o4scratch);
-  return checkLaunch(launchO4BoxOperator(a, (cudaStream_t)stream), "hc_box_rhs_o4");
+  int rc = HC_OK;
+  O4Batch* batch = cachedBatch(c, a, &rc);
+  if (!batch) return rc;
+  return checkLaunch(launchO4Batch(batch, nullptr, (cudaStream_t)stream), "hc_box_rhs_o4");
+}
+
+}  // extern "C"
+
+struct hc_o4_batch {
+  O4Batch* batch = nullptr;
+  double* scratch = nullptr;
+  int gravity = 0;
+  int device = 0;
+};
+
+extern "C" {
+
+int hc_o4_batch_create(hc_ctx* c, const hc_box_work* boxes, int nbox, double scale, hc_o4_batch** out) {
+  if (!c || !boxes || !out || nbox <= 0) return fail(HC_ERR_ARG, "bad argument");
+  *out = nullptr;
+  if (c->P.spatial_order != 4) return fail(HC_ERR_UNSUPPORTED, "context was created with spatial_order != 4");
+  if (nbox > 65535) return fail(HC_ERR_ARG, "at most 65535 boxes per batch");
+  const int n[3] = {c->P.nr, c->P.na, c->P.na};
+  std::vector<size_t> off(nbox + 1, 0);
+  for (int b = 0; b < nbox; ++b) {
+    const hc_box& B = boxes[b].box;
+    if (!boxes[b].usph || !boxes[b].rhs) return fail(HC_ERR_ARG, "null usph or rhs in the batch");
+    if (B.block < 0 || B.block > 5) return fail(HC_ERR_ARG, "block must be 0..5");
+    if (B.ghost < kO4Ghost) return fail(HC_ERR_ARG, "the Berta operator needs ghost >= 5");
+    for (int d = 0; d < 3; ++d)
+      if (B.lo[d] < 0 || B.hi[d] >= n[d] || B.hi[d] < B.lo[d]) return fail(HC_ERR_ARG, "box outside the panel");
+    off[b + 1] = off[b] + o4ScratchDoubles(1, B.lo, B.hi, kO4Ghost);
+  }
+  hc_o4_batch* h = new (std::nothrow) hc_o4_batch;
+  if (!h) return fail(HC_ERR_NOMEM, "batch allocation");
+  h->gravity = c->P.sun_gravity;
+  h->device = c->device;
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, off[nbox] * sizeof(double));
+  if (e != cudaSuccess) {
+    delete h;
+    return cudaFail(e, "batch scratch");
+  }
+  h->scratch = static_cast<double*>(p);
+  std::vector<O4Args> args(nbox);
+  for (int b = 0; b < nbox; ++b) {
+    const hc_box& B = boxes[b].box;
+    O4Args& a = args[b];
+    a = O4Args{};
+    a.G = c->o4;
+    a.nbox = 1;
+    a.block0 = B.block;
+    a.ghost = kO4Ghost;
+    for (int d = 0; d < 3; ++d) {
+      a.vlo[d] = B.lo[d];
+      a.vhi[d] = B.hi[d];
+      a.ur.lo[d] = B.lo[d] - B.ghost;
+      a.ur.n[d] = B.hi[d] - B.lo[d] + 1 + 2 * B.ghost;
+      a.flux[d] = boxes[b].flux[d];
+    }
+    a.ur.N = (long)a.ur.n[0] * a.ur.n[1] * a.ur.n[2];
+    a.U = boxes[b].usph;
+    a.uStride = 8 * a.ur.N;
+    a.scale = scale;
+    a.rhs = boxes[b].rhs;
+    a.rhsStride = 8L * (B.hi[0] - B.lo[0] + 1) * (B.hi[1] - B.lo[1] + 1) * (B.hi[2] - B.lo[2] + 1);
+    carveO4Scratch(a, h->scratch + off[b]);
+  }
+  h->batch = o4BatchCreate(args.data(), nbox, &e);
+  if (!h->batch) {
+    cudaFree(h->scratch);
+    delete h;
+    return cudaFail(e, "batch contexts");
+  }
+  *out = h;
+  return HC_OK;
+}
+
+int hc_o4_batch_rhs(hc_ctx* c, hc_o4_batch* h, void* stream) {
+  if (!c || !h) return fail(HC_ERR_ARG, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (h->gravity) {
+    const int rc = checkLaunch(launchO4BatchGravity(h->batch, s), "batch gravity");
+    if (rc != HC_OK) return rc;
+  }
+  return checkLaunch(launchO4Batch(h->batch, nullptr, s), "batch operator");
+}
+
+int hc_o4_batch_destroy(hc_o4_batch* h) {
+  if (!h) return HC_OK;
+  cudaSetDevice(h->device);
+  o4BatchDestroy(h->batch);
+  if (h->scratch) cudaFree(h->scratch);
+  delete h;
+  return HC_OK;
 }
 
 int hc_box_gravity_o4(hc_ctx* c, const hc_box* box, const double* usph, double* rhs, void* stream) {
@@ -1006,7 +1148,10 @@ int hc_box_gravity_o4(hc_ctx* c, const hc_box* box, const double* usph, double* 
   a.uStride = 8 * a.ur.N;
   a.rhs = rhs;
   a.rhsStride = 8L * (B.hi[0] - B.lo[0] + 1) * (B.hi[1] - B.lo[1] + 1) * (B.hi[2] - B.lo[2] + 1);
-  return checkLaunch(launchO4Gravity(a, (cudaStream_t)stream), "hc_box_gravity_o4");
+  int rc = HC_OK;
+  O4Batch* Bt = cachedBatch(c, a, &rc);
+  if (!Bt) return rc;
+  return checkLaunch(launchO4BatchGravity(Bt, (cudaStream_t)stream), "hc_box_gravity_o4");
 }
 
 int hc_box_gravity(hc_ctx* c, const hc_box* box, const double* w, double* rhs, void* stream) {
@@ -1027,6 +1172,8 @@ int hc_level_prepare(hc_ctx* c, const double* ju, double* w, double t, void* str
   if (!c || !ju || !w) return fail(HC_ERR_ARG, "null argument");
   cudaStream_t s = (cudaStream_t)stream;
   if (c->P.spatial_order == 4) {
+    const int rc4 = ensureO4Buffers(c);
+    if (rc4 != HC_OK) return rc4;
     O4StageIO io{c->o4l, ju, c->o4cart, w, StageTime{t, nullptr, 0.0, nullptr, 0.0}};
     return checkLaunch(launchO4Prepare(io, s), "O4 prepare");
   }
@@ -1040,11 +1187,14 @@ int hc_level_rhs(hc_ctx* c, const double* w, double* k, void* stream) {
   if (!c || !w || !k) return fail(HC_ERR_ARG, "null argument");
   if (c->P.spatial_order == 4) {
     cudaStream_t s = (cudaStream_t)stream;
-    int rc = checkLaunch(cudaMemsetAsync(k, 0, sizeof(double) * 6 * NC * c->o4l.Nv, s), "O4 k");
-    const O4Args a = levelO4Args(c, w, k);
-    if (rc == HC_OK && c->P.sun_gravity) rc = checkLaunch(launchO4Gravity(a, s), "O4 gravity");
+    int rc = ensureO4Buffers(c);
     if (rc != HC_OK) return rc;
-    return checkLaunch(launchO4BoxOperator(a, s), "O4 operator");
+    O4Batch* B = (w == c->o4us && k == c->o4k) ? c->o4levelBatch : cachedBatch(c, levelO4Args(c, w, k), &rc);
+    if (!B) return rc;
+    rc = checkLaunch(cudaMemsetAsync(k, 0, sizeof(double) * 6 * NC * c->o4l.Nv, s), "O4 k");
+    if (rc == HC_OK && c->P.sun_gravity) rc = checkLaunch(launchO4BatchGravity(B, s), "O4 gravity");
+    if (rc != HC_OK) return rc;
+    return checkLaunch(launchO4Batch(B, nullptr, s), "O4 operator");
   }
   StageArgs a = levelArgs(c, w);
   a.rhs = k;
@@ -1057,7 +1207,10 @@ int hc_level_rk4_step(hc_ctx* c, double* ju, double dt, double t, void* stream) 
   if (!c || !ju) return fail(HC_ERR_ARG, "null argument");
   if (!(dt > 0)) return fail(HC_ERR_ARG, "dt must be positive");
   cudaStream_t s = (cudaStream_t)stream;
-  if (c->P.spatial_order == 4) return o4Step(c, ju, dt, nullptr, t, nullptr, s);
+  if (c->P.spatial_order == 4) {
+    const int rc4 = ensureO4Buffers(c);
+    return rc4 != HC_OK ? rc4 : o4Step(c, ju, dt, nullptr, t, nullptr, s);
+  }
   const int rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
   if (rc != HC_OK) return rc;
   return rkStep(c, ju, dt, nullptr, nullptr, t, nullptr, s);
@@ -1069,7 +1222,7 @@ int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, do
   cudaStream_t s = (cudaStream_t)stream;
   if (c->P.spatial_order == 4) {
     // dtCFL of the state at the start of each step, then the step.
-    int rc = HC_OK;
+    int rc = ensureO4Buffers(c);
     const double* invMax = reinterpret_cast<const double*>(c->invMax);
     for (int n = 0; n < nsteps && rc == HC_OK; ++n) {
       rc = checkLaunch(launchCfl(c->L, ju, c->invMax, s), "cfl");

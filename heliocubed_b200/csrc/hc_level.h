@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include <vector>
+
 #include "hc_common.h"
 
 namespace hc {
@@ -174,20 +176,34 @@ struct O4Args {
   double* face; // [nbox][kO4FaceArrays][F]
   double* mj;   // [nbox][V+1]
   double* kp;   // [nbox][8][V+2]
-  // seam flux register (level step only; boxes are whole panels): the
-  // final face flux of panel-boundary faces of directions 1, 2 is added
-  // times regWeight into reg [6][2][2][8][na][nr]
-  double* reg;
-  double regWeight;
-  const double* regWeightDev;  // when set, regWeight *= cfl / *regWeightDev
-  double cfl;
 };
 constexpr int kO4FaceArrays = 8 * 9 + 8;  // WL, WR, FS, QD/DP, FA, FM, FR, Fx (8 each) + thF, PS, BP, PA, T3, Bflux, Bprod, pad
 
-cudaError_t launchO4BoxOperator(const O4Args& a, cudaStream_t s);
-// Gravity_Euler on the valid boxes of `a` (reads U, G; adds into rhs).
-cudaError_t launchO4Gravity(const O4Args& a, cudaStream_t s);
 size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost);
+
+// Seam flux register of the level step (reg null: off): the final face flux
+// of panel-boundary faces of directions 1, 2 of whole-panel boxes is added
+// times w (times cfl / *wDev when wDev is set) into reg [6][2][2][8][na][nr].
+struct RegArgs {
+  double* reg;
+  double w;
+  const double* wDev;
+  double cfl;
+};
+
+// A batch of boxes of any sizes for the operator kernels: per box and
+// direction a kernel context in device memory; every kernel of the operator
+// is one launch over the whole batch (one CTA row per box).  Each entry of
+// `boxes` describes one box (nbox 1) with its own input, output and scratch.
+struct O4Batch;
+O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err);
+void o4BatchDestroy(O4Batch* b);
+// The one-box argument sets of a uniform multi-box O4Args (box b on panel
+// block0 + b, arrays at b x stride).
+void o4SplitArgs(const O4Args& a, std::vector<O4Args>& out);
+cudaError_t launchO4Batch(const O4Batch* b, const RegArgs* reg, cudaStream_t s);
+// Gravity_Euler on the valid boxes of the batch (reads U, adds into rhs).
+cudaError_t launchO4BatchGravity(const O4Batch* b, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // Fourth-order level step (hc_o4level.cu): one box per panel.

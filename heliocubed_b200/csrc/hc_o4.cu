@@ -10,6 +10,9 @@
 // handles one cell or face of one box.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "hc_device.cuh"
 #include "hc_level.h"
 
@@ -361,24 +364,26 @@ __device__ __forceinline__ double faceProd(double f4, double g4, double df0, dou
   return value;
 }
 
-// Decode thread -> (box, i, j, k) over box region b.
+
+// Thread -> (i, j, k) over region b of this CTA row's box (blockIdx.y
+// selects the box; every pointer in its Ctx is that box's, so the body sees
+// box index 0).
 template <class F>
 __device__ __forceinline__ void forRegion(const Box3& b, int nbox, F f) {
+  (void)nbox;
   const long n = b.size();
-  const long total = n * nbox;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const int box = (int)(t / n);
-    const long r = t - (long)box * n;
-    const int i = b.lo[0] + (int)(r % b.n(0));
-    const int j = b.lo[1] + (int)((r / b.n(0)) % b.n(1));
-    const int k = b.lo[2] + (int)(r / ((long)b.n(0) * b.n(1)));
-    f(box, i, j, k);
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = b.lo[0] + (int)(t % b.n(0));
+    const int j = b.lo[1] + (int)((t / b.n(0)) % b.n(1));
+    const int k = b.lo[2] + (int)(t / ((long)b.n(0) * b.n(1)));
+    f(0, i, j, k);
   }
 }
 
 // ---- kernels ------------------------------------------------------------------
 // 1. detector primitives of the averages, V(<U>) (:1776).
-__global__ void o4PrimAvgKernel(const Ctx c) {
+__global__ void o4PrimAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + 0];
   const O4Args& a = c.a;
   forRegion(c.G, a.nbox, [&](int b, int i, int j, int k) {
     double u[8], w[8];
@@ -389,6 +394,10 @@ __global__ void o4PrimAvgKernel(const Ctx c) {
     double* W = a.WA + (long)b * 8 * c.gr.N + roff(c.gr, i, j, k);
 #pragma unroll
     for (int q = 0; q < 8; ++q) W[q * c.gr.N] = w[q];
+    // the Powell accumulator -J div B starts at zero on V1
+    if (a.G.powell && i >= c.V1.lo[0] && i <= c.V1.hi[0] && j >= c.V1.lo[1] && j <= c.V1.hi[1] && k >= c.V1.lo[2] &&
+        k <= c.V1.hi[2])
+      a.mj[(long)b * c.v1r.N + roff(c.v1r, i, j, k)] = 0.0;
   });
 }
 
@@ -403,7 +412,8 @@ __device__ __forceinline__ double eta1(double qm, double q0, double qp) {
 }
 
 // 2. raw Jameson flag on G.grow(-1) (:347-402).
-__global__ void o4ThetaRawKernel(const Ctx c) {
+__global__ void o4ThetaRawKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + 0];
   const O4Args& a = c.a;
   forRegion(c.GR, a.nbox, [&](int b, int i, int j, int k) {
     const double* W = a.WA + (long)b * 8 * c.gr.N;
@@ -426,7 +436,8 @@ __global__ void o4ThetaRawKernel(const Ctx c) {
 
 // 3. dilated theta (0 outside G.grow(-2)), theta-aware average-to-point and
 // point primitives on G (:404-507, 696-741, 212-275).
-__global__ void o4PointKernel(const Ctx c) {
+__global__ void o4PointKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + 0];
   const O4Args& a = c.a;
   forRegion(c.G, a.nbox, [&](int b, int i, int j, int k) {
     const long N = c.gr.N, o = roff(c.gr, i, j, k);
@@ -469,7 +480,8 @@ __device__ __forceinline__ const double* faceBasis(const Ctx& c, int b, int j, i
 // 4. reconstruction (WENOZ / WENO3 / PLM with clamps), Roe repair, energies,
 // point flux sum, total-pressure sum, centred normal B, Rusanov jump (F).
 template <int D>
-__global__ void __launch_bounds__(128, 5) o4FaceReconKernel(const Ctx c) {
+__global__ void __launch_bounds__(128, 5) o4FaceReconKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const double dx2 = a.G.dx[d] * a.G.dx[d];
@@ -553,7 +565,8 @@ __global__ void __launch_bounds__(128, 5) o4FaceReconKernel(const Ctx c) {
 // 4b. pointwise factored Roe dissipation on the final faces + one transverse
 // ring (src/BoxOp_RoeCubedSphere.H:73-98).
 template <int D>
-__global__ void __launch_bounds__(128, 3) o4RoePointKernel(const Ctx c) {
+__global__ void __launch_bounds__(128, 3) o4RoePointKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const Box3 PB = c.V0.growTrans(d, 1);
@@ -571,7 +584,8 @@ __global__ void __launch_bounds__(128, 3) o4RoePointKernel(const Ctx c) {
 
 // 5. theta-aware point-to-average of the flux sum and total pressure (F1).
 template <int D>
-__global__ void o4FaceAvgKernel(const Ctx c) {
+__global__ void o4FaceAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   forRegion(c.F1, a.nbox, [&](int b, int i, int j, int k) {
@@ -593,7 +607,8 @@ __global__ void o4FaceAvgKernel(const Ctx c) {
 // 6. mapped flux with separable metrics (bertaMapHostBox, :35-95 and
 // :1361-1450) on F1; zero on F outside it.
 template <int D>
-__global__ void o4FaceMapKernel(const Ctx c) {
+__global__ void o4FaceMapKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
@@ -664,7 +679,8 @@ __global__ void o4FaceMapKernel(const Ctx c) {
 
 // 7. radial-area face products of the mapped flux and of <p_tot> (F1).
 template <int D>
-__global__ void o4FaceRadialKernel(const Ctx c) {
+__global__ void o4FaceRadialKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   forRegion(c.F1, a.nbox, [&](int b, int i, int j, int k) {
@@ -691,7 +707,8 @@ __global__ void o4FaceRadialKernel(const Ctx c) {
 // 8. pressure force, dissipation, combine on the final faces V0; writes the
 // flux (scratch and caller).
 template <int D>
-__global__ void __launch_bounds__(128, 4) o4FaceFinalKernel(const Ctx c) {
+__global__ void __launch_bounds__(128, 4) o4FaceFinalKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
@@ -817,13 +834,13 @@ __global__ void __launch_bounds__(128, 4) o4FaceFinalKernel(const Ctx c) {
 #pragma unroll
       for (int q = 0; q < 8; ++q) fo2[q * r0.N] = fx[q];
     }
-    if (a.reg && d > 0) {
+    if (rg.reg && d > 0) {
       const int f = d == 1 ? j : k;
       if (f == 0 || f == a.G.na) {
         const long nrna = (long)a.G.na * a.G.nr;
         const int side = f == 0 ? 0 : 1, s = d == 1 ? k : j;
-        const double w = a.regWeightDev ? a.regWeight * (a.cfl / *a.regWeightDev) : a.regWeight;
-        double* R = a.reg + (((long)blk * 2 + (d - 1)) * 2 + side) * 8 * nrna + (long)s * a.G.nr + i;
+        const double w = rg.wDev ? rg.w * (rg.cfl / *rg.wDev) : rg.w;
+        double* R = rg.reg + (((long)blk * 2 + (d - 1)) * 2 + side) * 8 * nrna + (long)s * a.G.nr + i;
 #pragma unroll
         for (int q = 0; q < 8; ++q) R[q * nrna] += w * fx[q];
       }
@@ -833,7 +850,8 @@ __global__ void __launch_bounds__(128, 4) o4FaceFinalKernel(const Ctx c) {
 
 // 9. flux divergence into rhs (V).
 template <int D>
-__global__ void o4DivKernel(const Ctx c) {
+__global__ void o4DivKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const double coef = -a.scale / a.G.dx[d];
@@ -849,7 +867,8 @@ __global__ void o4DivKernel(const Ctx c) {
 
 // 10. Powell face flux (DivBPowell1, src/BoxOp_DivBcleaning.H:35-74).
 template <int D>
-__global__ void o4PowellFluxKernel(const Ctx c) {
+__global__ void o4PowellFluxKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
@@ -888,7 +907,8 @@ __global__ void o4PowellFluxKernel(const Ctx c) {
 
 // 11. Powell radial-area product and divergence into -J div B (V+1).
 template <int D>
-__global__ void o4PowellProdKernel(const Ctx c) {
+__global__ void o4PowellProdKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
@@ -910,7 +930,8 @@ __global__ void o4PowellProdKernel(const Ctx c) {
 }
 
 template <int D>
-__global__ void o4PowellDivKernel(const Ctx c) {
+__global__ void o4PowellDivKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const double coef = -1.0 / a.G.dx[d];
@@ -923,7 +944,8 @@ __global__ void o4PowellDivKernel(const Ctx c) {
 }
 
 // 12. DivBPowell2 with point primitives (src/BoxOp_DivBcleaning.H:80-172).
-__global__ void o4PowellCoefKernel(const Ctx c) {
+__global__ void o4PowellCoefKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + 0];
   const O4Args& a = c.a;
   forRegion(c.V2, a.nbox, [&](int b, int i, int j, int k) {
     const long NG = c.gr.N, o = roff(c.gr, i, j, k);
@@ -949,7 +971,8 @@ __global__ void o4PowellCoefKernel(const Ctx c) {
   });
 }
 
-__global__ void o4PowellAvgKernel(const Ctx c) {
+__global__ void o4PowellAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + 0];
   const O4Args& a = c.a;
   forRegion(c.V1, a.nbox, [&](int b, int i, int j, int k) {
     const View KP{a.kp + (long)b * 16 * c.v2r.N, c.v2r};
@@ -959,7 +982,8 @@ __global__ void o4PowellAvgKernel(const Ctx c) {
   });
 }
 
-__global__ void o4PowellApplyKernel(const Ctx c) {
+__global__ void o4PowellApplyKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + 0];
   const O4Args& a = c.a;
   forRegion(c.V, a.nbox, [&](int b, int i, int j, int k) {
     const View KA{a.kp + (long)b * 16 * c.v2r.N + 8 * c.v2r.N, c.v2r};
@@ -981,7 +1005,8 @@ __global__ void o4PowellApplyKernel(const Ctx c) {
 // rhs(m_d) += -GM faceProduct(<det A A>(d, 0), <rho dr>, 0) and
 // rhs(E) += -GM faceProduct(<det A>, <rho V_r dr>, 0), faceProduct over the
 // two angular directions.
-__global__ void o4GravityKernel(const Ctx c) {
+__global__ void o4GravityKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+  const Ctx& c = tab[blockIdx.y * 3 + 0];
   const O4Args& a = c.a;
   const double minusGM = -kGrav * kMsun;
   forRegion(c.V, a.nbox, [&](int b, int i, int j, int k) {
@@ -1013,11 +1038,6 @@ __global__ void o4GravityKernel(const Ctx c) {
   });
 }
 
-int blocksFor(long n) {
-  long g = (n + 127) / 128;
-  if (g > 148L * 32) g = 148L * 32;
-  return (int)(g < 1 ? 1 : g);
-}
 
 }  // namespace
 
@@ -1031,50 +1051,120 @@ size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost)
   return (size_t)nbox * (8 * NG + 8 * NG + NG + NG + (size_t)kO4FaceArrays * NF + N1 + 16 * N2);
 }
 
-cudaError_t launchO4Gravity(const O4Args& a, cudaStream_t s) {
+// A batch: per box and direction the Ctx of a one-box O4Args, in device
+// memory (the kernels' argument) and mirrored on the host (launch sizes).
+struct O4Batch {
+  int nbox = 0;
+  Ctx* dev = nullptr;
+  std::vector<Ctx> host;
+  bool roe = false, powell = false;
+};
+
+O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
+  *err = cudaSuccess;
+  if (nbox <= 0 || nbox > 65535) {
+    *err = cudaErrorInvalidValue;
+    return nullptr;
+  }
+  O4Batch* B = new O4Batch;
+  B->nbox = nbox;
+  B->host.resize((size_t)nbox * 3);
+  for (int b = 0; b < nbox; ++b) {
+    O4Args one = boxes[b];
+    one.nbox = 1;
+    for (int d = 0; d < 3; ++d) B->host[(size_t)b * 3 + d] = makeCtx(one, d);
+  }
+  B->roe = boxes[0].G.roe;
+  B->powell = boxes[0].G.powell;
+  *err = cudaMalloc(&B->dev, sizeof(Ctx) * B->host.size());
+  if (*err == cudaSuccess) *err = cudaMemcpy(B->dev, B->host.data(), sizeof(Ctx) * B->host.size(), cudaMemcpyHostToDevice);
+  if (*err != cudaSuccess) {
+    o4BatchDestroy(B);
+    return nullptr;
+  }
+  return B;
+}
+
+void o4BatchDestroy(O4Batch* B) {
+  if (!B) return;
+  if (B->dev) cudaFree(B->dev);
+  delete B;
+}
+
+void o4SplitArgs(const O4Args& a, std::vector<O4Args>& out) {
   const Ctx c = makeCtx(a, 0);
-  o4GravityKernel<<<blocksFor(c.V.size() * a.nbox), 128, 0, s>>>(c);
+  out.assign(a.nbox, a);
+  for (int b = 0; b < a.nbox; ++b) {
+    O4Args& o = out[b];
+    o.nbox = 1;
+    o.block0 = a.block0 + b;
+    o.U = a.U + (long)b * a.uStride;
+    o.rhs = a.rhs + (long)b * a.rhsStride;
+    for (int d = 0; d < 3; ++d)
+      if (a.flux[d]) o.flux[d] = a.flux[d] + (long)b * 8 * c.V.extrude(d).size();
+    o.WA = a.WA + (long)b * 8 * c.gr.N;
+    o.WP = a.WP + (long)b * 8 * c.gr.N;
+    o.th = a.th + (long)b * c.gr.N;
+    o.thr = a.thr + (long)b * c.gr.N;
+    o.face = a.face + (long)b * kO4FaceArrays * c.fr.N;
+    o.mj = a.mj + (long)b * c.v1r.N;
+    o.kp = a.kp + (long)b * 16 * c.v2r.N;
+  }
+}
+
+namespace {
+// Grid of a launch over the batch: one CTA row per box (y), x sized for the
+// box with the largest region, the whole grid held near 148 x 32 CTAs (the
+// region loops stride over the rest).
+template <class R>
+dim3 gridOf(const O4Batch& B, int d, R region) {
+  long m = 1;
+  for (int b = 0; b < B.nbox; ++b) m = std::max(m, region(B.host[(size_t)b * 3 + d]).size());
+  const long need = (m + 127) / 128;
+  const long perBox = std::max(1L, 148L * 32 / B.nbox);
+  return dim3((unsigned)std::max(1L, std::min(need, perBox)), (unsigned)B.nbox, 1);
+}
+}  // namespace
+
+cudaError_t launchO4BatchGravity(const O4Batch* B, cudaStream_t s) {
+  const RegArgs none{};
+  o4GravityKernel<<<gridOf(*B, 0, [](const Ctx& c) { return c.V; }), 128, 0, s>>>(B->dev, none);
   return cudaGetLastError();
 }
 
-cudaError_t launchO4BoxOperator(const O4Args& a, cudaStream_t s) {
-  // scratch carve-up (see o4ScratchDoubles)
-  Ctx c0 = makeCtx(a, 0);
-  const long nb = a.nbox;
-  const int T = 128;
+cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) {
+  const RegArgs none{};
+  const RegArgs rg = reg ? *reg : none;
+  const Ctx* t = B->dev;
   cudaError_t e;
-#define HC_LAUNCH(kernel, ctx, region)                                                  \
-  kernel<<<blocksFor((region).size() * nb), T, 0, s>>>(ctx);                           \
+#define HC_LAUNCH(kernel, d, region)                                                     \
+  kernel<<<gridOf(*B, d, [](const Ctx& c) { return region; }), 128, 0, s>>>(t, rg);      \
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-#define HC_LAUNCH_D(kernel, ctx, region)                                                \
-  if ((ctx).d == 0) { HC_LAUNCH(kernel<0>, ctx, region) }                              \
-  else if ((ctx).d == 1) { HC_LAUNCH(kernel<1>, ctx, region) }                         \
-  else { HC_LAUNCH(kernel<2>, ctx, region) }
-  HC_LAUNCH(o4PrimAvgKernel, c0, c0.G)
-  HC_LAUNCH(o4ThetaRawKernel, c0, c0.GR)
-  HC_LAUNCH(o4PointKernel, c0, c0.G)
-  if (a.G.powell) {
-    if ((e = cudaMemsetAsync(a.mj, 0, sizeof(double) * nb * c0.v1r.N, s)) != cudaSuccess) return e;
-  }
+#define HC_LAUNCH_D(kernel, region)                                                      \
+  if (d == 0) { HC_LAUNCH(kernel<0>, 0, region) }                                       \
+  else if (d == 1) { HC_LAUNCH(kernel<1>, 1, region) }                                  \
+  else { HC_LAUNCH(kernel<2>, 2, region) }
+  HC_LAUNCH(o4PrimAvgKernel, 0, c.G)
+  HC_LAUNCH(o4ThetaRawKernel, 0, c.GR)
+  HC_LAUNCH(o4PointKernel, 0, c.G)
   for (int d = 0; d < 3; ++d) {
-    Ctx c = makeCtx(a, d);
-    HC_LAUNCH_D(o4FaceReconKernel, c, c.F)
-    if (a.G.roe) { HC_LAUNCH_D(o4RoePointKernel, c, c.V0.growTrans(d, 1)) }
-    HC_LAUNCH_D(o4FaceAvgKernel, c, c.F1)
-    HC_LAUNCH_D(o4FaceMapKernel, c, c.F)
-    HC_LAUNCH_D(o4FaceRadialKernel, c, c.F1)
-    HC_LAUNCH_D(o4FaceFinalKernel, c, c.V0)
-    HC_LAUNCH_D(o4DivKernel, c, c.V)
-    if (a.G.powell) {
-      HC_LAUNCH_D(o4PowellFluxKernel, c, c.V1.extrude(d).growTrans(d, 1))
-      HC_LAUNCH_D(o4PowellProdKernel, c, c.V1.extrude(d))
-      HC_LAUNCH_D(o4PowellDivKernel, c, c.V1)
+    HC_LAUNCH_D(o4FaceReconKernel, c.F)
+    if (B->roe) { HC_LAUNCH_D(o4RoePointKernel, c.V0.growTrans(c.d, 1)) }
+    HC_LAUNCH_D(o4FaceAvgKernel, c.F1)
+    HC_LAUNCH_D(o4FaceMapKernel, c.F)
+    HC_LAUNCH_D(o4FaceRadialKernel, c.F1)
+    HC_LAUNCH_D(o4FaceFinalKernel, c.V0)
+    HC_LAUNCH_D(o4DivKernel, c.V)
+    if (B->powell) {
+      HC_LAUNCH_D(o4PowellFluxKernel, c.V1.extrude(c.d).growTrans(c.d, 1))
+      HC_LAUNCH_D(o4PowellProdKernel, c.V1.extrude(c.d))
+      HC_LAUNCH_D(o4PowellDivKernel, c.V1)
     }
   }
-  if (a.G.powell) {
-    HC_LAUNCH(o4PowellCoefKernel, c0, c0.V2)
-    HC_LAUNCH(o4PowellAvgKernel, c0, c0.V1)
-    HC_LAUNCH(o4PowellApplyKernel, c0, c0.V)
+  if (B->powell) {
+    HC_LAUNCH(o4PowellCoefKernel, 0, c.V2)
+    HC_LAUNCH(o4PowellAvgKernel, 0, c.V1)
+    HC_LAUNCH(o4PowellApplyKernel, 0, c.V)
   }
 #undef HC_LAUNCH_D
 #undef HC_LAUNCH

@@ -169,6 +169,39 @@ def perturbed_wind_state(params: Params, det: np.ndarray, dvolr: np.ndarray, see
     return ju
 
 
+def wind_box_state(params: Params, lo, hi, ghost: int, seed: int, spec: "InitSpec | None" = None) -> np.ndarray:
+    """Native conserved averages of one box on valid.grow(ghost), [8][k][j][i]
+    flattened: the Parker-like wind of InitSpec (rho ~ r^-2, v_r, p ~
+    r^-2 gamma, B_r ~ r^-2) with seeded smooth tangential perturbations of a
+    few percent (synthetic input for operator batches; the native basis
+    has the radial unit vector as its first column)."""
+    spec = spec or InitSpec()
+    rng = np.random.default_rng(seed)
+    gam = params.gamma
+    r0, r1, C = params.inner_radius, params.outer_radius, params.radial_stretch
+    Rt = (r1 - r0) / np.expm1(C)
+    i = np.arange(lo[0] - ghost, hi[0] + ghost + 1)
+    j = np.arange(lo[1] - ghost, hi[1] + ghost + 1)
+    k = np.arange(lo[2] - ghost, hi[2] + ghost + 1)
+    r = r0 + Rt * np.expm1(C * (i + 0.5) / params.nr)
+    s = spec.r_ref / r
+    ph = rng.uniform(0, 2 * np.pi, 3)
+    h = 1.0 / params.na
+    ang = (np.sin(2 * np.pi * (j + 0.5) * h + ph[0])[None, :, None]
+           * np.cos(2 * np.pi * (k + 0.5) * h + ph[1])[:, None, None])
+    rho = spec.rho0 * s ** 2 * (1 + 0.05 * ang)
+    p = spec.p0 * s ** (2 * gam) * (1 + 0.02 * ang)
+    U = np.zeros((8,) + rho.shape)
+    U[0] = rho
+    U[1] = rho * spec.vr
+    U[2] = rho * spec.vr * 0.01 * ang
+    U[3] = rho * spec.vr * 0.01 * np.cos(2 * np.pi * (j + 0.5) * h + ph[2])[None, :, None]
+    U[5] = spec.b0 * s ** 2
+    U[6] = 0.02 * spec.b0 * s * ang
+    U[4] = p / (gam - 1) + 0.5 * rho * spec.vr ** 2 + U[5] ** 2 / (8 * np.pi)
+    return np.ascontiguousarray(U.reshape(-1))
+
+
 def _ptr(t: torch.Tensor | None):
     if t is None:
         return None
@@ -307,6 +340,11 @@ class Shell:
     def box_gravity(self, box: N.HcBox, w: torch.Tensor, rhs: torch.Tensor) -> None:
         N.check(self._lib.hc_box_gravity(self._ctx, C.byref(box), _ptr(w), _ptr(rhs), _stream()), "hc_box_gravity")
 
+    def o4_batch(self, works, scale: float = 1.0) -> "O4Batch":
+        """A batch of boxes of any sizes for the fourth-order operator:
+        works = [(box, usph, rhs, fluxes or None), ...] over device tensors."""
+        return O4Batch(self, works, scale)
+
     def box_gravity_o4(self, box: N.HcBox, usph: torch.Tensor, rhs: torch.Tensor) -> None:
         """Gravity_Euler (src/BoxOp_Gravity.H:84-164) on one box of native
         averages (valid.grow(ghost >= 1)); rhs[valid] += source."""
@@ -330,3 +368,37 @@ def make_box(lo, hi, ghost: int, block: int) -> N.HcBox:
     b.ghost = ghost
     b.block = block
     return b
+
+
+class O4Batch:
+    """hc_o4_batch: the fourth-order operator on many boxes of any sizes, each
+    operator kernel one launch over all of them.  Keeps the tensors alive."""
+
+    def __init__(self, shell: Shell, works, scale: float = 1.0):
+        self.shell = shell
+        self._keep = []
+        arr = (N.HcBoxWork * len(works))()
+        for q, (box, usph, rhs, fluxes) in enumerate(works):
+            arr[q].box = box
+            arr[q].usph = usph.data_ptr()
+            arr[q].rhs = rhs.data_ptr()
+            for d in range(3):
+                arr[q].flux[d] = fluxes[d].data_ptr() if fluxes is not None and fluxes[d] is not None else None
+            self._keep.append((usph, rhs, fluxes))
+        h = C.c_void_p()
+        N.check(shell._lib.hc_o4_batch_create(shell._ctx, arr, len(works), scale, C.byref(h)), "hc_o4_batch_create")
+        self._h = h
+
+    def rhs(self) -> None:
+        N.check(self.shell._lib.hc_o4_batch_rhs(self.shell._ctx, self._h, _stream()), "hc_o4_batch_rhs")
+
+    def close(self) -> None:
+        if self._h:
+            self.shell._lib.hc_o4_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -135,6 +135,35 @@ int hc_box_rhs_o4(hc_ctx* ctx, const hc_box* box, const double* usph,
 int hc_box_gravity(hc_ctx* ctx, const hc_box* box, const double* w,
                    double* rhs, void* stream);
 
+/* One box of a fourth-order operator batch: the box (ghost >= 5), its
+ * native averages on valid.grow(ghost), its rhs on valid (accumulated) and
+ * optional face fluxes on valid.extrude(d) (overwritten; NULL to skip). */
+typedef struct hc_box_work {
+  hc_box box;
+  const double* usph;
+  double* rhs;
+  double* flux[3];
+} hc_box_work;
+
+typedef struct hc_o4_batch hc_o4_batch;
+
+/* A batch of boxes of any sizes on this context's level (spatial_order 4):
+ * allocates every box's operator scratch and builds the per-box kernel
+ * contexts in device memory, once.  The arrays of `boxes` must stay
+ * allocated while the batch lives.  Replaces the per-patch loop of the AMR
+ * level evaluation (GridLevel::evaluate, src/MHD_AMR.H:1417-1499), which
+ * calls the operator once per patch. */
+int hc_o4_batch_create(hc_ctx* ctx, const hc_box_work* boxes, int nbox,
+                       double scale, hc_o4_batch** out);
+
+/* Evaluate every box of the batch: gravity (Gravity_Euler, when the context
+ * has sun_gravity) and the Berta operator, each operator kernel one launch
+ * over all boxes.  No allocation, no host synchronisation: may be captured
+ * in a CUDA graph. */
+int hc_o4_batch_rhs(hc_ctx* ctx, hc_o4_batch* batch, void* stream);
+
+int hc_o4_batch_destroy(hc_o4_batch* batch);
+
 /* Solar gravity at fourth order on native averages, rhs[valid] += source
  * (fourth-order cell and face products of dr/dxi, <rho>, <rho V_r> and the
  * averaged metrics; context created with spatial_order 4).  usph lives on

@@ -43,6 +43,7 @@ def test_struct_layouts_match_header(product_lib_path):
     assert C.sizeof(_native.HcParams) == 16 * 4 + 14 * 8 + 0 * 8 or C.sizeof(_native.HcParams) == 64 + 112
     assert C.sizeof(_native.HcBox) == 8 * 4
     assert C.sizeof(_native.HcInit) == 8 * 4 + 11 * 8
+    assert C.sizeof(_native.HcBoxWork) == 8 * 4 + 5 * 8
 
 
 @pytest.mark.parametrize("fields,code", [

@@ -51,8 +51,9 @@ def launches_per_step(args) -> int:
     if args.order == 2:
         return 11  # prim + cfl + 4 x (ghosts, stage) + time (prologue in every 1-step call)
     roe, powell = int(args.riemann == 2), 1
-    per_stage = 3 + 3 + 3 * (6 + roe + 3 * powell) + 3 * powell + 1  # prepare, operator, update
-    return 1 + 4 * per_stage + 2 + 1                                  # cfl, stages, reflux, time
+    operator = 3 + 3 * (6 + roe + 3 * powell) + 3 * powell
+    per_stage = 4 + int(args.gravity) + operator + 1               # prepare, gravity, operator, update
+    return 1 + 4 * per_stage + 2 + 1                               # cfl, stages, reflux, time
 
 
 def workload_params(args, nr=None, na=None):
@@ -76,7 +77,9 @@ def workload_config(args, flush: bool):
         "scheme": {"spatial_order": args.order, "limiter": args.limiter if args.order == 2 else None,
                    "riemann_solver": args.riemann, "powell": 1, "gravity": args.gravity, "temporal_order": 4,
                    "cfl": 0.4},
-        "init": ("Parker-like wind + seeded 5% tangential v and B (stream-function curl)" if args.order == 4
+        "init": ("Parker-like wind + cone cloud 1500 km/s, 45 deg half-width, 4x density (tapered edges)"
+                 if args.init == "cone" else
+                 "Parker-like wind + seeded 5% tangential v and B (stream-function curl)" if args.order == 4
                  else "Parker-like wind + seeded Gaussian pressure pulse"),
         "l2": "flushed between timed steps (256 MiB write)" if flush else "working set larger than L2",
         "dt": "device CFL reduction every step",
@@ -248,7 +251,11 @@ def run_b200(args, world, rank, local):
     params = workload_params(args)
     shell = Shell(params, device=local)
     cells = shell.cells
-    if args.order == 4:
+    if args.init == "cone":
+        from heliocubed_b200 import serve
+        req = serve.Request(0, args.nr, args.na, args.order, 0, cone=serve.Cone(1500.0, 45.0, 0.0, 0.0, 4.0))
+        ju0 = torch.from_numpy(serve.initial_state(shell, req)).to(shell._dev)
+    elif args.order == 4:
         ju0 = shell.init_perturbed_wind(args.seed)
     else:
         ju0 = shell.init(InitSpec.seeded(args.seed, args.nr, args.na))
@@ -526,6 +533,8 @@ def main() -> int:
     ap.add_argument("--limiter", type=int, default=3)
     ap.add_argument("--riemann", type=int, default=None)
     ap.add_argument("--gravity", type=int, default=0)
+    ap.add_argument("--init", choices=["default", "cone"], default="default",
+                    help="cone: the wind with a 1500 km/s, 45 deg cone cloud (the large-solve workload)")
     ap.add_argument("--seed", type=int, default=20261204)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", dest="graph", action="store_false",

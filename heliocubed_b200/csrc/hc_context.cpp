@@ -256,6 +256,7 @@ struct hc_ctx {
   double* o4k = nullptr;       // stage right-hand side [6][8][Nv]
   double* o4reg = nullptr;     // seam flux register [6][2][2][8][na][nr]
   double* o4lvlScratch = nullptr;
+  double* o4pv = nullptr;      // seam interpolation point values [6][8][npts][nr]
   O4Batch* o4levelBatch = nullptr;  // the six panels on o4us -> o4k
   // operator batches of recent argument sets (hc_box_rhs_o4, hc_level_rhs on
   // caller arrays), oldest first
@@ -627,7 +628,23 @@ int buildO4Level(hc_ctx* c) {
     for (int j = -ga; j < na + ga; ++j)
       if (!(j >= 0 && j < na && k >= 0 && k < na)) ringJK.push_back(make_int2(j, k));
   O.nring = (int)ringJK.size();
-  std::vector<O4Point> ring((size_t)6 * O.nring * 5);
+  // interpolation points: ghost centres and their 4 neighbours
+  static const int off[5][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+  const int nP = na + 2 * ga + 2;  // point grid [-ga-1, na+ga+1)
+  std::vector<int> ptIndex((size_t)nP * nP, -1), ringPt((size_t)O.nring * 5);
+  std::vector<int2> ptJK;
+  for (int r = 0; r < O.nring; ++r)
+    for (int q = 0; q < 5; ++q) {
+      const int j = ringJK[r].x + off[q][0], k = ringJK[r].y + off[q][1];
+      int& idx = ptIndex[(size_t)(k + ga + 1) * nP + (j + ga + 1)];
+      if (idx < 0) {
+        idx = (int)ptJK.size();
+        ptJK.push_back(make_int2(j, k));
+      }
+      ringPt[(size_t)r * 5 + q] = idx;
+    }
+  O.npts = (int)ptJK.size();
+  std::vector<O4Point> pts((size_t)6 * O.npts);
   auto aIdx = [&](int b, int j, int k) { return ((size_t)b * nA + (k + ga)) * nA + (j + ga); };
   for (int b = 0; b < 6; ++b) {
     for (int k = -ga; k < na + ga; ++k)
@@ -670,22 +687,20 @@ int buildO4Level(hc_ctx* c) {
         basisAt(b, (j + 0.5) * h, (k + 0.5) * h, A, X);
         for (int q = 0; q < 3; ++q) xhat[(((size_t)b * nG + (k + g)) * nG + (j + g)) * 3 + q] = X[q];
       }
-    static const int off[5][2] = {{0, 0}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}};
-    for (int r = 0; r < O.nring; ++r)
-      for (int q = 0; q < 5; ++q) {
-        const int j = ringJK[r].x + off[q][0], k = ringJK[r].y + off[q][1];
-        double A[3][3], X[3], y1, y2;
-        basisAt(b, (j + 0.5) * h, (k + 0.5) * h, A, X);
-        O4Point pt{};
-        pt.p = locateTie(X);
-        panelCoords(pt.p, X, y1, y2);
-        const long double u1 = (long double)y1 / h, u2 = (long double)y2 / h;
-        pt.j0 = std::max(0, std::min(na - 4, (int)std::floor((double)u1) - 1));
-        pt.k0 = std::max(0, std::min(na - 4, (int)std::floor((double)u2) - 1));
-        averageInterp(u1, pt.j0, pt.wj, q == 0 ? 5.0L / 6.0L : 1.0L / 24.0L);
-        averageInterp(u2, pt.k0, pt.wk, 1.0L);
-        ring[((size_t)b * O.nring + r) * 5 + q] = pt;
-      }
+    for (int q = 0; q < O.npts; ++q) {
+      const int j = ptJK[q].x, k = ptJK[q].y;
+      double A[3][3], X[3], y1, y2;
+      basisAt(b, (j + 0.5) * h, (k + 0.5) * h, A, X);
+      O4Point pt{};
+      pt.p = locateTie(X);
+      panelCoords(pt.p, X, y1, y2);
+      const long double u1 = (long double)y1 / h, u2 = (long double)y2 / h;
+      pt.j0 = std::max(0, std::min(na - 4, (int)std::floor((double)u1) - 1));
+      pt.k0 = std::max(0, std::min(na - 4, (int)std::floor((double)u2) - 1));
+      averageInterp(u1, pt.j0, pt.wj, 1.0L);
+      averageInterp(u2, pt.k0, pt.wk, 1.0L);
+      pts[(size_t)b * O.npts + q] = pt;
+    }
   }
   std::vector<double2> radial(nr + 2 * g + 2);
   for (int i = -g - 1; i <= nr + g; ++i) {
@@ -698,7 +713,8 @@ int buildO4Level(hc_ctx* c) {
   O.xhat = upload(xhat, c->owned, err);
   O.radial = upload(radial, c->owned, err);
   O.ringJK = upload(ringJK, c->owned, err);
-  O.ring = upload(ring, c->owned, err);
+  O.ringPt = upload(ringPt, c->owned, err);
+  O.pts = upload(pts, c->owned, err);
   if (err != cudaSuccess) return cudaFail(err, "O4 level tables");
   return HC_OK;
 }
@@ -850,12 +866,12 @@ int ensureO4Buffers(hc_ctx* c) {
   const O4Level& O = c->o4l;
   const int nr = O.nr, na = O.na;
   const int vlo[3] = {0, 0, 0}, vhi[3] = {nr - 1, na - 1, na - 1};
-  const size_t sizes[7] = {(size_t)6 * 8 * O.Ng, (size_t)6 * 8 * O.Nc, (size_t)6 * 8 * O.Nv, (size_t)6 * 8 * O.Nv,
+  const size_t sizes[8] = {(size_t)6 * 8 * O.Ng, (size_t)6 * 8 * O.Nc, (size_t)6 * 8 * O.Nv, (size_t)6 * 8 * O.Nv,
                            (size_t)6 * 2 * 2 * 8 * na * nr, o4ScratchDoubles(6, vlo, vhi, kO4Ghost),
-                           (size_t)6 * 8 * O.Nv};
-  double** dst[7] = {&c->o4us, &c->o4cart, &c->o4next, &c->o4k, &c->o4reg, &c->o4lvlScratch, &c->acc};
+                           (size_t)6 * 8 * O.Nv, (size_t)6 * 8 * O.npts * nr};
+  double** dst[8] = {&c->o4us, &c->o4cart, &c->o4next, &c->o4k, &c->o4reg, &c->o4lvlScratch, &c->acc, &c->o4pv};
   cudaError_t err;
-  for (int q = 0; q < 7; ++q) {
+  for (int q = 0; q < 8; ++q) {
     void* p = nullptr;
     if ((err = cudaMalloc(&p, sizes[q] * sizeof(double))) != cudaSuccess) return cudaFail(err, "O4 level buffers");
     c->owned.push_back(p);
@@ -876,7 +892,8 @@ int o4Step(hc_ctx* c, double* ju, double dtv, const double* invMax, double tbase
   const O4Level& O = c->o4l;
   int rc = checkLaunch(cudaMemsetAsync(c->o4reg, 0, sizeof(double) * 6 * 2 * 2 * 8 * O.na * O.nr, s), "register");
   for (int stage = 0; stage < 4 && rc == HC_OK; ++stage) {
-    O4StageIO io{O, stage == 0 ? ju : c->o4next, c->o4cart, c->o4us, StageTime{tbase, tdev, c4[stage], invMax, dtv}};
+    O4StageIO io{O, stage == 0 ? ju : c->o4next, c->o4cart, c->o4us, c->o4pv,
+                 StageTime{tbase, tdev, c4[stage], invMax, dtv}};
     rc = checkLaunch(launchO4Prepare(io, s), "O4 prepare");
     if (rc == HC_OK) rc = checkLaunch(cudaMemsetAsync(c->o4k, 0, sizeof(double) * 6 * 8 * O.Nv, s), "O4 k");
     if (rc != HC_OK) break;
@@ -1174,7 +1191,7 @@ int hc_level_prepare(hc_ctx* c, const double* ju, double* w, double t, void* str
   if (c->P.spatial_order == 4) {
     const int rc4 = ensureO4Buffers(c);
     if (rc4 != HC_OK) return rc4;
-    O4StageIO io{c->o4l, ju, c->o4cart, w, StageTime{t, nullptr, 0.0, nullptr, 0.0}};
+    O4StageIO io{c->o4l, ju, c->o4cart, w, c->o4pv, StageTime{t, nullptr, 0.0, nullptr, 0.0}};
     return checkLaunch(launchO4Prepare(io, s), "O4 prepare");
   }
   int rc = checkLaunch(launchPrimValid(c->L, ju, w, s), "prim");

@@ -210,8 +210,9 @@ cudaError_t launchO4BatchGravity(const O4Batch* b, cudaStream_t s);
 // ---------------------------------------------------------------------------
 constexpr int kO4Cart = 6;  // angular ghost layers of the Cartesian averages
 
-// One point of a seam ghost average: panel p, 4 x 4 donor cells starting at
-// (j0, k0), tensor weights wj (times the point's coefficient) and wk.
+// One interpolation point of the seam ghosts: the point value at a cell
+// centre of the ghost panel's grid from panel p's 4 x 4 donor cell averages
+// starting at (j0, k0), tensor weights wj and wk.
 struct O4Point {
   int p, j0, k0, pad;
   double wj[4], wk[4];
@@ -221,13 +222,15 @@ struct O4Level {
   int nr, na, g, ga;        // g = kO4Ghost, ga = kO4Cart
   int nA, nG;               // na + 2 ga, na + 2 g
   int nring;                // seam ghost positions per panel
+  int npts;                 // interpolation points per panel
   long Nv, Ng, Nc;          // per panel: valid, ghosted native, Cartesian
   const double* coef;       // [6][nA][nA][27]: <A>^-1, D1 <A>, D2 <A> (row-major)
   const double* detx;       // [6][na+2][na+2]: <det A>, j, k in [-1, na]
   const double* xhat;       // [6][nG][nG][3]: unit direction of the cell centre
   const double2* radial;    // [nr + 2g + 2], index i + g + 1: {dVolr, cell-centre radius}
   const int2* ringJK;       // [nring]: (j, k) of each seam ghost position
-  const O4Point* ring;      // [6][nring][5]
+  const int* ringPt;        // [nring][5]: points at the ghost centre and its 4 neighbours
+  const O4Point* pts;       // [6][npts]
   double gamma, r0, strength, cfl;
 };
 
@@ -237,6 +240,7 @@ struct O4StageIO {
   const double* ju;   // stage state [6][8][Nv]
   double* cart;       // [6][8][Nc]
   double* us;         // [6][8][Ng]
+  double* pv;         // point values [6][8][npts][nr]
   StageTime t;
 };
 

@@ -6,9 +6,11 @@
 //   1. o4CartesianKernel: JU -> fourth-order Cartesian averages U inside each
 //      panel (quotient by <det A> with the (1/12) D(JU/det) D(det) angular
 //      correction, then by dVolr with the radial one);
-//   2. o4SeamKernel: U on kO4Cart angular ghost layers (panel corners
-//      included) from the panels that contain the ghost cells (own
-//      fourth-order average interpolation; the tables come from the host);
+//   2. o4SeamPointKernel, o4SeamKernel: U on kO4Cart angular ghost layers
+//      (panel corners included) from the panels that contain the ghost cells
+//      (own fourth-order average interpolation; the tables come from the
+//      host): point values at the ghost centres and their neighbours, then
+//      each ghost average from five of them;
 //   3. o4NativeKernel: U -> native averages USph with the fourth-order matrix
 //      quotient of src/MHD_CachedCartesianConversion.H:65-210 on the ghosted
 //      box, and the radial ghosts of src/BoxOp_PreStage.H:57-228 (inner:
@@ -110,7 +112,40 @@ __global__ void o4CartesianKernel(const O4StageIO io) {
   }
 }
 
-// 2. Seam ghosts of the Cartesian averages.
+// 2a. Point values of the Cartesian averages at the interpolation points
+// (ghost centres and their neighbours): the tensor-product cubic matching
+// the 4 x 4 donor cell averages, evaluated at the point.
+__global__ void o4SeamPointKernel(const O4StageIO io) {
+  const O4Level& O = io.O;
+  const long n = 6L * O.npts * O.nr;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % O.nr);
+    const long q = t / O.nr;
+    const int pt = (int)(q % O.npts);
+    const int b = (int)(q / O.npts);
+    const O4Point P = O.pts[(long)b * O.npts + pt];
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      double row[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const long base = cIdx(O, P.p, 0, i, P.j0 + m, P.k0 + kk);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) row[c] += P.wj[m] * io.cart[base + (long)c * O.Nc];
+      }
+#pragma unroll
+      for (int c = 0; c < 8; ++c) v[c] += P.wk[kk] * row[c];
+    }
+    double* out = io.pv + ((long)b * 8 * O.npts + pt) * O.nr + i;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) out[(long)c * O.npts * O.nr] = v[c];
+  }
+}
+
+// 2b. Seam ghost averages: (5/6) U(centre) + (1/24) sum of U at the four
+// neighbouring centres, a fourth-order cell average in the ghost panel's
+// coordinates.
 __global__ void o4SeamKernel(const O4StageIO io) {
   const O4Level& O = io.O;
   const long n = 6L * O.nring * O.nr;
@@ -120,26 +155,15 @@ __global__ void o4SeamKernel(const O4StageIO io) {
     const int pos = (int)(q % O.nring);
     const int b = (int)(q / O.nring);
     const int2 jk = O.ringJK[pos];
-    const O4Point* pts = O.ring + ((long)b * O.nring + pos) * 5;
-    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll 1
-    for (int p = 0; p < 5; ++p) {
-      const O4Point pt = pts[p];
+    const int* pt = O.ringPt + (long)pos * 5;
+    const double* pv = io.pv + (long)b * 8 * O.npts * O.nr + i;
+    const long cs = (long)O.npts * O.nr;
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        double row[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          const long base = cIdx(O, pt.p, 0, i, pt.j0 + m, pt.k0 + kk);
-#pragma unroll
-          for (int c = 0; c < 8; ++c) row[c] += pt.wj[m] * io.cart[base + (long)c * O.Nc];
-        }
-#pragma unroll
-        for (int c = 0; c < 8; ++c) v[c] += pt.wk[kk] * row[c];
-      }
+    for (int c = 0; c < 8; ++c) {
+      const double* v = pv + c * cs;
+      const double nb = (v[(long)pt[1] * O.nr] + v[(long)pt[2] * O.nr]) + (v[(long)pt[3] * O.nr] + v[(long)pt[4] * O.nr]);
+      io.cart[cIdx(O, b, c, i, jk.x, jk.y)] = (5.0 / 6.0) * v[(long)pt[0] * O.nr] + (1.0 / 24.0) * nb;
     }
-#pragma unroll
-    for (int c = 0; c < 8; ++c) io.cart[cIdx(O, b, c, i, jk.x, jk.y)] = v[c];
   }
 }
 
@@ -296,6 +320,8 @@ cudaError_t launchO4Prepare(const O4StageIO& io, cudaStream_t s) {
   o4CartesianKernel<<<blocksFor(6L * O.Nv), kThreads, 0, s>>>(io);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  o4SeamPointKernel<<<blocksFor(6L * O.npts * O.nr), kThreads, 0, s>>>(io);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   o4SeamKernel<<<blocksFor(6L * O.nring * O.nr), kThreads, 0, s>>>(io);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   o4NativeKernel<<<blocksFor(6L * (O.nr + 2 * O.g) * O.nG * O.nG), kThreads, 0, s>>>(io);

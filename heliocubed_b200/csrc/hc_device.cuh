@@ -226,26 +226,31 @@ __device__ __forceinline__ bool roe8Body(double out[8], const double* wl, const 
   const double sih = BX >= zero ? 1.0 : -1.0;
   double du[8] = {RhoL - RhoR, RUL - RUR, RVL - RVR, RWL - RWR, EL - ER, BXL - BXR, BYL - BYR, BZL - BZR};
   du[4] = -hgamma * (-kk * du[0] + U * du[1] + V * du[2] + W * du[3] - du[4] + (BX * du[5] + BY * du[6] + BZ * du[7]) * d_1_4PI);
-  du[1] = (-U * du[0] + du[1]) / Rho;
-  du[2] = (-V * du[0] + du[2]) / Rho;
-  du[3] = (-W * du[0] + du[3]) / Rho;
+  // The left-eigenvector entries divide by a few common factors; their
+  // reciprocals are taken once (one rounding from the reference's
+  // repeated divisions).
+  const double iRho = 1.0 / Rho;
+  du[1] = (-U * du[0] + du[1]) * iRho;
+  du[2] = (-V * du[0] + du[2]) * iRho;
+  du[3] = (-W * du[0] + du[3]) * iRho;
   const double sqPiRho = sqrt(d_PI * Rho), sq2PiRho = sqrt(d_2PI * Rho);
+  const double icc = 1.0 / cc, iccRho = 1.0 / (cc * Rho), icSqPi = 1.0 / (c * sqPiRho), iSq2Pi = 1.0 / sq2PiRho;
   RoeEig e{Rho, alf, als, af, as, hyy, hzz, sih, cc, c, sqPiRho, sq2PiRho};
   // Left-eigenvector projections alpha_k = sum_c so[k][c] du[c]
   // (src/MHD_Roe8Wave.H:428-498, zeros skipped).
   double al[8];
-  al[0] = du[0] + (-1.0 / cc) * du[4];
+  al[0] = du[0] + (-icc) * du[4];
   al[1] = du[5];
-  al[2] = -hzz * d_SQRT_2 * du[2] + hyy * d_SQRT_2 * du[3] + half * hzz * sih / sq2PiRho * du[6] + -half * hyy * sih / sq2PiRho * du[7];
-  al[3] = -hzz * d_SQRT_2 * du[2] + hyy * d_SQRT_2 * du[3] + -half * hzz * sih / sq2PiRho * du[6] + half * hyy * sih / sq2PiRho * du[7];
-  al[4] = half * alf * af / cc * du[1] + -half * als * as * hyy * sih / cc * du[2] + -half * als * as * hzz * sih / cc * du[3] +
-          half * alf / (cc * Rho) * du[4] + 0.25 * als * hyy / (c * sqPiRho) * du[6] + 0.25 * als * hzz / (c * sqPiRho) * du[7];
-  al[5] = -half * alf * af / cc * du[1] + half * als * as * hyy * sih / cc * du[2] + half * als * as * hzz * sih / cc * du[3] +
-          half * alf / (cc * Rho) * du[4] + 0.25 * als * hyy / (c * sqPiRho) * du[6] + 0.25 * als * hzz / (c * sqPiRho) * du[7];
-  al[6] = half * als * as / cc * du[1] + half * alf * af * hyy * sih / cc * du[2] + half * alf * af * hzz * sih / cc * du[3] +
-          half * als / (Rho * cc) * du[4] + -0.25 * alf * hyy / (c * sqPiRho) * du[6] + -0.25 * alf * hzz / (c * sqPiRho) * du[7];
-  al[7] = -half * als * as / cc * du[1] + -half * alf * af * hyy * sih / cc * du[2] + -half * alf * af * hzz * sih / cc * du[3] +
-          half * als / (Rho * cc) * du[4] + -0.25 * alf * hyy / (c * sqPiRho) * du[6] + -0.25 * alf * hzz / (c * sqPiRho) * du[7];
+  al[2] = -hzz * d_SQRT_2 * du[2] + hyy * d_SQRT_2 * du[3] + half * hzz * sih * iSq2Pi * du[6] + -half * hyy * sih * iSq2Pi * du[7];
+  al[3] = -hzz * d_SQRT_2 * du[2] + hyy * d_SQRT_2 * du[3] + -half * hzz * sih * iSq2Pi * du[6] + half * hyy * sih * iSq2Pi * du[7];
+  al[4] = half * alf * af * icc * du[1] + -half * als * as * hyy * sih * icc * du[2] + -half * als * as * hzz * sih * icc * du[3] +
+          half * alf * iccRho * du[4] + 0.25 * als * hyy * icSqPi * du[6] + 0.25 * als * hzz * icSqPi * du[7];
+  al[5] = -half * alf * af * icc * du[1] + half * als * as * hyy * sih * icc * du[2] + half * als * as * hzz * sih * icc * du[3] +
+          half * alf * iccRho * du[4] + 0.25 * als * hyy * icSqPi * du[6] + 0.25 * als * hzz * icSqPi * du[7];
+  al[6] = half * als * as * icc * du[1] + half * alf * af * hyy * sih * icc * du[2] + half * alf * af * hzz * sih * icc * du[3] +
+          half * als * iccRho * du[4] + -0.25 * alf * hyy * icSqPi * du[6] + -0.25 * alf * hzz * icSqPi * du[7];
+  al[7] = -half * als * as * icc * du[1] + -half * alf * af * hyy * sih * icc * du[2] + -half * alf * af * hzz * sih * icc * du[3] +
+          half * als * iccRho * du[4] + -0.25 * alf * hyy * icSqPi * du[6] + -0.25 * alf * hzz * icSqPi * du[7];
   if (CHECK) {
     // Walk the conservative wave fan in speed order (src/MHD_Roe8Wave.H:500-548).
     constexpr int order[8] = {5, 3, 7, 0, 1, 6, 2, 4};

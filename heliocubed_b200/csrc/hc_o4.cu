@@ -480,7 +480,7 @@ __device__ __forceinline__ const double* faceBasis(const Ctx& c, int b, int j, i
 // 4. reconstruction (WENOZ / WENO3 / PLM with clamps), Roe repair, energies,
 // point flux sum, total-pressure sum, centred normal B, Rusanov jump (F).
 template <int D>
-__global__ void __launch_bounds__(128, 5) o4FaceReconKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+__global__ void __launch_bounds__(128, 6) o4FaceReconKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
   const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
@@ -506,24 +506,29 @@ __global__ void __launch_bounds__(128, 5) o4FaceReconKernel(const Ctx* __restric
     value = dmin(value, th[cell[4]]);
     const double thR = dmin(value, th[cell[5]]);
     const bool smooth = thR > 0.5;
-    double l[8], r[8];
-#pragma unroll
+    // one copy of the reconstruction code for the eight components (a rolled
+    // loop; the states go through this thread's shared-memory column)
+    __shared__ double sLR[16][128];
+#pragma unroll 1
     for (int q = 0; q < 8; ++q) {
+      const double* Wq = WP + q * NG;
       double L, R;
       if (smooth) {
-        const double st[6] = {WP[q * NG + cell[0]], WP[q * NG + cell[1]], WP[q * NG + cell[2]],
-                              WP[q * NG + cell[3]], WP[q * NG + cell[4]], WP[q * NG + cell[5]]};
+        const double st[6] = {Wq[cell[0]], Wq[cell[1]], Wq[cell[2]], Wq[cell[3]], Wq[cell[4]], Wq[cell[5]]};
         wenozFace(st, L, R);
       } else {
-        const double st[4] = {WP[q * NG + cell[1]], WP[q * NG + cell[2]], WP[q * NG + cell[3]], WP[q * NG + cell[4]]};
+        const double st[4] = {Wq[cell[1]], Wq[cell[2]], Wq[cell[3]], Wq[cell[4]]};
         if (a.G.fallback == 0) weno3Face(st, dx2, L, R);
         else plmFallbackFace(st, L, R);
       }
       if (q == 0) { L = dmax(L, kRHO00); R = dmax(R, kRHO00); }
       if (q == 4) { L = dmax(L, 1.0e-12); R = dmax(R, 1.0e-12); }
-      l[q] = L;
-      r[q] = R;
+      sLR[q][threadIdx.x] = L;
+      sLR[8 + q][threadIdx.x] = R;
     }
+    double l[8], r[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { l[q] = sLR[q][threadIdx.x]; r[q] = sLR[8 + q][threadIdx.x]; }
     if (a.G.roe) {
       double cl[8], cr[8];
 #pragma unroll
@@ -707,7 +712,7 @@ __global__ void o4FaceRadialKernel(const Ctx* __restrict__ tab, const RegArgs rg
 // 8. pressure force, dissipation, combine on the final faces V0; writes the
 // flux (scratch and caller).
 template <int D>
-__global__ void __launch_bounds__(128, 4) o4FaceFinalKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+__global__ void __launch_bounds__(128, 6) o4FaceFinalKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
   const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
@@ -753,13 +758,22 @@ __global__ void __launch_bounds__(128, 4) o4FaceFinalKernel(const Ctx* __restric
 #pragma unroll
         for (int e = 0; e < 10; ++e) dM[q][e] = 0.5 * Ma[e] - 0.5 * Mb[e];
       }
+      // point-to-average and transverse differences of the eight point
+      // dissipations in a rolled loop through this thread's shared column
+      __shared__ double sQ[24][128];
+#pragma unroll 1
+      for (int q = 0; q < 8; ++q) {
+        const double pt = QD(q, i, j, k);
+        sQ[q][threadIdx.x] = sm ? pt + lapFace(QD, q, d, i, j, k) * (1.0 / 24.0) : pt;
+        sQ[8 + q][threadIdx.x] = cdiff(QD, q, t1, i, j, k);
+        sQ[16 + q][threadIdx.x] = cdiff(QD, q, t2, i, j, k);
+      }
       double avg[8], dP0[8], dP1[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        const double pt = QD(q, i, j, k);
-        avg[q] = sm ? pt + lapFace(QD, q, d, i, j, k) * (1.0 / 24.0) : pt;
-        dP0[q] = cdiff(QD, q, t1, i, j, k);
-        dP1[q] = cdiff(QD, q, t2, i, j, k);
+        avg[q] = sQ[q][threadIdx.x];
+        dP0[q] = sQ[8 + q][threadIdx.x];
+        dP1[q] = sQ[16 + q][threadIdx.x];
       }
       diss[0] = faceProd(M[9], avg[0], dM[0][9], dP0[0], dM[1][9], dP1[0]);
       diss[4] = faceProd(M[9], avg[4], dM[0][9], dP0[4], dM[1][9], dP1[4]);

@@ -570,7 +570,7 @@ __global__ void __launch_bounds__(128, 6) o4FaceReconKernel(const Ctx* __restric
 // 4b. pointwise factored Roe dissipation on the final faces + one transverse
 // ring (src/BoxOp_RoeCubedSphere.H:73-98).
 template <int D>
-__global__ void __launch_bounds__(128, 3) o4RoePointKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+__global__ void __launch_bounds__(128, 4) o4RoePointKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
   const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;

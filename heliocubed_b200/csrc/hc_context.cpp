@@ -707,6 +707,22 @@ int buildO4Level(hc_ctx* c) {
     const RadialRow rr = radialRow(P, i);
     radial[i + g + 1] = make_double2(rr.vol, rr.rhalf);
   }
+  // The inner analytic wind does not depend on time when its perturbation
+  // strength is zero: tabulate the inner radial ghosts once.
+  std::vector<double> inner;
+  if (P.init_condition_type == 1 && P.strength == 0.0) {
+    inner.resize((size_t)6 * nG * nG * g * 8);
+    for (int b = 0; b < 6; ++b)
+      for (int k = -g; k < na + g; ++k)
+        for (int j = -g; j < na + g; ++j) {
+          const size_t cell = ((size_t)b * nG + (k + g)) * nG + (j + g);
+          for (int i = -g; i < 0; ++i) {
+            const double radius = radial[i + g + 1].y;
+            const double X[3] = {radius * xhat[cell * 3], radius * xhat[cell * 3 + 1], radius * xhat[cell * 3 + 2]};
+            windNative(P, X, &inner[(cell * g + (i + g)) * 8]);
+          }
+        }
+  }
   cudaError_t err = cudaSuccess;
   O.coef = upload(coef, c->owned, err);
   O.detx = upload(detx, c->owned, err);
@@ -715,6 +731,7 @@ int buildO4Level(hc_ctx* c) {
   O.ringJK = upload(ringJK, c->owned, err);
   O.ringPt = upload(ringPt, c->owned, err);
   O.pts = upload(pts, c->owned, err);
+  O.inner = inner.empty() ? nullptr : upload(inner, c->owned, err);
   if (err != cudaSuccess) return cudaFail(err, "O4 level tables");
   return HC_OK;
 }

@@ -231,6 +231,7 @@ struct O4Level {
   const int2* ringJK;       // [nring]: (j, k) of each seam ghost position
   const int* ringPt;        // [nring][5]: points at the ghost centre and its 4 neighbours
   const O4Point* pts;       // [6][npts]
+  const double* inner;      // [6][nG][nG][g][8] inner radial ghosts when time independent, or null
   double gamma, r0, strength, cfl;
 };
 

@@ -49,21 +49,13 @@ __device__ __forceinline__ double detAt(const O4Level& O, int b, int j, int k) {
 }
 __device__ __forceinline__ double volAt(const O4Level& O, int i) { return O.radial[i + O.g + 1].x; }
 
-// 1. JU -> Cartesian averages, src/MHD_StateConversion.H:198-262.  Threads
-// run along the radial index, so a lane gets the angular quotients of its
-// radial neighbours from the neighbouring lanes (shuffles) and computes only
-// those its warp does not hold.
+// 1. JU -> Cartesian averages, src/MHD_StateConversion.H:198-262.
 __global__ void o4CartesianKernel(const O4StageIO io) {
   const O4Level& O = io.O;
   const long n = 6L * O.Nv;
-  const int lane = threadIdx.x & 31;
-  const long stride = (long)gridDim.x * blockDim.x;
-  // warp-uniform trip count: every lane takes part in the shuffles
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t - lane < n; t += stride) {
-    const bool act = t < n;
-    const long tt = act ? t : n - 1;
-    const int b = (int)(tt / O.Nv);
-    const long r = tt - (long)b * O.Nv;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int b = (int)(t / O.Nv);
+    const long r = t - (long)b * O.Nv;
     const int i = (int)(r % O.nr);
     const int j = (int)((r / O.nr) % O.na);
     const int k = (int)(r / ((long)O.nr * O.na));
@@ -100,39 +92,22 @@ __global__ void o4CartesianKernel(const O4StageIO io) {
     for (int q = 0; q < 3; ++q) invV[q] = 1.0 / volAt(O, ia + q);
     const double dv = 0.5 * (volAt(O, i + 1) - volAt(O, i - 1));
     const int slot = i - ia;
-    // lane offset of the window's cells, and whether that lane holds them
-    // (same column: consecutive threads of one column are consecutive i)
-    bool have[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      const int off = ia + q - i;
-      have[q] = lane + off >= 0 && lane + off < 32 && t + off < n;
-    }
     for (int c = 0; c < 8; ++c) {
-      auto angular = [&](int ii) {
+      double dq = 0.0, angI = 0.0;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int ii = ia + q;
         double d1 = 0.0, d2 = 0.0;
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
           d1 += wj[m] * (io.ju[vIdx(O, b, c, ii, ja + m, k)] * invJ[m]);
           d2 += wk[m] * (io.ju[vIdx(O, b, c, ii, j, ka + m)] * invK[m]);
         }
-        return (io.ju[vIdx(O, b, c, ii, j, k)] - (d1 * dd1 + d2 * dd2) * (1.0 / 12.0)) * invDet;
-      };
-      const double own = angular(i);
-      const double up1 = __shfl_down_sync(0xffffffffu, own, 1), up2 = __shfl_down_sync(0xffffffffu, own, 2);
-      const double dn1 = __shfl_up_sync(0xffffffffu, own, 1), dn2 = __shfl_up_sync(0xffffffffu, own, 2);
-      double dq = 0.0;
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const int off = ia + q - i;
-        double ang = own;
-        if (off != 0) {
-          ang = off == 1 ? up1 : off == 2 ? up2 : off == -1 ? dn1 : dn2;
-          if (!have[q]) ang = angular(ia + q);
-        }
+        const double ang = (io.ju[vIdx(O, b, c, ii, j, k)] - (d1 * dd1 + d2 * dd2) * (1.0 / 12.0)) * invDet;
         dq += wr[q] * (ang * invV[q]);
+        if (q == slot) angI = ang;
       }
-      if (act) io.cart[cIdx(O, b, c, i, j, k)] = (own - dq * dv * (1.0 / 12.0)) * invV[slot];
+      io.cart[cIdx(O, b, c, i, j, k)] = (angI - dq * dv * (1.0 / 12.0)) * invV[slot];
     }
   }
 }

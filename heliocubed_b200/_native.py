@@ -40,6 +40,8 @@ SIGNATURES = {
     "hc_level_valid": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hc_level_init": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hc_geometry_export": (C.c_long, [_VP, C.c_int, _VP]),
+    "hc_cone_prepare": (C.c_int, [_VP, C.c_double, _VP]),
+    "hc_level_insert_cone": (C.c_int, [_VP, _VP, C.c_double, _VP, _VP, _VP]),
 }
 
 
@@ -75,6 +77,21 @@ class HcInit(C.Structure):
 class HcBoxWork(C.Structure):
     """Mirror of hc_box_work in include/hc_abi.h."""
     _fields_ = [("box", HcBox), ("usph", C.c_void_p), ("rhs", C.c_void_p), ("flux", C.c_void_p * 3)]
+
+
+_CONE_SPEC = ("lat_deg", "lon_deg", "half_angle_deg", "apex_speed", "wind_speed", "drag_gamma",
+              "reference_height", "reference_time", "density", "temperature")
+_CONE = ("radius", "entry_shift", "entry_time", "speed", "end_time", "insertion_time", "density", "temperature")
+
+
+class HcConeSpec(C.Structure):
+    """Mirror of hc_cone_spec in include/hc_abi.h."""
+    _fields_ = [(n, C.c_double) for n in _CONE_SPEC] + [("reserved", C.c_double * 6)]
+
+
+class HcCone(C.Structure):
+    """Mirror of hc_cone in include/hc_abi.h."""
+    _fields_ = [("axis", C.c_double * 3)] + [(n, C.c_double) for n in _CONE] + [("reserved", C.c_double * 6)]
 
 
 class HcError(RuntimeError):

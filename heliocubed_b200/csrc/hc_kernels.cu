@@ -496,7 +496,7 @@ __global__ void validKernel(const DevLevel L, const double* __restrict__ ju, int
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(ok, 0);
 }
 
-// Seeded synthetic initial state, kind 1 (formula in hc_abi.h / DESIGN.md).
+// Seeded synthetic initial state, kind 1 (the formulas are in hc_abi.h, hc_init).
 struct InitArgs {
   int kind, pb, pi, pj, pk;
   double rho0, p0, vr, b0, r_ref, amp, width;

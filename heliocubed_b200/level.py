@@ -202,6 +202,45 @@ def wind_box_state(params: Params, lo, hi, ghost: int, seed: int, spec: "InitSpe
     return np.ascontiguousarray(U.reshape(-1))
 
 
+@dataclass
+class ConeSpec:
+    """Fitted parameters of a finite cone-CME cloud (hc_cone_spec; the
+    reference's CMEParameters of field model 4 with an analytic cone)."""
+    lat_deg: float = 0.0
+    lon_deg: float = 0.0
+    half_angle_deg: float = 30.0
+    apex_speed: float = 1200.0          # km/s at reference_time
+    wind_speed: float = 400.0           # km/s (drag-based model)
+    drag_gamma: float = 0.0             # 1/km (0: ballistic)
+    reference_height: float = 21.5      # leading edge at reference_time, solar radii
+    reference_time: float = 0.0         # s
+    density: float = 4 * 700.0 * C_MP   # g/cm^3
+    temperature: float = 1.0e6          # K
+
+    def to_c(self) -> N.HcConeSpec:
+        s = N.HcConeSpec()
+        for k in N._CONE_SPEC:
+            setattr(s, k, getattr(self, k))
+        return s
+
+    @classmethod
+    def on_inner_boundary(cls, inner_radius: float, **kw) -> "ConeSpec":
+        """A cloud that lies wholly inside the shell at reference_time,
+        touching the inner boundary: leading edge at r_inner (1 + 2 sin a)."""
+        spec = cls(**kw)
+        a = np.sin(np.radians(spec.half_angle_deg))
+        spec.reference_height = inner_radius * (1.0 + 2.0 * a) / C_SR
+        return spec
+
+
+def prepare_cone(spec: ConeSpec, inner_radius: float) -> N.HcCone:
+    """hc_cone_prepare: the cloud's geometry and timing (host arithmetic)."""
+    out = N.HcCone()
+    s = spec.to_c()
+    N.check(N.lib().hc_cone_prepare(C.byref(s), inner_radius, C.byref(out)), "hc_cone_prepare")
+    return out
+
+
 def _ptr(t: torch.Tensor | None):
     if t is None:
         return None
@@ -277,6 +316,14 @@ class Shell:
         dvolr = self.geometry(0).reshape(p.nr + 1, 4)[:p.nr, 3]
         ju = perturbed_wind_state(p, det, dvolr, seed, amp)
         return torch.from_numpy(np.ascontiguousarray(ju.reshape(-1))).to(self._dev)
+
+    def insert_cone(self, cone: N.HcCone, time: float, ju: torch.Tensor, stats: bool = False) -> torch.Tensor | None:
+        """Volume insertion of a prepared cone cloud into `ju` at `time`
+        (hc_level_insert_cone); with `stats` a device tensor [cells, grams]."""
+        out = torch.zeros(2, dtype=torch.float64, device=self._dev) if stats else None
+        N.check(self._lib.hc_level_insert_cone(self._ctx, C.byref(cone), time, _ptr(ju), _ptr(out), _stream()),
+                "hc_level_insert_cone")
+        return out
 
     def prepare(self, ju: torch.Tensor, t: float = 0.0, w: torch.Tensor | None = None) -> torch.Tensor:
         w = self.new_primitive() if w is None else w

@@ -75,7 +75,11 @@ typedef struct hc_box {
 
 /* Seeded synthetic initial states (the configs' own inputs; the reference
  * defines no such problem).  kind 1: Parker-like wind + Gaussian pressure
- * pulse; see DESIGN.md for the formulas. */
+ * pulse.  With s = r_ref / r at the cell-centre radius and X the cell-centre
+ * unit direction: rho = rho0 s^2, v = vr X, p = p0 s^(2 gamma) (1 + amp
+ * exp(-d^2 / (2 w^2))), B = b0 s^2 sign(X_z) X; d^2 = (i - pulse_i)^2 +
+ * (angle to the pulse cell's direction / angular cell width)^2.  JU = J U
+ * with J = dVolr <det A> of the cell. */
 typedef struct hc_init {
   int kind;
   int pulse_block, pulse_i, pulse_j, pulse_k;
@@ -235,6 +239,59 @@ int hc_level_valid(hc_ctx* ctx, const double* ju, int* ok, void* stream);
 
 /* Seeded synthetic initial state (valid cells) of the level. */
 int hc_level_init(hc_ctx* ctx, const hc_init* init, double* ju, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Cone CME, finite spherical cloud (CME field model 4, the analytic cone of
+ * src/MHD_ImportedCME.H:415-420 prepared by src/MHD_CME.H:1111-1136).
+ * ------------------------------------------------------------------------- */
+
+/* Fitted cone parameters (the reference's CMEParameters fields for a
+ * finite cone: lat, lon, halfangle, apex_speed, windSpeed, dragGamma, r1
+ * (r0 = 0), referenceTime, density, temperature). */
+typedef struct hc_cone_spec {
+  double lat_deg, lon_deg;   /* axis = orientation(lat, lon, 0) (0,0,1): (cos lat cos lon, cos lat sin lon, sin lat) */
+  double half_angle_deg;     /* cloud radius a = r_inner sin(half angle) */
+  double apex_speed;         /* km/s at reference_time */
+  double wind_speed;         /* km/s, drag-based model ambient speed */
+  double drag_gamma;         /* 1/km, drag-based model coefficient (0: ballistic), >= 0 */
+  double reference_height;   /* leading-edge height at reference_time, solar radii (6.96e10 cm) */
+  double reference_time;     /* s */
+  double density;            /* total cloud density, g/cm^3 */
+  double temperature;        /* K (equal proton and electron temperature) */
+  double reserved[6];
+} hc_cone_spec;
+
+/* The prepared cloud: a sphere of radius `radius` whose centre moves along
+ * `axis` at `speed`, its centre at distance entry_shift + speed (t -
+ * entry_time) from the origin.  It touches the inner boundary first at
+ * entry_time; the inner boundary feeds it while insertion_time <= t <
+ * end_time (src/MHD_CME.H:968). */
+typedef struct hc_cone {
+  double axis[3];
+  double radius;             /* cm */
+  double entry_shift;        /* cm: r_inner - radius */
+  double entry_time;         /* s */
+  double speed;              /* km/s, the drag-based speed at entry_time */
+  double end_time;           /* s: entry_time + 2 radius / speed */
+  double insertion_time;     /* s: volume insertion time (reference height reached) */
+  double density, temperature;
+  double reserved[6];
+} hc_cone;
+
+/* Host function (no device work): prepareConeCloud with the drag-based
+ * trajectory and boundary-contact bisection (src/MHD_CME.H:1069-1136) for
+ * the level's inner radius (cm).  HC_ERR_ARG where the reference throws
+ * (no outward trajectory to the inner boundary). */
+int hc_cone_prepare(const hc_cone_spec* spec, double inner_radius, hc_cone* cone);
+
+/* Volume insertion of the cloud at `time` into the level state JU (valid
+ * cells, device): every cell whose centre lies inside the cloud takes the
+ * cloud's density, radial velocity `speed` and pressure 2 k T rho / m_p,
+ * keeping its magnetic field (Insert_CME for cones,
+ * src/BoxOp_EulerCubedSphereImplem.H:1236-1300, at either order).
+ * stats (device, nullable): [0] cells changed, [1] mass added (g), summed
+ * in a fixed order. */
+int hc_level_insert_cone(hc_ctx* ctx, const hc_cone* cone, double time, double* ju, double* stats, void* stream);
 
 /* Host copies of the level geometry used by the kernels, for tests:
  * what = 0 radial line [nr+1][4]: rlow^2, (rhigh^2-rlow^2)/(2dxi0),

@@ -4,7 +4,8 @@
   -ffp-contract=off, OpenMP.  Built wherever the package is built and carried
   to the GPU box with the repository snapshot.
 * oracle/_ref/libhcref.so -- the reference's own standalone headers
-  (src/MHD_Roe8Wave.H, src/MHD_Reconstruction.H, src/MHD_SecondOrderFlux.H)
+  (src/MHD_Roe8Wave.H, src/MHD_Reconstruction.H, src/MHD_SecondOrderFlux.H,
+  src/MHD_CME.H with the headers it includes)
   compiled from the reference tree where it lies, through ref_pin.cpp.  Built
   only when the reference tree is present; the generated Proto_Accel.H is a
   two-line stub of our own (the reference's Proto dependency is absent).
@@ -57,8 +58,9 @@ def build_reference_pin(reference: str = DEFAULT_REFERENCE, force: bool = False)
         f.write("#pragma once\n#define ACCEL_DECORATION\n")
     src = os.path.join(HERE, "ref_pin.cpp")
     out = os.path.join(outdir, "libhcref.so")
-    deps = [src, os.path.join(refsrc, "MHD_Roe8Wave.H"), os.path.join(refsrc, "MHD_SecondOrderFlux.H"),
-            os.path.join(refsrc, "MHD_Reconstruction.H")]
+    deps = [src] + [os.path.join(refsrc, h) for h in (
+        "MHD_Roe8Wave.H", "MHD_SecondOrderFlux.H", "MHD_Reconstruction.H", "MHD_CME.H", "MHD_ImportedCME.H",
+        "MHD_Time.H", "MHD_JSON.H", "MHD_Constants.H")]
     if force or _stale(out, deps):
         # -iquote keeps the stub ahead of any other Proto_Accel.H; the reference
         # headers are compiled where they lie.

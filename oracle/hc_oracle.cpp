@@ -1148,6 +1148,154 @@ void levelInit(const Level& L, const hc_init& in, double* ju) {
       }
 }
 
+// ---------------------------------------------------------------------------
+// Finite cone cloud (CME field model 4).
+// Preparation: drag-based trajectory src/MHD_CME.H:1069-1085, boundary
+// contact :1087-1110, prepareConeCloud :1111-1136, the analytic cone's axis
+// orientation(lat, lon, 0) (0,0,1) of src/MHD_ImportedCME.H:72-79,415-418.
+// Per cell: sample() for the finite cloud :995-1018 at the shift of
+// expandedSource :1139-1143, increment() / thermalPressure() :1197-1238,
+// applied as Insert_CME does for cones (src/BoxOp_EulerCubedSphereImplem.H:
+// 1236-1300).
+// ---------------------------------------------------------------------------
+constexpr double c_SR = 69600000000.0;   // src/MHD_Constants.H:4
+constexpr double kBoltzmann = 1.380649e-16;
+constexpr double kPiCme = 3.1415926535897932384626433832795;
+
+struct ConeTrajectory {
+  double apex, wind, drag, height, reference;
+};
+
+bool coneTrajectory(const ConeTrajectory& c, double elapsed, double& height, double& speed) {
+  const double dv = c.apex - c.wind;
+  double distance = c.apex * elapsed;
+  speed = c.apex;
+  if (c.drag > 0 && dv != 0) {
+    const double argument = c.drag * std::abs(dv) * elapsed;
+    if (!(argument > -1)) return false;
+    distance = c.wind * elapsed + std::copysign(1., dv) * std::log1p(argument) / c.drag;
+    speed = c.wind + dv / (1 + argument);
+  }
+  height = c.height + 0.0 + distance * 1e5 / c_SR;
+  return std::isfinite(height) && std::isfinite(speed) && speed > 0;
+}
+
+// Time at which the leading edge reaches the inner boundary; false where the
+// reference throws.
+bool coneBoundaryStart(const ConeTrajectory& c, double innerRsun, double& start) {
+  double lower = -(c.height + 0.0 - innerRsun) * c_SR / (c.apex * 1e5), upper = 0;
+  const double dv = c.apex - c.wind;
+  if (c.drag == 0 || dv == 0) {
+    start = c.reference + lower;
+    return true;
+  }
+  if (c.drag > 0 && dv != 0) {
+    if (dv > 0)
+      lower = -(1 - 1e-12) / (c.drag * dv);
+    else
+      lower = (std::abs(dv) / c.wind - 1) / (c.drag * std::abs(dv));
+  }
+  double height, speed;
+  if (!coneTrajectory(c, lower * (1 - 1e-12), height, speed) || height > innerRsun + 1e-8) return false;
+  lower *= 1 - 1e-12;
+  for (int i = 0; i < 100; ++i) {
+    const double mid = .5 * (lower + upper);
+    if (!coneTrajectory(c, mid, height, speed) || height < innerRsun)
+      lower = mid;
+    else
+      upper = mid;
+  }
+  start = c.reference + .5 * (lower + upper);
+  return true;
+}
+
+int conePrepare(const hc_cone_spec& s, double innerRadius, hc_cone& o) {
+  const double innerRsun = innerRadius / c_SR;
+  const ConeTrajectory c{s.apex_speed, s.wind_speed, s.drag_gamma, s.reference_height, s.reference_time};
+  double entry, height, speed;
+  if (!coneBoundaryStart(c, innerRsun, entry)) return -1;
+  if (!coneTrajectory(c, entry - c.reference, height, speed)) return -2;
+  std::memset(&o, 0, sizeof(o));
+  const double inner = innerRsun * c_SR;
+  const double lat = s.lat_deg * kPiCme / 180, lon = s.lon_deg * kPiCme / 180;
+  const double alpha = s.half_angle_deg * kPiCme / 180;
+  o.axis[0] = std::cos(lon) * std::cos(lat);
+  o.axis[1] = -(-std::sin(lon) * std::cos(lat));
+  o.axis[2] = std::sin(lat);
+  o.radius = inner * std::sin(alpha);
+  o.entry_time = entry;
+  o.speed = speed;
+  o.entry_shift = inner - o.radius;
+  const double referenceShift = (s.reference_height + 0.0) * c_SR - o.radius;
+  o.end_time = entry + 2 * o.radius / (speed * 1e5);
+  o.insertion_time = entry + (referenceShift - o.entry_shift) / (speed * 1e5);
+  o.density = s.density;
+  o.temperature = s.temperature;
+  return 0;
+}
+
+// The conserved change of one cell at Cartesian position `pos` (cm) with
+// Cartesian primitive ambient state `old`; false outside the cloud.
+bool coneCellDelta(const hc_cone& c, double shift, const double pos[3], const double old[8], double gamma,
+                   double delta[8]) {
+  const double q[3] = {pos[0] - shift * c.axis[0], pos[1] - shift * c.axis[1], pos[2] - shift * c.axis[2]};
+  if (std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) > c.radius) return false;
+  const double radius = std::sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]) / c_SR;
+  if (!(radius > 0)) return false;
+  double v[3];
+  for (int d = 0; d < 3; ++d) v[d] = c.speed * 1e5 * pos[d] / (c_SR * radius);
+  const double weight = 1;  // volume insertion: plasmaWeight 1
+  const double density = (1 - weight) * old[0] + weight * c.density;
+  double oldKinetic = 0, newKinetic = 0, oldMagnetic = 0, newMagnetic = 0;
+  delta[0] = density - old[0];
+  for (int d = 0; d < 3; ++d) {
+    delta[1 + d] = density * v[d] - old[0] * old[1 + d];
+    delta[5 + d] = 0.0;
+    oldKinetic += .5 * old[0] * old[1 + d] * old[1 + d];
+    newKinetic += .5 * density * v[d] * v[d];
+    oldMagnetic += old[5 + d] * old[5 + d] / (8 * kPiCme);
+    newMagnetic += (old[5 + d] + 0.0) * (old[5 + d] + 0.0) / (8 * kPiCme);
+  }
+  const double target = 2 * kBoltzmann * c.temperature * c.density / c_MP;
+  const double pressure = (1 - weight) * std::max(0., old[4]) + weight * target;
+  const double addedPressure = pressure - std::max(0., old[4]);
+  delta[4] = addedPressure / (gamma - 1) + newKinetic - oldKinetic + newMagnetic - oldMagnetic;
+  return true;
+}
+
+void levelInsertCone(const Level& L, const hc_cone& c, double time, double* ju, double stats[2]) {
+  LevelArrays I(L);
+  const int nr = L.nr, na = L.na;
+  const double shift = c.entry_shift + c.speed * 1e5 * (time - c.entry_time);
+  const double dx0 = 1.0 / nr, dx1 = L.h;
+  long long affected = 0;
+  double added = 0;
+  for (int b = 0; b < 6; ++b)
+    for (int k = 0; k < na; ++k)
+      for (int j = 0; j < na; ++j) {
+        LD Xl[3];
+        unitPoint(b, (j + 0.5L) * L.h, (k + 0.5L) * L.h, Xl);
+        const double X[3] = {(double)Xl[0], (double)Xl[1], (double)Xl[2]};
+        const double det = L.det[L.cellIdx(b, j, k)];
+        for (int i = 0; i < nr; ++i) {
+          const Radial& r = L.rad(i);
+          const double pos[3] = {r.rad * X[0], r.rad * X[1], r.rad * X[2]};
+          const double J = r.vol * det;
+          double u[8], w[8], delta[8];
+          for (int q = 0; q < NC; ++q) u[q] = ju[I.v(b, q, i, j, k)];
+          cartesianPrimitiveFromConserved(w, u, 1.0 / J, L.P.gamma);
+          if (!coneCellDelta(c, shift, pos, w, L.P.gamma, delta)) continue;
+          for (int q = 0; q < NC; ++q) ju[I.v(b, q, i, j, k)] += J * delta[q];
+          ++affected;
+          added += delta[0] * (J * dx0 * dx1 * dx1);
+        }
+      }
+  if (stats) {
+    stats[0] = (double)affected;
+    stats[1] = added;
+  }
+}
+
 #include "hc_oracle_o4.inc"
 
 }  // namespace
@@ -1203,6 +1351,19 @@ int orc_level_rk4_step(void* L, double* ju, double dt, double t) { levelRk4(*sta
 double orc_level_inv_dt(void* L, const double* ju) { return levelInvDt(*static_cast<Level*>(L), ju); }
 int orc_level_valid(void* L, const double* ju) { return levelValid(*static_cast<Level*>(L), ju); }
 int orc_level_init(void* L, const hc_init* in, double* ju) { levelInit(*static_cast<Level*>(L), *in, ju); return 0; }
+int orc_cone_prepare(const hc_cone_spec* spec, double inner_radius, hc_cone* out) {
+  return conePrepare(*spec, inner_radius, *out);
+}
+// One cell of the insertion: 1 and delta[8] when `pos` lies in the cloud at `time`.
+int orc_cone_cell(const hc_cone* c, double time, const double* pos, const double* ambient, double gamma,
+                  double* delta) {
+  const double shift = c->entry_shift + c->speed * 1e5 * (time - c->entry_time);
+  return coneCellDelta(*c, shift, pos, ambient, gamma, delta) ? 1 : 0;
+}
+int orc_level_insert_cone(void* L, const hc_cone* c, double time, double* ju, double* stats) {
+  levelInsertCone(*static_cast<Level*>(L), *c, time, ju, stats);
+  return 0;
+}
 
 // Geometry export in the layout of hc_geometry_export.
 long orc_geometry(void* Lp, int what, double* out) {

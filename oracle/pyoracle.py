@@ -43,6 +43,22 @@ class HcInit(C.Structure):
     ]
 
 
+CONE_SPEC_FIELDS = ("lat_deg", "lon_deg", "half_angle_deg", "apex_speed", "wind_speed", "drag_gamma",
+                    "reference_height", "reference_time", "density", "temperature")
+CONE_FIELDS = ("radius", "entry_shift", "entry_time", "speed", "end_time", "insertion_time", "density",
+               "temperature")
+
+
+class HcConeSpec(C.Structure):
+    """Mirror of hc_cone_spec in include/hc_abi.h."""
+    _fields_ = [(n, C.c_double) for n in CONE_SPEC_FIELDS] + [("reserved", C.c_double * 6)]
+
+
+class HcCone(C.Structure):
+    """Mirror of hc_cone in include/hc_abi.h."""
+    _fields_ = [("axis", C.c_double * 3)] + [(n, C.c_double) for n in CONE_FIELDS] + [("reserved", C.c_double * 6)]
+
+
 def dptr(a: np.ndarray):
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(_D)
@@ -84,6 +100,9 @@ def lib() -> C.CDLL:
         L.orc_face_flux.argtypes = [_D, _D, _D, C.c_double, C.c_double, C.c_double, C.c_int, _D]
         L.orc_plm.argtypes = [_D, _D, _D, _D, C.c_int, _D, _D]
         L.orc_cart_prim.argtypes = [_D, C.c_double, C.c_double, _D]
+        L.orc_cone_prepare.argtypes = [C.POINTER(HcConeSpec), C.c_double, C.POINTER(HcCone)]
+        L.orc_cone_cell.argtypes = [C.POINTER(HcCone), C.c_double, _D, _D, C.c_double, _D]
+        L.orc_level_insert_cone.argtypes = [C.c_void_p, C.POINTER(HcCone), C.c_double, _D, _D]
         L.orc_o4_level_create.restype = C.c_void_p
         L.orc_o4_level_create.argtypes = [C.c_void_p]
         L.orc_o4_level_destroy.argtypes = [C.c_void_p]
@@ -115,6 +134,8 @@ def ref_lib() -> C.CDLL | None:
         L.ref_mapped_roe.argtypes = [_D, _D, _D, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, _D]
         L.ref_factored_roe.argtypes = [_D, _D, _D, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, _D]
         L.ref_usable_primitive.argtypes = [_D, C.c_double]
+        L.ref_cone_prepare.argtypes = [_D, C.c_double, _D]
+        L.ref_cone_cell.argtypes = [_D, C.c_double, C.c_double, _D, _D, C.c_double, _D]
         _ref = L
     return _ref
 
@@ -174,6 +195,12 @@ class OracleLevel:
         w = np.zeros(self.ng)
         self.L.orc_level_prepare(self.h, dptr(ju), dptr(w), t)
         return w
+
+    def insert_cone(self, cone: HcCone, time: float, ju: np.ndarray) -> np.ndarray:
+        """Cone volume insertion into ju (in place); returns [cells, grams]."""
+        stats = np.zeros(2)
+        self.L.orc_level_insert_cone(self.h, C.byref(cone), time, dptr(ju), dptr(stats))
+        return stats
 
     def rhs(self, w: np.ndarray) -> np.ndarray:
         k = np.zeros(self.nv)
@@ -263,3 +290,39 @@ class OracleLevelO4:
 
     def inv_dt(self, ju: np.ndarray) -> float:
         return self.L.orc_o4_inv_dt(self.h, dptr(ju))
+
+
+def cone_prepare(spec: HcConeSpec, inner_radius: float) -> HcCone | None:
+    """The oracle's prepareConeCloud restatement (None where it fails)."""
+    out = HcCone()
+    return out if lib().orc_cone_prepare(C.byref(spec), inner_radius, C.byref(out)) == 0 else None
+
+
+def cone_cell(cone: HcCone, time: float, pos, ambient, gamma: float):
+    """(inside, delta[8]) of one cell of the oracle's cone insertion."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    amb = np.ascontiguousarray(ambient, dtype=np.float64)
+    delta = np.zeros(8)
+    inside = lib().orc_cone_cell(C.byref(cone), time, dptr(pos), dptr(amb), gamma, dptr(delta))
+    return bool(inside), delta
+
+
+def ref_cone_prepare(spec: HcConeSpec, inner_radius: float) -> np.ndarray | None:
+    """The reference's prepareConeCloud (src/MHD_CME.H) compiled from source:
+    [axis(3), radius, entry shift, entry time, speed, end time, insertion time]."""
+    R = ref_lib()
+    vec = np.array([getattr(spec, k) for k in CONE_SPEC_FIELDS])
+    out = np.zeros(9)
+    return out if R.ref_cone_prepare(dptr(vec), inner_radius / 6.96e10, dptr(out)) == 0 else None
+
+
+def ref_cone_cell(spec: HcConeSpec, inner_radius: float, time: float, pos, ambient, gamma: float):
+    """(inside, delta[8]) of the reference's sample + loadDensity + increment."""
+    R = ref_lib()
+    vec = np.array([getattr(spec, k) for k in CONE_SPEC_FIELDS])
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    amb = np.ascontiguousarray(ambient, dtype=np.float64)
+    delta = np.zeros(8)
+    rc = R.ref_cone_cell(dptr(vec), inner_radius / 6.96e10, time, dptr(pos), dptr(amb), gamma, dptr(delta))
+    assert rc >= 0
+    return bool(rc), delta

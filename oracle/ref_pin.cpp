@@ -8,6 +8,10 @@
 //                             mappedRoe8WaveDissipation, factoredRoe8WaveDissipation
 //   src/MHD_Reconstruction.H  complete-state guards
 //   src/MHD_SecondOrderFlux.H secondOrderFrame, secondOrderFaceFlux
+// and the cone-CME model, which needs only the standard library:
+//   src/MHD_CME.H             prepareConeCloud, expandedSource, sample,
+//                             loadDensity, increment (with MHD_ImportedCME.H
+//                             analyticCone, MHD_Time.H, MHD_JSON.H)
 // The output library oracle/_ref/libhcref.so is git-ignored and is used by
 // tests/test_oracle_pin.py to pin the oracle restatement.
 
@@ -19,6 +23,7 @@ using std::min;
 #include "MHD_Roe8Wave.H"
 #include "MHD_Reconstruction.H"
 #include "MHD_SecondOrderFlux.H"
+#include "MHD_CME.H"
 
 namespace {
 struct Arr8 {
@@ -75,5 +80,70 @@ void ref_factored_roe(const double* wl, const double* wr, const double* A9, doub
 int ref_usable_primitive(const double* w, double floor) {
   CArr8 s{w};
   return MHD_Reconstruction::usablePrimitiveState<8>(s, floor) ? 1 : 0;
+}
+
+namespace {
+// spec: lat, lon, half angle (deg), apex speed, wind speed (km/s), drag
+// (1/km), reference height (Rsun), reference time (s), density, temperature.
+CMEParameters coneSource(const double* spec) {
+  CMEParameters c;
+  c.fieldModel = 4;
+  c.lat = spec[0];
+  c.lon = spec[1];
+  c.halfangle = spec[2];
+  c.apex_speed = spec[3];
+  c.windSpeed = spec[4];
+  c.dragGamma = spec[5];
+  c.r1 = spec[6];
+  c.r0 = 0;
+  c.referenceTime = spec[7];
+  c.insertionTime = spec[7];
+  c.density = spec[8];
+  c.temperature = spec[9];
+  c.imported = ImportedCME::Model::analyticCone(spec[6], spec[2], spec[0], spec[1], CalendarEpoch{2024, 0.0L});
+  return c;
+}
+}  // namespace
+
+// prepareConeCloud; out: axis[3], radius, entry shift, entry time, speed,
+// end time, insertion time.  Returns -1 where the reference throws.
+int ref_cone_prepare(const double* spec, double innerRsun, double* out) {
+  CMEParameters c = coneSource(spec);
+  try {
+    CMEModel::prepareConeCloud(c, innerRsun);
+  } catch (const std::exception&) {
+    return -1;
+  }
+  for (int d = 0; d < 3; ++d) out[d] = c.cloudAxis[d];
+  out[3] = c.cloudSphereRadius;
+  out[4] = c.cloudEntryShift;
+  out[5] = c.cloudEntryTime;
+  out[6] = c.cloudSpeed;
+  out[7] = c.cloudEndTime;
+  out[8] = c.insertionTime;
+  return 0;
+}
+
+// The cone branch of Insert_CME for one cell: expandedSource at `time`,
+// sample at `pos`, loadDensity and increment on the Cartesian primitive
+// ambient state.  Returns 1 and delta[8] inside the cloud.
+int ref_cone_cell(const double* spec, double innerRsun, double time, const double* pos, const double* ambient,
+                  double gamma, double* delta) {
+  CMEParameters c = coneSource(spec);
+  try {
+    CMEModel::prepareConeCloud(c, innerRsun);
+  } catch (const std::exception&) {
+    return -1;
+  }
+  CMEParameters current;
+  if (!CMEModel::expandedSource(c, time, current)) return 0;
+  CMEModel::Sample source;
+  if (!CMEModel::sample(current, {pos[0], pos[1], pos[2]}, source)) return 0;
+  std::array<double, 8> a;
+  for (int q = 0; q < 8; ++q) a[q] = ambient[q];
+  CMEModel::loadDensity(source, a);
+  const auto change = CMEModel::increment(a, source, gamma, current.plasmaBeta);
+  for (int q = 0; q < 8; ++q) delta[q] = change[q];
+  return 1;
 }
 }

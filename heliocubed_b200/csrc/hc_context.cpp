@@ -697,6 +697,9 @@ int buildO4Level(hc_ctx* c) {
       const long double u1 = (long double)y1 / h, u2 = (long double)y2 / h;
       pt.j0 = std::max(0, std::min(na - 4, (int)std::floor((double)u1) - 1));
       pt.k0 = std::max(0, std::min(na - 4, (int)std::floor((double)u2) - 1));
+      const int jc = std::max(0, std::min(na - 1, (int)std::floor((double)u1)));
+      const int kc = std::max(0, std::min(na - 1, (int)std::floor((double)u2)));
+      pt.cell = (jc - pt.j0) | ((kc - pt.k0) << 2);
       averageInterp(u1, pt.j0, pt.wj, 1.0L);
       averageInterp(u2, pt.k0, pt.wk, 1.0L);
       pts[(size_t)b * O.npts + q] = pt;

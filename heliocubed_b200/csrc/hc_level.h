@@ -212,9 +212,10 @@ constexpr int kO4Cart = 6;  // angular ghost layers of the Cartesian averages
 
 // One interpolation point of the seam ghosts: the point value at a cell
 // centre of the ghost panel's grid from panel p's 4 x 4 donor cell averages
-// starting at (j0, k0), tensor weights wj and wk.
+// starting at (j0, k0), tensor weights wj and wk.  cell: the donor cell that
+// contains the point, (j0 + (cell & 3), k0 + (cell >> 2)).
 struct O4Point {
-  int p, j0, k0, pad;
+  int p, j0, k0, cell;
   double wj[4], wk[4];
 };
 

@@ -145,7 +145,11 @@ __global__ void o4SeamPointKernel(const O4StageIO io) {
 
 // 2b. Seam ghost averages: (5/6) U(centre) + (1/24) sum of U at the four
 // neighbouring centres, a fourth-order cell average in the ghost panel's
-// coordinates.
+// coordinates.  An inadmissible average (non-finite, density below RHO00 or
+// negative thermal energy: a jump, where the linear stencil overshoots)
+// takes the average of the donor cell containing the ghost centre, the
+// fallback of the reference's AMR ghost interpolation (src/MHD_AMR.H:
+// 1382-1391).
 __global__ void o4SeamKernel(const O4StageIO io) {
   const O4Level& O = io.O;
   const long n = 6L * O.nring * O.nr;
@@ -158,12 +162,29 @@ __global__ void o4SeamKernel(const O4StageIO io) {
     const int* pt = O.ringPt + (long)pos * 5;
     const double* pv = io.pv + (long)b * 8 * O.npts * O.nr + i;
     const long cs = (long)O.npts * O.nr;
+    double u[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       const double* v = pv + c * cs;
       const double nb = (v[(long)pt[1] * O.nr] + v[(long)pt[2] * O.nr]) + (v[(long)pt[3] * O.nr] + v[(long)pt[4] * O.nr]);
-      io.cart[cIdx(O, b, c, i, jk.x, jk.y)] = (5.0 / 6.0) * v[(long)pt[0] * O.nr] + (1.0 / 24.0) * nb;
+      u[c] = (5.0 / 6.0) * v[(long)pt[0] * O.nr] + (1.0 / 24.0) * nb;
     }
+    bool valid = true;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) valid &= isfinite(u[c]);
+    double thermal = u[4];
+    if (u[0] > 0) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) thermal -= 0.5 * u[1 + d] * u[1 + d] / u[0] + u[5 + d] * u[5 + d] / (8 * kPi);
+    }
+    if (!(valid && u[0] >= kRHO00 && thermal >= 0 && isfinite(thermal))) {
+      const O4Point P = O.pts[(long)b * O.npts + pt[0]];
+      const long src = cIdx(O, P.p, 0, i, P.j0 + (P.cell & 3), P.k0 + (P.cell >> 2));
+#pragma unroll
+      for (int c = 0; c < 8; ++c) u[c] = io.cart[src + (long)c * O.Nc];
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) io.cart[cIdx(O, b, c, i, jk.x, jk.y)] = u[c];
   }
 }
 

@@ -112,3 +112,34 @@ def test_inserted_cloud_steps():
         shell.advance(ju, 10, time)
         assert shell.valid(ju), order
         assert math.isfinite(time.item())
+
+
+def test_o4_step_with_cloud_matches_oracle(oracle_lib):
+    """Stage preparation and one RK4 step of a level holding a sharp cloud
+    that reaches the panel seams: the seam ghosts whose fourth-order
+    interpolation is inadmissible fall back to their donor cell's average on
+    both sides alike.  Tolerances as for smooth states (prepare 1e-12, one
+    step 1e-12), since the fallback decisions sit far from their bounds."""
+    _need_gpu()
+    po = oracle_lib
+    n = 16
+    kw = dict(nr=n, na=n, spatial_order=4, riemann_solver=2, berta_fallback_type=0)
+    shell = hc.Shell(hc.Params(**kw))
+    orc = po.OracleLevelO4(po.make_params(**kw))
+    base = po.OracleLevel(po.make_params(**kw))
+    ju = _wind(po, base)
+    spec = hc.ConeSpec.on_inner_boundary(INNER, lat_deg=30.0, lon_deg=30.0, half_angle_deg=60.0, apex_speed=2000.0,
+                                         density=6 * 700 * C_MP)
+    ocone = po.cone_prepare(po.HcConeSpec(**{k: getattr(spec, k) for k in po.CONE_SPEC_FIELDS}), INNER)
+    base.insert_cone(ocone, ocone.insertion_time, ju)
+    ref = orc.prepare(ju, 0.0)
+    got = shell.prepare(torch.from_numpy(ju).cuda(), 0.0).cpu().numpy()
+    err = rel_err_components(got.reshape(6, 8, -1), ref.reshape(6, 8, -1))
+    assert err.max() < 1e-12, err
+    dt = 0.3 / orc.inv_dt(ju)
+    g = torch.from_numpy(ju.copy()).cuda()
+    orc.rk4_step(ju, dt, 0.0)
+    shell.rk4_step(g, dt, 0.0)
+    assert shell.valid(g)
+    err = rel_err_components(g.cpu().numpy().reshape(6, 8, -1), ju.reshape(6, 8, -1))
+    assert err.max() < 1e-12, err

@@ -52,8 +52,12 @@ def seam_error(na, nr=2):
     ex = exact_averages(na, ga)
     valid = np.zeros((nA, nA), bool)
     valid[ga:ga + na, ga:ga + na] = True
+    # an admissible state (positive density and thermal energy) whose z
+    # momentum is the smooth test function
     cart = np.zeros((6, 8, nA, nA, nr))
-    cart[:, :, valid, :] = ex[:, None, valid, None]
+    cart[:, 0][:, valid, :] = 2.0 + ex[:, valid, None]
+    cart[:, 3][:, valid, :] = ex[:, valid, None]
+    cart[:, 4][:, valid, :] = 100.0
     cart = np.ascontiguousarray(cart.reshape(-1))
     O.seams(cart)
     got = cart.reshape(6, 8, nA, nA, nr)[:, 3, :, :, nr - 1]
@@ -64,6 +68,37 @@ def test_seam_interpolation_is_fourth_order():
     e16, e32 = seam_error(16), seam_error(32)
     assert e32 < 2e-5
     assert e16 / e32 > 12.0, (e16, e32)
+
+
+def test_seam_ghosts_at_a_jump_stay_admissible():
+    """A density jump of 1:100 next to the seams: the fourth-order stencil
+    undershoots below zero there, and those ghosts take the average of the
+    donor cell that contains their centre; every ghost stays admissible."""
+    na, nr = 16, 2
+    O = po.OracleLevelO4(po.make_params(nr=nr, na=na, spatial_order=4, riemann_solver=2))
+    ga = O.ga
+    nA = na + 2 * ga
+    valid = np.zeros((nA, nA), bool)
+    valid[ga:ga + na, ga:ga + na] = True
+    rng = np.random.default_rng(4)
+    rho = np.where(rng.random((6, nA, nA)) < 0.5, 1.0, 100.0)
+    cart = np.zeros((6, 8, nA, nA, nr))
+    cart[:, 0][:, valid, :] = rho[:, valid, None]
+    cart[:, 1][:, valid, :] = 3.0 * rho[:, valid, None]
+    cart[:, 4][:, valid, :] = 1000.0 * rho[:, valid, None]
+    before = cart.copy()
+    flat = np.ascontiguousarray(cart.reshape(-1))
+    O.seams(flat)
+    out = flat.reshape(6, 8, nA, nA, nr)
+    ghosts = out[:, :, ~valid, :]
+    rho_g = ghosts[:, 0]
+    thermal = ghosts[:, 4] - 0.5 * ghosts[:, 1] ** 2 / rho_g
+    assert np.isfinite(ghosts).all()
+    assert (rho_g > 0).all() and (thermal >= 0).all()
+    # some ghosts took a donor cell's average: exactly one of the two levels
+    donor = np.isin(rho_g, [1.0, 100.0])
+    assert donor.sum() > 0
+    np.testing.assert_array_equal(out[:, :, valid, :], before[:, :, valid, :])
 
 
 def test_constant_cartesian_state_is_preserved():

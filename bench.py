@@ -77,7 +77,8 @@ def workload_config(args, flush: bool):
         "scheme": {"spatial_order": args.order, "limiter": args.limiter if args.order == 2 else None,
                    "riemann_solver": args.riemann, "powell": 1, "gravity": args.gravity, "temporal_order": 4,
                    "cfl": 0.4},
-        "init": ("Parker-like wind + cone cloud 1500 km/s, 45 deg half-width, 4x density (tapered edges)"
+        "init": ("Parker-like wind + finite cone-CME cloud (field model 4) 1500 km/s, 45 deg, 4x density, "
+                 "seeded axis, inserted on the device at the inner boundary"
                  if args.init == "cone" else
                  "Parker-like wind + seeded 5% tangential v and B (stream-function curl)" if args.order == 4
                  else "Parker-like wind + seeded Gaussian pressure pulse"),
@@ -244,6 +245,17 @@ def run_reference(args, world, rank):
     print(json.dumps(out), flush=True)
 
 
+def cone_request(args):
+    """The large-solve workload's input: the wind with a 1500 km/s, 45 deg,
+    4x density cone cloud on a seeded axis (lat/lon U[-30, 30] deg)
+    inserted at the inner boundary."""
+    from heliocubed_b200 import serve
+    rng = np.random.default_rng(args.seed)
+    cone = serve.Cone(speed_kms=1500.0, half_width_deg=45.0, lat_deg=rng.uniform(-30, 30),
+                      lon_deg=rng.uniform(-30, 30), density_ratio=4.0)
+    return serve.Request(0, args.nr, args.na, args.order, 0, cone=cone)
+
+
 def run_b200(args, world, rank, local):
     import torch
     from heliocubed_b200.level import InitSpec, Shell
@@ -253,8 +265,7 @@ def run_b200(args, world, rank, local):
     cells = shell.cells
     if args.init == "cone":
         from heliocubed_b200 import serve
-        req = serve.Request(0, args.nr, args.na, args.order, 0, cone=serve.Cone(1500.0, 45.0, 0.0, 0.0, 4.0))
-        ju0 = torch.from_numpy(serve.initial_state(shell, req)).to(shell._dev)
+        ju0 = torch.from_numpy(serve.initial_state(shell, cone_request(args))).to(shell._dev)
     elif args.order == 4:
         ju0 = shell.init_perturbed_wind(args.seed)
     else:
@@ -398,12 +409,11 @@ def run_serve(args, world, rank, local):
     torch.cuda.set_device(local)
     reqs = serve.synthetic_requests(args.serve_requests, args.seed, None, args.serve_steps,
                                     radial=(32, 48, 64), angular=(32, 48))
-    shells, states = {}, {}
+    shells = {}
     for r in reqs:
         shp = (r.nr, r.na, r.order)
         if shp not in shells:
             shells[shp] = serve.Shell(r.params(), device=local)
-        states[r.rid] = serve.initial_state(shells[shp], r)
     server = serve.EnsembleServer(hbm_budget=args.serve_budget_gb * 1e9, max_inflight=args.serve_inflight,
                                   chunk=10, device=local)
     counts = {}
@@ -413,14 +423,14 @@ def run_serve(args, world, rank, local):
         server.warm([r for r in reqs if (r.nr, r.na, r.order) == shp], per_shape=min(n, args.serve_inflight))
     # warm the plain path's contexts with one step each
     for shp, sh in shells.items():
-        rid = next(r.rid for r in reqs if (r.nr, r.na, r.order) == shp)
-        ju = torch.from_numpy(states[rid]).to(sh._dev)
+        req = next(r for r in reqs if (r.nr, r.na, r.order) == shp)
+        ju = torch.from_numpy(serve.initial_state(sh, req)).to(sh._dev)
         sh.advance(ju, 1, torch.zeros(1, dtype=torch.float64, device=sh._dev))
     torch.cuda.synchronize()
     sampler = ClockSampler(local)
     sampler.start()
-    plain = serve.run_plain(reqs, states, device=local, shells=shells)
-    batched = server.run(reqs, states)
+    plain = serve.run_plain(reqs, device=local, shells=shells)
+    batched = server.run(reqs)
     clocks = sampler.stop()
     same = all(np.array_equal(a.state, b.state, equal_nan=True) for a, b in
                zip(sorted(plain, key=lambda r: r.rid), sorted(batched, key=lambda r: r.rid)))
@@ -556,7 +566,7 @@ def main() -> int:
     ap.add_argument("--riemann", type=int, default=None)
     ap.add_argument("--gravity", type=int, default=0)
     ap.add_argument("--init", choices=["default", "cone"], default="default",
-                    help="cone: the wind with a 1500 km/s, 45 deg cone cloud (the large-solve workload)")
+                    help="cone: the wind with a 1500 km/s, 45 deg cone-CME cloud (the large-solve workload)")
     ap.add_argument("--seed", type=int, default=20261204)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", dest="graph", action="store_false",

@@ -1,9 +1,10 @@
 """Served ensemble of cubed-sphere MHD solves on one GPU.
 
 A request is one solve: a six-panel shell of its own size and scheme (second
-order PLM-MC + Rusanov, or fourth order Berta WENOZ + Roe), a synthetic
-cone-shaped plasma cloud inserted at admission, and a number of RK4 steps
-with dt from the device CFL reduction.  The server keeps every admitted
+order PLM-MC + Rusanov, or fourth order Berta WENOZ + Roe), the cone-CME
+cloud of its parameters inserted on the device at admission into the
+ambient wind, and a number of RK4 steps with dt from the device CFL
+reduction.  The server keeps every admitted
 state resident in HBM and overlaps requests on the GPU:
 
 * admission: requests are admitted in arrival order while the HBM estimate
@@ -13,8 +14,8 @@ state resident in HBM and overlaps requests on the GPU:
 * slots: a slot is a level context (geometry tables and stage workspace),
   its state buffer, its own CUDA stream and a CUDA graph of `chunk`
   hc_level_advance_cfl steps captured on that buffer; slots are pooled by
-  shape and reused, so admission costs a host-to-device copy, not a context
-  build;
+  shape and reused, so admission costs two kernels (wind, cone insertion)
+  on the slot's stream, not a context build;
 * progress: every slot whose previous chunk has completed gets its next
   chunk; the GPU runs the chunks of different slots concurrently.
 
@@ -25,32 +26,44 @@ order independent) and every slot owns its buffers.
 """
 from __future__ import annotations
 
-import math
 import time
 from dataclasses import dataclass, field
 
 import numpy as np
 import torch
 
-from .level import C_SR, InitSpec, Params, Shell, cell_directions
+from . import _native as N
+from .level import ConeSpec, InitSpec, Params, Shell, prepare_cone
 
 
 @dataclass
 class Cone:
-    """Synthetic cone-shaped cloud: inside `half_width_deg` of the axis at
-    (lat, lon) and below `r_top` (cm), the density is `density_ratio` times
-    the wind's and the radial speed `speed_kms`; pressure and field are the
-    wind's.  The edges are tapered smoothly (cos^2 over +-`edge` of the half
-    width and of r_top): a sharp-edged cloud moving at up to 2000 km/s
-    through the 400 km/s wind is a discontinuous initial state that the
-    fourth-order scheme need not survive at coarse grids."""
+    """Cone-CME parameters of a request: a finite spherical cloud (the
+    reference's cone field model 4, ConeSpec) of `density_ratio` times the
+    wind's density at the inner boundary, moving radially at `speed_kms`,
+    its axis at (lat, lon) and its radius r_inner sin(half width).  The cloud
+    lies wholly in the shell, touching the inner boundary, when it is
+    inserted on the device at admission (hc_level_insert_cone)."""
     speed_kms: float = 1000.0
     half_width_deg: float = 30.0
     lat_deg: float = 0.0
     lon_deg: float = 0.0
     density_ratio: float = 4.0
-    r_top: float = 30.0 * C_SR
-    edge: float = 0.25
+    temperature: float = 1.0e6
+
+    def prepared(self, params: Params, wind: InitSpec | None = None) -> N.HcCone:
+        wind = wind or wind_spec()
+        rho_inner = wind.rho0 * (wind.r_ref / params.inner_radius) ** 2
+        spec = ConeSpec.on_inner_boundary(params.inner_radius, lat_deg=self.lat_deg, lon_deg=self.lon_deg,
+                                          half_angle_deg=self.half_width_deg, apex_speed=self.speed_kms,
+                                          density=self.density_ratio * rho_inner, temperature=self.temperature)
+        return prepare_cone(spec, params.inner_radius)
+
+
+def wind_spec() -> InitSpec:
+    """The ambient state of every request: the Parker-like wind of InitSpec
+    without its pressure pulse."""
+    return InitSpec(pulse_amp=0.0)
 
 
 @dataclass
@@ -73,47 +86,22 @@ class Request:
         return Params(nr=self.nr, na=self.na, spatial_order=2, limiter=3, riemann_solver=1)
 
 
-def cone_state(params: Params, det: np.ndarray, dvolr: np.ndarray, cone: Cone,
-               spec: InitSpec | None = None) -> np.ndarray:
-    """JU [6][8][k][j][i] of the Parker-like wind of InitSpec with the cone
-    cloud; cell averages as J x centre values (J = <det A> dVolr)."""
-    spec = spec or InitSpec()
-    nr, na, gam = params.nr, params.na, params.gamma
-    r0, r1, C = params.inner_radius, params.outer_radius, params.radial_stretch
-    Rt = (r1 - r0) / np.expm1(C)
-    r = r0 + Rt * np.expm1(C * (np.arange(nr) + 0.5) / nr)
-    s = spec.r_ref / r
-    X = cell_directions(na)                                      # [6][3][k][j]
-    lat, lon = math.radians(cone.lat_deg), math.radians(cone.lon_deg)
-    axis = np.array([math.cos(lat) * math.cos(lon), math.cos(lat) * math.sin(lon), math.sin(lat)])
-    def taper(x, x0, width):
-        """1 below x0 - width, 0 above x0 + width, cos^2 in between."""
-        t = np.clip((x - (x0 - width)) / (2 * width), 0.0, 1.0)
-        return np.cos(0.5 * np.pi * t) ** 2
-
-    angle = np.arccos(np.clip(np.einsum("q,bqkj->bkj", axis, X), -1.0, 1.0))
-    hw = math.radians(cone.half_width_deg)
-    weight = taper(angle, hw, cone.edge * hw)[..., None] * taper(r, cone.r_top, cone.edge * (cone.r_top - r0))
-    rho = spec.rho0 * s ** 2 * (1.0 + (cone.density_ratio - 1.0) * weight)
-    vr = spec.vr + (cone.speed_kms * 1e5 - spec.vr) * weight
-    p = spec.p0 * s ** (2 * gam) * np.ones_like(rho)
-    Br = spec.b0 * s[None, None, None, :] ** 2 * np.sign(X[:, 2])[..., None]
-    J = det[:, :, :, None] * dvolr[None, None, None, :]
-    ju = np.zeros((6, 8, na, na, nr))
-    v = vr[:, None] * X[..., None]
-    B = Br[:, None] * X[..., None]
-    ju[:, 0] = rho * J
-    ju[:, 1:4] = rho[:, None] * v * J[:, None]
-    ju[:, 5:8] = B * J[:, None]
-    ju[:, 4] = (p / (gam - 1) + 0.5 * rho * (v ** 2).sum(1) + (B ** 2).sum(1) / (8 * np.pi)) * J
-    return ju
+def admit(shell: Shell, req: Request, ju: torch.Tensor, time_dev: torch.Tensor) -> None:
+    """Device-side admission on the current stream: the wind into `ju`, the
+    request's cone cloud inserted at its insertion time, the model time set
+    to that time."""
+    shell.init(wind_spec(), ju)
+    cone = req.cone.prepared(shell.params)
+    shell.insert_cone(cone, cone.insertion_time, ju)
+    time_dev.fill_(cone.insertion_time)
 
 
 def initial_state(shell: Shell, req: Request) -> np.ndarray:
-    p = shell.params
-    det = shell.geometry(4).reshape(6, p.na, p.na)
-    dvolr = shell.geometry(0).reshape(p.nr + 1, 4)[:p.nr, 3]
-    return np.ascontiguousarray(cone_state(p, det, dvolr, req.cone).reshape(-1))
+    """Host copy of the state `admit` builds (for checks and reports)."""
+    ju = shell.new_state()
+    t = torch.zeros(1, dtype=torch.float64, device=ju.device)
+    admit(shell, req, ju, t)
+    return ju.cpu().numpy()
 
 
 class Slot:
@@ -128,12 +116,11 @@ class Slot:
         self.stream = torch.cuda.Stream(device=device)
         self.state = self.shell.new_state()
         self.time = torch.zeros(1, dtype=torch.float64, device=self.shell._dev)
-        self.host_in = torch.empty(self.state.numel(), dtype=torch.float64).pin_memory()
-        self.host_out = torch.empty_like(self.host_in).pin_memory()
+        self.host_out = torch.empty(self.state.numel(), dtype=torch.float64).pin_memory()
         self.host_time = torch.empty(1, dtype=torch.float64).pin_memory()
-        # capture on a valid (wind) state; requests overwrite the buffer
-        warm = Request(0, nr, na, order, 0, cone=Cone(density_ratio=1.0, speed_kms=400.0))
-        self.state.copy_(torch.from_numpy(initial_state(self.shell, warm)).to(self.state.device))
+        # capture on a valid (wind) state; admission overwrites the buffer
+        self.shell.init(wind_spec(), self.state)
+        torch.cuda.synchronize(device)
         with torch.cuda.stream(self.stream):
             self.graph = self.shell.capture_advance(self.state, chunk, self.time)
         torch.cuda.synchronize(device)
@@ -143,14 +130,12 @@ class Slot:
         self.event: torch.cuda.Event | None = None
         self.t_start = 0.0
 
-    def start(self, req: Request, host_state: np.ndarray, now: float) -> None:
+    def start(self, req: Request, now: float) -> None:
         self.req = req
         self.left = req.steps
         self.t_start = now
-        self.host_in.numpy()[:] = host_state
         with torch.cuda.stream(self.stream):
-            self.state.copy_(self.host_in, non_blocking=True)
-            self.time.zero_()
+            admit(self.shell, req, self.state, self.time)
         self.event = None
 
     def issue(self) -> None:
@@ -227,9 +212,8 @@ class EnsembleServer:
         slot.req = None
         self.pool[slot.shape].append(slot)
 
-    def run(self, requests: list[Request], states: dict[int, np.ndarray]) -> list[Result]:
-        """Serve `requests` (arrival times relative to the call); `states`
-        maps request id to its initial host state."""
+    def run(self, requests: list[Request]) -> list[Result]:
+        """Serve `requests` (arrival times relative to the call)."""
         pending = sorted(requests, key=lambda r: (r.arrival, r.rid))
         active: list[Slot] = []
         results: list[Result] = []
@@ -241,7 +225,7 @@ class EnsembleServer:
                 if slot is None:
                     break
                 req = pending.pop(0)
-                slot.start(req, states[req.rid], now)
+                slot.start(req, now)
                 slot.issue()
                 active.append(slot)
             progressed = False
@@ -266,11 +250,11 @@ class EnsembleServer:
         return results
 
 
-def run_plain(requests: list[Request], states: dict[int, np.ndarray], device: int | None = None,
+def run_plain(requests: list[Request], device: int | None = None,
               shells: dict[tuple, Shell] | None = None) -> list[Result]:
     """The same requests one after another through eager per-solve launches
-    (`Shell.advance`), with host copies in and out; contexts are cached by
-    shape so neither path pays for context builds."""
+    (`admit`, `Shell.advance`, the result copied to the host); contexts are
+    cached by shape so neither path pays for context builds."""
     device = torch.cuda.current_device() if device is None else device
     shells = {} if shells is None else shells
     results = []
@@ -284,9 +268,9 @@ def run_plain(requests: list[Request], states: dict[int, np.ndarray], device: in
             shells[shp] = Shell(req.params(), device=device)
         sh = shells[shp]
         t_start = time.perf_counter() - t0
-        host = torch.from_numpy(states[req.rid]).pin_memory()
-        ju = host.to(sh._dev, non_blocking=True)
+        ju = sh.new_state()
         t = torch.zeros(1, dtype=torch.float64, device=sh._dev)
+        admit(sh, req, ju, t)
         sh.advance(ju, req.steps, t)
         out = ju.cpu().numpy()
         results.append(Result(req.rid, req.cells, req.steps, req.arrival, t_start, time.perf_counter() - t0, out,

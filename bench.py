@@ -106,6 +106,38 @@ def profiled_traffic_per_cell_stage(order: int):
     return float(m.group(1)) if m else None
 
 
+def profiled_fp64_flops_per_cell_stage(order: int):
+    """FP64 flops (dadd + dmul + 2 dfma thread instructions, ncu counters)
+    per cell-stage of the operator from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "o2_stage_kernel.md" if order == 2 else "o4_operator.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"fp64_flops_per_cell_stage:\s*([0-9.eE+-]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def measure_fp64_peak() -> float:
+    """FP64 TFLOP/s of a cuBLAS DGEMM (8192^3, best of 3, CUDA events) on
+    this GPU: the denominator of the FP64-pipe roofline."""
+    import torch
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn_like(a)
+    c = torch.empty_like(a)
+    torch.matmul(a, b, out=c)
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -328,6 +360,8 @@ def run_b200(args, world, rank, local):
     peak, peak_kind = peaks()
     achieved = OPERATOR_BYTES_PER_CELL_STAGE * cells / (kms * 1e-3) / 1e9
     tr = profiled_traffic_per_cell_stage(args.order)
+    fl = profiled_fp64_flops_per_cell_stage(args.order)
+    fp64_peak = measure_fp64_peak()
 
     # End to end through the public API with host buffers: every step copies
     # its input from pinned host memory, advances one RK4 step and copies the
@@ -385,6 +419,13 @@ def run_b200(args, world, rank, local):
                          "algorithmic_bytes": f"{OPERATOR_BYTES_PER_CELL_STAGE} B/cell-stage x {cells} cells",
                          "kernel_ms": kms,
                          "traffic": None if tr is None else tr * cells},
+            # The operator does no contraction; its binding roofline is the
+            # FP64 pipe (flops from ncu instruction counters, peak from a
+            # DGEMM measured in this run).
+            "fp64_roofline": None if fl is None else {
+                "bound": "fp64", "flops_per_cell_stage": fl, "achieved": fl * cells / (kms * 1e-3) / 1e12,
+                "peak": fp64_peak, "unit": "TFLOP/s", "frac": fl * cells / (kms * 1e-3) / 1e12 / fp64_peak,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (best of 3)"},
             "e2e": {"value": cells * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes,
                     "pipeline": f"{nlanes} context(s) on {nlanes} stream(s); a step's copies overlap the other "

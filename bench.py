@@ -303,6 +303,17 @@ def run_b200(args, world, rank, local):
     else:
         ju0 = shell.init(InitSpec.seeded(args.seed, args.nr, args.na))
     ju = ju0.clone()
+    tuning = None
+    if args.order == 2:
+        # stage-tile autotuner: time the candidate tiles on this level, keep the fastest
+        from heliocubed_b200.level import stage_tiles
+        (trk, trhs), tms = shell.autotune(ju0)
+        shapes = stage_tiles()
+        tuning = {"rk_stage_tile": [int(x) for x in shapes[trk]], "operator_tile": [int(x) for x in shapes[trhs]],
+                  "candidates": [[int(x) for x in r] for r in shapes],
+                  "rk_stage_ms": [round(float(x), 5) for x in tms[0]],
+                  "operator_ms": [round(float(x), 5) for x in tms[1]],
+                  "tile_fields": "cells x, y, z, min CTAs/SM Rusanov, Roe"}
     time_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
     state_bytes = ju.numel() * 8
@@ -410,7 +421,8 @@ def run_b200(args, world, rank, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(workload_config(args, flush), parallelism=f"replicas x{world}"),
+            "config": dict(workload_config(args, flush), parallelism=f"replicas x{world}",
+                           **({"autotune": tuning} if tuning else {})),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "kernel": ("o2StageKernel (operator: read primitives, write rhs)" if args.order == 2 else

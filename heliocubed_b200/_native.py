@@ -41,6 +41,9 @@ SIGNATURES = {
     "hc_level_init": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hc_geometry_export": (C.c_long, [_VP, C.c_int, _VP]),
     "hc_cone_prepare": (C.c_int, [_VP, C.c_double, _VP]),
+    "hc_stage_tiles": (C.c_int, [_VP, C.c_int]),
+    "hc_ctx_autotune": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "hc_ctx_set_tiles": (C.c_int, [_VP, C.c_int, C.c_int]),
     "hc_level_insert_cone": (C.c_int, [_VP, _VP, C.c_double, _VP, _VP, _VP]),
 }
 
@@ -52,7 +55,7 @@ class HcParams(C.Structure):
         ("divergence_cleaning", C.c_int), ("sun_gravity", C.c_int),
         ("init_condition_type", C.c_int), ("temporal_order", C.c_int),
         ("nr", C.c_int), ("na", C.c_int), ("spatial_operator", C.c_int), ("berta_detector_type", C.c_int),
-        ("berta_fallback_type", C.c_int), ("reserved_i", C.c_int * 4),
+        ("berta_fallback_type", C.c_int), ("autotune", C.c_int), ("reserved_i", C.c_int * 3),
         ("gamma", C.c_double), ("entropy_fix_coeff", C.c_double), ("cfl", C.c_double),
         ("inner_radius", C.c_double), ("outer_radius", C.c_double),
         ("radial_stretch", C.c_double), ("strength", C.c_double), ("berta_eta_d", C.c_double),

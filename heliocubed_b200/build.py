@@ -34,9 +34,12 @@ def _stale(out: str, deps: list[str]) -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile the stale translation units (in parallel, one nvcc process
+    each) and link the library."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(REPO, "include", "hc_abi.h")]
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src + ".o")
@@ -47,7 +50,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
                 cmd += ["-Xptxas", "-v"]
             if src.endswith(".cpp"):
                 cmd = [NVCC, *ARCH, *COMMON, "-x", "c++", "-c", path, "-o", obj]
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
+    if cmds:
+        with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+            for r in list(pool.map(lambda c: subprocess.run(c), cmds)):
+                if r.returncode != 0:
+                    raise subprocess.CalledProcessError(r.returncode, r.args)
     if force or _stale(LIB, objs):
         subprocess.run([NVCC, *ARCH, "-shared", "--cudart", "static", *objs, "-o", LIB], check=True)
     return LIB

@@ -11,6 +11,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -244,6 +246,9 @@ struct hc_ctx {
   double* acc = nullptr;              // RK accumulator [6][8][na][na][nr]
   unsigned long long* invMax = nullptr;  // two CFL slots (bit patterns), ping-pong per step
   int* flag = nullptr;
+  // cell tiles of the order-2 stage kernel: fused RK stage, operator alone
+  int tileRK = 0, tileRHS = 0;
+  bool tuned = false;
   // fourth-order operator: metric tables and grow-only scratch
   O4Geo o4{};
   double* o4scratch = nullptr;
@@ -818,7 +823,7 @@ int rkStep(hc_ctx* c, double* ju, double dtv, const double* invMax, unsigned lon
     a.invMaxOut = stage == 3 ? invMaxOut : nullptr;
     a.invalid = nullptr;
     rc = checkLaunch(launchStage(a, MODE_RK, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
-                                 c->P.sun_gravity == 1, s),
+                                 c->P.sun_gravity == 1, s, c->tileRK),
                      "stage");
     if (rc != HC_OK) return rc;
   }
@@ -1236,8 +1241,147 @@ int hc_level_rhs(hc_ctx* c, const double* w, double* k, void* stream) {
   StageArgs a = levelArgs(c, w);
   a.rhs = k;
   return checkLaunch(launchStage(a, MODE_RHS, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
-                                 c->P.sun_gravity == 1, (cudaStream_t)stream),
+                                 c->P.sun_gravity == 1, (cudaStream_t)stream, c->tileRHS),
                      "hc_level_rhs");
+}
+
+}  // extern "C"
+
+namespace {
+
+// Tiles chosen per device, level size and scheme, shared by the contexts of
+// the process (a served ensemble creates many contexts of a few shapes).
+std::mutex g_tileMutex;
+std::map<std::string, std::pair<int, int>> g_tileCache;
+
+std::string tileKey(const hc_ctx* c) {
+  const hc_params& P = c->P;
+  char key[160];
+  std::snprintf(key, sizeof key, "%d:%d:%d:%d:%d:%d:%d", c->device, P.nr, P.na, P.limiter == 0 ? 0 : P.limiter == 3 ? 3 : 1,
+                P.riemann_solver == 2 ? 1 : 0, P.divergence_cleaning == 1 ? 1 : 0, P.sun_gravity == 1 ? 1 : 0);
+  return key;
+}
+
+// Median launch time (ms) of `launch` over `reps` launches after 2 warm-ups.
+template <class F>
+int timeLaunches(F launch, cudaStream_t s, int reps, double* ms) {
+  cudaEvent_t e[2 * 16];
+  reps = std::min(reps, 16);
+  for (int i = 0; i < 2 * reps; ++i)
+    if (cudaEventCreate(&e[i]) != cudaSuccess) {
+      for (int j = 0; j < i; ++j) cudaEventDestroy(e[j]);
+      return cudaFail(cudaGetLastError(), "autotune events");
+    }
+  int rc = HC_OK;
+  for (int i = 0; i < 2 && rc == HC_OK; ++i) rc = launch();
+  for (int i = 0; i < reps && rc == HC_OK; ++i) {
+    cudaEventRecord(e[2 * i], s);
+    rc = launch();
+    cudaEventRecord(e[2 * i + 1], s);
+  }
+  if (rc == HC_OK) rc = checkLaunch(cudaStreamSynchronize(s), "autotune sync");
+  std::vector<float> t;
+  for (int i = 0; i < reps && rc == HC_OK; ++i) {
+    float v = 0;
+    rc = checkLaunch(cudaEventElapsedTime(&v, e[2 * i], e[2 * i + 1]), "autotune timing");
+    t.push_back(v);
+  }
+  for (int i = 0; i < 2 * reps; ++i) cudaEventDestroy(e[i]);
+  if (rc != HC_OK) return rc;
+  std::sort(t.begin(), t.end());
+  *ms = t[t.size() / 2];
+  return HC_OK;
+}
+
+int autotuneStage(hc_ctx* c, const double* ju, cudaStream_t s, int* tilesOut, double* msOut) {
+  const bool roe = c->P.riemann_solver == 2, powell = c->P.divergence_cleaning == 1, grav = c->P.sun_gravity == 1;
+  // primitives of ju with ghosts in W[0]; the timed launches write only the
+  // workspace (W[1], acc), never ju
+  int rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "autotune prim");
+  StageTime st{0.0, nullptr, 0.0, nullptr, 0.0};
+  if (rc == HC_OK) rc = checkLaunch(launchGhosts(c->L, c->W[0], st, s), "autotune ghosts");
+  double best[2] = {1e300, 1e300};
+  int pick[2] = {0, 0};
+  for (int mode = 0; mode < 2 && rc == HC_OK; ++mode)
+    for (int t = 0; t < kStageTiles && rc == HC_OK; ++t) {
+      StageArgs a = levelArgs(c, c->W[0]);
+      if (mode == 0) {
+        a.stage = 0;  // reads ju, writes acc and the next stage's primitives
+        a.invDtMax = nullptr;
+        a.dtv = 0.0;
+        a.ju = const_cast<double*>(ju);
+        a.acc = c->acc;
+        a.wOut = c->W[1];
+        a.invMaxOut = nullptr;
+        a.invalid = nullptr;
+      } else {
+        a.rhs = c->acc;
+      }
+      double ms = 0;
+      rc = timeLaunches(
+          [&]() {
+            return checkLaunch(launchStage(a, mode == 0 ? MODE_RK : MODE_RHS, c->P.limiter, roe, powell, grav, s, t),
+                               "autotune launch");
+          },
+          s, 7, &ms);
+      if (rc != HC_OK) break;
+      if (msOut) msOut[mode * kStageTiles + t] = ms;
+      if (ms < best[mode]) { best[mode] = ms; pick[mode] = t; }
+    }
+  if (rc != HC_OK) return rc;
+  c->tileRK = pick[0];
+  c->tileRHS = pick[1];
+  c->tuned = true;
+  {
+    std::lock_guard<std::mutex> lock(g_tileMutex);
+    g_tileCache[tileKey(c)] = {pick[0], pick[1]};
+  }
+  if (tilesOut) { tilesOut[0] = pick[0]; tilesOut[1] = pick[1]; }
+  return HC_OK;
+}
+
+// With hc_params.autotune set: take a cached choice, or time the tiles once
+// (outside stream capture only; a capturing stream keeps the current tiles).
+int maybeAutotune(hc_ctx* c, const double* ju, cudaStream_t s) {
+  if (!c->P.autotune || c->tuned || c->P.spatial_order != 2) return HC_OK;
+  {
+    std::lock_guard<std::mutex> lock(g_tileMutex);
+    auto it = g_tileCache.find(tileKey(c));
+    if (it != g_tileCache.end()) {
+      c->tileRK = it->second.first;
+      c->tileRHS = it->second.second;
+      c->tuned = true;
+      return HC_OK;
+    }
+  }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return HC_OK;
+  return autotuneStage(c, ju, s, nullptr, nullptr);
+}
+
+}  // namespace
+
+extern "C" {
+
+int hc_stage_tiles(int* shapes, int capacity) {
+  for (int t = 0; shapes && t < kStageTiles && t < capacity; ++t) stageTileShape(t, shapes + 5 * t);
+  return kStageTiles;
+}
+
+int hc_ctx_autotune(hc_ctx* c, const double* ju, int* tiles, double* ms, void* stream) {
+  if (!c || !ju) return fail(HC_ERR_ARG, "null argument");
+  if (c->P.spatial_order != 2) return fail(HC_ERR_UNSUPPORTED, "hc_ctx_autotune: order-2 contexts only");
+  return autotuneStage(c, ju, (cudaStream_t)stream, tiles, ms);
+}
+
+int hc_ctx_set_tiles(hc_ctx* c, int tileRK, int tileRHS) {
+  if (!c) return fail(HC_ERR_ARG, "null argument");
+  if (tileRK < -1 || tileRK >= kStageTiles || tileRHS < -1 || tileRHS >= kStageTiles)
+    return fail(HC_ERR_ARG, "tile index out of range");
+  if (tileRK >= 0) c->tileRK = tileRK;
+  if (tileRHS >= 0) c->tileRHS = tileRHS;
+  c->tuned = true;
+  return HC_OK;
 }
 
 int hc_level_rk4_step(hc_ctx* c, double* ju, double dt, double t, void* stream) {
@@ -1248,7 +1392,8 @@ int hc_level_rk4_step(hc_ctx* c, double* ju, double dt, double t, void* stream) 
     const int rc4 = ensureO4Buffers(c);
     return rc4 != HC_OK ? rc4 : o4Step(c, ju, dt, nullptr, t, nullptr, s);
   }
-  const int rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
+  int rc = maybeAutotune(c, ju, s);
+  if (rc == HC_OK) rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
   if (rc != HC_OK) return rc;
   return rkStep(c, ju, dt, nullptr, nullptr, t, nullptr, s);
 }
@@ -1270,7 +1415,8 @@ int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, do
   }
   // The first step's primitives and CFL rate come from ju; every later
   // step's come from the previous step's last stage.
-  int rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
+  int rc = maybeAutotune(c, ju, s);
+  if (rc == HC_OK) rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
   if (rc == HC_OK) rc = checkLaunch(launchCfl(c->L, ju, c->invMax, s), "cfl");
   for (int n = 0; n < nsteps && rc == HC_OK; ++n) {
     const int cur = n % 2;

@@ -1,7 +1,7 @@
 // sm_100a kernels of the second-order (PLM) per-box MHD update and the RK4
 // stage that consumes it.  FP64 throughout.
 //
-// o2StageKernel -- one CTA per TX x TY x TZ cell tile of one box.  Phase 1
+// o2StageKernel -- one CTA per X x Y x Z cell tile (Tile) of one box.  Phase 1
 // computes every face of the tile in all three directions (flat loop over
 // faces, radial index fastest so stencil loads are coalesced) and keeps the
 // face fluxes in shared memory; phase 2 forms the flux divergence, Powell and
@@ -17,10 +17,27 @@ namespace hc {
 
 namespace {
 
-constexpr int TX = 16, TY = 4, TZ = 2;
-constexpr int NT = TX * TY * TZ;
-constexpr int NF0 = (TX + 1) * TY * TZ, NF1 = TX * (TY + 1) * TZ, NF2 = TX * TY * (TZ + 1);
-constexpr int NF = NF0 + NF1 + NF2;
+// Cell tiles of o2StageKernel: X x Y x Z cells per CTA (128 threads, one
+// cell each) and the minimum resident CTAs per SM that caps the registers
+// (Rusanov, Roe).  The autotuner (hc_ctx_autotune) times them per limiter /
+// solver pair on the caller's level; every tile computes every face and cell
+// with the same arithmetic, so results do not depend on the choice.
+template <int X, int Y, int Z, int MB_RUS, int MB_ROE>
+struct Tile {
+  static constexpr int TX = X, TY = Y, TZ = Z, NT = X * Y * Z;
+  static constexpr int NF0 = (X + 1) * Y * Z, NF1 = X * (Y + 1) * Z, NF2 = X * Y * (Z + 1);
+  static constexpr int NF = NF0 + NF1 + NF2;
+  static constexpr int minBlocks(bool roe) { return roe ? MB_ROE : MB_RUS; }
+};
+using Tile0 = Tile<16, 4, 2, 3, 2>;
+using Tile1 = Tile<32, 2, 2, 3, 2>;
+using Tile2 = Tile<8, 8, 2, 3, 2>;
+using Tile3 = Tile<16, 2, 4, 3, 2>;
+using Tile4 = Tile<16, 4, 2, 4, 3>;
+using Tile5 = Tile<32, 4, 1, 3, 2>;
+static_assert(Tile0::NT == 128 && Tile1::NT == 128 && Tile2::NT == 128 && Tile3::NT == 128 && Tile4::NT == 128 &&
+                  Tile5::NT == 128,
+              "stage tiles are 128 threads");
 
 __device__ __forceinline__ long cellOffset(int i, int j, int k, const int lo[3], const int n[3]) {
   return (long)(i - lo[0]) + (long)n[0] * ((long)(j - lo[1]) + (long)n[1] * (long)(k - lo[2]));
@@ -189,10 +206,11 @@ __device__ __forceinline__ void warpMaxAtomic(double v, unsigned long long* out)
   if ((threadIdx.x & 31) == 0 && v > 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
 }
 
-template <int DIR, int LIM, bool ROE, int MODE>
+template <class TL, int DIR, int LIM, bool ROE, int MODE>
 __device__ __forceinline__ void o2FaceLoop(const StageArgs& a, const double* __restrict__ w, int block, int oi,
                                            int oj, int ok, int v0, int v1, int v2, double* sF, int base,
                                            bool powell) {
+  constexpr int TX = TL::TX, TY = TL::TY, TZ = TL::TZ, NT = TL::NT, NF = TL::NF;
   constexpr int EX = TX + (DIR == 0), EY = TY + (DIR == 1), EZ = TZ + (DIR == 2);
   constexpr int NFD = EX * EY * EZ;
   for (int f = threadIdx.x; f < NFD; f += NT) {
@@ -220,8 +238,10 @@ __device__ __forceinline__ void o2FaceLoop(const StageArgs& a, const double* __r
   }
 }
 
-template <int LIM, bool ROE, int MODE>
-__global__ void __launch_bounds__(NT, ROE ? 2 : 3) o2StageKernel(const StageArgs a, const int powell, const int grav) {
+template <class TL, int LIM, bool ROE, int MODE>
+__global__ void __launch_bounds__(TL::NT, TL::minBlocks(ROE))
+    o2StageKernel(const StageArgs a, const int powell, const int grav) {
+  constexpr int TX = TL::TX, TY = TL::TY, TZ = TL::TZ, NF = TL::NF, NF0 = TL::NF0, NF1 = TL::NF1;
   extern __shared__ double sF[];  // [9][NF]: 8 flux components + Powell face B_n
   const int v0 = a.hi[0] - a.lo[0] + 1, v1 = a.hi[1] - a.lo[1] + 1, v2 = a.hi[2] - a.lo[2] + 1;
   const int nbx = (v0 + TX - 1) / TX, nby = (v1 + TY - 1) / TY, nbz = (v2 + TZ - 1) / TZ;
@@ -234,9 +254,9 @@ __global__ void __launch_bounds__(NT, ROE ? 2 : 3) o2StageKernel(const StageArgs
   const int oi = a.lo[0] + bx * TX, oj = a.lo[1] + by * TY, ok = a.lo[2] + bz * TZ;
   const double* __restrict__ w = a.w + (long)box * a.wBoxStride;
 
-  o2FaceLoop<0, LIM, ROE, MODE>(a, w, block, oi, oj, ok, v0, v1, v2, sF, 0, powell != 0);
-  o2FaceLoop<1, LIM, ROE, MODE>(a, w, block, oi, oj, ok, v0, v1, v2, sF, NF0, powell != 0);
-  o2FaceLoop<2, LIM, ROE, MODE>(a, w, block, oi, oj, ok, v0, v1, v2, sF, NF0 + NF1, powell != 0);
+  o2FaceLoop<TL, 0, LIM, ROE, MODE>(a, w, block, oi, oj, ok, v0, v1, v2, sF, 0, powell != 0);
+  o2FaceLoop<TL, 1, LIM, ROE, MODE>(a, w, block, oi, oj, ok, v0, v1, v2, sF, NF0, powell != 0);
+  o2FaceLoop<TL, 2, LIM, ROE, MODE>(a, w, block, oi, oj, ok, v0, v1, v2, sF, NF0 + NF1, powell != 0);
   __syncthreads();
 
   const int li = threadIdx.x % TX, lj = (threadIdx.x / TX) % TY, lk = threadIdx.x / (TX * TY);
@@ -571,26 +591,68 @@ int gridFor(long n, int threads) {
   return (int)(g < 1 ? 1 : g);
 }
 
-template <int LIM, bool ROE>
+template <class TL, int LIM, bool ROE>
 cudaError_t launchStageT(const StageArgs& a, int mode, bool powell, bool grav, cudaStream_t s) {
   const int v0 = a.hi[0] - a.lo[0] + 1, v1 = a.hi[1] - a.lo[1] + 1, v2 = a.hi[2] - a.lo[2] + 1;
-  const long blocks = (long)a.nbox * ((v0 + TX - 1) / TX) * ((v1 + TY - 1) / TY) * ((v2 + TZ - 1) / TZ);
-  const size_t smem = stageSmemBytes(mode);
-  if (mode == MODE_BOX) o2StageKernel<LIM, ROE, MODE_BOX><<<(unsigned)blocks, NT, smem, s>>>(a, powell, grav);
-  else if (mode == MODE_RK) o2StageKernel<LIM, ROE, MODE_RK><<<(unsigned)blocks, NT, smem, s>>>(a, powell, grav);
-  else o2StageKernel<LIM, ROE, MODE_RHS><<<(unsigned)blocks, NT, smem, s>>>(a, powell, grav);
+  const long blocks = (long)a.nbox * ((v0 + TL::TX - 1) / TL::TX) * ((v1 + TL::TY - 1) / TL::TY) *
+                      ((v2 + TL::TZ - 1) / TL::TZ);
+  const size_t smem = sizeof(double) * 9 * TL::NF;
+  if (mode == MODE_RK) o2StageKernel<TL, LIM, ROE, MODE_RK><<<(unsigned)blocks, TL::NT, smem, s>>>(a, powell, grav);
+  else o2StageKernel<TL, LIM, ROE, MODE_RHS><<<(unsigned)blocks, TL::NT, smem, s>>>(a, powell, grav);
   return cudaGetLastError();
+}
+
+template <int LIM, bool ROE>
+cudaError_t launchStageTile(const StageArgs& a, int mode, bool powell, bool grav, int tile, cudaStream_t s) {
+  if (mode == MODE_BOX) {
+    // per-box calls keep the default tile
+    const int v0 = a.hi[0] - a.lo[0] + 1, v1 = a.hi[1] - a.lo[1] + 1, v2 = a.hi[2] - a.lo[2] + 1;
+    const long blocks = (long)a.nbox * ((v0 + Tile0::TX - 1) / Tile0::TX) * ((v1 + Tile0::TY - 1) / Tile0::TY) *
+                        ((v2 + Tile0::TZ - 1) / Tile0::TZ);
+    o2StageKernel<Tile0, LIM, ROE, MODE_BOX>
+        <<<(unsigned)blocks, Tile0::NT, sizeof(double) * 9 * Tile0::NF, s>>>(a, powell, grav);
+    return cudaGetLastError();
+  }
+  switch (tile) {
+    case 1: return launchStageT<Tile1, LIM, ROE>(a, mode, powell, grav, s);
+    case 2: return launchStageT<Tile2, LIM, ROE>(a, mode, powell, grav, s);
+    case 3: return launchStageT<Tile3, LIM, ROE>(a, mode, powell, grav, s);
+    case 4: return launchStageT<Tile4, LIM, ROE>(a, mode, powell, grav, s);
+    case 5: return launchStageT<Tile5, LIM, ROE>(a, mode, powell, grav, s);
+    default: return launchStageT<Tile0, LIM, ROE>(a, mode, powell, grav, s);
+  }
+}
+
+template <class TL>
+void tileShape(int* out) {
+  out[0] = TL::TX; out[1] = TL::TY; out[2] = TL::TZ; out[3] = TL::minBlocks(false); out[4] = TL::minBlocks(true);
 }
 
 }  // namespace
 
-size_t stageSmemBytes(int) { return sizeof(double) * 9 * NF; }
+int stageTileShape(int tile, int out[5]) {
+  switch (tile) {
+    case 0: tileShape<Tile0>(out); return 1;
+    case 1: tileShape<Tile1>(out); return 1;
+    case 2: tileShape<Tile2>(out); return 1;
+    case 3: tileShape<Tile3>(out); return 1;
+    case 4: tileShape<Tile4>(out); return 1;
+    case 5: tileShape<Tile5>(out); return 1;
+    default: return 0;
+  }
+}
 
-cudaError_t launchStage(const StageArgs& a, int mode, int limiter, bool roe, bool powell, bool grav, cudaStream_t s) {
+cudaError_t launchStage(const StageArgs& a, int mode, int limiter, bool roe, bool powell, bool grav, cudaStream_t s,
+                        int tile) {
   const int lim = limiter == 0 ? 0 : limiter == 3 ? 3 : 1;
-  if (lim == 0) return roe ? launchStageT<0, true>(a, mode, powell, grav, s) : launchStageT<0, false>(a, mode, powell, grav, s);
-  if (lim == 1) return roe ? launchStageT<1, true>(a, mode, powell, grav, s) : launchStageT<1, false>(a, mode, powell, grav, s);
-  return roe ? launchStageT<3, true>(a, mode, powell, grav, s) : launchStageT<3, false>(a, mode, powell, grav, s);
+  if (lim == 0)
+    return roe ? launchStageTile<0, true>(a, mode, powell, grav, tile, s)
+               : launchStageTile<0, false>(a, mode, powell, grav, tile, s);
+  if (lim == 1)
+    return roe ? launchStageTile<1, true>(a, mode, powell, grav, tile, s)
+               : launchStageTile<1, false>(a, mode, powell, grav, tile, s);
+  return roe ? launchStageTile<3, true>(a, mode, powell, grav, tile, s)
+             : launchStageTile<3, false>(a, mode, powell, grav, tile, s);
 }
 
 cudaError_t launchPrimValid(const DevLevel& L, const double* ju, double* w, cudaStream_t s) {

@@ -102,8 +102,13 @@ struct StageArgs {
 enum { MODE_BOX = 0, MODE_RK = 1, MODE_RHS = 2 };
 
 // Host launchers (hc_kernels.cu).  Every launcher returns a cudaError_t.
+// tile: cell tile of the stage kernel (0 .. kStageTiles-1, see
+// stageTileShape); MODE_BOX launches always use tile 0.
+constexpr int kStageTiles = 6;
 cudaError_t launchStage(const StageArgs& a, int mode, int limiter, bool roe, bool powell, bool grav,
-                        cudaStream_t s);
+                        cudaStream_t s, int tile = 0);
+// {X, Y, Z, min CTAs/SM with Rusanov, with Roe} of a stage tile; 0 if none.
+int stageTileShape(int tile, int out[5]);
 cudaError_t launchPrimValid(const DevLevel& L, const double* ju, double* w, cudaStream_t s);
 // Time of a stage: t = tbase + (tdev ? *tdev : 0) + cfrac * dt, with
 // dt = invDtMax ? cfl / *invDtMax : dtv.
@@ -122,7 +127,6 @@ cudaError_t launchBoxGravity(const DevLevel& L, const int lo[3], const int hi[3]
                              const int wlo[3], const int wn[3], double* rhs, cudaStream_t s);
 cudaError_t launchAdvanceTime(double* time, const double* invDtMax, double cfl, double* dtOut, cudaStream_t s);
 cudaError_t launchBitsToDouble(const unsigned long long* bits, double* out, cudaStream_t s);
-size_t stageSmemBytes(int mode);
 
 }  // namespace hc
 

@@ -55,13 +55,14 @@ class Params:
     berta_detector_type: int = 0   # Jameson
     berta_fallback_type: int = 0   # 0 WENO3, 1 PLM
     berta_eta_d: float = 0.02
+    autotune: int = 0              # order 2: time the stage tiles on the first step
 
     def to_c(self) -> N.HcParams:
         p = N.HcParams()
         for k in ("nr", "na", "spatial_order", "limiter", "riemann_solver", "divergence_cleaning",
                   "sun_gravity", "init_condition_type", "temporal_order", "gamma", "entropy_fix_coeff",
                   "cfl", "inner_radius", "outer_radius", "radial_stretch", "strength", "spatial_operator",
-                  "berta_detector_type", "berta_fallback_type", "berta_eta_d"):
+                  "berta_detector_type", "berta_fallback_type", "berta_eta_d", "autotune"):
             setattr(p, k, getattr(self, k))
         return p
 
@@ -233,6 +234,16 @@ class ConeSpec:
         return spec
 
 
+def stage_tiles() -> np.ndarray:
+    """Candidate tiles of the order-2 stage kernel, [tiles][5]: cells x, y,
+    z, min CTAs per SM with Rusanov, with Roe (hc_stage_tiles)."""
+    lib = N.lib()
+    n = lib.hc_stage_tiles(None, 0)
+    out = (C.c_int * (5 * n))()
+    lib.hc_stage_tiles(out, n)
+    return np.array(out[:], dtype=np.int64).reshape(n, 5)
+
+
 def prepare_cone(spec: ConeSpec, inner_radius: float) -> N.HcCone:
     """hc_cone_prepare: the cloud's geometry and timing (host arithmetic)."""
     out = N.HcCone()
@@ -316,6 +327,20 @@ class Shell:
         dvolr = self.geometry(0).reshape(p.nr + 1, 4)[:p.nr, 3]
         ju = perturbed_wind_state(p, det, dvolr, seed, amp)
         return torch.from_numpy(np.ascontiguousarray(ju.reshape(-1))).to(self._dev)
+
+    def autotune(self, ju: torch.Tensor) -> tuple[tuple[int, int], np.ndarray]:
+        """hc_ctx_autotune (order 2): time the stage tiles on this level with
+        the state `ju` (not modified); returns ((RK stage tile, operator
+        tile), median ms [2][tiles])."""
+        n = stage_tiles().shape[0]
+        tiles = (C.c_int * 2)()
+        ms = np.zeros(2 * n)
+        N.check(self._lib.hc_ctx_autotune(self._ctx, _ptr(ju), tiles, ms.ctypes.data_as(C.c_void_p), _stream()),
+                "hc_ctx_autotune")
+        return (tiles[0], tiles[1]), ms.reshape(2, n)
+
+    def set_tiles(self, tile_rk: int = -1, tile_rhs: int = -1) -> None:
+        N.check(self._lib.hc_ctx_set_tiles(self._ctx, tile_rk, tile_rhs), "hc_ctx_set_tiles")
 
     def insert_cone(self, cone: N.HcCone, time: float, ju: torch.Tensor, stats: bool = False) -> torch.Tensor | None:
         """Volume insertion of a prepared cone cloud into `ju` at `time`

@@ -52,7 +52,8 @@ typedef struct hc_params {
   int spatial_operator;     /* at order 4: 2 = Berta WENOZ (Inputs_Parsing.H:78) */
   int berta_detector_type;  /* 0 Jameson (Inputs_Parsing.H:82-84) */
   int berta_fallback_type;  /* 0 WENO3, 1 PLM (theta = 1.5 minmod3) */
-  int reserved_i[4];
+  int autotune;             /* 1: time the order-2 stage tiles on the first level step (hc_ctx_autotune) */
+  int reserved_i[3];
   double gamma;             /* ratio of specific heats */
   double entropy_fix_coeff; /* Roe entropy fix, default 0.3 */
   double cfl;               /* dt = cfl / max(inverse dt) */
@@ -236,6 +237,33 @@ int hc_level_dt_cfl(hc_ctx* ctx, const double* ju, double* inv_dt_max,
  * and density is positive, else 0.  Replaces validConservedState
  * (src/BoxOp_EulerCubedSphereImplem.H:817-876). */
 int hc_level_valid(hc_ctx* ctx, const double* ju, int* ok, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Tile autotuner of the second-order stage kernel (no reference counterpart:
+ * the reference runs the face loop on the host).  The stage kernel runs one
+ * CTA per cell tile; the tiles differ in shape and in the register cap
+ * (resident CTAs per SM), and the fastest depends on the limiter / solver
+ * pair and the level size.  Results never depend on the tile.
+ * ------------------------------------------------------------------------- */
+
+/* Number of candidate tiles; with shapes non-null, shapes[5 t .. 5 t + 4] =
+ * {cells x, y, z, min CTAs per SM with Rusanov, with Roe} for t < capacity. */
+int hc_stage_tiles(int* shapes, int capacity);
+
+/* Time every tile on this context's level with the state ju (device, not
+ * modified): the fused RK stage (its first stage, into the context's
+ * workspace) and the operator alone (hc_level_rhs), a few launches each on
+ * `stream`, and keep the fastest of each for the context.  Blocks the host
+ * until the timing is done: call it outside stream capture.  tiles (host,
+ * nullable) gets {RK stage tile, operator tile}; ms (host, nullable,
+ * 2 x count) the median launch times, RK stage first.  The choice is also
+ * kept process-wide for contexts of the same device, level size and scheme,
+ * which then skip the timing.  Order-2 contexts only. */
+int hc_ctx_autotune(hc_ctx* ctx, const double* ju, int* tiles, double* ms, void* stream);
+
+/* Use the given tiles (0 .. count-1) for the RK stage and the operator
+ * alone; -1 keeps the current one. */
+int hc_ctx_set_tiles(hc_ctx* ctx, int tile_rk, int tile_rhs);
 
 /* Seeded synthetic initial state (valid cells) of the level. */
 int hc_level_init(hc_ctx* ctx, const hc_init* init, double* ju, void* stream);

@@ -303,9 +303,8 @@ def run_b200(args, world, rank, local):
     else:
         ju0 = shell.init(InitSpec.seeded(args.seed, args.nr, args.na))
     ju = ju0.clone()
-    tuning = None
+    # autotuner: time the candidates on this level, keep the fastest
     if args.order == 2:
-        # stage-tile autotuner: time the candidate tiles on this level, keep the fastest
         from heliocubed_b200.level import stage_tiles
         (trk, trhs), tms = shell.autotune(ju0)
         shapes = stage_tiles()
@@ -314,6 +313,14 @@ def run_b200(args, world, rank, local):
                   "rk_stage_ms": [round(float(x), 5) for x in tms[0]],
                   "operator_ms": [round(float(x), 5) for x in tms[1]],
                   "tile_fields": "cells x, y, z, min CTAs/SM Rusanov, Roe"}
+    else:
+        from heliocubed_b200.level import o4_variants
+        var, vms = shell.autotune(ju0)
+        mb = o4_variants()
+        names = ("reconstruction", "roe_point", "final_flux")
+        tuning = {"min_ctas_per_sm": {n: int(mb[q, var[q]]) for q, n in enumerate(names)},
+                  "candidates": {n: [int(x) for x in mb[q]] for q, n in enumerate(names)},
+                  "operator_ms": {n: [round(float(x), 4) for x in vms[q]] for q, n in enumerate(names)}}
     time_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
     state_bytes = ju.numel() * 8

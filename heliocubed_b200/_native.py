@@ -44,6 +44,8 @@ SIGNATURES = {
     "hc_stage_tiles": (C.c_int, [_VP, C.c_int]),
     "hc_ctx_autotune": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "hc_ctx_set_tiles": (C.c_int, [_VP, C.c_int, C.c_int]),
+    "hc_o4_variants": (C.c_int, [_VP, C.c_int]),
+    "hc_ctx_set_o4_variants": (C.c_int, [_VP, _VP]),
     "hc_level_insert_cone": (C.c_int, [_VP, _VP, C.c_double, _VP, _VP, _VP]),
 }
 

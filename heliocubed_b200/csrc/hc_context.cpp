@@ -248,6 +248,8 @@ struct hc_ctx {
   int* flag = nullptr;
   // cell tiles of the order-2 stage kernel: fused RK stage, operator alone
   int tileRK = 0, tileRHS = 0;
+  // register-cap variants of the fourth-order operator's tuned kernels
+  int o4var[kO4TunedKernels] = {0, 0, 0};
   bool tuned = false;
   // fourth-order operator: metric tables and grow-only scratch
   O4Geo o4{};
@@ -927,6 +929,7 @@ int o4Step(hc_ctx* c, double* ju, double dtv, const double* invMax, double tbase
       if (rc != HC_OK) break;
     }
     const RegArgs rg{c->o4reg, invMax ? b4[stage] : dtv * b4[stage], invMax, c->P.cfl};
+    o4BatchSetVariants(c->o4levelBatch, c->o4var);
     rc = checkLaunch(launchO4Batch(c->o4levelBatch, &rg, s), "O4 operator");
     if (rc == HC_OK)
       rc = checkLaunch(launchO4Update(O, stage, c->o4k, ju, c->acc, c->o4next, invMax, c->P.cfl, dtv, s), "O4 update");
@@ -1075,6 +1078,7 @@ int hc_box_rhs_o4(hc_ctx* c, const hc_box* box, const double* usph, double scale
   int rc = HC_OK;
   O4Batch* batch = cachedBatch(c, a, &rc);
   if (!batch) return rc;
+  o4BatchSetVariants(batch, c->o4var);
   return checkLaunch(launchO4Batch(batch, nullptr, (cudaStream_t)stream), "hc_box_rhs_o4");
 }
 
@@ -1157,6 +1161,7 @@ int hc_o4_batch_rhs(hc_ctx* c, hc_o4_batch* h, void* stream) {
     const int rc = checkLaunch(launchO4BatchGravity(h->batch, s), "batch gravity");
     if (rc != HC_OK) return rc;
   }
+  o4BatchSetVariants(h->batch, c->o4var);
   return checkLaunch(launchO4Batch(h->batch, nullptr, s), "batch operator");
 }
 
@@ -1236,6 +1241,7 @@ int hc_level_rhs(hc_ctx* c, const double* w, double* k, void* stream) {
     rc = checkLaunch(cudaMemsetAsync(k, 0, sizeof(double) * 6 * NC * c->o4l.Nv, s), "O4 k");
     if (rc == HC_OK && c->P.sun_gravity) rc = checkLaunch(launchO4BatchGravity(B, s), "O4 gravity");
     if (rc != HC_OK) return rc;
+    o4BatchSetVariants(B, c->o4var);
     return checkLaunch(launchO4Batch(B, nullptr, s), "O4 operator");
   }
   StageArgs a = levelArgs(c, w);
@@ -1340,23 +1346,84 @@ int autotuneStage(hc_ctx* c, const double* ju, cudaStream_t s, int* tilesOut, do
   return HC_OK;
 }
 
-// With hc_params.autotune set: take a cached choice, or time the tiles once
-// (outside stream capture only; a capturing stream keeps the current tiles).
-int maybeAutotune(hc_ctx* c, const double* ju, cudaStream_t s) {
-  if (!c->P.autotune || c->tuned || c->P.spatial_order != 2) return HC_OK;
+std::map<std::string, std::vector<int>> g_o4Cache;
+
+std::string o4Key(const hc_ctx* c) {
+  const hc_params& P = c->P;
+  char key[160];
+  std::snprintf(key, sizeof key, "o4:%d:%d:%d:%d:%d:%d:%d", c->device, P.nr, P.na, P.riemann_solver == 2 ? 1 : 0,
+                P.divergence_cleaning == 1 ? 1 : 0, P.sun_gravity == 1 ? 1 : 0, P.berta_fallback_type);
+  return key;
+}
+
+// Fourth order: the state's stage preparation into the level workspace, then
+// the level operator timed for each register-cap variant of one tuned kernel
+// at a time, the others held at the best found so far (coordinate descent
+// over reconstruction, Roe point dissipation, final flux).
+int autotuneO4(hc_ctx* c, const double* ju, cudaStream_t s, int* tilesOut, double* msOut) {
+  int rc = ensureO4Buffers(c);
+  if (rc != HC_OK) return rc;
+  O4StageIO io{c->o4l, ju, c->o4cart, c->o4us, c->o4pv, StageTime{0.0, nullptr, 0.0, nullptr, 0.0}};
+  rc = checkLaunch(launchO4Prepare(io, s), "autotune O4 prepare");
+  int best[kO4TunedKernels] = {0, 0, 0};
+  for (int q = 0; q < kO4TunedKernels && rc == HC_OK; ++q) {
+    if (q == 1 && c->P.riemann_solver != 2) {  // no Roe point kernel with Rusanov
+      for (int v = 0; v < kO4Variants && msOut; ++v) msOut[q * kO4Variants + v] = 0.0;
+      continue;
+    }
+    double bestMs = 1e300;
+    for (int v = 0; v < kO4Variants && rc == HC_OK; ++v) {
+      int var[kO4TunedKernels] = {best[0], best[1], best[2]};
+      var[q] = v;
+      o4BatchSetVariants(c->o4levelBatch, var);
+      double ms = 0;
+      rc = timeLaunches([&]() { return checkLaunch(launchO4Batch(c->o4levelBatch, nullptr, s), "autotune O4"); }, s, 5,
+                        &ms);
+      if (rc != HC_OK) break;
+      if (msOut) msOut[q * kO4Variants + v] = ms;
+      if (ms < bestMs) { bestMs = ms; best[q] = v; }
+    }
+  }
+  o4BatchSetVariants(c->o4levelBatch, c->o4var);
+  if (rc != HC_OK) return rc;
+  for (int q = 0; q < kO4TunedKernels; ++q) c->o4var[q] = best[q];
+  c->tuned = true;
   {
     std::lock_guard<std::mutex> lock(g_tileMutex);
-    auto it = g_tileCache.find(tileKey(c));
-    if (it != g_tileCache.end()) {
-      c->tileRK = it->second.first;
-      c->tileRHS = it->second.second;
-      c->tuned = true;
-      return HC_OK;
+    g_o4Cache[o4Key(c)] = std::vector<int>(best, best + kO4TunedKernels);
+  }
+  if (tilesOut)
+    for (int q = 0; q < kO4TunedKernels; ++q) tilesOut[q] = best[q];
+  return HC_OK;
+}
+
+// With hc_params.autotune set: take a cached choice, or time the candidates
+// once (outside stream capture only; a capturing stream keeps the current
+// choice).
+int maybeAutotune(hc_ctx* c, const double* ju, cudaStream_t s) {
+  if (!c->P.autotune || c->tuned) return HC_OK;
+  {
+    std::lock_guard<std::mutex> lock(g_tileMutex);
+    if (c->P.spatial_order == 2) {
+      auto it = g_tileCache.find(tileKey(c));
+      if (it != g_tileCache.end()) {
+        c->tileRK = it->second.first;
+        c->tileRHS = it->second.second;
+        c->tuned = true;
+        return HC_OK;
+      }
+    } else {
+      auto it = g_o4Cache.find(o4Key(c));
+      if (it != g_o4Cache.end()) {
+        for (int q = 0; q < kO4TunedKernels; ++q) c->o4var[q] = it->second[q];
+        c->tuned = true;
+        return HC_OK;
+      }
     }
   }
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return HC_OK;
-  return autotuneStage(c, ju, s, nullptr, nullptr);
+  return c->P.spatial_order == 2 ? autotuneStage(c, ju, s, nullptr, nullptr) : autotuneO4(c, ju, s, nullptr, nullptr);
 }
 
 }  // namespace
@@ -1370,8 +1437,25 @@ int hc_stage_tiles(int* shapes, int capacity) {
 
 int hc_ctx_autotune(hc_ctx* c, const double* ju, int* tiles, double* ms, void* stream) {
   if (!c || !ju) return fail(HC_ERR_ARG, "null argument");
-  if (c->P.spatial_order != 2) return fail(HC_ERR_UNSUPPORTED, "hc_ctx_autotune: order-2 contexts only");
+  if (c->P.spatial_order == 4) return autotuneO4(c, ju, (cudaStream_t)stream, tiles, ms);
   return autotuneStage(c, ju, (cudaStream_t)stream, tiles, ms);
+}
+
+int hc_o4_variants(int* min_blocks, int capacity) {
+  for (int q = 0; min_blocks && q < kO4TunedKernels; ++q)
+    for (int v = 0; v < kO4Variants && q * kO4Variants + v < capacity; ++v)
+      min_blocks[q * kO4Variants + v] = o4VariantMinBlocks(q, v);
+  return kO4Variants;
+}
+
+int hc_ctx_set_o4_variants(hc_ctx* c, const int* variants) {
+  if (!c || !variants) return fail(HC_ERR_ARG, "null argument");
+  for (int q = 0; q < kO4TunedKernels; ++q)
+    if (variants[q] < -1 || variants[q] >= kO4Variants) return fail(HC_ERR_ARG, "variant index out of range");
+  for (int q = 0; q < kO4TunedKernels; ++q)
+    if (variants[q] >= 0) c->o4var[q] = variants[q];
+  c->tuned = true;
+  return HC_OK;
 }
 
 int hc_ctx_set_tiles(hc_ctx* c, int tileRK, int tileRHS) {
@@ -1389,7 +1473,8 @@ int hc_level_rk4_step(hc_ctx* c, double* ju, double dt, double t, void* stream) 
   if (!(dt > 0)) return fail(HC_ERR_ARG, "dt must be positive");
   cudaStream_t s = (cudaStream_t)stream;
   if (c->P.spatial_order == 4) {
-    const int rc4 = ensureO4Buffers(c);
+    int rc4 = ensureO4Buffers(c);
+    if (rc4 == HC_OK) rc4 = maybeAutotune(c, ju, s);
     return rc4 != HC_OK ? rc4 : o4Step(c, ju, dt, nullptr, t, nullptr, s);
   }
   int rc = maybeAutotune(c, ju, s);
@@ -1405,6 +1490,7 @@ int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, do
   if (c->P.spatial_order == 4) {
     // dtCFL of the state at the start of each step, then the step.
     int rc = ensureO4Buffers(c);
+    if (rc == HC_OK) rc = maybeAutotune(c, ju, s);
     const double* invMax = reinterpret_cast<const double*>(c->invMax);
     for (int n = 0; n < nsteps && rc == HC_OK; ++n) {
       rc = checkLaunch(launchCfl(c->L, ju, c->invMax, s), "cfl");

@@ -200,6 +200,12 @@ struct RegArgs {
 // is one launch over the whole batch (one CTA row per box).  Each entry of
 // `boxes` describes one box (nbox 1) with its own input, output and scratch.
 struct O4Batch;
+// Register-cap variants of the operator's three heaviest kernels
+// (reconstruction, Roe point dissipation, final flux), chosen by the
+// autotuner; results do not depend on them.
+constexpr int kO4TunedKernels = 3, kO4Variants = 3;
+void o4BatchSetVariants(O4Batch* b, const int v[kO4TunedKernels]);
+int o4VariantMinBlocks(int kernel, int variant);
 O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err);
 void o4BatchDestroy(O4Batch* b);
 // The one-box argument sets of a uniform multi-box O4Args (box b on panel

@@ -479,8 +479,8 @@ __device__ __forceinline__ const double* faceBasis(const Ctx& c, int b, int j, i
 
 // 4. reconstruction (WENOZ / WENO3 / PLM with clamps), Roe repair, energies,
 // point flux sum, total-pressure sum, centred normal B, Rusanov jump (F).
-template <int D>
-__global__ void __launch_bounds__(128, 6) o4FaceReconKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+template <int D, int MB>
+__global__ void __launch_bounds__(128, MB) o4FaceReconKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
   const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
@@ -569,8 +569,8 @@ __global__ void __launch_bounds__(128, 6) o4FaceReconKernel(const Ctx* __restric
 
 // 4b. pointwise factored Roe dissipation on the final faces + one transverse
 // ring (src/BoxOp_RoeCubedSphere.H:73-98).
-template <int D>
-__global__ void __launch_bounds__(128, 4) o4RoePointKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+template <int D, int MB>
+__global__ void __launch_bounds__(128, MB) o4RoePointKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
   const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
@@ -711,8 +711,8 @@ __global__ void o4FaceRadialKernel(const Ctx* __restrict__ tab, const RegArgs rg
 
 // 8. pressure force, dissipation, combine on the final faces V0; writes the
 // flux (scratch and caller).
-template <int D>
-__global__ void __launch_bounds__(128, 6) o4FaceFinalKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
+template <int D, int MB>
+__global__ void __launch_bounds__(128, MB) o4FaceFinalKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
   const Ctx& c = tab[blockIdx.y * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
@@ -1072,7 +1072,22 @@ struct O4Batch {
   Ctx* dev = nullptr;
   std::vector<Ctx> host;
   bool roe = false, powell = false;
+  int var[kO4TunedKernels] = {0, 0, 0};  // register-cap variant of the tuned kernels
 };
+
+// Minimum resident CTAs per SM (the register cap) of each variant of the
+// tuned kernels: reconstruction, Roe point dissipation, final flux.
+// Variant 0 is the default.
+constexpr int kO4MinBlocks[kO4TunedKernels][kO4Variants] = {{6, 4, 8}, {4, 3, 5}, {6, 4, 8}};
+
+void o4BatchSetVariants(O4Batch* B, const int v[kO4TunedKernels]) {
+  for (int q = 0; q < kO4TunedKernels; ++q) B->var[q] = v[q] >= 0 && v[q] < kO4Variants ? v[q] : 0;
+}
+
+int o4VariantMinBlocks(int kernel, int variant) {
+  return kernel >= 0 && kernel < kO4TunedKernels && variant >= 0 && variant < kO4Variants ? kO4MinBlocks[kernel][variant]
+                                                                                          : 0;
+}
 
 O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
   *err = cudaSuccess;
@@ -1158,16 +1173,27 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
   if (d == 0) { HC_LAUNCH(kernel<0>, 0, region) }                                       \
   else if (d == 1) { HC_LAUNCH(kernel<1>, 1, region) }                                  \
   else { HC_LAUNCH(kernel<2>, 2, region) }
+#define HC_LAUNCH_DM(kernel, q, region)                                                  \
+  if (B->var[q] == 1) { HC_LAUNCH_DV(kernel, kO4MinBlocks[q][1], region) }                \
+  else if (B->var[q] == 2) { HC_LAUNCH_DV(kernel, kO4MinBlocks[q][2], region) }           \
+  else { HC_LAUNCH_DV(kernel, kO4MinBlocks[q][0], region) }
+#define HC_LAUNCH_T(d, region, ...)                                                      \
+  __VA_ARGS__<<<gridOf(*B, d, [](const Ctx& c) { return region; }), 128, 0, s>>>(t, rg);  \
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+#define HC_LAUNCH_DV(kernel, mb, region)                                                 \
+  if (d == 0) { HC_LAUNCH_T(0, region, kernel<0, mb>) }                                 \
+  else if (d == 1) { HC_LAUNCH_T(1, region, kernel<1, mb>) }                            \
+  else { HC_LAUNCH_T(2, region, kernel<2, mb>) }
   HC_LAUNCH(o4PrimAvgKernel, 0, c.G)
   HC_LAUNCH(o4ThetaRawKernel, 0, c.GR)
   HC_LAUNCH(o4PointKernel, 0, c.G)
   for (int d = 0; d < 3; ++d) {
-    HC_LAUNCH_D(o4FaceReconKernel, c.F)
-    if (B->roe) { HC_LAUNCH_D(o4RoePointKernel, c.V0.growTrans(c.d, 1)) }
+    HC_LAUNCH_DM(o4FaceReconKernel, 0, c.F)
+    if (B->roe) { HC_LAUNCH_DM(o4RoePointKernel, 1, c.V0.growTrans(c.d, 1)) }
     HC_LAUNCH_D(o4FaceAvgKernel, c.F1)
     HC_LAUNCH_D(o4FaceMapKernel, c.F)
     HC_LAUNCH_D(o4FaceRadialKernel, c.F1)
-    HC_LAUNCH_D(o4FaceFinalKernel, c.V0)
+    HC_LAUNCH_DM(o4FaceFinalKernel, 2, c.V0)
     HC_LAUNCH_D(o4DivKernel, c.V)
     if (B->powell) {
       HC_LAUNCH_D(o4PowellFluxKernel, c.V1.extrude(c.d).growTrans(c.d, 1))
@@ -1180,6 +1206,9 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
     HC_LAUNCH(o4PowellAvgKernel, 0, c.V1)
     HC_LAUNCH(o4PowellApplyKernel, 0, c.V)
   }
+#undef HC_LAUNCH_DV
+#undef HC_LAUNCH_T
+#undef HC_LAUNCH_DM
 #undef HC_LAUNCH_D
 #undef HC_LAUNCH
   return cudaSuccess;

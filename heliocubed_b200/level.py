@@ -234,6 +234,17 @@ class ConeSpec:
         return spec
 
 
+def o4_variants() -> np.ndarray:
+    """Minimum resident CTAs per SM of each register-cap variant of the
+    fourth-order operator's tuned kernels, [kernel][variant]: reconstruction,
+    Roe point dissipation, final flux (hc_o4_variants)."""
+    lib = N.lib()
+    n = lib.hc_o4_variants(None, 0)
+    out = (C.c_int * (3 * n))()
+    lib.hc_o4_variants(out, 3 * n)
+    return np.array(out[:], dtype=np.int64).reshape(3, n)
+
+
 def stage_tiles() -> np.ndarray:
     """Candidate tiles of the order-2 stage kernel, [tiles][5]: cells x, y,
     z, min CTAs per SM with Rusanov, with Roe (hc_stage_tiles)."""
@@ -328,16 +339,24 @@ class Shell:
         ju = perturbed_wind_state(p, det, dvolr, seed, amp)
         return torch.from_numpy(np.ascontiguousarray(ju.reshape(-1))).to(self._dev)
 
-    def autotune(self, ju: torch.Tensor) -> tuple[tuple[int, int], np.ndarray]:
-        """hc_ctx_autotune (order 2): time the stage tiles on this level with
-        the state `ju` (not modified); returns ((RK stage tile, operator
-        tile), median ms [2][tiles])."""
-        n = stage_tiles().shape[0]
-        tiles = (C.c_int * 2)()
-        ms = np.zeros(2 * n)
+    def autotune(self, ju: torch.Tensor) -> tuple[tuple[int, ...], np.ndarray]:
+        """hc_ctx_autotune with the state `ju` (not modified).  Order 2:
+        ((RK stage tile, operator tile), median ms [2][tiles]).  Order 4:
+        ((reconstruction, Roe point, final flux variant), operator ms
+        [3][variants])."""
+        if self.params.spatial_order == 4:
+            rows, n = 3, o4_variants().shape[1]
+        else:
+            rows, n = 2, stage_tiles().shape[0]
+        tiles = (C.c_int * rows)()
+        ms = np.zeros(rows * n)
         N.check(self._lib.hc_ctx_autotune(self._ctx, _ptr(ju), tiles, ms.ctypes.data_as(C.c_void_p), _stream()),
                 "hc_ctx_autotune")
-        return (tiles[0], tiles[1]), ms.reshape(2, n)
+        return tuple(tiles[:]), ms.reshape(rows, n)
+
+    def set_o4_variants(self, recon: int = -1, roe: int = -1, final: int = -1) -> None:
+        v = (C.c_int * 3)(recon, roe, final)
+        N.check(self._lib.hc_ctx_set_o4_variants(self._ctx, v), "hc_ctx_set_o4_variants")
 
     def set_tiles(self, tile_rk: int = -1, tile_rhs: int = -1) -> None:
         N.check(self._lib.hc_ctx_set_tiles(self._ctx, tile_rk, tile_rhs), "hc_ctx_set_tiles")

@@ -82,7 +82,8 @@ class Request:
 
     def params(self) -> Params:
         if self.order == 4:
-            return Params(nr=self.nr, na=self.na, spatial_order=4, riemann_solver=2, berta_fallback_type=0)
+            return Params(nr=self.nr, na=self.na, spatial_order=4, riemann_solver=2, berta_fallback_type=0,
+                          autotune=1)
         return Params(nr=self.nr, na=self.na, spatial_order=2, limiter=3, riemann_solver=1, autotune=1)
 
 

@@ -239,27 +239,45 @@ int hc_level_dt_cfl(hc_ctx* ctx, const double* ju, double* inv_dt_max,
 int hc_level_valid(hc_ctx* ctx, const double* ju, int* ok, void* stream);
 
 /* ---------------------------------------------------------------------------
- * Tile autotuner of the second-order stage kernel (no reference counterpart:
- * the reference runs the face loop on the host).  The stage kernel runs one
- * CTA per cell tile; the tiles differ in shape and in the register cap
- * (resident CTAs per SM), and the fastest depends on the limiter / solver
- * pair and the level size.  Results never depend on the tile.
+ * Autotuner (no reference counterpart: the reference runs its face loops on
+ * the host).  Order 2: the stage kernel runs one CTA per cell tile; the
+ * tiles differ in shape and in the register cap (resident CTAs per SM), and
+ * the fastest depends on the limiter / solver pair and the level size.
+ * Order 4: the reconstruction, Roe point and final-flux kernels each come
+ * in register-cap variants.  Order-2 results do not depend on the tile.  The
+ * order-4 variants agree to round-off only: the code generator may contract
+ * a multiply and an add into one fused operation differently under each
+ * register cap.  Contexts that take the process-wide choice all use the same
+ * variants.
  * ------------------------------------------------------------------------- */
 
 /* Number of candidate tiles; with shapes non-null, shapes[5 t .. 5 t + 4] =
  * {cells x, y, z, min CTAs per SM with Rusanov, with Roe} for t < capacity. */
 int hc_stage_tiles(int* shapes, int capacity);
 
-/* Time every tile on this context's level with the state ju (device, not
- * modified): the fused RK stage (its first stage, into the context's
- * workspace) and the operator alone (hc_level_rhs), a few launches each on
- * `stream`, and keep the fastest of each for the context.  Blocks the host
- * until the timing is done: call it outside stream capture.  tiles (host,
- * nullable) gets {RK stage tile, operator tile}; ms (host, nullable,
- * 2 x count) the median launch times, RK stage first.  The choice is also
- * kept process-wide for contexts of the same device, level size and scheme,
- * which then skip the timing.  Order-2 contexts only. */
+/* Order 2: time every tile on this context's level with the state ju
+ * (device, not modified): the fused RK stage (its first stage, into the
+ * context's workspace) and the operator alone (hc_level_rhs), a few launches
+ * each on `stream`, and keep the fastest of each for the context.  tiles
+ * (host, nullable, 2 ints) gets {RK stage tile, operator tile}; ms (host,
+ * nullable, 2 x count doubles) the median launch times, RK stage first.
+ * Order 4: time the level operator (after the stage preparation of ju) for
+ * each register-cap variant of the reconstruction, Roe point dissipation
+ * and final-flux kernels in turn, keeping the best of each; tiles (3 ints)
+ * gets the variants, ms (3 x hc_o4_variants() doubles) the operator times.
+ * Blocks the host until the timing is done: call it outside stream capture.
+ * The choice is also kept process-wide for contexts of the same device,
+ * level size and scheme, which then skip the timing when created with
+ * hc_params.autotune = 1. */
 int hc_ctx_autotune(hc_ctx* ctx, const double* ju, int* tiles, double* ms, void* stream);
+
+/* Number of register-cap variants per tuned fourth-order kernel; with
+ * min_blocks non-null, min_blocks[3 q + v] = minimum resident CTAs per SM of
+ * variant v of kernel q (0 reconstruction, 1 Roe point, 2 final flux). */
+int hc_o4_variants(int* min_blocks, int capacity);
+
+/* Use the given variants (3 ints, -1 keeps the current one). */
+int hc_ctx_set_o4_variants(hc_ctx* ctx, const int* variants);
 
 /* Use the given tiles (0 .. count-1) for the RK stage and the operator
  * alone; -1 keeps the current one. */

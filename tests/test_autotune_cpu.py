@@ -38,3 +38,12 @@ def test_capacity_is_respected():
     n = lib.hc_stage_tiles(buf, 1)
     assert n == stage_tiles().shape[0]
     assert buf[5] == -7 and buf[0] == 16
+
+
+def test_o4_variants_table():
+    from heliocubed_b200.level import o4_variants
+    v = o4_variants()
+    assert v.shape == (3, 3)
+    # variant 0 is the default register cap of each kernel; all caps fit 128-thread CTAs
+    assert tuple(v[:, 0]) == (6, 4, 6)
+    assert (v >= 1).all() and (65536 // (v * 128) >= 64).all()

@@ -1,8 +1,9 @@
-"""Stage-tile autotuner on the GPU (hc_ctx_autotune, hc_ctx_set_tiles): every
-candidate tile of the order-2 stage kernel gives bit-identical RK4 steps and
-operator results (the tile only changes which CTA computes a face), the tuner
-leaves the state untouched and picks a timed candidate, and automatic tuning
-on the first step changes no result.  Tolerance: exact."""
+"""Autotuner on the GPU (hc_ctx_autotune, hc_ctx_set_tiles,
+hc_ctx_set_o4_variants).  Order 2: every candidate tile of the stage kernel
+gives bit-identical RK4 steps and operator results (the tile only changes
+which CTA computes a face), the tuner leaves the state untouched and picks a
+timed candidate, and automatic tuning on the first step changes no result
+(exact).  Order 4: the register-cap variants agree to round-off (1e-13)."""
 from __future__ import annotations
 
 import numpy as np
@@ -73,3 +74,35 @@ def test_automatic_tuning_changes_no_result():
     tuned.advance(b, 3, tb)
     torch.cuda.synchronize()
     assert torch.equal(a, b) and torch.equal(ta, tb)
+
+
+def test_o4_variants_agree_and_tune():
+    """Every register-cap variant of the fourth-order operator's tuned
+    kernels gives the same level step to round-off (1e-13 normwise per
+    component: the code generator contracts multiply-adds per variant), and
+    the tuner picks the fastest timed variant of each without touching the
+    state; with the variant fixed, steps repeat bit for bit."""
+    _need_gpu()
+    from conftest import rel_err_components
+    sh = hc.Shell(hc.Params(nr=16, na=16, spatial_order=4, riemann_solver=2))
+    ju0 = sh.init_perturbed_wind(4)
+    ref = None
+    for v in range(3):
+        sh.set_o4_variants(v, v, v)
+        ju = ju0.clone()
+        sh.rk4_step(ju, 50.0, 0.0)
+        again = ju0.clone()
+        sh.rk4_step(again, 50.0, 0.0)
+        torch.cuda.synchronize()
+        assert torch.equal(ju, again), v
+        if ref is None:
+            ref = ju
+        else:
+            err = rel_err_components(ju.cpu().numpy().reshape(6, 8, -1), ref.cpu().numpy().reshape(6, 8, -1))
+            assert err.max() < 1e-13, (v, err)
+    before = ju0.clone()
+    var, ms = sh.autotune(ju0)
+    assert torch.equal(ju0, before)
+    assert ms.shape == (3, 3) and (ms > 0).all()
+    for q in range(3):
+        assert ms[q, var[q]] == ms[q].min()

@@ -45,6 +45,10 @@ SIGNATURES = {
     "hc_ctx_autotune": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "hc_ctx_set_tiles": (C.c_int, [_VP, C.c_int, C.c_int]),
     "hc_o4_variants": (C.c_int, [_VP, C.c_int]),
+    "hc_amr_plan_create": (C.c_int, [_VP, _VP, C.c_int, _VP, C.c_int, _VP]),
+    "hc_amr_plan_destroy": (C.c_int, [_VP]),
+    "hc_amr_rk_stage": (C.c_int, [_VP, _VP, C.c_int, C.c_int, C.c_double, _VP]),
+    "hc_amr_restrict": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_ctx_set_o4_variants": (C.c_int, [_VP, _VP]),
     "hc_level_insert_cone": (C.c_int, [_VP, _VP, C.c_double, _VP, _VP, _VP]),
 }
@@ -97,6 +101,18 @@ class HcConeSpec(C.Structure):
 class HcCone(C.Structure):
     """Mirror of hc_cone in include/hc_abi.h."""
     _fields_ = [("axis", C.c_double * 3)] + [(n, C.c_double) for n in _CONE] + [("reserved", C.c_double * 6)]
+
+
+class HcRkBox(C.Structure):
+    """Mirror of hc_rk_box in include/hc_abi.h."""
+    _fields_ = [("ncells", C.c_longlong), ("state", C.c_void_p), ("stage", C.c_void_p), ("rk", C.c_void_p * 4)]
+
+
+class HcRestrictBox(C.Structure):
+    """Mirror of hc_restrict_box in include/hc_abi.h."""
+    _fields_ = [("fine", C.c_void_p), ("coarse", C.c_void_p), ("fine_lo", C.c_int * 3), ("fine_n", C.c_int * 3),
+                ("coarse_lo", C.c_int * 3), ("coarse_n", C.c_int * 3), ("lo", C.c_int * 3), ("hi", C.c_int * 3),
+                ("ratio", C.c_int * 3), ("reserved", C.c_int)]
 
 
 class HcError(RuntimeError):

@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", os.path.join(REPO, "include")]
-SOURCES = ["hc_kernels.cu", "hc_context.cpp", "hc_noalloc.cu", "hc_o4.cu", "hc_o4level.cu", "hc_cme.cu"]
+SOURCES = ["hc_kernels.cu", "hc_context.cpp", "hc_noalloc.cu", "hc_o4.cu", "hc_o4level.cu", "hc_cme.cu", "hc_amr.cu"]
 HEADERS = ["hc_device.cuh", "hc_level.h", "hc_common.h"]
 
 

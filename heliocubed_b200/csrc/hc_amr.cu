@@ -1,0 +1,208 @@
+// AMR Runge-Kutta stage logic on uneven boxes: the tableau combination of
+// advanceRungeKuttaSynchronous (src/MHD_AMRRungeKutta.H:5-41) and the
+// fine-to-coarse restriction restrictTo / Stencil::AvgDown
+// (src/MHD_AMR.H:597-609), each one launch over a device work list of boxes
+// (one CTA row per box, the CTAs of a row striding over the box's cells).
+// The operator itself runs through hc_o4_batch_rhs on the same boxes.
+//
+// Every increment is rounded as the reference's BoxData::increment rounds
+// it, (scale * source) then the add, with explicit round-to-nearest
+// operations, so the results do not depend on multiply-add contraction.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <vector>
+
+#include "../../include/hc_abi.h"
+#include "hc_level.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// Kutta RK3 and classical RK4 tableaus (src/MHD_AMRRungeKutta.H:9-12).
+constexpr double kA3[4][4] = {{0, 0, 0, 0}, {0.5, 0, 0, 0}, {-1, 2, 0, 0}, {0, 0, 0, 0}};
+constexpr double kA4[4][4] = {{0, 0, 0, 0}, {0.5, 0, 0, 0}, {0, 0.5, 0, 0}, {0, 0, 1, 0}};
+constexpr double kB3[4] = {1.0 / 6, 2.0 / 3, 1.0 / 6, 0};
+constexpr double kB4[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+
+// Factors of one launch: stage state = state + sum_p f[p] rk[p] over the
+// used p (stage < order), or state += f[p] rk[p] for p < order (final).
+struct RkFactors {
+  double f[4];
+  int use[4];
+  int final;
+};
+
+__global__ void __launch_bounds__(kThreads) rkCombineKernel(const hc_rk_box* __restrict__ boxes, const RkFactors F) {
+  const hc_rk_box B = boxes[blockIdx.y];
+  const long long n = 8LL * B.ncells;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    double v = B.state[t];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+      if (F.use[p]) v = __dadd_rn(v, __dmul_rn(F.f[p], B.rk[p][t]));
+    if (F.final)
+      B.state[t] = v;
+    else
+      B.stage[t] = v;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) restrictKernel(const hc_restrict_box* __restrict__ items) {
+  const hc_restrict_box R = items[blockIdx.y];
+  const int n0 = R.hi[0] - R.lo[0] + 1, n1 = R.hi[1] - R.lo[1] + 1, n2 = R.hi[2] - R.lo[2] + 1;
+  const long long cells = (long long)n0 * n1 * n2;
+  const long long fineN = (long long)R.fine_n[0] * R.fine_n[1] * R.fine_n[2];
+  const long long coarseN = (long long)R.coarse_n[0] * R.coarse_n[1] * R.coarse_n[2];
+  const double w = 1.0 / (double)(R.ratio[0] * R.ratio[1] * R.ratio[2]);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 8 * cells;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / cells);
+    const long long r = t - (long long)c * cells;
+    const int I = R.lo[0] + (int)(r % n0);
+    const int J = R.lo[1] + (int)((r / n0) % n1);
+    const int K = R.lo[2] + (int)(r / ((long long)n0 * n1));
+    const double* src = R.fine + (long long)c * fineN;
+    double sum = 0.0;
+    for (int kk = 0; kk < R.ratio[2]; ++kk)
+      for (int jj = 0; jj < R.ratio[1]; ++jj)
+        for (int ii = 0; ii < R.ratio[0]; ++ii) {
+          const int fi = I * R.ratio[0] + ii - R.fine_lo[0];
+          const int fj = J * R.ratio[1] + jj - R.fine_lo[1];
+          const int fk = K * R.ratio[2] + kk - R.fine_lo[2];
+          sum = __dadd_rn(sum, __dmul_rn(w, src[fi + (long long)R.fine_n[0] * (fj + (long long)R.fine_n[1] * fk)]));
+        }
+    const long long co = (long long)(I - R.coarse_lo[0]) +
+                         (long long)R.coarse_n[0] * ((J - R.coarse_lo[1]) + (long long)R.coarse_n[1] * (K - R.coarse_lo[2]));
+    R.coarse[(long long)c * coarseN + co] = sum;
+  }
+}
+
+int cudaFailed(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return HC_OK;
+  char msg[256];
+  std::snprintf(msg, sizeof msg, "%s: %s", what, cudaGetErrorString(e));
+  return hc::setLastError(HC_ERR_CUDA, msg);
+}
+
+dim3 gridFor(long long maxElems, int nitems) {
+  long long g = (maxElems + kThreads - 1) / kThreads;
+  const long long cap = 148LL * 8;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return dim3((unsigned)g, (unsigned)nitems);
+}
+
+int argFail(const char* msg) { return hc::setLastError(HC_ERR_ARG, msg); }
+
+}  // namespace
+
+struct hc_amr_plan {
+  hc_rk_box* boxes = nullptr;           // device copy
+  hc_restrict_box* restricts = nullptr; // device copy
+  int nbox = 0, nrestrict = 0;
+  long long maxBoxCells = 0;
+  std::vector<long long> restrictCells;  // coarse cells written by each item
+};
+
+extern "C" int hc_amr_plan_create(hc_ctx* ctx, const hc_rk_box* boxes, int nbox, const hc_restrict_box* restricts,
+                                  int nrestrict, hc_amr_plan** out) {
+  if (!ctx || !out || (nbox && !boxes) || (nrestrict && !restricts)) return argFail("hc_amr_plan_create: null argument");
+  if (nbox < 0 || nrestrict < 0) return argFail("hc_amr_plan_create: negative count");
+  *out = nullptr;
+  hc_amr_plan* P = new hc_amr_plan;
+  P->nbox = nbox;
+  P->nrestrict = nrestrict;
+  for (int b = 0; b < nbox; ++b) {
+    const hc_rk_box& B = boxes[b];
+    if (B.ncells < 0 || (B.ncells > 0 && (!B.state || !B.stage))) {
+      delete P;
+      return argFail("hc_amr_plan_create: a box needs ncells >= 0, state and stage");
+    }
+    for (int q = 0; q < 4; ++q)
+      if (B.ncells > 0 && !B.rk[q]) {
+        delete P;
+        return argFail("hc_amr_plan_create: a box needs its four stage right-hand sides");
+      }
+    P->maxBoxCells = B.ncells > P->maxBoxCells ? B.ncells : P->maxBoxCells;
+  }
+  for (int r = 0; r < nrestrict; ++r) {
+    const hc_restrict_box& R = restricts[r];
+    bool ok = R.fine && R.coarse;
+    for (int d = 0; d < 3 && ok; ++d) {
+      ok = R.ratio[d] >= 1 && R.ratio[d] <= 16 && R.lo[d] <= R.hi[d] && R.fine_n[d] >= 1 && R.coarse_n[d] >= 1 &&
+           R.lo[d] >= R.coarse_lo[d] && R.hi[d] < R.coarse_lo[d] + R.coarse_n[d] &&
+           (long long)R.lo[d] * R.ratio[d] >= R.fine_lo[d] &&
+           ((long long)R.hi[d] + 1) * R.ratio[d] <= (long long)R.fine_lo[d] + R.fine_n[d];
+    }
+    if (!ok) {
+      delete P;
+      return argFail("hc_amr_plan_create: a restriction's coarse cells must lie in its coarse box and cover fine "
+                     "cells inside its fine box (ratio 1..16)");
+    }
+    P->restrictCells.push_back((long long)(R.hi[0] - R.lo[0] + 1) * (R.hi[1] - R.lo[1] + 1) * (R.hi[2] - R.lo[2] + 1));
+  }
+  cudaError_t e = cudaSuccess;
+  if (nbox) {
+    e = cudaMalloc(&P->boxes, sizeof(hc_rk_box) * nbox);
+    if (e == cudaSuccess) e = cudaMemcpy(P->boxes, boxes, sizeof(hc_rk_box) * nbox, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && nrestrict) {
+    e = cudaMalloc(&P->restricts, sizeof(hc_restrict_box) * nrestrict);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(P->restricts, restricts, sizeof(hc_restrict_box) * nrestrict, cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(P->boxes);
+    cudaFree(P->restricts);
+    delete P;
+    return cudaFailed(e, "hc_amr_plan_create");
+  }
+  *out = P;
+  return HC_OK;
+}
+
+extern "C" int hc_amr_plan_destroy(hc_amr_plan* P) {
+  if (!P) return HC_OK;
+  cudaFree(P->boxes);
+  cudaFree(P->restricts);
+  delete P;
+  return HC_OK;
+}
+
+extern "C" int hc_amr_rk_stage(hc_ctx* ctx, const hc_amr_plan* P, int order, int stage, double dt, void* stream) {
+  if (!ctx || !P) return argFail("hc_amr_rk_stage: null argument");
+  if (order != 3 && order != 4) return argFail("hc_amr_rk_stage: order must be 3 or 4");
+  if (stage < 0 || stage > order) return argFail("hc_amr_rk_stage: stage must be 0..order");
+  if (P->nbox > 65535) return argFail("hc_amr_rk_stage: at most 65535 boxes per plan");
+  if (P->nbox == 0 || P->maxBoxCells == 0) return HC_OK;
+  const auto& a = order == 3 ? kA3 : kA4;
+  const auto& b = order == 3 ? kB3 : kB4;
+  RkFactors F{};
+  F.final = stage == order ? 1 : 0;
+  for (int p = 0; p < 4; ++p) {
+    if (F.final) {
+      F.use[p] = p < order;
+      F.f[p] = dt * b[p];
+    } else {
+      F.use[p] = p < stage && a[stage][p] != 0.0;
+      F.f[p] = dt * a[stage][p];
+    }
+  }
+  rkCombineKernel<<<gridFor(8 * P->maxBoxCells, P->nbox), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->boxes,
+                                                                                                               F);
+  return cudaFailed(cudaGetLastError(), "hc_amr_rk_stage");
+}
+
+extern "C" int hc_amr_restrict(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, void* stream) {
+  if (!ctx || !P) return argFail("hc_amr_restrict: null argument");
+  if (first < 0 || count < 0 || first + count > P->nrestrict) return argFail("hc_amr_restrict: range outside the plan");
+  if (count > 65535) return argFail("hc_amr_restrict: at most 65535 restrictions per launch");
+  if (count == 0) return HC_OK;
+  long long maxCells = 0;
+  for (int r = first; r < first + count; ++r) maxCells = P->restrictCells[r] > maxCells ? P->restrictCells[r] : maxCells;
+  restrictKernel<<<gridFor(8 * maxCells, count), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->restricts +
+                                                                                                      first);
+  return cudaFailed(cudaGetLastError(), "hc_amr_restrict");
+}

@@ -493,3 +493,51 @@ class O4Batch:
             self.close()
         except Exception:
             pass
+
+
+class AmrPlan:
+    """The AMR Runge-Kutta stage logic of a set of boxes (any levels, any
+    sizes): hc_amr_plan_create / hc_amr_rk_stage / hc_amr_restrict.
+
+    boxes: (state, stage, [rk0, rk1, rk2, rk3]) device tensors of 8 x
+    ncells doubles each.  restricts: dicts with fine, coarse (device
+    tensors), fine_lo, fine_n, coarse_lo, coarse_n, lo, hi, ratio (3 ints
+    each).  The tensors must outlive the plan."""
+
+    def __init__(self, shell: "Shell", boxes, restricts=()):
+        self._shell = shell
+        self._lib = shell._lib
+        nb, nr = len(boxes), len(restricts)
+        bx = (N.HcRkBox * max(nb, 1))()
+        for b, (state, stage, rk) in enumerate(boxes):
+            bx[b].ncells = state.numel() // 8
+            bx[b].state = state.data_ptr()
+            bx[b].stage = stage.data_ptr()
+            for q in range(4):
+                bx[b].rk[q] = rk[q].data_ptr()
+        rx = (N.HcRestrictBox * max(nr, 1))()
+        for r, d in enumerate(restricts):
+            rx[r].fine = d["fine"].data_ptr()
+            rx[r].coarse = d["coarse"].data_ptr()
+            for k in ("fine_lo", "fine_n", "coarse_lo", "coarse_n", "lo", "hi", "ratio"):
+                getattr(rx[r], k)[:] = list(d[k])
+        self._h = C.c_void_p()
+        N.check(self._lib.hc_amr_plan_create(shell._ctx, bx, nb, rx, nr, C.byref(self._h)), "hc_amr_plan_create")
+
+    def rk_stage(self, order: int, stage: int, dt: float) -> None:
+        N.check(self._lib.hc_amr_rk_stage(self._shell._ctx, self._h, order, stage, dt, _stream()), "hc_amr_rk_stage")
+
+    def restrict(self, first: int, count: int) -> None:
+        N.check(self._lib.hc_amr_restrict(self._shell._ctx, self._h, first, count, _stream()), "hc_amr_restrict")
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.hc_amr_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

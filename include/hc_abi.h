@@ -239,6 +239,58 @@ int hc_level_dt_cfl(hc_ctx* ctx, const double* ju, double* inv_dt_max,
 int hc_level_valid(hc_ctx* ctx, const double* ju, int* ok, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * AMR Runge-Kutta stage logic on uneven boxes (advanceRungeKuttaSynchronous,
+ * src/MHD_AMRRungeKutta.H:5-41, and restrictTo, src/MHD_AMR.H:597-609).
+ * The hierarchy itself (layouts, regrid, coarse-fine ghosts, flux
+ * registers) stays with the caller; these entries do the per-box arithmetic
+ * of every box of every level in one launch each.
+ * ------------------------------------------------------------------------- */
+
+/* One box: its valid cells (arrays of 8 x ncells doubles, component-major,
+ * the caller's cell order), the state U^n, the stage state and the four
+ * stage right-hand sides (device pointers). */
+typedef struct hc_rk_box {
+  long long ncells;
+  double* state;
+  double* stage;
+  double* rk[4];
+} hc_rk_box;
+
+/* One restriction: the coarse cells lo..hi (inclusive, coarse index space)
+ * of `coarse` (stored over coarse_lo + [0, coarse_n)) become the mean of
+ * the ratio[0] x ratio[1] x ratio[2] cells of `fine` (stored over fine_lo +
+ * [0, fine_n), fine index space) they cover: Stencil::AvgDown(ratio). */
+typedef struct hc_restrict_box {
+  const double* fine;
+  double* coarse;
+  int fine_lo[3], fine_n[3];
+  int coarse_lo[3], coarse_n[3];
+  int lo[3], hi[3];
+  int ratio[3];
+  int reserved;
+} hc_restrict_box;
+
+typedef struct hc_amr_plan hc_amr_plan;
+
+/* Validate the boxes and restrictions (host arrays; every restriction must
+ * read and write inside its boxes) and keep a device copy of each list. */
+int hc_amr_plan_create(hc_ctx* ctx, const hc_rk_box* boxes, int nbox, const hc_restrict_box* restricts,
+                       int nrestrict, hc_amr_plan** out);
+int hc_amr_plan_destroy(hc_amr_plan* plan);
+
+/* The tableau (order 3: Kutta RK3, 4: classical RK4, src/MHD_AMRRungeKutta.H:
+ * 9-12) on every box of the plan.  stage s < order: stage = state, then
+ * stage += (dt a[s][p]) rk[p] for each p < s with a[s][p] != 0 (amrCopyValid
+ * + increment, :22-27); stage = order: state += (dt b[p]) rk[p] for p < order
+ * in order (:37).  Each increment rounds the product, then the sum. */
+int hc_amr_rk_stage(hc_ctx* ctx, const hc_amr_plan* plan, int order, int stage, double dt, void* stream);
+
+/* Restrictions first .. first+count-1 of the plan in one launch.  The
+ * reference restricts the finest level first (:26); give each level's
+ * restrictions their own call, finest first, when levels chain. */
+int hc_amr_restrict(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Autotuner (no reference counterpart: the reference runs its face loops on
  * the host).  Order 2: the stage kernel runs one CTA per cell tile; the
  * tiles differ in shape and in the register cap (resident CTAs per SM), and

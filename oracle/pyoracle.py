@@ -326,3 +326,48 @@ def ref_cone_cell(spec: HcConeSpec, inner_radius: float, time: float, pos, ambie
     rc = R.ref_cone_cell(dptr(vec), inner_radius / 6.96e10, time, dptr(pos), dptr(amb), gamma, dptr(delta))
     assert rc >= 0
     return bool(rc), delta
+
+
+# ---------------------------------------------------------------------------
+# AMR Runge-Kutta stage logic (numpy; every increment rounds the product,
+# then the sum, as BoxData::increment does).
+# advanceRungeKuttaSynchronous: src/MHD_AMRRungeKutta.H:5-41 (tableaus :9-12).
+# restrictTo / Stencil::AvgDown: src/MHD_AMR.H:597-609.
+# ---------------------------------------------------------------------------
+RK_A = {3: ((0, 0, 0, 0), (0.5, 0, 0, 0), (-1, 2, 0, 0), (0, 0, 0, 0)),
+        4: ((0, 0, 0, 0), (0.5, 0, 0, 0), (0, 0.5, 0, 0), (0, 0, 1, 0))}
+RK_B = {3: (1.0 / 6, 2.0 / 3, 1.0 / 6, 0), 4: (1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6)}
+
+
+def amr_rk_stage(state: np.ndarray, stage: np.ndarray, rk: list, order: int, s: int, dt: float) -> None:
+    """One box: s < order writes the stage state (amrCopyValid + increments,
+    :22-27); s == order updates the state in place (:37)."""
+    if s < order:
+        v = state.copy()
+        for p in range(s):
+            if RK_A[order][s][p] != 0:
+                v = v + (dt * RK_A[order][s][p]) * rk[p]
+        stage[...] = v
+    else:
+        for p in range(order):
+            state[...] = state + (dt * RK_B[order][p]) * rk[p]
+
+
+def amr_restrict(fine: np.ndarray, fine_lo, coarse: np.ndarray, coarse_lo, lo, hi, ratio) -> None:
+    """Coarse cells lo..hi of coarse [8][n2][n1][n0] (low corner coarse_lo)
+    = mean of the fine cells of fine [8][m2][m1][m0] (low corner fine_lo)
+    they cover, summed radial-fastest as (1/prod ratio) * value terms."""
+    w = 1.0 / float(ratio[0] * ratio[1] * ratio[2])
+    I = np.arange(lo[0], hi[0] + 1)
+    J = np.arange(lo[1], hi[1] + 1)
+    K = np.arange(lo[2], hi[2] + 1)
+    total = np.zeros((8, K.size, J.size, I.size))
+    for kk in range(ratio[2]):
+        for jj in range(ratio[1]):
+            for ii in range(ratio[0]):
+                fi = I * ratio[0] + ii - fine_lo[0]
+                fj = J * ratio[1] + jj - fine_lo[1]
+                fk = K * ratio[2] + kk - fine_lo[2]
+                total = total + w * fine[:, fk[:, None, None], fj[None, :, None], fi[None, None, :]]
+    coarse[:, K[0] - coarse_lo[2]:K[-1] - coarse_lo[2] + 1, J[0] - coarse_lo[1]:J[-1] - coarse_lo[1] + 1,
+           I[0] - coarse_lo[0]:I[-1] - coarse_lo[0] + 1] = total

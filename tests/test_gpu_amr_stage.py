@@ -1,0 +1,86 @@
+"""AMR Runge-Kutta stage logic on the GPU (hc_amr_plan_create,
+hc_amr_rk_stage, hc_amr_restrict) against the numpy restatement in the
+oracle: uneven boxes in one launch, both tableaus, every stage, and
+restrictions with isotropic and radial-only ratios.  Tolerance: exact (the
+device rounds every product and sum as written)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+
+pytestmark = pytest.mark.gpu
+
+if gpu_available():
+    import torch
+
+    import heliocubed_b200 as hc
+    from heliocubed_b200.level import AmrPlan
+
+
+def _need_gpu():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+
+
+SIZES = [(8, 8, 8), (12, 8, 16), (16, 16, 16), (1, 1, 1), (32, 8, 8)]
+
+
+@pytest.mark.parametrize("order", [3, 4])
+def test_rk_stages_match_oracle(oracle_lib, order):
+    _need_gpu()
+    po = oracle_lib
+    rng = np.random.default_rng(order)
+    sh = hc.Shell(hc.Params(nr=8, na=8))
+    host = []
+    dev = []
+    for n in SIZES:
+        cells = n[0] * n[1] * n[2]
+        state = rng.normal(size=8 * cells) * 10.0 ** rng.integers(-20, 20, size=8 * cells)
+        host.append({"state": state, "stage": np.zeros_like(state), "rk": [np.zeros_like(state) for _ in range(4)]})
+        dev.append((torch.from_numpy(state.copy()).cuda(), torch.zeros(8 * cells, dtype=torch.float64, device="cuda"),
+                    [torch.zeros(8 * cells, dtype=torch.float64, device="cuda") for _ in range(4)]))
+    plan = AmrPlan(sh, dev)
+    dt = 0.37
+    for s in range(order):
+        plan.rk_stage(order, s, dt)
+        for h, d in zip(host, dev):
+            po.amr_rk_stage(h["state"], h["stage"], h["rk"], order, s, dt)
+            assert np.array_equal(d[1].cpu().numpy(), h["stage"])
+            k = rng.normal(size=h["state"].size) * np.abs(h["state"]).max()
+            h["rk"][s][...] = k
+            d[2][s].copy_(torch.from_numpy(k))
+    plan.rk_stage(order, order, dt)
+    for h, d in zip(host, dev):
+        po.amr_rk_stage(h["state"], h["stage"], h["rk"], order, order, dt)
+        assert np.array_equal(d[0].cpu().numpy(), h["state"])
+    plan.close()
+
+
+def test_restrictions_match_oracle(oracle_lib):
+    _need_gpu()
+    po = oracle_lib
+    rng = np.random.default_rng(9)
+    sh = hc.Shell(hc.Params(nr=8, na=8))
+    cases = [dict(fine_lo=(2, 4, 6), fine_n=(8, 6, 4), coarse_lo=(0, 1, 2), coarse_n=(5, 5, 5), lo=(1, 2, 3),
+                  hi=(4, 4, 4), ratio=(2, 2, 2)),
+             dict(fine_lo=(0, 0, 0), fine_n=(16, 4, 4), coarse_lo=(0, 0, 0), coarse_n=(8, 4, 4), lo=(0, 0, 0),
+                  hi=(7, 3, 3), ratio=(2, 1, 1)),
+             dict(fine_lo=(10, 0, 2), fine_n=(4, 8, 8), coarse_lo=(4, 0, 0), coarse_n=(4, 6, 6), lo=(5, 0, 1),
+                  hi=(6, 3, 4), ratio=(2, 2, 2))]
+    items, ref = [], []
+    for c in cases:
+        fine = rng.normal(size=(8, c["fine_n"][2], c["fine_n"][1], c["fine_n"][0]))
+        coarse = rng.normal(size=(8, c["coarse_n"][2], c["coarse_n"][1], c["coarse_n"][0]))
+        expect = coarse.copy()
+        po.amr_restrict(fine, c["fine_lo"], expect, c["coarse_lo"], c["lo"], c["hi"], c["ratio"])
+        d = dict(c, fine=torch.from_numpy(fine.reshape(-1).copy()).cuda(),
+                 coarse=torch.from_numpy(coarse.reshape(-1).copy()).cuda())
+        items.append(d)
+        ref.append(expect)
+    plan = AmrPlan(sh, [], items)
+    plan.restrict(0, len(items))
+    for d, expect in zip(items, ref):
+        assert np.array_equal(d["coarse"].cpu().numpy(), expect.reshape(-1))
+    plan.close()

@@ -576,11 +576,37 @@ def run_amr(args, world, rank, local):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps
 
+    # the RK4 stage logic of the same boxes (all levels, one plan): each box's
+    # valid state, stage state and four stage right-hand sides (the operator
+    # output of stage s is rk[s]); one combine launch per stage
+    from heliocubed_b200.level import AmrPlan
+    rk_boxes = []
+    for _, sh, works, _, _ in levels:
+        for w in works:
+            nv = w[2].numel()
+            rk_boxes.append((torch.zeros(nv, dtype=torch.float64, device=sh._dev),
+                             torch.zeros(nv, dtype=torch.float64, device=sh._dev),
+                             [w[2]] + [torch.zeros(nv, dtype=torch.float64, device=sh._dev) for _ in range(3)]))
+    plan = AmrPlan(levels[0][1], rk_boxes)
+
+    def stage_logic():
+        for s in range(5):
+            plan.rk_stage(4, s, 1.0e-3)
+
+    def batched_step():
+        for s in range(4):
+            batched()
+            plan.rk_stage(4, s, 1.0e-3)
+        plan.rk_stage(4, 4, 1.0e-3)
+
     sampler = ClockSampler(local)
     sampler.start()
     ms_b = timed(batched, args.amr_reps)
     ms_p = timed(plain, max(1, args.amr_reps // 4))
+    ms_rk = timed(stage_logic, args.amr_reps)
+    ms_step = timed(batched_step, max(1, args.amr_reps // 4))
     clocks = sampler.stop()
+    plan.close()
     # identical results
     for _, _, works, _, _ in levels:
         for w in works:
@@ -604,7 +630,14 @@ def run_amr(args, world, rank, local):
                "batched": {"ms_per_evaluation": ms_b, "launches": 3 * 36},
                "plain": {"ms_per_evaluation": ms_p, "cell_stage_per_s": cells / (ms_p * 1e-3),
                          "launches": 36 * nboxes},
-               "batched_over_plain": ms_p / ms_b, "identical_results": same, "clocks": clocks}
+               "batched_over_plain": ms_p / ms_b, "identical_results": same,
+               "rk4_stage_logic": {"ms_per_step": ms_rk, "launches": 5,
+                                   "what": "tableau combine of every box of every level, 4 stages + final"},
+               "rk4_step_without_ghost_fill": {"ms": ms_step, "cell_updates_per_s": cells / (ms_step * 1e-3),
+                                               "what": "4 x (batched operator of each level + stage combine) + "
+                                                       "final combine; coarse-fine ghost fill and registers are "
+                                                       "the caller's"},
+               "clocks": clocks}
         print(json.dumps(out), flush=True)
     for _, sh, _, batch, singles in levels:
         batch.close()

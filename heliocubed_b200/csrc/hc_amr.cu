@@ -1,8 +1,9 @@
 // AMR Runge-Kutta stage logic on uneven boxes: the tableau combination of
 // advanceRungeKuttaSynchronous (src/MHD_AMRRungeKutta.H:5-41) and the
 // fine-to-coarse restriction restrictTo / Stencil::AvgDown
-// (src/MHD_AMR.H:597-609), each one launch over a device work list of boxes
-// (one CTA row per box, the CTAs of a row striding over the box's cells).
+// (src/MHD_AMR.H:597-609), each one launch over a device work list: fixed
+// chunks of 16384 elements of the boxes (or restrictions), one CTA each, so
+// uneven boxes load the GPU evenly.
 // The operator itself runs through hc_o4_batch_rhs on the same boxes.
 //
 // Every increment is rounded as the reference's BoxData::increment rounds
@@ -34,10 +35,19 @@ struct RkFactors {
   int final;
 };
 
-__global__ void __launch_bounds__(kThreads) rkCombineKernel(const hc_rk_box* __restrict__ boxes, const RkFactors F) {
-  const hc_rk_box B = boxes[blockIdx.y];
-  const long long n = 8LL * B.ncells;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+// One work-list entry: elements [begin, end) of item `item` (a box's 8 x
+// ncells doubles, or a restriction's 8 x coarse cells).
+struct Chunk {
+  int item, pad;
+  long long begin, end;
+};
+constexpr long long kChunk = 16384;  // elements per CTA: 64 per thread
+
+__global__ void __launch_bounds__(kThreads) rkCombineKernel(const hc_rk_box* __restrict__ boxes,
+                                                            const Chunk* __restrict__ chunks, const RkFactors F) {
+  const Chunk ch = chunks[blockIdx.x];
+  const hc_rk_box B = boxes[ch.item];
+  for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
     double v = B.state[t];
 #pragma unroll
     for (int p = 0; p < 4; ++p)
@@ -49,15 +59,16 @@ __global__ void __launch_bounds__(kThreads) rkCombineKernel(const hc_rk_box* __r
   }
 }
 
-__global__ void __launch_bounds__(kThreads) restrictKernel(const hc_restrict_box* __restrict__ items) {
-  const hc_restrict_box R = items[blockIdx.y];
+__global__ void __launch_bounds__(kThreads) restrictKernel(const hc_restrict_box* __restrict__ items,
+                                                            const Chunk* __restrict__ chunks) {
+  const Chunk ch = chunks[blockIdx.x];
+  const hc_restrict_box R = items[ch.item];
   const int n0 = R.hi[0] - R.lo[0] + 1, n1 = R.hi[1] - R.lo[1] + 1, n2 = R.hi[2] - R.lo[2] + 1;
   const long long cells = (long long)n0 * n1 * n2;
   const long long fineN = (long long)R.fine_n[0] * R.fine_n[1] * R.fine_n[2];
   const long long coarseN = (long long)R.coarse_n[0] * R.coarse_n[1] * R.coarse_n[2];
   const double w = 1.0 / (double)(R.ratio[0] * R.ratio[1] * R.ratio[2]);
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 8 * cells;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
     const int c = (int)(t / cells);
     const long long r = t - (long long)c * cells;
     const int I = R.lo[0] + (int)(r % n0);
@@ -86,12 +97,8 @@ int cudaFailed(cudaError_t e, const char* what) {
   return hc::setLastError(HC_ERR_CUDA, msg);
 }
 
-dim3 gridFor(long long maxElems, int nitems) {
-  long long g = (maxElems + kThreads - 1) / kThreads;
-  const long long cap = 148LL * 8;
-  if (g > cap) g = cap;
-  if (g < 1) g = 1;
-  return dim3((unsigned)g, (unsigned)nitems);
+void addChunks(std::vector<Chunk>& out, int item, long long elems) {
+  for (long long b = 0; b < elems; b += kChunk) out.push_back(Chunk{item, 0, b, b + kChunk < elems ? b + kChunk : elems});
 }
 
 int argFail(const char* msg) { return hc::setLastError(HC_ERR_ARG, msg); }
@@ -101,9 +108,10 @@ int argFail(const char* msg) { return hc::setLastError(HC_ERR_ARG, msg); }
 struct hc_amr_plan {
   hc_rk_box* boxes = nullptr;           // device copy
   hc_restrict_box* restricts = nullptr; // device copy
-  int nbox = 0, nrestrict = 0;
-  long long maxBoxCells = 0;
-  std::vector<long long> restrictCells;  // coarse cells written by each item
+  Chunk* boxChunks = nullptr;           // work list of the combine (device)
+  Chunk* restrictChunks = nullptr;      // work list of the restrictions (device), by item
+  int nbox = 0, nrestrict = 0, nBoxChunks = 0;
+  std::vector<int> restrictChunkStart;  // first chunk of each restriction (+ total at the end)
 };
 
 extern "C" int hc_amr_plan_create(hc_ctx* ctx, const hc_rk_box* boxes, int nbox, const hc_restrict_box* restricts,
@@ -125,7 +133,6 @@ extern "C" int hc_amr_plan_create(hc_ctx* ctx, const hc_rk_box* boxes, int nbox,
         delete P;
         return argFail("hc_amr_plan_create: a box needs its four stage right-hand sides");
       }
-    P->maxBoxCells = B.ncells > P->maxBoxCells ? B.ncells : P->maxBoxCells;
   }
   for (int r = 0; r < nrestrict; ++r) {
     const hc_restrict_box& R = restricts[r];
@@ -141,10 +148,27 @@ extern "C" int hc_amr_plan_create(hc_ctx* ctx, const hc_rk_box* boxes, int nbox,
       return argFail("hc_amr_plan_create: a restriction's coarse cells must lie in its coarse box and cover fine "
                      "cells inside its fine box (ratio 1..16)");
     }
-    P->restrictCells.push_back((long long)(R.hi[0] - R.lo[0] + 1) * (R.hi[1] - R.lo[1] + 1) * (R.hi[2] - R.lo[2] + 1));
   }
+  std::vector<Chunk> bc, rc;
+  for (int b = 0; b < nbox; ++b) addChunks(bc, b, 8 * boxes[b].ncells);
+  for (int r = 0; r < nrestrict; ++r) {
+    const hc_restrict_box& R = restricts[r];
+    P->restrictChunkStart.push_back((int)rc.size());
+    addChunks(rc, r, 8LL * (R.hi[0] - R.lo[0] + 1) * (R.hi[1] - R.lo[1] + 1) * (R.hi[2] - R.lo[2] + 1));
+  }
+  P->restrictChunkStart.push_back((int)rc.size());
+  P->nBoxChunks = (int)bc.size();
   cudaError_t e = cudaSuccess;
-  if (nbox) {
+  if (!bc.empty()) {
+    e = cudaMalloc(&P->boxChunks, sizeof(Chunk) * bc.size());
+    if (e == cudaSuccess) e = cudaMemcpy(P->boxChunks, bc.data(), sizeof(Chunk) * bc.size(), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && !rc.empty()) {
+    e = cudaMalloc(&P->restrictChunks, sizeof(Chunk) * rc.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpy(P->restrictChunks, rc.data(), sizeof(Chunk) * rc.size(), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && nbox) {
     e = cudaMalloc(&P->boxes, sizeof(hc_rk_box) * nbox);
     if (e == cudaSuccess) e = cudaMemcpy(P->boxes, boxes, sizeof(hc_rk_box) * nbox, cudaMemcpyHostToDevice);
   }
@@ -156,6 +180,8 @@ extern "C" int hc_amr_plan_create(hc_ctx* ctx, const hc_rk_box* boxes, int nbox,
   if (e != cudaSuccess) {
     cudaFree(P->boxes);
     cudaFree(P->restricts);
+    cudaFree(P->boxChunks);
+    cudaFree(P->restrictChunks);
     delete P;
     return cudaFailed(e, "hc_amr_plan_create");
   }
@@ -167,6 +193,8 @@ extern "C" int hc_amr_plan_destroy(hc_amr_plan* P) {
   if (!P) return HC_OK;
   cudaFree(P->boxes);
   cudaFree(P->restricts);
+  cudaFree(P->boxChunks);
+  cudaFree(P->restrictChunks);
   delete P;
   return HC_OK;
 }
@@ -175,8 +203,7 @@ extern "C" int hc_amr_rk_stage(hc_ctx* ctx, const hc_amr_plan* P, int order, int
   if (!ctx || !P) return argFail("hc_amr_rk_stage: null argument");
   if (order != 3 && order != 4) return argFail("hc_amr_rk_stage: order must be 3 or 4");
   if (stage < 0 || stage > order) return argFail("hc_amr_rk_stage: stage must be 0..order");
-  if (P->nbox > 65535) return argFail("hc_amr_rk_stage: at most 65535 boxes per plan");
-  if (P->nbox == 0 || P->maxBoxCells == 0) return HC_OK;
+  if (P->nBoxChunks == 0) return HC_OK;
   const auto& a = order == 3 ? kA3 : kA4;
   const auto& b = order == 3 ? kB3 : kB4;
   RkFactors F{};
@@ -190,19 +217,15 @@ extern "C" int hc_amr_rk_stage(hc_ctx* ctx, const hc_amr_plan* P, int order, int
       F.f[p] = dt * a[stage][p];
     }
   }
-  rkCombineKernel<<<gridFor(8 * P->maxBoxCells, P->nbox), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->boxes,
-                                                                                                               F);
+  rkCombineKernel<<<P->nBoxChunks, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->boxes, P->boxChunks, F);
   return cudaFailed(cudaGetLastError(), "hc_amr_rk_stage");
 }
 
 extern "C" int hc_amr_restrict(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, void* stream) {
   if (!ctx || !P) return argFail("hc_amr_restrict: null argument");
   if (first < 0 || count < 0 || first + count > P->nrestrict) return argFail("hc_amr_restrict: range outside the plan");
-  if (count > 65535) return argFail("hc_amr_restrict: at most 65535 restrictions per launch");
-  if (count == 0) return HC_OK;
-  long long maxCells = 0;
-  for (int r = first; r < first + count; ++r) maxCells = P->restrictCells[r] > maxCells ? P->restrictCells[r] : maxCells;
-  restrictKernel<<<gridFor(8 * maxCells, count), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->restricts +
-                                                                                                      first);
+  const int c0 = P->restrictChunkStart[first], c1 = P->restrictChunkStart[first + count];
+  if (c1 == c0) return HC_OK;
+  restrictKernel<<<c1 - c0, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->restricts, P->restrictChunks + c0);
   return cudaFailed(cudaGetLastError(), "hc_amr_restrict");
 }

@@ -54,6 +54,40 @@ struct Ctx {
   Reg gr, fr, v1r, v2r, vr;
 };
 
+// Regions the operator's kernels loop over (host and device agree through
+// this one table): the work lists of a batch are built from it.
+enum RegionId { RG_G = 0, RG_GR, RG_F, RG_PB, RG_F1, RG_V0, RG_V, RG_PF, RG_PP, RG_V1, RG_V2, RG_COUNT };
+__host__ __device__ inline Box3 regionOf(const Ctx& c, int id) {
+  switch (id) {
+    case RG_G: return c.G;
+    case RG_GR: return c.GR;
+    case RG_F: return c.F;
+    case RG_PB: return c.V0.growTrans(c.d, 1);
+    case RG_F1: return c.F1;
+    case RG_V0: return c.V0;
+    case RG_V: return c.V;
+    case RG_PF: return c.V1.extrude(c.d).growTrans(c.d, 1);
+    case RG_PP: return c.V1.extrude(c.d);
+    case RG_V1: return c.V1;
+    default: return c.V2;
+  }
+}
+
+// One CTA's work: flat points begin, begin + stride, ... below end (each
+// thread adds its index) of one region of box `box`.
+struct WorkChunk {
+  int box, stride;
+  long begin, end;
+};
+// Points per CTA (128 threads) of a work list: its total points over about
+// 148 x 32 CTAs, rounded up to whole passes of the CTA and held within
+// [128, 1024], so one launch has as many CTAs whatever the box sizes.
+inline long chunkPoints(long total) {
+  const long target = (total + 148L * 32 - 1) / (148L * 32);
+  const long c = ((target + 127) / 128) * 128;
+  return c < 128 ? 128 : c > 1024 ? 1024 : c;
+}
+
 Ctx makeCtx(const O4Args& a, int d) {
   Ctx c;
   c.a = a;
@@ -365,14 +399,13 @@ __device__ __forceinline__ double faceProd(double f4, double g4, double df0, dou
 }
 
 
-// Thread -> (i, j, k) over region b of this CTA row's box (blockIdx.y
-// selects the box; every pointer in its Ctx is that box's, so the body sees
-// box index 0).
+// Thread -> (i, j, k) over the chunk's points of region b (flat index,
+// radial fastest) of the chunk's box; the end is clamped to the region.
 template <class F>
-__device__ __forceinline__ void forRegion(const Box3& b, int nbox, F f) {
-  (void)nbox;
+__device__ __forceinline__ void forRegion(const Box3& b, const WorkChunk& w, F f) {
   const long n = b.size();
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+  const long end = w.end < n ? w.end : n;
+  for (long t = w.begin + threadIdx.x; t < end; t += w.stride) {
     const int i = b.lo[0] + (int)(t % b.n(0));
     const int j = b.lo[1] + (int)((t / b.n(0)) % b.n(1));
     const int k = b.lo[2] + (int)(t / ((long)b.n(0) * b.n(1)));
@@ -382,10 +415,11 @@ __device__ __forceinline__ void forRegion(const Box3& b, int nbox, F f) {
 
 // ---- kernels ------------------------------------------------------------------
 // 1. detector primitives of the averages, V(<U>) (:1776).
-__global__ void o4PrimAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + 0];
+__global__ void o4PrimAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + 0];
   const O4Args& a = c.a;
-  forRegion(c.G, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.G, wc, [&](int b, int i, int j, int k) {
     double u[8], w[8];
     const double* U = a.U + b * a.uStride + roff(a.ur, i, j, k);
 #pragma unroll
@@ -412,10 +446,11 @@ __device__ __forceinline__ double eta1(double qm, double q0, double qp) {
 }
 
 // 2. raw Jameson flag on G.grow(-1) (:347-402).
-__global__ void o4ThetaRawKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + 0];
+__global__ void o4ThetaRawKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + 0];
   const O4Args& a = c.a;
-  forRegion(c.GR, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.GR, wc, [&](int b, int i, int j, int k) {
     const double* W = a.WA + (long)b * 8 * c.gr.N;
     const long N = c.gr.N, o = roff(c.gr, i, j, k);
     double et[3];
@@ -436,10 +471,11 @@ __global__ void o4ThetaRawKernel(const Ctx* __restrict__ tab, const RegArgs rg) 
 
 // 3. dilated theta (0 outside G.grow(-2)), theta-aware average-to-point and
 // point primitives on G (:404-507, 696-741, 212-275).
-__global__ void o4PointKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + 0];
+__global__ void o4PointKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + 0];
   const O4Args& a = c.a;
-  forRegion(c.G, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.G, wc, [&](int b, int i, int j, int k) {
     const long N = c.gr.N, o = roff(c.gr, i, j, k);
     const double* R = a.thr + (long)b * N;
     double t = 0.0;
@@ -480,12 +516,13 @@ __device__ __forceinline__ const double* faceBasis(const Ctx& c, int b, int j, i
 // 4. reconstruction (WENOZ / WENO3 / PLM with clamps), Roe repair, energies,
 // point flux sum, total-pressure sum, centred normal B, Rusanov jump (F).
 template <int D, int MB>
-__global__ void __launch_bounds__(128, MB) o4FaceReconKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + D];
+__global__ void __launch_bounds__(128, MB) o4FaceReconKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const double dx2 = a.G.dx[d] * a.G.dx[d];
-  forRegion(c.F, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.F, wc, [&](int b, int i, int j, int k) {
     const long NG = c.gr.N, NF = c.fr.N;
     const double* th = a.th + (long)b * NG;
     const double* WP = a.WP + (long)b * 8 * NG;
@@ -570,12 +607,13 @@ __global__ void __launch_bounds__(128, MB) o4FaceReconKernel(const Ctx* __restri
 // 4b. pointwise factored Roe dissipation on the final faces + one transverse
 // ring (src/BoxOp_RoeCubedSphere.H:73-98).
 template <int D, int MB>
-__global__ void __launch_bounds__(128, MB) o4RoePointKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + D];
+__global__ void __launch_bounds__(128, MB) o4RoePointKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const Box3 PB = c.V0.growTrans(d, 1);
-  forRegion(PB, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(PB, wc, [&](int b, int i, int j, int k) {
     const long NF = c.fr.N;
     double* base = a.face + (long)b * kO4FaceArrays * NF + roff(c.fr, i, j, k);
     double l[8], r[8], o[8];
@@ -589,11 +627,12 @@ __global__ void __launch_bounds__(128, MB) o4RoePointKernel(const Ctx* __restric
 
 // 5. theta-aware point-to-average of the flux sum and total pressure (F1).
 template <int D>
-__global__ void o4FaceAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + D];
+__global__ void o4FaceAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
-  forRegion(c.F1, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.F1, wc, [&](int b, int i, int j, int k) {
     const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
     double* base = a.face + (long)b * kO4FaceArrays * NF;
     const bool sm = base[F_THF * NF + fo] > 0.5;
@@ -612,13 +651,14 @@ __global__ void o4FaceAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
 // 6. mapped flux with separable metrics (bertaMapHostBox, :35-95 and
 // :1361-1450) on F1; zero on F outside it.
 template <int D>
-__global__ void o4FaceMapKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + D];
+__global__ void o4FaceMapKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
   const bool skipFirst = t1 == 0;
-  forRegion(c.F, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.F, wc, [&](int b, int i, int j, int k) {
     const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
     double* base = a.face + (long)b * kO4FaceArrays * NF;
     const bool in1 = (d == 0 || (i >= c.F1.lo[0] && i <= c.F1.hi[0])) && (d == 1 || (j >= c.F1.lo[1] && j <= c.F1.hi[1])) &&
@@ -684,11 +724,12 @@ __global__ void o4FaceMapKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
 
 // 7. radial-area face products of the mapped flux and of <p_tot> (F1).
 template <int D>
-__global__ void o4FaceRadialKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + D];
+__global__ void o4FaceRadialKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
-  forRegion(c.F1, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.F1, wc, [&](int b, int i, int j, int k) {
     const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
     double* base = a.face + (long)b * kO4FaceArrays * NF;
     const double s = adjDr(a.G, d, i);
@@ -712,13 +753,14 @@ __global__ void o4FaceRadialKernel(const Ctx* __restrict__ tab, const RegArgs rg
 // 8. pressure force, dissipation, combine on the final faces V0; writes the
 // flux (scratch and caller).
 template <int D, int MB>
-__global__ void __launch_bounds__(128, MB) o4FaceFinalKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + D];
+__global__ void __launch_bounds__(128, MB) o4FaceFinalKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
   const int tr[2] = {t1, t2};
-  forRegion(c.V0, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.V0, wc, [&](int b, int i, int j, int k) {
     const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
     double* base = a.face + (long)b * kO4FaceArrays * NF;
     const int blk = a.block0 + b;
@@ -864,12 +906,13 @@ __global__ void __launch_bounds__(128, MB) o4FaceFinalKernel(const Ctx* __restri
 
 // 9. flux divergence into rhs (V).
 template <int D>
-__global__ void o4DivKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + D];
+__global__ void o4DivKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const double coef = -a.scale / a.G.dx[d];
-  forRegion(c.V, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.V, wc, [&](int b, int i, int j, int k) {
     const View FX = faceView(c, b, F_FX);
     int p[3] = {i, j, k};
     p[d] += 1;
@@ -881,14 +924,15 @@ __global__ void o4DivKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
 
 // 10. Powell face flux (DivBPowell1, src/BoxOp_DivBcleaning.H:35-74).
 template <int D>
-__global__ void o4PowellFluxKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + D];
+__global__ void o4PowellFluxKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
   const int tr[2] = {t1, t2};
   const Box3 BF = c.V1.extrude(d).growTrans(d, 1);
-  forRegion(BF, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(BF, wc, [&](int b, int i, int j, int k) {
     const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
     double* base = a.face + (long)b * kO4FaceArrays * NF;
     const int blk = a.block0 + b;
@@ -921,14 +965,15 @@ __global__ void o4PowellFluxKernel(const Ctx* __restrict__ tab, const RegArgs rg
 
 // 11. Powell radial-area product and divergence into -J div B (V+1).
 template <int D>
-__global__ void o4PowellProdKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + D];
+__global__ void o4PowellProdKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
   const int tr[2] = {t1, t2};
   const Box3 BP = c.V1.extrude(d);
-  forRegion(BP, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(BP, wc, [&](int b, int i, int j, int k) {
     const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
     double* base = a.face + (long)b * kO4FaceArrays * NF;
     const View BF = faceView(c, b, F_BFLUX);
@@ -944,12 +989,13 @@ __global__ void o4PowellProdKernel(const Ctx* __restrict__ tab, const RegArgs rg
 }
 
 template <int D>
-__global__ void o4PowellDivKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + D];
+__global__ void o4PowellDivKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + D];
   const O4Args& a = c.a;
   constexpr int d = D;
   const double coef = -1.0 / a.G.dx[d];
-  forRegion(c.V1, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.V1, wc, [&](int b, int i, int j, int k) {
     const View BP = faceView(c, b, F_BPROD);
     int p[3] = {i, j, k};
     p[d] += 1;
@@ -958,10 +1004,11 @@ __global__ void o4PowellDivKernel(const Ctx* __restrict__ tab, const RegArgs rg)
 }
 
 // 12. DivBPowell2 with point primitives (src/BoxOp_DivBcleaning.H:80-172).
-__global__ void o4PowellCoefKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + 0];
+__global__ void o4PowellCoefKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + 0];
   const O4Args& a = c.a;
-  forRegion(c.V2, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.V2, wc, [&](int b, int i, int j, int k) {
     const long NG = c.gr.N, o = roff(c.gr, i, j, k);
     const double* WP = a.WP + (long)b * 8 * NG;
     const double* A = cellBasis(a.G, a.block0 + b, j, k);
@@ -985,10 +1032,11 @@ __global__ void o4PowellCoefKernel(const Ctx* __restrict__ tab, const RegArgs rg
   });
 }
 
-__global__ void o4PowellAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + 0];
+__global__ void o4PowellAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + 0];
   const O4Args& a = c.a;
-  forRegion(c.V1, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.V1, wc, [&](int b, int i, int j, int k) {
     const View KP{a.kp + (long)b * 16 * c.v2r.N, c.v2r};
     double* KA = a.kp + (long)b * 16 * c.v2r.N + 8 * c.v2r.N + roff(c.v2r, i, j, k);
 #pragma unroll
@@ -996,10 +1044,11 @@ __global__ void o4PowellAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg)
   });
 }
 
-__global__ void o4PowellApplyKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + 0];
+__global__ void o4PowellApplyKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + 0];
   const O4Args& a = c.a;
-  forRegion(c.V, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.V, wc, [&](int b, int i, int j, int k) {
     const View KA{a.kp + (long)b * 16 * c.v2r.N + 8 * c.v2r.N, c.v2r};
     const View MJ{a.mj + (long)b * c.v1r.N, c.v1r};
     double* R = a.rhs + b * a.rhsStride + roff(c.vr, i, j, k);
@@ -1019,11 +1068,12 @@ __global__ void o4PowellApplyKernel(const Ctx* __restrict__ tab, const RegArgs r
 // rhs(m_d) += -GM faceProduct(<det A A>(d, 0), <rho dr>, 0) and
 // rhs(E) += -GM faceProduct(<det A>, <rho V_r dr>, 0), faceProduct over the
 // two angular directions.
-__global__ void o4GravityKernel(const Ctx* __restrict__ tab, const RegArgs rg) {
-  const Ctx& c = tab[blockIdx.y * 3 + 0];
+__global__ void o4GravityKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + 0];
   const O4Args& a = c.a;
   const double minusGM = -kGrav * kMsun;
-  forRegion(c.V, a.nbox, [&](int b, int i, int j, int k) {
+  forRegion(c.V, wc, [&](int b, int i, int j, int k) {
     const View U{a.U + b * a.uStride, a.ur};
     const int blk = a.block0 + b;
     const double dr0 = radialRow(a.G, i).z;
@@ -1072,6 +1122,11 @@ struct O4Batch {
   Ctx* dev = nullptr;
   std::vector<Ctx> host;
   bool roe = false, powell = false;
+  // work lists: per region kind and direction, chunks of kO4Chunk points of
+  // every box's region, all in one device array
+  WorkChunk* chunks = nullptr;
+  long chunkOff[RG_COUNT][3] = {};
+  int chunkCount[RG_COUNT][3] = {};
   int var[kO4TunedKernels] = {0, 0, 0};  // register-cap variant of the tuned kernels
 };
 
@@ -1105,8 +1160,48 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
   }
   B->roe = boxes[0].G.roe;
   B->powell = boxes[0].G.powell;
+  std::vector<WorkChunk> work;
+  for (int id = 0; id < RG_COUNT; ++id)
+    for (int d = 0; d < 3; ++d) {
+      B->chunkOff[id][d] = (long)work.size();
+      long total = 0, largest = 0;
+      bool equal = true;
+      for (int b = 0; b < nbox; ++b) {
+        const long n = regionOf(B->host[(size_t)b * 3 + d], id).size();
+        total += n;
+        equal = equal && (b == 0 || n == largest);
+        largest = n > largest ? n : largest;
+      }
+      if (equal) {
+        // boxes of one size: each box's CTAs stride over it together
+        // (about 148 x 32 CTAs in all)
+        const long need = (largest + 127) / 128;
+        const long perBox = std::max(1L, std::min(need, 148L * 32 / nbox));
+        for (int b = 0; b < nbox; ++b)
+          for (long x = 0; x < perBox; ++x) work.push_back(WorkChunk{b, (int)(perBox * 128), x * 128, largest});
+      } else {
+        // uneven boxes: contiguous chunks of equal work
+        const long chunk = chunkPoints(total);
+        for (int b = 0; b < nbox; ++b) {
+          const long n = regionOf(B->host[(size_t)b * 3 + d], id).size();
+          for (long t = 0; t < n; t += chunk) work.push_back(WorkChunk{b, 128, t, t + chunk < n ? t + chunk : n});
+        }
+      }
+      const long count = (long)work.size() - B->chunkOff[id][d];
+      if (count > 0x7fffffffL) {
+        *err = cudaErrorInvalidValue;
+        o4BatchDestroy(B);
+        return nullptr;
+      }
+      B->chunkCount[id][d] = (int)count;
+    }
   *err = cudaMalloc(&B->dev, sizeof(Ctx) * B->host.size());
   if (*err == cudaSuccess) *err = cudaMemcpy(B->dev, B->host.data(), sizeof(Ctx) * B->host.size(), cudaMemcpyHostToDevice);
+  if (*err == cudaSuccess && !work.empty()) {
+    *err = cudaMalloc(&B->chunks, sizeof(WorkChunk) * work.size());
+    if (*err == cudaSuccess)
+      *err = cudaMemcpy(B->chunks, work.data(), sizeof(WorkChunk) * work.size(), cudaMemcpyHostToDevice);
+  }
   if (*err != cudaSuccess) {
     o4BatchDestroy(B);
     return nullptr;
@@ -1117,6 +1212,7 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
 void o4BatchDestroy(O4Batch* B) {
   if (!B) return;
   if (B->dev) cudaFree(B->dev);
+  if (B->chunks) cudaFree(B->chunks);
   delete B;
 }
 
@@ -1142,22 +1238,12 @@ void o4SplitArgs(const O4Args& a, std::vector<O4Args>& out) {
 }
 
 namespace {
-// Grid of a launch over the batch: one CTA row per box (y), x sized for the
-// box with the largest region, the whole grid held near 148 x 32 CTAs (the
-// region loops stride over the rest).
-template <class R>
-dim3 gridOf(const O4Batch& B, int d, R region) {
-  long m = 1;
-  for (int b = 0; b < B.nbox; ++b) m = std::max(m, region(B.host[(size_t)b * 3 + d]).size());
-  const long need = (m + 127) / 128;
-  const long perBox = std::max(1L, 148L * 32 / B.nbox);
-  return dim3((unsigned)std::max(1L, std::min(need, perBox)), (unsigned)B.nbox, 1);
-}
 }  // namespace
 
 cudaError_t launchO4BatchGravity(const O4Batch* B, cudaStream_t s) {
   const RegArgs none{};
-  o4GravityKernel<<<gridOf(*B, 0, [](const Ctx& c) { return c.V; }), 128, 0, s>>>(B->dev, none);
+  if (B->chunkCount[RG_V][0] == 0) return cudaSuccess;
+  o4GravityKernel<<<B->chunkCount[RG_V][0], 128, 0, s>>>(B->dev, none, B->chunks + B->chunkOff[RG_V][0]);
   return cudaGetLastError();
 }
 
@@ -1166,9 +1252,11 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
   const RegArgs rg = reg ? *reg : none;
   const Ctx* t = B->dev;
   cudaError_t e;
-#define HC_LAUNCH(kernel, d, region)                                                     \
-  kernel<<<gridOf(*B, d, [](const Ctx& c) { return region; }), 128, 0, s>>>(t, rg);      \
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+#define HC_LAUNCH(kernel, d, region)                                                          \
+  if (B->chunkCount[region][d]) {                                                             \
+    kernel<<<B->chunkCount[region][d], 128, 0, s>>>(t, rg, B->chunks + B->chunkOff[region][d]); \
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;                                    \
+  }
 #define HC_LAUNCH_D(kernel, region)                                                      \
   if (d == 0) { HC_LAUNCH(kernel<0>, 0, region) }                                       \
   else if (d == 1) { HC_LAUNCH(kernel<1>, 1, region) }                                  \
@@ -1177,34 +1265,36 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
   if (B->var[q] == 1) { HC_LAUNCH_DV(kernel, kO4MinBlocks[q][1], region) }                \
   else if (B->var[q] == 2) { HC_LAUNCH_DV(kernel, kO4MinBlocks[q][2], region) }           \
   else { HC_LAUNCH_DV(kernel, kO4MinBlocks[q][0], region) }
-#define HC_LAUNCH_T(d, region, ...)                                                      \
-  __VA_ARGS__<<<gridOf(*B, d, [](const Ctx& c) { return region; }), 128, 0, s>>>(t, rg);  \
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+#define HC_LAUNCH_T(d, region, ...)                                                               \
+  if (B->chunkCount[region][d]) {                                                                 \
+    __VA_ARGS__<<<B->chunkCount[region][d], 128, 0, s>>>(t, rg, B->chunks + B->chunkOff[region][d]); \
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;                                        \
+  }
 #define HC_LAUNCH_DV(kernel, mb, region)                                                 \
   if (d == 0) { HC_LAUNCH_T(0, region, kernel<0, mb>) }                                 \
   else if (d == 1) { HC_LAUNCH_T(1, region, kernel<1, mb>) }                            \
   else { HC_LAUNCH_T(2, region, kernel<2, mb>) }
-  HC_LAUNCH(o4PrimAvgKernel, 0, c.G)
-  HC_LAUNCH(o4ThetaRawKernel, 0, c.GR)
-  HC_LAUNCH(o4PointKernel, 0, c.G)
+  HC_LAUNCH(o4PrimAvgKernel, 0, RG_G)
+  HC_LAUNCH(o4ThetaRawKernel, 0, RG_GR)
+  HC_LAUNCH(o4PointKernel, 0, RG_G)
   for (int d = 0; d < 3; ++d) {
-    HC_LAUNCH_DM(o4FaceReconKernel, 0, c.F)
-    if (B->roe) { HC_LAUNCH_DM(o4RoePointKernel, 1, c.V0.growTrans(c.d, 1)) }
-    HC_LAUNCH_D(o4FaceAvgKernel, c.F1)
-    HC_LAUNCH_D(o4FaceMapKernel, c.F)
-    HC_LAUNCH_D(o4FaceRadialKernel, c.F1)
-    HC_LAUNCH_DM(o4FaceFinalKernel, 2, c.V0)
-    HC_LAUNCH_D(o4DivKernel, c.V)
+    HC_LAUNCH_DM(o4FaceReconKernel, 0, RG_F)
+    if (B->roe) { HC_LAUNCH_DM(o4RoePointKernel, 1, RG_PB) }
+    HC_LAUNCH_D(o4FaceAvgKernel, RG_F1)
+    HC_LAUNCH_D(o4FaceMapKernel, RG_F)
+    HC_LAUNCH_D(o4FaceRadialKernel, RG_F1)
+    HC_LAUNCH_DM(o4FaceFinalKernel, 2, RG_V0)
+    HC_LAUNCH_D(o4DivKernel, RG_V)
     if (B->powell) {
-      HC_LAUNCH_D(o4PowellFluxKernel, c.V1.extrude(c.d).growTrans(c.d, 1))
-      HC_LAUNCH_D(o4PowellProdKernel, c.V1.extrude(c.d))
-      HC_LAUNCH_D(o4PowellDivKernel, c.V1)
+      HC_LAUNCH_D(o4PowellFluxKernel, RG_PF)
+      HC_LAUNCH_D(o4PowellProdKernel, RG_PP)
+      HC_LAUNCH_D(o4PowellDivKernel, RG_V1)
     }
   }
   if (B->powell) {
-    HC_LAUNCH(o4PowellCoefKernel, 0, c.V2)
-    HC_LAUNCH(o4PowellAvgKernel, 0, c.V1)
-    HC_LAUNCH(o4PowellApplyKernel, 0, c.V)
+    HC_LAUNCH(o4PowellCoefKernel, 0, RG_V2)
+    HC_LAUNCH(o4PowellAvgKernel, 0, RG_V1)
+    HC_LAUNCH(o4PowellApplyKernel, 0, RG_V)
   }
 #undef HC_LAUNCH_DV
 #undef HC_LAUNCH_T

@@ -49,6 +49,8 @@ SIGNATURES = {
     "hc_amr_plan_destroy": (C.c_int, [_VP]),
     "hc_amr_rk_stage": (C.c_int, [_VP, _VP, C.c_int, C.c_int, C.c_double, _VP]),
     "hc_amr_restrict": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
+    "hc_amr_plan_set_reflux": (C.c_int, [_VP, _VP, C.c_int]),
+    "hc_amr_reflux": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_ctx_set_o4_variants": (C.c_int, [_VP, _VP]),
     "hc_level_insert_cone": (C.c_int, [_VP, _VP, C.c_double, _VP, _VP, _VP]),
 }
@@ -113,6 +115,15 @@ class HcRestrictBox(C.Structure):
     _fields_ = [("fine", C.c_void_p), ("coarse", C.c_void_p), ("fine_lo", C.c_int * 3), ("fine_n", C.c_int * 3),
                 ("coarse_lo", C.c_int * 3), ("coarse_n", C.c_int * 3), ("lo", C.c_int * 3), ("hi", C.c_int * 3),
                 ("ratio", C.c_int * 3), ("reserved", C.c_int)]
+
+
+class HcRefluxBox(C.Structure):
+    """Mirror of hc_reflux_box in include/hc_abi.h."""
+    _fields_ = [("fine_flux", C.c_void_p), ("coarse_flux", C.c_void_p), ("rhs", C.c_void_p),
+                ("fine_lo", C.c_int * 3), ("fine_n", C.c_int * 3), ("coarse_lo", C.c_int * 3),
+                ("coarse_n", C.c_int * 3), ("rhs_lo", C.c_int * 3), ("rhs_n", C.c_int * 3), ("lo", C.c_int * 3),
+                ("hi", C.c_int * 3), ("ratio", C.c_int * 3), ("dir", C.c_int), ("fine_side", C.c_int),
+                ("reserved", C.c_int), ("scale", C.c_double)]
 
 
 class HcError(RuntimeError):

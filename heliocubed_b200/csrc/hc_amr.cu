@@ -90,6 +90,50 @@ __global__ void __launch_bounds__(kThreads) restrictKernel(const hc_restrict_box
   }
 }
 
+// Reflux of coarse faces covered by the fine level: coarse rhs += coef *
+// (mean of the fine faces - coarse face flux), coef = -scale when the fine
+// cells lie above the face (the corrected coarse cell is the one below),
+// +scale otherwise.
+__global__ void __launch_bounds__(kThreads) refluxKernel(const hc_reflux_box* __restrict__ items,
+                                                         const Chunk* __restrict__ chunks) {
+  const Chunk ch = chunks[blockIdx.x];
+  const hc_reflux_box R = items[ch.item];
+  const int d = R.dir;
+  const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+  const int n0 = R.hi[0] - R.lo[0] + 1, n1 = R.hi[1] - R.lo[1] + 1, n2 = R.hi[2] - R.lo[2] + 1;
+  const long long faces = (long long)n0 * n1 * n2;
+  const long long fineN = (long long)R.fine_n[0] * R.fine_n[1] * R.fine_n[2];
+  const long long coarseN = (long long)R.coarse_n[0] * R.coarse_n[1] * R.coarse_n[2];
+  const long long rhsN = (long long)R.rhs_n[0] * R.rhs_n[1] * R.rhs_n[2];
+  const double w = 1.0 / (double)(R.ratio[t1] * R.ratio[t2]);
+  const double coef = R.fine_side ? -R.scale : R.scale;
+  for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
+    const int c = (int)(t / faces);
+    const long long r = t - (long long)c * faces;
+    int f[3] = {R.lo[0] + (int)(r % n0), R.lo[1] + (int)((r / n0) % n1), R.lo[2] + (int)(r / ((long long)n0 * n1))};
+    double mean = 0.0;
+    for (int b2 = 0; b2 < R.ratio[t2]; ++b2)
+      for (int b1 = 0; b1 < R.ratio[t1]; ++b1) {
+        int g[3];
+        g[d] = f[d] * R.ratio[d];
+        g[t1] = f[t1] * R.ratio[t1] + b1;
+        g[t2] = f[t2] * R.ratio[t2] + b2;
+        const long long o = (long long)(g[0] - R.fine_lo[0]) +
+                            (long long)R.fine_n[0] * ((g[1] - R.fine_lo[1]) + (long long)R.fine_n[1] * (g[2] - R.fine_lo[2]));
+        mean = __dadd_rn(mean, __dmul_rn(w, R.fine_flux[(long long)c * fineN + o]));
+      }
+    const long long co = (long long)(f[0] - R.coarse_lo[0]) +
+                         (long long)R.coarse_n[0] * ((f[1] - R.coarse_lo[1]) + (long long)R.coarse_n[1] * (f[2] - R.coarse_lo[2]));
+    const double diff = __dsub_rn(mean, R.coarse_flux[(long long)c * coarseN + co]);
+    int cell[3] = {f[0], f[1], f[2]};
+    if (R.fine_side) cell[d] -= 1;
+    const long long ro = (long long)(cell[0] - R.rhs_lo[0]) +
+                         (long long)R.rhs_n[0] * ((cell[1] - R.rhs_lo[1]) + (long long)R.rhs_n[1] * (cell[2] - R.rhs_lo[2]));
+    double* out = R.rhs + (long long)c * rhsN + ro;
+    *out = __dadd_rn(*out, __dmul_rn(coef, diff));
+  }
+}
+
 int cudaFailed(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return HC_OK;
   char msg[256];
@@ -105,9 +149,33 @@ int argFail(const char* msg) { return hc::setLastError(HC_ERR_ARG, msg); }
 
 }  // namespace
 
+// Faces of a reflux patch inside its boxes (false if any index leaves them).
+static bool refluxInside(const hc_reflux_box& R) {
+  if (!R.fine_flux || !R.coarse_flux || !R.rhs || R.dir < 0 || R.dir > 2 || (R.fine_side != 0 && R.fine_side != 1))
+    return false;
+  for (int d = 0; d < 3; ++d) {
+    if (R.ratio[d] < 1 || R.ratio[d] > 16 || R.lo[d] > R.hi[d] || R.fine_n[d] < 1 || R.coarse_n[d] < 1 || R.rhs_n[d] < 1)
+      return false;
+    // coarse faces
+    if (R.lo[d] < R.coarse_lo[d] || R.hi[d] >= R.coarse_lo[d] + R.coarse_n[d]) return false;
+    // fine faces: ratio * I along dir; ratio * I + 0 .. ratio-1 across
+    const long long flo = (long long)R.lo[d] * R.ratio[d];
+    const long long fhi = (long long)R.hi[d] * R.ratio[d] + (d == R.dir ? 0 : R.ratio[d] - 1);
+    if (flo < R.fine_lo[d] || fhi >= (long long)R.fine_lo[d] + R.fine_n[d]) return false;
+    // corrected coarse cells
+    const int shift = (d == R.dir && R.fine_side) ? 1 : 0;
+    if (R.lo[d] - shift < R.rhs_lo[d] || R.hi[d] - shift >= R.rhs_lo[d] + R.rhs_n[d]) return false;
+  }
+  return true;
+}
+
 struct hc_amr_plan {
   hc_rk_box* boxes = nullptr;           // device copy
   hc_restrict_box* restricts = nullptr; // device copy
+  hc_reflux_box* reflux = nullptr;      // device copy
+  Chunk* refluxChunks = nullptr;        // work list of the reflux patches (device), by patch
+  std::vector<hc_reflux_box> refluxHost;
+  std::vector<int> refluxChunkStart;
   Chunk* boxChunks = nullptr;           // work list of the combine (device)
   Chunk* restrictChunks = nullptr;      // work list of the restrictions (device), by item
   int nbox = 0, nrestrict = 0, nBoxChunks = 0;
@@ -195,8 +263,69 @@ extern "C" int hc_amr_plan_destroy(hc_amr_plan* P) {
   cudaFree(P->restricts);
   cudaFree(P->boxChunks);
   cudaFree(P->restrictChunks);
+  cudaFree(P->reflux);
+  cudaFree(P->refluxChunks);
   delete P;
   return HC_OK;
+}
+
+extern "C" int hc_amr_plan_set_reflux(hc_amr_plan* P, const hc_reflux_box* patches, int npatch) {
+  if (!P || (npatch && !patches) || npatch < 0) return argFail("hc_amr_plan_set_reflux: bad argument");
+  for (int r = 0; r < npatch; ++r)
+    if (!refluxInside(patches[r]))
+      return argFail("hc_amr_plan_set_reflux: a reflux patch must read its faces and write its cells inside its "
+                     "arrays' boxes (dir 0..2, side 0/1, ratio 1..16)");
+  std::vector<Chunk> rc;
+  std::vector<int> start;
+  for (int r = 0; r < npatch; ++r) {
+    const hc_reflux_box& R = patches[r];
+    start.push_back((int)rc.size());
+    addChunks(rc, r, 8LL * (R.hi[0] - R.lo[0] + 1) * (R.hi[1] - R.lo[1] + 1) * (R.hi[2] - R.lo[2] + 1));
+  }
+  start.push_back((int)rc.size());
+  hc_reflux_box* dev = nullptr;
+  Chunk* devChunks = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (npatch) {
+    e = cudaMalloc(&dev, sizeof(hc_reflux_box) * npatch);
+    if (e == cudaSuccess) e = cudaMemcpy(dev, patches, sizeof(hc_reflux_box) * npatch, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&devChunks, sizeof(Chunk) * rc.size());
+    if (e == cudaSuccess) e = cudaMemcpy(devChunks, rc.data(), sizeof(Chunk) * rc.size(), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(dev);
+    cudaFree(devChunks);
+    return cudaFailed(e, "hc_amr_plan_set_reflux");
+  }
+  cudaFree(P->reflux);
+  cudaFree(P->refluxChunks);
+  P->reflux = dev;
+  P->refluxChunks = devChunks;
+  P->refluxHost.assign(patches, patches + npatch);
+  P->refluxChunkStart = start;
+  return HC_OK;
+}
+
+extern "C" int hc_amr_reflux(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, void* stream) {
+  if (!ctx || !P) return argFail("hc_amr_reflux: null argument");
+  const int n = (int)P->refluxHost.size();
+  if (first < 0 || count < 0 || first + count > n) return argFail("hc_amr_reflux: range outside the plan");
+  // patches of one launch must correct disjoint coarse cells of each rhs array
+  for (int a = first; a < first + count; ++a)
+    for (int b = a + 1; b < first + count; ++b) {
+      const hc_reflux_box &A = P->refluxHost[a], &B = P->refluxHost[b];
+      if (A.rhs != B.rhs) continue;
+      bool overlap = true;
+      for (int d = 0; d < 3 && overlap; ++d) {
+        const int sa = (d == A.dir && A.fine_side) ? 1 : 0, sb = (d == B.dir && B.fine_side) ? 1 : 0;
+        overlap = A.lo[d] - sa <= B.hi[d] - sb && B.lo[d] - sb <= A.hi[d] - sa;
+      }
+      if (overlap) return argFail("hc_amr_reflux: two patches of one launch correct the same coarse cells");
+    }
+  const int c0 = count ? P->refluxChunkStart[first] : 0, c1 = count ? P->refluxChunkStart[first + count] : 0;
+  if (c1 == c0) return HC_OK;
+  refluxKernel<<<c1 - c0, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->reflux, P->refluxChunks + c0);
+  return cudaFailed(cudaGetLastError(), "hc_amr_reflux");
 }
 
 extern "C" int hc_amr_rk_stage(hc_ctx* ctx, const hc_amr_plan* P, int order, int stage, double dt, void* stream) {

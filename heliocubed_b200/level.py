@@ -530,6 +530,24 @@ class AmrPlan:
     def restrict(self, first: int, count: int) -> None:
         N.check(self._lib.hc_amr_restrict(self._shell._ctx, self._h, first, count, _stream()), "hc_amr_restrict")
 
+    def set_reflux(self, patches) -> None:
+        """patches: dicts with fine_flux, coarse_flux, rhs (device tensors),
+        fine_lo, fine_n, coarse_lo, coarse_n, rhs_lo, rhs_n, lo, hi, ratio
+        (3 ints each), dir, fine_side and scale (hc_reflux_box)."""
+        n = len(patches)
+        arr = (N.HcRefluxBox * max(n, 1))()
+        for r, d in enumerate(patches):
+            arr[r].fine_flux = d["fine_flux"].data_ptr()
+            arr[r].coarse_flux = d["coarse_flux"].data_ptr()
+            arr[r].rhs = d["rhs"].data_ptr()
+            for k in ("fine_lo", "fine_n", "coarse_lo", "coarse_n", "rhs_lo", "rhs_n", "lo", "hi", "ratio"):
+                getattr(arr[r], k)[:] = list(d[k])
+            arr[r].dir, arr[r].fine_side, arr[r].scale = d["dir"], d["fine_side"], d["scale"]
+        N.check(self._lib.hc_amr_plan_set_reflux(self._h, arr, n), "hc_amr_plan_set_reflux")
+
+    def reflux(self, first: int, count: int) -> None:
+        N.check(self._lib.hc_amr_reflux(self._shell._ctx, self._h, first, count, _stream()), "hc_amr_reflux")
+
     def close(self) -> None:
         if self._h:
             self._lib.hc_amr_plan_destroy(self._h)

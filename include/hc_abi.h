@@ -270,12 +270,45 @@ typedef struct hc_restrict_box {
   int reserved;
 } hc_restrict_box;
 
+/* One coarse-fine interface patch of the reflux (the flux-register
+ * correction of src/MHD_AMR.H:651-665,916-931): the coarse faces lo..hi
+ * (inclusive, coarse index space; faces of direction dir, face I between
+ * cells I-1 and I) are covered by the fine level on side `fine_side` (1:
+ * the fine cells are at and above the face, the coarse cell corrected is
+ * I-1, whose high face it is; 0: the fine cells are below, the corrected
+ * cell is I).  For each face, Fbar = mean of the ratio x ratio fine faces
+ * covering it (fine face index ratio[dir] * I along dir), and
+ *   rhs(C) += coef * (Fbar - F_coarse)   (fine_side 1: coef = -scale,
+ *                                          fine_side 0: coef = +scale),
+ * scale being the operator's scale / dxi[dir] of the coarse level.  Arrays
+ * are 8 components, component-major over their storage boxes: fine_flux
+ * and coarse_flux over face boxes (lo, n), rhs over a cell box. */
+typedef struct hc_reflux_box {
+  const double* fine_flux;
+  const double* coarse_flux;
+  double* rhs;
+  int fine_lo[3], fine_n[3];
+  int coarse_lo[3], coarse_n[3];
+  int rhs_lo[3], rhs_n[3];
+  int lo[3], hi[3];
+  int ratio[3];
+  int dir, fine_side;
+  int reserved;
+  double scale;
+} hc_reflux_box;
+
 typedef struct hc_amr_plan hc_amr_plan;
 
-/* Validate the boxes and restrictions (host arrays; every restriction must
- * read and write inside its boxes) and keep a device copy of each list. */
+/* Validate the boxes, restrictions and reflux patches (host arrays; every
+ * restriction and patch must read and write inside its arrays' boxes) and
+ * keep a device copy of each list. */
 int hc_amr_plan_create(hc_ctx* ctx, const hc_rk_box* boxes, int nbox, const hc_restrict_box* restricts,
                        int nrestrict, hc_amr_plan** out);
+int hc_amr_plan_set_reflux(hc_amr_plan* plan, const hc_reflux_box* patches, int npatch);
+
+/* Reflux patches first .. first+count-1 of the plan in one launch (patches
+ * of one launch must not correct the same coarse cell). */
+int hc_amr_reflux(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
 int hc_amr_plan_destroy(hc_amr_plan* plan);
 
 /* The tableau (order 3: Kutta RK3, 4: classical RK4, src/MHD_AMRRungeKutta.H:

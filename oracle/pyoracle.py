@@ -371,3 +371,34 @@ def amr_restrict(fine: np.ndarray, fine_lo, coarse: np.ndarray, coarse_lo, lo, h
                 total = total + w * fine[:, fk[:, None, None], fj[None, :, None], fi[None, None, :]]
     coarse[:, K[0] - coarse_lo[2]:K[-1] - coarse_lo[2] + 1, J[0] - coarse_lo[1]:J[-1] - coarse_lo[1] + 1,
            I[0] - coarse_lo[0]:I[-1] - coarse_lo[0] + 1] = total
+
+
+def amr_reflux(fine_flux, fine_lo, coarse_flux, coarse_lo, rhs, rhs_lo, lo, hi, ratio, d, fine_side, scale) -> None:
+    """Reflux of coarse faces lo..hi of direction d covered by the fine level
+    (src/MHD_AMR.H:651-665,916-931, the flux-register correction): for each
+    face, the mean of the ratio x ratio covering fine faces (products then
+    sums, the higher transverse index outer) minus the coarse face flux,
+    times -scale (fine_side 1: the corrected cell is below the face) or
+    +scale (fine_side 0: the cell above), added to the coarse rhs.  Arrays
+    are [8][k][j][i] over boxes with the given low corners."""
+    t1, t2 = [x for x in range(3) if x != d]
+    w = 1.0 / float(ratio[t1] * ratio[t2])
+    coef = -scale if fine_side else scale
+    for K in range(lo[2], hi[2] + 1):
+        for J in range(lo[1], hi[1] + 1):
+            for I in range(lo[0], hi[0] + 1):
+                f = [I, J, K]
+                mean = np.zeros(8)
+                for b2 in range(ratio[t2]):
+                    for b1 in range(ratio[t1]):
+                        g = [0, 0, 0]
+                        g[d] = f[d] * ratio[d]
+                        g[t1] = f[t1] * ratio[t1] + b1
+                        g[t2] = f[t2] * ratio[t2] + b2
+                        mean = mean + w * fine_flux[:, g[2] - fine_lo[2], g[1] - fine_lo[1], g[0] - fine_lo[0]]
+                diff = mean - coarse_flux[:, K - coarse_lo[2], J - coarse_lo[1], I - coarse_lo[0]]
+                cell = list(f)
+                if fine_side:
+                    cell[d] -= 1
+                idx = (slice(None), cell[2] - rhs_lo[2], cell[1] - rhs_lo[1], cell[0] - rhs_lo[0])
+                rhs[idx] = rhs[idx] + coef * diff

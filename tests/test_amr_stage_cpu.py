@@ -69,3 +69,54 @@ def test_plan_rejects_boxes_without_arrays():
     arr = (N.HcRkBox * 1)(b)
     out = C.c_void_p()
     assert lib.hc_amr_plan_create(C.c_void_p(1), arr, 1, None, 0, C.byref(out)) == -1
+
+
+def test_reflux_oracle_signs_and_zero_correction():
+    """Equal fine and coarse fluxes leave the rhs unchanged; a fine excess
+    delta on a face corrects the coarse cell below it (fine above) by
+    -scale * delta and the cell above it (fine below) by +scale * delta."""
+    rng = np.random.default_rng(1)
+    coarse_flux = rng.normal(size=(8, 4, 4, 5))            # faces of dir 0 over lo (0,0,0)
+    fine_flux = np.zeros((8, 8, 8, 9))                     # fine faces of dir 0, ratio 2
+    for I in range(5):
+        fine_flux[:, :, :, 2 * I] = np.repeat(np.repeat(coarse_flux[:, :, :, I], 2, axis=1), 2, axis=2)
+    rhs = rng.normal(size=(8, 4, 4, 4))
+    before = rhs.copy()
+    po.amr_reflux(fine_flux, (0, 0, 0), coarse_flux, (0, 0, 0), rhs, (0, 0, 0), (2, 0, 0), (2, 3, 3), (2, 2, 2), 0,
+                  1, 3.0)
+    assert np.allclose(rhs, before, atol=1e-15)
+    fine_flux[:, :, :, 4] += 0.5        # fine faces at coarse face I = 2
+    po.amr_reflux(fine_flux, (0, 0, 0), coarse_flux, (0, 0, 0), rhs, (0, 0, 0), (2, 0, 0), (2, 3, 3), (2, 2, 2), 0,
+                  1, 3.0)
+    assert np.allclose(rhs[:, :, :, 1] - before[:, :, :, 1], -1.5)
+    assert np.array_equal(rhs[:, :, :, 2], before[:, :, :, 2])
+    rhs2 = before.copy()
+    po.amr_reflux(fine_flux, (0, 0, 0), coarse_flux, (0, 0, 0), rhs2, (0, 0, 0), (2, 0, 0), (2, 3, 3), (2, 2, 2), 0,
+                  0, 3.0)
+    assert np.allclose(rhs2[:, :, :, 2] - before[:, :, :, 2], 1.5)
+
+
+def _patch(**kw):
+    r = N.HcRefluxBox()
+    r.fine_flux, r.coarse_flux, r.rhs = 8, 16, 24
+    d = dict(fine_lo=(0, 0, 0), fine_n=(9, 8, 8), coarse_lo=(0, 0, 0), coarse_n=(5, 4, 4), rhs_lo=(0, 0, 0),
+             rhs_n=(4, 4, 4), lo=(2, 0, 0), hi=(2, 3, 3), ratio=(2, 2, 2))
+    d.update(kw)
+    for k, v in d.items():
+        getattr(r, k)[:] = list(v)
+    r.dir, r.fine_side, r.scale = kw.get("dir", 0), kw.get("fine_side", 1), 1.0
+    return r
+
+
+@pytest.mark.parametrize("bad", [dict(hi=(2, 4, 3)), dict(fine_n=(9, 7, 8)), dict(rhs_lo=(2, 0, 0)),
+                                 dict(lo=(0, 0, 0), hi=(0, 3, 3)), dict(ratio=(2, 0, 2))])
+def test_reflux_patches_outside_their_boxes_are_rejected(bad):
+    lib = N.lib()
+    plan = C.c_void_p()
+    assert lib.hc_amr_plan_create(C.c_void_p(1), None, 0, None, 0, C.byref(plan)) == 0
+    try:
+        arr = (N.HcRefluxBox * 1)(_patch(**bad))
+        assert lib.hc_amr_plan_set_reflux(plan, arr, 1) == -1
+        assert b"reflux patch" in lib.hc_last_error()
+    finally:
+        lib.hc_amr_plan_destroy(plan)

@@ -84,3 +84,56 @@ def test_restrictions_match_oracle(oracle_lib):
     for d, expect in zip(items, ref):
         assert np.array_equal(d["coarse"].cpu().numpy(), expect.reshape(-1))
     plan.close()
+
+
+REFLUX = [
+    dict(dir=0, fine_side=1, ratio=(2, 2, 2), lo=(2, 1, 0), hi=(2, 3, 2)),
+    dict(dir=1, fine_side=0, ratio=(2, 2, 2), lo=(0, 1, 1), hi=(3, 1, 2)),
+    dict(dir=2, fine_side=1, ratio=(2, 1, 1), lo=(1, 0, 3), hi=(3, 2, 3)),
+]
+
+
+@pytest.mark.parametrize("case", REFLUX)
+def test_reflux_matches_oracle(oracle_lib, case):
+    _need_gpu()
+    po = oracle_lib
+    rng = np.random.default_rng(case["dir"])
+    sh = hc.Shell(hc.Params(nr=8, na=8))
+    d, r = case["dir"], case["ratio"]
+    coarse_n = [5, 5, 5]
+    coarse_n[d] += 1                      # face box
+    fine_n = [10 * r[0] // 2 + 2, 10 * r[1] // 2 + 2, 10 * r[2] // 2 + 2]
+    rhs_n = (5, 5, 5)
+    coarse_flux = rng.normal(size=(8, coarse_n[2], coarse_n[1], coarse_n[0]))
+    fine_flux = rng.normal(size=(8, fine_n[2], fine_n[1], fine_n[0]))
+    rhs = rng.normal(size=(8, rhs_n[2], rhs_n[1], rhs_n[0]))
+    expect = rhs.copy()
+    po.amr_reflux(fine_flux, (0, 0, 0), coarse_flux, (0, 0, 0), expect, (0, 0, 0), case["lo"], case["hi"], r, d,
+                  case["fine_side"], 7.5)
+    t = {k: torch.from_numpy(v.reshape(-1).copy()).cuda() for k, v in
+         (("fine_flux", fine_flux), ("coarse_flux", coarse_flux), ("rhs", rhs))}
+    plan = AmrPlan(sh, [])
+    plan.set_reflux([dict(t, fine_lo=(0, 0, 0), fine_n=fine_n, coarse_lo=(0, 0, 0), coarse_n=coarse_n,
+                          rhs_lo=(0, 0, 0), rhs_n=rhs_n, lo=case["lo"], hi=case["hi"], ratio=r, dir=d,
+                          fine_side=case["fine_side"], scale=7.5)])
+    plan.reflux(0, 1)
+    assert np.array_equal(t["rhs"].cpu().numpy(), expect.reshape(-1))
+    plan.close()
+
+
+def test_reflux_launch_rejects_overlapping_patches():
+    _need_gpu()
+    sh = hc.Shell(hc.Params(nr=8, na=8))
+    flux = torch.zeros(8 * 6 * 5 * 5, dtype=torch.float64, device="cuda")
+    fine = torch.zeros(8 * 12 * 12 * 12, dtype=torch.float64, device="cuda")
+    rhs = torch.zeros(8 * 125, dtype=torch.float64, device="cuda")
+    base = dict(fine_flux=fine, coarse_flux=flux, rhs=rhs, fine_lo=(0, 0, 0), fine_n=(12, 12, 12),
+                coarse_lo=(0, 0, 0), coarse_n=(6, 5, 5), rhs_lo=(0, 0, 0), rhs_n=(5, 5, 5), ratio=(2, 2, 2),
+                dir=0, fine_side=1, scale=1.0)
+    plan = AmrPlan(sh, [])
+    plan.set_reflux([dict(base, lo=(2, 0, 0), hi=(2, 3, 3)), dict(base, lo=(2, 2, 2), hi=(2, 4, 4))])
+    with pytest.raises(hc.HcError):
+        plan.reflux(0, 2)
+    plan.reflux(0, 1)
+    plan.reflux(1, 1)
+    plan.close()

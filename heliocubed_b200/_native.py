@@ -53,6 +53,8 @@ SIGNATURES = {
     "hc_amr_reflux": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_ctx_set_o4_variants": (C.c_int, [_VP, _VP]),
     "hc_level_insert_cone": (C.c_int, [_VP, _VP, C.c_double, _VP, _VP, _VP]),
+    "hc_cone_event": (C.c_int, [_VP, _VP]),
+    "hc_level_set_cme_schedule": (C.c_int, [_VP, _VP, C.c_int, _VP]),
 }
 
 
@@ -124,6 +126,12 @@ class HcRefluxBox(C.Structure):
                 ("coarse_n", C.c_int * 3), ("rhs_lo", C.c_int * 3), ("rhs_n", C.c_int * 3), ("lo", C.c_int * 3),
                 ("hi", C.c_int * 3), ("ratio", C.c_int * 3), ("dir", C.c_int), ("fine_side", C.c_int),
                 ("reserved", C.c_int), ("scale", C.c_double)]
+
+
+class HcCmeEvent(C.Structure):
+    """Mirror of hc_cme_event in include/hc_abi.h."""
+    _fields_ = [("insertion_time", C.c_double), ("feeding_end", C.c_double), ("boundary", C.c_int),
+                ("reserved", C.c_int)]
 
 
 class HcError(RuntimeError):

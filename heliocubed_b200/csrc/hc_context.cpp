@@ -250,6 +250,10 @@ struct hc_ctx {
   int tileRK = 0, tileRHS = 0;
   // register-cap variants of the fourth-order operator's tuned kernels
   int o4var[kO4TunedKernels] = {0, 0, 0};
+  // CME insertion schedule (device) and the Rusanov-window flag it sets
+  CmeSchedule* sched = nullptr;
+  int* rusanovFlag = nullptr;
+  int schedEvents = 0;
   bool tuned = false;
   // fourth-order operator: metric tables and grow-only scratch
   O4Geo o4{};
@@ -572,6 +576,14 @@ int buildO4Geometry(hc_ctx* c) {
   g.gamma = P.gamma; g.invGm1 = 1.0 / (P.gamma - 1.0); g.entropy = P.entropy_fix_coeff; g.eta_d = P.berta_eta_d;
   g.dx[0] = 1.0 / nr; g.dx[1] = 1.0 / na; g.dx[2] = 1.0 / na;
   g.roe = P.riemann_solver == 2; g.powell = P.divergence_cleaning == 1; g.fallback = P.berta_fallback_type;
+  // the CME insertion window's Rusanov flag (0 until a schedule sets it)
+  {
+    cudaError_t ferr = cudaMalloc(&c->rusanovFlag, sizeof(int));
+    if (ferr == cudaSuccess) ferr = cudaMemset(c->rusanovFlag, 0, sizeof(int));
+    if (ferr != cudaSuccess) return cudaFail(ferr, "O4 flag");
+    c->owned.push_back(c->rusanovFlag);
+  }
+  g.rusanov = c->rusanovFlag;
   if (err != cudaSuccess) return cudaFail(err, "O4 geometry upload");
   return HC_OK;
 }
@@ -1430,6 +1442,50 @@ int maybeAutotune(hc_ctx* c, const double* ju, cudaStream_t s) {
 
 extern "C" {
 
+int hc_cone_event(const hc_cone* cone, hc_cme_event* out) {
+  if (!cone || !out) return fail(HC_ERR_ARG, "null argument");
+  // a finite cloud feeds through the inner boundary while it crosses it
+  // (src/MHD_CME.H:1251-1253): boundary source iff it ends after insertion
+  std::memset(out, 0, sizeof *out);
+  out->insertion_time = cone->insertion_time;
+  out->boundary = cone->end_time > cone->insertion_time ? 1 : 0;
+  out->feeding_end = std::max(cone->insertion_time, cone->end_time);
+  return HC_OK;
+}
+
+int hc_level_set_cme_schedule(hc_ctx* c, const hc_cme_event* events, int n, void* stream) {
+  if (!c || (n && !events)) return fail(HC_ERR_ARG, "null argument");
+  if (n < 0 || n > kCmeEvents) return fail(HC_ERR_ARG, "at most 8 CME events");
+  for (int i = 1; i < n; ++i)
+    if (events[i].insertion_time < events[i - 1].insertion_time)
+      return fail(HC_ERR_ARG, "CME events must be ordered by insertion time");
+  CmeSchedule h{};
+  h.n = n;
+  h.roe = c->P.riemann_solver == 2 && c->P.spatial_order == 4 ? 1 : 0;
+  h.cfl = c->P.cfl;
+  h.feeding = c->P.riemann_solver == 2 ? .5 : 1.;
+  for (int i = 0; i < n; ++i) {
+    const hc_cme_event& e = events[i];
+    h.t[i] = e.insertion_time;
+    h.boundary[i] = e.boundary ? 1 : 0;
+    // stabilizationEnd, src/MHD_CME.H:1329-1332
+    h.stabEnd[i] = e.boundary ? std::max(e.feeding_end + 600, e.insertion_time + 2400) : e.insertion_time + 600;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!c->sched) {
+    cudaError_t err = cudaMalloc(&c->sched, sizeof(CmeSchedule));
+    if (err != cudaSuccess) return cudaFail(err, "CME schedule");
+    c->owned.push_back(c->sched);
+  }
+  // pageable source: the copy is staged before the call returns, then
+  // ordered on the stream after the work already queued there
+  cudaError_t err = cudaMemcpyAsync(c->sched, &h, sizeof h, cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess && n == 0 && c->rusanovFlag) err = cudaMemsetAsync(c->rusanovFlag, 0, sizeof(int), s);
+  if (err != cudaSuccess) return cudaFail(err, "CME schedule");
+  c->schedEvents = n;
+  return HC_OK;
+}
+
 int hc_stage_tiles(int* shapes, int capacity) {
   for (int t = 0; shapes && t < kStageTiles && t < capacity; ++t) stageTileShape(t, shapes + 5 * t);
   return kStageTiles;
@@ -1494,6 +1550,8 @@ int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, do
     const double* invMax = reinterpret_cast<const double*>(c->invMax);
     for (int n = 0; n < nsteps && rc == HC_OK; ++n) {
       rc = checkLaunch(launchCfl(c->L, ju, c->invMax, s), "cfl");
+      if (rc == HC_OK && c->sched && time_dev)
+        rc = checkLaunch(launchCmeSchedule(c->sched, c->invMax, time_dev, c->rusanovFlag, s), "CME schedule");
       if (rc == HC_OK) rc = o4Step(c, ju, 0.0, invMax, 0.0, time_dev, s);
       if (rc == HC_OK) rc = checkLaunch(launchAdvanceTime(time_dev, invMax, c->P.cfl, dt_dev, s), "time");
     }
@@ -1509,6 +1567,8 @@ int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, do
     unsigned long long* next = c->invMax + (1 - cur);
     const double* invMax = reinterpret_cast<const double*>(c->invMax + cur);
     rc = checkLaunch(cudaMemsetAsync(next, 0, sizeof(unsigned long long), s), "cfl reset");
+    if (rc == HC_OK && c->sched && time_dev)
+      rc = checkLaunch(launchCmeSchedule(c->sched, c->invMax + cur, time_dev, nullptr, s), "CME schedule");
     if (rc == HC_OK) rc = rkStep(c, ju, 0.0, invMax, n + 1 < nsteps ? next : nullptr, 0.0, time_dev, s);
     if (rc == HC_OK) rc = checkLaunch(launchAdvanceTime(time_dev, invMax, c->P.cfl, dt_dev, s), "time");
   }

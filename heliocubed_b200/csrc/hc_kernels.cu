@@ -578,6 +578,30 @@ __global__ void boxGravityKernel(const DevLevel L, int lo0, int lo1, int lo2, in
   }
 }
 
+// src/MHD_CME.H:1275-1297 (cfl) and :1267-1271, 1329-1332 (rusanovEndTime).
+__global__ void cmeScheduleKernel(const CmeSchedule* S, unsigned long long* invMaxBits, const double* time,
+                                  int* rusanov) {
+  const double t = *time;
+  double fraction = 1;
+  double end = -INFINITY;
+  for (int i = 0; i < S->n; ++i) {
+    if (!(t >= S->t[i])) continue;  // not inserted yet
+    const double early = fmin(fmax((t - S->t[i] - 600) / 1800., 0.), 1.);
+    double sourceFraction = .2 + .8 * early;
+    if (S->boundary[i]) {
+      const double recovery = fmin(fmax((t - S->stabEnd[i]) / 1800., 0.), 1.);
+      sourceFraction = .2 + (S->feeding - .2) * early + (1 - S->feeding) * recovery;
+    }
+    fraction = fmin(fraction, sourceFraction);
+    end = fmax(end, S->stabEnd[i]);
+  }
+  const bool window = S->roe && t < end - 1e-9 * fmax(1.0, fabs(end));
+  double rate = __longlong_as_double((long long)*invMaxBits) / fraction;
+  if (window) rate = fmax(rate, S->cfl / (end - t));
+  *invMaxBits = (unsigned long long)__double_as_longlong(rate);
+  if (rusanov) *rusanov = window ? 1 : 0;
+}
+
 __global__ void advanceTimeKernel(double* time, const double* invDtMax, double cfl, double* dtOut) {
   const double dt = cfl / *invDtMax;
   if (time) *time += dt;
@@ -690,6 +714,12 @@ cudaError_t launchBoxGravity(const DevLevel& L, const int lo[3], const int hi[3]
   const long wN = (long)wn[0] * wn[1] * wn[2];
   boxGravityKernel<<<gridFor((long)v0 * v1 * v2, 256), 256, 0, s>>>(L, lo[0], lo[1], lo[2], v0, v1, v2, block, w, wlo[0],
                                                                      wlo[1], wlo[2], wn[0], wn[1], wN, rhs);
+  return cudaGetLastError();
+}
+
+cudaError_t launchCmeSchedule(const CmeSchedule* sched, unsigned long long* invMaxBits, const double* time,
+                              int* rusanov, cudaStream_t s) {
+  cmeScheduleKernel<<<1, 1, 0, s>>>(sched, invMaxBits, time, rusanov);
   return cudaGetLastError();
 }
 

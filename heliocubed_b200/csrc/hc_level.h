@@ -126,6 +126,23 @@ cudaError_t launchInit(const DevLevel& L, const void* init, double* ju, cudaStre
 cudaError_t launchBoxGravity(const DevLevel& L, const int lo[3], const int hi[3], int block, const double* w,
                              const int wlo[3], const int wn[3], double* rhs, cudaStream_t s);
 cudaError_t launchAdvanceTime(double* time, const double* invDtMax, double cfl, double* dtOut, cudaStream_t s);
+
+// CME insertion schedule (src/MHD_CME.H:1243-1334 CMEInsertionSchedule):
+// sources inserted at t (device: once time >= t), their stabilisation ends
+// and whether they feed through the boundary.
+constexpr int kCmeEvents = 8;
+struct CmeSchedule {
+  int n, roe;
+  double cfl, feeding;  // target CFL; feeding fraction (0.5 with Roe, 1 with Rusanov, exec/main.cpp:374)
+  double t[kCmeEvents], stabEnd[kCmeEvents];
+  int boundary[kCmeEvents];
+};
+// At the start of a step: the CFL rate in *invMaxBits (a non-negative double's
+// bits) becomes rate / fraction(time), and no smaller than cfl / (window end
+// - time) inside the Rusanov window, so dt = cfl / rate lands on the window's
+// end; *rusanov = Roe context inside the window.
+cudaError_t launchCmeSchedule(const CmeSchedule* sched, unsigned long long* invMaxBits, const double* time,
+                              int* rusanov, cudaStream_t s);
 cudaError_t launchBitsToDouble(const unsigned long long* bits, double* out, cudaStream_t s);
 
 }  // namespace hc
@@ -149,6 +166,7 @@ struct O4Geo {
   const double4* radial;  // [nr+2*kO4Rad+1], index i+kO4Rad: {rlow^2, areaT, Dr0, dVolr}
   double gamma, invGm1, entropy, eta_d, dx[3];
   int roe, powell, fallback;
+  const int* rusanov;     // device flag (may be null): nonzero runs a Roe context with Rusanov dissipation
 };
 
 // A box region: low corner, extents, cell count.

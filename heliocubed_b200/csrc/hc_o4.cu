@@ -413,6 +413,10 @@ __device__ __forceinline__ void forRegion(const Box3& b, const WorkChunk& w, F f
   }
 }
 
+// Roe dissipation unless the device flag switches a Roe context to Rusanov
+// (the CME insertion window, exec/main.cpp:406-420).
+__device__ __forceinline__ bool roeNow(const O4Geo& G) { return G.roe && !(G.rusanov && *G.rusanov); }
+
 // ---- kernels ------------------------------------------------------------------
 // 1. detector primitives of the averages, V(<U>) (:1776).
 __global__ void o4PrimAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
@@ -566,7 +570,7 @@ __global__ void __launch_bounds__(128, MB) o4FaceReconKernel(const Ctx* __restri
     double l[8], r[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) { l[q] = sLR[q][threadIdx.x]; r[q] = sLR[8 + q][threadIdx.x]; }
-    if (a.G.roe) {
+    if (roeNow(a.G)) {
       double cl[8], cr[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) { cl[q] = WA[q * NG + cell[2]]; cr[q] = WA[q * NG + cell[3]]; }
@@ -590,7 +594,7 @@ __global__ void __launch_bounds__(128, MB) o4FaceReconKernel(const Ctx* __restri
     for (int q = 0; q < 8; ++q) base[(F_FS + q) * NF] = fl[q] + fr[q];
     base[F_PS * NF] = (l[4] + ml) + (r[4] + mr);
     base[F_BP * NF] = (l[5 + d] + r[5 + d]) * 0.5;
-    if (!a.G.roe) {
+    if (!roeNow(a.G)) {
       const double rad = radialPoint(a.G, d, i);
       const double g = a.G.gamma;
       base[(F_QD + 0) * NF] = rad * r[0] - rad * l[0];
@@ -611,6 +615,7 @@ __global__ void __launch_bounds__(128, MB) o4RoePointKernel(const Ctx* __restric
   const WorkChunk wc = wk[blockIdx.x];
   const Ctx& c = tab[wc.box * 3 + D];
   const O4Args& a = c.a;
+  if (!roeNow(a.G)) return;  // the Rusanov window: the reconstruction wrote the Rusanov jump
   constexpr int d = D;
   const Box3 PB = c.V0.growTrans(d, 1);
   forRegion(PB, wc, [&](int b, int i, int j, int k) {
@@ -788,7 +793,7 @@ __global__ void __launch_bounds__(128, MB) o4FaceFinalKernel(const Ctx* __restri
     const bool sm = base[F_THF * NF + fo] > 0.5;
     const View QD = faceView(c, b, F_QD);
     double diss[8];
-    if (a.G.roe) {
+    if (roeNow(a.G)) {
       double dM[2][10];
 #pragma unroll
       for (int q = 0; q < 2; ++q) {

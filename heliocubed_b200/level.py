@@ -339,6 +339,19 @@ class Shell:
         ju = perturbed_wind_state(p, det, dvolr, seed, amp)
         return torch.from_numpy(np.ascontiguousarray(ju.reshape(-1))).to(self._dev)
 
+    def set_cme_schedule(self, events) -> None:
+        """hc_level_set_cme_schedule on the current stream: events are
+        hc_cme_event structures or prepared cones (their schedule events via
+        hc_cone_event)."""
+        n = len(events)
+        arr = (N.HcCmeEvent * max(n, 1))()
+        for i, e in enumerate(events):
+            if isinstance(e, N.HcCone):
+                N.check(self._lib.hc_cone_event(C.byref(e), C.byref(arr[i])), "hc_cone_event")
+            else:
+                arr[i] = e
+        N.check(self._lib.hc_level_set_cme_schedule(self._ctx, arr, n, _stream()), "hc_level_set_cme_schedule")
+
     def autotune(self, ju: torch.Tensor) -> tuple[tuple[int, ...], np.ndarray]:
         """hc_ctx_autotune with the state `ju` (not modified).  Order 2:
         ((RK stage tile, operator tile), median ms [2][tiles]).  Order 4:

@@ -90,10 +90,13 @@ class Request:
 def admit(shell: Shell, req: Request, ju: torch.Tensor, time_dev: torch.Tensor) -> None:
     """Device-side admission on the current stream: the wind into `ju`, the
     request's cone cloud inserted at its insertion time, the model time set
-    to that time."""
+    to that time, and the insertion schedule (CFL ramp, and the Rusanov
+    window of fourth-order Roe solves) that the reference's driver applies
+    after an insertion."""
     shell.init(wind_spec(), ju)
     cone = req.cone.prepared(shell.params)
     shell.insert_cone(cone, cone.insertion_time, ju)
+    shell.set_cme_schedule([cone])
     time_dev.fill_(cone.insertion_time)
 
 
@@ -119,8 +122,10 @@ class Slot:
         self.time = torch.zeros(1, dtype=torch.float64, device=self.shell._dev)
         self.host_out = torch.empty(self.state.numel(), dtype=torch.float64).pin_memory()
         self.host_time = torch.empty(1, dtype=torch.float64).pin_memory()
-        # capture on a valid (wind) state; admission overwrites the buffer
+        # capture on a valid (wind) state with the (empty) insertion schedule
+        # in the step; admission overwrites the buffer and the schedule
         self.shell.init(wind_spec(), self.state)
+        self.shell.set_cme_schedule([])
         torch.cuda.synchronize(device)
         with torch.cuda.stream(self.stream):
             self.graph = self.shell.capture_advance(self.state, chunk, self.time)

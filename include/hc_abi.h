@@ -424,6 +424,39 @@ int hc_cone_prepare(const hc_cone_spec* spec, double inner_radius, hc_cone* cone
  * in a fixed order. */
 int hc_level_insert_cone(hc_ctx* ctx, const hc_cone* cone, double time, double* ju, double* stats, void* stream);
 
+/* One inserted CME source of the insertion schedule (src/MHD_CME.H:
+ * 1243-1334, CMEInsertionSchedule): its insertion time, whether it feeds
+ * through the inner boundary, and when that feeding ends. */
+typedef struct hc_cme_event {
+  double insertion_time;
+  double feeding_end;
+  int boundary;
+  int reserved;
+} hc_cme_event;
+
+/* The schedule event of a prepared cone cloud: a boundary source while the
+ * cloud still crosses the inner boundary after insertion (:1251-1253). */
+int hc_cone_event(const hc_cone* cone, hc_cme_event* event);
+
+/* The driver's stabilisation after CME insertions (exec/main.cpp:374-420),
+ * applied by hc_level_advance_cfl on the device with no host sync.  Each
+ * step's dt uses CFL x fraction(time): the minimum over the sources inserted
+ * by then (time >= insertion_time) of 0.2 + 0.8 early for a volume source,
+ * or 0.2 + (f - 0.2) early + (1 - f) recovery for a boundary source, with
+ * early = clamp((time - t - 600) / 1800, 0, 1), recovery = clamp((time -
+ * end) / 1800, 0, 1), f = 0.5 with Roe and 1 with Rusanov, and end the
+ * source's stabilisation end (t + 600, or max(feeding_end + 600, t + 2400)
+ * for a boundary source) (src/MHD_CME.H:1275-1297, 1329-1332).  A
+ * fourth-order Roe context uses Rusanov dissipation while time is before the
+ * latest stabilisation end, with dt shortened to land on it (the reference's
+ * Rusanov window; second-order contexts get the CFL ramp only).  n = 0
+ * clears; at most 8 events, ordered by insertion time.  The schedule is
+ * copied to the device in order on `stream`.  After the first call every
+ * hc_level_advance_cfl step runs the schedule (with no events it changes
+ * nothing), so a graph captured after a call with n = 0 takes later
+ * schedules. */
+int hc_level_set_cme_schedule(hc_ctx* ctx, const hc_cme_event* events, int n, void* stream);
+
 /* Host copies of the level geometry used by the kernels, for tests:
  * what = 0 radial line [nr+1][4]: rlow^2, (rhigh^2-rlow^2)/(2dxi0),
  *          (rhigh-rlow)/dxi0, dVolr (last row: face only)

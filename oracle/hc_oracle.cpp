@@ -1296,6 +1296,27 @@ void levelInsertCone(const Level& L, const hc_cone& c, double time, double* ju, 
   }
 }
 
+// CME insertion schedule, src/MHD_CME.H:1243-1334: the CFL fraction of
+// cfl() (:1275-1297) and rusanovEndTime() (:1267-1271) over the sources
+// inserted by `time`, stabilizationEnd (:1329-1332).
+void cmeSchedule(const hc_cme_event* ev, int n, double time, double feeding, double& fraction, double& end) {
+  fraction = 1;
+  end = -std::numeric_limits<double>::infinity();
+  for (int i = 0; i < n; ++i) {
+    if (!(time >= ev[i].insertion_time)) continue;
+    const double t = ev[i].insertion_time;
+    const double stab = ev[i].boundary ? std::max(ev[i].feeding_end + 600, t + 2400) : t + 600;
+    const double early = std::clamp((time - t - 600) / 1800., 0., 1.);
+    double sourceFraction = .2 + .8 * early;
+    if (ev[i].boundary) {
+      const double recovery = std::clamp((time - stab) / 1800., 0., 1.);
+      sourceFraction = .2 + (feeding - .2) * early + (1 - feeding) * recovery;
+    }
+    fraction = std::min(fraction, sourceFraction);
+    end = std::max(end, stab);
+  }
+}
+
 #include "hc_oracle_o4.inc"
 
 }  // namespace
@@ -1359,6 +1380,9 @@ int orc_cone_cell(const hc_cone* c, double time, const double* pos, const double
                   double* delta) {
   const double shift = c->entry_shift + c->speed * 1e5 * (time - c->entry_time);
   return coneCellDelta(*c, shift, pos, ambient, gamma, delta) ? 1 : 0;
+}
+void orc_cme_schedule(const hc_cme_event* ev, int n, double time, double feeding, double* out) {
+  cmeSchedule(ev, n, time, feeding, out[0], out[1]);
 }
 int orc_level_insert_cone(void* L, const hc_cone* c, double time, double* ju, double* stats) {
   levelInsertCone(*static_cast<Level*>(L), *c, time, ju, stats);

@@ -54,6 +54,12 @@ class HcConeSpec(C.Structure):
     _fields_ = [(n, C.c_double) for n in CONE_SPEC_FIELDS] + [("reserved", C.c_double * 6)]
 
 
+class HcCmeEvent(C.Structure):
+    """Mirror of hc_cme_event in include/hc_abi.h."""
+    _fields_ = [("insertion_time", C.c_double), ("feeding_end", C.c_double), ("boundary", C.c_int),
+                ("reserved", C.c_int)]
+
+
 class HcCone(C.Structure):
     """Mirror of hc_cone in include/hc_abi.h."""
     _fields_ = [("axis", C.c_double * 3)] + [(n, C.c_double) for n in CONE_FIELDS] + [("reserved", C.c_double * 6)]
@@ -103,6 +109,7 @@ def lib() -> C.CDLL:
         L.orc_cone_prepare.argtypes = [C.POINTER(HcConeSpec), C.c_double, C.POINTER(HcCone)]
         L.orc_cone_cell.argtypes = [C.POINTER(HcCone), C.c_double, _D, _D, C.c_double, _D]
         L.orc_level_insert_cone.argtypes = [C.c_void_p, C.POINTER(HcCone), C.c_double, _D, _D]
+        L.orc_cme_schedule.argtypes = [C.POINTER(HcCmeEvent), C.c_int, C.c_double, C.c_double, _D]
         L.orc_o4_level_create.restype = C.c_void_p
         L.orc_o4_level_create.argtypes = [C.c_void_p]
         L.orc_o4_level_destroy.argtypes = [C.c_void_p]
@@ -136,6 +143,7 @@ def ref_lib() -> C.CDLL | None:
         L.ref_usable_primitive.argtypes = [_D, C.c_double]
         L.ref_cone_prepare.argtypes = [_D, C.c_double, _D]
         L.ref_cone_cell.argtypes = [_D, C.c_double, C.c_double, _D, _D, C.c_double, _D]
+        L.ref_cme_schedule.argtypes = [_D, _D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _D]
         _ref = L
     return _ref
 
@@ -402,3 +410,21 @@ def amr_reflux(fine_flux, fine_lo, coarse_flux, coarse_lo, rhs, rhs_lo, lo, hi, 
                     cell[d] -= 1
                 idx = (slice(None), cell[2] - rhs_lo[2], cell[1] - rhs_lo[1], cell[0] - rhs_lo[0])
                 rhs[idx] = rhs[idx] + coef * diff
+
+
+def cme_schedule(events, time: float, feeding: float) -> tuple[float, float]:
+    """(CFL fraction, Rusanov window end) of the oracle's schedule."""
+    n = len(events)
+    arr = (HcCmeEvent * max(n, 1))(*events)
+    out = np.zeros(2)
+    lib().orc_cme_schedule(arr, n, time, feeding, dptr(out))
+    return float(out[0]), float(out[1])
+
+
+def ref_cme_schedule(times, cloud_end, inserted: int, time: float, target: float, feeding: float):
+    """The reference's CMEInsertionSchedule (finite cone sources)."""
+    t = np.ascontiguousarray(times, dtype=np.float64)
+    e = np.ascontiguousarray(cloud_end, dtype=np.float64)
+    out = np.zeros(2)
+    ref_lib().ref_cme_schedule(dptr(t), dptr(e), len(t), inserted, time, target, feeding, dptr(out))
+    return float(out[0]), float(out[1])

@@ -146,4 +146,22 @@ int ref_cone_cell(const double* spec, double innerRsun, double time, const doubl
   for (int q = 0; q < 8; ++q) delta[q] = change[q];
   return 1;
 }
+
+// CMEInsertionSchedule of finite cone sources (field model 4) inserted at
+// times[i] whose clouds end at cloud_end[i]; the first `inserted` are marked
+// inserted.  out: cfl(time, target, feeding), rusanovEndTime().
+void ref_cme_schedule(const double* times, const double* cloud_end, int n, int inserted, double time, double target,
+                      double feeding, double* out) {
+  std::vector<CMEParameters> sources(n);
+  for (int i = 0; i < n; ++i) {
+    sources[i].fieldModel = 4;
+    sources[i].injectionMethod = 0;
+    sources[i].insertionTime = times[i];
+    sources[i].cloudEndTime = cloud_end[i];
+  }
+  CMEInsertionSchedule sched(sources);
+  for (int i = 0; i < inserted; ++i) sched.markInserted();
+  out[0] = sched.cfl(time, target, feeding);
+  out[1] = sched.rusanovEndTime();
+}
 }

@@ -143,3 +143,76 @@ def test_o4_step_with_cloud_matches_oracle(oracle_lib):
     assert shell.valid(g)
     err = rel_err_components(g.cpu().numpy().reshape(6, 8, -1), ju.reshape(6, 8, -1))
     assert err.max() < 1e-12, err
+
+
+def _volume_event(t):
+    from heliocubed_b200 import _native as N
+    ev = N.HcCmeEvent()
+    ev.insertion_time, ev.feeding_end, ev.boundary = t, t, 0
+    return ev
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_schedule_scales_the_cfl_step(oracle_lib, order):
+    """With a schedule, every hc_level_advance_cfl step's dt is CFL /
+    (rate / fraction(time)) for the rate of the step's initial state, the
+    fraction from the oracle's restatement of the reference schedule
+    (1e-14), and a fourth-order Roe context's steps land on the Rusanov
+    window's end."""
+    _need_gpu()
+    po = oracle_lib
+    n = 16
+    kw = dict(nr=n, na=n, spatial_order=order, riemann_solver=2 if order == 4 else 1)
+    sh = hc.Shell(hc.Params(**kw))
+    ju = sh.init(hc.InitSpec())
+    t0 = 1000.0
+    ev = [_volume_event(t0 - 500.0), _volume_event(t0 + 300.0)]
+    sh.set_cme_schedule(ev)
+    oev = []
+    for e in ev:
+        o = po.HcCmeEvent()
+        o.insertion_time, o.feeding_end, o.boundary = e.insertion_time, e.feeding_end, e.boundary
+        oev.append(o)
+    time = torch.full((1,), t0, dtype=torch.float64, device="cuda")
+    dt = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ends = []
+    for _ in range(6):
+        rate = float(sh.inv_dt_max(ju).item())
+        t = float(time.item())
+        frac, end = po.cme_schedule(oev, t, 0.5 if order == 4 else 1.0)
+        sh.advance(ju, 1, time, dt)
+        expect = 0.4 / (rate / frac)
+        if order == 4 and t < end - 1e-9 * max(1.0, abs(end)):
+            expect = 0.4 / max(rate / frac, 0.4 / (end - t))
+            ends.append(end)
+        assert float(dt.item()) == pytest.approx(expect, rel=1e-14)
+    assert sh.valid(ju)
+    if order == 4:
+        assert ends, "the steps never entered the Rusanov window"
+
+
+def test_rusanov_window_runs_the_rusanov_operator():
+    """Inside the window a fourth-order Roe context's step equals, bit for
+    bit, the same step of a Rusanov context with the same schedule."""
+    _need_gpu()
+    n = 16
+    roe = hc.Shell(hc.Params(nr=n, na=n, spatial_order=4, riemann_solver=2))
+    rus = hc.Shell(hc.Params(nr=n, na=n, spatial_order=4, riemann_solver=1))
+    ju0 = roe.init(hc.InitSpec())
+    for sh in (roe, rus):
+        sh.set_cme_schedule([_volume_event(0.0)])
+    a, b = ju0.clone(), ju0.clone()
+    ta = torch.zeros(1, dtype=torch.float64, device="cuda")
+    tb = torch.zeros(1, dtype=torch.float64, device="cuda")
+    roe.advance(a, 1, ta)
+    rus.advance(b, 1, tb)
+    torch.cuda.synchronize()
+    assert float(ta.item()) < 600.0          # still inside the window
+    assert torch.equal(ta, tb)
+    assert torch.equal(a, b)
+    # without a schedule the Roe context differs
+    roe.set_cme_schedule([])
+    c = ju0.clone()
+    tc = torch.zeros(1, dtype=torch.float64, device="cuda")
+    roe.advance(c, 1, tc)
+    assert not torch.equal(c, a)

@@ -10,6 +10,8 @@
   cells inside take the cloud's density, radial speed and pressure
   2 k T rho / m_p with their field kept, and the mass statistic is the
   summed change of the density averages.
+* The insertion schedule (CFL fraction, Rusanov window end) equals the
+  reference's CMEInsertionSchedule bit for bit.
 """
 from __future__ import annotations
 
@@ -195,3 +197,50 @@ def test_level_insertion_properties():
     again = ju.copy()
     orc.insert_cone(cone, cone.insertion_time, again)
     assert np.abs(again - ju).max() <= 1e-13 * np.abs(ju).max()
+
+
+def _events(times, ends):
+    out = []
+    for t, e in zip(times, ends):
+        ev = po.HcCmeEvent()
+        ev.insertion_time = t
+        ev.boundary = 1 if e > t else 0
+        ev.feeding_end = max(t, e)
+        out.append(ev)
+    return out
+
+
+@pytest.mark.parametrize("feeding", [0.5, 1.0])
+def test_cme_schedule_matches_reference(feeding):
+    """The oracle's CFL fraction and Rusanov window end equal the reference's
+    CMEInsertionSchedule (compiled from src/MHD_CME.H) bit for bit: volume
+    and boundary sources, before, inside and after their windows."""
+    _need_ref()
+    rng = np.random.default_rng(int(feeding * 10))
+    for _ in range(30):
+        n = int(rng.integers(1, 5))
+        times = np.sort(rng.uniform(0, 2e4, n))
+        ends = times + np.where(rng.random(n) < 0.5, rng.uniform(-500, 0, n), rng.uniform(10, 5000, n))
+        events = _events(times, ends)
+        for time in rng.uniform(-100, 3e4, 12):
+            inserted = int((times <= time).sum())
+            ref = po.ref_cme_schedule(times, ends, inserted, time, 1.0, feeding)
+            got = po.cme_schedule(events, time, feeding)
+            assert got[0] == ref[0], (time, got, ref)
+            if inserted:
+                assert got[1] == ref[1]
+
+
+def test_library_cone_event_matches_schedule_rule():
+    """hc_cone_event marks a cone as a boundary source exactly when its
+    cloud ends after insertion (src/MHD_CME.H:1251-1253)."""
+    import heliocubed_b200 as hc
+    from heliocubed_b200 import _native as N
+    lib = N.lib()
+    for spec in (hc.ConeSpec.on_inner_boundary(INNER, half_angle_deg=30.0),
+                 hc.ConeSpec(reference_height=21.5, half_angle_deg=30.0, apex_speed=1000.0)):
+        cone = hc.prepare_cone(spec, INNER)
+        ev = N.HcCmeEvent()
+        assert lib.hc_cone_event(C.byref(cone), C.byref(ev)) == 0
+        assert ev.boundary == (1 if cone.end_time > cone.insertion_time else 0)
+        assert ev.feeding_end == max(cone.insertion_time, cone.end_time)

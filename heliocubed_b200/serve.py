@@ -87,24 +87,26 @@ class Request:
         return Params(nr=self.nr, na=self.na, spatial_order=2, limiter=3, riemann_solver=1, autotune=1)
 
 
-def admit(shell: Shell, req: Request, ju: torch.Tensor, time_dev: torch.Tensor) -> None:
+def admit(shell: Shell, req: Request, ju: torch.Tensor, time_dev: torch.Tensor, schedule: bool = True) -> None:
     """Device-side admission on the current stream: the wind into `ju`, the
     request's cone cloud inserted at its insertion time, the model time set
     to that time, and the insertion schedule (CFL ramp, and the Rusanov
     window of fourth-order Roe solves) that the reference's driver applies
-    after an insertion."""
+    after an insertion (schedule=False: the state only)."""
     shell.init(wind_spec(), ju)
     cone = req.cone.prepared(shell.params)
     shell.insert_cone(cone, cone.insertion_time, ju)
-    shell.set_cme_schedule([cone])
+    if schedule:
+        shell.set_cme_schedule([cone])
     time_dev.fill_(cone.insertion_time)
 
 
 def initial_state(shell: Shell, req: Request) -> np.ndarray:
-    """Host copy of the state `admit` builds (for checks and reports)."""
+    """Host copy of the state `admit` builds (for checks and reports); the
+    shell's insertion schedule is left as it was."""
     ju = shell.new_state()
     t = torch.zeros(1, dtype=torch.float64, device=ju.device)
-    admit(shell, req, ju, t)
+    admit(shell, req, ju, t, schedule=False)
     return ju.cpu().numpy()
 
 

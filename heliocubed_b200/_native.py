@@ -55,6 +55,7 @@ SIGNATURES = {
     "hc_level_insert_cone": (C.c_int, [_VP, _VP, C.c_double, _VP, _VP, _VP]),
     "hc_cone_event": (C.c_int, [_VP, _VP]),
     "hc_level_set_cme_schedule": (C.c_int, [_VP, _VP, C.c_int, _VP]),
+    "hc_level_set_inlet": (C.c_int, [_VP, _VP, C.c_int, _VP]),
 }
 
 

@@ -7,6 +7,7 @@ namespace hc {
 constexpr int NC = 8;
 // src/BoxOp_EulerCubedSphere.H:36 and src/MHD_Constants.H:4-7
 constexpr double kMP = 1.67262192e-24;
+constexpr double kSolarRadiusCm = 69600000000.0;  // c_SR, src/MHD_Constants.H:4
 constexpr double kRHO00 = 1.67262192e-24 / 100.;
 constexpr double kGrav = 6.67430e-8;
 constexpr double kMsun = 1.98847e33;

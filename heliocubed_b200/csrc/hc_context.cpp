@@ -252,8 +252,10 @@ struct hc_ctx {
   int o4var[kO4TunedKernels] = {0, 0, 0};
   // CME insertion schedule (device) and the Rusanov-window flag it sets
   CmeSchedule* sched = nullptr;
+  CmeSchedule schedHost{};
   int* rusanovFlag = nullptr;
   int schedEvents = 0;
+  InletCone* inletDev = nullptr;  // cones fed through the inner boundary (device, kInletCones)
   bool tuned = false;
   // fourth-order operator: metric tables and grow-only scratch
   O4Geo o4{};
@@ -836,6 +838,8 @@ int rkStep(hc_ctx* c, double* ju, double dtv, const double* invMax, unsigned lon
     a.wOut = c->W[(stage + 1) % 2];
     a.invMaxOut = stage == 3 ? invMaxOut : nullptr;
     a.invalid = nullptr;
+    a.tbase = tbase;
+    a.tdev = tdev;
     rc = checkLaunch(launchStage(a, MODE_RK, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
                                  c->P.sun_gravity == 1, s, c->tileRK),
                      "stage");
@@ -1459,7 +1463,7 @@ int hc_level_set_cme_schedule(hc_ctx* c, const hc_cme_event* events, int n, void
   for (int i = 1; i < n; ++i)
     if (events[i].insertion_time < events[i - 1].insertion_time)
       return fail(HC_ERR_ARG, "CME events must be ordered by insertion time");
-  CmeSchedule h{};
+  CmeSchedule& h = c->schedHost;
   h.n = n;
   h.roe = c->P.riemann_solver == 2 && c->P.spatial_order == 4 ? 1 : 0;
   h.cfl = c->P.cfl;
@@ -1483,6 +1487,61 @@ int hc_level_set_cme_schedule(hc_ctx* c, const hc_cme_event* events, int n, void
   if (err == cudaSuccess && n == 0 && c->rusanovFlag) err = cudaMemsetAsync(c->rusanovFlag, 0, sizeof(int), s);
   if (err != cudaSuccess) return cudaFail(err, "CME schedule");
   c->schedEvents = n;
+  return HC_OK;
+}
+
+int hc_level_set_inlet(hc_ctx* c, const hc_cone* cones, int n, void* stream) {
+  if (!c || (n && !cones)) return fail(HC_ERR_ARG, "null argument");
+  if (n < 0 || n > kInletCones) return fail(HC_ERR_ARG, "at most 8 inlet cones");
+  if (n && c->P.spatial_order != 2) return fail(HC_ERR_UNSUPPORTED, "the boundary inlet is built for order-2 contexts");
+  if (n && c->P.init_condition_type != 1) return fail(HC_ERR_UNSUPPORTED, "the inlet needs the analytic-wind inner boundary");
+  InletCone h[kInletCones] = {};
+  for (int i = 0; i < n; ++i) {
+    const hc_cone& k = cones[i];
+    if (!(k.radius > 0) || !(k.speed > 0) || !(k.density > 0) || !(k.temperature >= 0))
+      return fail(HC_ERR_ARG, "inlet cone not prepared (radius, speed, density, temperature)");
+    for (int d = 0; d < 3; ++d) h[i].axis[d] = k.axis[d];
+    h[i].radius = k.radius;
+    h[i].entryShift = k.entry_shift;
+    h[i].entryTime = k.entry_time;
+    h[i].speed = k.speed;
+    h[i].endTime = k.end_time;
+    h[i].insertionTime = k.insertion_time;
+    h[i].density = k.density;
+    h[i].temperature = k.temperature;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t err = cudaSuccess;
+  if (!c->inletDev) {
+    err = cudaMalloc(&c->inletDev, sizeof(InletCone) * kInletCones);
+    if (err != cudaSuccess) return cudaFail(err, "inlet");
+    c->owned.push_back(c->inletDev);
+  }
+  if (!c->sched) {
+    err = cudaMalloc(&c->sched, sizeof(CmeSchedule));
+    if (err != cudaSuccess) return cudaFail(err, "inlet schedule");
+    c->owned.push_back(c->sched);
+    c->schedHost = CmeSchedule{};
+    c->schedHost.cfl = c->P.cfl;
+    c->schedHost.feeding = c->P.riemann_solver == 2 ? .5 : 1.;
+  }
+  err = cudaMemcpyAsync(c->inletDev, h, sizeof h, cudaMemcpyHostToDevice, s);
+  // the clouds' crossing rate in the step's CFL rate (exec/main.cpp:365-383)
+  CmeSchedule& S = c->schedHost;
+  S.ninlet = n;
+  for (int i = 0; i < n; ++i) {
+    S.inletT[i] = cones[i].insertion_time;
+    S.inletEnd[i] = cones[i].end_time;
+    S.inletSpeed[i] = cones[i].speed;
+    S.inletTemp[i] = cones[i].temperature;
+  }
+  const double C = c->P.radial_stretch, span = c->P.outer_radius - c->P.inner_radius;
+  S.width = span * (C == 0 ? 1. / c->P.nr : std::expm1(C / c->P.nr) / std::expm1(C));
+  S.gamma = c->P.gamma;
+  if (err == cudaSuccess) err = cudaMemcpyAsync(c->sched, &S, sizeof S, cudaMemcpyHostToDevice, s);
+  if (err != cudaSuccess) return cudaFail(err, "inlet");
+  c->L.inlet = n ? c->inletDev : nullptr;
+  c->L.ninlet = n;
   return HC_OK;
 }
 

@@ -58,6 +58,75 @@ __device__ __forceinline__ void nativeToPrimitive(const double u[8], const doubl
   cartesianPrimitiveFromConserved(out, ww, 1.0, gamma);
 }
 
+// Inlet of the cone clouds crossing the inner boundary at time t into the
+// native conserved ghost state u at Cartesian position pos
+// (src/BoxOp_PreStage.H:329-400, finite clouds: the inlet state is sampled on
+// the physical boundary sphere; taper weight 1).  A: cell basis, Ai: its
+// inverse.
+__device__ void inletGhost(const DevLevel& L, double t, const double pos[3], const double* A, const double* Ai,
+                           double u[8]) {
+  const double radius = sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]);
+  for (int s = 0; s < L.ninlet; ++s) {
+    const InletCone c = L.inlet[s];
+    if (!(t >= c.insertionTime && t < c.endTime)) continue;
+    const double shift = c.entryShift + c.speed * 1e5 * (t - c.entryTime);
+    const double face[3] = {pos[0] * L.r0 / radius, pos[1] * L.r0 / radius, pos[2] * L.r0 / radius};
+    const double q0 = face[0] - shift * c.axis[0], q1 = face[1] - shift * c.axis[1], q2 = face[2] - shift * c.axis[2];
+    if (sqrt(q0 * q0 + q1 * q1 + q2 * q2) > c.radius) continue;
+    const double fr = sqrt(face[0] * face[0] + face[1] * face[1] + face[2] * face[2]) / kSolarRadiusCm;
+    if (!(fr > 0)) continue;
+    double v[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v[d] = c.speed * 1e5 * face[d] / (kSolarRadiusCm * fr);
+    double old[8] = {u[0], 0, 0, 0, 0, 0, 0, 0};
+    double ke = 0, me = 0, radialOld = 0, radialCME = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        old[1 + d] += A[3 * d + q] * u[1 + q] / old[0];
+        old[5 + d] += A[3 * d + q] * u[5 + q];
+      }
+      ke += .5 * old[0] * old[1 + d] * old[1 + d];
+      me += old[5 + d] * old[5 + d] / (8 * kPi);
+      radialOld += old[1 + d] * pos[d] / radius;
+      radialCME += v[d] * pos[d] / radius;
+    }
+    old[4] = fmax(0., (u[4] - ke - me) * (L.gamma - 1));
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v[d] = radialCME * pos[d] / radius;
+    // taperBoundarySource with weight 1, then increment() with the
+    // prescribed cone plasma (src/MHD_CME.H:982-990, 1215-1238)
+    const double weight = 1;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v[d] = old[1 + d] + weight * (v[d] - old[1 + d]);
+    const double density = (1 - weight) * old[0] + weight * c.density;
+    double oldKinetic = 0, newKinetic = 0, oldMagnetic = 0, newMagnetic = 0, delta[8];
+    delta[0] = density - old[0];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      delta[1 + d] = density * v[d] - old[0] * old[1 + d];
+      delta[5 + d] = 0.0;
+      oldKinetic += .5 * old[0] * old[1 + d] * old[1 + d];
+      newKinetic += .5 * density * v[d] * v[d];
+      oldMagnetic += old[5 + d] * old[5 + d] / (8 * kPi);
+      newMagnetic += (old[5 + d] + 0.0) * (old[5 + d] + 0.0) / (8 * kPi);
+    }
+    const double target = 2 * 1.380649e-16 * c.temperature * c.density / kMP;
+    const double pressure = (1 - weight) * fmax(0., old[4]) + weight * target;
+    delta[4] = (pressure - fmax(0., old[4])) / (L.gamma - 1) + newKinetic - oldKinetic + newMagnetic - oldMagnetic;
+    u[0] += delta[0];
+    u[4] += delta[4];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        u[1 + d] += Ai[3 * d + q] * delta[1 + q];
+        u[5 + d] += Ai[3 * d + q] * delta[5 + q];
+      }
+  }
+}
+
 // Analytic inner wind, src/BoxOp_PreStage.H:7-47 (time-dependent form).
 __device__ void analyticWind(const DevLevel& L, const double X[3], double t, double u[8]) {
   windConserved(L.gamma, L.r0, L.strength, X, t, u);
@@ -132,6 +201,46 @@ __device__ __forceinline__ void o2Face(const StageArgs& a, const double* __restr
     }
   }
   const FaceGeom& g = L.face[((size_t)dir * 6 + block) * (L.na + 1) * (L.na + 1) + (size_t)k * (L.na + 1) + j];
+  if (MODE == MODE_RK && dir == 0 && i == 0 && L.ninlet) {
+    // Inlet footprint on the inner face (src/BoxOp_SecondOrder.H:175-181,
+    // 282-311): where an emerging cloud covers the face, the interior state
+    // is extrapolated from owned cells only and the ghost side takes the
+    // interior's normal field.
+    const double dtS = a.invDtMax ? L.cfl_number / *a.invDtMax : a.dtv;
+    constexpr double c4[4] = {0, 0.5, 0.5, 1};
+    const double t = a.tbase + (a.tdev ? *a.tdev : 0.0) + c4[a.stage] * dtS;
+    bool footprint = false;
+    for (int s = 0; s < L.ninlet && !footprint; ++s) {
+      const InletCone c = L.inlet[s];
+      if (!(t >= c.insertionTime && t < c.endTime)) continue;
+      const double shift = c.entryShift + c.speed * 1e5 * (t - c.entryTime);
+      const double pos[3] = {L.r0 * g.f[0], L.r0 * g.f[1], L.r0 * g.f[2]};
+      const double q0 = pos[0] - shift * c.axis[0], q1 = pos[1] - shift * c.axis[1], q2 = pos[2] - shift * c.axis[2];
+      if (sqrt(q0 * q0 + q1 * q1 + q2 * q2) > c.radius) continue;
+      footprint = sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]) / kSolarRadiusCm > 0;
+    }
+    if (footprint) {
+#pragma unroll
+      for (int q = 0; q < NC; ++q) {
+        const double cc = __ldg(w + q * sN + c0), pp = __ldg(w + q * sN + c0 + step),
+                     qq = __ldg(w + q * sN + c0 + 2 * step);
+        const double da = pp - cc, db = qq - pp;
+        double slope = 0.5 * (da + db);
+        if (LIM != 0) slope = da * db <= 0 ? 0.0 : (da > 0 ? fmin(da, db) : fmax(da, db));
+        if (LIM == 3 && da * db > 0) slope = (da > 0 ? 1.0 : -1.0) * fmin(0.5 * fabs(da + db), 2.0 * fmin(fabs(da), fabs(db)));
+        r[q] = cc - 0.5 * slope;
+      }
+      if (!(r[0] >= kRHO00 && r[4] > 0)) {
+#pragma unroll
+        for (int q = 0; q < NC; ++q) r[q] = __ldg(w + q * sN + c0);
+      }
+      double jump = 0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) jump += (r[5 + d] - l[5 + d]) * g.f[d];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) l[5 + d] += jump * g.f[d];
+    }
+  }
   const double4 rd = L.radial[i + L.g];
   const double area = dir == 0 ? rd.x : rd.y;
   secondOrderFaceFlux<ROE>(out, l, r, g, area, L.gamma, L.invGm1, L.entropy);
@@ -429,17 +538,19 @@ __global__ void ghostsKernel(const DevLevel L, double* __restrict__ w, const Sta
       if (L.innerBCType == 1) {
         for (int i = -L.g; i < 0; ++i) {
           double u[8], out[8];
+          const bool need = !L.innerBC || L.ninlet;
+          const double dt = need ? (st.invDtMax ? L.cfl_number / *st.invDtMax : st.dtv) : 0.0;
+          const double time = need ? st.tbase + (st.tdev ? *st.tdev : 0.0) + st.cfrac * dt : 0.0;
+          const GravCell gc = L.grav[cidx];
+          const double radius = L.rc[i + L.g];
+          const double X[3] = {radius * gc.x[0], radius * gc.x[1], radius * gc.x[2]};
           if (L.innerBC) {
 #pragma unroll
             for (int c = 0; c < NC; ++c) u[c] = L.innerBC[(cidx * L.g + (i + L.g)) * NC + c];
           } else {
-            const double dt = st.invDtMax ? L.cfl_number / *st.invDtMax : st.dtv;
-            const double time = st.tbase + (st.tdev ? *st.tdev : 0.0) + st.cfrac * dt;
-            const GravCell gc = L.grav[cidx];
-            const double radius = L.rc[i + L.g];
-            const double X[3] = {radius * gc.x[0], radius * gc.x[1], radius * gc.x[2]};
             analyticWind(L, X, time, u);
           }
+          if (L.ninlet) inletGhost(L, time, X, A, L.basisInv + cidx * 9, u);
           nativeToPrimitive(u, A, L.gamma, out);
           const long o = gIdx(L, b, i, j, k);
 #pragma unroll
@@ -596,7 +707,12 @@ __global__ void cmeScheduleKernel(const CmeSchedule* S, unsigned long long* invM
     end = fmax(end, S->stabEnd[i]);
   }
   const bool window = S->roe && t < end - 1e-9 * fmax(1.0, fabs(end));
-  double rate = __longlong_as_double((long long)*invMaxBits) / fraction;
+  double rate = __longlong_as_double((long long)*invMaxBits);
+  // boundaryCFLRate (src/MHD_CME.H:1165-1191) for clouds still crossing r_inner
+  for (int i = 0; i < S->ninlet; ++i)
+    if (t >= S->inletT[i] && t < S->inletEnd[i])
+      rate += (S->inletSpeed[i] * 1e5 + sqrt(S->gamma * 2 * 1.380649e-16 * S->inletTemp[i] / kMP)) / S->width;
+  rate = rate / fraction;
   if (window) rate = fmax(rate, S->cfl / (end - t));
   *invMaxBits = (unsigned long long)__double_as_longlong(rate);
   if (rusanov) *rusanov = window ? 1 : 0;

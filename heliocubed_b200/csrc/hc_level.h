@@ -47,6 +47,14 @@ struct GravCell {
   double pad;
 };
 
+// A cone cloud fed through the inner boundary while it crosses it (the
+// finite cloud of hc_cone, src/MHD_CME.H:968,1111-1143).
+struct InletCone {
+  double axis[3];
+  double radius, entryShift, entryTime, speed, endTime, insertionTime, density, temperature;
+};
+constexpr int kInletCones = 8;
+
 struct DevLevel {
   int nr, na, g;
   int n0, n1;            // ghosted dims nr+2g, na+2g
@@ -66,6 +74,8 @@ struct DevLevel {
   double outerScale2[kGhost], outerScale1[kGhost];
   double gamma, invGm1, entropy, cfl_number, strength, r0;
   int innerBCType;
+  const InletCone* inlet;  // device array of cones fed through r_inner, or null
+  int ninlet;
 };
 
 // Operator launch: boxes share the valid region [lo,hi]; box b lies on panel
@@ -97,6 +107,10 @@ struct StageArgs {
   double* wOut;
   unsigned long long* invMaxOut;
   int* invalid;            // OR-ed validity flag of the new state (stage 3)
+  // time of the step's start (MODE_RK): tbase + *tdev; the stage adds
+  // c_s dt.  Only the inlet footprint of the inner face reads it.
+  double tbase;
+  const double* tdev;
 };
 
 enum { MODE_BOX = 0, MODE_RK = 1, MODE_RHS = 2 };
@@ -136,6 +150,11 @@ struct CmeSchedule {
   double cfl, feeding;  // target CFL; feeding fraction (0.5 with Roe, 1 with Rusanov, exec/main.cpp:374)
   double t[kCmeEvents], stabEnd[kCmeEvents];
   int boundary[kCmeEvents];
+  // the inlet clouds' crossing rate (src/MHD_CME.H:1165-1191, finite
+  // clouds): + (speed + sound speed of the cloud) / first radial cell width
+  int ninlet;
+  double inletT[kInletCones], inletEnd[kInletCones], inletSpeed[kInletCones], inletTemp[kInletCones];
+  double width, gamma;
 };
 // At the start of a step: the CFL rate in *invMaxBits (a non-negative double's
 // bits) becomes rate / fraction(time), and no smaller than cfl / (window end

@@ -126,6 +126,7 @@ extern "C" int hc_level_rk4_step_noalloc(hc_ctx* ctx, double* ju, double dt, dou
     a.wOut = W[(stage + 1) % 2];
     a.invMaxOut = nullptr;
     a.invalid = nullptr;
+    a.tbase = t;
     rc = launched(launchStage(a, MODE_RK, P.limiter, P.riemann_solver == 2, P.divergence_cleaning == 1,
                               P.sun_gravity == 1, s),
                   "stage");

@@ -352,6 +352,13 @@ class Shell:
                 arr[i] = e
         N.check(self._lib.hc_level_set_cme_schedule(self._ctx, arr, n, _stream()), "hc_level_set_cme_schedule")
 
+    def set_inlet(self, cones) -> None:
+        """hc_level_set_inlet: prepared cones fed through the inner boundary
+        while they cross it (order 2)."""
+        n = len(cones)
+        arr = (N.HcCone * max(n, 1))(*cones)
+        N.check(self._lib.hc_level_set_inlet(self._ctx, arr, n, _stream()), "hc_level_set_inlet")
+
     def autotune(self, ju: torch.Tensor) -> tuple[tuple[int, ...], np.ndarray]:
         """hc_ctx_autotune with the state `ju` (not modified).  Order 2:
         ((RK stage tile, operator tile), median ms [2][tiles]).  Order 4:

@@ -457,6 +457,22 @@ int hc_cone_event(const hc_cone* cone, hc_cme_event* event);
  * schedules. */
 int hc_level_set_cme_schedule(hc_ctx* ctx, const hc_cme_event* events, int n, void* stream);
 
+/* Feed prepared cone clouds through the inner boundary of an order-2 level
+ * while they cross it (insertion_time <= t < end_time; the reference's
+ * boundary source of a finite cloud).  Each stage's inner radial ghosts
+ * whose point on the boundary sphere lies in a cloud take the cloud's
+ * density, radial speed and pressure over the analytic wind, keeping its
+ * field (src/BoxOp_PreStage.H:329-400).  In hc_level_rk4_step and
+ * hc_level_advance_cfl the inner faces such a cloud covers take their
+ * interior state from owned cells only and share that state's normal field
+ * (src/BoxOp_SecondOrder.H:175-181, 282-311); hc_level_rhs and hc_box_rhs,
+ * which take no time, do not.  hc_level_advance_cfl adds each crossing
+ * cloud's (speed + sound speed) / first radial cell width to the step's
+ * CFL rate (src/MHD_CME.H:1165-1191).  At most 8 cones; n = 0 stops the
+ * inlet.  The cones are copied on `stream`; launches captured in a graph
+ * keep the inlet set when they were captured. */
+int hc_level_set_inlet(hc_ctx* ctx, const hc_cone* cones, int n, void* stream);
+
 /* Host copies of the level geometry used by the kernels, for tests:
  * what = 0 radial line [nr+1][4]: rlow^2, (rhigh^2-rlow^2)/(2dxi0),
  *          (rhigh-rlow)/dxi0, dVolr (last row: face only)

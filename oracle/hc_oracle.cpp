@@ -529,6 +529,11 @@ struct Level {
   struct SeamFace { int b, axis, side; std::vector<int> s; };
   SeamFace edges[6][2][2];
 
+  // cone clouds fed through the inner boundary (hc_level_set_inlet) and the
+  // operator's time (the stage time of levelRk4; NaN: no time, no footprint)
+  std::vector<hc_cone> inlet;
+  mutable double opTime = std::numeric_limits<double>::quiet_NaN();
+
   explicit Level(const hc_params& p) : P(p), nr(p.nr), na(p.na), g(2) {
     h = 1.0 / na;
     radial.resize(nr + 2 * g + 1);
@@ -688,6 +693,20 @@ struct LevelArrays {
 // face mask, no CME emergence and no constant-background magnetic test.
 // w is on valid.grow(ghost); rhs on valid; flux[d] on valid.extrude(d).
 // ---------------------------------------------------------------------------
+// A finite cone cloud at time t (expandedSource + sample, src/MHD_CME.H:
+// 995-1018, 1139-1143) while its boundary feeding lasts (:968): inside
+// flag and, when inside, the radial cloud velocity at `pos`.
+bool inletSample(const hc_cone& c, double t, const double pos[3], double v[3]) {
+  if (!(t >= c.insertion_time && t < c.end_time)) return false;
+  const double shift = c.entry_shift + c.speed * 1e5 * (t - c.entry_time);
+  const double q[3] = {pos[0] - shift * c.axis[0], pos[1] - shift * c.axis[1], pos[2] - shift * c.axis[2]};
+  if (std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) > c.radius) return false;
+  const double radius = std::sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]) / 69600000000.0;
+  if (!(radius > 0)) return false;
+  for (int d = 0; d < 3; ++d) v[d] = c.speed * 1e5 * pos[d] / (69600000000.0 * radius);
+  return true;
+}
+
 void boxOperator(const Level& L, const int lo[3], const int hi[3], int ghost, int block,
                  const double* w, const double* const* panel, double scale, double* rhs,
                  double* const* fluxOut) {
@@ -730,6 +749,31 @@ void boxOperator(const Level& L, const int lo[3], const int hi[3], int ghost, in
           int fp[3] = {i, j, k};
           if (pLow && fp[dir] == flo[dir]) for (int q = 0; q < NC; ++q) l[q] = pLow[q * SL.N + SL(i, j, k)];
           if (pHigh && fp[dir] == fhi[dir]) for (int q = 0; q < NC; ++q) r[q] = pHigh[q * SH.N + SH(i, j, k)];
+          if (dir == 0 && i == 0 && !L.inlet.empty() && !std::isnan(L.opTime)) {
+            // inlet footprint, src/BoxOp_SecondOrder.H:175-181, 282-311
+            const double pos[3] = {P.inner_radius * fr.f[0][0], P.inner_radius * fr.f[0][1], P.inner_radius * fr.f[0][2]};
+            bool footprint = false;
+            for (const hc_cone& cone : L.inlet) {
+              double v[3];
+              if (inletSample(cone, L.opTime, pos, v)) { footprint = true; break; }
+            }
+            if (footprint) {
+              for (int q = 0; q < NC; ++q) {
+                const double* s = w + q * W.N + c0;
+                const double a = s[step] - s[0], b = s[2 * step] - s[step];
+                double slope = 0.5 * (a + b);
+                if (limiter != 0) slope = a * b <= 0 ? 0.0 : (a > 0 ? std::min(a, b) : std::max(a, b));
+                if (limiter == 3 && a * b > 0)
+                  slope = (a > 0 ? 1.0 : -1.0) * std::min(0.5 * std::fabs(a + b), 2.0 * std::min(std::fabs(a), std::fabs(b)));
+                r[q] = s[0] - 0.5 * slope;
+              }
+              if (!(r[iRHO] >= RHO00 && r[iP] > 0))
+                for (int q = 0; q < NC; ++q) r[q] = w[q * W.N + c0];
+              double jump = 0;
+              for (int d = 0; d < 3; ++d) jump += (r[5 + d] - l[5 + d]) * fr.f[0][d];
+              for (int d = 0; d < 3; ++d) l[5 + d] += jump * fr.f[0][d];
+            }
+          }
           const double area = dir == 0 ? L.rad(i).area0 : L.rad(i).areaT;
           double out[8];
           faceFlux(out, l, r, fr, area, P.gamma, P.entropy_fix_coeff, roe);
@@ -828,6 +872,59 @@ void analyticWind(const hc_params& P, double radius, const double X[3], double t
   (void)radius;
 }
 
+// Inner-ghost inlet of the clouds crossing r_inner, src/BoxOp_PreStage.H:
+// 329-400 (finite clouds: sampled on the boundary sphere, taper weight 1):
+// u native conserved, A the cell basis, inv its inverse, pos the ghost
+// centre.
+void inletGhost(const Level& L, double t, const double pos[3], const double A[3][3], const double inv[3][3],
+                double u[8]) {
+  const hc_params& P = L.P;
+  const double radius = std::sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]);
+  const double inner = P.inner_radius;
+  for (const hc_cone& c : L.inlet) {
+    double v[3];
+    const double face[3] = {pos[0] * inner / radius, pos[1] * inner / radius, pos[2] * inner / radius};
+    if (!inletSample(c, t, face, v)) continue;
+    double old[8] = {u[0], 0, 0, 0, 0, 0, 0, 0};
+    double ke = 0, me = 0, radialOld = 0, radialCME = 0;
+    for (int d = 0; d < 3; ++d) {
+      for (int q = 0; q < 3; ++q) {
+        old[1 + d] += A[d][q] * u[1 + q] / old[0];
+        old[5 + d] += A[d][q] * u[5 + q];
+      }
+      ke += .5 * old[0] * old[1 + d] * old[1 + d];
+      me += old[5 + d] * old[5 + d] / (8 * M_PI);
+      radialOld += old[1 + d] * pos[d] / radius;
+      radialCME += v[d] * pos[d] / radius;
+    }
+    old[4] = std::max(0., (u[4] - ke - me) * (P.gamma - 1));
+    for (int d = 0; d < 3; ++d) v[d] = radialCME * pos[d] / radius;
+    const double weight = 1;
+    for (int d = 0; d < 3; ++d) v[d] = old[1 + d] + weight * (v[d] - old[1 + d]);
+    const double density = (1 - weight) * old[0] + weight * c.density;
+    double oldKinetic = 0, newKinetic = 0, oldMagnetic = 0, newMagnetic = 0, delta[8];
+    delta[0] = density - old[0];
+    for (int d = 0; d < 3; ++d) {
+      delta[1 + d] = density * v[d] - old[0] * old[1 + d];
+      delta[5 + d] = 0.0;
+      oldKinetic += .5 * old[0] * old[1 + d] * old[1 + d];
+      newKinetic += .5 * density * v[d] * v[d];
+      oldMagnetic += old[5 + d] * old[5 + d] / (8 * M_PI);
+      newMagnetic += (old[5 + d] + 0.0) * (old[5 + d] + 0.0) / (8 * M_PI);
+    }
+    const double target = 2 * 1.380649e-16 * c.temperature * c.density / c_MP;
+    const double pressure = (1 - weight) * std::max(0., old[4]) + weight * target;
+    delta[4] = (pressure - std::max(0., old[4])) / (P.gamma - 1) + newKinetic - oldKinetic + newMagnetic - oldMagnetic;
+    u[0] += delta[0];
+    u[4] += delta[4];
+    for (int d = 0; d < 3; ++d)
+      for (int q = 0; q < 3; ++q) {
+        u[1 + d] += inv[d][q] * delta[1 + q];
+        u[5 + d] += inv[d][q] * delta[5 + q];
+      }
+  }
+}
+
 void levelPrepare(const Level& L, const double* ju, double* w, double t) {
   const hc_params& P = L.P;
   LevelArrays I(L);
@@ -903,6 +1000,7 @@ void levelPrepare(const Level& L, const double* ju, double* w, double t) {
             double X[3] = {radius * (double)Xl[0], radius * (double)Xl[1], radius * (double)Xl[2]};
             double u[8], out[8];
             analyticWind(P, radius, X, t, u);
+            if (!L.inlet.empty()) inletGhost(L, t, X, A, inv, u);
             toPrim(u, out);
             for (int c = 0; c < NC; ++c) w[I.w(b, c, i, j, k)] = out[c];
           }
@@ -1014,7 +1112,9 @@ void levelRk4(const Level& L, double* ju, double dt, double t) {
       }
     levelPrepare(L, stage.data(), w.data(), t + c4[s] * dt);
     k[s].resize(n);
+    L.opTime = t + c4[s] * dt;
     levelRhs(L, w.data(), k[s].data());
+    L.opTime = std::numeric_limits<double>::quiet_NaN();
   }
   for (int s = 0; s < 4; ++s) {
     const double f = dt * b4[s];
@@ -1372,6 +1472,10 @@ int orc_level_rk4_step(void* L, double* ju, double dt, double t) { levelRk4(*sta
 double orc_level_inv_dt(void* L, const double* ju) { return levelInvDt(*static_cast<Level*>(L), ju); }
 int orc_level_valid(void* L, const double* ju) { return levelValid(*static_cast<Level*>(L), ju); }
 int orc_level_init(void* L, const hc_init* in, double* ju) { levelInit(*static_cast<Level*>(L), *in, ju); return 0; }
+int orc_level_set_inlet(void* L, const hc_cone* cones, int n) {
+  static_cast<Level*>(L)->inlet.assign(cones, cones + n);
+  return 0;
+}
 int orc_cone_prepare(const hc_cone_spec* spec, double inner_radius, hc_cone* out) {
   return conePrepare(*spec, inner_radius, *out);
 }

@@ -110,6 +110,7 @@ def lib() -> C.CDLL:
         L.orc_cone_cell.argtypes = [C.POINTER(HcCone), C.c_double, _D, _D, C.c_double, _D]
         L.orc_level_insert_cone.argtypes = [C.c_void_p, C.POINTER(HcCone), C.c_double, _D, _D]
         L.orc_cme_schedule.argtypes = [C.POINTER(HcCmeEvent), C.c_int, C.c_double, C.c_double, _D]
+        L.orc_level_set_inlet.argtypes = [C.c_void_p, C.POINTER(HcCone), C.c_int]
         L.orc_o4_level_create.restype = C.c_void_p
         L.orc_o4_level_create.argtypes = [C.c_void_p]
         L.orc_o4_level_destroy.argtypes = [C.c_void_p]
@@ -203,6 +204,11 @@ class OracleLevel:
         w = np.zeros(self.ng)
         self.L.orc_level_prepare(self.h, dptr(ju), dptr(w), t)
         return w
+
+    def set_inlet(self, cones) -> None:
+        """Cone clouds fed through the inner boundary while they cross it."""
+        arr = (HcCone * max(len(cones), 1))(*cones)
+        self.L.orc_level_set_inlet(self.h, arr, len(cones))
 
     def insert_cone(self, cone: HcCone, time: float, ju: np.ndarray) -> np.ndarray:
         """Cone volume insertion into ju (in place); returns [cells, grams]."""

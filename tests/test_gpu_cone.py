@@ -216,3 +216,69 @@ def test_rusanov_window_runs_the_rusanov_operator():
     tc = torch.zeros(1, dtype=torch.float64, device="cuda")
     roe.advance(c, 1, tc)
     assert not torch.equal(c, a)
+
+
+def _entering(hcmod):
+    spec = hcmod.ConeSpec(lat_deg=10.0, lon_deg=-20.0, half_angle_deg=40.0, apex_speed=1000.0,
+                          reference_height=21.5, reference_time=0.0, density=4 * 700 * C_MP, temperature=1.0e6)
+    return spec
+
+
+@pytest.mark.parametrize("limiter,solver", [(3, 1), (1, 2)])
+def test_inlet_matches_oracle(oracle_lib, limiter, solver):
+    """A cloud entering through the inner boundary of an order-2 level:
+    the prepared primitives (inner-ghost inlet, 1e-13) and one RK4 step
+    (ghost inlet every stage and the footprint of the inner faces, 1e-12)
+    against the oracle."""
+    _need_gpu()
+    po = oracle_lib
+    n = 16
+    kw = dict(nr=n, na=n, spatial_order=2, limiter=limiter, riemann_solver=solver)
+    shell = hc.Shell(hc.Params(**kw))
+    orc = po.OracleLevel(po.make_params(**kw))
+    spec = _entering(hc)
+    cone = hc.prepare_cone(spec, INNER)
+    ocone = po.cone_prepare(po.HcConeSpec(**{k: getattr(spec, k) for k in po.CONE_SPEC_FIELDS}), INNER)
+    shell.set_inlet([cone])
+    orc.set_inlet([ocone])
+    ju = _wind(po, orc)
+    t = 3000.0
+    ref = orc.prepare(ju, t)
+    got = shell.prepare(torch.from_numpy(ju).cuda(), t).cpu().numpy()
+    w0 = orc.prepare(ju, 0.0)
+    assert not np.array_equal(ref, w0)
+    err = rel_err_components(got.reshape(6, 8, -1), ref.reshape(6, 8, -1))
+    assert err.max() < 1e-13, err
+    dt = 0.3 / orc.inv_dt(ju)
+    g = torch.from_numpy(ju.copy()).cuda()
+    ref_state = ju.copy()
+    orc.rk4_step(ref_state, dt, t)
+    shell.rk4_step(g, dt, t)
+    assert shell.valid(g)
+    err = rel_err_components(g.cpu().numpy().reshape(6, 8, -1), ref_state.reshape(6, 8, -1))
+    assert err.max() < 1e-12, err
+    # the inlet changed the step
+    plain = ju.copy()
+    orc.set_inlet([])
+    orc.rk4_step(plain, dt, t)
+    assert not np.array_equal(plain, ref_state)
+
+
+def test_inlet_adds_the_crossing_rate():
+    """hc_level_advance_cfl with a crossing cloud: dt = CFL / (rate + (speed
+    + sound speed) / first radial cell width)."""
+    _need_gpu()
+    n = 16
+    p = hc.Params(nr=n, na=n)
+    shell = hc.Shell(p)
+    cone = hc.prepare_cone(_entering(hc), INNER)
+    shell.set_inlet([cone])
+    ju = shell.init(hc.InitSpec())
+    time = torch.full((1,), 3000.0, dtype=torch.float64, device="cuda")
+    dt = torch.zeros(1, dtype=torch.float64, device="cuda")
+    rate = float(shell.inv_dt_max(ju).item())
+    shell.advance(ju, 1, time, dt)
+    width = (p.outer_radius - p.inner_radius) * math.expm1(p.radial_stretch / n) / math.expm1(p.radial_stretch)
+    boundary = (cone.speed * 1e5 + math.sqrt(p.gamma * 2 * 1.380649e-16 * cone.temperature / C_MP)) / width
+    assert float(dt.item()) == pytest.approx(p.cfl / (rate + boundary), rel=1e-13)
+    assert shell.valid(ju)

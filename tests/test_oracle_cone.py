@@ -244,3 +244,47 @@ def test_library_cone_event_matches_schedule_rule():
         assert lib.hc_cone_event(C.byref(cone), C.byref(ev)) == 0
         assert ev.boundary == (1 if cone.end_time > cone.insertion_time else 0)
         assert ev.feeding_end == max(cone.insertion_time, cone.end_time)
+
+
+def _entering_cone(t_ref=0.0):
+    s = po.HcConeSpec()
+    s.lat_deg, s.lon_deg, s.half_angle_deg = 10.0, -20.0, 40.0
+    s.apex_speed, s.wind_speed, s.drag_gamma = 1000.0, 400.0, 0.0
+    s.reference_height, s.reference_time = 21.5, t_ref      # leading edge on r_inner: entering now
+    s.density, s.temperature = 4 * 700 * C_MP, 1.0e6
+    return po.cone_prepare(s, INNER)
+
+
+def test_inlet_prescribes_the_cloud_in_inner_ghosts():
+    """The oracle's inner ghosts under an entering cloud carry the cloud's
+    density, radial speed and pressure with the wind's field; ghosts outside
+    it keep the wind; without the inlet nothing changes."""
+    nr, na = 12, 12
+    params = po.make_params(nr=nr, na=na)
+    orc = po.OracleLevel(params)
+    init = po.HcInit()
+    init.kind = 1
+    init.rho0, init.p0, init.vr, init.b0, init.r_ref = 700 * C_MP, 1e-7, 400e5, 5e-3, INNER
+    ju = orc.init(init)
+    cone = _entering_cone()
+    assert cone.insertion_time <= 0.0 < cone.end_time
+    t = 3000.0
+    base = orc.prepare(ju, t).reshape(6, 8, na + 4, na + 4, nr + 4)
+    orc.set_inlet([cone])
+    got = orc.prepare(ju, t).reshape(6, 8, na + 4, na + 4, nr + 4)
+    ghosts = (slice(None), slice(None), slice(2, na + 2), slice(2, na + 2), slice(0, 2))
+    changed = np.any(got[ghosts] != base[ghosts], axis=1)
+    assert changed.sum() > 4
+    g, b = got[ghosts], base[ghosts]
+    assert np.allclose(g[:, 0][changed], cone.density, rtol=1e-13)
+    speed = np.sqrt((g[:, 1:4] ** 2).sum(1))[changed]
+    assert np.allclose(speed, cone.speed * 1e5, rtol=1e-12)
+    assert np.allclose(g[:, 4][changed], 2 * K_B * cone.temperature * cone.density / C_MP, rtol=1e-10)
+    assert np.allclose(np.moveaxis(g[:, 5:8], 1, -1)[changed], np.moveaxis(b[:, 5:8], 1, -1)[changed], rtol=1e-12,
+                       atol=1e-30)
+    # everything but the inner ghosts is untouched
+    inner = np.zeros(got.shape, bool)
+    inner[ghosts] = True
+    assert np.array_equal(got[~inner], base[~inner])
+    orc.set_inlet([])
+    assert np.array_equal(orc.prepare(ju, t), base.reshape(-1))

@@ -1620,7 +1620,7 @@ int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, do
   // step's come from the previous step's last stage.
   int rc = maybeAutotune(c, ju, s);
   if (rc == HC_OK) rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
-  if (rc == HC_OK) rc = checkLaunch(launchCfl(c->L, ju, c->invMax, s), "cfl");
+  if (rc == HC_OK) rc = checkLaunch(launchCfl(c->L, ju, c->invMax, s, time_dev), "cfl");
   for (int n = 0; n < nsteps && rc == HC_OK; ++n) {
     const int cur = n % 2;
     unsigned long long* next = c->invMax + (1 - cur);

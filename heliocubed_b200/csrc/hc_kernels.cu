@@ -254,7 +254,18 @@ __device__ __forceinline__ void o2Face(const StageArgs& a, const double* __restr
 
 // CFL rate of one valid cell from its conserved state,
 // src/BoxOp_SecondOrderCFL.H:138-202 (no mapped scale, no cone density).
-__device__ __forceinline__ double cflRate(const DevLevel& L, int b, int i, int j, int k, const double u[8]) {
+// Smallest density of the cone clouds being fed through r_inner at time t
+// (minimumConeBoundaryDensity, src/MHD_CME.H:1152-1160), 0 if none.
+__device__ __forceinline__ double coneBoundaryDensity(const DevLevel& L, double t) {
+  double density = 0;
+  for (int s = 0; s < L.ninlet; ++s)
+    if (t >= L.inlet[s].insertionTime && t < L.inlet[s].endTime)
+      density = density > 0 ? fmin(density, L.inlet[s].density) : L.inlet[s].density;
+  return density;
+}
+
+__device__ __forceinline__ double cflRate(const DevLevel& L, int b, int i, int j, int k, const double u[8],
+                                          double coneDensity = 0) {
   const CflCell& a = L.cfl[((size_t)b * L.na + k) * L.na + j];
   const double4 rd = L.radial[i + L.g];
   const double volume = rd.w, inverseVolume = 1.0 / rd.w, width0 = rd.z * L.dxi0;
@@ -297,7 +308,10 @@ __device__ __forceinline__ double cflRate(const DevLevel& L, int b, int i, int j
       fullB2 += field * field;
     }
     const double width = d == 0 ? width0 : volume * a.det[d] * L.h / area[d] / a.normal[d];
-    const double wave = sqrt(L.gamma * pressure / rho + fullB2 / 4.0 / kPi / rho);
+    // src/BoxOp_SecondOrderCFL.H:196-200: a cone may impose a lighter total
+    // density under the ambient field; bound that Alfven speed
+    const double magneticDensity = coneDensity > 0 ? fmin(rho, coneDensity) : rho;
+    const double wave = sqrt(L.gamma * pressure / rho + fullB2 / 4.0 / kPi / magneticDensity);
     inverseDt += (wave + sqrt(v2)) / width;
   }
   return inverseDt;
@@ -456,7 +470,11 @@ __global__ void __launch_bounds__(TL::NT, TL::minBlocks(ROE))
           bad = bad || !isfinite(u[q]) || (q == 0 && !(u[q] > 0));
         }
         if (bad && a.invalid) atomicOr(a.invalid, 1);
-        if (a.invMaxOut) rate = cflRate(L, box, i, j, k, u);
+        if (a.invMaxOut) {
+          // the new state's rate, at the end of the step
+          const double tEnd = a.tbase + (a.tdev ? *a.tdev : 0.0) + dt;
+          rate = cflRate(L, box, i, j, k, u, L.ninlet ? coneBoundaryDensity(L, tEnd) : 0.0);
+        }
       }
       // src/BoxOp_SecondOrderPreStage.H:46-54: JU/J -> Cartesian primitives.
       double wv[8];
@@ -594,8 +612,10 @@ __global__ void ghostsKernel(const DevLevel L, double* __restrict__ w, const Sta
 // CFL rate (src/BoxOp_SecondOrderCFL.H:117-209): max over cells of
 // sum_d (fast bound + |v|)/width_d.  Warp-shuffle then one atomic per warp.
 // ---------------------------------------------------------------------------
-__global__ void cflKernel(const DevLevel L, const double* __restrict__ ju, unsigned long long* invMaxBits) {
+__global__ void cflKernel(const DevLevel L, const double* __restrict__ ju, unsigned long long* invMaxBits,
+                          const double* __restrict__ time) {
   const long n = 6L * L.Nv;
+  const double cone = time && L.ninlet ? coneBoundaryDensity(L, *time) : 0.0;
   double best = 0.0;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
     const int b = (int)(t / L.Nv);
@@ -607,7 +627,7 @@ __global__ void cflKernel(const DevLevel L, const double* __restrict__ ju, unsig
     const double* src = ju + (long)b * NC * L.Nv + r;
 #pragma unroll
     for (int c = 0; c < NC; ++c) u[c] = src[c * L.Nv];
-    const double inverseDt = cflRate(L, b, i, j, k, u);
+    const double inverseDt = cflRate(L, b, i, j, k, u, cone);
     best = best < inverseDt ? inverseDt : best;  // std::max(localMaximum, x)
   }
   warpMaxAtomic(best, invMaxBits);
@@ -806,10 +826,11 @@ cudaError_t launchGhosts(const DevLevel& L, double* w, const StageTime& t, cudaS
   return cudaGetLastError();
 }
 
-cudaError_t launchCfl(const DevLevel& L, const double* ju, unsigned long long* invMaxBits, cudaStream_t s) {
+cudaError_t launchCfl(const DevLevel& L, const double* ju, unsigned long long* invMaxBits, cudaStream_t s,
+                      const double* time) {
   cudaError_t e = cudaMemsetAsync(invMaxBits, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
-  cflKernel<<<gridFor(6L * L.Nv, 256), 256, 0, s>>>(L, ju, invMaxBits);
+  cflKernel<<<gridFor(6L * L.Nv, 256), 256, 0, s>>>(L, ju, invMaxBits, time);
   return cudaGetLastError();
 }
 

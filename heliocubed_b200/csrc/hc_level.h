@@ -134,7 +134,10 @@ struct StageTime {
   double dtv;
 };
 cudaError_t launchGhosts(const DevLevel& L, double* w, const StageTime& t, cudaStream_t s);
-cudaError_t launchCfl(const DevLevel& L, const double* ju, unsigned long long* invMaxBits, cudaStream_t s);
+// time (device, may be null): with inlet cones active then, the cone
+// density floor of the Alfven speed applies.
+cudaError_t launchCfl(const DevLevel& L, const double* ju, unsigned long long* invMaxBits, cudaStream_t s,
+                      const double* time = nullptr);
 cudaError_t launchValid(const DevLevel& L, const double* ju, int* ok, cudaStream_t s);
 cudaError_t launchInit(const DevLevel& L, const void* init, double* ju, cudaStream_t s);
 cudaError_t launchBoxGravity(const DevLevel& L, const int lo[3], const int hi[3], int block, const double* w,

@@ -570,11 +570,13 @@ __global__ void __launch_bounds__(128, MB) o4FaceReconKernel(const Ctx* __restri
     double l[8], r[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) { l[q] = sLR[q][threadIdx.x]; r[q] = sLR[8 + q][threadIdx.x]; }
-    if (roeNow(a.G)) {
+    // Roe repair: only faces whose reconstructed states are unusable read
+    // the adjacent cells' average primitives (most faces never do)
+    if (roeNow(a.G) && !(usablePrimitive(l) && usablePrimitive(r))) {
       double cl[8], cr[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) { cl[q] = WA[q * NG + cell[2]]; cr[q] = WA[q * NG + cell[3]]; }
-      if (!(usablePrimitive(l) && usablePrimitive(r)) && usablePrimitive(cl) && usablePrimitive(cr)) {
+      if (usablePrimitive(cl) && usablePrimitive(cr)) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) { l[q] = cl[q]; r[q] = cr[q]; }
         thF = 0.0;

@@ -468,7 +468,10 @@ int hc_level_set_cme_schedule(hc_ctx* ctx, const hc_cme_event* events, int n, vo
  * (src/BoxOp_SecondOrder.H:175-181, 282-311); hc_level_rhs and hc_box_rhs,
  * which take no time, do not.  hc_level_advance_cfl adds each crossing
  * cloud's (speed + sound speed) / first radial cell width to the step's
- * CFL rate (src/MHD_CME.H:1165-1191).  At most 8 cones; n = 0 stops the
+ * CFL rate (src/MHD_CME.H:1165-1191), and its rate takes the Alfven speeds
+ * with density min(rho, the lightest crossing cloud's density)
+ * (src/BoxOp_SecondOrderCFL.H:196-200); hc_level_dt_cfl, which takes no
+ * time, does not.  At most 8 cones; n = 0 stops the
  * inlet.  The cones are copied on `stream`; launches captured in a graph
  * keep the inlet set when they were captured. */
 int hc_level_set_inlet(hc_ctx* ctx, const hc_cone* cones, int n, void* stream);

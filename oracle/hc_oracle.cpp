@@ -1124,7 +1124,7 @@ void levelRk4(const Level& L, double* ju, double dt, double t) {
 }
 
 // src/BoxOp_SecondOrderCFL.H:99-210 (no mapped scale, no cone density).
-double levelInvDt(const Level& L, const double* ju) {
+double levelInvDt(const Level& L, const double* ju, double coneDensity = 0) {
   const hc_params& P = L.P;
   LevelArrays I(L);
   const int nr = L.nr, na = L.na;
@@ -1183,7 +1183,9 @@ double levelInvDt(const Level& L, const double* ju) {
               fullB2 += field * field;
             }
             const double width = d == 0 ? width0 : r.vol * fdet[d] * h / area[d] / normal[d];
-            const double wave = std::sqrt(gamma * pressure / rho + fullB2 / 4.0 / M_PI / rho);
+            // src/BoxOp_SecondOrderCFL.H:196-200
+            const double magneticDensity = coneDensity > 0 ? std::min(rho, coneDensity) : rho;
+            const double wave = std::sqrt(gamma * pressure / rho + fullB2 / 4.0 / M_PI / magneticDensity);
             inverseDt += (wave + std::sqrt(v2)) / width;
           }
           gmax = std::max(gmax, inverseDt);
@@ -1472,6 +1474,15 @@ int orc_level_rk4_step(void* L, double* ju, double dt, double t) { levelRk4(*sta
 double orc_level_inv_dt(void* L, const double* ju) { return levelInvDt(*static_cast<Level*>(L), ju); }
 int orc_level_valid(void* L, const double* ju) { return levelValid(*static_cast<Level*>(L), ju); }
 int orc_level_init(void* L, const hc_init* in, double* ju) { levelInit(*static_cast<Level*>(L), *in, ju); return 0; }
+// The CFL rate with the cone density floor of the inlet cones active at t
+// (minimumConeBoundaryDensity, src/MHD_CME.H:1152-1160).
+double orc_level_inv_dt_at(void* Lp, const double* ju, double t) {
+  const Level& L = *static_cast<Level*>(Lp);
+  double density = 0;
+  for (const hc_cone& c : L.inlet)
+    if (t >= c.insertion_time && t < c.end_time) density = density > 0 ? std::min(density, c.density) : c.density;
+  return levelInvDt(L, ju, density);
+}
 int orc_level_set_inlet(void* L, const hc_cone* cones, int n) {
   static_cast<Level*>(L)->inlet.assign(cones, cones + n);
   return 0;

@@ -111,6 +111,8 @@ def lib() -> C.CDLL:
         L.orc_level_insert_cone.argtypes = [C.c_void_p, C.POINTER(HcCone), C.c_double, _D, _D]
         L.orc_cme_schedule.argtypes = [C.POINTER(HcCmeEvent), C.c_int, C.c_double, C.c_double, _D]
         L.orc_level_set_inlet.argtypes = [C.c_void_p, C.POINTER(HcCone), C.c_int]
+        L.orc_level_inv_dt_at.restype = C.c_double
+        L.orc_level_inv_dt_at.argtypes = [C.c_void_p, _D, C.c_double]
         L.orc_o4_level_create.restype = C.c_void_p
         L.orc_o4_level_create.argtypes = [C.c_void_p]
         L.orc_o4_level_destroy.argtypes = [C.c_void_p]
@@ -204,6 +206,10 @@ class OracleLevel:
         w = np.zeros(self.ng)
         self.L.orc_level_prepare(self.h, dptr(ju), dptr(w), t)
         return w
+
+    def inv_dt_at(self, ju: np.ndarray, t: float) -> float:
+        """CFL rate with the cone density floor of the inlet active at t."""
+        return self.L.orc_level_inv_dt_at(self.h, dptr(ju), t)
 
     def set_inlet(self, cones) -> None:
         """Cone clouds fed through the inner boundary while they cross it."""

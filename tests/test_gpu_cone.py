@@ -264,19 +264,31 @@ def test_inlet_matches_oracle(oracle_lib, limiter, solver):
     assert not np.array_equal(plain, ref_state)
 
 
-def test_inlet_adds_the_crossing_rate():
+@pytest.mark.parametrize("density_factor", [4.0, 0.25])
+def test_inlet_adds_the_crossing_rate(oracle_lib, density_factor):
     """hc_level_advance_cfl with a crossing cloud: dt = CFL / (rate + (speed
-    + sound speed) / first radial cell width)."""
+    + sound speed) / first radial cell width), the rate's Alfven speeds
+    taken with density min(rho, cone density) (the oracle's rate, 1e-13):
+    a light cone raises the rate."""
     _need_gpu()
+    po = oracle_lib
     n = 16
     p = hc.Params(nr=n, na=n)
     shell = hc.Shell(p)
-    cone = hc.prepare_cone(_entering(hc), INNER)
+    orc = po.OracleLevel(po.make_params(nr=n, na=n))
+    spec = _entering(hc)
+    spec.density = density_factor * 700 * C_MP
+    cone = hc.prepare_cone(spec, INNER)
+    ocone = po.cone_prepare(po.HcConeSpec(**{k: getattr(spec, k) for k in po.CONE_SPEC_FIELDS}), INNER)
     shell.set_inlet([cone])
-    ju = shell.init(hc.InitSpec())
+    orc.set_inlet([ocone])
+    ju0 = _wind(po, orc)
+    ju = torch.from_numpy(ju0.copy()).cuda()
     time = torch.full((1,), 3000.0, dtype=torch.float64, device="cuda")
     dt = torch.zeros(1, dtype=torch.float64, device="cuda")
-    rate = float(shell.inv_dt_max(ju).item())
+    rate = orc.inv_dt_at(ju0, 3000.0)
+    plain = orc.inv_dt(ju0)
+    assert (rate > plain * (1 + 1e-9)) == (density_factor < 1)
     shell.advance(ju, 1, time, dt)
     width = (p.outer_radius - p.inner_radius) * math.expm1(p.radial_stretch / n) / math.expm1(p.radial_stretch)
     boundary = (cone.speed * 1e5 + math.sqrt(p.gamma * 2 * 1.380649e-16 * cone.temperature / C_MP)) / width

@@ -840,9 +840,24 @@ int rkStep(hc_ctx* c, double* ju, double dtv, const double* invMax, unsigned lon
     a.invalid = nullptr;
     a.tbase = tbase;
     a.tdev = tdev;
-    rc = checkLaunch(launchStage(a, MODE_RK, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
-                                 c->P.sun_gravity == 1, s, c->tileRK),
-                     "stage");
+    if (c->P.riemann_solver == 2 && c->sched && c->rusanovFlag) {
+      // Roe context under an insertion schedule: the window flag picks the
+      // Roe or the Rusanov stage kernel on the device
+      a.solverFlag = c->rusanovFlag;
+      a.exitOnFlag = 1;
+      rc = checkLaunch(launchStage(a, MODE_RK, c->P.limiter, true, c->P.divergence_cleaning == 1,
+                                   c->P.sun_gravity == 1, s, c->tileRK),
+                       "stage");
+      a.exitOnFlag = 0;
+      if (rc == HC_OK)
+        rc = checkLaunch(launchStage(a, MODE_RK, c->P.limiter, false, c->P.divergence_cleaning == 1,
+                                     c->P.sun_gravity == 1, s, c->tileRK),
+                         "stage");
+    } else {
+      rc = checkLaunch(launchStage(a, MODE_RK, c->P.limiter, c->P.riemann_solver == 2, c->P.divergence_cleaning == 1,
+                                   c->P.sun_gravity == 1, s, c->tileRK),
+                       "stage");
+    }
     if (rc != HC_OK) return rc;
   }
   return HC_OK;
@@ -1465,7 +1480,7 @@ int hc_level_set_cme_schedule(hc_ctx* c, const hc_cme_event* events, int n, void
       return fail(HC_ERR_ARG, "CME events must be ordered by insertion time");
   CmeSchedule& h = c->schedHost;
   h.n = n;
-  h.roe = c->P.riemann_solver == 2 && c->P.spatial_order == 4 ? 1 : 0;
+  h.roe = c->P.riemann_solver == 2 ? 1 : 0;
   h.cfl = c->P.cfl;
   h.feeding = c->P.riemann_solver == 2 ? .5 : 1.;
   for (int i = 0; i < n; ++i) {
@@ -1476,6 +1491,12 @@ int hc_level_set_cme_schedule(hc_ctx* c, const hc_cme_event* events, int n, void
     h.stabEnd[i] = e.boundary ? std::max(e.feeding_end + 600, e.insertion_time + 2400) : e.insertion_time + 600;
   }
   cudaStream_t s = (cudaStream_t)stream;
+  if (!c->rusanovFlag) {  // order 2 (order 4 allocates it with its geometry)
+    cudaError_t err = cudaMalloc(&c->rusanovFlag, sizeof(int));
+    if (err == cudaSuccess) err = cudaMemsetAsync(c->rusanovFlag, 0, sizeof(int), s);
+    if (err != cudaSuccess) return cudaFail(err, "CME window flag");
+    c->owned.push_back(c->rusanovFlag);
+  }
   if (!c->sched) {
     cudaError_t err = cudaMalloc(&c->sched, sizeof(CmeSchedule));
     if (err != cudaSuccess) return cudaFail(err, "CME schedule");
@@ -1587,6 +1608,12 @@ int hc_level_rk4_step(hc_ctx* c, double* ju, double dt, double t, void* stream) 
   if (!c || !ju) return fail(HC_ERR_ARG, "null argument");
   if (!(dt > 0)) return fail(HC_ERR_ARG, "dt must be positive");
   cudaStream_t s = (cudaStream_t)stream;
+  // the insertion schedule belongs to hc_level_advance_cfl: a fixed-dt step
+  // runs the context's own solver
+  if (c->sched && c->rusanovFlag) {
+    const int rcf = checkLaunch(cudaMemsetAsync(c->rusanovFlag, 0, sizeof(int), s), "CME window flag");
+    if (rcf != HC_OK) return rcf;
+  }
   if (c->P.spatial_order == 4) {
     int rc4 = ensureO4Buffers(c);
     if (rc4 == HC_OK) rc4 = maybeAutotune(c, ju, s);
@@ -1627,7 +1654,7 @@ int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, do
     const double* invMax = reinterpret_cast<const double*>(c->invMax + cur);
     rc = checkLaunch(cudaMemsetAsync(next, 0, sizeof(unsigned long long), s), "cfl reset");
     if (rc == HC_OK && c->sched && time_dev)
-      rc = checkLaunch(launchCmeSchedule(c->sched, c->invMax + cur, time_dev, nullptr, s), "CME schedule");
+      rc = checkLaunch(launchCmeSchedule(c->sched, c->invMax + cur, time_dev, c->rusanovFlag, s), "CME schedule");
     if (rc == HC_OK) rc = rkStep(c, ju, 0.0, invMax, n + 1 < nsteps ? next : nullptr, 0.0, time_dev, s);
     if (rc == HC_OK) rc = checkLaunch(launchAdvanceTime(time_dev, invMax, c->P.cfl, dt_dev, s), "time");
   }

@@ -366,6 +366,7 @@ __global__ void __launch_bounds__(TL::NT, TL::minBlocks(ROE))
     o2StageKernel(const StageArgs a, const int powell, const int grav) {
   constexpr int TX = TL::TX, TY = TL::TY, TZ = TL::TZ, NF = TL::NF, NF0 = TL::NF0, NF1 = TL::NF1;
   extern __shared__ double sF[];  // [9][NF]: 8 flux components + Powell face B_n
+  if (a.solverFlag && ((*a.solverFlag != 0) == (a.exitOnFlag != 0))) return;  // the other solver's launch
   const int v0 = a.hi[0] - a.lo[0] + 1, v1 = a.hi[1] - a.lo[1] + 1, v2 = a.hi[2] - a.lo[2] + 1;
   const int nbx = (v0 + TX - 1) / TX, nby = (v1 + TY - 1) / TY, nbz = (v2 + TZ - 1) / TZ;
   int t = blockIdx.x;

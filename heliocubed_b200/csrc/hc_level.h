@@ -111,6 +111,11 @@ struct StageArgs {
   // c_s dt.  Only the inlet footprint of the inner face reads it.
   double tbase;
   const double* tdev;
+  // CME insertion window (device flag, may be null): the launch returns at
+  // once when (*solverFlag != 0) == exitOnFlag, so a Roe context launches
+  // its Roe kernel (exit on 1) and its Rusanov kernel (exit on 0)
+  const int* solverFlag;
+  int exitOnFlag;
 };
 
 enum { MODE_BOX = 0, MODE_RK = 1, MODE_RHS = 2 };

@@ -446,10 +446,12 @@ int hc_cone_event(const hc_cone* cone, hc_cme_event* event);
  * early = clamp((time - t - 600) / 1800, 0, 1), recovery = clamp((time -
  * end) / 1800, 0, 1), f = 0.5 with Roe and 1 with Rusanov, and end the
  * source's stabilisation end (t + 600, or max(feeding_end + 600, t + 2400)
- * for a boundary source) (src/MHD_CME.H:1275-1297, 1329-1332).  A
- * fourth-order Roe context uses Rusanov dissipation while time is before the
+ * for a boundary source) (src/MHD_CME.H:1275-1297, 1329-1332).  A Roe
+ * context uses Rusanov dissipation while time is before the
  * latest stabilisation end, with dt shortened to land on it (the reference's
- * Rusanov window; second-order contexts get the CFL ramp only).  n = 0
+ * Rusanov window; at order 2 the device picks between the Roe and the
+ * Rusanov stage kernels, both launched, each returning at once unless it
+ * is the one wanted).  n = 0
  * clears; at most 8 events, ordered by insertion time.  The schedule is
  * copied to the device in order on `stream`.  After the first call every
  * hc_level_advance_cfl step runs the schedule (with no events it changes

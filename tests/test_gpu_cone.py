@@ -191,13 +191,15 @@ def test_schedule_scales_the_cfl_step(oracle_lib, order):
         assert ends, "the steps never entered the Rusanov window"
 
 
-def test_rusanov_window_runs_the_rusanov_operator():
-    """Inside the window a fourth-order Roe context's step equals, bit for
-    bit, the same step of a Rusanov context with the same schedule."""
+@pytest.mark.parametrize("order", [2, 4])
+def test_rusanov_window_runs_the_rusanov_operator(order):
+    """Inside the window a Roe context's step equals, bit for bit, the same
+    step of a Rusanov context with the same schedule; a fixed-dt step after
+    it runs Roe again."""
     _need_gpu()
     n = 16
-    roe = hc.Shell(hc.Params(nr=n, na=n, spatial_order=4, riemann_solver=2))
-    rus = hc.Shell(hc.Params(nr=n, na=n, spatial_order=4, riemann_solver=1))
+    roe = hc.Shell(hc.Params(nr=n, na=n, spatial_order=order, riemann_solver=2))
+    rus = hc.Shell(hc.Params(nr=n, na=n, spatial_order=order, riemann_solver=1))
     ju0 = roe.init(hc.InitSpec())
     for sh in (roe, rus):
         sh.set_cme_schedule([_volume_event(0.0)])
@@ -210,6 +212,11 @@ def test_rusanov_window_runs_the_rusanov_operator():
     assert float(ta.item()) < 600.0          # still inside the window
     assert torch.equal(ta, tb)
     assert torch.equal(a, b)
+    # a fixed-dt step runs the context's own solver
+    d1, d2 = ju0.clone(), ju0.clone()
+    roe.rk4_step(d1, 30.0, 0.0)
+    rus.rk4_step(d2, 30.0, 0.0)
+    assert not torch.equal(d1, d2)
     # without a schedule the Roe context differs
     roe.set_cme_schedule([])
     c = ju0.clone()

@@ -998,6 +998,11 @@ int hc_ctx_create(const hc_params* p, int device, hc_ctx** out) {
   if (p->riemann_solver != 1 && p->riemann_solver != 2) return fail(HC_ERR_ARG, "Riemann_solver_type must be 1 or 2");
   if (p->temporal_order != 4) return fail(HC_ERR_UNSUPPORTED, "temporal_order must be 4 (classical RK4)");
   if (p->nr < 4 || p->na < 4) return fail(HC_ERR_ARG, "need nr >= 4 and na >= 4");
+  // The level kernels index cells and components in 32 bits: every ghosted
+  // component array of the level (ghost layers of either order) must stay
+  // below 2^31 entries.
+  if (48.0 * (p->nr + 12.0) * (p->na + 12.0) * (p->na + 12.0) >= 2147483647.0)
+    return fail(HC_ERR_ARG, "level too large: 48 (nr + 12) (na + 12)^2 must stay below 2^31");
   if (!(p->gamma > 1.0)) return fail(HC_ERR_ARG, "gamma must exceed 1");
   if (!(p->inner_radius > 0.0 && p->outer_radius > p->inner_radius))
     return fail(HC_ERR_ARG, "need 0 < inner_radius < outer_radius");

@@ -15,6 +15,16 @@
 
 namespace hc {
 
+// Level kernels loop over flat indices below 2^31 (hc_ctx_create bounds
+// the level size), so their loops and index splits run in 32-bit unsigned
+// arithmetic.  takeMod returns t mod n and leaves t / n in t.
+HC_DEV unsigned takeMod(unsigned& t, unsigned n) {
+  const unsigned q = t / n, r = t - q * n;
+  t = q;
+  return r;
+}
+#define HC_LEVEL_LOOP(t, n) for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < (n); t += gridDim.x * blockDim.x)
+
 HC_DEV double dmin(double a, double b) { return b < a ? b : a; }  // std::min
 HC_DEV double dmax(double a, double b) { return a < b ? b : a; }  // std::max
 

@@ -493,13 +493,14 @@ __global__ void __launch_bounds__(TL::NT, TL::minBlocks(ROE))
 // Stage preparation (src/BoxOp_SecondOrderPreStage.H:7-218).
 // ---------------------------------------------------------------------------
 __global__ void primValidKernel(const DevLevel L, const double* __restrict__ ju, double* __restrict__ w) {
-  const long n = 6L * L.Nv;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int b = (int)(t / L.Nv);
-    const long r = t - (long)b * L.Nv;
-    const int i = (int)(r % L.nr);
-    const int j = (int)((r / L.nr) % L.na);
-    const int k = (int)(r / ((long)L.nr * L.na));
+  const unsigned n = (unsigned)(6L * L.Nv);
+  HC_LEVEL_LOOP(t, n) {
+    unsigned q = t;
+    const int i = (int)takeMod(q, L.nr);
+    const int j = (int)takeMod(q, L.na);
+    const int k = (int)takeMod(q, L.na);
+    const int b = (int)q;
+    const long r = (long)t - (long)b * L.Nv;
     double in[8], out[8];
     const double* src = ju + (long)b * NC * L.Nv + r;
 #pragma unroll
@@ -517,19 +518,19 @@ __device__ __forceinline__ long gIdx(const DevLevel& L, int b, int i, int j, int
 }
 
 __global__ void ghostsKernel(const DevLevel L, double* __restrict__ w, const StageTime st) {
-  const long nSeam = 6L * 2 * 2 * L.g * L.na * L.nr;
-  const long nRad = 6L * L.na * L.na;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nSeam + nRad; t += (long)gridDim.x * blockDim.x) {
+  const unsigned nSeam = (unsigned)(6L * 2 * 2 * L.g * L.na * L.nr);
+  const unsigned nRad = (unsigned)(6L * L.na * L.na);
+  HC_LEVEL_LOOP(t, nSeam + nRad) {
     if (t < nSeam) {
       // Panel-seam ghost: 4-point along-edge interpolation of the adjacent
       // panel's Cartesian primitives, then the floors of :70-75.
-      const int i = (int)(t % L.nr);
-      long q = t / L.nr;
-      const int s = (int)(q % L.na); q /= L.na;
-      const int m = (int)(q % L.g); q /= L.g;
-      const int side = (int)(q % 2); q /= 2;
-      const int ax = (int)(q % 2);
-      const int b = (int)(q / 2);
+      unsigned q = t;
+      const int i = (int)takeMod(q, L.nr);
+      const int s = (int)takeMod(q, L.na);
+      const int m = (int)takeMod(q, L.g);
+      const int side = (int)(q & 1u);
+      const int ax = (int)((q >> 1) & 1u);
+      const int b = (int)(q >> 2);
       const SeamDonor dn = L.seam[((((long)b * 2 + ax) * 2 + side) * L.g + m) * L.na + s];
       const int n = side == 0 ? -1 - m : L.na + m;
       const int gj = ax == 0 ? n : s, gk = ax == 0 ? s : n;
@@ -547,10 +548,10 @@ __global__ void ghostsKernel(const DevLevel L, double* __restrict__ w, const Sta
 #pragma unroll
       for (int c = 0; c < NC; ++c) w[o + c * L.Ng] = v[c];
     } else {
-      const long r = t - nSeam;
-      const int j = (int)(r % L.na);
-      const int k = (int)((r / L.na) % L.na);
-      const int b = (int)(r / ((long)L.na * L.na));
+      unsigned r = t - nSeam;
+      const int j = (int)takeMod(r, L.na);
+      const int k = (int)takeMod(r, L.na);
+      const int b = (int)r;
       const size_t cidx = ((size_t)b * L.na + k) * L.na + j;
       const double* A = L.basis + cidx * 9;
       // Inner radial ghosts: analytic wind (src/BoxOp_PreStage.H:215-228).
@@ -615,15 +616,16 @@ __global__ void ghostsKernel(const DevLevel L, double* __restrict__ w, const Sta
 // ---------------------------------------------------------------------------
 __global__ void cflKernel(const DevLevel L, const double* __restrict__ ju, unsigned long long* invMaxBits,
                           const double* __restrict__ time) {
-  const long n = 6L * L.Nv;
+  const unsigned n = (unsigned)(6L * L.Nv);
   const double cone = time && L.ninlet ? coneBoundaryDensity(L, *time) : 0.0;
   double best = 0.0;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int b = (int)(t / L.Nv);
-    const long r = t - (long)b * L.Nv;
-    const int i = (int)(r % L.nr);
-    const int j = (int)((r / L.nr) % L.na);
-    const int k = (int)(r / ((long)L.nr * L.na));
+  HC_LEVEL_LOOP(t, n) {
+    unsigned q = t;
+    const int i = (int)takeMod(q, L.nr);
+    const int j = (int)takeMod(q, L.na);
+    const int k = (int)takeMod(q, L.na);
+    const int b = (int)q;
+    const long r = (long)t - (long)b * L.Nv;
     double u[8];
     const double* src = ju + (long)b * NC * L.Nv + r;
 #pragma unroll
@@ -638,11 +640,11 @@ __global__ void setIntKernel(int* p, int v) { *p = v; }
 
 // src/BoxOp_EulerCubedSphereImplem.H:817-876: finite components, rho > 0.
 __global__ void validKernel(const DevLevel L, const double* __restrict__ ju, int* ok) {
-  const long n = 6L * NC * L.Nv;
+  const unsigned n = (unsigned)(6L * NC * L.Nv), nv = (unsigned)L.Nv;
   bool bad = false;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+  HC_LEVEL_LOOP(t, n) {
     const double v = ju[t];
-    const int c = (int)((t / L.Nv) % NC);
+    const int c = (int)((t / nv) % NC);
     bad = bad || !isfinite(v) || (c == 0 && !(v > 0));
   }
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicExch(ok, 0);

@@ -401,14 +401,19 @@ __device__ __forceinline__ double faceProd(double f4, double g4, double df0, dou
 
 // Thread -> (i, j, k) over the chunk's points of region b (flat index,
 // radial fastest) of the chunk's box; the end is clamped to the region.
+// Regions hold fewer than 2^31 points (o4BatchCreate rejects larger boxes),
+// so the index split runs in 32-bit unsigned arithmetic: two hardware-sized
+// divisions per point instead of three 64-bit ones.
 template <class F>
 __device__ __forceinline__ void forRegion(const Box3& b, const WorkChunk& w, F f) {
-  const long n = b.size();
-  const long end = w.end < n ? w.end : n;
-  for (long t = w.begin + threadIdx.x; t < end; t += w.stride) {
-    const int i = b.lo[0] + (int)(t % b.n(0));
-    const int j = b.lo[1] + (int)((t / b.n(0)) % b.n(1));
-    const int k = b.lo[2] + (int)(t / ((long)b.n(0) * b.n(1)));
+  const unsigned n0 = (unsigned)b.n(0), n1 = (unsigned)b.n(1);
+  const unsigned n = n0 * n1 * (unsigned)b.n(2);
+  const unsigned end = w.end < (long)n ? (unsigned)w.end : n;
+  for (unsigned t = (unsigned)w.begin + threadIdx.x; t < end; t += (unsigned)w.stride) {
+    const unsigned q = t / n0, kk = q / n1;
+    const int i = b.lo[0] + (int)(t - q * n0);
+    const int j = b.lo[1] + (int)(q - kk * n1);
+    const int k = b.lo[2] + (int)kk;
     f(0, i, j, k);
   }
 }
@@ -550,15 +555,24 @@ __global__ void __launch_bounds__(128, MB) o4FaceReconKernel(const Ctx* __restri
     // one copy of the reconstruction code for the eight components (a rolled
     // loop; the states go through this thread's shared-memory column)
     __shared__ double sLR[16][128];
+    // the next component's six cells are loaded while this one is
+    // reconstructed (all six cells lie in G for every face of F)
+    double nx[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) nx[s] = WP[cell[s]];
 #pragma unroll 1
     for (int q = 0; q < 8; ++q) {
-      const double* Wq = WP + q * NG;
+      const double cur[6] = {nx[0], nx[1], nx[2], nx[3], nx[4], nx[5]};
+      if (q < 7) {
+        const double* Wn = WP + (q + 1) * NG;
+#pragma unroll
+        for (int s = 0; s < 6; ++s) nx[s] = Wn[cell[s]];
+      }
       double L, R;
       if (smooth) {
-        const double st[6] = {Wq[cell[0]], Wq[cell[1]], Wq[cell[2]], Wq[cell[3]], Wq[cell[4]], Wq[cell[5]]};
-        wenozFace(st, L, R);
+        wenozFace(cur, L, R);
       } else {
-        const double st[4] = {Wq[cell[1]], Wq[cell[2]], Wq[cell[3]], Wq[cell[4]]};
+        const double st[4] = {cur[1], cur[2], cur[3], cur[4]};
         if (a.G.fallback == 0) weno3Face(st, dx2, L, R);
         else plmFallbackFace(st, L, R);
       }
@@ -644,14 +658,21 @@ __global__ void o4FaceAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg, c
     double* base = a.face + (long)b * kO4FaceArrays * NF;
     const bool sm = base[F_THF * NF + fo] > 0.5;
     const View FS = faceView(c, b, F_FS);
+    const View PS = faceView(c, b, F_PS);
+    // All loads come before the first store: the stores go to the same face
+    // scratch, so the compiler may not hoist a later load above one, and
+    // interleaving them would serialise one memory round trip per component.
+    double out[9];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const double pt = FS(q, i, j, k);
-      base[(F_FA + q) * NF + fo] = sm ? pt + lapFace(FS, q, d, i, j, k) * (1.0 / 24.0) : pt;
+      out[q] = sm ? pt + lapFace(FS, q, d, i, j, k) * (1.0 / 24.0) : pt;
     }
-    const View PS = faceView(c, b, F_PS);
     const double pp = PS(0, i, j, k);
-    base[F_PA * NF + fo] = sm ? pp + lapFace(PS, 0, d, i, j, k) * (1.0 / 24.0) : pp;
+    out[8] = sm ? pp + lapFace(PS, 0, d, i, j, k) * (1.0 / 24.0) : pp;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) base[(F_FA + q) * NF + fo] = out[q];
+    base[F_PA * NF + fo] = out[8];
   });
 }
 
@@ -742,18 +763,23 @@ __global__ void o4FaceRadialKernel(const Ctx* __restrict__ tab, const RegArgs rg
     const double s = adjDr(a.G, d, i);
     const double ds = 0.5 * adjDr(a.G, d, i + 1) - 0.5 * adjDr(a.G, d, i - 1);
     const View FM = faceView(c, b, F_FM);
+    const View PA = faceView(c, b, F_PA);
+    // all loads before the first store into the shared face scratch
+    double out[9];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       double value = 0.0;
       if (d != 0) value += (0.5 * FM(q, i + 1, j, k) - 0.5 * FM(q, i - 1, j, k)) * ds * (1.0 / 12.0);
       value += FM(q, i, j, k) * s * 1.0;
-      base[(F_FR + q) * NF + fo] = value;
+      out[q] = value;
     }
-    const View PA = faceView(c, b, F_PA);
     double value = 0.0;
     if (d != 0) value += (0.5 * PA(0, i + 1, j, k) - 0.5 * PA(0, i - 1, j, k)) * ds * (1.0 / 12.0);
     value += PA(0, i, j, k) * s * 1.0;
-    base[F_T3 * NF + fo] = value;
+    out[8] = value;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) base[(F_FR + q) * NF + fo] = out[q];
+    base[F_T3 * NF + fo] = out[8];
   });
 }
 
@@ -810,12 +836,19 @@ __global__ void __launch_bounds__(128, MB) o4FaceFinalKernel(const Ctx* __restri
       // point-to-average and transverse differences of the eight point
       // dissipations in a rolled loop through this thread's shared column
       __shared__ double sQ[24][128];
+      // (the five values of a component are loaded once: lapFace and cdiff
+      // restated on them, so the stores to the column cannot force reloads)
+      int m1[3] = {i, j, k}, p1[3] = {i, j, k}, m2[3] = {i, j, k}, p2[3] = {i, j, k};
+      m1[t1] -= 1; p1[t1] += 1; m2[t2] -= 1; p2[t2] += 1;
 #pragma unroll 1
       for (int q = 0; q < 8; ++q) {
         const double pt = QD(q, i, j, k);
-        sQ[q][threadIdx.x] = sm ? pt + lapFace(QD, q, d, i, j, k) * (1.0 / 24.0) : pt;
-        sQ[8 + q][threadIdx.x] = cdiff(QD, q, t1, i, j, k);
-        sQ[16 + q][threadIdx.x] = cdiff(QD, q, t2, i, j, k);
+        const double a1 = QD(q, m1[0], m1[1], m1[2]), b1 = QD(q, p1[0], p1[1], p1[2]);
+        const double a2 = QD(q, m2[0], m2[1], m2[2]), b2 = QD(q, p2[0], p2[1], p2[2]);
+        const double lap = (a1 + b1) + (a2 + b2) - 4.0 * pt;
+        sQ[q][threadIdx.x] = sm ? pt + lap * (1.0 / 24.0) : pt;
+        sQ[8 + q][threadIdx.x] = 0.5 * b1 - 0.5 * a1;
+        sQ[16 + q][threadIdx.x] = 0.5 * b2 - 0.5 * a2;
       }
       double avg[8], dP0[8], dP1[8];
 #pragma unroll
@@ -924,8 +957,15 @@ __global__ void o4DivKernel(const Ctx* __restrict__ tab, const RegArgs rg, const
     int p[3] = {i, j, k};
     p[d] += 1;
     double* R = a.rhs + b * a.rhsStride + roff(c.vr, i, j, k);
+    // all loads (fluxes and the accumulated rhs) before the first store
+    double dfx[8], rv[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) R[q * c.vr.N] += coef * (FX(q, p[0], p[1], p[2]) - FX(q, i, j, k));
+    for (int q = 0; q < 8; ++q) {
+      dfx[q] = FX(q, p[0], p[1], p[2]) - FX(q, i, j, k);
+      rv[q] = R[q * c.vr.N];
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) R[q * c.vr.N] = rv[q] + coef * dfx[q];
   });
 }
 
@@ -1046,8 +1086,12 @@ __global__ void o4PowellAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg,
   forRegion(c.V1, wc, [&](int b, int i, int j, int k) {
     const View KP{a.kp + (long)b * 16 * c.v2r.N, c.v2r};
     double* KA = a.kp + (long)b * 16 * c.v2r.N + 8 * c.v2r.N + roff(c.v2r, i, j, k);
+    // all loads before the first store (KA and KP share one array)
+    double out[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) KA[q * c.v2r.N] = KP(q, i, j, k) + lapCell(KP, q, i, j, k) * (1.0 / 24.0);
+    for (int q = 0; q < 8; ++q) out[q] = KP(q, i, j, k) + lapCell(KP, q, i, j, k) * (1.0 / 24.0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) KA[q * c.v2r.N] = out[q];
   });
 }
 
@@ -1059,13 +1103,23 @@ __global__ void o4PowellApplyKernel(const Ctx* __restrict__ tab, const RegArgs r
     const View KA{a.kp + (long)b * 16 * c.v2r.N + 8 * c.v2r.N, c.v2r};
     const View MJ{a.mj + (long)b * c.v1r.N, c.v1r};
     double* R = a.rhs + b * a.rhsStride + roff(c.vr, i, j, k);
+    // all loads (including the accumulated rhs) before the first store
+    double dmj[3];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) dmj[t] = cdiff(MJ, 0, t, i, j, k);
+    const double mj0 = MJ(0, i, j, k);
+    double add[8], rv[8];
+#pragma unroll
     for (int q = 1; q < 8; ++q) {
       double value = 0.0;
 #pragma unroll
-      for (int t = 0; t < 3; ++t) value += cdiff(MJ, 0, t, i, j, k) * cdiff(KA, q, t, i, j, k) * (1.0 / 12.0);
-      value += MJ(0, i, j, k) * KA(q, i, j, k) * 1.0;
-      R[q * c.vr.N] += value;
+      for (int t = 0; t < 3; ++t) value += dmj[t] * cdiff(KA, q, t, i, j, k) * (1.0 / 12.0);
+      value += mj0 * KA(q, i, j, k) * 1.0;
+      add[q] = value;
+      rv[q] = R[q * c.vr.N];
     }
+#pragma unroll
+    for (int q = 1; q < 8; ++q) R[q * c.vr.N] = rv[q] + add[q];
   });
 }
 
@@ -1175,6 +1229,11 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
       bool equal = true;
       for (int b = 0; b < nbox; ++b) {
         const long n = regionOf(B->host[(size_t)b * 3 + d], id).size();
+        if (n >= 0x7fffffffL) {  // forRegion splits indices in 32 bits
+          *err = cudaErrorInvalidValue;
+          o4BatchDestroy(B);
+          return nullptr;
+        }
         total += n;
         equal = equal && (b == 0 || n == largest);
         largest = n > largest ? n : largest;

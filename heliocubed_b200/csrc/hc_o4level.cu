@@ -52,13 +52,13 @@ __device__ __forceinline__ double volAt(const O4Level& O, int i) { return O.radi
 // 1. JU -> Cartesian averages, src/MHD_StateConversion.H:198-262.
 __global__ void o4CartesianKernel(const O4StageIO io) {
   const O4Level& O = io.O;
-  const long n = 6L * O.Nv;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int b = (int)(t / O.Nv);
-    const long r = t - (long)b * O.Nv;
-    const int i = (int)(r % O.nr);
-    const int j = (int)((r / O.nr) % O.na);
-    const int k = (int)(r / ((long)O.nr * O.na));
+  const unsigned n = (unsigned)(6L * O.Nv);
+  HC_LEVEL_LOOP(t, n) {
+    unsigned r = t;
+    const int i = (int)takeMod(r, O.nr);
+    const int j = (int)takeMod(r, O.na);
+    const int k = (int)takeMod(r, O.na);
+    const int b = (int)r;
     const int na = O.na;
     // Quotients use reciprocals of <det A> and dVolr (one rounding from the
     // reference's divisions).
@@ -92,6 +92,10 @@ __global__ void o4CartesianKernel(const O4StageIO io) {
     for (int q = 0; q < 3; ++q) invV[q] = 1.0 / volAt(O, ia + q);
     const double dv = 0.5 * (volAt(O, i + 1) - volAt(O, i - 1));
     const int slot = i - ia;
+    // all loads before the first store (the compiler cannot tell ju and
+    // cart apart, so interleaved stores would serialise the components)
+    double res[8];
+#pragma unroll
     for (int c = 0; c < 8; ++c) {
       double dq = 0.0, angI = 0.0;
 #pragma unroll
@@ -107,8 +111,10 @@ __global__ void o4CartesianKernel(const O4StageIO io) {
         dq += wr[q] * (ang * invV[q]);
         if (q == slot) angI = ang;
       }
-      io.cart[cIdx(O, b, c, i, j, k)] = (angI - dq * dv * (1.0 / 12.0)) * invV[slot];
+      res[c] = (angI - dq * dv * (1.0 / 12.0)) * invV[slot];
     }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) io.cart[cIdx(O, b, c, i, j, k)] = res[c];
   }
 }
 
@@ -117,12 +123,12 @@ __global__ void o4CartesianKernel(const O4StageIO io) {
 // the 4 x 4 donor cell averages, evaluated at the point.
 __global__ void o4SeamPointKernel(const O4StageIO io) {
   const O4Level& O = io.O;
-  const long n = 6L * O.npts * O.nr;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % O.nr);
-    const long q = t / O.nr;
-    const int pt = (int)(q % O.npts);
-    const int b = (int)(q / O.npts);
+  const unsigned n = (unsigned)(6L * O.npts * O.nr);
+  HC_LEVEL_LOOP(t, n) {
+    unsigned q = t;
+    const int i = (int)takeMod(q, O.nr);
+    const int pt = (int)takeMod(q, O.npts);
+    const int b = (int)q;
     const O4Point P = O.pts[(long)b * O.npts + pt];
     double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -152,12 +158,12 @@ __global__ void o4SeamPointKernel(const O4StageIO io) {
 // 1382-1391).
 __global__ void o4SeamKernel(const O4StageIO io) {
   const O4Level& O = io.O;
-  const long n = 6L * O.nring * O.nr;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % O.nr);
-    const long q = t / O.nr;
-    const int pos = (int)(q % O.nring);
-    const int b = (int)(q / O.nring);
+  const unsigned n = (unsigned)(6L * O.nring * O.nr);
+  HC_LEVEL_LOOP(t, n) {
+    unsigned q = t;
+    const int i = (int)takeMod(q, O.nr);
+    const int pos = (int)takeMod(q, O.nring);
+    const int b = (int)q;
     const int2 jk = O.ringJK[pos];
     const int* pt = O.ringPt + (long)pos * 5;
     const double* pv = io.pv + (long)b * 8 * O.npts * O.nr + i;
@@ -247,14 +253,13 @@ __device__ void nativeCell(const O4Level& O, const double* __restrict__ cart, in
 __global__ void o4NativeKernel(const O4StageIO io) {
   const O4Level& O = io.O;
   const int n0 = O.nr + 2 * O.g;
-  const long n = 6L * n0 * O.nG * O.nG;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % n0) - O.g;
-    long q = t / n0;
-    const int j = (int)(q % O.nG) - O.g;
-    q /= O.nG;
-    const int k = (int)(q % O.nG) - O.g;
-    const int b = (int)(q / O.nG);
+  const unsigned n = (unsigned)(6L * n0 * O.nG * O.nG);
+  HC_LEVEL_LOOP(t, n) {
+    unsigned q = t;
+    const int i = (int)takeMod(q, n0) - O.g;
+    const int j = (int)takeMod(q, O.nG) - O.g;
+    const int k = (int)takeMod(q, O.nG) - O.g;
+    const int b = (int)q;
     double u[8];
     if (i < 0) {
       const long cell = ((long)b * O.nG + (k + O.g)) * O.nG + (j + O.g);
@@ -315,14 +320,13 @@ __global__ void o4UpdateKernel(const O4Level O, int stage, const double* __restr
 __global__ void o4RefluxKernel(const O4Level O, const DevLevel L, int ax, const double* __restrict__ reg,
                                double* __restrict__ ju) {
   const long nrna = (long)O.na * O.nr;
-  const long n = 6L * 2 * nrna;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % O.nr);
-    long q = t / O.nr;
-    const int s = (int)(q % O.na);
-    q /= O.na;
-    const int side = (int)(q % 2);
-    const int b = (int)(q / 2);
+  const unsigned n = (unsigned)(6L * 2 * nrna);
+  HC_LEVEL_LOOP(t, n) {
+    unsigned q = t;
+    const int i = (int)takeMod(q, O.nr);
+    const int s = (int)takeMod(q, O.na);
+    const int side = (int)(q & 1u);
+    const int b = (int)(q >> 1);
     const int e = (ax - 1) * 2 + side;
     const EdgeLink nb = L.edge[b * 4 + e];
     const int sn = L.faceMap[((long)b * 4 + e) * O.na + s];
@@ -343,8 +347,16 @@ __global__ void o4RefluxKernel(const O4Level O, const DevLevel L, int ax, const 
 
 }  // namespace
 
+// Every flat index range of the level kernels fits in 31 bits.
+bool levelIndexable(const O4Level& O) {
+  const long lim = 0x7fffffffL;
+  return 6L * (O.nr + 2 * O.g) * O.nG * O.nG < lim && 6L * O.Nv < lim && 6L * O.npts * O.nr < lim &&
+         6L * O.nring * O.nr < lim && 12L * O.na * O.nr < lim;
+}
+
 cudaError_t launchO4Prepare(const O4StageIO& io, cudaStream_t s) {
   const O4Level& O = io.O;
+  if (!levelIndexable(O)) return cudaErrorInvalidValue;
   o4CartesianKernel<<<blocksFor(6L * O.Nv), kThreads, 0, s>>>(io);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -363,6 +375,7 @@ cudaError_t launchO4Update(const O4Level& O, int stage, const double* k, double*
 }
 
 cudaError_t launchO4Reflux(const O4Level& O, const DevLevel& L, const double* reg, double* ju, cudaStream_t s) {
+  if (!levelIndexable(O)) return cudaErrorInvalidValue;
   for (int ax = 1; ax <= 2; ++ax) {
     o4RefluxKernel<<<blocksFor(6L * 2 * O.na * O.nr), kThreads, 0, s>>>(O, L, ax, reg, ju);
     const cudaError_t e = cudaGetLastError();

@@ -499,7 +499,6 @@ __global__ void o4PointKernel(const Ctx* __restrict__ tab, const RegArgs rg, con
       t = dmin(t, R[roff(c.gr, i, j, k - 1)]);
       t = dmin(t, R[roff(c.gr, i, j, k + 1)]);
     }
-    a.th[(long)b * N + o] = t;
     const bool inner = i >= c.GR.lo[0] && i <= c.GR.hi[0] && j >= c.GR.lo[1] && j <= c.GR.hi[1] &&
                        k >= c.GR.lo[2] && k <= c.GR.hi[2];
     View U{a.U + b * a.uStride, a.ur};
@@ -510,6 +509,9 @@ __global__ void o4PointKernel(const Ctx* __restrict__ tab, const RegArgs rg, con
     double* W = a.WP + (long)b * 8 * N + o;
 #pragma unroll
     for (int q = 0; q < 8; ++q) W[q * N] = w[q];
+    // stored last: a store ahead of the state loads would hold them back
+    // until the dilation's loads return
+    a.th[(long)b * N + o] = t;
   });
 }
 
@@ -836,15 +838,25 @@ __global__ void __launch_bounds__(128, MB) o4FaceFinalKernel(const Ctx* __restri
       // point-to-average and transverse differences of the eight point
       // dissipations in a rolled loop through this thread's shared column
       __shared__ double sQ[24][128];
-      // (the five values of a component are loaded once: lapFace and cdiff
-      // restated on them, so the stores to the column cannot force reloads)
+      // (the five values of a component are loaded once, lapFace and cdiff
+      // restated on them; the next component's five are loaded while this
+      // one is processed, since the loop's stores to the column keep the
+      // compiler from moving loads above them)
       int m1[3] = {i, j, k}, p1[3] = {i, j, k}, m2[3] = {i, j, k}, p2[3] = {i, j, k};
       m1[t1] -= 1; p1[t1] += 1; m2[t2] -= 1; p2[t2] += 1;
+      double nx[5];
+      auto loadQ = [&](int q) {
+        nx[0] = QD(q, i, j, k);
+        nx[1] = QD(q, m1[0], m1[1], m1[2]);
+        nx[2] = QD(q, p1[0], p1[1], p1[2]);
+        nx[3] = QD(q, m2[0], m2[1], m2[2]);
+        nx[4] = QD(q, p2[0], p2[1], p2[2]);
+      };
+      loadQ(0);
 #pragma unroll 1
       for (int q = 0; q < 8; ++q) {
-        const double pt = QD(q, i, j, k);
-        const double a1 = QD(q, m1[0], m1[1], m1[2]), b1 = QD(q, p1[0], p1[1], p1[2]);
-        const double a2 = QD(q, m2[0], m2[1], m2[2]), b2 = QD(q, p2[0], p2[1], p2[2]);
+        const double pt = nx[0], a1 = nx[1], b1 = nx[2], a2 = nx[3], b2 = nx[4];
+        if (q < 7) loadQ(q + 1);
         const double lap = (a1 + b1) + (a2 + b2) - 4.0 * pt;
         sQ[q][threadIdx.x] = sm ? pt + lap * (1.0 / 24.0) : pt;
         sQ[8 + q][threadIdx.x] = 0.5 * b1 - 0.5 * a1;

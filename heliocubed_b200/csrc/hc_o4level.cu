@@ -92,11 +92,15 @@ __global__ void o4CartesianKernel(const O4StageIO io) {
     for (int q = 0; q < 3; ++q) invV[q] = 1.0 / volAt(O, ia + q);
     const double dv = 0.5 * (volAt(O, i + 1) - volAt(O, i - 1));
     const int slot = i - ia;
+    // JU addressed from the box's base with fixed strides (component, j, k)
+    const long sv = O.Nv, sj = O.nr, sk = (long)O.nr * O.na;
+    const double* U0 = io.ju + (long)b * 8 * sv;
     // all loads before the first store (the compiler cannot tell ju and
     // cart apart, so interleaved stores would serialise the components)
     double res[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
+      const double* Uc = U0 + c * sv;
       double dq = 0.0, angI = 0.0;
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
@@ -104,10 +108,10 @@ __global__ void o4CartesianKernel(const O4StageIO io) {
         double d1 = 0.0, d2 = 0.0;
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-          d1 += wj[m] * (io.ju[vIdx(O, b, c, ii, ja + m, k)] * invJ[m]);
-          d2 += wk[m] * (io.ju[vIdx(O, b, c, ii, j, ka + m)] * invK[m]);
+          d1 += wj[m] * (Uc[ii + (ja + m) * sj + k * sk] * invJ[m]);
+          d2 += wk[m] * (Uc[ii + j * sj + (ka + m) * sk] * invK[m]);
         }
-        const double ang = (io.ju[vIdx(O, b, c, ii, j, k)] - (d1 * dd1 + d2 * dd2) * (1.0 / 12.0)) * invDet;
+        const double ang = (Uc[ii + j * sj + k * sk] - (d1 * dd1 + d2 * dd2) * (1.0 / 12.0)) * invDet;
         dq += wr[q] * (ang * invV[q]);
         if (q == slot) angI = ang;
       }
@@ -130,15 +134,18 @@ __global__ void o4SeamPointKernel(const O4StageIO io) {
     const int pt = (int)takeMod(q, O.npts);
     const int b = (int)q;
     const O4Point P = O.pts[(long)b * O.npts + pt];
+    // donors addressed from one base with fixed strides (j, k, component)
+    const long sj = O.nr, sk = (long)O.nr * O.nA, sc = O.Nc;
+    const double* base = io.cart + cIdx(O, P.p, 0, i, P.j0, P.k0);
     double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk) {
       double row[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
-        const long base = cIdx(O, P.p, 0, i, P.j0 + m, P.k0 + kk);
+        const double* x = base + kk * sk + m * sj;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) row[c] += P.wj[m] * io.cart[base + (long)c * O.Nc];
+        for (int c = 0; c < 8; ++c) row[c] += P.wj[m] * x[c * sc];
       }
 #pragma unroll
       for (int c = 0; c < 8; ++c) v[c] += P.wk[kk] * row[c];
@@ -195,22 +202,31 @@ __global__ void o4SeamKernel(const O4StageIO io) {
 }
 
 // Native conversion of one cell (src/MHD_CachedCartesianConversion.H:65-124).
+// Every operand is addressed from one base pointer per array with fixed
+// strides (cell j +- 1, k +- 1, component), so the cell's ~150 loads share
+// one index computation.
 __device__ void nativeCell(const O4Level& O, const double* __restrict__ cart, int b, int i, int j, int k, double out[8]) {
+  const long sj = O.nr, sk = (long)O.nr * O.nA, sc = O.Nc;
+  const long cj = 27, ck = 27L * O.nA;
+  const double* c0 = cart + cIdx(O, b, 0, i, j, k);
   const double* cf = O.coef + (((long)b * O.nA + (k + O.ga)) * O.nA + (j + O.ga)) * 27;
-  out[0] = cart[cIdx(O, b, 0, i, j, k)];
-  out[4] = cart[cIdx(O, b, 4, i, j, k)];
+  out[0] = c0[0];
+  out[4] = c0[4 * sc];
+  // neighbours (j + 1), (j - 1), (k + 1), (k - 1)
+  const long nOff[4] = {sj, -sj, sk, -sk};
+  const long cOff[4] = {cj, -cj, ck, -ck};
 #pragma unroll
   for (int grp = 0; grp < 2; ++grp) {
     const int st = grp == 0 ? 1 : 5;
+    const double* cs = c0 + st * sc;
     double q[4][3];
-    const int nj[4] = {j + 1, j - 1, j, j};
-    const int nk[4] = {k, k, k + 1, k - 1};
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
-      const double* I = O.coef + (((long)b * O.nA + (nk[e] + O.ga)) * O.nA + (nj[e] + O.ga)) * 27;
-      const double x0 = cart[cIdx(O, b, st, i, nj[e], nk[e])];
-      const double x1 = cart[cIdx(O, b, st + 1, i, nj[e], nk[e])];
-      const double x2 = cart[cIdx(O, b, st + 2, i, nj[e], nk[e])];
+      const double* I = cf + cOff[e];
+      const double* x = cs + nOff[e];
+      const double x0 = x[0];
+      const double x1 = x[sc];
+      const double x2 = x[2 * sc];
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
         double v = 0.0;
@@ -237,7 +253,7 @@ __device__ void nativeCell(const O4Level& O, const double* __restrict__ cart, in
       double correction = 0.0;
       correction += first;
       correction += second;
-      corrected[r] = cart[cIdx(O, b, st + r, i, j, k)] + correction;
+      corrected[r] = cs[r * sc] + correction;
     }
 #pragma unroll
     for (int r = 0; r < 3; ++r) {

@@ -39,8 +39,12 @@ __host__ __device__ inline Reg regOf(const Box3& b) {
   return r;
 }
 
+// Offset of (i, j, k) in an array laid out on region r.  Every array of a
+// box holds fewer than 2^31 points per component (o4BatchCreate rejects
+// larger boxes), so the offset is formed in 32-bit arithmetic, which the
+// compiler shares between the neighbours of a stencil.
 __device__ __forceinline__ long roff(const Reg& r, int i, int j, int k) {
-  return (long)(i - r.lo[0]) + (long)r.n[0] * ((long)(j - r.lo[1]) + (long)r.n[1] * (long)(k - r.lo[2]));
+  return (long)((i - r.lo[0]) + r.n[0] * ((j - r.lo[1]) + r.n[1] * (k - r.lo[2])));
 }
 
 // Offsets of the face arrays inside a box's face scratch (units of F.N).
@@ -1223,6 +1227,11 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
     *err = cudaErrorInvalidValue;
     return nullptr;
   }
+  for (int b = 0; b < nbox; ++b)
+    if (boxes[b].ur.N >= 0x7fffffffL) {  // roff forms offsets in 32 bits
+      *err = cudaErrorInvalidValue;
+      return nullptr;
+    }
   O4Batch* B = new O4Batch;
   B->nbox = nbox;
   B->host.resize((size_t)nbox * 3);

@@ -51,6 +51,8 @@ def test_struct_layouts_match_header(product_lib_path):
     ({"temporal_order": 2}, -3), ({"nr": 2}, -1), ({"gamma": 1.0}, -1), ({"init_condition_type": 0}, -3),
     ({"spatial_order": 4, "spatial_operator": 1}, -3), ({"spatial_order": 4, "berta_detector_type": 1}, -3),
     ({"spatial_order": 4, "berta_fallback_type": 2}, -1), ({"spatial_order": 4}, -1),  # na = 8 < 16
+    # 48 (nr + 12)(na + 12)^2 >= 2^31: the level kernels index in 32 bits
+    ({"nr": 4096, "na": 1024}, -1),
 ])
 def test_bad_options_rejected(product_lib_path, fields, code):
     from heliocubed_b200 import _native

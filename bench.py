@@ -315,12 +315,19 @@ def run_b200(args, world, rank, local):
                   "tile_fields": "cells x, y, z, min CTAs/SM Rusanov, Roe"}
     else:
         from heliocubed_b200.level import o4_variants
-        var, vms = shell.autotune(ju0)
         mb = o4_variants()
         names = ("reconstruction", "roe_point", "final_flux")
-        tuning = {"min_ctas_per_sm": {n: int(mb[q, var[q]]) for q, n in enumerate(names)},
-                  "candidates": {n: [int(x) for x in mb[q]] for q, n in enumerate(names)},
-                  "operator_ms": {n: [round(float(x), 4) for x in vms[q]] for q, n in enumerate(names)}}
+        if args.o4_variants:
+            # fixed variants (profiling: timings taken under a profiler would
+            # steer the tuner to a different choice than the plain run's)
+            var = [int(x) for x in args.o4_variants.split(",")]
+            shell.set_o4_variants(*var)
+            tuning = {"min_ctas_per_sm": {n: int(mb[q, var[q]]) for q, n in enumerate(names)}, "fixed": True}
+        else:
+            var, vms = shell.autotune(ju0)
+            tuning = {"min_ctas_per_sm": {n: int(mb[q, var[q]]) for q, n in enumerate(names)},
+                      "candidates": {n: [int(x) for x in mb[q]] for q, n in enumerate(names)},
+                      "operator_ms": {n: [round(float(x), 4) for x in vms[q]] for q, n in enumerate(names)}}
     time_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
     state_bytes = ju.numel() * 8
@@ -664,6 +671,9 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="launch the step eagerly instead of replaying a captured CUDA graph")
+    ap.add_argument("--o4-variants", default=None, metavar="R,P,F",
+                    help="order 4: use these register-cap variants of the reconstruction, Roe point and final-flux "
+                         "kernels instead of timing them (for profiler runs)")
     ap.add_argument("--cpu-max-steps", type=int, default=60)
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--serve", action="store_true", help="run the served-ensemble benchmark instead")

@@ -840,38 +840,38 @@ __global__ void __launch_bounds__(128, MB) o4FaceFinalKernel(const Ctx* __restri
         for (int e = 0; e < 10; ++e) dM[q][e] = 0.5 * Ma[e] - 0.5 * Mb[e];
       }
       // point-to-average and transverse differences of the eight point
-      // dissipations in a rolled loop through this thread's shared column
-      __shared__ double sQ[24][128];
-      // (the five values of a component are loaded once, lapFace and cdiff
-      // restated on them; the next component's five are loaded while this
-      // one is processed, since the loop's stores to the column keep the
-      // compiler from moving loads above them)
-      int m1[3] = {i, j, k}, p1[3] = {i, j, k}, m2[3] = {i, j, k}, p2[3] = {i, j, k};
-      m1[t1] -= 1; p1[t1] += 1; m2[t2] -= 1; p2[t2] += 1;
-      double nx[5];
-      auto loadQ = [&](int q) {
-        nx[0] = QD(q, i, j, k);
-        nx[1] = QD(q, m1[0], m1[1], m1[2]);
-        nx[2] = QD(q, p1[0], p1[1], p1[2]);
-        nx[3] = QD(q, m2[0], m2[1], m2[2]);
-        nx[4] = QD(q, p2[0], p2[1], p2[2]);
-      };
-      loadQ(0);
-#pragma unroll 1
-      for (int q = 0; q < 8; ++q) {
-        const double pt = nx[0], a1 = nx[1], b1 = nx[2], a2 = nx[3], b2 = nx[4];
-        if (q < 7) loadQ(q + 1);
-        const double lap = (a1 + b1) + (a2 + b2) - 4.0 * pt;
-        sQ[q][threadIdx.x] = sm ? pt + lap * (1.0 / 24.0) : pt;
-        sQ[8 + q][threadIdx.x] = 0.5 * b1 - 0.5 * a1;
-        sQ[16 + q][threadIdx.x] = 0.5 * b2 - 0.5 * a2;
+      // dissipations.  Their 40 inputs (8 components x the face and its four
+      // transverse neighbours) are copied into this thread's shared column
+      // with asynchronous copies, all in flight at once: the gathers from
+      // the face scratch are this kernel's bound, and loads into registers
+      // would be issued a few at a time under the register cap.
+      __shared__ double sRaw[40][128];
+      {
+        int m1[3] = {i, j, k}, p1[3] = {i, j, k}, m2[3] = {i, j, k}, p2[3] = {i, j, k};
+        m1[t1] -= 1; p1[t1] += 1; m2[t2] -= 1; p2[t2] += 1;
+        const long off[5] = {roff(QD.r, i, j, k), roff(QD.r, m1[0], m1[1], m1[2]), roff(QD.r, p1[0], p1[1], p1[2]),
+                             roff(QD.r, m2[0], m2[1], m2[2]), roff(QD.r, p2[0], p2[1], p2[2])};
+        const unsigned col = (unsigned)__cvta_generic_to_shared(&sRaw[0][threadIdx.x]);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+#pragma unroll
+          for (int e = 0; e < 5; ++e) {
+            const size_t src = __cvta_generic_to_global(QD.p + q * QD.r.N + off[e]);
+            const unsigned dst = col + (unsigned)((q * 5 + e) * 128 * sizeof(double));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+          }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
       }
       double avg[8], dP0[8], dP1[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        avg[q] = sQ[q][threadIdx.x];
-        dP0[q] = sQ[8 + q][threadIdx.x];
-        dP1[q] = sQ[16 + q][threadIdx.x];
+        const double pt = sRaw[q * 5][threadIdx.x], a1 = sRaw[q * 5 + 1][threadIdx.x], b1 = sRaw[q * 5 + 2][threadIdx.x];
+        const double a2 = sRaw[q * 5 + 3][threadIdx.x], b2 = sRaw[q * 5 + 4][threadIdx.x];
+        const double lap = (a1 + b1) + (a2 + b2) - 4.0 * pt;
+        avg[q] = sm ? pt + lap * (1.0 / 24.0) : pt;
+        dP0[q] = 0.5 * b1 - 0.5 * a1;
+        dP1[q] = 0.5 * b2 - 0.5 * a2;
       }
       diss[0] = faceProd(M[9], avg[0], dM[0][9], dP0[0], dM[1][9], dP1[0]);
       diss[4] = faceProd(M[9], avg[4], dM[0][9], dP0[4], dM[1][9], dP1[4]);
@@ -1209,8 +1209,9 @@ struct O4Batch {
 
 // Minimum resident CTAs per SM (the register cap) of each variant of the
 // tuned kernels: reconstruction, Roe point dissipation, final flux.
-// Variant 0 is the default.
-constexpr int kO4MinBlocks[kO4TunedKernels][kO4Variants] = {{6, 4, 8}, {4, 3, 5}, {6, 4, 8}};
+// Variant 0 is the default.  The final flux's 40 KB shared staging column
+// admits at most 5 CTAs per SM, so its caps stay at or below 5.
+constexpr int kO4MinBlocks[kO4TunedKernels][kO4Variants] = {{6, 4, 8}, {4, 3, 5}, {4, 5, 3}};
 
 void o4BatchSetVariants(O4Batch* B, const int v[kO4TunedKernels]) {
   for (int q = 0; q < kO4TunedKernels; ++q) B->var[q] = v[q] >= 0 && v[q] < kO4Variants ? v[q] : 0;

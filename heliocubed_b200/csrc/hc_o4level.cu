@@ -50,7 +50,9 @@ __device__ __forceinline__ double detAt(const O4Level& O, int b, int j, int k) {
 __device__ __forceinline__ double volAt(const O4Level& O, int i) { return O.radial[i + O.g + 1].x; }
 
 // 1. JU -> Cartesian averages, src/MHD_StateConversion.H:198-262.
-__global__ void o4CartesianKernel(const O4StageIO io) {
+// Capped at 102 registers (5 CTAs of 128 threads per SM): the unrolled
+// component loop would otherwise take 128 and hold occupancy at 4 CTAs.
+__global__ void __launch_bounds__(128, 5) o4CartesianKernel(const O4StageIO io) {
   const O4Level& O = io.O;
   const unsigned n = (unsigned)(6L * O.Nv);
   HC_LEVEL_LOOP(t, n) {

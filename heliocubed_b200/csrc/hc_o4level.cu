@@ -127,34 +127,31 @@ __global__ void __launch_bounds__(128, 5) o4CartesianKernel(const O4StageIO io) 
 // 2a. Point values of the Cartesian averages at the interpolation points
 // (ghost centres and their neighbours): the tensor-product cubic matching
 // the 4 x 4 donor cell averages, evaluated at the point.
+// One thread per (radial cell, component, point): the 16 donor loads of a
+// component are independent of the other components', so splitting them
+// over threads puts more of them in flight than a thread's registers hold.
 __global__ void o4SeamPointKernel(const O4StageIO io) {
   const O4Level& O = io.O;
-  const unsigned n = (unsigned)(6L * O.npts * O.nr);
+  const unsigned n = (unsigned)(6L * 8 * O.npts * O.nr);
   HC_LEVEL_LOOP(t, n) {
     unsigned q = t;
     const int i = (int)takeMod(q, O.nr);
+    const int c = (int)takeMod(q, 8);
     const int pt = (int)takeMod(q, O.npts);
     const int b = (int)q;
-    const O4Point P = O.pts[(long)b * O.npts + pt];
-    // donors addressed from one base with fixed strides (j, k, component)
-    const long sj = O.nr, sk = (long)O.nr * O.nA, sc = O.Nc;
-    const double* base = io.cart + cIdx(O, P.p, 0, i, P.j0, P.k0);
-    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const O4Point& P = O.pts[(long)b * O.npts + pt];
+    // donors addressed from one base with fixed strides (j, k)
+    const long sj = O.nr, sk = (long)O.nr * O.nA;
+    const double* base = io.cart + cIdx(O, P.p, c, i, P.j0, P.k0);
+    double v = 0.0;
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk) {
-      double row[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      double row = 0.0;
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const double* x = base + kk * sk + m * sj;
-#pragma unroll
-        for (int c = 0; c < 8; ++c) row[c] += P.wj[m] * x[c * sc];
-      }
-#pragma unroll
-      for (int c = 0; c < 8; ++c) v[c] += P.wk[kk] * row[c];
+      for (int m = 0; m < 4; ++m) row += P.wj[m] * base[kk * sk + m * sj];
+      v += P.wk[kk] * row;
     }
-    double* out = io.pv + ((long)b * 8 * O.npts + pt) * O.nr + i;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) out[(long)c * O.npts * O.nr] = v[c];
+    io.pv[(((long)b * 8 + c) * O.npts + pt) * O.nr + i] = v;
   }
 }
 
@@ -368,7 +365,7 @@ __global__ void o4RefluxKernel(const O4Level O, const DevLevel L, int ax, const 
 // Every flat index range of the level kernels fits in 31 bits.
 bool levelIndexable(const O4Level& O) {
   const long lim = 0x7fffffffL;
-  return 6L * (O.nr + 2 * O.g) * O.nG * O.nG < lim && 6L * O.Nv < lim && 6L * O.npts * O.nr < lim &&
+  return 6L * (O.nr + 2 * O.g) * O.nG * O.nG < lim && 6L * O.Nv < lim && 48L * O.npts * O.nr < lim &&
          6L * O.nring * O.nr < lim && 12L * O.na * O.nr < lim;
 }
 
@@ -378,7 +375,7 @@ cudaError_t launchO4Prepare(const O4StageIO& io, cudaStream_t s) {
   o4CartesianKernel<<<blocksFor(6L * O.Nv), kThreads, 0, s>>>(io);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  o4SeamPointKernel<<<blocksFor(6L * O.npts * O.nr), kThreads, 0, s>>>(io);
+  o4SeamPointKernel<<<blocksFor(6L * 8 * O.npts * O.nr), kThreads, 0, s>>>(io);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   o4SeamKernel<<<blocksFor(6L * O.nring * O.nr), kThreads, 0, s>>>(io);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -1205,6 +1205,11 @@ struct O4Batch {
   long chunkOff[RG_COUNT][3] = {};
   int chunkCount[RG_COUNT][3] = {};
   int var[kO4TunedKernels] = {0, 0, 0};  // register-cap variant of the tuned kernels
+  // The Powell face chain of a direction (face flux, radial product,
+  // divergence into -J div B) runs on a side stream beside the main face
+  // chain: fork after the reconstruction, join before the next direction.
+  cudaStream_t side = nullptr;
+  cudaEvent_t forkEv[3] = {}, joinEv[3] = {};
 };
 
 // Minimum resident CTAs per SM (the register cap) of each variant of the
@@ -1290,6 +1295,13 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
     if (*err == cudaSuccess)
       *err = cudaMemcpy(B->chunks, work.data(), sizeof(WorkChunk) * work.size(), cudaMemcpyHostToDevice);
   }
+  if (*err == cudaSuccess && B->powell) {
+    *err = cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking);
+    for (int d = 0; d < 3 && *err == cudaSuccess; ++d) {
+      *err = cudaEventCreateWithFlags(&B->forkEv[d], cudaEventDisableTiming);
+      if (*err == cudaSuccess) *err = cudaEventCreateWithFlags(&B->joinEv[d], cudaEventDisableTiming);
+    }
+  }
   if (*err != cudaSuccess) {
     o4BatchDestroy(B);
     return nullptr;
@@ -1301,6 +1313,11 @@ void o4BatchDestroy(O4Batch* B) {
   if (!B) return;
   if (B->dev) cudaFree(B->dev);
   if (B->chunks) cudaFree(B->chunks);
+  for (int d = 0; d < 3; ++d) {
+    if (B->forkEv[d]) cudaEventDestroy(B->forkEv[d]);
+    if (B->joinEv[d]) cudaEventDestroy(B->joinEv[d]);
+  }
+  if (B->side) cudaStreamDestroy(B->side);
   delete B;
 }
 
@@ -1340,10 +1357,11 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
   const RegArgs rg = reg ? *reg : none;
   const Ctx* t = B->dev;
   cudaError_t e;
-#define HC_LAUNCH(kernel, d, region)                                                          \
-  if (B->chunkCount[region][d]) {                                                             \
-    kernel<<<B->chunkCount[region][d], 128, 0, s>>>(t, rg, B->chunks + B->chunkOff[region][d]); \
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;                                    \
+  cudaStream_t st = s;  // the stream the macros below launch on
+#define HC_LAUNCH(kernel, d, region)                                                           \
+  if (B->chunkCount[region][d]) {                                                              \
+    kernel<<<B->chunkCount[region][d], 128, 0, st>>>(t, rg, B->chunks + B->chunkOff[region][d]); \
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;                                     \
   }
 #define HC_LAUNCH_D(kernel, region)                                                      \
   if (d == 0) { HC_LAUNCH(kernel<0>, 0, region) }                                       \
@@ -1353,10 +1371,10 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
   if (B->var[q] == 1) { HC_LAUNCH_DV(kernel, kO4MinBlocks[q][1], region) }                \
   else if (B->var[q] == 2) { HC_LAUNCH_DV(kernel, kO4MinBlocks[q][2], region) }           \
   else { HC_LAUNCH_DV(kernel, kO4MinBlocks[q][0], region) }
-#define HC_LAUNCH_T(d, region, ...)                                                               \
-  if (B->chunkCount[region][d]) {                                                                 \
-    __VA_ARGS__<<<B->chunkCount[region][d], 128, 0, s>>>(t, rg, B->chunks + B->chunkOff[region][d]); \
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;                                        \
+#define HC_LAUNCH_T(d, region, ...)                                                                \
+  if (B->chunkCount[region][d]) {                                                                  \
+    __VA_ARGS__<<<B->chunkCount[region][d], 128, 0, st>>>(t, rg, B->chunks + B->chunkOff[region][d]); \
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;                                         \
   }
 #define HC_LAUNCH_DV(kernel, mb, region)                                                 \
   if (d == 0) { HC_LAUNCH_T(0, region, kernel<0, mb>) }                                 \
@@ -1367,17 +1385,26 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
   HC_LAUNCH(o4PointKernel, 0, RG_G)
   for (int d = 0; d < 3; ++d) {
     HC_LAUNCH_DM(o4FaceReconKernel, 0, RG_F)
+    if (B->powell) {
+      // the Powell chain reads the reconstruction's flags and normal B and
+      // writes only its own face arrays and -J div B: fork it
+      if ((e = cudaEventRecord(B->forkEv[d], s)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(B->side, B->forkEv[d], 0)) != cudaSuccess) return e;
+      st = B->side;
+      HC_LAUNCH_D(o4PowellFluxKernel, RG_PF)
+      HC_LAUNCH_D(o4PowellProdKernel, RG_PP)
+      HC_LAUNCH_D(o4PowellDivKernel, RG_V1)
+      st = s;
+      if ((e = cudaEventRecord(B->joinEv[d], B->side)) != cudaSuccess) return e;
+    }
     if (B->roe) { HC_LAUNCH_DM(o4RoePointKernel, 1, RG_PB) }
     HC_LAUNCH_D(o4FaceAvgKernel, RG_F1)
     HC_LAUNCH_D(o4FaceMapKernel, RG_F)
     HC_LAUNCH_D(o4FaceRadialKernel, RG_F1)
     HC_LAUNCH_DM(o4FaceFinalKernel, 2, RG_V0)
     HC_LAUNCH_D(o4DivKernel, RG_V)
-    if (B->powell) {
-      HC_LAUNCH_D(o4PowellFluxKernel, RG_PF)
-      HC_LAUNCH_D(o4PowellProdKernel, RG_PP)
-      HC_LAUNCH_D(o4PowellDivKernel, RG_V1)
-    }
+    // join before the next direction's reconstruction rewrites the flags
+    if (B->powell && (e = cudaStreamWaitEvent(s, B->joinEv[d], 0)) != cudaSuccess) return e;
   }
   if (B->powell) {
     HC_LAUNCH(o4PowellCoefKernel, 0, RG_V2)

@@ -1208,8 +1208,10 @@ struct O4Batch {
   // The Powell face chain of a direction (face flux, radial product,
   // divergence into -J div B) runs on a side stream beside the main face
   // chain: fork after the reconstruction, join before the next direction.
+  // The cell-product coefficients and their averages (DivBPowell2's
+  // inputs, from the point primitives) go first on the same side stream.
   cudaStream_t side = nullptr;
-  cudaEvent_t forkEv[3] = {}, joinEv[3] = {};
+  cudaEvent_t pointEv = nullptr, forkEv[3] = {}, joinEv[3] = {};
 };
 
 // Minimum resident CTAs per SM (the register cap) of each variant of the
@@ -1297,6 +1299,7 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
   }
   if (*err == cudaSuccess && B->powell) {
     *err = cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking);
+    if (*err == cudaSuccess) *err = cudaEventCreateWithFlags(&B->pointEv, cudaEventDisableTiming);
     for (int d = 0; d < 3 && *err == cudaSuccess; ++d) {
       *err = cudaEventCreateWithFlags(&B->forkEv[d], cudaEventDisableTiming);
       if (*err == cudaSuccess) *err = cudaEventCreateWithFlags(&B->joinEv[d], cudaEventDisableTiming);
@@ -1313,6 +1316,7 @@ void o4BatchDestroy(O4Batch* B) {
   if (!B) return;
   if (B->dev) cudaFree(B->dev);
   if (B->chunks) cudaFree(B->chunks);
+  if (B->pointEv) cudaEventDestroy(B->pointEv);
   for (int d = 0; d < 3; ++d) {
     if (B->forkEv[d]) cudaEventDestroy(B->forkEv[d]);
     if (B->joinEv[d]) cudaEventDestroy(B->joinEv[d]);
@@ -1383,6 +1387,16 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
   HC_LAUNCH(o4PrimAvgKernel, 0, RG_G)
   HC_LAUNCH(o4ThetaRawKernel, 0, RG_GR)
   HC_LAUNCH(o4PointKernel, 0, RG_G)
+  if (B->powell) {
+    // DivBPowell2's coefficients need only the point primitives: fork them
+    // (the side stream runs them before the first direction's Powell chain)
+    if ((e = cudaEventRecord(B->pointEv, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(B->side, B->pointEv, 0)) != cudaSuccess) return e;
+    st = B->side;
+    HC_LAUNCH(o4PowellCoefKernel, 0, RG_V2)
+    HC_LAUNCH(o4PowellAvgKernel, 0, RG_V1)
+    st = s;
+  }
   for (int d = 0; d < 3; ++d) {
     HC_LAUNCH_DM(o4FaceReconKernel, 0, RG_F)
     if (B->powell) {
@@ -1406,11 +1420,8 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
     // join before the next direction's reconstruction rewrites the flags
     if (B->powell && (e = cudaStreamWaitEvent(s, B->joinEv[d], 0)) != cudaSuccess) return e;
   }
-  if (B->powell) {
-    HC_LAUNCH(o4PowellCoefKernel, 0, RG_V2)
-    HC_LAUNCH(o4PowellAvgKernel, 0, RG_V1)
-    HC_LAUNCH(o4PowellApplyKernel, 0, RG_V)
-  }
+  // after the last join: -J div B complete, coefficients averaged
+  if (B->powell) { HC_LAUNCH(o4PowellApplyKernel, 0, RG_V) }
 #undef HC_LAUNCH_DV
 #undef HC_LAUNCH_T
 #undef HC_LAUNCH_DM

@@ -1212,6 +1212,12 @@ struct O4Batch {
   // inputs, from the point primitives) go first on the same side stream.
   cudaStream_t side = nullptr;
   cudaEvent_t pointEv = nullptr, forkEv[3] = {}, joinEv[3] = {};
+  // The Roe point dissipation (reads the face states, writes only the
+  // dissipation) runs on a second side stream beside the face-average,
+  // mapped-flux and radial-product kernels, which do not read it; the final
+  // flux waits for it.
+  cudaStream_t roeSide = nullptr;
+  cudaEvent_t roeFork[3] = {}, roeJoin[3] = {};
 };
 
 // Minimum resident CTAs per SM (the register cap) of each variant of the
@@ -1297,6 +1303,13 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
     if (*err == cudaSuccess)
       *err = cudaMemcpy(B->chunks, work.data(), sizeof(WorkChunk) * work.size(), cudaMemcpyHostToDevice);
   }
+  if (*err == cudaSuccess && B->roe) {
+    *err = cudaStreamCreateWithFlags(&B->roeSide, cudaStreamNonBlocking);
+    for (int d = 0; d < 3 && *err == cudaSuccess; ++d) {
+      *err = cudaEventCreateWithFlags(&B->roeFork[d], cudaEventDisableTiming);
+      if (*err == cudaSuccess) *err = cudaEventCreateWithFlags(&B->roeJoin[d], cudaEventDisableTiming);
+    }
+  }
   if (*err == cudaSuccess && B->powell) {
     *err = cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking);
     if (*err == cudaSuccess) *err = cudaEventCreateWithFlags(&B->pointEv, cudaEventDisableTiming);
@@ -1318,10 +1331,13 @@ void o4BatchDestroy(O4Batch* B) {
   if (B->chunks) cudaFree(B->chunks);
   if (B->pointEv) cudaEventDestroy(B->pointEv);
   for (int d = 0; d < 3; ++d) {
+    if (B->roeFork[d]) cudaEventDestroy(B->roeFork[d]);
+    if (B->roeJoin[d]) cudaEventDestroy(B->roeJoin[d]);
     if (B->forkEv[d]) cudaEventDestroy(B->forkEv[d]);
     if (B->joinEv[d]) cudaEventDestroy(B->joinEv[d]);
   }
   if (B->side) cudaStreamDestroy(B->side);
+  if (B->roeSide) cudaStreamDestroy(B->roeSide);
   delete B;
 }
 
@@ -1411,10 +1427,18 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
       st = s;
       if ((e = cudaEventRecord(B->joinEv[d], B->side)) != cudaSuccess) return e;
     }
-    if (B->roe) { HC_LAUNCH_DM(o4RoePointKernel, 1, RG_PB) }
+    if (B->roe) {
+      if ((e = cudaEventRecord(B->roeFork[d], s)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(B->roeSide, B->roeFork[d], 0)) != cudaSuccess) return e;
+      st = B->roeSide;
+      HC_LAUNCH_DM(o4RoePointKernel, 1, RG_PB)
+      st = s;
+      if ((e = cudaEventRecord(B->roeJoin[d], B->roeSide)) != cudaSuccess) return e;
+    }
     HC_LAUNCH_D(o4FaceAvgKernel, RG_F1)
     HC_LAUNCH_D(o4FaceMapKernel, RG_F)
     HC_LAUNCH_D(o4FaceRadialKernel, RG_F1)
+    if (B->roe && (e = cudaStreamWaitEvent(s, B->roeJoin[d], 0)) != cudaSuccess) return e;
     HC_LAUNCH_DM(o4FaceFinalKernel, 2, RG_V0)
     HC_LAUNCH_D(o4DivKernel, RG_V)
     // join before the next direction's reconstruction rewrites the flags

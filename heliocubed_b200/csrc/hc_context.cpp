@@ -887,8 +887,9 @@ O4Args levelO4Args(hc_ctx* c, const double* us, double* k) {
   return a;
 }
 
-// The operator batch of an argument set, built on first use (a cudaMalloc
-// and a copy: not inside a stream capture) and kept for the next calls.
+// The operator batch of an argument set, built on first use (device
+// allocations, a copy, the batch's side streams and events: not inside a
+// stream capture) and kept for the next calls.
 O4Batch* cachedBatch(hc_ctx* c, const O4Args& a, int* rc) {
   std::string key;
   auto put = [&key](const void* p, size_t n) { key.append(static_cast<const char*>(p), n); };

@@ -51,6 +51,9 @@ SIGNATURES = {
     "hc_amr_restrict": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_amr_plan_set_reflux": (C.c_int, [_VP, _VP, C.c_int]),
     "hc_amr_reflux": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
+    "hc_amr_cf_weights": (C.c_int, [C.c_int, C.c_int, _VP]),
+    "hc_amr_plan_set_cf_interp": (C.c_int, [_VP, _VP, C.c_int]),
+    "hc_amr_cf_interpolate": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_ctx_set_o4_variants": (C.c_int, [_VP, _VP]),
     "hc_level_insert_cone": (C.c_int, [_VP, _VP, C.c_double, _VP, _VP, _VP]),
     "hc_cone_event": (C.c_int, [_VP, _VP]),
@@ -127,6 +130,13 @@ class HcRefluxBox(C.Structure):
                 ("coarse_n", C.c_int * 3), ("rhs_lo", C.c_int * 3), ("rhs_n", C.c_int * 3), ("lo", C.c_int * 3),
                 ("hi", C.c_int * 3), ("ratio", C.c_int * 3), ("dir", C.c_int), ("fine_side", C.c_int),
                 ("reserved", C.c_int), ("scale", C.c_double)]
+
+
+class HcCfBox(C.Structure):
+    """Mirror of hc_cf_box in include/hc_abi.h."""
+    _fields_ = [("coarse", C.c_void_p), ("fine", C.c_void_p), ("coarse_lo", C.c_int * 3), ("coarse_n", C.c_int * 3),
+                ("fine_lo", C.c_int * 3), ("fine_n", C.c_int * 3), ("valid_lo", C.c_int * 3),
+                ("valid_hi", C.c_int * 3), ("ratio", C.c_int * 3), ("ncomp", C.c_int)]
 
 
 class HcCmeEvent(C.Structure):

@@ -10,8 +10,10 @@
 // it, (scale * source) then the add, with explicit round-to-nearest
 // operations, so the results do not depend on multiply-add contraction.
 #include <cuda_runtime.h>
+#include <math_constants.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "../../include/hc_abi.h"
@@ -134,6 +136,72 @@ __global__ void __launch_bounds__(kThreads) refluxKernel(const hc_reflux_box* __
   }
 }
 
+// Coarse-fine ghost interpolation (src/MHD_AMRInterpolation.H:39-155,
+// applied by src/MHD_AMRFourthOrder.H:27-39).  One thread per fine storage
+// cell; the quartic average of the 5 x 5 x 5 coarse cells around the parent
+// is summed pass by pass as the reference's separable sweeps do (first
+// index, then second, then third; each in increasing index, zero weights
+// skipped), every product and sum rounded as written.
+constexpr int kCfMaxRatio = 8, kCfMaxComp = 16;
+struct CfItem {
+  hc_cf_box box;
+  double w[3][kCfMaxRatio][5];  // direction, child, coarse offset -2..2
+};
+
+__device__ __forceinline__ int floorDiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+__global__ void __launch_bounds__(kThreads) cfInterpKernel(const CfItem* __restrict__ items,
+                                                           const Chunk* __restrict__ chunks) {
+  const Chunk ch = chunks[blockIdx.x];
+  const CfItem& it = items[ch.item];
+  const hc_cf_box& B = it.box;
+  const long long fineN = (long long)B.fine_n[0] * B.fine_n[1] * B.fine_n[2];
+  const long long coarseN = (long long)B.coarse_n[0] * B.coarse_n[1] * B.coarse_n[2];
+  for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
+    const int p[3] = {B.fine_lo[0] + (int)(t % B.fine_n[0]), B.fine_lo[1] + (int)((t / B.fine_n[0]) % B.fine_n[1]),
+                      B.fine_lo[2] + (int)(t / ((long long)B.fine_n[0] * B.fine_n[1]))};
+    bool inside = true;
+    for (int d = 0; d < 3; ++d) inside = inside && p[d] >= B.valid_lo[d] && p[d] <= B.valid_hi[d];
+    if (inside) continue;  // valid cells keep their own data
+    int q[3];
+    const double* w[3];
+    for (int d = 0; d < 3; ++d) {
+      q[d] = floorDiv(p[d], B.ratio[d]);
+      w[d] = it.w[d][p[d] - q[d] * B.ratio[d]];
+    }
+    double out[kCfMaxComp];
+    bool finite = true;
+    for (int c = 0; c < B.ncomp; ++c) {
+      const double* src = B.coarse + (long long)c * coarseN;
+      double value = 0.0;
+      for (int k2 = -2; k2 <= 2; ++k2) {
+        if (w[2][k2 + 2] == 0.0) continue;
+        double v1 = 0.0;
+        for (int k1 = -2; k1 <= 2; ++k1) {
+          if (w[1][k1 + 2] == 0.0) continue;
+          double v0 = 0.0;
+          for (int k0 = -2; k0 <= 2; ++k0) {
+            if (w[0][k0 + 2] == 0.0) continue;
+            const int a = q[0] + k0 - B.coarse_lo[0], b = q[1] + k1 - B.coarse_lo[1], e = q[2] + k2 - B.coarse_lo[2];
+            if (a < 0 || a >= B.coarse_n[0] || b < 0 || b >= B.coarse_n[1] || e < 0 || e >= B.coarse_n[2]) {
+              v0 = CUDART_NAN;  // the reference's out-of-box marker
+              break;
+            }
+            v0 = __dadd_rn(v0, __dmul_rn(w[0][k0 + 2], src[a + (long long)B.coarse_n[0] * (b + (long long)B.coarse_n[1] * e)]));
+          }
+          v1 = __dadd_rn(v1, __dmul_rn(w[1][k1 + 2], v0));
+        }
+        value = __dadd_rn(value, __dmul_rn(w[2][k2 + 2], v1));
+      }
+      out[c] = value;
+      finite = finite && isfinite(value);
+    }
+    if (!finite) continue;  // left for the caller's fill
+    const long long fo = t;
+    for (int c = 0; c < B.ncomp; ++c) B.fine[(long long)c * fineN + fo] = out[c];
+  }
+}
+
 int cudaFailed(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return HC_OK;
   char msg[256];
@@ -180,6 +248,10 @@ struct hc_amr_plan {
   Chunk* restrictChunks = nullptr;      // work list of the restrictions (device), by item
   int nbox = 0, nrestrict = 0, nBoxChunks = 0;
   std::vector<int> restrictChunkStart;  // first chunk of each restriction (+ total at the end)
+  CfItem* cf = nullptr;                 // coarse-fine interpolation boxes with their weights (device)
+  Chunk* cfChunks = nullptr;
+  std::vector<hc_cf_box> cfHost;
+  std::vector<int> cfChunkStart;
 };
 
 extern "C" int hc_amr_plan_create(hc_ctx* ctx, const hc_rk_box* boxes, int nbox, const hc_restrict_box* restricts,
@@ -265,6 +337,8 @@ extern "C" int hc_amr_plan_destroy(hc_amr_plan* P) {
   cudaFree(P->restrictChunks);
   cudaFree(P->reflux);
   cudaFree(P->refluxChunks);
+  cudaFree(P->cf);
+  cudaFree(P->cfChunks);
   delete P;
   return HC_OK;
 }
@@ -357,4 +431,177 @@ extern "C" int hc_amr_restrict(hc_ctx* ctx, const hc_amr_plan* P, int first, int
   if (c1 == c0) return HC_OK;
   restrictKernel<<<c1 - c0, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->restricts, P->restrictChunks + c0);
   return cudaFailed(cudaGetLastError(), "hc_amr_restrict");
+}
+
+// ---------------------------------------------------------------------------
+// Coarse-fine interpolation weights (src/MHD_AMRInterpolation.H:39-56).
+// Host arithmetic: the inverse of the five coarse cells' moment matrix in
+// exact rationals, rounded to double once, then the child's moments in
+// double.
+namespace {
+
+struct Rational {
+  long long n = 0, d = 1;
+};
+long long gcdLL(long long a, long long b) {
+  a = a < 0 ? -a : a;
+  b = b < 0 ? -b : b;
+  while (b) {
+    const long long t = a % b;
+    a = b;
+    b = t;
+  }
+  return a ? a : 1;
+}
+Rational mk(long long n, long long d) {
+  if (d < 0) { n = -n; d = -d; }
+  const long long g = gcdLL(n, d);
+  return Rational{n / g, d / g};
+}
+Rational sub(Rational a, Rational b) { return mk(a.n * b.d - b.n * a.d, a.d * b.d); }
+Rational mul(Rational a, Rational b) { return mk(a.n * b.n, a.d * b.d); }
+Rational divr(Rational a, Rational b) { return mk(a.n * b.d, a.d * b.n); }
+
+// inverse[n][i]: coefficient of the average over coarse cell i (centre
+// i - 2) in the n-th coefficient of the quartic matching five averages.
+// Row i of the moment matrix holds the averages of x^n over [c - 1/2,
+// c + 1/2], c = i - 2: 1, c, c^2 + 1/12, c^3 + c/4, c^4 + c^2/2 + 1/80.
+struct InverseMoments {
+  double v[5][5];
+};
+InverseMoments computeInverseMoments() {
+  InverseMoments out{};
+  Rational a[5][10];
+  for (int i = 0; i < 5; ++i) {
+    const long long c = i - 2;
+    a[i][0] = mk(1, 1);
+    a[i][1] = mk(c, 1);
+    a[i][2] = mk(12 * c * c + 1, 12);
+    a[i][3] = mk(4 * c * c * c + c, 4);
+    a[i][4] = mk(80 * c * c * c * c + 40 * c * c + 1, 80);
+    for (int j = 0; j < 5; ++j) a[i][5 + j] = mk(i == j ? 1 : 0, 1);
+  }
+  for (int col = 0; col < 5; ++col) {  // Gauss-Jordan, exact (the matrix is regular)
+    int piv = col;
+    while (piv < 4 && a[piv][col].n == 0) ++piv;
+    if (piv != col)
+      for (int j = 0; j < 10; ++j) std::swap(a[piv][j], a[col][j]);
+    const Rational pv = a[col][col];
+    for (int j = 0; j < 10; ++j) a[col][j] = divr(a[col][j], pv);
+    for (int r = 0; r < 5; ++r) {
+      if (r == col || a[r][col].n == 0) continue;
+      const Rational f = a[r][col];
+      for (int j = 0; j < 10; ++j) a[r][j] = sub(a[r][j], mul(f, a[col][j]));
+    }
+  }
+  // a = [I | A^-1] with A[i][n]; A^-1 is indexed [n][i]
+  for (int n = 0; n < 5; ++n)
+    for (int i = 0; i < 5; ++i) out.v[n][i] = (double)a[n][5 + i].n / (double)a[n][5 + i].d;
+  return out;
+}
+const double (*inverseMoments())[5] {
+  static const InverseMoments table = computeInverseMoments();  // initialised once, thread-safe
+  return table.v;
+}
+
+void cfWeights(int ratio, int child, double w[5]) {
+  if (ratio == 1) {
+    const double unit[5] = {0, 0, 1, 0, 0};
+    for (int i = 0; i < 5; ++i) w[i] = unit[i];
+    return;
+  }
+  const double x = (child + 0.5) / ratio - 0.5, inverse = 1.0 / ratio;
+  const double moment[5] = {1, x, x * x + inverse * inverse / 12, x * x * x + x * inverse * inverse / 4,
+                            x * x * x * x + x * x * inverse * inverse / 2 + inverse * inverse * inverse * inverse / 80};
+  const double(*inv)[5] = inverseMoments();
+  for (int i = 0; i < 5; ++i) {
+    double v = 0.0;
+    for (int n = 0; n < 5; ++n) v += moment[n] * inv[n][i];
+    w[i] = v;
+  }
+}
+
+bool cfBoxOk(const hc_cf_box& B) {
+  if (!B.coarse || !B.fine || B.ncomp < 1 || B.ncomp > kCfMaxComp) return false;
+  long long fineN = 1, coarseN = 1;
+  for (int d = 0; d < 3; ++d) {
+    if (B.ratio[d] < 1 || B.ratio[d] > kCfMaxRatio || B.fine_n[d] < 1 || B.coarse_n[d] < 1) return false;
+    fineN *= B.fine_n[d];
+    coarseN *= B.coarse_n[d];
+  }
+  return fineN < 0x7fffffffLL && coarseN < 0x7fffffffLL;
+}
+
+}  // namespace
+
+extern "C" int hc_amr_cf_weights(int ratio, int child, double* w) {
+  if (!w || ratio < 1 || ratio > kCfMaxRatio || child < 0 || child >= ratio)
+    return argFail("hc_amr_cf_weights: ratio 1..8 and child 0..ratio-1");
+  cfWeights(ratio, child, w);
+  return HC_OK;
+}
+
+extern "C" int hc_amr_plan_set_cf_interp(hc_amr_plan* P, const hc_cf_box* boxes, int nbox) {
+  if (!P || nbox < 0 || (nbox && !boxes)) return argFail("hc_amr_plan_set_cf_interp: bad argument");
+  std::vector<CfItem> items(nbox);
+  std::vector<Chunk> cc;
+  std::vector<int> start;
+  for (int b = 0; b < nbox; ++b) {
+    if (!cfBoxOk(boxes[b]))
+      return argFail("hc_amr_plan_set_cf_interp: a box needs its arrays, ratio 1..8, ncomp 1..16 and boxes of "
+                     "fewer than 2^31 cells");
+    CfItem& it = items[b];
+    it.box = boxes[b];
+    for (int d = 0; d < 3; ++d)
+      for (int child = 0; child < kCfMaxRatio; ++child) {
+        if (child < boxes[b].ratio[d])
+          cfWeights(boxes[b].ratio[d], child, it.w[d][child]);
+        else
+          for (int i = 0; i < 5; ++i) it.w[d][child][i] = 0.0;
+      }
+    start.push_back((int)cc.size());
+    addChunks(cc, b, (long long)boxes[b].fine_n[0] * boxes[b].fine_n[1] * boxes[b].fine_n[2]);
+  }
+  start.push_back((int)cc.size());
+  CfItem* dev = nullptr;
+  Chunk* devChunks = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (nbox) {
+    e = cudaMalloc(&dev, sizeof(CfItem) * nbox);
+    if (e == cudaSuccess) e = cudaMemcpy(dev, items.data(), sizeof(CfItem) * nbox, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&devChunks, sizeof(Chunk) * cc.size());
+    if (e == cudaSuccess) e = cudaMemcpy(devChunks, cc.data(), sizeof(Chunk) * cc.size(), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(dev);
+    cudaFree(devChunks);
+    return cudaFailed(e, "hc_amr_plan_set_cf_interp");
+  }
+  cudaFree(P->cf);
+  cudaFree(P->cfChunks);
+  P->cf = dev;
+  P->cfChunks = devChunks;
+  P->cfHost.assign(boxes, boxes + nbox);
+  P->cfChunkStart = start;
+  return HC_OK;
+}
+
+extern "C" int hc_amr_cf_interpolate(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, void* stream) {
+  if (!ctx || !P) return argFail("hc_amr_cf_interpolate: null argument");
+  const int n = (int)P->cfHost.size();
+  if (first < 0 || count < 0 || first + count > n) return argFail("hc_amr_cf_interpolate: range outside the plan");
+  // boxes of one launch must write disjoint fine regions of each array
+  for (int a = first; a < first + count; ++a)
+    for (int b = a + 1; b < first + count; ++b) {
+      const hc_cf_box &A = P->cfHost[a], &B = P->cfHost[b];
+      if (A.fine != B.fine) continue;
+      bool overlap = true;
+      for (int d = 0; d < 3 && overlap; ++d)
+        overlap = A.fine_lo[d] < B.fine_lo[d] + B.fine_n[d] && B.fine_lo[d] < A.fine_lo[d] + A.fine_n[d];
+      if (overlap) return argFail("hc_amr_cf_interpolate: two boxes of one launch write the same fine array region");
+    }
+  const int c0 = count ? P->cfChunkStart[first] : 0, c1 = count ? P->cfChunkStart[first + count] : 0;
+  if (c1 == c0) return HC_OK;
+  cfInterpKernel<<<c1 - c0, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->cf, P->cfChunks + c0);
+  return cudaFailed(cudaGetLastError(), "hc_amr_cf_interpolate");
 }

@@ -515,6 +515,14 @@ class O4Batch:
             pass
 
 
+def amr_cf_weights(ratio: int, child: int) -> np.ndarray:
+    """hc_amr_cf_weights: the five coarse weights of child `child` of a cell
+    refined by `ratio` (host arithmetic; no device needed)."""
+    w = (C.c_double * 5)()
+    N.check(N.lib().hc_amr_cf_weights(ratio, child, w), "hc_amr_cf_weights")
+    return np.array(w[:])
+
+
 class AmrPlan:
     """The AMR Runge-Kutta stage logic of a set of boxes (any levels, any
     sizes): hc_amr_plan_create / hc_amr_rk_stage / hc_amr_restrict.
@@ -567,6 +575,24 @@ class AmrPlan:
 
     def reflux(self, first: int, count: int) -> None:
         N.check(self._lib.hc_amr_reflux(self._shell._ctx, self._h, first, count, _stream()), "hc_amr_reflux")
+
+    def set_cf_interp(self, boxes) -> None:
+        """boxes: dicts with coarse, fine (device tensors of ncomp x box
+        cells), coarse_lo, coarse_n, fine_lo, fine_n, valid_lo, valid_hi,
+        ratio (3 ints each) and ncomp (hc_cf_box)."""
+        n = len(boxes)
+        arr = (N.HcCfBox * max(n, 1))()
+        for b, d in enumerate(boxes):
+            arr[b].coarse = d["coarse"].data_ptr()
+            arr[b].fine = d["fine"].data_ptr()
+            for k in ("coarse_lo", "coarse_n", "fine_lo", "fine_n", "valid_lo", "valid_hi", "ratio"):
+                getattr(arr[b], k)[:] = list(d[k])
+            arr[b].ncomp = d["ncomp"]
+        N.check(self._lib.hc_amr_plan_set_cf_interp(self._h, arr, n), "hc_amr_plan_set_cf_interp")
+
+    def cf_interpolate(self, first: int, count: int) -> None:
+        N.check(self._lib.hc_amr_cf_interpolate(self._shell._ctx, self._h, first, count, _stream()),
+                "hc_amr_cf_interpolate")
 
     def close(self) -> None:
         if self._h:

@@ -323,6 +323,48 @@ int hc_amr_rk_stage(hc_ctx* ctx, const hc_amr_plan* plan, int order, int stage, 
  * restrictions their own call, finest first, when levels chain. */
 int hc_amr_restrict(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
 
+/* Coarse-fine ghost interpolation of one fine box (the fourth-order
+ * interpolation of src/MHD_AMRInterpolation.H:39-155 as
+ * src/MHD_AMRFourthOrder.H:27-39 applies it to the donor data): every cell
+ * p of the fine storage region fine_lo .. fine_lo + fine_n - 1 (fine index
+ * space) outside the valid region valid_lo .. valid_hi gets, in each of its
+ * ncomp components, the average over the cell of the tensor-product quartic
+ * that matches the 5 x 5 x 5 coarse cell averages around its parent.  The
+ * parent is q = floor(p / ratio) per direction and the weights of direction
+ * d are those of hc_amr_cf_weights(ratio[d], p[d] - q[d] ratio[d]) (ratio
+ * 1: the parent alone).  The sums run direction by direction as the
+ * reference's passes do: first along i (coarse points q0-2 .. q0+2), then
+ * along j over those results, then along k, each in increasing index and
+ * skipping points of weight zero; products and sums are rounded as
+ * written.  A first-pass point of nonzero weight outside the coarse array's
+ * box (coarse_lo, coarse_n) makes its partial sum NaN.  A cell whose result
+ * is not finite in every component is left unchanged (the reference leaves
+ * its donor at zero for the exchange to fill).  Arrays are [ncomp][k][j][i]
+ * SoA over their boxes (device); ratio 1..8, ncomp 1..16. */
+typedef struct hc_cf_box {
+  const double* coarse;
+  double* fine;
+  int coarse_lo[3], coarse_n[3];
+  int fine_lo[3], fine_n[3];
+  int valid_lo[3], valid_hi[3];
+  int ratio[3];
+  int ncomp;
+} hc_cf_box;
+
+/* Weights w[0..4] (coarse cells q-2 .. q+2 along one direction) of child
+ * `child` (0 .. ratio-1) of a coarse cell: the average over the child of
+ * the quartic whose averages over the five coarse cells are the data, from
+ * the exact inverse of the five cells' moment matrix and the child's
+ * moments (ratio 1: {0, 0, 1, 0, 0}).  Host arithmetic, no device needed. */
+int hc_amr_cf_weights(int ratio, int child, double* w);
+
+/* Validate and keep a device copy of the plan's interpolation boxes. */
+int hc_amr_plan_set_cf_interp(hc_amr_plan* plan, const hc_cf_box* boxes, int nbox);
+
+/* Interpolation boxes first .. first+count-1 of the plan in one launch
+ * (boxes of one launch must not write the same fine array region). */
+int hc_amr_cf_interpolate(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Autotuner (no reference counterpart: the reference runs its face loops on
  * the host).  Order 2: the stage kernel runs one CTA per cell tile; the

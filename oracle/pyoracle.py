@@ -424,6 +424,98 @@ def amr_reflux(fine_flux, fine_lo, coarse_flux, coarse_lo, rhs, rhs_lo, lo, hi, 
                 rhs[idx] = rhs[idx] + coef * diff
 
 
+# ---------------------------------------------------------------------------
+# Coarse-fine fourth-order interpolation: src/MHD_AMRInterpolation.H:39-155,
+# applied to the donor data by src/MHD_AMRFourthOrder.H:27-39.
+# ---------------------------------------------------------------------------
+def amr_cf_inverse_moments():
+    """Exact inverse (Fractions, indexed [n][i]) of the moment matrix
+    A[i][n] = average of x^n over coarse cell i (centre i - 2, unit width):
+    the quartic matching five cell averages has coefficients a = A^-1 u."""
+    from fractions import Fraction as F
+    A = []
+    for i in range(5):
+        c = F(i - 2)
+        A.append([F(1), c, c * c + F(1, 12), c ** 3 + c / 4, c ** 4 + c * c / 2 + F(1, 80)])
+    n = 5
+    M = [A[r] + [F(int(r == j)) for j in range(n)] for r in range(n)]
+    for col in range(n):
+        piv = next(r for r in range(col, n) if M[r][col] != 0)
+        M[col], M[piv] = M[piv], M[col]
+        pv = M[col][col]
+        M[col] = [v / pv for v in M[col]]
+        for r in range(n):
+            if r != col and M[r][col] != 0:
+                f = M[r][col]
+                M[r] = [a - f * b for a, b in zip(M[r], M[col])]
+    return [[M[r][n + j] for j in range(n)] for r in range(n)]
+
+
+def amr_cf_weights(ratio: int, child: int) -> np.ndarray:
+    """amrFourthOrderWeights (:39-56): the child's moments in double times
+    the exact inverse rounded to double, summed over the moments in order."""
+    if ratio == 1:
+        return np.array([0.0, 0.0, 1.0, 0.0, 0.0])
+    inv = [[float(v) for v in row] for row in amr_cf_inverse_moments()]
+    x = (child + 0.5) / ratio - 0.5
+    h = 1.0 / ratio
+    moment = [1.0, x, x * x + h * h / 12, x * x * x + x * h * h / 4,
+              x * x * x * x + x * x * h * h / 2 + h * h * h * h / 80]
+    w = []
+    for i in range(5):
+        v = 0.0
+        for n in range(5):
+            v += moment[n] * inv[n][i]
+        w.append(v)
+    return np.array(w)
+
+
+def amr_cf_interpolate(coarse: np.ndarray, coarse_lo, fine: np.ndarray, fine_lo, valid_lo, valid_hi, ratio) -> None:
+    """The separable passes of amrInterpolateFourthOrder (:122-155) for every
+    fine storage cell outside the valid region, then the donor update of
+    MHD_AMRFourthOrder.H:31-38 (finite in every component, else unchanged).
+    coarse [C][k][j][i] over its box (low corner coarse_lo), fine likewise."""
+    C = coarse.shape[0]
+    fn = fine.shape[1:][::-1]
+    cn = coarse.shape[1:][::-1]
+    weights = [[amr_cf_weights(ratio[d], ch) for ch in range(ratio[d])] for d in range(3)]
+    with np.errstate(all="ignore"):
+        for k in range(fn[2]):
+            for j in range(fn[1]):
+                for i in range(fn[0]):
+                    p = (fine_lo[0] + i, fine_lo[1] + j, fine_lo[2] + k)
+                    if all(valid_lo[d] <= p[d] <= valid_hi[d] for d in range(3)):
+                        continue
+                    q = [p[d] // ratio[d] for d in range(3)]   # floor division
+                    w = [weights[d][p[d] - q[d] * ratio[d]] for d in range(3)]
+                    out = np.zeros(C)
+                    for c in range(C):
+                        value = 0.0
+                        for k2 in range(-2, 3):
+                            if w[2][k2 + 2] == 0:
+                                continue
+                            v1 = 0.0
+                            for k1 in range(-2, 3):
+                                if w[1][k1 + 2] == 0:
+                                    continue
+                                v0 = 0.0
+                                for k0 in range(-2, 3):
+                                    if w[0][k0 + 2] == 0:
+                                        continue
+                                    a = q[0] + k0 - coarse_lo[0]
+                                    b = q[1] + k1 - coarse_lo[1]
+                                    e = q[2] + k2 - coarse_lo[2]
+                                    if not (0 <= a < cn[0] and 0 <= b < cn[1] and 0 <= e < cn[2]):
+                                        v0 = float("nan")
+                                        break
+                                    v0 = v0 + w[0][k0 + 2] * float(coarse[c, e, b, a])
+                                v1 = v1 + w[1][k1 + 2] * v0
+                            value = value + w[2][k2 + 2] * v1
+                        out[c] = value
+                    if np.all(np.isfinite(out)):
+                        fine[:, k, j, i] = out
+
+
 def cme_schedule(events, time: float, feeding: float) -> tuple[float, float]:
     """(CFL fraction, Rusanov window end) of the oracle's schedule."""
     n = len(events)

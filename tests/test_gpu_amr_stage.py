@@ -137,3 +137,60 @@ def test_reflux_launch_rejects_overlapping_patches():
     plan.reflux(0, 1)
     plan.reflux(1, 1)
     plan.close()
+
+
+def test_cf_interpolation_matches_oracle(oracle_lib):
+    """Coarse-fine fourth-order ghost interpolation (hc_amr_cf_interpolate)
+    of two fine boxes in one launch, ratio 2 in every direction and 2 in the
+    angular ones only, ghost cells at negative indices, a coarse box that
+    does not cover every stencil and a NaN in the coarse data: bit for bit
+    against the oracle, cells without data left as they were."""
+    _need_gpu()
+    po = oracle_lib
+    rng = np.random.default_rng(7)
+    sh = hc.Shell(hc.Params(nr=8, na=8))
+    plan = AmrPlan(sh, [])
+    cases = [
+        # coarse_lo, coarse_n, fine_lo, fine_n, valid_lo, valid_hi, ratio
+        ((-3, -3, -3), (9, 9, 8), (-3, -3, -3), (8, 8, 8), (0, 0, 0), (3, 3, 3), (2, 2, 2)),
+        ((-2, -4, -4), (8, 10, 11), (-2, -5, -5), (8, 10, 10), (0, 0, 0), (3, 3, 3), (1, 2, 2)),
+    ]
+    host, boxes = [], []
+    for b, (clo, cn, flo, fn, vlo, vhi, ratio) in enumerate(cases):
+        coarse = rng.normal(size=(8, cn[2], cn[1], cn[0])) * 10.0 ** rng.integers(-3, 3, size=(8, 1, 1, 1))
+        if b == 1:
+            coarse[5, 4, 5, 3] = np.nan
+        fine = rng.normal(size=(8, fn[2], fn[1], fn[0]))
+        want = fine.copy()
+        po.amr_cf_interpolate(coarse, clo, want, flo, vlo, vhi, ratio)
+        dc = torch.from_numpy(coarse.copy()).cuda()
+        df = torch.from_numpy(fine.copy()).cuda()
+        host.append((want, fine, df))
+        boxes.append({"coarse": dc, "fine": df, "coarse_lo": clo, "coarse_n": cn, "fine_lo": flo, "fine_n": fn,
+                      "valid_lo": vlo, "valid_hi": vhi, "ratio": ratio, "ncomp": 8, "_keep": dc})
+    plan.set_cf_interp(boxes)
+    plan.cf_interpolate(0, len(boxes))
+    torch.cuda.synchronize()
+    for want, fine, df in host:
+        got = df.cpu().numpy()
+        assert np.array_equal(got, want)
+        changed = np.any(got != fine, axis=0)
+        assert changed.any() and not changed.all()   # some ghosts filled, valid cells and data-less ghosts kept
+    plan.close()
+
+
+def test_cf_interpolation_rejects_bad_boxes():
+    _need_gpu()
+    sh = hc.Shell(hc.Params(nr=8, na=8))
+    plan = AmrPlan(sh, [])
+    t = torch.zeros(8 * 64, dtype=torch.float64, device="cuda")
+    good = {"coarse": t, "fine": t, "coarse_lo": (0, 0, 0), "coarse_n": (4, 4, 4), "fine_lo": (0, 0, 0),
+            "fine_n": (4, 4, 4), "valid_lo": (1, 1, 1), "valid_hi": (2, 2, 2), "ratio": (2, 2, 2), "ncomp": 8}
+    for key, value in (("ratio", (9, 2, 2)), ("ncomp", 17), ("fine_n", (0, 4, 4))):
+        with pytest.raises(hc.HcError):
+            plan.set_cf_interp([dict(good, **{key: value})])
+    plan.set_cf_interp([good, dict(good, fine=torch.zeros(8 * 64, dtype=torch.float64, device="cuda"))])
+    with pytest.raises(hc.HcError):
+        plan.set_cf_interp([good, good])
+        plan.cf_interpolate(0, 2)                     # both write the same fine region
+    plan.close()

@@ -606,14 +606,40 @@ def run_amr(args, world, rank, local):
             plan.rk_stage(4, s, 1.0e-3)
         plan.rk_stage(4, 4, 1.0e-3)
 
+    # the fourth-order coarse-fine ghost interpolation of every box of the
+    # refined levels: each box's ghosted storage (a copy, so the operator
+    # inputs stay as they are) from a coarse array over its parents'
+    # stencil footprint (synthetic averages in [1, 2)), one launch for all
+    cf_boxes, ghost_cells = [], 0
+    for _, sh, works, _, _ in levels[1:]:
+        for w in works:
+            box = w[0]
+            flo = [box.lo[d] - box.ghost for d in range(3)]
+            fhi = [box.hi[d] + box.ghost for d in range(3)]
+            clo = [flo[d] // 2 - 2 for d in range(3)]
+            cn = [fhi[d] // 2 + 2 - clo[d] + 1 for d in range(3)]
+            coarse = torch.rand(8 * cn[0] * cn[1] * cn[2], dtype=torch.float64, device=sh._dev) + 1.0
+            fn = [fhi[d] - flo[d] + 1 for d in range(3)]
+            ghost_cells += fn[0] * fn[1] * fn[2] - (box.hi[0] - box.lo[0] + 1) ** 3
+            cf_boxes.append({"coarse": coarse, "fine": w[1].clone(), "coarse_lo": clo, "coarse_n": cn, "fine_lo": flo,
+                             "fine_n": fn, "valid_lo": list(box.lo), "valid_hi": list(box.hi), "ratio": (2, 2, 2),
+                             "ncomp": 8})
+    cf_plan = AmrPlan(levels[0][1], [])
+    cf_plan.set_cf_interp(cf_boxes)
+
+    def cf_fill():
+        cf_plan.cf_interpolate(0, len(cf_boxes))
+
     sampler = ClockSampler(local)
     sampler.start()
     ms_b = timed(batched, args.amr_reps)
     ms_p = timed(plain, max(1, args.amr_reps // 4))
     ms_rk = timed(stage_logic, args.amr_reps)
     ms_step = timed(batched_step, max(1, args.amr_reps // 4))
+    ms_cf = timed(cf_fill, args.amr_reps)
     clocks = sampler.stop()
     plan.close()
+    cf_plan.close()
     # identical results
     for _, _, works, _, _ in levels:
         for w in works:
@@ -644,6 +670,11 @@ def run_amr(args, world, rank, local):
                                                "what": "4 x (batched operator of each level + stage combine) + "
                                                        "final combine; coarse-fine ghost fill and registers are "
                                                        "the caller's"},
+               "coarse_fine_interpolation": {"ms": ms_cf, "boxes": len(cf_boxes), "ghost_cells": ghost_cells,
+                                             "launches": 1,
+                                             "what": "fourth-order quartic interpolation of the 5 ghost layers of "
+                                                     "every box of the two refined levels from coarse averages, "
+                                                     "8 components, one launch"},
                "clocks": clocks}
         print(json.dumps(out), flush=True)
     for _, sh, _, batch, singles in levels:

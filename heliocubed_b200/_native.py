@@ -54,6 +54,9 @@ SIGNATURES = {
     "hc_amr_cf_weights": (C.c_int, [C.c_int, C.c_int, _VP]),
     "hc_amr_plan_set_cf_interp": (C.c_int, [_VP, _VP, C.c_int]),
     "hc_amr_cf_interpolate": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
+    "hc_amr_plan_set_cf_fine": (C.c_int, [_VP, _VP, C.c_int]),
+    "hc_amr_cf_mapped": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
+    "hc_amr_cf_quotient": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_ctx_set_o4_variants": (C.c_int, [_VP, _VP]),
     "hc_level_insert_cone": (C.c_int, [_VP, _VP, C.c_double, _VP, _VP, _VP]),
     "hc_cone_event": (C.c_int, [_VP, _VP]),
@@ -137,6 +140,16 @@ class HcCfBox(C.Structure):
     _fields_ = [("coarse", C.c_void_p), ("fine", C.c_void_p), ("coarse_lo", C.c_int * 3), ("coarse_n", C.c_int * 3),
                 ("fine_lo", C.c_int * 3), ("fine_n", C.c_int * 3), ("valid_lo", C.c_int * 3),
                 ("valid_hi", C.c_int * 3), ("ratio", C.c_int * 3), ("ncomp", C.c_int)]
+
+
+class HcCfFineBox(C.Structure):
+    """Mirror of hc_cf_fine_box in include/hc_abi.h."""
+    _fields_ = [("jac", C.c_void_p), ("donor", C.c_void_p), ("state", C.c_void_p), ("mapped", C.c_void_p),
+                ("out", C.c_void_p), ("jac_lo", C.c_int * 3), ("jac_n", C.c_int * 3), ("donor_lo", C.c_int * 3),
+                ("donor_n", C.c_int * 3), ("state_lo", C.c_int * 3), ("state_n", C.c_int * 3),
+                ("mapped_lo", C.c_int * 3), ("mapped_n", C.c_int * 3), ("out_lo", C.c_int * 3),
+                ("out_n", C.c_int * 3), ("valid_lo", C.c_int * 3), ("valid_hi", C.c_int * 3),
+                ("block_lo", C.c_int * 3), ("block_hi", C.c_int * 3)]
 
 
 class HcCmeEvent(C.Structure):

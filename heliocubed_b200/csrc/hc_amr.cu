@@ -202,6 +202,101 @@ __global__ void __launch_bounds__(kThreads) cfInterpKernel(const CfItem* __restr
   }
 }
 
+// Fourth-order <JU> of the ghost cells and <U> of the valid cells of a fine
+// box (src/MHD_AMRFourthOrder.H:41-80); every operation rounded as written.
+__device__ __forceinline__ long long boxOff(const int lo[3], const int n[3], int i, int j, int k) {
+  return (long long)(i - lo[0]) + (long long)n[0] * ((j - lo[1]) + (long long)n[1] * (k - lo[2]));
+}
+__device__ __forceinline__ long long boxSize(const int n[3]) { return (long long)n[0] * n[1] * n[2]; }
+__device__ __forceinline__ bool inValid(const hc_cf_fine_box& B, const int p[3]) {
+  return p[0] >= B.valid_lo[0] && p[0] <= B.valid_hi[0] && p[1] >= B.valid_lo[1] && p[1] <= B.valid_hi[1] &&
+         p[2] >= B.valid_lo[2] && p[2] <= B.valid_hi[2];
+}
+
+__global__ void __launch_bounds__(kThreads) cfMappedKernel(const hc_cf_fine_box* __restrict__ items,
+                                                           const Chunk* __restrict__ chunks) {
+  const Chunk ch = chunks[blockIdx.x];
+  const hc_cf_fine_box& B = items[ch.item];
+  const long long mN = boxSize(B.mapped_n), dN = boxSize(B.donor_n), sN = boxSize(B.state_n);
+  for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
+    const int p[3] = {B.mapped_lo[0] + (int)(t % B.mapped_n[0]), B.mapped_lo[1] + (int)((t / B.mapped_n[0]) % B.mapped_n[1]),
+                      B.mapped_lo[2] + (int)(t / ((long long)B.mapped_n[0] * B.mapped_n[1]))};
+    if (inValid(B, p)) {
+      const long long so = boxOff(B.state_lo, B.state_n, p[0], p[1], p[2]);
+      for (int c = 0; c < 8; ++c) B.mapped[c * mN + t] = B.state[c * sN + so];
+      continue;
+    }
+    const double J = B.jac[boxOff(B.jac_lo, B.jac_n, p[0], p[1], p[2])];
+    double dJ[3];
+    long long up[3], dn[3];
+    for (int d = 0; d < 3; ++d) {
+      int a[3] = {p[0], p[1], p[2]}, b[3] = {p[0], p[1], p[2]};
+      a[d] += 1;
+      b[d] -= 1;
+      dJ[d] = __dsub_rn(B.jac[boxOff(B.jac_lo, B.jac_n, a[0], a[1], a[2])], B.jac[boxOff(B.jac_lo, B.jac_n, b[0], b[1], b[2])]);
+      up[d] = boxOff(B.donor_lo, B.donor_n, a[0], a[1], a[2]);
+      dn[d] = boxOff(B.donor_lo, B.donor_n, b[0], b[1], b[2]);
+    }
+    const long long o = boxOff(B.donor_lo, B.donor_n, p[0], p[1], p[2]);
+    for (int c = 0; c < 8; ++c) {
+      const double* U = B.donor + c * dN;
+      double value = __dmul_rn(J, U[o]);
+      for (int d = 0; d < 3; ++d)
+        value = __dadd_rn(value, __ddiv_rn(__dmul_rn(dJ[d], __dsub_rn(U[up[d]], U[dn[d]])), 48.0));
+      B.mapped[c * mN + t] = value;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) cfQuotientKernel(const hc_cf_fine_box* __restrict__ items,
+                                                             const Chunk* __restrict__ chunks) {
+  const Chunk ch = chunks[blockIdx.x];
+  const hc_cf_fine_box& B = items[ch.item];
+  const long long mN = boxSize(B.mapped_n), oN = boxSize(B.out_n);
+  const int vn[3] = {B.valid_hi[0] - B.valid_lo[0] + 1, B.valid_hi[1] - B.valid_lo[1] + 1, B.valid_hi[2] - B.valid_lo[2] + 1};
+  for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
+    const int p[3] = {B.valid_lo[0] + (int)(t % vn[0]), B.valid_lo[1] + (int)((t / vn[0]) % vn[1]),
+                      B.valid_lo[2] + (int)(t / ((long long)vn[0] * vn[1]))};
+    auto jacAt = [&](const int x[3]) { return B.jac[boxOff(B.jac_lo, B.jac_n, x[0], x[1], x[2])]; };
+    const double Jp = jacAt(p);
+    // per direction: the derivative's three cells and weights, and dJ
+    int base[3];
+    double w[3][3], dj[3];
+    for (int d = 0; d < 3; ++d) {
+      if (p[d] == B.block_lo[d]) {
+        base[d] = p[d];
+        w[d][0] = -1.5; w[d][1] = 2.0; w[d][2] = -0.5;
+      } else if (p[d] == B.block_hi[d]) {
+        base[d] = p[d] - 2;
+        w[d][0] = 0.5; w[d][1] = -2.0; w[d][2] = 1.5;
+      } else {
+        base[d] = p[d] - 1;
+        w[d][0] = -0.5; w[d][1] = 0.0; w[d][2] = 0.5;
+      }
+      int a[3] = {p[0], p[1], p[2]}, b[3] = {p[0], p[1], p[2]};
+      a[d] += 1;
+      b[d] -= 1;
+      dj[d] = __dmul_rn(0.5, __dsub_rn(jacAt(a), jacAt(b)));
+    }
+    const long long op = boxOff(B.out_lo, B.out_n, p[0], p[1], p[2]);
+    for (int c = 0; c < 8; ++c) {
+      const double* M = B.mapped + c * mN;
+      auto Q = [&](const int x[3]) { return __ddiv_rn(M[boxOff(B.mapped_lo, B.mapped_n, x[0], x[1], x[2])], jacAt(x)); };
+      double correction = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        double derivative = 0.0;
+        for (int m = 0; m < 3; ++m) {
+          int x[3] = {p[0], p[1], p[2]};
+          x[d] = base[d] + m;
+          derivative = __dadd_rn(derivative, __dmul_rn(w[d][m], Q(x)));
+        }
+        correction = __dadd_rn(correction, __dmul_rn(dj[d], derivative));
+      }
+      B.out[c * oN + op] = __dsub_rn(Q(p), __ddiv_rn(correction, __dmul_rn(12.0, Jp)));
+    }
+  }
+}
+
 int cudaFailed(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return HC_OK;
   char msg[256];
@@ -248,6 +343,11 @@ struct hc_amr_plan {
   Chunk* restrictChunks = nullptr;      // work list of the restrictions (device), by item
   int nbox = 0, nrestrict = 0, nBoxChunks = 0;
   std::vector<int> restrictChunkStart;  // first chunk of each restriction (+ total at the end)
+  hc_cf_fine_box* cfFine = nullptr;     // fine boxes of the <JU> / <U> recovery (device)
+  Chunk* cfMappedChunks = nullptr;
+  Chunk* cfQuotientChunks = nullptr;
+  std::vector<hc_cf_fine_box> cfFineHost;
+  std::vector<int> cfMappedStart, cfQuotientStart;
   CfItem* cf = nullptr;                 // coarse-fine interpolation boxes with their weights (device)
   Chunk* cfChunks = nullptr;
   std::vector<hc_cf_box> cfHost;
@@ -339,6 +439,9 @@ extern "C" int hc_amr_plan_destroy(hc_amr_plan* P) {
   cudaFree(P->refluxChunks);
   cudaFree(P->cf);
   cudaFree(P->cfChunks);
+  cudaFree(P->cfFine);
+  cudaFree(P->cfMappedChunks);
+  cudaFree(P->cfQuotientChunks);
   delete P;
   return HC_OK;
 }
@@ -604,4 +707,123 @@ extern "C" int hc_amr_cf_interpolate(hc_ctx* ctx, const hc_amr_plan* P, int firs
   if (c1 == c0) return HC_OK;
   cfInterpKernel<<<c1 - c0, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->cf, P->cfChunks + c0);
   return cudaFailed(cudaGetLastError(), "hc_amr_cf_interpolate");
+}
+
+namespace {
+
+// region lo .. hi (inclusive) inside the box (lo, n)
+bool regionIn(const int lo[3], const int hi[3], const int blo[3], const int bn[3]) {
+  for (int d = 0; d < 3; ++d)
+    if (lo[d] < blo[d] || hi[d] >= (long long)blo[d] + bn[d]) return false;
+  return true;
+}
+
+bool cfFineOk(const hc_cf_fine_box& B) {
+  if (!B.jac || !B.donor || !B.state || !B.mapped || !B.out) return false;
+  int g3lo[3], g3hi[3], g2lo[3], g2hi[3];
+  for (int d = 0; d < 3; ++d) {
+    if (B.valid_lo[d] > B.valid_hi[d] || B.block_hi[d] - B.block_lo[d] < 2) return false;
+    if (B.valid_lo[d] < B.block_lo[d] || B.valid_hi[d] > B.block_hi[d]) return false;
+    if (B.jac_n[d] < 1 || B.donor_n[d] < 1 || B.state_n[d] < 1 || B.mapped_n[d] < 1 || B.out_n[d] < 1) return false;
+    g3lo[d] = B.valid_lo[d] - 3; g3hi[d] = B.valid_hi[d] + 3;
+    g2lo[d] = B.valid_lo[d] - 2; g2hi[d] = B.valid_hi[d] + 2;
+  }
+  const int* vlo = B.valid_lo;
+  const int* vhi = B.valid_hi;
+  // the mapped box is valid.grow(2) (its cells read J and the donor one
+  // cell further out)
+  for (int d = 0; d < 3; ++d)
+    if (B.mapped_lo[d] != g2lo[d] || B.mapped_n[d] != g2hi[d] - g2lo[d] + 1) return false;
+  long long sizes[5] = {1, 1, 1, 1, 1};
+  for (int d = 0; d < 3; ++d) {
+    sizes[0] *= B.jac_n[d]; sizes[1] *= B.donor_n[d]; sizes[2] *= B.state_n[d];
+    sizes[3] *= B.mapped_n[d]; sizes[4] *= B.out_n[d];
+  }
+  for (long long v : sizes)
+    if (8 * v >= 0x7fffffffLL) return false;
+  return regionIn(g3lo, g3hi, B.jac_lo, B.jac_n) && regionIn(g3lo, g3hi, B.donor_lo, B.donor_n) &&
+         regionIn(vlo, vhi, B.state_lo, B.state_n) && regionIn(vlo, vhi, B.out_lo, B.out_n);
+}
+
+}  // namespace
+
+extern "C" int hc_amr_plan_set_cf_fine(hc_amr_plan* P, const hc_cf_fine_box* boxes, int nbox) {
+  if (!P || nbox < 0 || (nbox && !boxes)) return argFail("hc_amr_plan_set_cf_fine: bad argument");
+  std::vector<Chunk> mc, qc;
+  std::vector<int> ms, qs;
+  for (int b = 0; b < nbox; ++b) {
+    const hc_cf_fine_box& B = boxes[b];
+    if (!cfFineOk(B))
+      return argFail("hc_amr_plan_set_cf_fine: a box needs its five arrays, J and the donor on valid.grow(3), the "
+                     "mapped box equal to valid.grow(2), state and out on valid, a block containing valid and at "
+                     "least 3 cells wide");
+    ms.push_back((int)mc.size());
+    addChunks(mc, b, (long long)B.mapped_n[0] * B.mapped_n[1] * B.mapped_n[2]);
+    qs.push_back((int)qc.size());
+    addChunks(qc, b, (long long)(B.valid_hi[0] - B.valid_lo[0] + 1) * (B.valid_hi[1] - B.valid_lo[1] + 1) *
+                         (B.valid_hi[2] - B.valid_lo[2] + 1));
+  }
+  ms.push_back((int)mc.size());
+  qs.push_back((int)qc.size());
+  hc_cf_fine_box* dev = nullptr;
+  Chunk *devM = nullptr, *devQ = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (nbox) {
+    e = cudaMalloc(&dev, sizeof(hc_cf_fine_box) * nbox);
+    if (e == cudaSuccess) e = cudaMemcpy(dev, boxes, sizeof(hc_cf_fine_box) * nbox, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&devM, sizeof(Chunk) * mc.size());
+    if (e == cudaSuccess) e = cudaMemcpy(devM, mc.data(), sizeof(Chunk) * mc.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&devQ, sizeof(Chunk) * qc.size());
+    if (e == cudaSuccess) e = cudaMemcpy(devQ, qc.data(), sizeof(Chunk) * qc.size(), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(dev);
+    cudaFree(devM);
+    cudaFree(devQ);
+    return cudaFailed(e, "hc_amr_plan_set_cf_fine");
+  }
+  cudaFree(P->cfFine);
+  cudaFree(P->cfMappedChunks);
+  cudaFree(P->cfQuotientChunks);
+  P->cfFine = dev;
+  P->cfMappedChunks = devM;
+  P->cfQuotientChunks = devQ;
+  P->cfFineHost.assign(boxes, boxes + nbox);
+  P->cfMappedStart = ms;
+  P->cfQuotientStart = qs;
+  return HC_OK;
+}
+
+namespace {
+int cfFineLaunch(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, void* stream, bool mapped) {
+  const char* what = mapped ? "hc_amr_cf_mapped" : "hc_amr_cf_quotient";
+  if (!ctx || !P) return argFail(mapped ? "hc_amr_cf_mapped: null argument" : "hc_amr_cf_quotient: null argument");
+  const int n = (int)P->cfFineHost.size();
+  if (first < 0 || count < 0 || first + count > n)
+    return argFail(mapped ? "hc_amr_cf_mapped: range outside the plan" : "hc_amr_cf_quotient: range outside the plan");
+  for (int a = first; a < first + count; ++a)
+    for (int b = a + 1; b < first + count; ++b) {
+      const hc_cf_fine_box &A = P->cfFineHost[a], &B = P->cfFineHost[b];
+      if ((mapped && A.mapped == B.mapped) || (!mapped && A.out == B.out))
+        return argFail(mapped ? "hc_amr_cf_mapped: two boxes of one launch write the same array"
+                              : "hc_amr_cf_quotient: two boxes of one launch write the same array");
+    }
+  const std::vector<int>& st = mapped ? P->cfMappedStart : P->cfQuotientStart;
+  const int c0 = count ? st[first] : 0, c1 = count ? st[first + count] : 0;
+  if (c1 == c0) return HC_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (mapped)
+    cfMappedKernel<<<c1 - c0, kThreads, 0, s>>>(P->cfFine, P->cfMappedChunks + c0);
+  else
+    cfQuotientKernel<<<c1 - c0, kThreads, 0, s>>>(P->cfFine, P->cfQuotientChunks + c0);
+  return cudaFailed(cudaGetLastError(), what);
+}
+}  // namespace
+
+extern "C" int hc_amr_cf_mapped(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, void* stream) {
+  return cfFineLaunch(ctx, P, first, count, stream, true);
+}
+
+extern "C" int hc_amr_cf_quotient(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, void* stream) {
+  return cfFineLaunch(ctx, P, first, count, stream, false);
 }

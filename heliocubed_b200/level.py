@@ -594,6 +594,28 @@ class AmrPlan:
         N.check(self._lib.hc_amr_cf_interpolate(self._shell._ctx, self._h, first, count, _stream()),
                 "hc_amr_cf_interpolate")
 
+    def set_cf_fine(self, boxes) -> None:
+        """boxes: dicts with jac, donor, state, mapped, out (device tensors)
+        and their *_lo / *_n boxes, valid_lo, valid_hi, block_lo, block_hi
+        (3 ints each) (hc_cf_fine_box)."""
+        n = len(boxes)
+        arr = (N.HcCfFineBox * max(n, 1))()
+        for b, d in enumerate(boxes):
+            for a in ("jac", "donor", "state", "mapped", "out"):
+                setattr(arr[b], a, d[a].data_ptr())
+                getattr(arr[b], a + "_lo")[:] = list(d[a + "_lo"])
+                getattr(arr[b], a + "_n")[:] = list(d[a + "_n"])
+            for k in ("valid_lo", "valid_hi", "block_lo", "block_hi"):
+                getattr(arr[b], k)[:] = list(d[k])
+        N.check(self._lib.hc_amr_plan_set_cf_fine(self._h, arr, n), "hc_amr_plan_set_cf_fine")
+
+    def cf_mapped(self, first: int, count: int) -> None:
+        N.check(self._lib.hc_amr_cf_mapped(self._shell._ctx, self._h, first, count, _stream()), "hc_amr_cf_mapped")
+
+    def cf_quotient(self, first: int, count: int) -> None:
+        N.check(self._lib.hc_amr_cf_quotient(self._shell._ctx, self._h, first, count, _stream()),
+                "hc_amr_cf_quotient")
+
     def close(self) -> None:
         if self._h:
             self._lib.hc_amr_plan_destroy(self._h)

@@ -365,6 +365,47 @@ int hc_amr_plan_set_cf_interp(hc_amr_plan* plan, const hc_cf_box* boxes, int nbo
  * (boxes of one launch must not write the same fine array region). */
 int hc_amr_cf_interpolate(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
 
+/* The fourth-order <JU> and <U> of a fine box around the caller's
+ * same-level exchange (src/MHD_AMRFourthOrder.H:41-80), two launches:
+ *
+ * hc_amr_cf_mapped, on every cell p of the mapped region (mapped_lo,
+ * mapped_n; the reference's valid.grow(2)): valid cells copy the box's
+ * state <JU>; the others get
+ *   <JU>(p) = J(p) U(p) + sum_d (J(p+e_d) - J(p-e_d)) (U(p+e_d) - U(p-e_d)) / 48
+ * from the donor Cartesian averages U (after hc_amr_cf_interpolate).
+ *
+ * hc_amr_cf_quotient, on every valid cell (after the caller's exchange of
+ * the mapped ghosts): with Q = <JU> / J,
+ *   out(p) = Q(p) - (sum_d 0.5 (J(p+e_d) - J(p-e_d)) D_d Q(p)) / (12 J(p)),
+ * D_d the undivided derivative along d: centred, and second-order one-sided
+ * on the block's (the panel's domain box at this level) first and last
+ * cells (weights -3/2, 2, -1/2 and 1/2, -2, 3/2, summed over three cells
+ * in increasing index).  Every product, sum and quotient is rounded as
+ * written, the terms in the order shown, directions in order.
+ *
+ * Arrays are SoA over their own boxes: jac 1 component (its box must
+ * contain valid.grow(3)), donor, state, mapped, out 8 components (donor:
+ * valid.grow(3); state and out: valid; mapped: valid.grow(2)); the block
+ * contains valid and is at least 3 cells wide in each direction. */
+typedef struct hc_cf_fine_box {
+  const double* jac;
+  const double* donor;
+  const double* state;
+  double* mapped;
+  double* out;
+  int jac_lo[3], jac_n[3];
+  int donor_lo[3], donor_n[3];
+  int state_lo[3], state_n[3];
+  int mapped_lo[3], mapped_n[3];
+  int out_lo[3], out_n[3];
+  int valid_lo[3], valid_hi[3];
+  int block_lo[3], block_hi[3];
+} hc_cf_fine_box;
+
+int hc_amr_plan_set_cf_fine(hc_amr_plan* plan, const hc_cf_fine_box* boxes, int nbox);
+int hc_amr_cf_mapped(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
+int hc_amr_cf_quotient(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Autotuner (no reference counterpart: the reference runs its face loops on
  * the host).  Order 2: the stage kernel runs one CTA per cell tile; the

@@ -516,6 +516,68 @@ def amr_cf_interpolate(coarse: np.ndarray, coarse_lo, fine: np.ndarray, fine_lo,
                         fine[:, k, j, i] = out
 
 
+def _at(a: np.ndarray, lo, x, c=None):
+    """Value of SoA array a ([C][k][j][i] or [k][j][i]) over a box with low corner lo at point x."""
+    idx = (x[2] - lo[2], x[1] - lo[1], x[0] - lo[0])
+    return float(a[idx]) if c is None else float(a[(c,) + idx])
+
+
+def amr_cf_mapped(jac, jac_lo, donor, donor_lo, state, state_lo, mapped, mapped_lo, valid_lo, valid_hi) -> None:
+    """<JU> on valid.grow(2) (src/MHD_AMRFourthOrder.H:41-61): valid cells copy
+    the state; the others J U + sum_d (J(p+e) - J(p-e)) (U(p+e) - U(p-e)) / 48."""
+    mn = mapped.shape[1:][::-1]
+    for k in range(mn[2]):
+        for j in range(mn[1]):
+            for i in range(mn[0]):
+                p = (mapped_lo[0] + i, mapped_lo[1] + j, mapped_lo[2] + k)
+                if all(valid_lo[d] <= p[d] <= valid_hi[d] for d in range(3)):
+                    for c in range(8):
+                        mapped[c, k, j, i] = _at(state, state_lo, p, c)
+                    continue
+                J = _at(jac, jac_lo, p)
+                for c in range(8):
+                    value = J * _at(donor, donor_lo, p, c)
+                    for d in range(3):
+                        a = list(p); b = list(p)
+                        a[d] += 1; b[d] -= 1
+                        dJ = _at(jac, jac_lo, a) - _at(jac, jac_lo, b)
+                        value = value + dJ * (_at(donor, donor_lo, a, c) - _at(donor, donor_lo, b, c)) / 48
+                    mapped[c, k, j, i] = value
+
+
+def amr_cf_quotient(jac, jac_lo, mapped, mapped_lo, out, out_lo, valid_lo, valid_hi, block_lo, block_hi) -> None:
+    """<U> on the valid cells (src/MHD_AMRFourthOrder.H:62-80): Q = <JU>/J,
+    out = Q - (sum_d 0.5 (J(p+e) - J(p-e)) D_d Q) / (12 J), D_d the
+    undivided derivative (centred; second-order one-sided on the block's
+    first and last cells, the restatement of deriv3case)."""
+    for k in range(valid_lo[2], valid_hi[2] + 1):
+        for j in range(valid_lo[1], valid_hi[1] + 1):
+            for i in range(valid_lo[0], valid_hi[0] + 1):
+                p = (i, j, k)
+                Jp = _at(jac, jac_lo, p)
+                for c in range(8):
+                    def Q(x):
+                        return _at(mapped, mapped_lo, x, c) / _at(jac, jac_lo, x)
+                    correction = 0.0
+                    for d in range(3):
+                        if p[d] == block_lo[d]:
+                            base, w = p[d], (-1.5, 2.0, -0.5)
+                        elif p[d] == block_hi[d]:
+                            base, w = p[d] - 2, (0.5, -2.0, 1.5)
+                        else:
+                            base, w = p[d] - 1, (-0.5, 0.0, 0.5)
+                        derivative = 0.0
+                        for m in range(3):
+                            x = list(p)
+                            x[d] = base + m
+                            derivative = derivative + w[m] * Q(x)
+                        a = list(p); b = list(p)
+                        a[d] += 1; b[d] -= 1
+                        dj = 0.5 * (_at(jac, jac_lo, a) - _at(jac, jac_lo, b))
+                        correction = correction + dj * derivative
+                    out[c, k - out_lo[2], j - out_lo[1], i - out_lo[0]] = Q(p) - correction / (12.0 * Jp)
+
+
 def cme_schedule(events, time: float, feeding: float) -> tuple[float, float]:
     """(CFL fraction, Rusanov window end) of the oracle's schedule."""
     n = len(events)

@@ -110,3 +110,83 @@ def test_oracle_leaves_cells_without_coarse_data():
     coarse[1, 2, 2, 2] = 1.0
     po.amr_cf_interpolate(coarse, (-2, -2, -2), fine2, (0, 0, 0), (1, 1, 1), (0, 0, 0), (2, 2, 2))
     assert np.allclose(fine2, 1.0, rtol=0, atol=1e-14)
+
+
+def _fine_case(rng, valid_lo, valid_hi, jac_fn, u_fn):
+    """Arrays of one fine box: J and the donor on valid.grow(3), the state
+    <JU> on valid, the mapped box valid.grow(2)."""
+    g3lo = [v - 3 for v in valid_lo]
+    g3n = [valid_hi[d] - valid_lo[d] + 7 for d in range(3)]
+    jac = np.zeros(g3n[::-1])
+    donor = np.zeros([8] + g3n[::-1])
+    for k in range(g3n[2]):
+        for j in range(g3n[1]):
+            for i in range(g3n[0]):
+                x = (g3lo[0] + i, g3lo[1] + j, g3lo[2] + k)
+                jac[k, j, i] = jac_fn(x)
+                donor[:, k, j, i] = u_fn(x)
+    vn = [valid_hi[d] - valid_lo[d] + 1 for d in range(3)]
+    state = rng.normal(size=[8] + vn[::-1])
+    g2lo = [v - 2 for v in valid_lo]
+    mapped = np.zeros([8] + [n + 4 for n in vn][::-1])
+    return g3lo, jac, donor, state, g2lo, mapped
+
+
+def test_oracle_fine_recovery_is_exact_for_constant_and_linear_data():
+    rng = np.random.default_rng(3)
+    vlo, vhi = (0, 0, 0), (3, 3, 3)
+    block_lo, block_hi = (0, -10, -10), (20, 20, 20)     # the radial block starts at the valid box
+    # constant J: the product and quotient corrections vanish
+    g3lo, jac, donor, state, g2lo, mapped = _fine_case(rng, vlo, vhi, lambda x: 2.0, lambda x: np.arange(8) + 1.0)
+    po.amr_cf_mapped(jac, g3lo, donor, g3lo, state, vlo, mapped, g2lo, vlo, vhi)
+    assert np.array_equal(mapped[:, 2:6, 2:6, 2:6], state)            # valid cells copy the state
+    ghost = np.ones(mapped.shape[1:], bool)
+    ghost[2:6, 2:6, 2:6] = False
+    assert np.all(mapped[:, ghost] == 2.0 * (np.arange(8) + 1.0)[:, None])
+    out = np.zeros((8, 4, 4, 4))
+    po.amr_cf_quotient(jac, g3lo, mapped, g2lo, out, vlo, vlo, vhi, block_lo, block_hi)
+    assert np.array_equal(out, state / 2.0)
+    # linear J, constant U: <JU> = J U exactly, and the quotient returns U
+    g3lo, jac, donor, state, g2lo, mapped = _fine_case(rng, vlo, vhi, lambda x: 1.0 + 0.25 * x[0] + 0.125 * x[1],
+                                                       lambda x: np.full(8, 3.0))
+    state[...] = 0.0
+    for k in range(4):
+        for j in range(4):
+            for i in range(4):
+                state[:, k, j, i] = 3.0 * (1.0 + 0.25 * i + 0.125 * j)
+    po.amr_cf_mapped(jac, g3lo, donor, g3lo, state, vlo, mapped, g2lo, vlo, vhi)
+    po.amr_cf_quotient(jac, g3lo, mapped, g2lo, out, vlo, vlo, vhi, block_lo, block_hi)
+    assert np.max(np.abs(out - 3.0)) < 1e-14
+
+
+def test_oracle_fine_quotient_is_fourth_order():
+    # smooth J and U: the quotient of the exact product averages recovers
+    # the exact U averages to O(h^4) (h the cell width in units of the data)
+    def case(h):
+        def avg(f, x):
+            # Gauss-Legendre 3 points per direction over the cell [x, x + 1] * h
+            g = (0.5 - np.sqrt(15) / 10, 0.5, 0.5 + np.sqrt(15) / 10)
+            wts = (5 / 18, 8 / 18, 5 / 18)
+            tot = 0.0
+            for a, wa in zip(g, wts):
+                for b, wb in zip(g, wts):
+                    for c, wc in zip(g, wts):
+                        tot = tot + wa * wb * wc * f(((x[0] + a) * h, (x[1] + b) * h, (x[2] + c) * h))
+            return tot
+        Jf = lambda y: 1.0 + 0.3 * np.sin(y[0] + 0.5 * y[1]) + 0.2 * y[2] * y[2]
+        Uf = lambda y: np.cos(y[0] - y[2]) + 0.5 * y[1]
+        vlo, vhi = (0, 0, 0), (1, 1, 1)
+        g3lo, jac, donor, state, g2lo, mapped = _fine_case(np.random.default_rng(0), vlo, vhi,
+                                                           lambda x: avg(Jf, x), lambda x: np.full(8, avg(Uf, x)))
+        for k in range(2):
+            for j in range(2):
+                for i in range(2):
+                    state[:, k, j, i] = avg(lambda y: Jf(y) * Uf(y), (i, j, k))
+        # ghosts from the donor's U averages, valid from the exact <JU>
+        po.amr_cf_mapped(jac, g3lo, donor, g3lo, state, vlo, mapped, g2lo, vlo, vhi)
+        out = np.zeros((8, 2, 2, 2))
+        po.amr_cf_quotient(jac, g3lo, mapped, g2lo, out, vlo, vlo, vhi, (-50, -50, -50), (50, 50, 50))
+        exact = np.array([[[avg(Uf, (i, j, k)) for i in range(2)] for j in range(2)] for k in range(2)])
+        return np.max(np.abs(out[0] - exact))
+    e1, e2 = case(0.2), case(0.1)
+    assert e1 / e2 > 12.0, (e1, e2)

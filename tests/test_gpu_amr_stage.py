@@ -194,3 +194,50 @@ def test_cf_interpolation_rejects_bad_boxes():
         plan.set_cf_interp([good, good])
         plan.cf_interpolate(0, 2)                     # both write the same fine region
     plan.close()
+
+
+def test_cf_fine_recovery_matches_oracle(oracle_lib):
+    """<JU> of the ghost cells (hc_amr_cf_mapped) and <U> of the valid cells
+    (hc_amr_cf_quotient) of two fine boxes in one launch each, one touching
+    its block's low radial end and one its high angular end: bit for bit
+    against the oracle."""
+    _need_gpu()
+    po = oracle_lib
+    rng = np.random.default_rng(11)
+    sh = hc.Shell(hc.Params(nr=8, na=8))
+    plan = AmrPlan(sh, [])
+    cases = [((0, 2, 3), (5, 6, 6), (0, -20, -20), (40, 40, 40)),
+             ((4, -3, 1), (9, 2, 4), (-20, -20, -20), (40, 2, 40))]
+    host, boxes = [], []
+    for vlo, vhi, blo, bhi in cases:
+        vn = [vhi[d] - vlo[d] + 1 for d in range(3)]
+        g3lo = [v - 3 for v in vlo]
+        g3n = [n + 6 for n in vn]
+        g2lo = [v - 2 for v in vlo]
+        g2n = [n + 4 for n in vn]
+        jac = 1.0 + rng.random(g3n[::-1])
+        donor = rng.normal(size=[8] + g3n[::-1])
+        state = rng.normal(size=[8] + vn[::-1])
+        want_m = np.zeros([8] + g2n[::-1])
+        want_o = np.zeros([8] + vn[::-1])
+        po.amr_cf_mapped(jac, g3lo, donor, g3lo, state, vlo, want_m, g2lo, vlo, vhi)
+        po.amr_cf_quotient(jac, g3lo, want_m, g2lo, want_o, vlo, vlo, vhi, blo, bhi)
+        t = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in
+             (("jac", jac), ("donor", donor), ("state", state))}
+        t["mapped"] = torch.zeros(want_m.size, dtype=torch.float64, device="cuda")
+        t["out"] = torch.zeros(want_o.size, dtype=torch.float64, device="cuda")
+        host.append((want_m, want_o, t))
+        boxes.append(dict(t, jac_lo=g3lo, jac_n=g3n, donor_lo=g3lo, donor_n=g3n, state_lo=vlo, state_n=vn,
+                          mapped_lo=g2lo, mapped_n=g2n, out_lo=vlo, out_n=vn, valid_lo=vlo, valid_hi=vhi,
+                          block_lo=blo, block_hi=bhi))
+    plan.set_cf_fine(boxes)
+    plan.cf_mapped(0, 2)
+    plan.cf_quotient(0, 2)
+    torch.cuda.synchronize()
+    for want_m, want_o, t in host:
+        assert np.array_equal(t["mapped"].cpu().numpy().reshape(want_m.shape), want_m)
+        assert np.array_equal(t["out"].cpu().numpy().reshape(want_o.shape), want_o)
+    bad = dict(boxes[0], mapped_n=[n + 1 for n in boxes[0]["mapped_n"]])
+    with pytest.raises(hc.HcError):
+        plan.set_cf_fine([bad])
+    plan.close()

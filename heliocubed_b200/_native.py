@@ -55,6 +55,8 @@ SIGNATURES = {
     "hc_amr_plan_set_cf_interp": (C.c_int, [_VP, _VP, C.c_int]),
     "hc_amr_cf_interpolate": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_amr_plan_set_cf_fine": (C.c_int, [_VP, _VP, C.c_int]),
+    "hc_amr_plan_set_copies": (C.c_int, [_VP, _VP, C.c_int]),
+    "hc_amr_copy": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_amr_cf_mapped": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_amr_cf_quotient": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_ctx_set_o4_variants": (C.c_int, [_VP, _VP]),
@@ -140,6 +142,13 @@ class HcCfBox(C.Structure):
     _fields_ = [("coarse", C.c_void_p), ("fine", C.c_void_p), ("coarse_lo", C.c_int * 3), ("coarse_n", C.c_int * 3),
                 ("fine_lo", C.c_int * 3), ("fine_n", C.c_int * 3), ("valid_lo", C.c_int * 3),
                 ("valid_hi", C.c_int * 3), ("ratio", C.c_int * 3), ("ncomp", C.c_int)]
+
+
+class HcCopyBox(C.Structure):
+    """Mirror of hc_copy_box in include/hc_abi.h."""
+    _fields_ = [("src", C.c_void_p), ("dst", C.c_void_p), ("src_lo", C.c_int * 3), ("src_n", C.c_int * 3),
+                ("dst_lo", C.c_int * 3), ("dst_n", C.c_int * 3), ("lo", C.c_int * 3), ("hi", C.c_int * 3),
+                ("perm", C.c_int * 3), ("sign", C.c_int * 3), ("shift", C.c_int * 3), ("ncomp", C.c_int)]
 
 
 class HcCfFineBox(C.Structure):

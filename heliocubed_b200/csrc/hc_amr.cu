@@ -12,8 +12,11 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <functional>
+#include <utility>
 #include <vector>
 
 #include "../../include/hc_abi.h"
@@ -297,6 +300,23 @@ __global__ void __launch_bounds__(kThreads) cfQuotientKernel(const hc_cf_fine_bo
   }
 }
 
+// Region copies with a signed-permutation index map (exchanges).
+__global__ void __launch_bounds__(kThreads) copyKernel(const hc_copy_box* __restrict__ items,
+                                                       const Chunk* __restrict__ chunks) {
+  const Chunk ch = chunks[blockIdx.x];
+  const hc_copy_box& B = items[ch.item];
+  const int n0 = B.hi[0] - B.lo[0] + 1, n1 = B.hi[1] - B.lo[1] + 1;
+  const long long sN = boxSize(B.src_n), dN = boxSize(B.dst_n);
+  for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
+    const int x[3] = {B.lo[0] + (int)(t % n0), B.lo[1] + (int)((t / n0) % n1), B.lo[2] + (int)(t / ((long long)n0 * n1))};
+    const int y[3] = {B.sign[0] * x[B.perm[0]] + B.shift[0], B.sign[1] * x[B.perm[1]] + B.shift[1],
+                      B.sign[2] * x[B.perm[2]] + B.shift[2]};
+    const long long so = boxOff(B.src_lo, B.src_n, x[0], x[1], x[2]);
+    const long long dO = boxOff(B.dst_lo, B.dst_n, y[0], y[1], y[2]);
+    for (int c = 0; c < B.ncomp; ++c) B.dst[c * dN + dO] = B.src[c * sN + so];
+  }
+}
+
 int cudaFailed(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return HC_OK;
   char msg[256];
@@ -343,6 +363,11 @@ struct hc_amr_plan {
   Chunk* restrictChunks = nullptr;      // work list of the restrictions (device), by item
   int nbox = 0, nrestrict = 0, nBoxChunks = 0;
   std::vector<int> restrictChunkStart;  // first chunk of each restriction (+ total at the end)
+  hc_copy_box* copies = nullptr;        // region copies (device)
+  Chunk* copyChunks = nullptr;
+  std::vector<hc_copy_box> copyHost;
+  std::vector<int> copyStart;
+  mutable std::vector<std::pair<int, int>> copyRangesChecked;  // launch ranges already found race free
   hc_cf_fine_box* cfFine = nullptr;     // fine boxes of the <JU> / <U> recovery (device)
   Chunk* cfMappedChunks = nullptr;
   Chunk* cfQuotientChunks = nullptr;
@@ -442,6 +467,8 @@ extern "C" int hc_amr_plan_destroy(hc_amr_plan* P) {
   cudaFree(P->cfFine);
   cudaFree(P->cfMappedChunks);
   cudaFree(P->cfQuotientChunks);
+  cudaFree(P->copies);
+  cudaFree(P->copyChunks);
   delete P;
   return HC_OK;
 }
@@ -826,4 +853,120 @@ extern "C" int hc_amr_cf_mapped(hc_ctx* ctx, const hc_amr_plan* P, int first, in
 
 extern "C" int hc_amr_cf_quotient(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, void* stream) {
   return cfFineLaunch(ctx, P, first, count, stream, false);
+}
+
+// ---------------------------------------------------------------------------
+// Region copies.
+namespace {
+
+struct Box3i {
+  int lo[3], hi[3];
+};
+bool overlaps(const Box3i& a, const Box3i& b) {
+  for (int d = 0; d < 3; ++d)
+    if (a.hi[d] < b.lo[d] || b.hi[d] < a.lo[d]) return false;
+  return true;
+}
+// image of the copy's region in the destination index space
+Box3i copyImage(const hc_copy_box& C) {
+  Box3i r;
+  for (int d = 0; d < 3; ++d) {
+    const int a = C.sign[d] * C.lo[C.perm[d]] + C.shift[d], b = C.sign[d] * C.hi[C.perm[d]] + C.shift[d];
+    r.lo[d] = a < b ? a : b;
+    r.hi[d] = a < b ? b : a;
+  }
+  return r;
+}
+Box3i copyRegion(const hc_copy_box& C) {
+  Box3i r;
+  for (int d = 0; d < 3; ++d) { r.lo[d] = C.lo[d]; r.hi[d] = C.hi[d]; }
+  return r;
+}
+bool copyOk(const hc_copy_box& C) {
+  if (!C.src || !C.dst || C.ncomp < 1 || C.ncomp > 16) return false;
+  bool seen[3] = {false, false, false};
+  long long sN = 1, dN = 1;
+  for (int d = 0; d < 3; ++d) {
+    if (C.perm[d] < 0 || C.perm[d] > 2 || seen[C.perm[d]]) return false;
+    seen[C.perm[d]] = true;
+    if (C.sign[d] != 1 && C.sign[d] != -1) return false;
+    if (C.lo[d] > C.hi[d] || C.src_n[d] < 1 || C.dst_n[d] < 1) return false;
+    sN *= C.src_n[d];
+    dN *= C.dst_n[d];
+  }
+  if (16 * sN >= 0x7fffffffLL || 16 * dN >= 0x7fffffffLL) return false;
+  const Box3i img = copyImage(C);
+  return regionIn(C.lo, C.hi, C.src_lo, C.src_n) && regionIn(img.lo, img.hi, C.dst_lo, C.dst_n);
+}
+
+}  // namespace
+
+extern "C" int hc_amr_plan_set_copies(hc_amr_plan* P, const hc_copy_box* copies, int ncopy) {
+  if (!P || ncopy < 0 || (ncopy && !copies)) return argFail("hc_amr_plan_set_copies: bad argument");
+  std::vector<Chunk> cc;
+  std::vector<int> start;
+  for (int q = 0; q < ncopy; ++q) {
+    if (!copyOk(copies[q]))
+      return argFail("hc_amr_plan_set_copies: a copy needs both arrays, a signed permutation, ncomp 1..16, its "
+                     "region in the source box and the region's image in the destination box");
+    start.push_back((int)cc.size());
+    const hc_copy_box& C = copies[q];
+    addChunks(cc, q, (long long)(C.hi[0] - C.lo[0] + 1) * (C.hi[1] - C.lo[1] + 1) * (C.hi[2] - C.lo[2] + 1));
+  }
+  start.push_back((int)cc.size());
+  hc_copy_box* dev = nullptr;
+  Chunk* devChunks = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (ncopy) {
+    e = cudaMalloc(&dev, sizeof(hc_copy_box) * ncopy);
+    if (e == cudaSuccess) e = cudaMemcpy(dev, copies, sizeof(hc_copy_box) * ncopy, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&devChunks, sizeof(Chunk) * cc.size());
+    if (e == cudaSuccess) e = cudaMemcpy(devChunks, cc.data(), sizeof(Chunk) * cc.size(), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(dev);
+    cudaFree(devChunks);
+    return cudaFailed(e, "hc_amr_plan_set_copies");
+  }
+  cudaFree(P->copies);
+  cudaFree(P->copyChunks);
+  P->copies = dev;
+  P->copyChunks = devChunks;
+  P->copyHost.assign(copies, copies + ncopy);
+  P->copyStart = start;
+  P->copyRangesChecked.clear();
+  return HC_OK;
+}
+
+extern "C" int hc_amr_copy(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, void* stream) {
+  if (!ctx || !P) return argFail("hc_amr_copy: null argument");
+  const int n = (int)P->copyHost.size();
+  if (first < 0 || count < 0 || first + count > n) return argFail("hc_amr_copy: range outside the plan");
+  // per array: every written region against every other access of that
+  // array in the launch (reads and writes), grouped by array; a range found
+  // race free is remembered (the copies of a plan do not change)
+  const std::pair<int, int> range{first, count};
+  const bool known = std::find(P->copyRangesChecked.begin(), P->copyRangesChecked.end(), range) !=
+                     P->copyRangesChecked.end();
+  std::vector<std::pair<const void*, std::pair<Box3i, int>>> acc;  // array, (region, copy index * 2 + write)
+  for (int q = first; q < first + count && !known; ++q) {
+    const hc_copy_box& C = P->copyHost[q];
+    acc.push_back({C.src, {copyRegion(C), 2 * q}});
+    acc.push_back({C.dst, {copyImage(C), 2 * q + 1}});
+  }
+  std::sort(acc.begin(), acc.end(), [](const auto& a, const auto& b) {
+    return std::less<const void*>()(a.first, b.first);
+  });
+  for (size_t a = 0; a < acc.size(); ++a)
+    for (size_t b = a + 1; b < acc.size() && acc[b].first == acc[a].first; ++b) {
+      const bool wa = acc[a].second.second & 1, wb = acc[b].second.second & 1;
+      if (!wa && !wb) continue;
+      if (overlaps(acc[a].second.first, acc[b].second.first))
+        return argFail("hc_amr_copy: a copy of the launch writes a region another access of the launch uses");
+    }
+  if (!known) P->copyRangesChecked.push_back(range);
+  const int c0 = count ? P->copyStart[first] : 0, c1 = count ? P->copyStart[first + count] : 0;
+  if (c1 == c0) return HC_OK;
+  copyKernel<<<c1 - c0, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->copies, P->copyChunks + c0);
+  return cudaFailed(cudaGetLastError(), "hc_amr_copy");
 }

@@ -594,6 +594,23 @@ class AmrPlan:
         N.check(self._lib.hc_amr_cf_interpolate(self._shell._ctx, self._h, first, count, _stream()),
                 "hc_amr_cf_interpolate")
 
+    def set_copies(self, copies) -> None:
+        """copies: dicts with src, dst (device tensors), src_lo, src_n,
+        dst_lo, dst_n, lo, hi, perm, sign, shift (3 ints each) and ncomp
+        (hc_copy_box)."""
+        n = len(copies)
+        arr = (N.HcCopyBox * max(n, 1))()
+        for q, d in enumerate(copies):
+            arr[q].src = d["src"].data_ptr()
+            arr[q].dst = d["dst"].data_ptr()
+            for k in ("src_lo", "src_n", "dst_lo", "dst_n", "lo", "hi", "perm", "sign", "shift"):
+                getattr(arr[q], k)[:] = list(d[k])
+            arr[q].ncomp = d["ncomp"]
+        N.check(self._lib.hc_amr_plan_set_copies(self._h, arr, n), "hc_amr_plan_set_copies")
+
+    def copy(self, first: int, count: int) -> None:
+        N.check(self._lib.hc_amr_copy(self._shell._ctx, self._h, first, count, _stream()), "hc_amr_copy")
+
     def set_cf_fine(self, boxes) -> None:
         """boxes: dicts with jac, donor, state, mapped, out (device tensors)
         and their *_lo / *_n boxes, valid_lo, valid_hi, block_lo, block_hi

@@ -402,6 +402,34 @@ typedef struct hc_cf_fine_box {
   int block_lo[3], block_hi[3];
 } hc_cf_fine_box;
 
+/* One region copy between two SoA arrays: the same-level exchanges and
+ * the coarse-to-fine source copies of the AMR prepare
+ * (src/MHD_AMRFourthOrder.H:19-24,58,83-85).  For every point x of the
+ * region lo .. hi (source index space) and every component c,
+ *   dst(y, c) = src(x, c),   y[d] = sign[d] * x[perm[d]] + shift[d],
+ * perm a permutation of {0, 1, 2} and sign[d] = +1 or -1: the index map
+ * between two panels of the cubed sphere is a signed permutation; within
+ * a panel perm = {0, 1, 2}, sign = {1, 1, 1}.  The region must lie in the
+ * source box and its image in the destination box; ncomp 1..16. */
+typedef struct hc_copy_box {
+  const double* src;
+  double* dst;
+  int src_lo[3], src_n[3];
+  int dst_lo[3], dst_n[3];
+  int lo[3], hi[3];
+  int perm[3], sign[3], shift[3];
+  int ncomp;
+} hc_copy_box;
+
+/* Validate and keep a device copy of the plan's copies. */
+int hc_amr_plan_set_copies(hc_amr_plan* plan, const hc_copy_box* copies, int ncopy);
+
+/* Copies first .. first+count-1 of the plan in one launch.  Within one
+ * launch no written region may overlap another copy's written or read
+ * region of the same array (an exchange writes ghosts and reads valid
+ * cells, so a level's exchange is one launch). */
+int hc_amr_copy(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
+
 int hc_amr_plan_set_cf_fine(hc_amr_plan* plan, const hc_cf_fine_box* boxes, int nbox);
 int hc_amr_cf_mapped(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
 int hc_amr_cf_quotient(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);

@@ -578,6 +578,18 @@ def amr_cf_quotient(jac, jac_lo, mapped, mapped_lo, out, out_lo, valid_lo, valid
                     out[c, k - out_lo[2], j - out_lo[1], i - out_lo[0]] = Q(p) - correction / (12.0 * Jp)
 
 
+def amr_copy(src, src_lo, dst, dst_lo, lo, hi, perm, sign, shift) -> None:
+    """dst(y) = src(x) over the region lo..hi, y[d] = sign[d] x[perm[d]] + shift[d]
+    (the exchanges and coarse copies of src/MHD_AMRFourthOrder.H:19-24,58,83-85)."""
+    for k in range(lo[2], hi[2] + 1):
+        for j in range(lo[1], hi[1] + 1):
+            for i in range(lo[0], hi[0] + 1):
+                x = (i, j, k)
+                y = [sign[d] * x[perm[d]] + shift[d] for d in range(3)]
+                dst[:, y[2] - dst_lo[2], y[1] - dst_lo[1], y[0] - dst_lo[0]] = \
+                    src[:, k - src_lo[2], j - src_lo[1], i - src_lo[0]]
+
+
 def cme_schedule(events, time: float, feeding: float) -> tuple[float, float]:
     """(CFL fraction, Rusanov window end) of the oracle's schedule."""
     n = len(events)

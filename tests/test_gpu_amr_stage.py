@@ -241,3 +241,46 @@ def test_cf_fine_recovery_matches_oracle(oracle_lib):
     with pytest.raises(hc.HcError):
         plan.set_cf_fine([bad])
     plan.close()
+
+
+def test_region_copies_match_oracle(oracle_lib):
+    """hc_amr_copy: an in-panel ghost exchange between two boxes and a
+    cross-panel copy with a signed axis permutation, one launch; a launch
+    whose write overlaps another copy's read is refused."""
+    _need_gpu()
+    po = oracle_lib
+    rng = np.random.default_rng(5)
+    sh = hc.Shell(hc.Params(nr=8, na=8))
+    plan = AmrPlan(sh, [])
+    a = rng.normal(size=(8, 10, 10, 10))      # box A over -1 .. 8 (1 ghost around 0 .. 7)
+    b = rng.normal(size=(8, 10, 10, 10))      # box B over 7 .. 16 along i, -1 .. 8 otherwise
+    c = rng.normal(size=(8, 6, 8, 4))         # another panel's array over (0..3, 0..7, 0..5)
+    ta, tb, tc = (torch.from_numpy(x.copy()).cuda() for x in (a, b, c))
+    copies = [
+        # B's low ghost layer (i = 7) from A's valid i = 7
+        dict(src=ta, dst=tb, src_lo=(-1, -1, -1), src_n=(10, 10, 10), dst_lo=(7, -1, -1), dst_n=(10, 10, 10),
+             lo=(7, 0, 0), hi=(7, 7, 7), perm=(0, 1, 2), sign=(1, 1, 1), shift=(0, 0, 0), ncomp=8),
+        # A's high ghost layer (i = 8) from B's valid i = 8
+        dict(src=tb, dst=ta, src_lo=(7, -1, -1), src_n=(10, 10, 10), dst_lo=(-1, -1, -1), dst_n=(10, 10, 10),
+             lo=(8, 0, 0), hi=(8, 7, 7), perm=(0, 1, 2), sign=(1, 1, 1), shift=(0, 0, 0), ncomp=8),
+        # C's layer k = 0 into A's low k ghost layer with a signed permutation:
+        # y = (j, 3 - i, k - 1), i.e. A cells (0..7, 0..3, -1)
+        dict(src=tc, dst=ta, src_lo=(0, 0, 0), src_n=(4, 8, 6), dst_lo=(-1, -1, -1), dst_n=(10, 10, 10),
+             lo=(0, 0, 0), hi=(3, 7, 0), perm=(1, 0, 2), sign=(1, -1, 1), shift=(0, 3, -1), ncomp=8),
+    ]
+    plan.set_copies(copies)
+    plan.copy(0, 3)
+    torch.cuda.synchronize()
+    wa, wb = a.copy(), b.copy()
+    po.amr_copy(a, (-1, -1, -1), wb, (7, -1, -1), (7, 0, 0), (7, 7, 7), (0, 1, 2), (1, 1, 1), (0, 0, 0))
+    po.amr_copy(b, (7, -1, -1), wa, (-1, -1, -1), (8, 0, 0), (8, 7, 7), (0, 1, 2), (1, 1, 1), (0, 0, 0))
+    po.amr_copy(c, (0, 0, 0), wa, (-1, -1, -1), (0, 0, 0), (3, 7, 0), (1, 0, 2), (1, -1, 1), (0, 3, -1))
+    assert np.array_equal(ta.cpu().numpy(), wa)
+    assert np.array_equal(tb.cpu().numpy(), wb)
+    # a copy writing A's valid cells while another reads them: refused
+    racy = dict(copies[0], src=tb, dst=ta, src_lo=(7, -1, -1), dst_lo=(-1, -1, -1), lo=(8, 0, 0), hi=(8, 7, 7),
+                shift=(-1, 0, 0))
+    plan.set_copies([copies[0], racy])
+    with pytest.raises(hc.HcError):
+        plan.copy(0, 2)
+    plan.close()

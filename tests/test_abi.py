@@ -73,3 +73,38 @@ def test_no_device_is_an_error_not_a_fallback(product_lib_path):
     from heliocubed_b200 import HcError, Params, Shell
     with pytest.raises(HcError):
         Shell(Params(nr=8, na=8))
+
+
+def _c_name(cls_name: str) -> str:
+    """HcCfFineBox -> hc_cf_fine_box."""
+    return "hc" + re.sub(r"([A-Z])", lambda m: "_" + m.group(1).lower(), cls_name[2:])
+
+
+def test_every_struct_layout_matches_the_compiler(tmp_path):
+    """Sizes and field offsets of every ctypes mirror against what the C
+    compiler lays out for the header's structs (gcc on the host)."""
+    import shutil
+    import subprocess
+    from heliocubed_b200 import _native
+    if shutil.which("gcc") is None:
+        pytest.skip("no host C compiler")
+    mirrors = [getattr(_native, n) for n in dir(_native)
+               if n.startswith("Hc") and isinstance(getattr(_native, n), type)
+               and issubclass(getattr(_native, n), C.Structure)]
+    assert len(mirrors) >= 12
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
+    expect = []
+    for cls in mirrors:
+        cname = _c_name(cls.__name__)
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        expect.append(C.sizeof(cls))
+        for field, _ in cls._fields_:
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {field}));')
+            expect.append(getattr(cls, field).offset)
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == expect

@@ -377,6 +377,7 @@ struct hc_amr_plan {
   Chunk* cfChunks = nullptr;
   std::vector<hc_cf_box> cfHost;
   std::vector<int> cfChunkStart;
+  mutable std::vector<std::pair<int, int>> cfRangesChecked, cfFineRangesChecked[2];
 };
 
 extern "C" int hc_amr_plan_create(hc_ctx* ctx, const hc_rk_box* boxes, int nbox, const hc_restrict_box* restricts,
@@ -713,6 +714,7 @@ extern "C" int hc_amr_plan_set_cf_interp(hc_amr_plan* P, const hc_cf_box* boxes,
   P->cfChunks = devChunks;
   P->cfHost.assign(boxes, boxes + nbox);
   P->cfChunkStart = start;
+  P->cfRangesChecked.clear();
   return HC_OK;
 }
 
@@ -721,15 +723,20 @@ extern "C" int hc_amr_cf_interpolate(hc_ctx* ctx, const hc_amr_plan* P, int firs
   const int n = (int)P->cfHost.size();
   if (first < 0 || count < 0 || first + count > n) return argFail("hc_amr_cf_interpolate: range outside the plan");
   // boxes of one launch must write disjoint fine regions of each array
-  for (int a = first; a < first + count; ++a)
-    for (int b = a + 1; b < first + count; ++b) {
-      const hc_cf_box &A = P->cfHost[a], &B = P->cfHost[b];
-      if (A.fine != B.fine) continue;
-      bool overlap = true;
-      for (int d = 0; d < 3 && overlap; ++d)
-        overlap = A.fine_lo[d] < B.fine_lo[d] + B.fine_n[d] && B.fine_lo[d] < A.fine_lo[d] + A.fine_n[d];
-      if (overlap) return argFail("hc_amr_cf_interpolate: two boxes of one launch write the same fine array region");
-    }
+  // (checked once per launch range: the boxes of a plan do not change)
+  const std::pair<int, int> range{first, count};
+  if (std::find(P->cfRangesChecked.begin(), P->cfRangesChecked.end(), range) == P->cfRangesChecked.end()) {
+    for (int a = first; a < first + count; ++a)
+      for (int b = a + 1; b < first + count; ++b) {
+        const hc_cf_box &A = P->cfHost[a], &B = P->cfHost[b];
+        if (A.fine != B.fine) continue;
+        bool overlap = true;
+        for (int d = 0; d < 3 && overlap; ++d)
+          overlap = A.fine_lo[d] < B.fine_lo[d] + B.fine_n[d] && B.fine_lo[d] < A.fine_lo[d] + A.fine_n[d];
+        if (overlap) return argFail("hc_amr_cf_interpolate: two boxes of one launch write the same fine array region");
+      }
+    P->cfRangesChecked.push_back(range);
+  }
   const int c0 = count ? P->cfChunkStart[first] : 0, c1 = count ? P->cfChunkStart[first + count] : 0;
   if (c1 == c0) return HC_OK;
   cfInterpKernel<<<c1 - c0, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->cf, P->cfChunks + c0);
@@ -818,6 +825,8 @@ extern "C" int hc_amr_plan_set_cf_fine(hc_amr_plan* P, const hc_cf_fine_box* box
   P->cfFineHost.assign(boxes, boxes + nbox);
   P->cfMappedStart = ms;
   P->cfQuotientStart = qs;
+  P->cfFineRangesChecked[0].clear();
+  P->cfFineRangesChecked[1].clear();
   return HC_OK;
 }
 
@@ -828,13 +837,18 @@ int cfFineLaunch(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, void* 
   const int n = (int)P->cfFineHost.size();
   if (first < 0 || count < 0 || first + count > n)
     return argFail(mapped ? "hc_amr_cf_mapped: range outside the plan" : "hc_amr_cf_quotient: range outside the plan");
-  for (int a = first; a < first + count; ++a)
-    for (int b = a + 1; b < first + count; ++b) {
-      const hc_cf_fine_box &A = P->cfFineHost[a], &B = P->cfFineHost[b];
-      if ((mapped && A.mapped == B.mapped) || (!mapped && A.out == B.out))
-        return argFail(mapped ? "hc_amr_cf_mapped: two boxes of one launch write the same array"
-                              : "hc_amr_cf_quotient: two boxes of one launch write the same array");
-    }
+  auto& checked = P->cfFineRangesChecked[mapped ? 0 : 1];
+  const std::pair<int, int> range{first, count};
+  if (std::find(checked.begin(), checked.end(), range) == checked.end()) {
+    for (int a = first; a < first + count; ++a)
+      for (int b = a + 1; b < first + count; ++b) {
+        const hc_cf_fine_box &A = P->cfFineHost[a], &B = P->cfFineHost[b];
+        if ((mapped && A.mapped == B.mapped) || (!mapped && A.out == B.out))
+          return argFail(mapped ? "hc_amr_cf_mapped: two boxes of one launch write the same array"
+                                : "hc_amr_cf_quotient: two boxes of one launch write the same array");
+      }
+    checked.push_back(range);
+  }
   const std::vector<int>& st = mapped ? P->cfMappedStart : P->cfQuotientStart;
   const int c0 = count ? st[first] : 0, c1 = count ? st[first + count] : 0;
   if (c1 == c0) return HC_OK;

@@ -515,6 +515,33 @@ class O4Batch:
             pass
 
 
+def amr_exchange_copies(boxes, ghost: int):
+    """Same-panel ghost exchange of one level as region copies
+    (hc_copy_box descriptors without the array pointers): for every ordered
+    pair of boxes (b, a) on the same panel, the cells of box a's storage
+    region (valid.grow(ghost)) that lie in box b's valid region are copied
+    from b to a with the identity index map.  boxes: (panel, lo, hi) per
+    box, inclusive valid bounds.  Returns dicts with src_box and dst_box (box
+    indices), lo, hi, perm, sign and shift; the caller adds the arrays and
+    their boxes (valid.grow(ghost)) and passes them to AmrPlan.set_copies.
+    Copies across panels (signed permutations of the index space) are the
+    caller's."""
+    out = []
+    for a, (pa, alo, ahi) in enumerate(boxes):
+        slo = [alo[d] - ghost for d in range(3)]
+        shi = [ahi[d] + ghost for d in range(3)]
+        for b, (pb, blo, bhi) in enumerate(boxes):
+            if b == a or pb != pa:
+                continue
+            lo = [max(slo[d], blo[d]) for d in range(3)]
+            hi = [min(shi[d], bhi[d]) for d in range(3)]
+            if any(lo[d] > hi[d] for d in range(3)):
+                continue
+            out.append({"src_box": b, "dst_box": a, "lo": lo, "hi": hi, "perm": (0, 1, 2), "sign": (1, 1, 1),
+                        "shift": (0, 0, 0)})
+    return out
+
+
 def amr_cf_weights(ratio: int, child: int) -> np.ndarray:
     """hc_amr_cf_weights: the five coarse weights of child `child` of a cell
     refined by `ratio` (host arithmetic; no device needed)."""

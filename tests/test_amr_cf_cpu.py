@@ -190,3 +190,47 @@ def test_oracle_fine_quotient_is_fourth_order():
         return np.max(np.abs(out[0] - exact))
     e1, e2 = case(0.2), case(0.1)
     assert e1 / e2 > 12.0, (e1, e2)
+
+
+def test_exchange_copies_fill_ghosts_from_neighbours():
+    """amr_exchange_copies on three boxes of one panel (and one on another
+    panel): applied with the oracle's region copy, every ghost cell covered
+    by a neighbour's valid cells gets the neighbour's value of a global
+    field; ghosts outside every neighbour keep their fill; no valid cell is
+    written."""
+    from heliocubed_b200.level import amr_exchange_copies
+    g = 2
+    boxes = [(0, (0, 0, 0), (3, 3, 3)), (0, (4, 0, 0), (7, 3, 3)), (0, (0, 4, 0), (3, 7, 3)), (1, (4, 0, 0), (7, 3, 3))]
+    field = lambda x: 1000.0 * x[0] + 100.0 * x[1] + 10.0 * x[2]
+    arrays = []
+    for panel, lo, hi in boxes:
+        n = [hi[d] - lo[d] + 1 + 2 * g for d in range(3)]
+        a = np.full((1, n[2], n[1], n[0]), -1.0)
+        for k in range(lo[2], hi[2] + 1):
+            for j in range(lo[1], hi[1] + 1):
+                for i in range(lo[0], hi[0] + 1):
+                    a[0, k - lo[2] + g, j - lo[1] + g, i - lo[0] + g] = field((i, j, k)) + 1e6 * panel
+        arrays.append(a)
+    before = [a.copy() for a in arrays]
+    copies = amr_exchange_copies(boxes, g)
+    assert all(boxes[c["src_box"]][0] == boxes[c["dst_box"]][0] for c in copies)
+    for c in copies:
+        sb, db = boxes[c["src_box"]], boxes[c["dst_box"]]
+        po.amr_copy(before[c["src_box"]], [v - g for v in sb[1]], arrays[c["dst_box"]], [v - g for v in db[1]],
+                    c["lo"], c["hi"], c["perm"], c["sign"], c["shift"])
+    for b, (panel, lo, hi) in enumerate(boxes):
+        a = arrays[b]
+        n = a.shape[1:][::-1]
+        for k in range(n[2]):
+            for j in range(n[1]):
+                for i in range(n[0]):
+                    x = (lo[0] - g + i, lo[1] - g + j, lo[2] - g + k)
+                    valid = all(lo[d] <= x[d] <= hi[d] for d in range(3))
+                    owner = [q for q, (pq, ql, qh) in enumerate(boxes)
+                             if pq == panel and all(ql[d] <= x[d] <= qh[d] for d in range(3))]
+                    if valid:
+                        assert a[0, k, j, i] == before[b][0, k, j, i]
+                    elif owner:
+                        assert a[0, k, j, i] == field(x) + 1e6 * panel
+                    else:
+                        assert a[0, k, j, i] == -1.0

@@ -25,6 +25,9 @@
 #include <limits>
 #include <cstdint>
 #include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <vector>
 
 #include "../include/hc_abi.h"
@@ -1566,4 +1569,87 @@ void orc_plm(const double* mm, const double* m, const double* c, const double* p
 void orc_cart_prim(const double* in, double inverseJ, double gamma, double* out) {
   cartesianPrimitiveFromConserved(out, in, inverseJ, gamma);
 }
+
+// Fourth-order (Berta) pointwise pieces for pinning against the reference's
+// own kernels.  States of 8 components, stencils laid out [cell][component].
+void orc_berta_wenoz(const double* cells, double* wl, double* wr) {
+  for (int c = 0; c < 8; ++c) {
+    double in[6];
+    for (int s = 0; s < 6; ++s) in[s] = cells[8 * s + c];
+    wenozFace(in, wl[c], wr[c]);
+  }
+}
+void orc_berta_weno3(const double* cells, double dx2, double* wl, double* wr) {
+  for (int c = 0; c < 8; ++c) {
+    double in[4];
+    for (int s = 0; s < 4; ++s) in[s] = cells[8 * s + c];
+    weno3Face(in, dx2, wl[c], wr[c]);
+  }
+}
+void orc_berta_plm(const double* cells, double* wl, double* wr) {
+  for (int c = 0; c < 8; ++c) {
+    double in[4];
+    for (int s = 0; s < 4; ++s) in[s] = cells[8 * s + c];
+    plmFallbackFace(in, wl[c], wr[c]);
+  }
+}
+// n = 4 or 6 values, normalised in place; returns the scale.
+double orc_berta_normalize(double* v, int n) {
+  if (n == 4) return normalizeStencil(*reinterpret_cast<double(*)[4]>(v));
+  if (n == 6) return normalizeStencil(*reinterpret_cast<double(*)[6]>(v));
+  return std::nan("");
+}
+// cells [7][8]: the cell, then the low and high neighbours in directions 0, 1, 2.
+double orc_berta_jameson(const double* cells, double eta_d) {
+  const double* lo[3] = {cells + 8, cells + 24, cells + 40};
+  const double* hi[3] = {cells + 16, cells + 32, cells + 48};
+  return jamesonRawFlag(cells, lo, hi, eta_d);
+}
+void orc_berta_avg_to_point(const double* avg, const double* lap, double theta, double* out) {
+  for (int c = 0; c < 8; ++c) out[c] = avgToPoint(avg[c], lap[c], theta);
+}
+void orc_berta_flux_to_avg(const double* pt, const double* lap, double theta, double* out) {
+  for (int c = 0; c < 8; ++c) out[c] = fluxPointToAvg(pt[c], lap[c], theta);
+}
+// The stencil-flag choice between the WENOZ states (wl4, wr4) and the
+// fallback states, then the positivity clamp.
+void orc_berta_select(const double* wl4, const double* wr4, const double* wlf, const double* wrf, double theta,
+                      double* wl, double* wr) {
+  const bool smooth = theta > 0.5;
+  for (int c = 0; c < 8; ++c) {
+    wl[c] = smooth ? wl4[c] : wlf[c];
+    wr[c] = smooth ? wr4[c] : wrf[c];
+    clampReconstructed(c, wl[c], wr[c]);
+  }
+}
+// Matrices and fluxes laid out [column][cell], n columns, `size` cells.
+void orc_berta_mapped_line(int n, int both, const double* m, const double* m1, const double* m2, const double* f,
+                           const double* f1, const double* f2, int size, double* out) {
+  for (int cell = 0; cell < size; ++cell) {
+    double a[3], a1[3], a2[3], g[3], g1[3], g2[3];
+    for (int col = 0; col < n; ++col) {
+      const size_t q = (size_t)col * size + cell;
+      a[col] = m[q]; a1[col] = m1[q]; a2[col] = m2[q]; g[col] = f[q]; g1[col] = f1[q]; g2[col] = f2[q];
+    }
+    out[cell] = mappedSum(n, both != 0, a, a1, a2, g, g1, g2);
+  }
+}
+void orc_sph_to_prim_raw(const double* u, double* w) { sphToPrimRaw(u, w); }
+void orc_prim_flux(const double* w, double ke, double me, double vb, double gamma, int c, double* f) {
+  primFlux(f, w, ke, me, vb, gamma, c);
+}
+void orc_mapped_roe(const double* wl, const double* wr, const double* A9, double radialArea, int dir, double gamma,
+                    double ef, double floor, double* out) {
+  double A[3][3];
+  for (int r = 0; r < 3; ++r) for (int s = 0; s < 3; ++s) A[r][s] = A9[3 * r + s];
+  mappedRoe(out, wl, wr, A, radialArea, dir, gamma, ef, floor);
+}
+void orc_factored_roe(const double* wl, const double* wr, const double* A9, double radialArea, int dir, double gamma,
+                      double ef, double floor, double* out) {
+  double A[3][3];
+  for (int r = 0; r < 3; ++r) for (int s = 0; s < 3; ++s) A[r][s] = A9[3 * r + s];
+  factoredRoe(out, wl, wr, A, radialArea, dir, gamma, ef, floor);
+}
+int orc_usable_primitive(const double* w) { return usablePrimitive(w) ? 1 : 0; }
+double orc_rho_floor() { return RHO00; }
 }

@@ -125,8 +125,33 @@ def lib() -> C.CDLL:
         L.orc_o4_rk4_step.argtypes = [C.c_void_p, _D, C.c_double, C.c_double]
         L.orc_o4_inv_dt.restype = C.c_double
         L.orc_o4_inv_dt.argtypes = [C.c_void_p, _D]
+        _berta_signatures(L, "orc")
+        L.orc_usable_primitive.argtypes = [_D]
         _orc = L
     return _orc
+
+
+def _berta_signatures(L: C.CDLL, prefix: str) -> None:
+    """Signatures shared by the oracle's and the reference pin's fourth-order
+    pointwise exports (prefix orc_ or ref_)."""
+    f = lambda name: getattr(L, f"{prefix}_{name}")  # noqa: E731
+    f("berta_wenoz").argtypes = [_D, _D, _D]
+    f("berta_weno3").argtypes = [_D, C.c_double, _D, _D]
+    f("berta_plm").argtypes = [_D, _D, _D]
+    f("berta_normalize").argtypes = [_D, C.c_int]
+    f("berta_normalize").restype = C.c_double
+    f("berta_jameson").argtypes = [_D, C.c_double]
+    f("berta_jameson").restype = C.c_double
+    f("berta_avg_to_point").argtypes = [_D, _D, C.c_double, _D]
+    f("berta_flux_to_avg").argtypes = [_D, _D, C.c_double, _D]
+    f("berta_select").argtypes = [_D, _D, _D, _D, C.c_double, _D, _D]
+    f("berta_mapped_line").argtypes = [C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, C.c_int, _D]
+    f("sph_to_prim_raw").argtypes = [_D, _D]
+    f("prim_flux").argtypes = [_D, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _D]
+    f("rho_floor").restype = C.c_double
+    if prefix == "orc":
+        f("mapped_roe").argtypes = [_D, _D, _D, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, _D]
+        f("factored_roe").argtypes = [_D, _D, _D, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, _D]
 
 
 def ref_lib() -> C.CDLL | None:
@@ -147,6 +172,7 @@ def ref_lib() -> C.CDLL | None:
         L.ref_cone_prepare.argtypes = [_D, C.c_double, _D]
         L.ref_cone_cell.argtypes = [_D, C.c_double, C.c_double, _D, _D, C.c_double, _D]
         L.ref_cme_schedule.argtypes = [_D, _D, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _D]
+        _berta_signatures(L, "ref")
         _ref = L
     return _ref
 

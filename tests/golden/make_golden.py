@@ -1,13 +1,19 @@
 """Generate tests/golden/riemann_pin.npz from the reference's own pointwise
 solvers (src/MHD_Roe8Wave.H, src/MHD_SecondOrderFlux.H compiled from the
-reference tree by oracle/build.py into oracle/_ref/libhcref.so).
+reference tree by oracle/build.py into oracle/_ref/libhcref.so), and
+tests/golden/berta_pin.npz from the reference's fourth-order pointwise
+kernels (WENOZ/WENO3/PLM face states, stencil normalisation, Jameson flag,
+point/average corrections, reconstruction select, mapped-flux line,
+f_sphToPrim, f_primflux, mapped and factored Roe, usable-state check; the
+inputs are oracle/berta_pin.cases(20261205)).
 
 The fixture pins the oracle's restatement (tests/test_oracle_pin.py) on
 machines where the reference tree is absent.  Inputs are seeded random
 solar-wind-like primitive states (CGS) in the face frame, including cases
 where the Roe fan check falls back to Rusanov.
 
-Run: python tests/golden/make_golden.py   (needs python oracle/build.py first)
+Run: python tests/golden/make_golden.py
+(needs HC_REFERENCE=<reference tree> python oracle/build.py first)
 """
 from __future__ import annotations
 
@@ -22,6 +28,8 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from oracle import pyoracle as po  # noqa: E402
 
 C_MP = 1.67262192e-24
+BERTA_SEED = 20261205
+BERTA_CASES = 256
 
 
 def states(rng, n):
@@ -66,6 +74,12 @@ def main() -> int:
                         roe_nocheck_ok=roe_nc_ok, rusanov=rus, flux_rusanov=flux_rus, flux_roe=flux_roe,
                         frames=frames, norms=norms)
     print("wrote riemann_pin.npz;", int((roe_ok == 0).sum()), "Roe fallbacks of", n)
+    from oracle import berta_pin
+    cases = berta_pin.cases(BERTA_SEED, n=BERTA_CASES)
+    outs = berta_pin.evaluate(R, "ref", cases)
+    np.savez_compressed(os.path.join(HERE, "berta_pin.npz"), **{f"in_{k}": v for k, v in cases.items()},
+                        **{f"out_{k}": v for k, v in outs.items()})
+    print("wrote berta_pin.npz;", BERTA_CASES, "cases")
     return 0
 
 

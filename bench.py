@@ -1,27 +1,42 @@
-"""Benchmark: FP64 cell-updates/s of the cubed-sphere MHD RK4 step on B200.
+"""Benchmark: FP64 cell-updates/s of the cubed-sphere MHD update on one B200,
+batched (served ensemble) vs plain per-solve launches, with the ensemble's
+p50/p99 time-to-solution.
 
-One step = one classical RK4 step of the whole six-panel shell (4 operator
-evaluations with their stage preparation and RK update), with dt = cfl /
-max CFL rate computed on the device before every step.  One cell-update =
-one valid cell advanced one full RK4 step.
+One cell-update = one valid cell advanced one full RK4 step (4 operator
+evaluations with their stage preparation and RK update), dt = cfl / max CFL
+rate computed on the device before every step.
 
 Workloads (synthetic input; the reference ships no data for them), gamma
 5/3, r in [21.5, 215] Rsun, radial stretch 1.5, CFL 0.4, Powell on:
-  --order 4 (default): fourth-order Berta pointwise WENOZ (Jameson detector,
-      WENO3 fallback) + Roe 8-wave, 64 radial x 64 x 64 angular cells per
-      panel (1,572,864 cells); Parker-like wind with seeded 5 % tangential
-      perturbations of v and of B (B_t the surface curl of a seeded stream
-      function).
-  --order 2: second-order PLM-MC + Rusanov, 32 x 32^2 x 6 (196,608 cells);
-      Parker-like wind + seeded Gaussian pressure pulse.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--order 2|4]
+  --workload serve (default): the served CME ensemble.  256 requests arrive
+      as a seeded Poisson stream whose rate puts about 8 solves in flight;
+      each has a grid of {32,48,64,96} radial x {32,48,64}^2 cells per panel,
+      the scheme PLM-MC + Rusanov or Berta WENOZ + Roe (50/50) and a
+      cone-CME cloud (speed U[500, 2000] km/s, half-width U[20, 60] deg,
+      lat/lon U[-30, 30] deg, density ratio U[2, 6]) inserted on the device
+      at admission; --steps RK4 steps per request.  The same requests run
+      through the continuous-batching server (value) and one after another
+      through plain per-solve launches (plain).  e2e: the served run with
+      every request's initial state copied from pinned host memory at
+      admission.  The same line carries the large single solve
+      (large_solve: 256 x 192^2 x 6, WENOZ + Roe + solar gravity, cone of
+      1500 km/s and 45 deg), whose operator gives the roofline.
+  --workload uniform: one solve advanced --steps RK4 steps (--order 4:
+      64 x 64^2 x 6 WENOZ + Roe on the perturbed wind; --order 2: 32 x 32^2
+      x 6 PLM-MC + Rusanov on the pressure pulse; --nr/--na/--gravity/--init
+      cone for other sizes).
+  --workload amr: the AMR-style box batch (boxes of 8^3-32^3 on three
+      levels), batched vs per-box launches.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ...]
 
 N > 1 (torchrun): every rank runs an independent replica of the workload
 (weak scaling; the path has no exchange between replicas), timed on the
 device and reduced as the max over ranks.  --impl reference times the CPU
 restatement of the reference's algorithm (the reference itself cannot be
-built: its Proto dependency is absent) on the host cores.
+built: its Proto dependency is absent) on the host cores, on a bounded
+sample of the same workload.
 """
 from __future__ import annotations
 
@@ -40,7 +55,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "FP64 cell-updates/s on 1 B200 (RK4 step of the cubed-sphere MHD update)"
+METRIC = "FP64 cell-updates/s on 1 B200, batched vs plain; ensemble p50/p99 latency"
+METRIC_UNIFORM = "FP64 cell-updates/s on 1 B200 (RK4 step of the cubed-sphere MHD update)"
 UNIT = "cell-updates/s"
 L2_BYTES = 126 * 1024 * 1024
 OPERATOR_BYTES_PER_CELL_STAGE = 128  # read 8 FP64 primitives, write 8 FP64 rhs
@@ -266,13 +282,29 @@ def cpu_baseline(args, budget_s: float = 12.0) -> dict:
 
 
 def run_reference(args, world, rank):
+    """The CPU arm: the oracle (the reference's algorithm restated; the
+    reference itself needs the absent Proto library) on the host cores, on
+    a bounded sample of the same workload, with the workload's metric."""
     if rank != 0:
         return
-    cb = cpu_baseline(args, budget_s=args.ref_budget)
-    out = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+    if args.workload == "serve":
+        reqs = serve_requests(args, None)
+        cb = cpu_baseline_serve(args, reqs, budget_s=args.ref_budget)
+        metric = METRIC
+        config = {"workload": "served CME ensemble (config 4): %d requests, %d RK4 steps each"
+                              % (len(reqs), args.steps),
+                  "requests": len(reqs), "steps_per_request": args.steps,
+                  "sample": "CPU oracle on the ensemble's smallest-grid requests (see cpu_baseline.sample)"}
+    else:
+        cb = cpu_baseline(args, budget_s=args.ref_budget)
+        metric = METRIC_UNIFORM
+        cfg = workload_config(args, flush=False)
+        config = {k: cfg[k] for k in ("workload", "cells", "scheme", "init")}
+        config["dt"] = "host CFL reduction every step"
+    out = {"impl": "reference", "metric": metric, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": workload_config(args, flush=False), "cpu_baseline": cb,
+           "config": config, "cpu_baseline": cb,
            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -289,6 +321,18 @@ def cone_request(args):
 
 
 def run_b200(args, world, rank, local):
+    out = measure_uniform(args, world, rank, local)
+    if rank == 0:
+        if not args.no_cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_baseline(args)
+        print(json.dumps(out), flush=True)
+
+
+def measure_uniform(args, world, rank, local, e2e_min_steps: int = 4) -> dict:
+    """One solve of the uniform workload of `args` advanced args.steps RK4
+    steps (graph replay, device CFL every step): the result line of the
+    uniform workload, with the operator's rooflines and the end-to-end rate
+    through the public API with host buffers."""
     import torch
     from heliocubed_b200.level import InitSpec, Shell
     torch.cuda.set_device(local)
@@ -410,7 +454,7 @@ def run_b200(args, world, rank, local):
             lane["shell"].advance(lane["dev"], 1, lane["t"])
             lane["out"].copy_(lane["dev"], non_blocking=True)
 
-    e2e_steps = max(4, args.steps // 2)
+    e2e_steps = max(e2e_min_steps, args.steps // 2)
     for n in range(2 * nlanes):
         e2e_step(n)
     torch.cuda.synchronize()
@@ -429,10 +473,9 @@ def run_b200(args, world, rank, local):
     for lane in lanes[1:]:
         lane["shell"].close()
 
-    if rank == 0:
-        value = cells * world * args.steps / (ms * 1e-3)
-        out = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    value = cells * world * args.steps / (ms * 1e-3)
+    out = {
+            "metric": METRIC_UNIFORM, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(workload_config(args, flush), parallelism=f"replicas x{world}",
@@ -459,65 +502,218 @@ def run_b200(args, world, rank, local):
             "gpu_launches": launches_per_step(args) * args.steps,
             "clocks": clocks,
             "valid_state": ok,
-        }
-        if not args.no_cpu_baseline and world == 1:
-            out["cpu_baseline"] = cpu_baseline(args)
-        print(json.dumps(out), flush=True)
+    }
     shell.close()
+    del lanes, scratch
+    torch.cuda.empty_cache()
+    return out
+
+
+SERVE_GRIDS = {"radial": (32, 48, 64, 96), "angular": (32, 48, 64)}
+
+
+def serve_requests(args, rate_hz):
+    from heliocubed_b200 import serve
+    return serve.synthetic_requests(args.serve_requests, args.seed, rate_hz, args.steps,
+                                    radial=SERVE_GRIDS["radial"], angular=SERVE_GRIDS["angular"])
+
+
+def serve_launches(reqs) -> int:
+    """Kernels of this library launched for `reqs` (admission, steps,
+    schedule): per request the wind, the cone insertion and the schedule,
+    then each RK4 step's launches of its order."""
+    total = 0
+    for r in reqs:
+        a = argparse.Namespace(order=r.order, riemann=2 if r.order == 4 else 1, gravity=0)
+        total += 3 + launches_per_step(a) * r.steps
+    return total
 
 
 def run_serve(args, world, rank, local):
-    """Served ensemble (config-4 style, scaled: see --serve-* flags): the same
-    seeded requests through the continuous-batching server and through the
-    plain one-at-a-time path; aggregate cell-updates/s of each and p50/p99
-    time-to-solution (all requests arrive at t = 0)."""
+    """The served CME ensemble (module docstring): continuous batching vs
+    plain per-solve launches on the same seeded Poisson stream, then the
+    host-staged (e2e) served run, then the large single solve."""
     import torch
     from heliocubed_b200 import serve
     torch.cuda.set_device(local)
-    reqs = serve.synthetic_requests(args.serve_requests, args.seed, None, args.serve_steps,
-                                    radial=(32, 48, 64), angular=(32, 48))
-    shells = {}
-    for r in reqs:
-        shp = (r.nr, r.na, r.order)
-        if shp not in shells:
-            shells[shp] = serve.Shell(r.params(), device=local)
-    server = serve.EnsembleServer(hbm_budget=args.serve_budget_gb * 1e9, max_inflight=args.serve_inflight,
-                                  chunk=10, device=local)
-    counts = {}
-    for r in reqs:
-        counts[(r.nr, r.na, r.order)] = counts.get((r.nr, r.na, r.order), 0) + 1
-    for shp, n in counts.items():
-        server.warm([r for r in reqs if (r.nr, r.na, r.order) == shp], per_shape=min(n, args.serve_inflight))
-    # warm the plain path's contexts with one step each
+    dev = torch.device("cuda", local)
+    probe = serve_requests(args, None)
+    shapes = sorted({(r.nr, r.na, r.order) for r in probe})
+    counts = {shp: sum(1 for r in probe if (r.nr, r.na, r.order) == shp) for shp in shapes}
+
+    # contexts of the plain path, one per shape; W warm-up steps each, timed
+    # with CUDA events to set the arrival rate (Little's law: about
+    # `serve_inflight` solves in flight at the plain path's service time)
+    shells = {shp: serve.Shell(serve.Request(0, *shp, 0).params(), device=local) for shp in shapes}
+    step_ms = {}
     for shp, sh in shells.items():
-        req = next(r for r in reqs if (r.nr, r.na, r.order) == shp)
-        ju = torch.from_numpy(serve.initial_state(sh, req)).to(sh._dev)
-        sh.advance(ju, 1, torch.zeros(1, dtype=torch.float64, device=sh._dev))
+        req = next(r for r in probe if (r.nr, r.na, r.order) == shp)
+        ju = torch.from_numpy(serve.initial_state(sh, req)).to(dev)
+        t = torch.zeros(1, dtype=torch.float64, device=dev)
+        sh.advance(ju, 1, t)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sh.advance(ju, args.warmup, t)
+        e1.record()
+        torch.cuda.synchronize()
+        step_ms[shp] = e0.elapsed_time(e1) / args.warmup
+    service_s = statistics.mean(step_ms[(r.nr, r.na, r.order)] * 1e-3 * args.steps for r in probe)
+    rate = args.serve_inflight / service_s
+    reqs = serve_requests(args, rate)
+
+    # the server's slots, pooled by shape (contexts, buffers, graphs of
+    # `chunk` steps), built before the timed runs as a long-running server has them
+    chunk = max(1, min(10, args.steps))
+    server = serve.EnsembleServer(hbm_budget=args.serve_budget_gb * 1e9, max_inflight=args.serve_inflight,
+                                  chunk=chunk, device=local, keep_states=False)
+    for shp in shapes:
+        server.warm([r for r in reqs if (r.nr, r.na, r.order) == shp], per_shape=min(counts[shp], 2))
     torch.cuda.synchronize()
+
+    # host-staged copies of the requests (pinned initial states) for e2e
+    staged = []
+    for r in reqs:
+        sh = shells[(r.nr, r.na, r.order)]
+        host = torch.from_numpy(serve.initial_state(sh, r)).pin_memory()
+        staged.append(serve.Request(r.rid, r.nr, r.na, r.order, r.steps, r.arrival, r.cone, initial=host))
+
     sampler = ClockSampler(local)
     sampler.start()
-    plain = serve.run_plain(reqs, device=local, shells=shells)
+    plain = serve.run_plain(reqs, device=local, shells=shells, keep_states=False)
     batched = server.run(reqs)
+    hosted = server.run(staged)
     clocks = sampler.stop()
-    same = all(np.array_equal(a.state, b.state, equal_nan=True) for a, b in
-               zip(sorted(plain, key=lambda r: r.rid), sorted(batched, key=lambda r: r.rid)))
-    finite = sum(int(np.isfinite(r.state).all()) for r in batched)
-    sp, sb = serve.summarize(plain), serve.summarize(batched)
-    if rank == 0:
-        out = {"metric": "FP64 cell-updates/s on 1 B200, batched vs plain; ensemble p50/p99 latency",
-               "value": sb["cell_updates_per_s"] * world, "unit": UNIT, "n_gpus": world,
-               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-               "data": "synthetic",
-               "config": {"workload": "served ensemble of cone-cloud solves (scaled config 4)",
-                          "requests": len(reqs), "steps_per_request": args.serve_steps,
-                          "grids": "nr in {32,48,64} x na in {32,48}, 50/50 PLM-MC+Rusanov / WENOZ+Roe",
-                          "arrivals": "all at t=0 (closed loop)", "max_inflight": args.serve_inflight,
-                          "hbm_budget_gb": args.serve_budget_gb, "chunk_steps": 10},
-               "batched": sb, "plain": sp, "batched_over_plain": sb["cell_updates_per_s"] / sp["cell_updates_per_s"],
-               "identical_results": same, "finite_results": finite, "clocks": clocks}
-        print(json.dumps(out), flush=True)
+
+    same = serve.same_results(plain, batched)
+    same_e2e = serve.same_results(batched, hosted)
+    finite = sum(int(bool(r.finite)) for r in batched)
+    sp, sb, se = serve.summarize(plain), serve.summarize(batched), serve.summarize(hosted)
+    state_bytes = sum(8 * 8 * r.cells for r in reqs)
+    request_steps = sum(r.steps for r in reqs)
     for sh in shells.values():
         sh.close()
+    server.close()
+    del staged, plain, batched, hosted
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+    large = None
+    if not args.no_large:
+        la = argparse.Namespace(**vars(args))
+        la.order, la.nr, la.na, la.riemann, la.gravity, la.init = 4, 256, 192, 2, 1, "cone"
+        la.steps, la.warmup = args.large_steps, 3
+        la.graph, la.o4_variants = True, None
+        large = measure_uniform(la, world, rank, local, e2e_min_steps=2)
+
+    if rank != 0:
+        return
+    out = {"metric": METRIC, "value": sb["cell_updates_per_s"] * world, "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": sb["makespan_s"] * 1e3 / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "served CME ensemble (config 4): %d requests, %d RK4 steps each"
+                                  % (len(reqs), args.steps),
+                      "requests": len(reqs), "steps_per_request": args.steps,
+                      "steps_note": "the configured 500 steps per request shrunk to --steps (a step of this line "
+                                    "is one RK4 step of every request)",
+                      "grids": "nr in {32,48,64,96} x na in {32,48,64}, scheme 50/50 PLM-MC+Rusanov / "
+                               "Berta WENOZ+Roe, cone speed U[500,2000] km/s, half-width U[20,60] deg, "
+                               "lat/lon U[-30,30] deg, density ratio U[2,6]",
+                      "arrivals": "seeded Poisson, rate %.3f /s (%d in flight at the plain path's mean service "
+                                  "time %.3f s)" % (rate, args.serve_inflight, service_s),
+                      "max_inflight": args.serve_inflight, "hbm_budget_gb": args.serve_budget_gb,
+                      "chunk_steps": chunk, "slots_per_shape": "min(requests of the shape, 2), built before timing",
+                      "l2": "working set of the in-flight solves larger than L2",
+                      "parallelism": f"replicas x{world}"},
+           "batched": sb, "plain": sp,
+           "batched_over_plain": sb["cell_updates_per_s"] / sp["cell_updates_per_s"],
+           "p50_s": sb["p50_s"], "p99_s": sb["p99_s"],
+           "identical_results": same, "finite_results": finite,
+           "e2e": {"value": se["cell_updates_per_s"] * world, "unit": UNIT,
+                   "h2d_bytes_per_step": state_bytes / request_steps,
+                   "d2h_bytes_per_step": state_bytes / request_steps,
+                   "p50_s": se["p50_s"], "p99_s": se["p99_s"], "identical_to_device_built": same_e2e,
+                   "pipeline": "served run with every request's initial state copied from pinned host memory at "
+                               "admission and its result copied back (bytes per request-step)"},
+           "gpu_launches": serve_launches(reqs),
+           "clocks": clocks}
+    if large is not None:
+        out["roofline"] = dict(large["roofline"], workload="large solve 256x192^2x6 (operator launch group)")
+        out["fp64_roofline"] = large["fp64_roofline"]
+        out["large_solve"] = {k: large[k] for k in ("value", "unit", "ms_per_step", "steps", "config", "e2e",
+                                                     "valid_state", "clocks", "gpu_launches")}
+    if not args.no_cpu_baseline and world == 1:
+        out["cpu_baseline"] = cpu_baseline_serve(args, reqs)
+    print(json.dumps(out), flush=True)
+
+
+def oracle_request(po, req):
+    """(oracle level, its state) of a served request, built by the oracle:
+    the wind and the request's cone cloud inserted at its insertion time."""
+    from heliocubed_b200 import serve
+    from heliocubed_b200.level import ConeSpec
+    prm = req.params()
+    kw = dict(nr=req.nr, na=req.na, spatial_order=req.order, limiter=prm.limiter, riemann_solver=prm.riemann_solver,
+              berta_fallback_type=prm.berta_fallback_type, sun_gravity=0)
+    p = po.make_params(**kw)
+    L = po.OracleLevelO4(p) if req.order == 4 else po.OracleLevel(p)
+    base = L.base if req.order == 4 else L
+    wind = serve.wind_spec()
+    s = po.HcInit()
+    s.kind = 1
+    for k in ("pulse_block", "pulse_i", "pulse_j", "pulse_k", "rho0", "p0", "vr", "b0", "r_ref", "pulse_amp",
+              "pulse_width"):
+        setattr(s, k, getattr(wind, k))
+    ju = base.init(s)
+    c = req.cone
+    rho_inner = wind.rho0 * (wind.r_ref / p.inner_radius) ** 2
+    spec = ConeSpec.on_inner_boundary(p.inner_radius, lat_deg=c.lat_deg, lon_deg=c.lon_deg,
+                                      half_angle_deg=c.half_width_deg, apex_speed=c.speed_kms,
+                                      density=c.density_ratio * rho_inner, temperature=c.temperature)
+    cs = po.HcConeSpec()
+    for k in po.CONE_SPEC_FIELDS:
+        setattr(cs, k, getattr(spec, k))
+    cone = po.cone_prepare(cs, p.inner_radius)
+    base.insert_cone(cone, cone.insertion_time, ju)
+    return L, ju, cone.insertion_time
+
+
+def cpu_baseline_serve(args, reqs, budget_s: float = 20.0) -> dict:
+    """The oracle on the host cores on a bounded sample of the ensemble: one
+    request of each scheme on the ensemble's smallest grid, each advanced
+    with CFL dt until its half of the time budget is spent.  The ensemble
+    rate combines the two schemes' rates by their shares of the ensemble's
+    cell-updates: total work / sum over schemes of (work / rate)."""
+    from oracle import pyoracle as po
+    cores = os.cpu_count() or 1
+    small = min((r.nr * r.na * r.na, r.nr, r.na) for r in reqs)
+    sample = [r for r in reqs if (r.nr, r.na) == small[1:]]
+    picks = [next((r for r in sample if r.order == o), None) for o in (2, 4)]
+    picks = [r for r in picks if r is not None]
+    rates, notes, el = {}, [], 0.0
+    for r in picks:
+        L, ju, t = oracle_request(po, r)
+        n = 0
+        t0 = time.perf_counter()
+        while n < args.steps:
+            dt = 0.4 / L.inv_dt(ju)
+            L.rk4_step(ju, dt, t)
+            t += dt
+            n += 1
+            if time.perf_counter() - t0 > budget_s / len(picks):
+                break
+        dt_s = time.perf_counter() - t0
+        el += dt_s
+        rates[r.order] = r.cells * n / dt_s
+        notes.append(f"{n} {'WENOZ+Roe' if r.order == 4 else 'PLM-MC+Rusanov'} steps "
+                     f"({rates[r.order]:.4g} cell-updates/s)")
+    work = {o: sum(r.cells * r.steps for r in reqs if r.order == o) for o in rates}
+    value = sum(work.values()) / sum(work[o] / rates[o] for o in rates)
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"one request of each scheme on the ensemble's smallest grid {small[1]}x{small[2]}^2x6 with "
+                      f"its cone: {', '.join(notes)}, CFL dt each step, OpenMP over {cores} host threads, "
+                      f"{el:.1f} s; combined by the schemes' shares of the ensemble's cell-updates"}
 
 
 def run_amr(args, world, rank, local):
@@ -690,7 +886,8 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--order", type=int, choices=[2, 4], default=4)
+    ap.add_argument("--order", type=int, choices=[2, 4], default=None,
+                    help="uniform workload: spatial order (default 4); implies --workload uniform")
     ap.add_argument("--nr", type=int, default=None)
     ap.add_argument("--na", type=int, default=None)
     ap.add_argument("--limiter", type=int, default=3)
@@ -707,21 +904,30 @@ def main() -> int:
                          "kernels instead of timing them (for profiler runs)")
     ap.add_argument("--cpu-max-steps", type=int, default=60)
     ap.add_argument("--ref-budget", type=float, default=20.0)
-    ap.add_argument("--serve", action="store_true", help="run the served-ensemble benchmark instead")
-    ap.add_argument("--amr", action="store_true", help="run the batched AMR-box operator benchmark instead")
+    ap.add_argument("--workload", choices=["serve", "uniform", "amr"], default=None,
+                    help="serve (default): the served CME ensemble with the large solve; uniform: one solve; "
+                         "amr: the AMR-style box batch")
+    ap.add_argument("--serve", action="store_true", help="same as --workload serve")
+    ap.add_argument("--amr", action="store_true", help="same as --workload amr")
+    ap.add_argument("--no-large", action="store_true", help="serve: leave out the large single solve")
+    ap.add_argument("--large-steps", type=int, default=5, help="serve: RK4 steps of the large single solve")
     ap.add_argument("--amr-l1", type=int, default=600)
     ap.add_argument("--amr-l2", type=int, default=1200)
     ap.add_argument("--amr-reps", type=int, default=8)
-    ap.add_argument("--serve-requests", type=int, default=24)
-    ap.add_argument("--serve-steps", type=int, default=40)
+    ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-inflight", type=int, default=8)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     args = ap.parse_args()
+    # --order, --nr, --na or --init cone without --workload select the uniform workload
+    uniform_opts = args.order is not None or args.nr is not None or args.na is not None or args.init != "default"
+    args.workload = args.workload or ("amr" if args.amr else "serve" if args.serve or not uniform_opts
+                                      else "uniform")
+    args.order = args.order or 4
     o4 = args.order == 4
     args.nr = args.nr or (64 if o4 else 32)
     args.na = args.na or (64 if o4 else 32)
     args.riemann = args.riemann or (2 if o4 else 1)
-    args.steps = args.steps or (100 if o4 else 2000)
+    args.steps = args.steps or (20 if args.workload == "serve" else 100 if o4 else 2000)
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
@@ -733,9 +939,9 @@ def main() -> int:
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
-        elif args.serve:
+        elif args.workload == "serve":
             run_serve(args, world, rank, local)
-        elif args.amr:
+        elif args.workload == "amr":
             run_amr(args, world, rank, local)
         else:
             run_b200(args, world, rank, local)

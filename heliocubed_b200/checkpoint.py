@@ -70,6 +70,17 @@ def save(path: str, params, state, time: float, step: int = 0, attributes: dict 
         f.flush()
         os.fsync(f.fileno())
     os.replace(tmp, path)
+    # make the rename itself durable: sync the directory entry
+    try:
+        fd = os.open(os.path.dirname(os.path.abspath(path)), os.O_RDONLY)
+    except OSError:
+        return  # platforms where a directory cannot be opened
+    try:
+        os.fsync(fd)
+    except OSError:
+        pass
+    finally:
+        os.close(fd)
 
 
 def load(path: str):

@@ -13,6 +13,7 @@
 #include <math_constants.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <functional>
@@ -978,6 +979,36 @@ extern "C" int hc_amr_copy(hc_ctx* ctx, const hc_amr_plan* P, int first, int cou
       if (overlaps(acc[a].second.first, acc[b].second.first))
         return argFail("hc_amr_copy: a copy of the launch writes a region another access of the launch uses");
     }
+  // distinct base pointers must not share memory where one of them is
+  // written (sub-views of one allocation would escape the check above)
+  if (!known) {
+    struct Span { uintptr_t lo, hi; const void* base; bool write; };
+    std::vector<Span> spans;
+    for (int q = first; q < first + count; ++q) {
+      const hc_copy_box& C = P->copyHost[q];
+      const uintptr_t ns = (uintptr_t)C.ncomp * C.src_n[0] * C.src_n[1] * C.src_n[2] * sizeof(double);
+      const uintptr_t nd = (uintptr_t)C.ncomp * C.dst_n[0] * C.dst_n[1] * C.dst_n[2] * sizeof(double);
+      spans.push_back({(uintptr_t)C.src, (uintptr_t)C.src + ns, C.src, false});
+      spans.push_back({(uintptr_t)C.dst, (uintptr_t)C.dst + nd, C.dst, true});
+    }
+    // one span per base pointer: its largest extent, written if any access writes
+    std::sort(spans.begin(), spans.end(), [](const Span& a, const Span& b) {
+      return a.lo != b.lo ? a.lo < b.lo : a.hi > b.hi;
+    });
+    std::vector<Span> merged;
+    for (const Span& x : spans) {
+      if (!merged.empty() && merged.back().base == x.base) {
+        merged.back().hi = std::max(merged.back().hi, x.hi);
+        merged.back().write = merged.back().write || x.write;
+      } else {
+        merged.push_back(x);
+      }
+    }
+    for (size_t a = 0; a < merged.size(); ++a)
+      for (size_t b = a + 1; b < merged.size() && merged[b].lo < merged[a].hi; ++b)
+        if (merged[a].write || merged[b].write)
+          return argFail("hc_amr_copy: two arrays of the launch share memory through different base pointers");
+  }
   if (!known) P->copyRangesChecked.push_back(range);
   const int c0 = count ? P->copyStart[first] : 0, c1 = count ? P->copyStart[first + count] : 0;
   if (c1 == c0) return HC_OK;

@@ -26,6 +26,7 @@ order independent) and every slot owns its buffers.
 """
 from __future__ import annotations
 
+import hashlib
 import time
 from dataclasses import dataclass, field
 
@@ -75,6 +76,11 @@ class Request:
     steps: int
     arrival: float = 0.0      # seconds after the start of the run
     cone: Cone = field(default_factory=Cone)
+    # Optional initial state from the host (pinned float64, the level's JU
+    # layout), e.g. a restart: copied to the device at admission in place of
+    # the on-device wind and cone insertion; the cone still sets the
+    # insertion schedule and the model time.
+    initial: "torch.Tensor | None" = None
 
     @property
     def cells(self) -> int:
@@ -93,20 +99,25 @@ def admit(shell: Shell, req: Request, ju: torch.Tensor, time_dev: torch.Tensor, 
     to that time, and the insertion schedule (CFL ramp, and the Rusanov
     window of fourth-order Roe solves) that the reference's driver applies
     after an insertion (schedule=False: the state only)."""
-    shell.init(wind_spec(), ju)
     cone = req.cone.prepared(shell.params)
-    shell.insert_cone(cone, cone.insertion_time, ju)
+    if req.initial is not None:
+        ju.copy_(req.initial, non_blocking=True)
+    else:
+        shell.init(wind_spec(), ju)
+        shell.insert_cone(cone, cone.insertion_time, ju)
     if schedule:
         shell.set_cme_schedule([cone])
     time_dev.fill_(cone.insertion_time)
 
 
 def initial_state(shell: Shell, req: Request) -> np.ndarray:
-    """Host copy of the state `admit` builds (for checks and reports); the
-    shell's insertion schedule is left as it was."""
+    """Host copy of the state `admit` builds from the request's parameters
+    (for checks, reports and host-staged requests); the shell's insertion
+    schedule is left as it was."""
     ju = shell.new_state()
     t = torch.zeros(1, dtype=torch.float64, device=ju.device)
-    admit(shell, req, ju, t, schedule=False)
+    params_only = Request(req.rid, req.nr, req.na, req.order, req.steps, req.arrival, req.cone)
+    admit(shell, params_only, ju, t, schedule=False)
     return ju.cpu().numpy()
 
 
@@ -174,6 +185,11 @@ class Result:
     t_done: float
     state: np.ndarray
     model_time: float
+    error: str | None = None   # set (and state empty) when the request was refused
+    # with keep_states=False: the state's SHA-256 and finiteness instead of
+    # the state itself (state empty)
+    digest: bytes | None = None
+    finite: bool | None = None
 
     @property
     def time_to_solution(self) -> float:
@@ -183,7 +199,9 @@ class Result:
 class EnsembleServer:
     """Continuous-batching server over pooled slots (see module docstring)."""
 
-    def __init__(self, hbm_budget: float, max_inflight: int = 8, chunk: int = 10, device: int | None = None):
+    def __init__(self, hbm_budget: float, max_inflight: int = 8, chunk: int = 10, device: int | None = None,
+                 keep_states: bool = True):
+        self.keep_states = keep_states
         self.budget = hbm_budget
         self.max_inflight = max_inflight
         self.chunk = chunk
@@ -204,9 +222,26 @@ class EnsembleServer:
                 self.pool.setdefault(shp, []).append(s)
                 self.slot_bytes[shp] = s.bytes
 
+    # Device bytes per cell of a slot of each order before any slot of that
+    # order was built (state, stage workspace, operator scratch and the
+    # graph's pool; generous, so an unseen shape is not admitted past the
+    # budget).  Measured slots replace it.
+    BYTES_PER_CELL_GUESS = {2: 64 * 8, 4: 64 * 40}
+
+    def estimate_bytes(self, shp: tuple[int, int, int]) -> int:
+        """HBM a slot of shape `shp` takes: its measured size, else the
+        largest measured bytes per cell of a slot of the same order times its
+        cells, else a fixed guess per cell."""
+        if shp in self.slot_bytes:
+            return self.slot_bytes[shp]
+        nr, na, order = shp
+        cells = 6 * nr * na * na
+        per_cell = [b / (6 * s[0] * s[1] * s[1]) for s, b in self.slot_bytes.items() if s[2] == order]
+        return int(cells * (max(per_cell) if per_cell else self.BYTES_PER_CELL_GUESS.get(order, 64 * 40)))
+
     def _acquire(self, req: Request) -> Slot | None:
         shp = self.shape(req)
-        need = self.slot_bytes.get(shp, 0)
+        need = self.estimate_bytes(shp)
         if self.in_use + need > self.budget:
             return None
         idle = self.pool.setdefault(shp, [])
@@ -231,6 +266,16 @@ class EnsembleServer:
             while pending and pending[0].arrival <= now and len(active) < self.max_inflight:
                 slot = self._acquire(pending[0])
                 if slot is None:
+                    if not active:
+                        # nothing runs, so nothing will free memory: the
+                        # request alone needs more than the whole budget
+                        req = pending.pop(0)
+                        need = self.estimate_bytes(self.shape(req))
+                        results.append(Result(req.rid, req.cells, req.steps, req.arrival, now, now,
+                                              np.empty(0), float("nan"),
+                                              error=f"request needs {need} B of HBM, over the budget of "
+                                                    f"{self.budget:.0f} B"))
+                        continue
                     break
                 req = pending.pop(0)
                 slot.start(req, now)
@@ -243,9 +288,8 @@ class EnsembleServer:
                 progressed = True
                 if slot.left == -1:
                     req = slot.req
-                    results.append(Result(req.rid, req.cells, req.steps, req.arrival, slot.t_start,
-                                          time.perf_counter() - t0, slot.host_out.numpy().copy(),
-                                          float(slot.host_time.item())))
+                    results.append(_result(req, slot.t_start, time.perf_counter() - t0, slot.host_out.numpy(),
+                                           float(slot.host_time.item()), self.keep_states))
                     active.remove(slot)
                     self._release(slot)
                 else:
@@ -258,8 +302,41 @@ class EnsembleServer:
         return results
 
 
+    def close(self) -> None:
+        """Release every pooled slot (contexts, buffers, graphs)."""
+        for slots in self.pool.values():
+            for slot in slots:
+                slot.graph = None
+                slot.shell.close()
+        self.pool.clear()
+
+
+def _result(req: Request, t_start: float, t_done: float, host_state: np.ndarray, model_time: float,
+            keep: bool) -> Result:
+    if keep:
+        return Result(req.rid, req.cells, req.steps, req.arrival, t_start, t_done, host_state.copy(), model_time)
+    return Result(req.rid, req.cells, req.steps, req.arrival, t_start, t_done, np.empty(0), model_time,
+                  digest=hashlib.sha256(host_state.tobytes()).digest(), finite=bool(np.isfinite(host_state).all()))
+
+
+def same_results(a: list[Result], b: list[Result]) -> bool:
+    """Bit-identical final states of the same requests in two runs (states or
+    digests, NaN patterns included)."""
+    if len(a) != len(b):
+        return False
+    for x, y in zip(sorted(a, key=lambda r: r.rid), sorted(b, key=lambda r: r.rid)):
+        if x.rid != y.rid:
+            return False
+        if x.digest is not None or y.digest is not None:
+            if x.digest != y.digest:
+                return False
+        elif not np.array_equal(x.state, y.state, equal_nan=True):
+            return False
+    return True
+
+
 def run_plain(requests: list[Request], device: int | None = None,
-              shells: dict[tuple, Shell] | None = None) -> list[Result]:
+              shells: dict[tuple, Shell] | None = None, keep_states: bool = True) -> list[Result]:
     """The same requests one after another through eager per-solve launches
     (`admit`, `Shell.advance`, the result copied to the host); contexts are
     cached by shape so neither path pays for context builds."""
@@ -281,8 +358,7 @@ def run_plain(requests: list[Request], device: int | None = None,
         admit(sh, req, ju, t)
         sh.advance(ju, req.steps, t)
         out = ju.cpu().numpy()
-        results.append(Result(req.rid, req.cells, req.steps, req.arrival, t_start, time.perf_counter() - t0, out,
-                              float(t.item())))
+        results.append(_result(req, t_start, time.perf_counter() - t0, out, float(t.item()), keep_states))
     return results
 
 
@@ -306,6 +382,7 @@ def synthetic_requests(n: int, seed: int, rate_hz: float | None, steps: int,
 
 
 def summarize(results: list[Result]) -> dict:
+    results = [r for r in results if r.error is None]
     tts = np.array([r.time_to_solution for r in results])
     span = max(r.t_done for r in results) - min(r.t_arrival for r in results)
     work = sum(r.cells * r.steps for r in results)

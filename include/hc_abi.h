@@ -427,7 +427,9 @@ int hc_amr_plan_set_copies(hc_amr_plan* plan, const hc_copy_box* copies, int nco
 /* Copies first .. first+count-1 of the plan in one launch.  Within one
  * launch no written region may overlap another copy's written or read
  * region of the same array (an exchange writes ghosts and reads valid
- * cells, so a level's exchange is one launch). */
+ * cells, so a level's exchange is one launch), and arrays given by
+ * different base pointers must not share memory where one is written
+ * (HC_ERR_ARG otherwise). */
 int hc_amr_copy(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
 
 int hc_amr_plan_set_cf_fine(hc_amr_plan* plan, const hc_cf_fine_box* boxes, int nbox);

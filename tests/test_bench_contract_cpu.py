@@ -12,8 +12,8 @@ REQUIRED = {"metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_b
 
 
 def test_reference_arm_prints_the_contract_line():
-    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--order", "2",
-                          "--steps", "1", "--warmup", "3", "--ref-budget", "2"],
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                          "uniform", "--order", "2", "--steps", "1", "--warmup", "3", "--ref-budget", "2"],
                          cwd=ROOT, capture_output=True, text=True, timeout=600, check=True).stdout
     lines = [ln for ln in out.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
@@ -30,3 +30,19 @@ def test_warmup_below_three_is_refused():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--warmup", "2"],
                        cwd=ROOT, capture_output=True, text=True, timeout=120)
     assert r.returncode != 0 and "warmup" in r.stderr
+
+
+def test_reference_arm_serving_workload_line():
+    """The default workload's CPU arm: the served-ensemble metric, sampled
+    on the ensemble's smallest-grid requests of both schemes."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "3", "--ref-budget", "1"],
+                         cwd=ROOT, capture_output=True, text=True, timeout=600, check=True).stdout
+    lines = [ln for ln in out.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert REQUIRED <= set(d), REQUIRED - set(d)
+    assert d["metric"] == "FP64 cell-updates/s on 1 B200, batched vs plain; ensemble p50/p99 latency"
+    assert d["config"]["requests"] == 256 and d["config"]["steps_per_request"] == 1
+    assert "PLM-MC+Rusanov" in d["cpu_baseline"]["sample"] and "WENOZ+Roe" in d["cpu_baseline"]["sample"]
+    assert d["value"] > 0

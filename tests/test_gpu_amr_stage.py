@@ -246,7 +246,8 @@ def test_cf_fine_recovery_matches_oracle(oracle_lib):
 def test_region_copies_match_oracle(oracle_lib):
     """hc_amr_copy: an in-panel ghost exchange between two boxes and a
     cross-panel copy with a signed axis permutation, one launch; a launch
-    whose write overlaps another copy's read is refused."""
+    whose write overlaps another copy's read, or that writes memory another
+    base pointer of the launch reaches, is refused."""
     _need_gpu()
     po = oracle_lib
     rng = np.random.default_rng(5)
@@ -281,6 +282,12 @@ def test_region_copies_match_oracle(oracle_lib):
     racy = dict(copies[0], src=tb, dst=ta, src_lo=(7, -1, -1), dst_lo=(-1, -1, -1), lo=(8, 0, 0), hi=(8, 7, 7),
                 shift=(-1, 0, 0))
     plan.set_copies([copies[0], racy])
+    with pytest.raises(hc.HcError):
+        plan.copy(0, 2)
+    # a destination that is a sub-view of A (another base pointer into the
+    # same memory) written in the same launch as A: refused
+    alias = dict(copies[2], dst=ta.view(-1)[4000:], ncomp=4)
+    plan.set_copies([copies[1], alias])
     with pytest.raises(hc.HcError):
         plan.copy(0, 2)
     plan.close()

@@ -151,3 +151,32 @@ def test_summary_of_results(fake_slots):
     s = serve.summarize(srv.run(reqs))
     assert s["requests"] == 5 and s["cell_updates"] == 5 * 20 * 6 * 8 * 8 * 8
     assert 0 < s["p50_s"] <= s["p99_s"] <= s["makespan_s"] + 1e-9
+
+
+def test_request_over_the_budget_is_refused(fake_slots):
+    """A request whose slot alone needs more than the budget is refused with
+    an error naming the sizes; the others are served and the loop ends."""
+    small = [_req(i) for i in range(3)]
+    big = _req(9, nr=32, na=32)
+    srv = serve.EnsembleServer(hbm_budget=2.5 * _slot_bytes(), max_inflight=8, chunk=10, device=0)
+    srv.warm(small + [big])
+    res = {r.rid: r for r in srv.run(small + [big])}
+    assert sorted(res) == [0, 1, 2, 9]
+    assert res[9].error is not None and "budget" in res[9].error and res[9].state.size == 0
+    assert all(res[i].error is None and res[i].state[0] == i for i in range(3))
+    assert serve.summarize(list(res.values()))["requests"] == 3
+    assert srv.in_use == 0
+
+
+def test_unseen_shape_admitted_by_estimate(fake_slots):
+    """A shape with no built slot is admitted by an estimate scaled from the
+    measured slots of its order, not with a size of zero."""
+    srv = serve.EnsembleServer(hbm_budget=3.5 * _slot_bytes(), max_inflight=8, chunk=10, device=0)
+    srv.warm([_req(0)])
+    assert srv.estimate_bytes((16, 8, 2)) == 2 * _slot_bytes()
+    reqs = [_req(0, steps=200), _req(1, steps=200), _req(2, nr=16, steps=20)]
+    res = {r.rid: r for r in srv.run(reqs)}
+    # the two small solves hold 2 of 3.5 budget units; the unseen 2-unit shape
+    # waits for one of them instead of being built past the budget
+    assert res[2].t_start >= min(res[0].t_done, res[1].t_done) - 1e-3
+    assert all(r.error is None for r in res.values())

@@ -5,7 +5,8 @@ allocator).  Its stage workspace is a fixed array inside the library.
 
 Called through the C ABI and checked against hc_level_rk4_step, the
 allocating entry point, on two calls in a row, with the tolerance of the
-other operator tests (1e-12 normwise per component).  The file sorts last so
+other operator tests (1e-12 normwise per component), after a call on a level
+of another shape has left its data in the shared array.  The file sorts last so
 a run that stops at the first failure has run every other test before it.
 """
 from __future__ import annotations
@@ -30,14 +31,26 @@ def test_noalloc_step_matches_allocating_step():
     import torch
 
     import heliocubed_b200 as hc
+    lib = hc.lib()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    # A first call on a level of another shape leaves its (non-zero) stage
+    # data in the shared array at offsets the 12 x 10 level uses
+    # differently: the steps below must not read any of it.
+    other = hc.Shell(hc.Params(nr=20, na=18, limiter=3, riemann_solver=1))
+    ju_other = other.init(hc.InitSpec.seeded(3, 20, 18, margin=2))
+    dt_other = 0.4 / other.inv_dt_max(ju_other).item()
+    rc = lib.hc_level_rk4_step_noalloc(other._ctx, C.c_void_p(ju_other.data_ptr()), dt_other, 0.0, stream)
+    assert rc == 0, lib.hc_last_error()
+    torch.cuda.synchronize()
+    assert other.valid(ju_other)
+    other.close()
+
     nr, na = 12, 10
     shell = hc.Shell(hc.Params(nr=nr, na=na, limiter=3, riemann_solver=2, sun_gravity=1))
     ju = shell.init(hc.InitSpec.seeded(7, nr, na, margin=2))
     a = ju.clone()
     b = ju.clone()
     dt = 0.4 / shell.inv_dt_max(ju).item()
-    lib = hc.lib()
-    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     for call in range(2):
         t = call * dt
         shell.rk4_step(a, dt, t)

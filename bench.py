@@ -67,7 +67,10 @@ def launches_per_step(args) -> int:
     if args.order == 2:
         return 11  # prim + cfl + 4 x (ghosts, stage) + time (prologue in every 1-step call)
     roe, powell = int(args.riemann == 2), 1
-    operator = 3 + 3 * (6 + roe + 3 * powell) + 3 * powell
+    # detector + point values (3); per direction reconstruction, Roe point
+    # dissipation, fused face chain and the Powell face chain (3); Powell
+    # coefficients, averages and application (3)
+    operator = 3 + 3 * (2 + roe + 3 * powell) + 3 * powell
     per_stage = 4 + int(args.gravity) + operator + 1               # prepare, gravity, operator, update
     return 1 + 4 * per_stage + 2 + 1                               # cfl, stages, reflux, time
 
@@ -238,11 +241,24 @@ def barrier(world: int):
         dist.barrier()
 
 
+def native_oracle() -> str:
+    """Build the oracle for this machine's CPU (-march=native) and load it;
+    returns how the timed library was built."""
+    from oracle import build as ob
+    from oracle import pyoracle as po
+    path = ob.build_oracle_native(os.path.join(ROOT, "oracle", "_native"))
+    if path is None:
+        return "g++ -O3 -march=x86-64-v3 (shipped; the native build failed)"
+    po.use_library(path)
+    return "g++ -O3 -march=native -ffp-contract=off -fopenmp, built on this machine"
+
+
 def cpu_baseline(args, budget_s: float = 12.0) -> dict:
     """The oracle (CPU restatement of the reference) on the host cores, on a
     bounded number of RK4 steps of the same scheme: the full grid at order 2,
     a 32 x 32^2 x 6 grid at order 4 (one step of the 64^3 grid takes minutes
     on the host)."""
+    build = native_oracle()
     from oracle import pyoracle as po
     cores = os.cpu_count() or 1
     nr, na = (args.nr, args.na) if args.order == 2 else (min(args.nr, 32), min(args.na, 32))
@@ -276,7 +292,7 @@ def cpu_baseline(args, budget_s: float = 12.0) -> dict:
     el = time.perf_counter() - t0
     value = 6 * nr * na * na * steps / el
     same = "the same" if (nr, na) == (args.nr, args.na) else f"the same scheme on a"
-    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "build": build,
             "sample": f"{steps} RK4 steps (CFL dt each step) of {same} {nr}x{na}^2x6 grid, "
                       f"OpenMP over {cores} host threads, {el:.1f} s"}
 
@@ -360,7 +376,7 @@ def measure_uniform(args, world, rank, local, e2e_min_steps: int = 4) -> dict:
     else:
         from heliocubed_b200.level import o4_variants
         mb = o4_variants()
-        names = ("reconstruction", "roe_point", "final_flux")
+        names = ("reconstruction", "roe_point", "face_chain")
         if args.o4_variants:
             # fixed variants (profiling: timings taken under a profiler would
             # steer the tuner to a different choice than the plain run's)
@@ -484,7 +500,7 @@ def measure_uniform(args, world, rank, local, e2e_min_steps: int = 4) -> dict:
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "kernel": ("o2StageKernel (operator: read primitives, write rhs)" if args.order == 2 else
                                     "Berta operator launch group (hc_level_rhs, %d kernels): read USph, write rhs"
-                                    % (3 + 3 * (6 + int(args.riemann == 2) + 3) + 3)),
+                                    % (3 + 3 * (2 + int(args.riemann == 2) + 3) + 3)),
                          "algorithmic_bytes": f"{OPERATOR_BYTES_PER_CELL_STAGE} B/cell-stage x {cells} cells",
                          "kernel_ms": kms,
                          "traffic": None if tr is None else tr * cells},
@@ -685,6 +701,7 @@ def cpu_baseline_serve(args, reqs, budget_s: float = 20.0) -> dict:
     with CFL dt until its half of the time budget is spent.  The ensemble
     rate combines the two schemes' rates by their shares of the ensemble's
     cell-updates: total work / sum over schemes of (work / rate)."""
+    build = native_oracle()
     from oracle import pyoracle as po
     cores = os.cpu_count() or 1
     small = min((r.nr * r.na * r.na, r.nr, r.na) for r in reqs)
@@ -710,7 +727,7 @@ def cpu_baseline_serve(args, reqs, budget_s: float = 20.0) -> dict:
                      f"({rates[r.order]:.4g} cell-updates/s)")
     work = {o: sum(r.cells * r.steps for r in reqs if r.order == o) for o in rates}
     value = sum(work.values()) / sum(work[o] / rates[o] for o in rates)
-    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "build": build,
             "sample": f"one request of each scheme on the ensemble's smallest grid {small[1]}x{small[2]}^2x6 with "
                       f"its cone: {', '.join(notes)}, CFL dt each step, OpenMP over {cores} host threads, "
                       f"{el:.1f} s; combined by the schemes' shares of the ensemble's cell-updates"}
@@ -856,9 +873,9 @@ def run_amr(args, world, rank, local):
                "config": {"workload": "AMR-style box batch (scaled config 3), Berta WENOZ + Roe + Powell",
                           "levels": [{"n": n, "boxes": len(w)} for n, _, w, _, _ in levels], "boxes": nboxes,
                           "cells": cells, "ghost": 5},
-               "batched": {"ms_per_evaluation": ms_b, "launches": 3 * 36},
+               "batched": {"ms_per_evaluation": ms_b, "launches": 3 * 24},
                "plain": {"ms_per_evaluation": ms_p, "cell_stage_per_s": cells / (ms_p * 1e-3),
-                         "launches": 36 * nboxes},
+                         "launches": 24 * nboxes},
                "batched_over_plain": ms_p / ms_b, "identical_results": same,
                "rk4_stage_logic": {"ms_per_step": ms_rk, "launches": 5,
                                    "what": "tableau combine of every box of every level, 4 stages + final"},

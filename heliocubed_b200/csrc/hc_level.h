@@ -226,7 +226,7 @@ struct O4Args {
   double* mj;   // [nbox][V+1]
   double* kp;   // [nbox][8][V+2]
 };
-constexpr int kO4FaceArrays = 8 * 9 + 8;  // WL, WR, FS, QD/DP, FA, FM, FR, Fx (8 each) + thF, PS, BP, PA, T3, Bflux, Bprod, pad
+constexpr int kO4FaceArrays = 8 * 4 + 5;  // WL, WR, FS, QD/DP (8 each) + thF, PS, BP, Bflux, Bprod
 
 size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost);
 

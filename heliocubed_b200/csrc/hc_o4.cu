@@ -3,11 +3,14 @@
 // src/BoxOp_RoeCubedSphere.H:29-145 and the Powell terms of
 // src/BoxOp_DivBcleaning.H:35-172.  FP64.
 //
-// One kernel per stage of the operator; every intermediate lives on the box
-// the reference computes it on (cell arrays on the ghosted box G, face arrays
-// on the reconstruction face box F = G.extrude(d).grow(-3) of direction d).
-// Each kernel covers the region where its result is defined; a thread
-// handles one cell or face of one box.
+// Kernels per evaluation: the detector and point values on the ghosted box
+// G (cell arrays); per direction d the reconstruction on the face box
+// F = G.extrude(d).grow(-3) and the Roe point dissipation (face arrays in
+// the face scratch), then one fused face-chain kernel that takes tiles of
+// the final faces through the flux average, mapped flux, radial products,
+// final flux and divergence with its intermediates in shared memory; the
+// Powell terms on a side stream.  Every intermediate covers the box the
+// reference computes it on.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,8 +51,8 @@ __device__ __forceinline__ long roff(const Reg& r, int i, int j, int k) {
 }
 
 // Offsets of the face arrays inside a box's face scratch (units of F.N).
-enum FaceArr { F_WL = 0, F_WR = 8, F_FS = 16, F_QD = 24, F_FA = 32, F_FM = 40, F_FR = 48, F_FX = 56,
-               F_THF = 64, F_PS = 65, F_BP = 66, F_PA = 67, F_T3 = 68, F_BFLUX = 69, F_BPROD = 70 };
+enum FaceArr { F_WL = 0, F_WR = 8, F_FS = 16, F_QD = 24, F_THF = 32, F_PS = 33, F_BP = 34, F_BFLUX = 35,
+               F_BPROD = 36 };
 
 struct Ctx {
   O4Args a;
@@ -213,9 +216,11 @@ __device__ __forceinline__ double normalizeStencil(double (&v)[N]) {
   return scale;
 }
 
-__device__ __forceinline__ void wenozSide(double m2, double m1, double c0, double p1, double p2, double& out) {
-  // a_k = d_k (1 + tau / D_k), D_k = beta_k + eps; out = sum a_k q_k / sum a_k
-  // evaluated with one division: a_k prop. to d_k (D_k + tau) prod_{j != k} D_j.
+__device__ __forceinline__ void wenozSide(double m2, double m1, double c0, double p1, double p2, double& num,
+                                          double& den) {
+  // a_k = d_k (1 + tau / D_k), D_k = beta_k + eps; the state is
+  // sum a_k q_k / sum a_k = num / den with a_k replaced by the proportional
+  // d_k (D_k + tau) prod_{j != k} D_j (no division here).
   const double eps = 1.0e-40, d0 = 1.0 / 16.0, d1 = 5.0 / 8.0, d2 = 5.0 / 16.0;
   const double q0 = (3.0 * m2 - 10.0 * m1 + 15.0 * c0) * 0.125;
   const double q1 = (-m1 + 6.0 * c0 + 3.0 * p1) * 0.125;
@@ -231,7 +236,8 @@ __device__ __forceinline__ void wenozSide(double m2, double m1, double c0, doubl
   const double w0 = d0 * (D0 + tau5) * (D1 * D2);
   const double w1 = d1 * (D1 + tau5) * (D0 * D2);
   const double w2 = d2 * (D2 + tau5) * (D0 * D1);
-  out = (w0 * q0 + w1 * q1 + w2 * q2) / (w0 + w1 + w2);
+  num = w0 * q0 + w1 * q1 + w2 * q2;
+  den = w0 + w1 + w2;
 }
 
 // f_wenoz_pointwise_faceF (:782-878), one component, cells W[i-3..i+2].
@@ -239,11 +245,15 @@ __device__ __forceinline__ void wenozFace(const double in[6], double& L, double&
   double v[6] = {in[0], in[1], in[2], in[3], in[4], in[5]};
   const double scale = normalizeStencil(v);
   if (scale == 0.0) { L = R = 0.0; return; }
-  double l, r;
-  wenozSide(v[0], v[1], v[2], v[3], v[4], l);
-  wenozSide(v[5], v[4], v[3], v[2], v[1], r);
-  L = scale * l;
-  R = scale * r;
+  // Both sides' quotients from one division: nl / dl = nl dr / (dl dr).
+  // On normalised stencils (|v| <= 1) every weight lies in [6e-122, 5e4], so
+  // the product of the denominators neither underflows nor overflows.
+  double nl, dl, nr, dr;
+  wenozSide(v[0], v[1], v[2], v[3], v[4], nl, dl);
+  wenozSide(v[5], v[4], v[3], v[2], v[1], nr, dr);
+  const double inv = 1.0 / (dl * dr);
+  L = scale * (nl * dr * inv);
+  R = scale * (nr * dl * inv);
 }
 
 // f_weno3_pointwise_faceF (:881-946), one component, cells W[i-2..i+1].
@@ -652,339 +662,6 @@ __global__ void __launch_bounds__(128, MB) o4RoePointKernel(const Ctx* __restric
   });
 }
 
-// 5. theta-aware point-to-average of the flux sum and total pressure (F1).
-template <int D>
-__global__ void o4FaceAvgKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
-  const WorkChunk wc = wk[blockIdx.x];
-  const Ctx& c = tab[wc.box * 3 + D];
-  const O4Args& a = c.a;
-  constexpr int d = D;
-  forRegion(c.F1, wc, [&](int b, int i, int j, int k) {
-    const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
-    double* base = a.face + (long)b * kO4FaceArrays * NF;
-    const bool sm = base[F_THF * NF + fo] > 0.5;
-    const View FS = faceView(c, b, F_FS);
-    const View PS = faceView(c, b, F_PS);
-    // All loads come before the first store: the stores go to the same face
-    // scratch, so the compiler may not hoist a later load above one, and
-    // interleaving them would serialise one memory round trip per component.
-    double out[9];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const double pt = FS(q, i, j, k);
-      out[q] = sm ? pt + lapFace(FS, q, d, i, j, k) * (1.0 / 24.0) : pt;
-    }
-    const double pp = PS(0, i, j, k);
-    out[8] = sm ? pp + lapFace(PS, 0, d, i, j, k) * (1.0 / 24.0) : pp;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) base[(F_FA + q) * NF + fo] = out[q];
-    base[F_PA * NF + fo] = out[8];
-  });
-}
-
-// 6. mapped flux with separable metrics (bertaMapHostBox, :35-95 and
-// :1361-1450) on F1; zero on F outside it.
-template <int D>
-__global__ void o4FaceMapKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
-  const WorkChunk wc = wk[blockIdx.x];
-  const Ctx& c = tab[wc.box * 3 + D];
-  const O4Args& a = c.a;
-  constexpr int d = D;
-  const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
-  const bool skipFirst = t1 == 0;
-  forRegion(c.F, wc, [&](int b, int i, int j, int k) {
-    const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
-    double* base = a.face + (long)b * kO4FaceArrays * NF;
-    const bool in1 = (d == 0 || (i >= c.F1.lo[0] && i <= c.F1.hi[0])) && (d == 1 || (j >= c.F1.lo[1] && j <= c.F1.hi[1])) &&
-                     (d == 2 || (k >= c.F1.lo[2] && k <= c.F1.hi[2]));
-    if (!in1) {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) base[(F_FM + q) * NF + fo] = 0.0;
-      return;
-    }
-    const int blk = a.block0 + b;
-    const double* M = faceRec(a.G, blk, d, j, k);
-    double dM[2][10];
-    const int tr[2] = {t1, t2};
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int t = tr[q];
-      int pa[3] = {i, j, k}, pb[3] = {i, j, k};
-      pa[t] += 1; pb[t] -= 1;
-      const double* Ma = faceRec(a.G, blk, d, pa[1], pa[2]);
-      const double* Mb = faceRec(a.G, blk, d, pb[1], pb[2]);
-#pragma unroll
-      for (int e = 0; e < 10; ++e) dM[q][e] = 0.5 * Ma[e] - 0.5 * Mb[e];
-    }
-    const View FA = faceView(c, b, F_FA);
-    double dF[2][8], fa[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      fa[q] = FA(q, i, j, k);
-      dF[0][q] = skipFirst ? 0.0 : cdiff(FA, q, t1, i, j, k);
-      dF[1][q] = cdiff(FA, q, t2, i, j, k);
-    }
-    double out[8];
-#pragma unroll
-    for (int qq = 0; qq < 2; ++qq) {
-      const int q = qq == 0 ? 0 : 4;
-      double term = 0.0;
-      if (!skipFirst) term += dM[0][9] * dF[0][q] * (1.0 / 12.0);
-      term += dM[1][9] * dF[1][q] * (1.0 / 12.0);
-      term += M[9] * fa[q] * 1.0;
-      out[q] = 0.0 + term;
-    }
-#pragma unroll
-    for (int bb = 0; bb < 2; ++bb) {
-      const int bs = bb == 0 ? 1 : 5;
-#pragma unroll
-      for (int row = 0; row < 3; ++row) {
-        double sum = 0.0;
-#pragma unroll
-        for (int col = 0; col < 3; ++col) {
-          double term = 0.0;
-          if (!skipFirst) term += dM[0][3 * row + col] * dF[0][bs + col] * (1.0 / 12.0);
-          term += dM[1][3 * row + col] * dF[1][bs + col] * (1.0 / 12.0);
-          term += M[3 * row + col] * fa[bs + col] * 1.0;
-          sum += term;
-        }
-        out[bs + row] = sum;
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) base[(F_FM + q) * NF + fo] = out[q];
-  });
-}
-
-// 7. radial-area face products of the mapped flux and of <p_tot> (F1).
-template <int D>
-__global__ void o4FaceRadialKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
-  const WorkChunk wc = wk[blockIdx.x];
-  const Ctx& c = tab[wc.box * 3 + D];
-  const O4Args& a = c.a;
-  constexpr int d = D;
-  forRegion(c.F1, wc, [&](int b, int i, int j, int k) {
-    const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
-    double* base = a.face + (long)b * kO4FaceArrays * NF;
-    const double s = adjDr(a.G, d, i);
-    const double ds = 0.5 * adjDr(a.G, d, i + 1) - 0.5 * adjDr(a.G, d, i - 1);
-    const View FM = faceView(c, b, F_FM);
-    const View PA = faceView(c, b, F_PA);
-    // all loads before the first store into the shared face scratch
-    double out[9];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      double value = 0.0;
-      if (d != 0) value += (0.5 * FM(q, i + 1, j, k) - 0.5 * FM(q, i - 1, j, k)) * ds * (1.0 / 12.0);
-      value += FM(q, i, j, k) * s * 1.0;
-      out[q] = value;
-    }
-    double value = 0.0;
-    if (d != 0) value += (0.5 * PA(0, i + 1, j, k) - 0.5 * PA(0, i - 1, j, k)) * ds * (1.0 / 12.0);
-    value += PA(0, i, j, k) * s * 1.0;
-    out[8] = value;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) base[(F_FR + q) * NF + fo] = out[q];
-    base[F_T3 * NF + fo] = out[8];
-  });
-}
-
-// 8. pressure force, dissipation, combine on the final faces V0; writes the
-// flux (scratch and caller).
-template <int D, int MB>
-__global__ void __launch_bounds__(128, MB) o4FaceFinalKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
-  const WorkChunk wc = wk[blockIdx.x];
-  const Ctx& c = tab[wc.box * 3 + D];
-  const O4Args& a = c.a;
-  constexpr int d = D;
-  const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
-  const int tr[2] = {t1, t2};
-  forRegion(c.V0, wc, [&](int b, int i, int j, int k) {
-    const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
-    double* base = a.face + (long)b * kO4FaceArrays * NF;
-    const int blk = a.block0 + b;
-    const double* M = faceRec(a.G, blk, d, j, k);
-    double fs[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) fs[q] = base[(F_FR + q) * NF + fo];
-    // pressure force: <adjA> x <p_tot adjDr> (bertaFaceTensorProduct)
-    const View T3 = faceView(c, b, F_T3);
-#pragma unroll
-    for (int row = 0; row < 3; ++row) {
-      double value = 0.0;
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int t = tr[q];
-        if (d != 0 && t == 0) continue;
-        int pa[3] = {i, j, k}, pb[3] = {i, j, k};
-        pa[t] += 1; pb[t] -= 1;
-        const double dn = 0.5 * faceRec(a.G, blk, d, pa[1], pa[2])[10 + row] - 0.5 * faceRec(a.G, blk, d, pb[1], pb[2])[10 + row];
-        value += dn * cdiff(T3, 0, t, i, j, k) * (1.0 / 12.0);
-      }
-      value += M[10 + row] * T3(0, i, j, k) * 1.0;
-      fs[1 + row] += value;
-    }
-    const bool sm = base[F_THF * NF + fo] > 0.5;
-    const View QD = faceView(c, b, F_QD);
-    double diss[8];
-    if (roeNow(a.G)) {
-      double dM[2][10];
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int t = tr[q];
-        int pa[3] = {i, j, k}, pb[3] = {i, j, k};
-        pa[t] += 1; pb[t] -= 1;
-        const double* Ma = faceRec(a.G, blk, d, pa[1], pa[2]);
-        const double* Mb = faceRec(a.G, blk, d, pb[1], pb[2]);
-#pragma unroll
-        for (int e = 0; e < 10; ++e) dM[q][e] = 0.5 * Ma[e] - 0.5 * Mb[e];
-      }
-      // point-to-average and transverse differences of the eight point
-      // dissipations.  Their 40 inputs (8 components x the face and its four
-      // transverse neighbours) are copied into this thread's shared column
-      // with asynchronous copies, all in flight at once: the gathers from
-      // the face scratch are this kernel's bound, and loads into registers
-      // would be issued a few at a time under the register cap.
-      __shared__ double sRaw[40][128];
-      {
-        int m1[3] = {i, j, k}, p1[3] = {i, j, k}, m2[3] = {i, j, k}, p2[3] = {i, j, k};
-        m1[t1] -= 1; p1[t1] += 1; m2[t2] -= 1; p2[t2] += 1;
-        const long off[5] = {roff(QD.r, i, j, k), roff(QD.r, m1[0], m1[1], m1[2]), roff(QD.r, p1[0], p1[1], p1[2]),
-                             roff(QD.r, m2[0], m2[1], m2[2]), roff(QD.r, p2[0], p2[1], p2[2])};
-        const unsigned col = (unsigned)__cvta_generic_to_shared(&sRaw[0][threadIdx.x]);
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-#pragma unroll
-          for (int e = 0; e < 5; ++e) {
-            const size_t src = __cvta_generic_to_global(QD.p + q * QD.r.N + off[e]);
-            const unsigned dst = col + (unsigned)((q * 5 + e) * 128 * sizeof(double));
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
-          }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-      }
-      double avg[8], dP0[8], dP1[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const double pt = sRaw[q * 5][threadIdx.x], a1 = sRaw[q * 5 + 1][threadIdx.x], b1 = sRaw[q * 5 + 2][threadIdx.x];
-        const double a2 = sRaw[q * 5 + 3][threadIdx.x], b2 = sRaw[q * 5 + 4][threadIdx.x];
-        const double lap = (a1 + b1) + (a2 + b2) - 4.0 * pt;
-        avg[q] = sm ? pt + lap * (1.0 / 24.0) : pt;
-        dP0[q] = 0.5 * b1 - 0.5 * a1;
-        dP1[q] = 0.5 * b2 - 0.5 * a2;
-      }
-      diss[0] = faceProd(M[9], avg[0], dM[0][9], dP0[0], dM[1][9], dP1[0]);
-      diss[4] = faceProd(M[9], avg[4], dM[0][9], dP0[4], dM[1][9], dP1[4]);
-#pragma unroll
-      for (int bb = 0; bb < 2; ++bb) {
-        const int bs = bb == 0 ? 1 : 5;
-#pragma unroll
-        for (int row = 0; row < 3; ++row) {
-          double sum = 0.0;
-#pragma unroll
-          for (int col = 0; col < 3; ++col)
-            sum += faceProd(M[3 * row + col], avg[bs + col], dM[0][3 * row + col], dP0[bs + col], dM[1][3 * row + col],
-                            dP1[bs + col]);
-          diss[bs + row] = sum;
-        }
-      }
-    } else {
-      double qv[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const double pt = QD(q, i, j, k);
-        qv[q] = sm ? pt + lapFace(QD, q, d, i, j, k) * (1.0 / 24.0) : pt;
-      }
-#pragma unroll
-      for (int bb = 0; bb < 2; ++bb) {
-        const int bs = bb == 0 ? 1 : 5;
-#pragma unroll
-        for (int row = 0; row < 3; ++row)
-          diss[bs + row] = M[3 * row] * qv[bs] * 1.0 + M[3 * row + 1] * qv[bs + 1] * 1.0 + M[3 * row + 2] * qv[bs + 2] * 1.0;
-      }
-      diss[0] = M[9] * qv[0];
-      diss[4] = M[9] * qv[4];
-      // face wave-speed bound (:1665-1720)
-      double l[8], r[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) { l[q] = base[(F_WL + q) * NF + fo]; r[q] = base[(F_WR + q) * NF + fo]; }
-      const double* A = faceBasis<D>(c, b, j, k);
-      double rho = 0.5 * (l[0] + r[0]);
-      const double w_d = 0.5 * (l[1 + d] + r[1 + d]);
-      const double bs3[3] = {0.5 * (l[5] + r[5]), 0.5 * (l[6] + r[6]), 0.5 * (l[7] + r[7])};
-      double p = 0.5 * (l[4] + r[4]);
-      if (p < 0.0) p = 0.0;
-      rho = dmax(rho, kRHO00);
-      double Bn = 0.0, Bm = 0.0;
-#pragma unroll
-      for (int e0 = 0; e0 < 3; ++e0) {
-        const double bC = A[3 * e0] * bs3[0] + A[3 * e0 + 1] * bs3[1] + A[3 * e0 + 2] * bs3[2];
-        Bn += A[3 * e0] * bC;
-        Bm += bC * bC;
-      }
-      Bm = sqrt(Bm);
-      const double g = a.G.gamma;
-      const double ce = sqrt(g * p / rho);
-      const double aa = ce * ce + Bm * Bm / (4.0 * kPi * rho);
-      const double bb2 = fabs(Bn) * ce / sqrt(kPi * rho);
-      const double af = 0.5 * (sqrt(dmax(0.0, aa + bb2)) + sqrt(dmax(0.0, aa - bb2)));
-      const double Am = sqrt(A[d] * A[d] + A[3 + d] * A[3 + d] + A[6 + d] * A[6 + d]);
-      const double speed = fabs(w_d) + af * Am;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) diss[q] *= speed;
-    }
-    double fx[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      fx[q] = 0.5 * (fs[q] - diss[q]);
-      base[(F_FX + q) * NF + fo] = fx[q];
-    }
-    if (a.flux[d]) {
-      Box3 V0 = c.V0;
-      const Reg r0 = regOf(V0);
-      double* fo2 = a.flux[d] + (long)b * 8 * r0.N + roff(r0, i, j, k);
-#pragma unroll
-      for (int q = 0; q < 8; ++q) fo2[q * r0.N] = fx[q];
-    }
-    if (rg.reg && d > 0) {
-      const int f = d == 1 ? j : k;
-      if (f == 0 || f == a.G.na) {
-        const long nrna = (long)a.G.na * a.G.nr;
-        const int side = f == 0 ? 0 : 1, s = d == 1 ? k : j;
-        const double w = rg.wDev ? rg.w * (rg.cfl / *rg.wDev) : rg.w;
-        double* R = rg.reg + (((long)blk * 2 + (d - 1)) * 2 + side) * 8 * nrna + (long)s * a.G.nr + i;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) R[q * nrna] += w * fx[q];
-      }
-    }
-  });
-}
-
-// 9. flux divergence into rhs (V).
-template <int D>
-__global__ void o4DivKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
-  const WorkChunk wc = wk[blockIdx.x];
-  const Ctx& c = tab[wc.box * 3 + D];
-  const O4Args& a = c.a;
-  constexpr int d = D;
-  const double coef = -a.scale / a.G.dx[d];
-  forRegion(c.V, wc, [&](int b, int i, int j, int k) {
-    const View FX = faceView(c, b, F_FX);
-    int p[3] = {i, j, k};
-    p[d] += 1;
-    double* R = a.rhs + b * a.rhsStride + roff(c.vr, i, j, k);
-    // all loads (fluxes and the accumulated rhs) before the first store
-    double dfx[8], rv[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      dfx[q] = FX(q, p[0], p[1], p[2]) - FX(q, i, j, k);
-      rv[q] = R[q * c.vr.N];
-    }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) R[q * c.vr.N] = rv[q] + coef * dfx[q];
-  });
-}
-
 // 10. Powell face flux (DivBPowell1, src/BoxOp_DivBcleaning.H:35-74).
 template <int D>
 __global__ void o4PowellFluxKernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
@@ -1180,6 +857,479 @@ __global__ void o4GravityKernel(const Ctx* __restrict__ tab, const RegArgs rg, c
 }
 
 
+// ---- fused face chain ----------------------------------------------------------
+// One CTA (128 threads) takes a tile of the final faces of direction d and
+// runs the whole chain after the reconstruction and the Roe point
+// dissipation on it: the theta-aware point-to-average of the flux sum and of
+// the total pressure (5), the mapped flux with its transverse products (6),
+// the radial-area products (7), the pressure force, the dissipation average
+// and the final flux (8), and the flux divergence into rhs (9).  The
+// intermediates (averaged fluxes, mapped fluxes, radial products) live in
+// shared memory; only the reconstruction's face arrays (FS, PS, thF, QD and,
+// for the Rusanov speed, WL and WR) are read from the face scratch, and the
+// only global writes are rhs, the caller's flux and the seam register.
+//
+// d = 1, 2: the threads cover TI radial x TT angular (t) faces; the CTA
+// walks the normal direction over a segment of cells [c0, c1], one face
+// slab after another, and keeps each face's flux in registers for the
+// divergence of the next cell.  d = 0: the threads cover TI radial cells
+// (TI + 1 faces) x TT rows of j and walk k over [c0, c1], the averages of
+// rows k - 1, k, k + 1 held in a ring of three shared slabs.
+//
+// Every product and sum is formed as in the separate steps of the chain
+// (same operands, same order), so the results do not depend on the tiling.
+struct ChainTile {
+  int box;
+  int i0, a0;  // first radial index; first angular index across the tile (t for d != 0, j for d = 0)
+  int c0, c1;  // walk range of cells (d != 0: along d; d = 0: along k)
+};
+
+template <int D>
+__device__ __forceinline__ void chainPt(int i, int n, int t, int p[3]) {
+  // d != 0: (radial i, normal n, angular t) -> (i, j, k)
+  p[0] = i;
+  p[1] = D == 1 ? n : t;
+  p[2] = D == 1 ? t : n;
+}
+
+// Final flux of one face from its mapped-and-radial flux fs (pressure force
+// added here), the dissipation inputs and the metrics (the final flux of
+// the reference's face pass).  dT3[q]: centred difference of the radial
+// pressure product along transverse q (unused where the separable metrics
+// skip it).
+template <int D>
+__device__ __forceinline__ void chainFinal(const Ctx& c, int i, int j, int k, double fs[8], const double t3,
+                                           const double dT3[2], double fx[8]) {
+  const O4Args& a = c.a;
+  constexpr int d = D;
+  const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+  const int tr[2] = {t1, t2};
+  const int blk = a.block0;
+  const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
+  const double* base = a.face;
+  const double* M = faceRec(a.G, blk, d, j, k);
+#pragma unroll
+  for (int row = 0; row < 3; ++row) {
+    double value = 0.0;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int t = tr[q];
+      if (d != 0 && t == 0) continue;
+      int pa[3] = {i, j, k}, pb[3] = {i, j, k};
+      pa[t] += 1; pb[t] -= 1;
+      const double dn = 0.5 * faceRec(a.G, blk, d, pa[1], pa[2])[10 + row] - 0.5 * faceRec(a.G, blk, d, pb[1], pb[2])[10 + row];
+      value += dn * dT3[q] * (1.0 / 12.0);
+    }
+    value += M[10 + row] * t3 * 1.0;
+    fs[1 + row] += value;
+  }
+  const bool sm = base[F_THF * NF + fo] > 0.5;
+  const View QD = faceView(c, 0, F_QD);
+  double diss[8];
+  if (roeNow(a.G)) {
+    double dM[2][10];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int t = tr[q];
+      int pa[3] = {i, j, k}, pb[3] = {i, j, k};
+      pa[t] += 1; pb[t] -= 1;
+      const double* Ma = faceRec(a.G, blk, d, pa[1], pa[2]);
+      const double* Mb = faceRec(a.G, blk, d, pb[1], pb[2]);
+#pragma unroll
+      for (int e = 0; e < 10; ++e) dM[q][e] = 0.5 * Ma[e] - 0.5 * Mb[e];
+    }
+    int m1[3] = {i, j, k}, p1[3] = {i, j, k}, m2[3] = {i, j, k}, p2[3] = {i, j, k};
+    m1[t1] -= 1; p1[t1] += 1; m2[t2] -= 1; p2[t2] += 1;
+    const long o0 = roff(QD.r, i, j, k), oa1 = roff(QD.r, m1[0], m1[1], m1[2]), ob1 = roff(QD.r, p1[0], p1[1], p1[2]);
+    const long oa2 = roff(QD.r, m2[0], m2[1], m2[2]), ob2 = roff(QD.r, p2[0], p2[1], p2[2]);
+    double avg[8], dP0[8], dP1[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const double* Q = QD.p + q * QD.r.N;
+      const double pt = Q[o0], a1 = Q[oa1], b1 = Q[ob1], a2 = Q[oa2], b2 = Q[ob2];
+      const double lap = (a1 + b1) + (a2 + b2) - 4.0 * pt;
+      avg[q] = sm ? pt + lap * (1.0 / 24.0) : pt;
+      dP0[q] = 0.5 * b1 - 0.5 * a1;
+      dP1[q] = 0.5 * b2 - 0.5 * a2;
+    }
+    diss[0] = faceProd(M[9], avg[0], dM[0][9], dP0[0], dM[1][9], dP1[0]);
+    diss[4] = faceProd(M[9], avg[4], dM[0][9], dP0[4], dM[1][9], dP1[4]);
+#pragma unroll
+    for (int bb = 0; bb < 2; ++bb) {
+      const int bs = bb == 0 ? 1 : 5;
+#pragma unroll
+      for (int row = 0; row < 3; ++row) {
+        double sum = 0.0;
+#pragma unroll
+        for (int col = 0; col < 3; ++col)
+          sum += faceProd(M[3 * row + col], avg[bs + col], dM[0][3 * row + col], dP0[bs + col], dM[1][3 * row + col],
+                          dP1[bs + col]);
+        diss[bs + row] = sum;
+      }
+    }
+  } else {
+    double qv[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const double pt = QD(q, i, j, k);
+      qv[q] = sm ? pt + lapFace(QD, q, d, i, j, k) * (1.0 / 24.0) : pt;
+    }
+#pragma unroll
+    for (int bb = 0; bb < 2; ++bb) {
+      const int bs = bb == 0 ? 1 : 5;
+#pragma unroll
+      for (int row = 0; row < 3; ++row)
+        diss[bs + row] = M[3 * row] * qv[bs] * 1.0 + M[3 * row + 1] * qv[bs + 1] * 1.0 + M[3 * row + 2] * qv[bs + 2] * 1.0;
+    }
+    diss[0] = M[9] * qv[0];
+    diss[4] = M[9] * qv[4];
+    // face wave-speed bound (:1665-1720)
+    double l[8], r[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { l[q] = base[(F_WL + q) * NF + fo]; r[q] = base[(F_WR + q) * NF + fo]; }
+    const double* A = faceBasis<D>(c, 0, j, k);
+    double rho = 0.5 * (l[0] + r[0]);
+    const double w_d = 0.5 * (l[1 + d] + r[1 + d]);
+    const double bs3[3] = {0.5 * (l[5] + r[5]), 0.5 * (l[6] + r[6]), 0.5 * (l[7] + r[7])};
+    double p = 0.5 * (l[4] + r[4]);
+    if (p < 0.0) p = 0.0;
+    rho = dmax(rho, kRHO00);
+    double Bn = 0.0, Bm = 0.0;
+#pragma unroll
+    for (int e0 = 0; e0 < 3; ++e0) {
+      const double bC = A[3 * e0] * bs3[0] + A[3 * e0 + 1] * bs3[1] + A[3 * e0 + 2] * bs3[2];
+      Bn += A[3 * e0] * bC;
+      Bm += bC * bC;
+    }
+    Bm = sqrt(Bm);
+    const double g = a.G.gamma;
+    const double ce = sqrt(g * p / rho);
+    const double aa = ce * ce + Bm * Bm / (4.0 * kPi * rho);
+    const double bb2 = fabs(Bn) * ce / sqrt(kPi * rho);
+    const double af = 0.5 * (sqrt(dmax(0.0, aa + bb2)) + sqrt(dmax(0.0, aa - bb2)));
+    const double Am = sqrt(A[d] * A[d] + A[3 + d] * A[3 + d] + A[6 + d] * A[6 + d]);
+    const double speed = fabs(w_d) + af * Am;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) diss[q] *= speed;
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) fx[q] = 0.5 * (fs[q] - diss[q]);
+}
+
+// The caller's flux and the seam register of one final face.
+template <int D>
+__device__ __forceinline__ void chainStore(const Ctx& c, const RegArgs& rg, int i, int j, int k, const double fx[8]) {
+  const O4Args& a = c.a;
+  constexpr int d = D;
+  if (a.flux[d]) {
+    const Reg r0 = regOf(c.V0);
+    double* fo2 = a.flux[d] + roff(r0, i, j, k);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) fo2[q * r0.N] = fx[q];
+  }
+  if (rg.reg && d > 0) {
+    const int f = d == 1 ? j : k;
+    if (f == 0 || f == a.G.na) {
+      const long nrna = (long)a.G.na * a.G.nr;
+      const int side = f == 0 ? 0 : 1, s = d == 1 ? k : j;
+      const double w = rg.wDev ? rg.w * (rg.cfl / *rg.wDev) : rg.w;
+      double* R = rg.reg + (((long)a.block0 * 2 + (d - 1)) * 2 + side) * 8 * nrna + (long)s * a.G.nr + i;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) R[q * nrna] += w * fx[q];
+    }
+  }
+}
+
+// Point-to-average of the flux sum and total pressure at one face (5).
+__device__ __forceinline__ void chainAverage(const Ctx& c, int d, int i, int j, int k, double fa[8], double& pa) {
+  const long NF = c.fr.N, fo = roff(c.fr, i, j, k);
+  const double* base = c.a.face;
+  const bool sm = base[F_THF * NF + fo] > 0.5;
+  const View FS = faceView(c, 0, F_FS);
+  const View PS = faceView(c, 0, F_PS);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const double pt = FS(q, i, j, k);
+    fa[q] = sm ? pt + lapFace(FS, q, d, i, j, k) * (1.0 / 24.0) : pt;
+  }
+  const double pp = PS(0, i, j, k);
+  pa = sm ? pp + lapFace(PS, 0, d, i, j, k) * (1.0 / 24.0) : pp;
+}
+
+// Directions 1, 2: walk the normal direction.
+template <int D, int TI, int MB>
+__global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restrict__ tab, const RegArgs rg,
+                                                             const ChainTile* __restrict__ tiles) {
+  static_assert(D == 1 || D == 2, "angular directions");
+  constexpr int TT = 128 / TI, NI = TI + 2, NT = TT + 2;
+  constexpr int tdim = D == 1 ? 2 : 1;
+  __shared__ double sFA[8][NI * NT];
+  __shared__ double sPA[NI * NT];
+  __shared__ double sFM[8][NI * TT];
+  __shared__ double sT3[TI * NT];
+  const ChainTile tl = tiles[blockIdx.x];
+  const Ctx& c = tab[tl.box * 3 + D];
+  const O4Args& a = c.a;
+  const int tid = threadIdx.x, li = tid % TI, lt = tid / TI;
+  const int i = tl.i0 + li, t = tl.a0 + lt;
+  const bool mine = i <= c.V.hi[0] && t <= c.V.hi[tdim];
+  // radial products: area at i and its centred difference
+  const double s = adjDr(a.G, D, i), ds = 0.5 * adjDr(a.G, D, i + 1) - 0.5 * adjDr(a.G, D, i - 1);
+  const double coef = -a.scale / a.G.dx[D];
+  const int ilo = c.V.lo[0] - 1, ihi = c.V.hi[0] + 1, tlo = c.V.lo[tdim] - 1, thi = c.V.hi[tdim] + 1;
+  double fxPrev[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) fxPrev[q] = 0.0;
+  const int nEnd = tl.c1 + 1;
+  const bool lastSegment = tl.c1 == c.V.hi[D];
+  for (int n = tl.c0; n <= nEnd; ++n) {
+    // (5) averages on radial i0-1 .. i0+TI x angular a0-1 .. a0+TT of face slab n
+    for (int q = tid; q < NI * NT; q += 128) {
+      const int ii = tl.i0 - 1 + q % NI, tt = tl.a0 - 1 + q / NI;
+      if (ii < ilo || ii > ihi || tt < tlo || tt > thi) continue;
+      int p[3];
+      chainPt<D>(ii, n, tt, p);
+      double fa[8], pa;
+      chainAverage(c, D, p[0], p[1], p[2], fa, pa);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) sFA[e][q] = fa[e];
+      sPA[q] = pa;
+    }
+    __syncthreads();
+    // (6) mapped flux on radial i0-1 .. i0+TI x angular a0 .. a0+TT-1; the
+    // radial transverse derivative of the angular metrics vanishes (skipped)
+    for (int q = tid; q < NI * TT; q += 128) {
+      const int ii = tl.i0 - 1 + q % NI, tt = tl.a0 + q / NI;
+      if (ii < ilo || ii > ihi || tt > c.V.hi[tdim]) continue;
+      int p[3];
+      chainPt<D>(ii, n, tt, p);
+      const double* M = faceRec(a.G, a.block0, D, p[1], p[2]);
+      int pa[3] = {p[0], p[1], p[2]}, pb[3] = {p[0], p[1], p[2]};
+      pa[tdim] += 1; pb[tdim] -= 1;
+      const double* Ma = faceRec(a.G, a.block0, D, pa[1], pa[2]);
+      const double* Mb = faceRec(a.G, a.block0, D, pb[1], pb[2]);
+      double dM[10];
+#pragma unroll
+      for (int e = 0; e < 10; ++e) dM[e] = 0.5 * Ma[e] - 0.5 * Mb[e];
+      const int qc = q + NI;  // (ii, tt) in the averages' frame (rows from a0 - 1)
+      const int qu = qc + NI, qd = qc - NI;
+      double fa[8], dF[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        fa[e] = sFA[e][qc];
+        dF[e] = 0.5 * sFA[e][qu] - 0.5 * sFA[e][qd];
+      }
+      double out[8];
+#pragma unroll
+      for (int qq = 0; qq < 2; ++qq) {
+        const int e = qq == 0 ? 0 : 4;
+        double term = 0.0;
+        term += dM[9] * dF[e] * (1.0 / 12.0);
+        term += M[9] * fa[e] * 1.0;
+        out[e] = 0.0 + term;
+      }
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb) {
+        const int bs = bb == 0 ? 1 : 5;
+#pragma unroll
+        for (int row = 0; row < 3; ++row) {
+          double sum = 0.0;
+#pragma unroll
+          for (int col = 0; col < 3; ++col) {
+            double term = 0.0;
+            term += dM[3 * row + col] * dF[bs + col] * (1.0 / 12.0);
+            term += M[3 * row + col] * fa[bs + col] * 1.0;
+            sum += term;
+          }
+          out[bs + row] = sum;
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e) sFM[e][q] = out[e];
+    }
+    // (7) radial product of <p_tot> on radial i0 .. i0+TI-1 x angular a0-1 .. a0+TT
+    for (int q = tid; q < TI * NT; q += 128) {
+      const int ii = tl.i0 + q % TI, tt = tl.a0 - 1 + q / TI;
+      if (ii > c.V.hi[0] || tt < tlo || tt > thi) continue;
+      const double si = adjDr(a.G, D, ii), dsi = 0.5 * adjDr(a.G, D, ii + 1) - 0.5 * adjDr(a.G, D, ii - 1);
+      const int qc = (q / TI) * NI + (q % TI) + 1;  // (ii, tt) in the averages' frame
+      double value = 0.0;
+      value += (0.5 * sPA[qc + 1] - 0.5 * sPA[qc - 1]) * dsi * (1.0 / 12.0);
+      value += sPA[qc] * si * 1.0;
+      sT3[q] = value;
+    }
+    __syncthreads();
+    // (7, 8, 9) this thread's face: radial product of the mapped flux, final
+    // flux, divergence of the cell below it
+    if (mine) {
+      int p[3];
+      chainPt<D>(i, n, t, p);
+      const int qm = lt * NI + li + 1;  // (i, t) in the mapped-flux frame
+      double fs[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        double value = 0.0;
+        value += (0.5 * sFM[e][qm + 1] - 0.5 * sFM[e][qm - 1]) * ds * (1.0 / 12.0);
+        value += sFM[e][qm] * s * 1.0;
+        fs[e] = value;
+      }
+      const int q3 = (lt + 1) * TI + li;  // (i, t) in the pressure-product frame
+      const double dT3[2] = {0.0, 0.5 * sT3[q3 + TI] - 0.5 * sT3[q3 - TI]};
+      double fx[8];
+      chainFinal<D>(c, p[0], p[1], p[2], fs, sT3[q3], dT3, fx);
+      if (n <= tl.c1 || lastSegment) chainStore<D>(c, rg, p[0], p[1], p[2], fx);
+      if (n > tl.c0) {
+        int pc[3];
+        chainPt<D>(i, n - 1, t, pc);
+        double* R = a.rhs + roff(c.vr, pc[0], pc[1], pc[2]);
+        double rv[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) rv[e] = R[e * c.vr.N];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) R[e * c.vr.N] = rv[e] + coef * (fx[e] - fxPrev[e]);
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e) fxPrev[e] = fx[e];
+    }
+    __syncthreads();
+  }
+}
+
+// Direction 0: walk k; shared memory (dynamic): averages of three rows of k
+// [3][8][NS], pressure averages [3][NS], final fluxes [8][(TI + 1) TT].
+template <int TI>
+constexpr int chain0Doubles() {
+  return 3 * 9 * (TI + 1) * (128 / TI + 2) + 8 * (TI + 1) * (128 / TI);
+}
+
+template <int TI, int MB>
+__global__ void __launch_bounds__(128, MB) o4FaceChain0Kernel(const Ctx* __restrict__ tab, const RegArgs rg,
+                                                              const ChainTile* __restrict__ tiles) {
+  constexpr int TT = 128 / TI, NI = TI + 1, NJ = TT + 2, NS = NI * NJ;
+  extern __shared__ double smem[];
+  double* sFA = smem;              // [3][8][NS]
+  double* sPA = sFA + 3 * 8 * NS;  // [3][NS]
+  double* sFX = sPA + 3 * NS;      // [8][NI * TT]
+  const ChainTile tl = tiles[blockIdx.x];
+  const Ctx& c = tab[tl.box * 3 + 0];
+  const O4Args& a = c.a;
+  const int tid = threadIdx.x;
+  const double coef = -a.scale / a.G.dx[0];
+  const int ihi = c.V.hi[0] + 1, jlo = c.V.lo[1] - 1, jhi = c.V.hi[1] + 1;
+  auto slot = [&](int k) { return (k - tl.c0 + 3) % 3; };
+  auto slab = [&](int k) {
+    double* fa = sFA + slot(k) * 8 * NS;
+    double* pa = sPA + slot(k) * NS;
+    for (int q = tid; q < NS; q += 128) {
+      const int ii = tl.i0 + q % NI, jj = tl.a0 - 1 + q / NI;
+      if (ii > ihi || jj < jlo || jj > jhi) continue;
+      double f[8], pp;
+      chainAverage(c, 0, ii, jj, k, f, pp);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) fa[e * NS + q] = f[e];
+      pa[q] = pp;
+    }
+  };
+  slab(tl.c0 - 1);
+  slab(tl.c0);
+  for (int k = tl.c0; k <= tl.c1; ++k) {
+    slab(k + 1);
+    __syncthreads();
+    const double* F0 = sFA + slot(k) * 8 * NS;
+    const double* Fm = sFA + slot(k - 1) * 8 * NS;
+    const double* Fp = sFA + slot(k + 1) * 8 * NS;
+    const double* P0 = sPA + slot(k) * NS;
+    const double* Pm = sPA + slot(k - 1) * NS;
+    const double* Pp = sPA + slot(k + 1) * NS;
+    // (6, 7, 8) faces i0 .. i0+TI x rows a0 .. a0+TT-1 of row k
+    for (int q = tid; q < NI * TT; q += 128) {
+      const int ii = tl.i0 + q % NI, jj = tl.a0 + q / NI;
+      if (ii > ihi || jj > c.V.hi[1]) continue;
+      const int qc = q + NI;  // (ii, jj) in the slab frame
+      const double* M = faceRec(a.G, a.block0, 0, jj, k);
+      const double* Mj1 = faceRec(a.G, a.block0, 0, jj + 1, k);
+      const double* Mj0 = faceRec(a.G, a.block0, 0, jj - 1, k);
+      const double* Mk1 = faceRec(a.G, a.block0, 0, jj, k + 1);
+      const double* Mk0 = faceRec(a.G, a.block0, 0, jj, k - 1);
+      double dM0[10], dM1[10];
+#pragma unroll
+      for (int e = 0; e < 10; ++e) {
+        dM0[e] = 0.5 * Mj1[e] - 0.5 * Mj0[e];
+        dM1[e] = 0.5 * Mk1[e] - 0.5 * Mk0[e];
+      }
+      double fa[8], dF0[8], dF1[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        fa[e] = F0[e * NS + qc];
+        dF0[e] = 0.5 * F0[e * NS + qc + NI] - 0.5 * F0[e * NS + qc - NI];
+        dF1[e] = 0.5 * Fp[e * NS + qc] - 0.5 * Fm[e * NS + qc];
+      }
+      double fm[8];
+#pragma unroll
+      for (int qq = 0; qq < 2; ++qq) {
+        const int e = qq == 0 ? 0 : 4;
+        double term = 0.0;
+        term += dM0[9] * dF0[e] * (1.0 / 12.0);
+        term += dM1[9] * dF1[e] * (1.0 / 12.0);
+        term += M[9] * fa[e] * 1.0;
+        fm[e] = 0.0 + term;
+      }
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb) {
+        const int bs = bb == 0 ? 1 : 5;
+#pragma unroll
+        for (int row = 0; row < 3; ++row) {
+          double sum = 0.0;
+#pragma unroll
+          for (int col = 0; col < 3; ++col) {
+            double term = 0.0;
+            term += dM0[3 * row + col] * dF0[bs + col] * (1.0 / 12.0);
+            term += dM1[3 * row + col] * dF1[bs + col] * (1.0 / 12.0);
+            term += M[3 * row + col] * fa[bs + col] * 1.0;
+            sum += term;
+          }
+          fm[bs + row] = sum;
+        }
+      }
+      // radial products (direction 0: no radial correction)
+      const double si = adjDr(a.G, 0, ii);
+      double fs[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        double value = 0.0;
+        value += fm[e] * si * 1.0;
+        fs[e] = value;
+      }
+      auto t3 = [&](double pav) {
+        double value = 0.0;
+        value += pav * si * 1.0;
+        return value;
+      };
+      const double dT3[2] = {0.5 * t3(P0[qc + NI]) - 0.5 * t3(P0[qc - NI]), 0.5 * t3(Pp[qc]) - 0.5 * t3(Pm[qc])};
+      double fx[8];
+      chainFinal<0>(c, ii, jj, k, fs, t3(P0[qc]), dT3, fx);
+      chainStore<0>(c, rg, ii, jj, k, fx);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) sFX[e * NI * TT + q] = fx[e];
+    }
+    __syncthreads();
+    // (9) divergence of the row's cells
+    {
+      const int li = tid % TI, lj = tid / TI;
+      const int i = tl.i0 + li, j = tl.a0 + lj;
+      if (i <= c.V.hi[0] && j <= c.V.hi[1]) {
+        const int q = lj * NI + li;
+        double* R = a.rhs + roff(c.vr, i, j, k);
+        double rv[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) rv[e] = R[e * c.vr.N];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) R[e * c.vr.N] = rv[e] + coef * (sFX[e * NI * TT + q + 1] - sFX[e * NI * TT + q]);
+      }
+    }
+  }
+}
+
 }  // namespace
 
 size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost) {
@@ -1205,6 +1355,12 @@ struct O4Batch {
   long chunkOff[RG_COUNT][3] = {};
   int chunkCount[RG_COUNT][3] = {};
   int var[kO4TunedKernels] = {0, 0, 0};  // register-cap variant of the tuned kernels
+  // tiles of the fused face chain, per direction, in one device array;
+  // chainTI: radial width of a tile (32, 16 or 8 by the narrowest box)
+  ChainTile* chainTiles = nullptr;
+  long chainOff[3] = {};
+  int chainCount[3] = {};
+  int chainTI = 32;
   // The Powell face chain of a direction (face flux, radial product,
   // divergence into -J div B) runs on a side stream beside the main face
   // chain: fork after the reconstruction, join before the next direction.
@@ -1221,10 +1377,45 @@ struct O4Batch {
 };
 
 // Minimum resident CTAs per SM (the register cap) of each variant of the
-// tuned kernels: reconstruction, Roe point dissipation, final flux.
-// Variant 0 is the default.  The final flux's 40 KB shared staging column
-// admits at most 5 CTAs per SM, so its caps stay at or below 5.
-constexpr int kO4MinBlocks[kO4TunedKernels][kO4Variants] = {{6, 4, 8}, {4, 3, 5}, {4, 5, 3}};
+// tuned kernels: reconstruction, Roe point dissipation, fused face chain.
+// Variant 0 is the default.  The direction-0 chain's 51 KB of shared memory
+// (32-wide tiles) admits at most 4 CTAs per SM.
+constexpr int kO4MinBlocks[kO4TunedKernels][kO4Variants] = {{6, 4, 8}, {4, 3, 5}, {4, 3, 5}};
+
+// Tiles of the fused face chain of direction d over the batch's boxes: TI
+// radial x 128/TI across (d = 0: j; d != 0: the other angular index),
+// walking d (d != 0) or k (d = 0) in segments of S cells, S the largest of
+// 64, 32, 16, 8 that still gives about 16 CTAs per SM.
+void chainTiles(const std::vector<Ctx>& host, int nbox, int d, int TI, std::vector<ChainTile>& out) {
+  const int TT = 128 / TI;
+  const int across = d == 0 ? 1 : (d == 1 ? 2 : 1), walk = d == 0 ? 2 : d;
+  long base = 0, longest = 1;
+  for (int b = 0; b < nbox; ++b) {
+    const Box3& V = host[(size_t)b * 3 + d].V;
+    base += (long)((V.n(0) + TI - 1) / TI) * ((V.n(across) + TT - 1) / TT);
+    longest = std::max<long>(longest, V.n(walk));
+  }
+  int S = 64;
+  while (S > 8 && base * ((longest + S - 1) / S) < 148L * 16) S /= 2;
+  for (int b = 0; b < nbox; ++b) {
+    const Box3& V = host[(size_t)b * 3 + d].V;
+    for (int c0 = V.lo[walk]; c0 <= V.hi[walk]; c0 += S)
+      for (int a0 = V.lo[across]; a0 <= V.hi[across]; a0 += TT)
+        for (int i0 = V.lo[0]; i0 <= V.hi[0]; i0 += TI)
+          out.push_back(ChainTile{b, i0, a0, c0, std::min(c0 + S - 1, V.hi[walk])});
+  }
+}
+
+template <int TI>
+cudaError_t chain0Smem() {
+  const int bytes = chain0Doubles<TI>() * (int)sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(o4FaceChain0Kernel<TI, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(o4FaceChain0Kernel<TI, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(o4FaceChain0Kernel<TI, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return e;
+}
 
 void o4BatchSetVariants(O4Batch* B, const int v[kO4TunedKernels]) {
   for (int q = 0; q < kO4TunedKernels; ++q) B->var[q] = v[q] >= 0 && v[q] < kO4Variants ? v[q] : 0;
@@ -1296,7 +1487,28 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
       }
       B->chunkCount[id][d] = (int)count;
     }
-  *err = cudaMalloc(&B->dev, sizeof(Ctx) * B->host.size());
+  {
+    int narrow = 1 << 30;
+    for (int b = 0; b < nbox; ++b) narrow = std::min(narrow, B->host[(size_t)b * 3].V.n(0));
+    B->chainTI = narrow >= 24 ? 32 : narrow >= 12 ? 16 : 8;
+  }
+  std::vector<ChainTile> tiles;
+  for (int d = 0; d < 3; ++d) {
+    B->chainOff[d] = (long)tiles.size();
+    chainTiles(B->host, nbox, d, B->chainTI, tiles);
+    const long count = (long)tiles.size() - B->chainOff[d];
+    if (count > 0x7fffffffL) {
+      *err = cudaErrorInvalidValue;
+      o4BatchDestroy(B);
+      return nullptr;
+    }
+    B->chainCount[d] = (int)count;
+  }
+  *err = B->chainTI == 32 ? chain0Smem<32>() : B->chainTI == 16 ? chain0Smem<16>() : chain0Smem<8>();
+  if (*err == cudaSuccess) *err = cudaMalloc(&B->chainTiles, sizeof(ChainTile) * std::max<size_t>(1, tiles.size()));
+  if (*err == cudaSuccess && !tiles.empty())
+    *err = cudaMemcpy(B->chainTiles, tiles.data(), sizeof(ChainTile) * tiles.size(), cudaMemcpyHostToDevice);
+  if (*err == cudaSuccess) *err = cudaMalloc(&B->dev, sizeof(Ctx) * B->host.size());
   if (*err == cudaSuccess) *err = cudaMemcpy(B->dev, B->host.data(), sizeof(Ctx) * B->host.size(), cudaMemcpyHostToDevice);
   if (*err == cudaSuccess && !work.empty()) {
     *err = cudaMalloc(&B->chunks, sizeof(WorkChunk) * work.size());
@@ -1329,6 +1541,7 @@ void o4BatchDestroy(O4Batch* B) {
   if (!B) return;
   if (B->dev) cudaFree(B->dev);
   if (B->chunks) cudaFree(B->chunks);
+  if (B->chainTiles) cudaFree(B->chainTiles);
   if (B->pointEv) cudaEventDestroy(B->pointEv);
   for (int d = 0; d < 3; ++d) {
     if (B->roeFork[d]) cudaEventDestroy(B->roeFork[d]);
@@ -1370,6 +1583,36 @@ cudaError_t launchO4BatchGravity(const O4Batch* B, cudaStream_t s) {
   if (B->chunkCount[RG_V][0] == 0) return cudaSuccess;
   o4GravityKernel<<<B->chunkCount[RG_V][0], 128, 0, s>>>(B->dev, none, B->chunks + B->chunkOff[RG_V][0]);
   return cudaGetLastError();
+}
+
+// The fused face chain of direction d over the batch's tiles.
+template <int TI, int MB>
+cudaError_t launchChainT(const O4Batch* B, const RegArgs& rg, int d, cudaStream_t s) {
+  const int n = B->chainCount[d];
+  const ChainTile* t = B->chainTiles + B->chainOff[d];
+  if (n == 0) return cudaSuccess;
+  if (d == 0)
+    o4FaceChain0Kernel<TI, MB><<<n, 128, chain0Doubles<TI>() * sizeof(double), s>>>(B->dev, rg, t);
+  else if (d == 1)
+    o4FaceChainKernel<1, TI, MB><<<n, 128, 0, s>>>(B->dev, rg, t);
+  else
+    o4FaceChainKernel<2, TI, MB><<<n, 128, 0, s>>>(B->dev, rg, t);
+  return cudaGetLastError();
+}
+
+template <int TI>
+cudaError_t launchChainV(const O4Batch* B, const RegArgs& rg, int d, cudaStream_t s) {
+  switch (kO4MinBlocks[2][B->var[2]]) {
+    case 3: return launchChainT<TI, 3>(B, rg, d, s);
+    case 5: return launchChainT<TI, 5>(B, rg, d, s);
+    default: return launchChainT<TI, 4>(B, rg, d, s);
+  }
+}
+
+cudaError_t launchChain(const O4Batch* B, const RegArgs& rg, int d, cudaStream_t s) {
+  if (B->chainTI == 32) return launchChainV<32>(B, rg, d, s);
+  if (B->chainTI == 16) return launchChainV<16>(B, rg, d, s);
+  return launchChainV<8>(B, rg, d, s);
 }
 
 cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) {
@@ -1435,12 +1678,8 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
       st = s;
       if ((e = cudaEventRecord(B->roeJoin[d], B->roeSide)) != cudaSuccess) return e;
     }
-    HC_LAUNCH_D(o4FaceAvgKernel, RG_F1)
-    HC_LAUNCH_D(o4FaceMapKernel, RG_F)
-    HC_LAUNCH_D(o4FaceRadialKernel, RG_F1)
     if (B->roe && (e = cudaStreamWaitEvent(s, B->roeJoin[d], 0)) != cudaSuccess) return e;
-    HC_LAUNCH_DM(o4FaceFinalKernel, 2, RG_V0)
-    HC_LAUNCH_D(o4DivKernel, RG_V)
+    if ((e = launchChain(B, rg, d, s)) != cudaSuccess) return e;
     // join before the next direction's reconstruction rewrites the flags
     if (B->powell && (e = cudaStreamWaitEvent(s, B->joinEv[d], 0)) != cudaSuccess) return e;
   }

@@ -237,7 +237,7 @@ class ConeSpec:
 def o4_variants() -> np.ndarray:
     """Minimum resident CTAs per SM of each register-cap variant of the
     fourth-order operator's tuned kernels, [kernel][variant]: reconstruction,
-    Roe point dissipation, final flux (hc_o4_variants)."""
+    Roe point dissipation, fused face chain (hc_o4_variants)."""
     lib = N.lib()
     n = lib.hc_o4_variants(None, 0)
     out = (C.c_int * (3 * n))()
@@ -362,7 +362,7 @@ class Shell:
     def autotune(self, ju: torch.Tensor) -> tuple[tuple[int, ...], np.ndarray]:
         """hc_ctx_autotune with the state `ju` (not modified).  Order 2:
         ((RK stage tile, operator tile), median ms [2][tiles]).  Order 4:
-        ((reconstruction, Roe point, final flux variant), operator ms
+        ((reconstruction, Roe point, face chain variant), operator ms
         [3][variants])."""
         if self.params.spatial_order == 4:
             rows, n = 3, o4_variants().shape[1]

@@ -471,7 +471,7 @@ int hc_ctx_autotune(hc_ctx* ctx, const double* ju, int* tiles, double* ms, void*
 
 /* Number of register-cap variants per tuned fourth-order kernel; with
  * min_blocks non-null, min_blocks[3 q + v] = minimum resident CTAs per SM of
- * variant v of kernel q (0 reconstruction, 1 Roe point, 2 final flux). */
+ * variant v of kernel q (0 reconstruction, 1 Roe point, 2 fused face chain). */
 int hc_o4_variants(int* min_blocks, int capacity);
 
 /* Use the given variants (3 ints, -1 keeps the current one). */

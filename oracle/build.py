@@ -87,11 +87,28 @@ def build_oracle(force: bool = False) -> str:
     return out
 
 
+def _cpu_key() -> str:
+    """Short hash of this CPU's model name and feature flags."""
+    import hashlib
+    text = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith(("model name", "flags")):
+                    text += line
+                if line.strip() == "":
+                    break
+    except OSError:
+        pass
+    return hashlib.sha256(text.encode()).hexdigest()[:12]
+
+
 def build_oracle_native(outdir: str) -> str | None:
     """A -march=native copy of the oracle for the machine that runs it (the
     timed CPU baseline), or None where g++ fails.  Results are the same as
     the portable library's: floating-point contraction stays off."""
     src = os.path.join(HERE, "hc_oracle.cpp")
+    outdir = os.path.join(outdir, _cpu_key())  # a build for one CPU model only
     os.makedirs(outdir, exist_ok=True)
     out = os.path.join(outdir, "libhc_oracle_native.so")
     if _stale(out, _oracle_sources()):

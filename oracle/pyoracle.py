@@ -80,10 +80,23 @@ _orc = None
 _ref = None
 
 
+_lib_path = None
+
+
+def use_library(path: str) -> None:
+    """Load the oracle from `path` (a build of the same source, e.g. the
+    -march=native copy of the timed CPU baseline) instead of the shipped
+    library; only before the first call of lib()."""
+    global _lib_path
+    if _orc is not None and path != _lib_path:
+        raise RuntimeError("the oracle library is already loaded")
+    _lib_path = path
+
+
 def lib() -> C.CDLL:
     global _orc
     if _orc is None:
-        L = _load(os.path.join(HERE, "libhc_oracle.so"))
+        L = _load(_lib_path or os.path.join(HERE, "libhc_oracle.so"))
         L.orc_level_create.restype = C.c_void_p
         L.orc_level_create.argtypes = [C.POINTER(HcParams)]
         L.orc_level_destroy.argtypes = [C.c_void_p]

@@ -32,9 +32,15 @@ SIGN = ((1, -1, -1), (1, 1, 1), (1, -1, 1), (1, 1, 1), (-1, 1, 1), (-1, -1, 1))
 C_MP = 1.67262192e-24
 
 
-def averaged_wind(p, ngl=3, rotation=0.0):
+def averaged_wind(p, ngl=3, rotation=0.0, alfven=None):
     """JU = <J U> over each cell, J = r^2 dr/dxi0 det(A) pointwise; with
-    `rotation` (cm/s) a solid-body rotation about z is added to the wind."""
+    `rotation` (cm/s) a solid-body rotation about z is added to the wind.
+    With alfven = (B0, eps, k): a radial field B0 (r0/r)^2 and on it a
+    torsional Alfven-wave packet, dB = eps B0 (r0/r)^2 g(r) (rhat x k) and
+    dv = -dB / sqrt(4 pi rho) (the wave travelling outward along B), g a
+    Gaussian in the radial mapped coordinate centred mid-shell (width 0.12).
+    dB is divergence-free for any g(r): div(g(r) rhat x k) = 0.  The cells
+    are built a few angular rows at a time (bounded memory at 128^3)."""
     nr, na, gam = p.nr, p.na, p.gamma
     r0, r1, C = p.inner_radius, p.outer_radius, p.radial_stretch
     Rt = (r1 - r0) / np.expm1(C)
@@ -45,26 +51,46 @@ def averaged_wind(p, ngl=3, rotation=0.0):
     drde = Rt * C * np.exp(C * eta)
     s = r0 / r
     xi = ((np.arange(na)[:, None] + gx[None, :]) / na).reshape(-1)
-    a = np.tan(-np.pi / 4 + np.pi / 2 * xi)[None, :]
-    c = np.tan(-np.pi / 4 + np.pi / 2 * xi)[:, None]
-    rh = np.sqrt(1 + a * a + c * c)
-    det = (np.pi / 2) ** 2 * (1 + a * a) * (1 + c * c) / rh ** 3
-    q = (1 / rh, a / rh, c / rh)
     w3 = gw[:, None, None] * gw[None, :, None] * gw[None, None, :]
     rho = 700 * C_MP * s ** 2
     pr = 1e-7 * s ** (2 * gam)
+    radial = dict(eta=eta, r2dr=r ** 2 * drde, s=s, rho=rho, pr=pr)
     ju = np.zeros((6, 8, na, na, nr))
+    rows = max(1, 16 * 32 ** 3 // (na * na * nr))
     for b in range(6):
-        X = np.stack([SIGN[b][k] * np.broadcast_to(q[PERM[b][k]], det.shape) for k in range(3)])
-        J = det[..., None] * (r ** 2 * drde)[None, None, :]
-        U = np.zeros((8,) + J.shape)
-        U[0] = rho
-        v = 500e5 * X[..., None] + rotation * np.stack([-X[1], X[0], np.zeros_like(X[0])])[..., None]
-        U[1:4] = rho * v
-        U[4] = pr / (gam - 1) + 0.5 * rho * (v ** 2).sum(0)
-        JU = (U * J[None]).reshape(8, na, ngl, na, ngl, nr, ngl)
-        ju[b] = np.einsum("ckpjqir,pqr->ckji", JU, w3)
+        for k0 in range(0, na, rows):
+            k1 = min(na, k0 + rows)
+            ju[b, :, k0:k1] = _averaged_rows(b, xi[k0 * ngl:k1 * ngl], xi, ngl, gam, w3, radial, rotation, alfven)
     return np.ascontiguousarray(ju.reshape(-1))
+
+
+def _averaged_rows(b, xk, xj, ngl, gam, w3, radial, rotation, alfven):
+    """<J U> [8][rows][na][nr] of panel b's cells whose Gauss points in k
+    are xk (and xj in j)."""
+    s, rho, pr = radial["s"], radial["rho"], radial["pr"]
+    a = np.tan(-np.pi / 4 + np.pi / 2 * xj)[None, :]
+    c = np.tan(-np.pi / 4 + np.pi / 2 * xk)[:, None]
+    rh = np.sqrt(1 + a * a + c * c)
+    det = (np.pi / 2) ** 2 * (1 + a * a) * (1 + c * c) / rh ** 3
+    q = (1 / rh, a / rh, c / rh)
+    X = np.stack([SIGN[b][k] * np.broadcast_to(q[PERM[b][k]], det.shape) for k in range(3)])
+    J = det[..., None] * radial["r2dr"][None, None, :]
+    U = np.zeros((8,) + J.shape)
+    U[0] = rho
+    v = 500e5 * X[..., None] + rotation * np.stack([-X[1], X[0], np.zeros_like(X[0])])[..., None]
+    B = np.zeros_like(v)
+    if alfven is not None:
+        B0, eps, k = alfven
+        g = np.exp(-0.5 * ((radial["eta"] - 0.5) / 0.12) ** 2)
+        rxk = np.cross(X, np.asarray(k, dtype=float)[:, None, None], axis=0)[..., None]
+        B = B0 * s ** 2 * X[..., None] + eps * B0 * (s ** 2 * g) * rxk
+        v = v - eps * B0 * (s ** 2 * g) * rxk / np.sqrt(4 * np.pi * rho)
+    U[1:4] = rho * v
+    U[5:8] = B
+    U[4] = pr / (gam - 1) + 0.5 * rho * (v ** 2).sum(0) + (B ** 2).sum(0) / (8 * np.pi)
+    nk, na, nr = len(xk) // ngl, len(xj) // ngl, len(s) // ngl
+    JU = (U * J[None]).reshape(8, nk, ngl, na, ngl, nr, ngl)
+    return np.einsum("ckpjqir,pqr->ckji", JU, w3)
 
 
 def test_fourth_order_self_convergence():
@@ -120,3 +146,46 @@ def test_operator_truncation_error_with_rotation():
         errs.append(e / np.maximum(np.abs(ks[li]).max(axis=(0, 2, 3, 4)), 1e-300))
     rates = np.log2(errs[0][:5] / errs[1][:5])
     assert np.all(rates >= 3.5), rates
+
+
+def test_alfven_wave_convergence_with_detector():
+    """Self-convergence on a smooth torsional Alfven-wave packet (5 % of a
+    5e-3 G radial field, on the wind) at 16, 32, 64 and 128 cells per
+    direction, WENOZ + Roe with the Jameson detector at its configured
+    eta_d = 0.02, to the same time with dt halved per level.  Errors over
+    panel interiors (the middle half of each angular index) and the middle
+    half radially.  At 16 cells the detector flags the wind's steep pressure
+    and the fallback reconstruction is second order, so the bar applies to
+    the 32 -> 64 -> 128 rates: >= 3.5 on every component."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    import torch
+
+    from heliocubed_b200.level import Params, Shell
+    levels, steps0 = (16, 32, 64, 128), 4
+    wave = (5e-3, 0.05, (0.36, 0.48, 0.8))
+    states, dt0 = [], None
+    for li, n in enumerate(levels):
+        sh = Shell(Params(nr=n, na=n, spatial_order=4, riemann_solver=2, berta_fallback_type=0))
+        assert sh.params.berta_eta_d == 0.02
+        ju = torch.from_numpy(averaged_wind(sh.params, alfven=wave)).cuda()
+        if dt0 is None:
+            dt0 = 0.3 / float(sh.inv_dt_max(ju).item())
+        dt = dt0 / 2 ** li
+        for s in range(steps0 * 2 ** li):
+            sh.rk4_step(ju, dt, s * dt)
+        assert sh.valid(ju)
+        states.append(ju.cpu().numpy().reshape(6, 8, n, n, n))
+        sh.close()
+        del ju
+        torch.cuda.empty_cache()
+    errs = []
+    for li in range(len(levels) - 1):
+        n = levels[li]
+        fine = states[li + 1].reshape(6, 8, n, 2, n, 2, n, 2).mean(axis=(3, 5, 7))
+        q = slice(n // 4, 3 * n // 4)
+        e = np.abs(fine - states[li])[:, :, q, q, q].max(axis=(0, 2, 3, 4))
+        errs.append(e / np.maximum(np.abs(states[li]).max(axis=(0, 2, 3, 4)), 1e-300))
+    rates = np.array([np.log2(errs[0] / errs[1]), np.log2(errs[1] / errs[2])])
+    print("Alfven-wave convergence rates (16->32->64, 32->64->128), per component:\n", np.round(rates, 2))
+    assert np.all(rates[1] >= 3.5), rates

@@ -775,6 +775,7 @@ void carveO4Scratch(O4Args& a, double* sp) {
   a.th = sp; sp += nb * ng;
   a.thr = sp; sp += nb * ng;
   a.face = sp; sp += nb * (long)kO4FaceArrays * nf;
+  a.face2 = sp; sp += nb * (long)kO4FaceArrays * nf;
   a.mj = sp; sp += nb * n1;
   a.kp = sp;
 }
@@ -897,7 +898,7 @@ O4Batch* cachedBatch(hc_ctx* c, const O4Args& a, int* rc) {
   put(a.vlo, sizeof a.vlo); put(a.vhi, sizeof a.vhi); put(&a.U, sizeof a.U); put(a.ur.lo, sizeof a.ur.lo);
   put(a.ur.n, sizeof a.ur.n); put(&a.uStride, sizeof a.uStride); put(&a.scale, sizeof a.scale);
   put(&a.rhs, sizeof a.rhs); put(&a.rhsStride, sizeof a.rhsStride); put(a.flux, sizeof a.flux);
-  put(&a.WA, sizeof a.WA); put(&a.face, sizeof a.face); put(&a.kp, sizeof a.kp);
+  put(&a.WA, sizeof a.WA); put(&a.face, sizeof a.face); put(&a.face2, sizeof a.face2); put(&a.kp, sizeof a.kp);
   for (auto& e : c->o4cache)
     if (e.first == key) return e.second;
   std::vector<O4Args> boxes;

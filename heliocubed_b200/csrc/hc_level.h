@@ -222,7 +222,8 @@ struct O4Args {
   double* WP;   // [nbox][8][G]
   double* th;   // [nbox][G]
   double* thr;  // [nbox][G] raw detector flag
-  double* face; // [nbox][kO4FaceArrays][F]
+  double* face; // [nbox][kO4FaceArrays][F]: face arrays of directions 0 and 2
+  double* face2; // [nbox][kO4FaceArrays][F]: face arrays of direction 1 (its pass overlaps its neighbours')
   double* mj;   // [nbox][V+1]
   double* kp;   // [nbox][8][V+2]
 };

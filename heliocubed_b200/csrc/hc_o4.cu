@@ -99,6 +99,9 @@ Ctx makeCtx(const O4Args& a, int d) {
   Ctx c;
   c.a = a;
   c.d = d;
+  // direction 1 keeps its face arrays apart, so its pass can run beside the
+  // passes of directions 0 and 2
+  if (d == 1) c.a.face = a.face2;
   for (int q = 0; q < 3; ++q) { c.V.lo[q] = a.vlo[q]; c.V.hi[q] = a.vhi[q]; }
   c.G = c.V.grow(a.ghost);
   c.GR = c.G.grow(-1);
@@ -1339,7 +1342,7 @@ size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost)
   Box3 FB = G.grow(-3);
   for (int q = 0; q < 3; ++q) FB.hi[q] += 1;
   const size_t NG = (size_t)G.size(), NF = (size_t)FB.size(), N1 = (size_t)V.grow(1).size(), N2 = (size_t)V.grow(2).size();
-  return (size_t)nbox * (8 * NG + 8 * NG + NG + NG + (size_t)kO4FaceArrays * NF + N1 + 16 * N2);
+  return (size_t)nbox * (8 * NG + 8 * NG + NG + NG + 2 * (size_t)kO4FaceArrays * NF + N1 + 16 * N2);
 }
 
 // A batch: per box and direction the Ctx of a one-box O4Args, in device
@@ -1570,6 +1573,7 @@ void o4SplitArgs(const O4Args& a, std::vector<O4Args>& out) {
     o.th = a.th + (long)b * c.gr.N;
     o.thr = a.thr + (long)b * c.gr.N;
     o.face = a.face + (long)b * kO4FaceArrays * c.fr.N;
+    o.face2 = a.face2 + (long)b * kO4FaceArrays * c.fr.N;
     o.mj = a.mj + (long)b * c.v1r.N;
     o.kp = a.kp + (long)b * 16 * c.v2r.N;
   }
@@ -1656,7 +1660,15 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
     HC_LAUNCH(o4PowellAvgKernel, 0, RG_V1)
     st = s;
   }
+  // Direction d's face arrays are face buffer d & 1 (direction 1 has its
+  // own), so the passes overlap: the Roe point dissipation of d (second side
+  // stream) runs beside the face chain of d - 1 and the reconstruction of
+  // d + 1 on the main stream; the Powell face chain of d (first side stream)
+  // beside them.  The reconstruction of d + 2 reuses d's buffer and waits
+  // for d's Powell chain; d's face chain waits for d's Roe dissipation;
+  // the chains add into rhs in direction order on the main stream.
   for (int d = 0; d < 3; ++d) {
+    if (d >= 2 && B->powell && (e = cudaStreamWaitEvent(s, B->joinEv[d - 2], 0)) != cudaSuccess) return e;
     HC_LAUNCH_DM(o4FaceReconKernel, 0, RG_F)
     if (B->powell) {
       // the Powell chain reads the reconstruction's flags and normal B and
@@ -1678,11 +1690,15 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
       st = s;
       if ((e = cudaEventRecord(B->roeJoin[d], B->roeSide)) != cudaSuccess) return e;
     }
-    if (B->roe && (e = cudaStreamWaitEvent(s, B->roeJoin[d], 0)) != cudaSuccess) return e;
-    if ((e = launchChain(B, rg, d, s)) != cudaSuccess) return e;
-    // join before the next direction's reconstruction rewrites the flags
-    if (B->powell && (e = cudaStreamWaitEvent(s, B->joinEv[d], 0)) != cudaSuccess) return e;
+    if (d >= 1) {
+      if (B->roe && (e = cudaStreamWaitEvent(s, B->roeJoin[d - 1], 0)) != cudaSuccess) return e;
+      if ((e = launchChain(B, rg, d - 1, s)) != cudaSuccess) return e;
+    }
   }
+  if (B->roe && (e = cudaStreamWaitEvent(s, B->roeJoin[2], 0)) != cudaSuccess) return e;
+  if ((e = launchChain(B, rg, 2, s)) != cudaSuccess) return e;
+  for (int d = 0; d < 3 && B->powell; ++d)
+    if ((e = cudaStreamWaitEvent(s, B->joinEv[d], 0)) != cudaSuccess) return e;
   // after the last join: -J div B complete, coefficients averaged
   if (B->powell) { HC_LAUNCH(o4PowellApplyKernel, 0, RG_V) }
 #undef HC_LAUNCH_DV

@@ -367,13 +367,15 @@ def synthetic_requests(n: int, seed: int, rate_hz: float | None, steps: int,
     """Seeded requests: grid from `radial` x `angular`^2, scheme 50/50 from
     `orders`, cone speed U[500, 2000] km/s, half-width U[20, 60] deg,
     lat/lon U[-30, 30] deg, density ratio U[2, 6]; Poisson arrivals at
-    `rate_hz` (all at t = 0 when None)."""
+    `rate_hz` (all at t = 0 when None).  The arrival times come from their
+    own stream, so the requests themselves do not depend on the rate."""
     rng = np.random.default_rng(seed)
+    arrivals = np.random.default_rng([seed, 1])
     t = 0.0
     out = []
     for rid in range(n):
         if rate_hz:
-            t += rng.exponential(1.0 / rate_hz)
+            t += arrivals.exponential(1.0 / rate_hz)
         cone = Cone(speed_kms=rng.uniform(500, 2000), half_width_deg=rng.uniform(20, 60),
                     lat_deg=rng.uniform(-30, 30), lon_deg=rng.uniform(-30, 30), density_ratio=rng.uniform(2, 6))
         out.append(Request(rid, int(rng.choice(radial)), int(rng.choice(angular)), int(rng.choice(orders)), steps,

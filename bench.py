@@ -584,7 +584,7 @@ def run_serve(args, world, rank, local):
     server = serve.EnsembleServer(hbm_budget=args.serve_budget_gb * 1e9, max_inflight=args.serve_inflight,
                                   chunk=chunk, device=local, keep_states=False)
     for shp in shapes:
-        server.warm([r for r in reqs if (r.nr, r.na, r.order) == shp], per_shape=min(counts[shp], 2))
+        server.warm([r for r in reqs if (r.nr, r.na, r.order) == shp], per_shape=min(counts[shp], 3))
     torch.cuda.synchronize()
 
     # host-staged copies of the requests (pinned initial states) for e2e
@@ -649,7 +649,7 @@ def run_serve(args, world, rank, local):
                       "arrivals": "seeded Poisson, rate %.3f /s (%d in flight at the plain path's mean service "
                                   "time %.3f s)" % (rate, args.serve_inflight, service_s),
                       "max_inflight": args.serve_inflight, "hbm_budget_gb": args.serve_budget_gb,
-                      "chunk_steps": chunk, "slots_per_shape": "min(requests of the shape, 2), built before timing",
+                      "chunk_steps": chunk, "slots_per_shape": "min(requests of the shape, 3), built before timing",
                       "l2": "working set of the in-flight solves larger than L2",
                       "parallelism": f"replicas x{world}"},
            "batched": sb, "plain": sp,

@@ -580,12 +580,13 @@ int buildO4Geometry(hc_ctx* c) {
   g.roe = P.riemann_solver == 2; g.powell = P.divergence_cleaning == 1; g.fallback = P.berta_fallback_type;
   // the CME insertion window's Rusanov flag (0 until a schedule sets it)
   {
-    cudaError_t ferr = cudaMalloc(&c->rusanovFlag, sizeof(int));
-    if (ferr == cudaSuccess) ferr = cudaMemset(c->rusanovFlag, 0, sizeof(int));
+    cudaError_t ferr = cudaMalloc(&c->rusanovFlag, 2 * sizeof(int));
+    if (ferr == cudaSuccess) ferr = cudaMemset(c->rusanovFlag, 0, 2 * sizeof(int));
     if (ferr != cudaSuccess) return cudaFail(ferr, "O4 flag");
     c->owned.push_back(c->rusanovFlag);
   }
   g.rusanov = c->rusanovFlag;
+  g.status = c->rusanovFlag + 1;
   if (err != cudaSuccess) return cudaFail(err, "O4 geometry upload");
   return HC_OK;
 }
@@ -761,24 +762,7 @@ int buildO4Level(hc_ctx* c) {
 }
 
 // Carve the operator scratch of nbox boxes (valid box [vlo, vhi]) from sp.
-void carveO4Scratch(O4Args& a, double* sp) {
-  long ng = 1, nf = 1, n1 = 1;
-  for (int d = 0; d < 3; ++d) {
-    const int ext = a.vhi[d] - a.vlo[d] + 1;
-    ng *= ext + 2 * kO4Ghost;
-    nf *= ext + 2 * kO4Ghost - 6 + 1;
-    n1 *= ext + 2;
-  }
-  const long nb = a.nbox;
-  a.WA = sp; sp += nb * 8 * ng;
-  a.WP = sp; sp += nb * 8 * ng;
-  a.th = sp; sp += nb * ng;
-  a.thr = sp; sp += nb * ng;
-  a.face = sp; sp += nb * (long)kO4FaceArrays * nf;
-  a.face2 = sp; sp += nb * (long)kO4FaceArrays * nf;
-  a.mj = sp; sp += nb * n1;
-  a.kp = sp;
-}
+void carveO4Scratch(O4Args& a, double* sp) { o4CarveScratch(a, sp); }
 
 int allocWorkspace(hc_ctx* c) {
   const size_t nv = 6 * NC * (size_t)c->L.Nv, ng = 6 * NC * (size_t)c->L.Ng;

@@ -194,6 +194,8 @@ struct O4Geo {
   double gamma, invGm1, entropy, eta_d, dx[3];
   int roe, powell, fallback;
   const int* rusanov;     // device flag (may be null): nonzero runs a Roe context with Rusanov dissipation
+  int* status;            // device word (may be null): set to 1 when a kernel's bounded wait for a
+                          // shared-memory tile gave up (that tile's rhs is then NaN)
 };
 
 // A box region: low corner, extents, cell count.
@@ -230,6 +232,10 @@ struct O4Args {
 constexpr int kO4FaceArrays = 8 * 4 + 5;  // WL, WR, FS, QD/DP (8 each) + thF, PS, BP, Bflux, Bprod
 
 size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost);
+// Carve the operator scratch of a.nbox boxes with the valid box a.vlo..vhi
+// from sp (every array starts on a 256-byte boundary when sp does);
+// returns the doubles used (o4ScratchDoubles).
+size_t o4CarveScratch(O4Args& a, double* sp);
 
 // Seam flux register of the level step (reg null: off): the final face flux
 // of panel-boundary faces of directions 1, 2 of whole-panel boxes is added

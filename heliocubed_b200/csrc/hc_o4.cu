@@ -11,9 +11,12 @@
 // final flux and divergence with its intermediates in shared memory; the
 // Powell terms on a side stream.  Every intermediate covers the box the
 // reference computes it on.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <math_constants.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <vector>
 
 #include "hc_device.cuh"
@@ -95,6 +98,17 @@ inline long chunkPoints(long total) {
   return c < 128 ? 128 : c > 1024 ? 1024 : c;
 }
 
+// The box the face arrays of every direction are laid out on: the face
+// boxes G.extrude(d).grow(-3) together, its radial extent rounded up to an
+// even count so that a radial row of doubles spans a multiple of 16 bytes
+// (the strides a TMA tensor map accepts).
+Box3 faceBox(const Box3& G) {
+  Box3 FB = G.grow(-3);
+  for (int q = 0; q < 3; ++q) FB.hi[q] += 1;
+  if (FB.n(0) & 1) FB.hi[0] += 1;
+  return FB;
+}
+
 Ctx makeCtx(const O4Args& a, int d) {
   Ctx c;
   c.a = a;
@@ -114,9 +128,7 @@ Ctx makeCtx(const O4Args& a, int d) {
   c.V2 = c.V.grow(2);
   c.gr = regOf(c.G);
   // face scratch is laid out on the largest face box over the directions
-  Box3 FB = c.G.grow(-3);
-  for (int q = 0; q < 3; ++q) FB.hi[q] += 1;
-  c.fr = regOf(FB);
+  c.fr = regOf(faceBox(c.G));
   c.v1r = regOf(c.V1);
   c.v2r = regOf(c.V2);
   c.vr = regOf(c.V);
@@ -900,9 +912,28 @@ __device__ __forceinline__ void chainPt(int i, int n, int t, int p[3]) {
 // the reference's face pass).  dT3[q]: centred difference of the radial
 // pressure product along transverse q (unused where the separable metrics
 // skip it).
+// The point Roe dissipations a final face averages: component stride and
+// the offsets of the face and its four transverse neighbours (lower and
+// upper along t1, then along t2), in the face scratch or in a shared tile.
+struct QdTaps {
+  const double* p;
+  long stride;
+  long o[5];
+};
+
+__device__ __forceinline__ QdTaps scratchTaps(const Ctx& c, int d, int i, int j, int k) {
+  const View QD = faceView(c, 0, F_QD);
+  const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+  int m1[3] = {i, j, k}, p1[3] = {i, j, k}, m2[3] = {i, j, k}, p2[3] = {i, j, k};
+  m1[t1] -= 1; p1[t1] += 1; m2[t2] -= 1; p2[t2] += 1;
+  return QdTaps{QD.p, QD.r.N,
+                {roff(QD.r, i, j, k), roff(QD.r, m1[0], m1[1], m1[2]), roff(QD.r, p1[0], p1[1], p1[2]),
+                 roff(QD.r, m2[0], m2[1], m2[2]), roff(QD.r, p2[0], p2[1], p2[2])}};
+}
+
 template <int D>
 __device__ __forceinline__ void chainFinal(const Ctx& c, int i, int j, int k, double fs[8], const double t3,
-                                           const double dT3[2], double fx[8]) {
+                                           const double dT3[2], const QdTaps& tap, double fx[8]) {
   const O4Args& a = c.a;
   constexpr int d = D;
   const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
@@ -941,15 +972,11 @@ __device__ __forceinline__ void chainFinal(const Ctx& c, int i, int j, int k, do
 #pragma unroll
       for (int e = 0; e < 10; ++e) dM[q][e] = 0.5 * Ma[e] - 0.5 * Mb[e];
     }
-    int m1[3] = {i, j, k}, p1[3] = {i, j, k}, m2[3] = {i, j, k}, p2[3] = {i, j, k};
-    m1[t1] -= 1; p1[t1] += 1; m2[t2] -= 1; p2[t2] += 1;
-    const long o0 = roff(QD.r, i, j, k), oa1 = roff(QD.r, m1[0], m1[1], m1[2]), ob1 = roff(QD.r, p1[0], p1[1], p1[2]);
-    const long oa2 = roff(QD.r, m2[0], m2[1], m2[2]), ob2 = roff(QD.r, p2[0], p2[1], p2[2]);
     double avg[8], dP0[8], dP1[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const double* Q = QD.p + q * QD.r.N;
-      const double pt = Q[o0], a1 = Q[oa1], b1 = Q[ob1], a2 = Q[oa2], b2 = Q[ob2];
+      const double* Q = tap.p + q * tap.stride;
+      const double pt = Q[tap.o[0]], a1 = Q[tap.o[1]], b1 = Q[tap.o[2]], a2 = Q[tap.o[3]], b2 = Q[tap.o[4]];
       const double lap = (a1 + b1) + (a2 + b2) - 4.0 * pt;
       avg[q] = sm ? pt + lap * (1.0 / 24.0) : pt;
       dP0[q] = 0.5 * b1 - 0.5 * a1;
@@ -1059,17 +1086,80 @@ __device__ __forceinline__ void chainAverage(const Ctx& c, int d, int i, int j, 
   pa = sm ? pp + lapFace(PS, 0, d, i, j, k) * (1.0 / 24.0) : pp;
 }
 
-// Directions 1, 2: walk the normal direction.
-template <int D, int TI, int MB>
+// Directions 1, 2: walk the normal direction.  With TMA, the slab's flux
+// sums, flags and total pressures (tile plus a two-face ring) and its point
+// Roe dissipations (tile plus a one-face ring) are copied into shared
+// memory by the tensor-memory accelerator, the next slab's copies issued as
+// soon as the current slab's are consumed, so they overlap the mapped-flux
+// and final-flux stages; without it (tensor maps unavailable) the same
+// stages read the face scratch through L1.
+template <int TI>
+struct ChainShape {
+  static constexpr int TT = 128 / TI, NI = TI + 2, NT = TT + 2;  // averages: tile plus a one-face ring
+  static constexpr int NX = TI + 4, NY = TT + 4, NXY = NX * NY;  // TMA tiles: tile plus a two-face ring
+  static constexpr int round16(int n) { return (n + 15) / 16 * 16; }
+  static constexpr int oFA = 0, oPA = oFA + round16(8 * NI * NT), oFM = oPA + round16(NI * NT),
+                       oT3 = oFM + round16(8 * NI * TT), oIn = oT3 + round16(TI * NT),
+                       oQD = oIn + round16(10 * NXY), oBar = oQD + round16(8 * NXY);
+  static constexpr int doubles(bool tma) { return tma ? oBar + 2 : oIn; }
+};
+
+__device__ __forceinline__ unsigned smemAddr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbarInit(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbarExpect(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
+}
+
+// Bounded wait for phase `parity` of an mbarrier: false when it has not
+// completed after kMbarPolls polls (each poll blocks for a short,
+// implementation-defined time), so a copy that never lands cannot hang the
+// GPU.
+constexpr int kMbarPolls = 1 << 22;
+__device__ __forceinline__ bool mbarWait(unsigned long long* bar, unsigned parity) {
+  const unsigned addr = smemAddr(bar);
+  for (int it = 0; it < kMbarPolls; ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// One tiled TMA copy of a 4-D box (radial, j, k, array) of the face scratch
+// into shared memory, completing on `bar`.
+__device__ __forceinline__ void tmaLoad(double* dst, const CUtensorMap* map, int x, int y, int z, int w,
+                                        unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smemAddr(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smemAddr(bar))
+      : "memory");
+}
+
+template <int D, int TI, int MB, bool TMA>
 __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restrict__ tab, const RegArgs rg,
-                                                             const ChainTile* __restrict__ tiles) {
+                                                             const ChainTile* __restrict__ tiles,
+                                                             const CUtensorMap* __restrict__ maps) {
   static_assert(D == 1 || D == 2, "angular directions");
-  constexpr int TT = 128 / TI, NI = TI + 2, NT = TT + 2;
+  using S = ChainShape<TI>;
+  constexpr int TT = S::TT, NI = S::NI, NT = S::NT, NX = S::NX, NXY = S::NXY;
   constexpr int tdim = D == 1 ? 2 : 1;
-  __shared__ double sFA[8][NI * NT];
-  __shared__ double sPA[NI * NT];
-  __shared__ double sFM[8][NI * TT];
-  __shared__ double sT3[TI * NT];
+  extern __shared__ __align__(128) double smem[];
+  double* sFA = smem + S::oFA;  // [8][NI * NT]
+  double* sPA = smem + S::oPA;  // [NI * NT]
+  double* sFM = smem + S::oFM;  // [8][NI * TT]
+  double* sT3 = smem + S::oT3;  // [TI * NT]
+  double* sIn = smem + S::oIn;  // TMA: [FS 8, thF, PS][NY][NX]
+  double* sQD = smem + S::oQD;  // TMA: [8][NY][NX]
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + S::oBar);
   const ChainTile tl = tiles[blockIdx.x];
   const Ctx& c = tab[tl.box * 3 + D];
   const O4Args& a = c.a;
@@ -1085,20 +1175,72 @@ __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restri
   for (int q = 0; q < 8; ++q) fxPrev[q] = 0.0;
   const int nEnd = tl.c1 + 1;
   const bool lastSegment = tl.c1 == c.V.hi[D];
-  for (int n = tl.c0; n <= nEnd; ++n) {
+  // TMA tiles: radial from i0 - 2 (an even offset from the face box's low
+  // corner: tiles start at the valid box's low radial index and TI is even),
+  // angular from a0 - 2, one face slab; map 0 copies 8 arrays, map 1 two
+  const CUtensorMap* map8 = TMA ? maps + ((long)tl.box * 2 + (D - 1)) * 2 : nullptr;
+  const CUtensorMap* map2 = TMA ? map8 + 1 : nullptr;
+  const int tx = tl.i0 - 2 - c.fr.lo[0], ta = tl.a0 - 2 - c.fr.lo[tdim], tnLo = c.fr.lo[D];
+  auto issue = [&](int n, bool inputs) {
+    const int y = D == 1 ? n - tnLo : ta, z = D == 1 ? ta : n - tnLo;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (inputs) {
+      mbarExpect(&bar[0], 10u * NXY * sizeof(double));
+      tmaLoad(sIn, map8, tx, y, z, F_FS, &bar[0]);
+      tmaLoad(sIn + 8 * NXY, map2, tx, y, z, F_THF, &bar[0]);
+    } else {
+      mbarExpect(&bar[1], 8u * NXY * sizeof(double));
+      tmaLoad(sQD, map8, tx, y, z, F_QD, &bar[1]);
+    }
+  };
+  bool failed = false;
+  if (TMA) {
+    if (tid == 0) {
+      mbarInit(&bar[0]);
+      mbarInit(&bar[1]);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+      issue(tl.c0, true);
+      issue(tl.c0, false);
+    }
+  }
+  for (int n = tl.c0; n <= nEnd && !failed; ++n) {
+    const unsigned parity = (unsigned)(n - tl.c0) & 1u;
+    if (TMA) {
+      failed = __syncthreads_or(!mbarWait(&bar[0], parity));
+      if (failed) break;
+    }
     // (5) averages on radial i0-1 .. i0+TI x angular a0-1 .. a0+TT of face slab n
     for (int q = tid; q < NI * NT; q += 128) {
       const int ii = tl.i0 - 1 + q % NI, tt = tl.a0 - 1 + q / NI;
       if (ii < ilo || ii > ihi || tt < tlo || tt > thi) continue;
-      int p[3];
-      chainPt<D>(ii, n, tt, p);
       double fa[8], pa;
-      chainAverage(c, D, p[0], p[1], p[2], fa, pa);
+      if (TMA) {
+        // (ii, tt) in the TMA tile; lapFace's order: radial pair, angular pair
+        const int x = q % NI + 1, y = q / NI + 1, o = y * NX + x;
+        const bool sm = sIn[8 * NXY + o] > 0.5;
 #pragma unroll
-      for (int e = 0; e < 8; ++e) sFA[e][q] = fa[e];
+        for (int e = 0; e < 8; ++e) {
+          const double* F = sIn + e * NXY;
+          const double pt = F[o];
+          fa[e] = sm ? pt + ((F[o - 1] + F[o + 1]) + (F[o - NX] + F[o + NX]) - 4.0 * pt) * (1.0 / 24.0) : pt;
+        }
+        const double* P = sIn + 9 * NXY;
+        const double pp = P[o];
+        pa = sm ? pp + ((P[o - 1] + P[o + 1]) + (P[o - NX] + P[o + NX]) - 4.0 * pp) * (1.0 / 24.0) : pp;
+      } else {
+        int p[3];
+        chainPt<D>(ii, n, tt, p);
+        chainAverage(c, D, p[0], p[1], p[2], fa, pa);
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e) sFA[e * NI * NT + q] = fa[e];
       sPA[q] = pa;
     }
     __syncthreads();
+    if (TMA && tid == 0 && n < nEnd) issue(n + 1, true);  // the inputs' tile is free again
     // (6) mapped flux on radial i0-1 .. i0+TI x angular a0 .. a0+TT-1; the
     // radial transverse derivative of the angular metrics vanishes (skipped)
     for (int q = tid; q < NI * TT; q += 128) {
@@ -1119,8 +1261,8 @@ __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restri
       double fa[8], dF[8];
 #pragma unroll
       for (int e = 0; e < 8; ++e) {
-        fa[e] = sFA[e][qc];
-        dF[e] = 0.5 * sFA[e][qu] - 0.5 * sFA[e][qd];
+        fa[e] = sFA[e * NI * NT + qc];
+        dF[e] = 0.5 * sFA[e * NI * NT + qu] - 0.5 * sFA[e * NI * NT + qd];
       }
       double out[8];
 #pragma unroll
@@ -1148,7 +1290,7 @@ __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restri
         }
       }
 #pragma unroll
-      for (int e = 0; e < 8; ++e) sFM[e][q] = out[e];
+      for (int e = 0; e < 8; ++e) sFM[e * NI * TT + q] = out[e];
     }
     // (7) radial product of <p_tot> on radial i0 .. i0+TI-1 x angular a0-1 .. a0+TT
     for (int q = tid; q < TI * NT; q += 128) {
@@ -1161,7 +1303,12 @@ __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restri
       value += sPA[qc] * si * 1.0;
       sT3[q] = value;
     }
-    __syncthreads();
+    if (TMA) {
+      failed = __syncthreads_or(!mbarWait(&bar[1], parity));
+      if (failed) break;
+    } else {
+      __syncthreads();
+    }
     // (7, 8, 9) this thread's face: radial product of the mapped flux, final
     // flux, divergence of the cell below it
     if (mine) {
@@ -1172,14 +1319,21 @@ __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restri
 #pragma unroll
       for (int e = 0; e < 8; ++e) {
         double value = 0.0;
-        value += (0.5 * sFM[e][qm + 1] - 0.5 * sFM[e][qm - 1]) * ds * (1.0 / 12.0);
-        value += sFM[e][qm] * s * 1.0;
+        value += (0.5 * sFM[e * NI * TT + qm + 1] - 0.5 * sFM[e * NI * TT + qm - 1]) * ds * (1.0 / 12.0);
+        value += sFM[e * NI * TT + qm] * s * 1.0;
         fs[e] = value;
       }
       const int q3 = (lt + 1) * TI + li;  // (i, t) in the pressure-product frame
       const double dT3[2] = {0.0, 0.5 * sT3[q3 + TI] - 0.5 * sT3[q3 - TI]};
+      QdTaps tap;
+      if (TMA) {
+        const int o = (lt + 2) * NX + (li + 2);  // (i, t) in the TMA tile
+        tap = QdTaps{sQD, NXY, {o, o - 1, o + 1, o - NX, o + NX}};
+      } else {
+        tap = scratchTaps(c, D, p[0], p[1], p[2]);
+      }
       double fx[8];
-      chainFinal<D>(c, p[0], p[1], p[2], fs, sT3[q3], dT3, fx);
+      chainFinal<D>(c, p[0], p[1], p[2], fs, sT3[q3], dT3, tap, fx);
       if (n <= tl.c1 || lastSegment) chainStore<D>(c, rg, p[0], p[1], p[2], fx);
       if (n > tl.c0) {
         int pc[3];
@@ -1195,6 +1349,26 @@ __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restri
       for (int e = 0; e < 8; ++e) fxPrev[e] = fx[e];
     }
     __syncthreads();
+    if (TMA && tid == 0 && n < nEnd) issue(n + 1, false);  // the dissipations' tile is free again
+  }
+  if (TMA && failed) {
+    // A copy did not land: report it, wait (bounded) for the copies still in
+    // flight, and make this tile's cells visibly invalid.
+    if (tid == 0) {
+      if (a.G.status) atomicExch(a.G.status, 1);
+      mbarWait(&bar[0], 0u);
+      mbarWait(&bar[1], 0u);
+      mbarWait(&bar[0], 1u);
+      mbarWait(&bar[1], 1u);
+    }
+    __syncthreads();
+    if (mine)
+      for (int n = tl.c0; n <= tl.c1; ++n) {
+        int pc[3];
+        chainPt<D>(i, n, t, pc);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) a.rhs[roff(c.vr, pc[0], pc[1], pc[2]) + e * c.vr.N] = CUDART_NAN;
+      }
   }
 }
 
@@ -1209,7 +1383,7 @@ template <int TI, int MB>
 __global__ void __launch_bounds__(128, MB) o4FaceChain0Kernel(const Ctx* __restrict__ tab, const RegArgs rg,
                                                               const ChainTile* __restrict__ tiles) {
   constexpr int TT = 128 / TI, NI = TI + 1, NJ = TT + 2, NS = NI * NJ;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(128) double smem[];
   double* sFA = smem;              // [3][8][NS]
   double* sPA = sFA + 3 * 8 * NS;  // [3][NS]
   double* sFX = sPA + 3 * NS;      // [8][NI * TT]
@@ -1310,7 +1484,7 @@ __global__ void __launch_bounds__(128, MB) o4FaceChain0Kernel(const Ctx* __restr
       };
       const double dT3[2] = {0.5 * t3(P0[qc + NI]) - 0.5 * t3(P0[qc - NI]), 0.5 * t3(Pp[qc]) - 0.5 * t3(Pm[qc])};
       double fx[8];
-      chainFinal<0>(c, ii, jj, k, fs, t3(P0[qc]), dT3, fx);
+      chainFinal<0>(c, ii, jj, k, fs, t3(P0[qc]), dT3, scratchTaps(c, 0, ii, jj, k), fx);
       chainStore<0>(c, rg, ii, jj, k, fx);
 #pragma unroll
       for (int e = 0; e < 8; ++e) sFX[e * NI * TT + q] = fx[e];
@@ -1335,14 +1509,34 @@ __global__ void __launch_bounds__(128, MB) o4FaceChain0Kernel(const Ctx* __restr
 
 }  // namespace
 
-size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost) {
+size_t o4CarveScratch(O4Args& a, double* sp) {
   Box3 V;
-  for (int q = 0; q < 3; ++q) { V.lo[q] = vlo[q]; V.hi[q] = vhi[q]; }
-  const Box3 G = V.grow(ghost);
-  Box3 FB = G.grow(-3);
-  for (int q = 0; q < 3; ++q) FB.hi[q] += 1;
-  const size_t NG = (size_t)G.size(), NF = (size_t)FB.size(), N1 = (size_t)V.grow(1).size(), N2 = (size_t)V.grow(2).size();
-  return (size_t)nbox * (8 * NG + 8 * NG + NG + NG + 2 * (size_t)kO4FaceArrays * NF + N1 + 16 * N2);
+  for (int q = 0; q < 3; ++q) { V.lo[q] = a.vlo[q]; V.hi[q] = a.vhi[q]; }
+  const Box3 G = V.grow(a.ghost);
+  const size_t NG = (size_t)G.size(), NF = (size_t)faceBox(G).size(), N1 = (size_t)V.grow(1).size(),
+               N2 = (size_t)V.grow(2).size(), nb = (size_t)a.nbox;
+  size_t off = 0;
+  auto take = [&](double*& dst, size_t n) {
+    if (sp) dst = sp + off;
+    off += (n + 31) / 32 * 32;  // 256-byte boundaries (TMA wants 16)
+  };
+  take(a.WA, nb * 8 * NG);
+  take(a.WP, nb * 8 * NG);
+  take(a.th, nb * NG);
+  take(a.thr, nb * NG);
+  take(a.face, nb * kO4FaceArrays * NF);
+  take(a.face2, nb * kO4FaceArrays * NF);
+  take(a.mj, nb * N1);
+  take(a.kp, nb * 16 * N2);
+  return off;
+}
+
+size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost) {
+  O4Args a{};
+  a.nbox = nbox;
+  a.ghost = ghost;
+  for (int q = 0; q < 3; ++q) { a.vlo[q] = vlo[q]; a.vhi[q] = vhi[q]; }
+  return o4CarveScratch(a, nullptr);
 }
 
 // A batch: per box and direction the Ctx of a one-box O4Args, in device
@@ -1364,6 +1558,10 @@ struct O4Batch {
   long chainOff[3] = {};
   int chainCount[3] = {};
   int chainTI = 32;
+  // TMA tensor maps of the angular chains' face slabs, per box and direction
+  // 1, 2: one copying 8 arrays, one copying 2 (device array; null without TMA)
+  CUtensorMap* maps = nullptr;
+  bool chainTma = false;
   // The Powell face chain of a direction (face flux, radial product,
   // divergence into -J div B) runs on a side stream beside the main face
   // chain: fork after the reconstruction, join before the next direction.
@@ -1407,6 +1605,68 @@ void chainTiles(const std::vector<Ctx>& host, int nbox, int d, int TI, std::vect
         for (int i0 = V.lo[0]; i0 <= V.hi[0]; i0 += TI)
           out.push_back(ChainTile{b, i0, a0, c0, std::min(c0 + S - 1, V.hi[walk])});
   }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library), or null where it is unavailable.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encodeTiled() {
+  static EncodeTiledFn fn = []() -> EncodeTiledFn {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// The tensor maps of the angular face chains of every box of a batch:
+// 4-D (radial, j, k, array) views of each box's face buffer for direction
+// d = 1, 2, boxes of (TI + 4) radial x (TT + 4) angular x 1 normal x 8 or 2
+// arrays.  False where a map cannot be made (then the chains read through
+// L1 instead).
+bool chainMaps(const std::vector<Ctx>& host, int nbox, int TI, std::vector<CUtensorMap>& out) {
+  const EncodeTiledFn enc = encodeTiled();
+  if (!enc) return false;
+  const int TT = 128 / TI;
+  out.resize((size_t)nbox * 4);
+  for (int b = 0; b < nbox; ++b)
+    for (int d = 1; d <= 2; ++d) {
+      const Ctx& c = host[(size_t)b * 3 + d];
+      const cuuint64_t n0 = c.fr.n[0], n1 = c.fr.n[1], n2 = c.fr.n[2];
+      // 16-byte aligned base and rows, and an even radial tile origin
+      // (tiles start at the valid box's low radial index, i0 - 2 - fr.lo)
+      if ((reinterpret_cast<uintptr_t>(c.a.face) & 15) || (n0 & 1) || ((c.V.lo[0] - 2 - c.fr.lo[0]) & 1)) return false;
+      const cuuint64_t dims[4] = {n0, n1, n2, (cuuint64_t)kO4FaceArrays};
+      const cuuint64_t strides[3] = {n0 * 8, n0 * n1 * 8, n0 * n1 * n2 * 8};
+      for (int w = 0; w < 2; ++w) {
+        const cuuint32_t box[4] = {(cuuint32_t)(TI + 4), d == 1 ? 1u : (cuuint32_t)(TT + 4),
+                                   d == 1 ? (cuuint32_t)(TT + 4) : 1u, w == 0 ? 8u : 2u};
+        const cuuint32_t es[4] = {1, 1, 1, 1};
+        if (enc(&out[((size_t)b * 2 + (d - 1)) * 2 + w], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, c.a.face, dims, strides,
+                box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+          return false;
+      }
+    }
+  return true;
+}
+
+// Dynamic shared memory of the angular chain kernels (with and without TMA).
+template <int TI, bool TMA>
+cudaError_t chainSmemT() {
+  const int bytes = ChainShape<TI>::doubles(TMA) * (int)sizeof(double);
+  cudaError_t e = cudaSuccess;
+#define HC_CHAIN_ATTR(D, MB)                                                                                \
+  if (e == cudaSuccess)                                                                                    \
+    e = cudaFuncSetAttribute(o4FaceChainKernel<D, TI, MB, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  HC_CHAIN_ATTR(1, 3) HC_CHAIN_ATTR(1, 4) HC_CHAIN_ATTR(1, 5) HC_CHAIN_ATTR(2, 3) HC_CHAIN_ATTR(2, 4) HC_CHAIN_ATTR(2, 5)
+#undef HC_CHAIN_ATTR
+  return e;
 }
 
 template <int TI>
@@ -1508,6 +1768,23 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
     B->chainCount[d] = (int)count;
   }
   *err = B->chainTI == 32 ? chain0Smem<32>() : B->chainTI == 16 ? chain0Smem<16>() : chain0Smem<8>();
+  if (*err == cudaSuccess)
+    *err = B->chainTI == 32   ? chainSmemT<32, false>()
+           : B->chainTI == 16 ? chainSmemT<16, false>()
+                              : chainSmemT<8, false>();
+  {
+    std::vector<CUtensorMap> maps;
+    if (*err == cudaSuccess && chainMaps(B->host, nbox, B->chainTI, maps)) {
+      cudaError_t e = B->chainTI == 32   ? chainSmemT<32, true>()
+                      : B->chainTI == 16 ? chainSmemT<16, true>()
+                                         : chainSmemT<8, true>();
+      if (e == cudaSuccess) e = cudaMalloc(&B->maps, sizeof(CUtensorMap) * maps.size());
+      if (e == cudaSuccess)
+        e = cudaMemcpy(B->maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice);
+      B->chainTma = e == cudaSuccess;
+      if (e != cudaSuccess) cudaGetLastError();  // no TMA: the chains read through L1
+    }
+  }
   if (*err == cudaSuccess) *err = cudaMalloc(&B->chainTiles, sizeof(ChainTile) * std::max<size_t>(1, tiles.size()));
   if (*err == cudaSuccess && !tiles.empty())
     *err = cudaMemcpy(B->chainTiles, tiles.data(), sizeof(ChainTile) * tiles.size(), cudaMemcpyHostToDevice);
@@ -1545,6 +1822,7 @@ void o4BatchDestroy(O4Batch* B) {
   if (B->dev) cudaFree(B->dev);
   if (B->chunks) cudaFree(B->chunks);
   if (B->chainTiles) cudaFree(B->chainTiles);
+  if (B->maps) cudaFree(B->maps);
   if (B->pointEv) cudaEventDestroy(B->pointEv);
   for (int d = 0; d < 3; ++d) {
     if (B->roeFork[d]) cudaEventDestroy(B->roeFork[d]);
@@ -1595,12 +1873,18 @@ cudaError_t launchChainT(const O4Batch* B, const RegArgs& rg, int d, cudaStream_
   const int n = B->chainCount[d];
   const ChainTile* t = B->chainTiles + B->chainOff[d];
   if (n == 0) return cudaSuccess;
+  const size_t smemTma = ChainShape<TI>::doubles(true) * sizeof(double);
+  const size_t smemL1 = ChainShape<TI>::doubles(false) * sizeof(double);
   if (d == 0)
     o4FaceChain0Kernel<TI, MB><<<n, 128, chain0Doubles<TI>() * sizeof(double), s>>>(B->dev, rg, t);
+  else if (d == 1 && B->chainTma)
+    o4FaceChainKernel<1, TI, MB, true><<<n, 128, smemTma, s>>>(B->dev, rg, t, B->maps);
   else if (d == 1)
-    o4FaceChainKernel<1, TI, MB><<<n, 128, 0, s>>>(B->dev, rg, t);
+    o4FaceChainKernel<1, TI, MB, false><<<n, 128, smemL1, s>>>(B->dev, rg, t, nullptr);
+  else if (B->chainTma)
+    o4FaceChainKernel<2, TI, MB, true><<<n, 128, smemTma, s>>>(B->dev, rg, t, B->maps);
   else
-    o4FaceChainKernel<2, TI, MB><<<n, 128, 0, s>>>(B->dev, rg, t);
+    o4FaceChainKernel<2, TI, MB, false><<<n, 128, smemL1, s>>>(B->dev, rg, t, nullptr);
   return cudaGetLastError();
 }
 

@@ -1096,6 +1096,7 @@ __device__ __forceinline__ void chainAverage(const Ctx& c, int d, int i, int j, 
 template <int TI>
 struct ChainShape {
   static constexpr int TT = 128 / TI, NI = TI + 2, NT = TT + 2;  // averages: tile plus a one-face ring
+  static constexpr int NTH = NI * TT;  // threads: one per mapped-flux point (the tile's faces and a radial ring)
   static constexpr int NX = TI + 4, NY = TT + 4, NXY = NX * NY;  // TMA tiles: tile plus a two-face ring
   static constexpr int round16(int n) { return (n + 15) / 16 * 16; }
   static constexpr int oFA = 0, oPA = oFA + round16(8 * NI * NT), oFM = oPA + round16(NI * NT),
@@ -1145,7 +1146,8 @@ __device__ __forceinline__ void tmaLoad(double* dst, const CUtensorMap* map, int
 }
 
 template <int D, int TI, int MB, bool TMA>
-__global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restrict__ tab, const RegArgs rg,
+__global__ void __launch_bounds__(ChainShape<TI>::NTH, MB) o4FaceChainKernel(const Ctx* __restrict__ tab,
+                                                                            const RegArgs rg,
                                                              const ChainTile* __restrict__ tiles,
                                                              const CUtensorMap* __restrict__ maps) {
   static_assert(D == 1 || D == 2, "angular directions");
@@ -1163,9 +1165,11 @@ __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restri
   const ChainTile tl = tiles[blockIdx.x];
   const Ctx& c = tab[tl.box * 3 + D];
   const O4Args& a = c.a;
+  constexpr int NTH = S::NTH;
   const int tid = threadIdx.x, li = tid % TI, lt = tid / TI;
   const int i = tl.i0 + li, t = tl.a0 + lt;
-  const bool mine = i <= c.V.hi[0] && t <= c.V.hi[tdim];
+  // threads beyond the tile's TI x TT faces only help with the shared stages
+  const bool mine = tid < TI * TT && i <= c.V.hi[0] && t <= c.V.hi[tdim];
   // radial products: area at i and its centred difference
   const double s = adjDr(a.G, D, i), ds = 0.5 * adjDr(a.G, D, i + 1) - 0.5 * adjDr(a.G, D, i - 1);
   const double coef = -a.scale / a.G.dx[D];
@@ -1213,7 +1217,7 @@ __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restri
       if (failed) break;
     }
     // (5) averages on radial i0-1 .. i0+TI x angular a0-1 .. a0+TT of face slab n
-    for (int q = tid; q < NI * NT; q += 128) {
+    for (int q = tid; q < NI * NT; q += NTH) {
       const int ii = tl.i0 - 1 + q % NI, tt = tl.a0 - 1 + q / NI;
       if (ii < ilo || ii > ihi || tt < tlo || tt > thi) continue;
       double fa[8], pa;
@@ -1243,7 +1247,7 @@ __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restri
     if (TMA && tid == 0 && n < nEnd) issue(n + 1, true);  // the inputs' tile is free again
     // (6) mapped flux on radial i0-1 .. i0+TI x angular a0 .. a0+TT-1; the
     // radial transverse derivative of the angular metrics vanishes (skipped)
-    for (int q = tid; q < NI * TT; q += 128) {
+    for (int q = tid; q < NI * TT; q += NTH) {
       const int ii = tl.i0 - 1 + q % NI, tt = tl.a0 + q / NI;
       if (ii < ilo || ii > ihi || tt > c.V.hi[tdim]) continue;
       int p[3];
@@ -1293,7 +1297,7 @@ __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restri
       for (int e = 0; e < 8; ++e) sFM[e * NI * TT + q] = out[e];
     }
     // (7) radial product of <p_tot> on radial i0 .. i0+TI-1 x angular a0-1 .. a0+TT
-    for (int q = tid; q < TI * NT; q += 128) {
+    for (int q = tid; q < TI * NT; q += NTH) {
       const int ii = tl.i0 + q % TI, tt = tl.a0 - 1 + q / TI;
       if (ii > c.V.hi[0] || tt < tlo || tt > thi) continue;
       const double si = adjDr(a.G, D, ii), dsi = 0.5 * adjDr(a.G, D, ii + 1) - 0.5 * adjDr(a.G, D, ii - 1);
@@ -1375,14 +1379,21 @@ __global__ void __launch_bounds__(128, MB) o4FaceChainKernel(const Ctx* __restri
 // Direction 0: walk k; shared memory (dynamic): averages of three rows of k
 // [3][8][NS], pressure averages [3][NS], final fluxes [8][(TI + 1) TT].
 template <int TI>
-constexpr int chain0Doubles() {
+__host__ __device__ constexpr int chain0Doubles() {
   return 3 * 9 * (TI + 1) * (128 / TI + 2) + 8 * (TI + 1) * (128 / TI);
 }
 
+// Threads of the direction-0 chain: one per final face of a row of the tile.
+template <int TI>
+__host__ __device__ constexpr int chain0Threads() {
+  return (TI + 1) * (128 / TI);
+}
+
 template <int TI, int MB>
-__global__ void __launch_bounds__(128, MB) o4FaceChain0Kernel(const Ctx* __restrict__ tab, const RegArgs rg,
-                                                              const ChainTile* __restrict__ tiles) {
-  constexpr int TT = 128 / TI, NI = TI + 1, NJ = TT + 2, NS = NI * NJ;
+__global__ void __launch_bounds__(chain0Threads<TI>(), MB) o4FaceChain0Kernel(const Ctx* __restrict__ tab,
+                                                                              const RegArgs rg,
+                                                                              const ChainTile* __restrict__ tiles) {
+  constexpr int TT = 128 / TI, NI = TI + 1, NJ = TT + 2, NS = NI * NJ, NTH = chain0Threads<TI>();
   extern __shared__ __align__(128) double smem[];
   double* sFA = smem;              // [3][8][NS]
   double* sPA = sFA + 3 * 8 * NS;  // [3][NS]
@@ -1397,7 +1408,7 @@ __global__ void __launch_bounds__(128, MB) o4FaceChain0Kernel(const Ctx* __restr
   auto slab = [&](int k) {
     double* fa = sFA + slot(k) * 8 * NS;
     double* pa = sPA + slot(k) * NS;
-    for (int q = tid; q < NS; q += 128) {
+    for (int q = tid; q < NS; q += NTH) {
       const int ii = tl.i0 + q % NI, jj = tl.a0 - 1 + q / NI;
       if (ii > ihi || jj < jlo || jj > jhi) continue;
       double f[8], pp;
@@ -1419,7 +1430,7 @@ __global__ void __launch_bounds__(128, MB) o4FaceChain0Kernel(const Ctx* __restr
     const double* Pm = sPA + slot(k - 1) * NS;
     const double* Pp = sPA + slot(k + 1) * NS;
     // (6, 7, 8) faces i0 .. i0+TI x rows a0 .. a0+TT-1 of row k
-    for (int q = tid; q < NI * TT; q += 128) {
+    for (int q = tid; q < NI * TT; q += NTH) {
       const int ii = tl.i0 + q % NI, jj = tl.a0 + q / NI;
       if (ii > ihi || jj > c.V.hi[1]) continue;
       const int qc = q + NI;  // (ii, jj) in the slab frame
@@ -1494,7 +1505,7 @@ __global__ void __launch_bounds__(128, MB) o4FaceChain0Kernel(const Ctx* __restr
     {
       const int li = tid % TI, lj = tid / TI;
       const int i = tl.i0 + li, j = tl.a0 + lj;
-      if (i <= c.V.hi[0] && j <= c.V.hi[1]) {
+      if (tid < TI * TT && i <= c.V.hi[0] && j <= c.V.hi[1]) {
         const int q = lj * NI + li;
         double* R = a.rhs + roff(c.vr, i, j, k);
         double rv[8];
@@ -1579,9 +1590,10 @@ struct O4Batch {
 
 // Minimum resident CTAs per SM (the register cap) of each variant of the
 // tuned kernels: reconstruction, Roe point dissipation, fused face chain.
-// Variant 0 is the default.  The direction-0 chain's 51 KB of shared memory
-// (32-wide tiles) admits at most 4 CTAs per SM.
-constexpr int kO4MinBlocks[kO4TunedKernels][kO4Variants] = {{6, 4, 8}, {4, 3, 5}, {4, 3, 5}};
+// Variant 0 is the default.  A chain CTA has one thread per face of a tile
+// row (132-144 threads); its shared memory (51-66 KB at 32-wide tiles)
+// admits at most 4 (direction 0) or 3 (with TMA) CTAs per SM.
+constexpr int kO4MinBlocks[kO4TunedKernels][kO4Variants] = {{6, 4, 8}, {4, 3, 5}, {3, 4, 2}};
 
 // Tiles of the fused face chain of direction d over the batch's boxes: TI
 // radial x 128/TI across (d = 0: j; d != 0: the other angular index),
@@ -1664,7 +1676,7 @@ cudaError_t chainSmemT() {
 #define HC_CHAIN_ATTR(D, MB)                                                                                \
   if (e == cudaSuccess)                                                                                    \
     e = cudaFuncSetAttribute(o4FaceChainKernel<D, TI, MB, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  HC_CHAIN_ATTR(1, 3) HC_CHAIN_ATTR(1, 4) HC_CHAIN_ATTR(1, 5) HC_CHAIN_ATTR(2, 3) HC_CHAIN_ATTR(2, 4) HC_CHAIN_ATTR(2, 5)
+  HC_CHAIN_ATTR(1, 2) HC_CHAIN_ATTR(1, 3) HC_CHAIN_ATTR(1, 4) HC_CHAIN_ATTR(2, 2) HC_CHAIN_ATTR(2, 3) HC_CHAIN_ATTR(2, 4)
 #undef HC_CHAIN_ATTR
   return e;
 }
@@ -1672,11 +1684,11 @@ cudaError_t chainSmemT() {
 template <int TI>
 cudaError_t chain0Smem() {
   const int bytes = chain0Doubles<TI>() * (int)sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(o4FaceChain0Kernel<TI, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t e = cudaFuncSetAttribute(o4FaceChain0Kernel<TI, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(o4FaceChain0Kernel<TI, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(o4FaceChain0Kernel<TI, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(o4FaceChain0Kernel<TI, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   return e;
 }
 
@@ -1876,24 +1888,24 @@ cudaError_t launchChainT(const O4Batch* B, const RegArgs& rg, int d, cudaStream_
   const size_t smemTma = ChainShape<TI>::doubles(true) * sizeof(double);
   const size_t smemL1 = ChainShape<TI>::doubles(false) * sizeof(double);
   if (d == 0)
-    o4FaceChain0Kernel<TI, MB><<<n, 128, chain0Doubles<TI>() * sizeof(double), s>>>(B->dev, rg, t);
+    o4FaceChain0Kernel<TI, MB><<<n, chain0Threads<TI>(), chain0Doubles<TI>() * sizeof(double), s>>>(B->dev, rg, t);
   else if (d == 1 && B->chainTma)
-    o4FaceChainKernel<1, TI, MB, true><<<n, 128, smemTma, s>>>(B->dev, rg, t, B->maps);
+    o4FaceChainKernel<1, TI, MB, true><<<n, ChainShape<TI>::NTH, smemTma, s>>>(B->dev, rg, t, B->maps);
   else if (d == 1)
-    o4FaceChainKernel<1, TI, MB, false><<<n, 128, smemL1, s>>>(B->dev, rg, t, nullptr);
+    o4FaceChainKernel<1, TI, MB, false><<<n, ChainShape<TI>::NTH, smemL1, s>>>(B->dev, rg, t, nullptr);
   else if (B->chainTma)
-    o4FaceChainKernel<2, TI, MB, true><<<n, 128, smemTma, s>>>(B->dev, rg, t, B->maps);
+    o4FaceChainKernel<2, TI, MB, true><<<n, ChainShape<TI>::NTH, smemTma, s>>>(B->dev, rg, t, B->maps);
   else
-    o4FaceChainKernel<2, TI, MB, false><<<n, 128, smemL1, s>>>(B->dev, rg, t, nullptr);
+    o4FaceChainKernel<2, TI, MB, false><<<n, ChainShape<TI>::NTH, smemL1, s>>>(B->dev, rg, t, nullptr);
   return cudaGetLastError();
 }
 
 template <int TI>
 cudaError_t launchChainV(const O4Batch* B, const RegArgs& rg, int d, cudaStream_t s) {
   switch (kO4MinBlocks[2][B->var[2]]) {
-    case 3: return launchChainT<TI, 3>(B, rg, d, s);
-    case 5: return launchChainT<TI, 5>(B, rg, d, s);
-    default: return launchChainT<TI, 4>(B, rg, d, s);
+    case 2: return launchChainT<TI, 2>(B, rg, d, s);
+    case 4: return launchChainT<TI, 4>(B, rg, d, s);
+    default: return launchChainT<TI, 3>(B, rg, d, s);
   }
 }
 

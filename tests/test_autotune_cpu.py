@@ -45,5 +45,5 @@ def test_o4_variants_table():
     v = o4_variants()
     assert v.shape == (3, 3)
     # variant 0 is the default register cap of each kernel; all caps fit 128-thread CTAs
-    assert tuple(v[:, 0]) == (6, 4, 4)
+    assert tuple(v[:, 0]) == (6, 4, 3)
     assert (v >= 1).all() and (65536 // (v * 128) >= 64).all()

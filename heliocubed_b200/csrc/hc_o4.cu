@@ -1564,11 +1564,13 @@ struct O4Batch {
   int chunkCount[RG_COUNT][3] = {};
   int var[kO4TunedKernels] = {0, 0, 0};  // register-cap variant of the tuned kernels
   // tiles of the fused face chain, per direction, in one device array;
-  // chainTI: radial width of a tile (32, 16 or 8 by the narrowest box)
+  // chainTI: radial width of an angular direction's tile (32, 16 or 8 by
+  // the narrowest box); chainTI0 that of direction 0 (16 or 8: its tiles
+  // are 8 rows of j deep, which halves the share of recomputed ring rows)
   ChainTile* chainTiles = nullptr;
   long chainOff[3] = {};
   int chainCount[3] = {};
-  int chainTI = 32;
+  int chainTI = 32, chainTI0 = 16;
   // TMA tensor maps of the angular chains' face slabs, per box and direction
   // 1, 2: one copying 8 arrays, one copying 2 (device array; null without TMA)
   CUtensorMap* maps = nullptr;
@@ -1766,11 +1768,12 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
     int narrow = 1 << 30;
     for (int b = 0; b < nbox; ++b) narrow = std::min(narrow, B->host[(size_t)b * 3].V.n(0));
     B->chainTI = narrow >= 24 ? 32 : narrow >= 12 ? 16 : 8;
+    B->chainTI0 = narrow >= 12 ? 16 : 8;
   }
   std::vector<ChainTile> tiles;
   for (int d = 0; d < 3; ++d) {
     B->chainOff[d] = (long)tiles.size();
-    chainTiles(B->host, nbox, d, B->chainTI, tiles);
+    chainTiles(B->host, nbox, d, d == 0 ? B->chainTI0 : B->chainTI, tiles);
     const long count = (long)tiles.size() - B->chainOff[d];
     if (count > 0x7fffffffL) {
       *err = cudaErrorInvalidValue;
@@ -1779,7 +1782,7 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
     }
     B->chainCount[d] = (int)count;
   }
-  *err = B->chainTI == 32 ? chain0Smem<32>() : B->chainTI == 16 ? chain0Smem<16>() : chain0Smem<8>();
+  *err = B->chainTI0 == 16 ? chain0Smem<16>() : chain0Smem<8>();
   if (*err == cudaSuccess)
     *err = B->chainTI == 32   ? chainSmemT<32, false>()
            : B->chainTI == 16 ? chainSmemT<16, false>()
@@ -1910,6 +1913,7 @@ cudaError_t launchChainV(const O4Batch* B, const RegArgs& rg, int d, cudaStream_
 }
 
 cudaError_t launchChain(const O4Batch* B, const RegArgs& rg, int d, cudaStream_t s) {
+  if (d == 0) return B->chainTI0 == 16 ? launchChainV<16>(B, rg, d, s) : launchChainV<8>(B, rg, d, s);
   if (B->chainTI == 32) return launchChainV<32>(B, rg, d, s);
   if (B->chainTI == 16) return launchChainV<16>(B, rg, d, s);
   return launchChainV<8>(B, rg, d, s);

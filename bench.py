@@ -62,15 +62,21 @@ L2_BYTES = 126 * 1024 * 1024
 OPERATOR_BYTES_PER_CELL_STAGE = 128  # read 8 FP64 primitives, write 8 FP64 rhs
 
 
+def operator_launches(args) -> int:
+    """Kernels of one fourth-order operator evaluation (hc_level_rhs)."""
+    roe, powell = int(args.riemann == 2), 1
+    # detector + point values (3); per direction reconstruction, Roe point
+    # dissipation, fused face chain and the Powell face chain (3); the radial
+    # face averages of the TMA-staged radial chain (1); Powell coefficients,
+    # averages and application (3)
+    return 3 + 3 * (2 + roe + 3 * powell) + 1 + 3 * powell
+
+
 def launches_per_step(args) -> int:
     """Kernels of this library launched by one hc_level_advance_cfl step."""
     if args.order == 2:
         return 11  # prim + cfl + 4 x (ghosts, stage) + time (prologue in every 1-step call)
-    roe, powell = int(args.riemann == 2), 1
-    # detector + point values (3); per direction reconstruction, Roe point
-    # dissipation, fused face chain and the Powell face chain (3); Powell
-    # coefficients, averages and application (3)
-    operator = 3 + 3 * (2 + roe + 3 * powell) + 3 * powell
+    operator = operator_launches(args)
     per_stage = 4 + int(args.gravity) + operator + 1               # prepare, gravity, operator, update
     return 1 + 4 * per_stage + 2 + 1                               # cfl, stages, reflux, time
 
@@ -500,7 +506,7 @@ def measure_uniform(args, world, rank, local, e2e_min_steps: int = 4) -> dict:
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "kernel": ("o2StageKernel (operator: read primitives, write rhs)" if args.order == 2 else
                                     "Berta operator launch group (hc_level_rhs, %d kernels): read USph, write rhs"
-                                    % (3 + 3 * (2 + int(args.riemann == 2) + 3) + 3)),
+                                    % operator_launches(args)),
                          "algorithmic_bytes": f"{OPERATOR_BYTES_PER_CELL_STAGE} B/cell-stage x {cells} cells",
                          "kernel_ms": kms,
                          "traffic": None if tr is None else tr * cells},
@@ -875,6 +881,7 @@ def run_amr(args, world, rank, local):
     plain()
     torch.cuda.synchronize()
     same = all(torch.equal(a, w[2]) for a, w in zip(ref, [w for lv in levels for w in lv[2]]))
+    nop = operator_launches(argparse.Namespace(riemann=2))
     if rank == 0:
         out = {"metric": "FP64 cell-stage evaluations/s, batched AMR boxes vs plain per-box launches",
                "value": cells / (ms_b * 1e-3) * world, "unit": "cell-stage evaluations/s", "n_gpus": world,
@@ -883,9 +890,9 @@ def run_amr(args, world, rank, local):
                "config": {"workload": "AMR-style box batch (scaled config 3), Berta WENOZ + Roe + Powell",
                           "levels": [{"n": n, "boxes": len(w)} for n, _, w, _, _ in levels], "boxes": nboxes,
                           "cells": cells, "ghost": 5},
-               "batched": {"ms_per_evaluation": ms_b, "launches": 3 * 24},
+               "batched": {"ms_per_evaluation": ms_b, "launches": len(levels) * nop},
                "plain": {"ms_per_evaluation": ms_p, "cell_stage_per_s": cells / (ms_p * 1e-3),
-                         "launches": 24 * nboxes},
+                         "launches": nop * nboxes},
                "batched_over_plain": ms_p / ms_b, "identical_results": same,
                "rk4_stage_logic": {"ms_per_step": ms_rk, "launches": 5,
                                    "what": "tableau combine of every box of every level, 4 stages + final"},

@@ -229,7 +229,7 @@ struct O4Args {
   double* mj;   // [nbox][V+1]
   double* kp;   // [nbox][8][V+2]
 };
-constexpr int kO4FaceArrays = 8 * 4 + 5;  // WL, WR, FS, QD/DP (8 each) + thF, PS, BP, Bflux, Bprod
+constexpr int kO4FaceArrays = 8 * 4 + 5 + 9;  // WL, WR, FS, QD/DP (8 each) + thF, PS, BP, Bflux, Bprod + averages (8 + 1)
 
 size_t o4ScratchDoubles(int nbox, const int vlo[3], const int vhi[3], int ghost);
 // Carve the operator scratch of a.nbox boxes with the valid box a.vlo..vhi

@@ -55,7 +55,7 @@ __device__ __forceinline__ long roff(const Reg& r, int i, int j, int k) {
 
 // Offsets of the face arrays inside a box's face scratch (units of F.N).
 enum FaceArr { F_WL = 0, F_WR = 8, F_FS = 16, F_QD = 24, F_THF = 32, F_PS = 33, F_BP = 34, F_BFLUX = 35,
-               F_BPROD = 36 };
+               F_BPROD = 36, F_FA0 = 37, F_PA0 = 45 };  // F_FA0, F_PA0: direction 0's averages (TMA path)
 
 struct Ctx {
   O4Args a;
@@ -1093,6 +1093,10 @@ __device__ __forceinline__ void chainAverage(const Ctx& c, int d, int i, int j, 
 // soon as the current slab's are consumed, so they overlap the mapped-flux
 // and final-flux stages; without it (tensor maps unavailable) the same
 // stages read the face scratch through L1.
+// TMA tensor maps per box: directions 1 and 2 (8 arrays, 2 arrays each),
+// then direction 0 (averages: 9 arrays; dissipations: 8).
+constexpr int kChainMaps = 6;
+
 template <int TI>
 struct ChainShape {
   static constexpr int TT = 128 / TI, NI = TI + 2, NT = TT + 2;  // averages: tile plus a one-face ring
@@ -1182,7 +1186,7 @@ __global__ void __launch_bounds__(ChainShape<TI>::NTH, MB) o4FaceChainKernel(con
   // TMA tiles: radial from i0 - 2 (an even offset from the face box's low
   // corner: tiles start at the valid box's low radial index and TI is even),
   // angular from a0 - 2, one face slab; map 0 copies 8 arrays, map 1 two
-  const CUtensorMap* map8 = TMA ? maps + ((long)tl.box * 2 + (D - 1)) * 2 : nullptr;
+  const CUtensorMap* map8 = TMA ? maps + (long)tl.box * kChainMaps + (D - 1) * 2 : nullptr;
   const CUtensorMap* map2 = TMA ? map8 + 1 : nullptr;
   const int tx = tl.i0 - 2 - c.fr.lo[0], ta = tl.a0 - 2 - c.fr.lo[tdim], tnLo = c.fr.lo[D];
   auto issue = [&](int n, bool inputs) {
@@ -1518,6 +1522,209 @@ __global__ void __launch_bounds__(chain0Threads<TI>(), MB) o4FaceChain0Kernel(co
   }
 }
 
+
+// Direction 0 with TMA, in two kernels.  First the theta-aware averages of
+// the flux sums and total pressures on the final faces plus a one-face ring
+// in j and k (the region of the Roe point dissipation), one thread per face,
+// into the face scratch (F_FA0, F_PA0); it runs beside the Roe point
+// dissipation.
+__global__ void o4FaceAvg0Kernel(const Ctx* __restrict__ tab, const RegArgs rg, const WorkChunk* __restrict__ wk) {
+  const WorkChunk wc = wk[blockIdx.x];
+  const Ctx& c = tab[wc.box * 3 + 0];
+  const Box3 PB = c.V0.growTrans(0, 1);
+  forRegion(PB, wc, [&](int b, int i, int j, int k) {
+    double fa[8], pa;
+    chainAverage(c, 0, i, j, k, fa, pa);
+    double* base = c.a.face + roff(c.fr, i, j, k);
+    const long NF = c.fr.N;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) base[(F_FA0 + e) * NF] = fa[e];
+    base[F_PA0 * NF] = pa;
+  });
+}
+
+// Then the chain itself: TI radial cells (TI + 1 faces) x TT rows of j per
+// CTA, walking k over [c0, c1]; a ring of three k-slabs of the averages
+// (8 + 1 arrays) and one of the point Roe dissipations (8 arrays), each slab
+// TI + 2 radial x TT + 2 rows, copied by TMA, the slab k + 2 issued as soon
+// as slab k - 1 is consumed.  Everything else as o4FaceChain0Kernel.
+template <int TI>
+struct Chain0Shape {
+  static constexpr int TT = 128 / TI, NI = TI + 1, NTH = NI * TT;
+  static constexpr int NX = TI + 2, NY = TT + 2, NXY = NX * NY;  // TMA slab: faces and one row either side
+  static constexpr int SA = 9 * NXY, SQ = 8 * NXY;                  // doubles per averages / dissipation slab
+  static constexpr int round16(int n) { return (n + 15) / 16 * 16; }
+  // slots start on 128-byte boundaries, as a tensor copy's destination must
+  static constexpr int PA = round16(SA), PQ = round16(SQ);
+  static constexpr int oA = 0, oQ = 3 * PA, oFX = oQ + 3 * PQ, oBar = oFX + round16(8 * NTH);
+  static constexpr int doubles() { return oBar + 6; }
+};
+
+template <int TI, int MB>
+__global__ void __launch_bounds__(Chain0Shape<TI>::NTH, MB)
+    o4FaceChain0TmaKernel(const Ctx* __restrict__ tab, const RegArgs rg, const ChainTile* __restrict__ tiles,
+                          const CUtensorMap* __restrict__ maps) {
+  using S = Chain0Shape<TI>;
+  constexpr int TT = S::TT, NI = S::NI, NX = S::NX, NXY = S::NXY, NTH = S::NTH;
+  extern __shared__ __align__(128) double smem[];
+  double* sA = smem + S::oA;    // [3 slots][9][NY][NX]
+  double* sQ = smem + S::oQ;    // [3 slots][8][NY][NX]
+  double* sFX = smem + S::oFX;  // [8][NTH]
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + S::oBar);  // [A 3][Q 3]
+  const ChainTile tl = tiles[blockIdx.x];
+  const Ctx& c = tab[tl.box * 3 + 0];
+  const O4Args& a = c.a;
+  const int tid = threadIdx.x;
+  const double coef = -a.scale / a.G.dx[0];
+  const int ihi = c.V.hi[0] + 1;
+  const CUtensorMap* mapA = maps + (long)tl.box * kChainMaps + 4;
+  const CUtensorMap* mapQ = mapA + 1;
+  const int tx = tl.i0 - c.fr.lo[0], ty = tl.a0 - 1 - c.fr.lo[1];
+  // slab k lives in slot (k - c0 + 1) % 3 and is that slot's ((k - c0 + 1) / 3)-th copy
+  auto slot = [&](int k) { return (k - tl.c0 + 1) % 3; };
+  auto use = [&](int k) { return (unsigned)((k - tl.c0 + 1) / 3) & 1u; };
+  const int kLast = tl.c1 + 1;
+  auto issue = [&](int k) {
+    const int sl = slot(k);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbarExpect(&bar[sl], (unsigned)S::SA * sizeof(double));
+    tmaLoad(sA + sl * S::PA, mapA, tx, ty, k - c.fr.lo[2], F_FA0, &bar[sl]);
+    mbarExpect(&bar[3 + sl], (unsigned)S::SQ * sizeof(double));
+    tmaLoad(sQ + sl * S::PQ, mapQ, tx, ty, k - c.fr.lo[2], F_QD, &bar[3 + sl]);
+  };
+  if (tid == 0) {
+    for (int q = 0; q < 6; ++q) mbarInit(&bar[q]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int k = tl.c0 - 1; k <= tl.c0 + 1; ++k) issue(k);
+  bool failed = false;
+  for (int k = tl.c0; k <= tl.c1 && !failed; ++k) {
+    bool ok = true;
+    if (k == tl.c0) ok = mbarWait(&bar[slot(k - 1)], use(k - 1)) && mbarWait(&bar[3 + slot(k - 1)], use(k - 1)) &&
+                        mbarWait(&bar[slot(k)], use(k)) && mbarWait(&bar[3 + slot(k)], use(k));
+    ok = ok && mbarWait(&bar[slot(k + 1)], use(k + 1)) && mbarWait(&bar[3 + slot(k + 1)], use(k + 1));
+    failed = __syncthreads_or(!ok);
+    if (failed) break;
+    const double* F0 = sA + slot(k) * S::PA;
+    const double* Fm = sA + slot(k - 1) * S::PA;
+    const double* Fp = sA + slot(k + 1) * S::PA;
+    // (6, 7, 8) faces i0 .. i0+TI x rows a0 .. a0+TT-1 of row k: one thread each
+    {
+      const int q = tid, ii = tl.i0 + q % NI, jj = tl.a0 + q / NI;
+      if (ii <= ihi && jj <= c.V.hi[1]) {
+        const int o = (q / NI + 1) * NX + q % NI;  // (ii, jj) in a slab
+        const double* M = faceRec(a.G, a.block0, 0, jj, k);
+        const double* Mj1 = faceRec(a.G, a.block0, 0, jj + 1, k);
+        const double* Mj0 = faceRec(a.G, a.block0, 0, jj - 1, k);
+        const double* Mk1 = faceRec(a.G, a.block0, 0, jj, k + 1);
+        const double* Mk0 = faceRec(a.G, a.block0, 0, jj, k - 1);
+        double dM0[10], dM1[10];
+#pragma unroll
+        for (int e = 0; e < 10; ++e) {
+          dM0[e] = 0.5 * Mj1[e] - 0.5 * Mj0[e];
+          dM1[e] = 0.5 * Mk1[e] - 0.5 * Mk0[e];
+        }
+        double fa[8], dF0[8], dF1[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          fa[e] = F0[e * NXY + o];
+          dF0[e] = 0.5 * F0[e * NXY + o + NX] - 0.5 * F0[e * NXY + o - NX];
+          dF1[e] = 0.5 * Fp[e * NXY + o] - 0.5 * Fm[e * NXY + o];
+        }
+        double fm[8];
+#pragma unroll
+        for (int qq = 0; qq < 2; ++qq) {
+          const int e = qq == 0 ? 0 : 4;
+          double term = 0.0;
+          term += dM0[9] * dF0[e] * (1.0 / 12.0);
+          term += dM1[9] * dF1[e] * (1.0 / 12.0);
+          term += M[9] * fa[e] * 1.0;
+          fm[e] = 0.0 + term;
+        }
+#pragma unroll
+        for (int bb = 0; bb < 2; ++bb) {
+          const int bs = bb == 0 ? 1 : 5;
+#pragma unroll
+          for (int row = 0; row < 3; ++row) {
+            double sum = 0.0;
+#pragma unroll
+            for (int col = 0; col < 3; ++col) {
+              double term = 0.0;
+              term += dM0[3 * row + col] * dF0[bs + col] * (1.0 / 12.0);
+              term += dM1[3 * row + col] * dF1[bs + col] * (1.0 / 12.0);
+              term += M[3 * row + col] * fa[bs + col] * 1.0;
+              sum += term;
+            }
+            fm[bs + row] = sum;
+          }
+        }
+        const double si = adjDr(a.G, 0, ii);
+        double fs[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          double value = 0.0;
+          value += fm[e] * si * 1.0;
+          fs[e] = value;
+        }
+        auto t3 = [&](double pav) {
+          double value = 0.0;
+          value += pav * si * 1.0;
+          return value;
+        };
+        const double* P0 = F0 + 8 * NXY;
+        const double dT3[2] = {0.5 * t3(P0[o + NX]) - 0.5 * t3(P0[o - NX]),
+                               0.5 * t3(Fp[8 * NXY + o]) - 0.5 * t3(Fm[8 * NXY + o])};
+        // the five dissipation taps: the face, rows j -+ 1 of slab k, slabs k -+ 1
+        const long so = (long)slot(k) * S::PQ + o;
+        const QdTaps tap{sQ, NXY, {so, so - NX, so + NX, (long)slot(k - 1) * S::PQ + o, (long)slot(k + 1) * S::PQ + o}};
+        double fx[8];
+        chainFinal<0>(c, ii, jj, k, fs, t3(P0[o]), dT3, tap, fx);
+        chainStore<0>(c, rg, ii, jj, k, fx);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) sFX[e * NTH + q] = fx[e];
+      }
+    }
+    __syncthreads();
+    // slab k - 1 is consumed: its slots take slab k + 2
+    if (tid == 0 && k + 2 <= kLast) issue(k + 2);
+    // (9) divergence of the row's cells
+    {
+      const int li = tid % TI, lj = tid / TI;
+      const int i = tl.i0 + li, j = tl.a0 + lj;
+      if (tid < TI * TT && i <= c.V.hi[0] && j <= c.V.hi[1]) {
+        const int q = lj * NI + li;
+        double* R = a.rhs + roff(c.vr, i, j, k);
+        double rv[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) rv[e] = R[e * c.vr.N];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) R[e * c.vr.N] = rv[e] + coef * (sFX[e * NTH + q + 1] - sFX[e * NTH + q]);
+      }
+    }
+    __syncthreads();
+  }
+  if (failed) {
+    // A copy did not land: report it, wait (bounded) for the copies still in
+    // flight, and make this tile's cells visibly invalid.
+    if (tid == 0) {
+      if (a.G.status) atomicExch(a.G.status, 1);
+      for (int q = 0; q < 6; ++q) {
+        mbarWait(&bar[q], 0u);
+        mbarWait(&bar[q], 1u);
+      }
+    }
+    __syncthreads();
+    const int li = tid % TI, lj = tid / TI;
+    const int i = tl.i0 + li, j = tl.a0 + lj;
+    if (tid < TI * TT && i <= c.V.hi[0] && j <= c.V.hi[1])
+      for (int k = tl.c0; k <= tl.c1; ++k)
+#pragma unroll
+        for (int e = 0; e < 8; ++e) a.rhs[roff(c.vr, i, j, k) + e * c.vr.N] = CUDART_NAN;
+  }
+}
+
 }  // namespace
 
 size_t o4CarveScratch(O4Args& a, double* sp) {
@@ -1643,12 +1850,29 @@ EncodeTiledFn encodeTiled() {
 // d = 1, 2, boxes of (TI + 4) radial x (TT + 4) angular x 1 normal x 8 or 2
 // arrays.  False where a map cannot be made (then the chains read through
 // L1 instead).
-bool chainMaps(const std::vector<Ctx>& host, int nbox, int TI, std::vector<CUtensorMap>& out) {
+bool chainMaps(const std::vector<Ctx>& host, int nbox, int TI, int TI0, std::vector<CUtensorMap>& out) {
   const EncodeTiledFn enc = encodeTiled();
   if (!enc) return false;
-  const int TT = 128 / TI;
-  out.resize((size_t)nbox * 4);
-  for (int b = 0; b < nbox; ++b)
+  const int TT = 128 / TI, TT0 = 128 / TI0;
+  out.resize((size_t)nbox * kChainMaps);
+  for (int b = 0; b < nbox; ++b) {
+    // direction 0: slabs of TI0 + 2 radial faces (an even count from an even
+    // offset) x TT0 + 2 rows of j x one k
+    {
+      const Ctx& c = host[(size_t)b * 3];
+      const cuuint64_t n0 = c.fr.n[0], n1 = c.fr.n[1], n2 = c.fr.n[2];
+      if ((reinterpret_cast<uintptr_t>(c.a.face) & 15) || (n0 & 1) || ((c.V.lo[0] - c.fr.lo[0]) & 1)) return false;
+      const cuuint64_t dims[4] = {n0, n1, n2, (cuuint64_t)kO4FaceArrays};
+      const cuuint64_t strides[3] = {n0 * 8, n0 * n1 * 8, n0 * n1 * n2 * 8};
+      for (int w = 0; w < 2; ++w) {
+        const cuuint32_t box[4] = {(cuuint32_t)(TI0 + 2), (cuuint32_t)(TT0 + 2), 1u, w == 0 ? 9u : 8u};
+        const cuuint32_t es[4] = {1, 1, 1, 1};
+        if (enc(&out[(size_t)b * kChainMaps + 4 + w], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, c.a.face, dims, strides,
+                box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+          return false;
+      }
+    }
     for (int d = 1; d <= 2; ++d) {
       const Ctx& c = host[(size_t)b * 3 + d];
       const cuuint64_t n0 = c.fr.n[0], n1 = c.fr.n[1], n2 = c.fr.n[2];
@@ -1661,12 +1885,13 @@ bool chainMaps(const std::vector<Ctx>& host, int nbox, int TI, std::vector<CUten
         const cuuint32_t box[4] = {(cuuint32_t)(TI + 4), d == 1 ? 1u : (cuuint32_t)(TT + 4),
                                    d == 1 ? (cuuint32_t)(TT + 4) : 1u, w == 0 ? 8u : 2u};
         const cuuint32_t es[4] = {1, 1, 1, 1};
-        if (enc(&out[((size_t)b * 2 + (d - 1)) * 2 + w], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, c.a.face, dims, strides,
-                box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+        if (enc(&out[(size_t)b * kChainMaps + (d - 1) * 2 + w], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, c.a.face, dims,
+                strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
           return false;
       }
     }
+  }
   return true;
 }
 
@@ -1680,6 +1905,17 @@ cudaError_t chainSmemT() {
     e = cudaFuncSetAttribute(o4FaceChainKernel<D, TI, MB, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   HC_CHAIN_ATTR(1, 2) HC_CHAIN_ATTR(1, 3) HC_CHAIN_ATTR(1, 4) HC_CHAIN_ATTR(2, 2) HC_CHAIN_ATTR(2, 3) HC_CHAIN_ATTR(2, 4)
 #undef HC_CHAIN_ATTR
+  return e;
+}
+
+template <int TI>
+cudaError_t chain0TmaSmem() {
+  const int bytes = Chain0Shape<TI>::doubles() * (int)sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(o4FaceChain0TmaKernel<TI, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(o4FaceChain0TmaKernel<TI, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(o4FaceChain0TmaKernel<TI, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   return e;
 }
 
@@ -1789,10 +2025,11 @@ O4Batch* o4BatchCreate(const O4Args* boxes, int nbox, cudaError_t* err) {
                               : chainSmemT<8, false>();
   {
     std::vector<CUtensorMap> maps;
-    if (*err == cudaSuccess && chainMaps(B->host, nbox, B->chainTI, maps)) {
+    if (*err == cudaSuccess && chainMaps(B->host, nbox, B->chainTI, B->chainTI0, maps)) {
       cudaError_t e = B->chainTI == 32   ? chainSmemT<32, true>()
                       : B->chainTI == 16 ? chainSmemT<16, true>()
                                          : chainSmemT<8, true>();
+      if (e == cudaSuccess) e = B->chainTI0 == 16 ? chain0TmaSmem<16>() : chain0TmaSmem<8>();
       if (e == cudaSuccess) e = cudaMalloc(&B->maps, sizeof(CUtensorMap) * maps.size());
       if (e == cudaSuccess)
         e = cudaMemcpy(B->maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice);
@@ -1890,7 +2127,10 @@ cudaError_t launchChainT(const O4Batch* B, const RegArgs& rg, int d, cudaStream_
   if (n == 0) return cudaSuccess;
   const size_t smemTma = ChainShape<TI>::doubles(true) * sizeof(double);
   const size_t smemL1 = ChainShape<TI>::doubles(false) * sizeof(double);
-  if (d == 0)
+  if (d == 0 && B->chainTma)
+    o4FaceChain0TmaKernel<TI, MB><<<n, Chain0Shape<TI>::NTH, Chain0Shape<TI>::doubles() * sizeof(double), s>>>(
+        B->dev, rg, t, B->maps);
+  else if (d == 0)
     o4FaceChain0Kernel<TI, MB><<<n, chain0Threads<TI>(), chain0Doubles<TI>() * sizeof(double), s>>>(B->dev, rg, t);
   else if (d == 1 && B->chainTma)
     o4FaceChainKernel<1, TI, MB, true><<<n, ChainShape<TI>::NTH, smemTma, s>>>(B->dev, rg, t, B->maps);
@@ -1970,6 +2210,9 @@ cudaError_t launchO4Batch(const O4Batch* B, const RegArgs* reg, cudaStream_t s) 
   for (int d = 0; d < 3; ++d) {
     if (d >= 2 && B->powell && (e = cudaStreamWaitEvent(s, B->joinEv[d - 2], 0)) != cudaSuccess) return e;
     HC_LAUNCH_DM(o4FaceReconKernel, 0, RG_F)
+    // direction 0's face averages for its TMA chain (beside the Roe point
+    // dissipation, which reads neither their inputs' outputs nor them)
+    if (d == 0 && B->chainTma) { HC_LAUNCH(o4FaceAvg0Kernel, 0, RG_PB) }
     if (B->powell) {
       // the Powell chain reads the reconstruction's flags and normal B and
       // writes only its own face arrays and -J div B: fork it

@@ -503,6 +503,42 @@ int buildLevel(hc_ctx* c) {
   return HC_OK;
 }
 
+// The face frame of the factored Roe dissipation for basis A (row-major
+// 3 x 3) and face direction dir, in the record layout of kO4RoeRec.
+void roeFrame(const double* A, int dir, double* out) {
+  const int t1 = (dir + 1) % 3, t2 = (dir + 2) % 3;
+  double f0[3], f1[3], normal2 = 0.0, tangent2 = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    const int j = (i + 1) % 3, k = (i + 2) % 3;
+    f0[i] = A[3 * j + t1] * A[3 * k + t2] - A[3 * k + t1] * A[3 * j + t2];
+    f1[i] = A[3 * i + t1];
+    normal2 += f0[i] * f0[i];
+    tangent2 += f1[i] * f1[i];
+  }
+  const double normalMag = std::sqrt(normal2), tangentMag = std::sqrt(tangent2);
+  const double invN = 1.0 / normalMag, invT = 1.0 / tangentMag;
+  for (int i = 0; i < 3; ++i) { f0[i] *= invN; f1[i] *= invT; }
+  for (int i = 0; i < 3; ++i) {
+    const int j = (i + 1) % 3, k = (i + 2) % 3;
+    out[i] = f0[i];
+    out[3 + i] = f1[i];
+    out[6 + i] = f0[j] * f1[k] - f0[k] * f1[j];
+  }
+  out[9] = normalMag;
+  double adj[3][3];
+  for (int dd = 0; dd < 3; ++dd) {
+    const int s1 = (dd + 1) % 3, s2 = (dd + 2) % 3;
+    for (int i = 0; i < 3; ++i) {
+      const int j = (i + 1) % 3, k = (i + 2) % 3;
+      adj[dd][i] = A[3 * j + s1] * A[3 * k + s2] - A[3 * k + s1] * A[3 * j + s2];
+      out[10 + 3 * dd + i] = adj[dd][i];
+    }
+  }
+  const double det = A[0] * adj[0][0] + A[3] * adj[0][1] + A[6] * adj[0][2];
+  out[19] = 1.0 / det;
+  out[20] = 1.0 / (det * det);
+}
+
 // Fourth-order metric tables over angular indices [-ext, na+ext] (ghost
 // cells beyond the panel edges use the gnomonic extension of the map) and the
 // radial table over [-kO4Rad, nr+kO4Rad].
@@ -564,6 +600,18 @@ int buildO4Geometry(hc_ctx* c) {
             for (int q = 0; q < 3; ++q) e[13 + 3 * r + q] = F[r][q];
         }
       }
+  // Roe frames (the geometry half of the factored Roe dissipation,
+  // src/MHD_Roe8Wave.H:634-740, which depends only on the face's angular
+  // position): computed once here instead of at every face of every stage.
+  std::vector<double> roe((size_t)6 * 3 * n * n * kO4RoeRec, 0.0);
+  for (int b = 0; b < 6; ++b)
+    for (int d = 0; d < 3; ++d)
+      for (int k = 0; k < n; ++k)
+        for (int j = 0; j < n; ++j) {
+          const size_t at = (((size_t)b * 3 + d) * n + k) * n + j;
+          const double* A = d == 0 ? &cell[((size_t)b * n + k) * n * 9 + (size_t)j * 9] : &face[at * kO4FaceRec + 13];
+          roeFrame(A, d, &roe[at * kO4RoeRec]);
+        }
   std::vector<double4> radial(nr + 2 * kO4Rad + 1);
   for (int i = -kO4Rad; i <= nr + kO4Rad; ++i) {
     const RadialRow r = radialRow(P, i);
@@ -574,6 +622,7 @@ int buildO4Geometry(hc_ctx* c) {
   g.nr = nr; g.na = na; g.ext = ext;
   g.face = upload(face, c->owned, err);
   g.cell = upload(cell, c->owned, err);
+  g.frames = upload(roe, c->owned, err);
   g.radial = upload(radial, c->owned, err);
   g.gamma = P.gamma; g.invGm1 = 1.0 / (P.gamma - 1.0); g.entropy = P.entropy_fix_coeff; g.eta_d = P.berta_eta_d;
   g.dx[0] = 1.0 / nr; g.dx[1] = 1.0 / na; g.dx[2] = 1.0 / na;

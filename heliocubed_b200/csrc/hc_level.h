@@ -185,11 +185,17 @@ constexpr int kO4Rad = 10;   // radial margin of the O4 radial table
 // Face metrics of direction d at angular (j,k): <det A A> (9), <det A> (1),
 // <adjA row d> (3), pointwise basis at the face centre (9; d = 0: cell centre).
 constexpr int kO4FaceRec = 22;
+// Frame of the factored Roe dissipation at a face of direction d (angular
+// (j,k)), from the face-centre basis A (d = 0: cell centre): unit normal f0,
+// unit tangent f1, f2 = f0 x f1 (9), |cofactor row d of A| (1), adj A (9),
+// 1 / det A, 1 / det A^2 (2); padded to 24 (16-byte aligned pairs).
+constexpr int kO4RoeRec = 24;
 
 struct O4Geo {
   int nr, na, ext;        // tables cover angular indices [-ext, na+ext]
   const double* face;     // [6][3][na+2ext+1 (k)][na+2ext+1 (j)][22]
   const double* cell;     // [6][na+2ext+1][na+2ext+1][9] cell-centre basis
+  const double* frames;   // [6][3][na+2ext+1 (k)][na+2ext+1 (j)][kO4RoeRec] Roe frames
   const double4* radial;  // [nr+2*kO4Rad+1], index i+kO4Rad: {rlow^2, areaT, Dr0, dVolr}
   double gamma, invGm1, entropy, eta_d, dx[3];
   int roe, powell, fallback;

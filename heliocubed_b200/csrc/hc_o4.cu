@@ -140,6 +140,10 @@ __device__ __forceinline__ const double* faceRec(const O4Geo& g, int block, int 
   const long n = g.na + 2 * g.ext + 1;
   return g.face + ((((long)block * 3 + d) * n + (k + g.ext)) * n + (j + g.ext)) * kO4FaceRec;
 }
+__device__ __forceinline__ const double* roeRec(const O4Geo& g, int block, int d, int j, int k) {
+  const long n = g.na + 2 * g.ext + 1;
+  return g.frames + ((((long)block * 3 + d) * n + (k + g.ext)) * n + (j + g.ext)) * kO4RoeRec;
+}
 __device__ __forceinline__ const double* cellBasis(const O4Geo& g, int block, int j, int k) {
   const long n = g.na + 2 * g.ext + 1;
   return g.cell + (((long)block * n + (k + g.ext)) * n + (j + g.ext)) * 9;
@@ -319,76 +323,71 @@ __device__ __forceinline__ bool usablePrimitive(const double w[8]) {
 }
 
 // mappedRoe8WaveDissipation + factoredRoe8WaveDissipation (src/MHD_Roe8Wave.H:634-740)
-__device__ __forceinline__ void factoredRoe(double out[8], const double* wl, const double* wr, const double* A, double radialArea,
-                            int dir, double gamma, double invGm1, double entropy) {
-  const int t1 = (dir + 1) % 3, t2 = (dir + 2) % 3;
-  double f0[3], f1[3], f2[3], normal2 = 0.0, tangent2 = 0.0;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const int j = (i + 1) % 3, k = (i + 2) % 3;
-    f0[i] = A[3 * j + t1] * A[3 * k + t2] - A[3 * k + t1] * A[3 * j + t2];
-    f1[i] = A[3 * i + t1];
-    normal2 += f0[i] * f0[i];
-    tangent2 += f1[i] * f1[i];
-  }
-  const double normalMag = sqrt(normal2), tangentMag = sqrt(tangent2);
-  const double invN = 1.0 / normalMag, invT = 1.0 / tangentMag;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) { f0[i] *= invN; f1[i] *= invT; }
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const int j = (i + 1) % 3, k = (i + 2) % 3;
-    f2[i] = f0[j] * f1[k] - f0[k] * f1[j];
-  }
+// with the face's frame from the Roe frame table R (kO4RoeRec): the states
+// are rotated into the frame, the 8-wave dissipation (Rusanov where the fan
+// check fails) is taken there, rotated back, scaled by the face area and
+// mapped through adj A / det A.  The frame is read again after the solver
+// (roeLoad2 is not merged with the first read), so it does not occupy
+// registers while the solver runs.
+__device__ __forceinline__ double2 roeLoad2(const double* p) {
+  double2 v;
+  asm volatile("ld.global.nc.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+
+__device__ __forceinline__ void factoredRoe(double out[8], const double* wl, const double* wr, const double* A,
+                                            const double* __restrict__ R, double radialArea, double gamma,
+                                            double invGm1, double entropy) {
   double loc[2][8];
+  {
+    double f[9];
 #pragma unroll
-  for (int side = 0; side < 2; ++side) {
-    const double* w = side == 0 ? wl : wr;
-    loc[side][0] = fmax(w[0], kRHO00);
-    loc[side][4] = fmax(w[4], 0.0);
-    double vC[3], bC[3];
+    for (int q = 0; q < 9; ++q) f[q] = R[q];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      vC[i] = A[3 * i] * w[1] + A[3 * i + 1] * w[2] + A[3 * i + 2] * w[3];
-      bC[i] = A[3 * i] * w[5] + A[3 * i + 1] * w[6] + A[3 * i + 2] * w[7];
+    for (int side = 0; side < 2; ++side) {
+      const double* w = side == 0 ? wl : wr;
+      loc[side][0] = fmax(w[0], kRHO00);
+      loc[side][4] = fmax(w[4], 0.0);
+      double vC[3], bC[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        vC[i] = A[3 * i] * w[1] + A[3 * i + 1] * w[2] + A[3 * i + 2] * w[3];
+        bC[i] = A[3 * i] * w[5] + A[3 * i + 1] * w[6] + A[3 * i + 2] * w[7];
+      }
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        loc[side][1 + r] = f[3 * r] * vC[0] + f[3 * r + 1] * vC[1] + f[3 * r + 2] * vC[2];
+        loc[side][5 + r] = f[3 * r] * bC[0] + f[3 * r + 1] * bC[1] + f[3 * r + 2] * bC[2];
+      }
     }
-    loc[side][1] = f0[0] * vC[0] + f0[1] * vC[1] + f0[2] * vC[2];
-    loc[side][2] = f1[0] * vC[0] + f1[1] * vC[1] + f1[2] * vC[2];
-    loc[side][3] = f2[0] * vC[0] + f2[1] * vC[1] + f2[2] * vC[2];
-    loc[side][5] = f0[0] * bC[0] + f0[1] * bC[1] + f0[2] * bC[2];
-    loc[side][6] = f1[0] * bC[0] + f1[1] * bC[1] + f1[2] * bC[2];
-    loc[side][7] = f2[0] * bC[0] + f2[1] * bC[1] + f2[2] * bC[2];
   }
   double diss[8];
   if (!roe8Body<true>(diss, loc[0], loc[1], gamma, entropy, invGm1))
     rusanovDissipation(diss, loc[0], loc[1], gamma, invGm1);
-  const double area = radialArea * normalMag;
+  double g[22];
+#pragma unroll
+  for (int q = 0; q < 11; ++q) {
+    const double2 v = roeLoad2(R + 2 * q);
+    g[2 * q] = v.x;
+    g[2 * q + 1] = v.y;
+  }
+  const double area = radialArea * g[9];
   double mapped[8];
   mapped[0] = area * diss[0];
   mapped[4] = area * diss[4];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    mapped[1 + i] = area * f0[i] * diss[1] + area * f1[i] * diss[2] + area * f2[i] * diss[3];
-    mapped[5 + i] = area * f0[i] * diss[5] + area * f1[i] * diss[6] + area * f2[i] * diss[7];
+    mapped[1 + i] = area * g[i] * diss[1] + area * g[3 + i] * diss[2] + area * g[6 + i] * diss[3];
+    mapped[5 + i] = area * g[i] * diss[5] + area * g[3 + i] * diss[6] + area * g[6 + i] * diss[7];
   }
-  double adj[3][3];
-#pragma unroll
-  for (int dd = 0; dd < 3; ++dd) {
-    const int s1 = (dd + 1) % 3, s2 = (dd + 2) % 3;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const int j = (i + 1) % 3, k = (i + 2) % 3;
-      adj[dd][i] = A[3 * j + s1] * A[3 * k + s2] - A[3 * k + s1] * A[3 * j + s2];
-    }
-  }
-  const double det = A[0] * adj[0][0] + A[3] * adj[0][1] + A[6] * adj[0][2];
-  const double invDet = 1.0 / det, invDet2 = 1.0 / (det * det);
+  const double* adj = g + 10;
+  const double invDet = g[19], invDet2 = g[20];
   out[0] = mapped[0] * invDet;
   out[4] = mapped[4] * invDet;
 #pragma unroll
   for (int dd = 0; dd < 3; ++dd) {
-    out[1 + dd] = (adj[dd][0] * mapped[1] + adj[dd][1] * mapped[2] + adj[dd][2] * mapped[3]) * invDet2;
-    out[5 + dd] = (adj[dd][0] * mapped[5] + adj[dd][1] * mapped[6] + adj[dd][2] * mapped[7]) * invDet2;
+    out[1 + dd] = (adj[3 * dd] * mapped[1] + adj[3 * dd + 1] * mapped[2] + adj[3 * dd + 2] * mapped[3]) * invDet2;
+    out[5 + dd] = (adj[3 * dd] * mapped[5] + adj[3 * dd + 1] * mapped[6] + adj[3 * dd + 2] * mapped[7]) * invDet2;
   }
 }
 
@@ -671,7 +670,8 @@ __global__ void __launch_bounds__(128, MB) o4RoePointKernel(const Ctx* __restric
     double l[8], r[8], o[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) { l[q] = base[(F_WL + q) * NF]; r[q] = base[(F_WR + q) * NF]; }
-    factoredRoe(o, l, r, faceBasis<D>(c, b, j, k), radialPoint(a.G, d, i), d, a.G.gamma, a.G.invGm1, a.G.entropy);
+    factoredRoe(o, l, r, faceBasis<D>(c, b, j, k), roeRec(a.G, a.block0 + b, D, j, k), radialPoint(a.G, d, i),
+                a.G.gamma, a.G.invGm1, a.G.entropy);
 #pragma unroll
     for (int q = 0; q < 8; ++q) base[(F_QD + q) * NF] = o[q];
   });

@@ -540,14 +540,22 @@ def serve_requests(args, rate_hz):
                                     radial=SERVE_GRIDS["radial"], angular=SERVE_GRIDS["angular"])
 
 
-def serve_launches(reqs) -> int:
+def serve_launches(reqs, cohort_steps: int | None = None) -> int:
     """Kernels of this library launched for `reqs` (admission, steps,
     schedule): per request the wind, the cone insertion and the schedule,
-    then each RK4 step's launches of its order."""
+    then each RK4 step's launches of its order.  With a fourth-order cohort
+    (cohort_steps = steps of all its chunks) a fourth-order request's steps
+    launch everything but the operator, which runs once per stage of every
+    cohort step for all members together."""
     total = 0
     for r in reqs:
         a = argparse.Namespace(order=r.order, riemann=2 if r.order == 4 else 1, gravity=0)
-        total += 3 + launches_per_step(a) * r.steps
+        per_step = launches_per_step(a)
+        if cohort_steps is not None and r.order == 4:
+            per_step -= 4 * operator_launches(a)
+        total += 3 + per_step * r.steps
+    if cohort_steps:
+        total += 4 * operator_launches(argparse.Namespace(riemann=2)) * cohort_steps
     return total
 
 
@@ -609,6 +617,7 @@ def run_serve(args, world, rank, local):
     plain = serve.run_plain(reqs, device=local, shells=shells, keep_states=False)
     barrier(world)
     batched = server.run(reqs)
+    cohort_steps = server.cohort.chunk_steps if server.cohort is not None else None
     barrier(world)
     hosted = server.run(staged)
     barrier(world)
@@ -656,6 +665,9 @@ def run_serve(args, world, rank, local):
                                   "time %.3f s)" % (rate, args.serve_inflight, service_s),
                       "max_inflight": args.serve_inflight, "hbm_budget_gb": args.serve_budget_gb,
                       "chunk_steps": chunk, "slots_per_shape": "min(requests of the shape, 3), built before timing",
+                      "fourth_order_cohort": "the fourth-order requests in flight step together (hc_ensemble): "
+                                             "each operator kernel one launch per stage over all their panels; "
+                                             "second-order requests on their own streams",
                       "l2": "working set of the in-flight solves larger than L2",
                       "parallelism": f"replicas x{world}"},
            "batched": sb, "plain": sp,
@@ -668,7 +680,7 @@ def run_serve(args, world, rank, local):
                    "p50_s": se["p50_s"], "p99_s": se["p99_s"], "identical_to_device_built": same_e2e,
                    "pipeline": "served run with every request's initial state copied from pinned host memory at "
                                "admission and its result copied back (bytes per request-step)"},
-           "gpu_launches": serve_launches(reqs),
+           "gpu_launches": serve_launches(reqs, cohort_steps),
            "clocks": clocks}
     if large is not None:
         out["roofline"] = dict(large["roofline"], workload="large solve 256x192^2x6 (operator launch group)")

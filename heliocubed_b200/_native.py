@@ -31,6 +31,9 @@ SIGNATURES = {
     "hc_o4_batch_create": (C.c_int, [_VP, _VP, C.c_int, C.c_double, _VP]),
     "hc_o4_batch_rhs": (C.c_int, [_VP, _VP, _VP]),
     "hc_o4_batch_destroy": (C.c_int, [_VP]),
+    "hc_ensemble_create": (C.c_int, [_VP, C.c_int, C.POINTER(_VP)]),
+    "hc_ensemble_advance_cfl": (C.c_int, [_VP, _VP, C.c_int, _VP, _VP, _VP]),
+    "hc_ensemble_destroy": (C.c_int, [_VP]),
     "hc_level_prepare": (C.c_int, [_VP, _VP, _VP, C.c_double, _VP]),
     "hc_level_rhs": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hc_level_rk4_step": (C.c_int, [_VP, _VP, C.c_double, C.c_double, _VP]),

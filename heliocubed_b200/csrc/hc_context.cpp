@@ -276,6 +276,17 @@ struct hc_ctx {
   std::vector<std::pair<std::string, O4Batch*>> o4cache;
 };
 
+// Several fourth-order levels stepped together: each level prepares its
+// own stages, takes its own CFL step, updates and reconciles its own seams;
+// the operator runs as one batch over all levels' panels, so every operator
+// kernel is one launch for the whole ensemble.
+struct hc_ensemble {
+  std::vector<hc_ctx*> members;
+  O4Batch* batch = nullptr;
+  int gravity = 0;
+  int device = 0;
+};
+
 namespace {
 
 int buildLevel(hc_ctx* c) {
@@ -1497,9 +1508,121 @@ int maybeAutotune(hc_ctx* c, const double* ju, cudaStream_t s) {
   return c->P.spatial_order == 2 ? autotuneStage(c, ju, s, nullptr, nullptr) : autotuneO4(c, ju, s, nullptr, nullptr);
 }
 
+// One CFL step of every member of an ensemble: the per-level sequence of
+// hc_level_advance_cfl (dtCFL, insertion schedule, four stages, seam
+// reconciliation, time) with the operator of each stage batched.
+int ensembleStep(hc_ensemble* E, double* const* ju, double* const* time, double* const* dtOut, cudaStream_t s) {
+  static const double c4[4] = {0, 0.5, 0.5, 1}, b4[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+  const int m = (int)E->members.size();
+  auto invMaxOf = [](const hc_ctx* c) { return reinterpret_cast<const double*>(c->invMax); };
+  int rc = HC_OK;
+  for (int q = 0; q < m && rc == HC_OK; ++q) {
+    hc_ctx* c = E->members[q];
+    double* tq = time ? time[q] : nullptr;
+    rc = checkLaunch(launchCfl(c->L, ju[q], c->invMax, s), "cfl");
+    if (rc == HC_OK && c->sched && tq)
+      rc = checkLaunch(launchCmeSchedule(c->sched, c->invMax, tq, c->rusanovFlag, s), "CME schedule");
+    if (rc == HC_OK)
+      rc = checkLaunch(cudaMemsetAsync(c->o4reg, 0, sizeof(double) * 6 * 2 * 2 * 8 * c->o4l.na * c->o4l.nr, s),
+                       "register");
+  }
+  for (int stage = 0; stage < 4 && rc == HC_OK; ++stage) {
+    for (int q = 0; q < m && rc == HC_OK; ++q) {
+      hc_ctx* c = E->members[q];
+      const O4StageIO io{c->o4l, stage == 0 ? ju[q] : c->o4next, c->o4cart, c->o4us, c->o4pv,
+                         StageTime{0.0, time ? time[q] : nullptr, c4[stage], invMaxOf(c), 0.0}};
+      rc = checkLaunch(launchO4Prepare(io, s), "O4 prepare");
+      if (rc == HC_OK) rc = checkLaunch(cudaMemsetAsync(c->o4k, 0, sizeof(double) * 6 * 8 * c->o4l.Nv, s), "O4 k");
+    }
+    if (rc == HC_OK && E->gravity) rc = checkLaunch(launchO4BatchGravity(E->batch, s), "O4 gravity");
+    if (rc != HC_OK) break;
+    const RegArgs rg{nullptr, b4[stage], nullptr, 0.0};  // each box carries its level's register
+    o4BatchSetVariants(E->batch, E->members[0]->o4var);
+    rc = checkLaunch(launchO4Batch(E->batch, &rg, s), "O4 operator");
+    for (int q = 0; q < m && rc == HC_OK; ++q) {
+      hc_ctx* c = E->members[q];
+      rc = checkLaunch(launchO4Update(c->o4l, stage, c->o4k, ju[q], c->acc, c->o4next, invMaxOf(c), c->P.cfl, 0.0, s),
+                       "O4 update");
+    }
+  }
+  for (int q = 0; q < m && rc == HC_OK; ++q) {
+    hc_ctx* c = E->members[q];
+    rc = checkLaunch(launchO4Reflux(c->o4l, c->L, c->o4reg, ju[q], s), "O4 reflux");
+    if (rc == HC_OK)
+      rc = checkLaunch(launchAdvanceTime(time ? time[q] : nullptr, invMaxOf(c), c->P.cfl, dtOut ? dtOut[q] : nullptr, s),
+                       "time");
+  }
+  return rc;
+}
+
 }  // namespace
 
 extern "C" {
+
+int hc_ensemble_create(hc_ctx* const* members, int m, hc_ensemble** out) {
+  if (!members || m <= 0 || !out) return fail(HC_ERR_ARG, "bad argument");
+  *out = nullptr;
+  if (m > 65535 / 6) return fail(HC_ERR_ARG, "at most 10922 levels per ensemble");
+  const hc_ctx* c0 = members[0];
+  if (!c0) return fail(HC_ERR_ARG, "null member");
+  for (int q = 0; q < m; ++q) {
+    const hc_ctx* c = members[q];
+    if (!c) return fail(HC_ERR_ARG, "null member");
+    if (c->P.spatial_order != 4) return fail(HC_ERR_UNSUPPORTED, "ensembles batch fourth-order levels only");
+    if (c->device != c0->device) return fail(HC_ERR_ARG, "ensemble members on different devices");
+    if (c->P.riemann_solver != c0->P.riemann_solver || c->P.divergence_cleaning != c0->P.divergence_cleaning ||
+        c->P.sun_gravity != c0->P.sun_gravity || c->P.berta_fallback_type != c0->P.berta_fallback_type)
+      return fail(HC_ERR_ARG, "ensemble members must share the Riemann solver, Powell, gravity and fallback");
+    for (int r = 0; r < q; ++r)
+      if (members[r] == c) return fail(HC_ERR_ARG, "a level appears twice in the ensemble");
+  }
+  std::vector<O4Args> boxes;
+  for (int q = 0; q < m; ++q) {
+    hc_ctx* c = members[q];
+    const int rc = ensureO4Buffers(c);
+    if (rc != HC_OK) return rc;
+    std::vector<O4Args> own;
+    o4SplitArgs(levelO4Args(c, c->o4us, c->o4k), own);
+    for (O4Args& a : own) {
+      a.seamReg = c->o4reg;
+      a.seamInvMax = reinterpret_cast<const double*>(c->invMax);
+      a.seamCfl = c->P.cfl;
+      boxes.push_back(a);
+    }
+  }
+  hc_ensemble* E = new (std::nothrow) hc_ensemble;
+  if (!E) return fail(HC_ERR_NOMEM, "ensemble allocation");
+  E->members.assign(members, members + m);
+  E->gravity = c0->P.sun_gravity;
+  E->device = c0->device;
+  cudaError_t e = cudaSuccess;
+  E->batch = o4BatchCreate(boxes.data(), (int)boxes.size(), &e);
+  if (!E->batch) {
+    delete E;
+    return cudaFail(e, "ensemble batch");
+  }
+  *out = E;
+  return HC_OK;
+}
+
+int hc_ensemble_advance_cfl(hc_ensemble* E, double* const* ju, int nsteps, double* const* time_dev,
+                            double* const* dt_dev, void* stream) {
+  if (!E || !ju || nsteps < 0) return fail(HC_ERR_ARG, "bad argument");
+  for (size_t q = 0; q < E->members.size(); ++q)
+    if (!ju[q]) return fail(HC_ERR_ARG, "null state");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = HC_OK;
+  for (int n = 0; n < nsteps && rc == HC_OK; ++n) rc = ensembleStep(E, ju, time_dev, dt_dev, s);
+  return rc;
+}
+
+int hc_ensemble_destroy(hc_ensemble* E) {
+  if (!E) return HC_OK;
+  cudaSetDevice(E->device);
+  o4BatchDestroy(E->batch);
+  delete E;
+  return HC_OK;
+}
 
 int hc_cone_event(const hc_cone* cone, hc_cme_event* out) {
   if (!cone || !out) return fail(HC_ERR_ARG, "null argument");

@@ -234,6 +234,13 @@ struct O4Args {
   double* face2; // [nbox][kO4FaceArrays][F]: face arrays of direction 1 (its pass overlaps its neighbours')
   double* mj;   // [nbox][V+1]
   double* kp;   // [nbox][8][V+2]
+  // The seam-flux register of the box's own level when the box runs in one
+  // launch with other levels' boxes (an ensemble): null takes the launch's
+  // RegArgs; else the face flux times (stage weight) * seamCfl / *seamInvMax
+  // is added into seamReg.
+  double* seamReg;
+  const double* seamInvMax;
+  double seamCfl;
 };
 constexpr int kO4FaceArrays = 8 * 4 + 5 + 9;  // WL, WR, FS, QD/DP (8 each) + thF, PS, BP, Bflux, Bprod + averages (8 + 1)
 

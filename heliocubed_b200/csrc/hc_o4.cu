@@ -1057,13 +1057,14 @@ __device__ __forceinline__ void chainStore(const Ctx& c, const RegArgs& rg, int 
 #pragma unroll
     for (int q = 0; q < 8; ++q) fo2[q * r0.N] = fx[q];
   }
-  if (rg.reg && d > 0) {
+  double* const reg = a.seamReg ? a.seamReg : rg.reg;
+  if (reg && d > 0) {
     const int f = d == 1 ? j : k;
     if (f == 0 || f == a.G.na) {
       const long nrna = (long)a.G.na * a.G.nr;
       const int side = f == 0 ? 0 : 1, s = d == 1 ? k : j;
-      const double w = rg.wDev ? rg.w * (rg.cfl / *rg.wDev) : rg.w;
-      double* R = rg.reg + (((long)a.block0 * 2 + (d - 1)) * 2 + side) * 8 * nrna + (long)s * a.G.nr + i;
+      const double w = a.seamReg ? rg.w * (a.seamCfl / *a.seamInvMax) : rg.wDev ? rg.w * (rg.cfl / *rg.wDev) : rg.w;
+      double* R = reg + (((long)a.block0 * 2 + (d - 1)) * 2 + side) * 8 * nrna + (long)s * a.G.nr + i;
 #pragma unroll
       for (int q = 0; q < 8; ++q) R[q * nrna] += w * fx[q];
     }

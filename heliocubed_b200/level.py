@@ -515,6 +515,48 @@ class O4Batch:
             pass
 
 
+class Ensemble:
+    """hc_ensemble: fourth-order levels of any sizes advanced together, each
+    with its own state, CFL dt, model time and insertion schedule, the stage
+    operator of all of them one batched launch per kernel.  The shells must
+    outlive the ensemble and must not step on their own while it is used."""
+
+    def __init__(self, shells: list[Shell]):
+        if not shells:
+            raise ValueError("an ensemble needs at least one level")
+        self.shells = list(shells)
+        self._lib = shells[0]._lib
+        arr = (C.c_void_p * len(shells))(*[s._ctx.value for s in shells])
+        h = C.c_void_p()
+        N.check(self._lib.hc_ensemble_create(arr, len(shells), C.byref(h)), "hc_ensemble_create")
+        self._h = h
+
+    def advance(self, states: list[torch.Tensor], nsteps: int, times: list[torch.Tensor] | None = None,
+                dts: list[torch.Tensor] | None = None) -> None:
+        """nsteps CFL steps of every level (states[q] of shells[q]; times[q]
+        and dts[q] device doubles as in Shell.advance)."""
+        m = len(self.shells)
+        if len(states) != m or (times is not None and len(times) != m) or (dts is not None and len(dts) != m):
+            raise ValueError("one state (and time, dt) per level")
+
+        def ptrs(ts):
+            return (C.c_void_p * m)(*[_ptr(t) for t in ts]) if ts is not None else None
+
+        N.check(self._lib.hc_ensemble_advance_cfl(self._h, ptrs(states), nsteps, ptrs(times), ptrs(dts), _stream()),
+                "hc_ensemble_advance_cfl")
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.hc_ensemble_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def amr_exchange_copies(boxes, ghost: int):
     """Same-panel ghost exchange of one level as region copies
     (hc_copy_box descriptors without the array pointers): for every ordered

@@ -17,7 +17,14 @@ state resident in HBM and overlaps requests on the GPU:
   shape and reused, so admission costs two kernels (wind, cone insertion)
   on the slot's stream, not a context build;
 * progress: every slot whose previous chunk has completed gets its next
-  chunk; the GPU runs the chunks of different slots concurrently.
+  chunk; the GPU runs the chunks of different slots concurrently;
+* fourth-order cohort (cobatch=True): the fourth-order requests in flight,
+  whatever their sizes, step together as one ensemble (hc_ensemble): each
+  keeps its own state, CFL dt, model time and insertion schedule, and each
+  kernel of the stage operator is one launch over all their panels.  The
+  cohort advances in chunks of min(chunk, fewest steps left) steps on its
+  own stream; between chunks finished requests leave (their results are
+  copied out) and newly admitted ones join.
 
 `run_plain` is the drop-in path beside it: the same requests one after
 another, each through the eager per-solve launches of `Shell.advance`.
@@ -34,7 +41,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-from .level import ConeSpec, InitSpec, Params, Shell, prepare_cone
+from .level import ConeSpec, Ensemble, InitSpec, Params, Shell, prepare_cone
 
 
 @dataclass
@@ -136,9 +143,10 @@ def fingerprint(state: torch.Tensor, out: torch.Tensor) -> None:
 
 
 class Slot:
-    """A pooled level context with its state buffer, stream and step graph."""
+    """A pooled level context with its state buffer, stream and step graph
+    (graph=False: no graph, for slots that step in a cohort)."""
 
-    def __init__(self, shape: tuple[int, int, int], chunk: int, device: int):
+    def __init__(self, shape: tuple[int, int, int], chunk: int, device: int, graph: bool = True):
         nr, na, order = shape
         free0 = torch.cuda.mem_get_info(device)[0]
         self.shape = shape
@@ -158,13 +166,19 @@ class Slot:
         self.shell.set_cme_schedule([])
         torch.cuda.synchronize(device)
         with torch.cuda.stream(self.stream):
-            self.graph = self.shell.capture_advance(self.state, chunk, self.time)
+            if graph:
+                self.graph = self.shell.capture_advance(self.state, chunk, self.time)
+            else:
+                # one eager step builds the stage buffers (and tunes) now
+                self.graph = None
+                self.shell.advance(self.state, 1, self.time)
         torch.cuda.synchronize(device)
         self.bytes = max(0, free0 - torch.cuda.mem_get_info(device)[0])
         self.req: Request | None = None
         self.left = 0
         self.event: torch.cuda.Event | None = None
         self.t_start = 0.0
+        self.in_cohort = False
 
     def start(self, req: Request, now: float) -> None:
         self.req = req
@@ -178,12 +192,13 @@ class Slot:
         """Enqueue the next chunk (a graph replay, or the eager remainder);
         with no steps left, the copy of the result to the host."""
         with torch.cuda.stream(self.stream):
-            if self.left >= self.chunk:
+            if self.left >= self.chunk and self.graph is not None:
                 self.graph.replay()
                 self.left -= self.chunk
             elif self.left > 0:
-                self.shell.advance(self.state, self.left, self.time)
-                self.left = 0
+                steps = self.left if self.graph is not None else min(self.left, self.chunk)
+                self.shell.advance(self.state, steps, self.time)
+                self.left -= steps
             else:
                 self.host_out.copy_(self.state, non_blocking=True)
                 self.host_time.copy_(self.time, non_blocking=True)
@@ -193,6 +208,88 @@ class Slot:
                 self.left = -1
             self.event = torch.cuda.Event()
             self.event.record(self.stream)
+
+
+class Cohort:
+    """The fourth-order slots in flight, stepped together as an ensemble on
+    one stream (see the module docstring).  Ensembles are kept by their
+    member slots (slots are pooled, so a membership can recur) until
+    close(): freeing device memory mid-run would synchronise the GPU.  The
+    device calls go through the methods at the end of the class."""
+
+    def __init__(self, chunk: int, device: int):
+        self.chunk = chunk
+        self.device = device
+        self.stream = self._new_stream()
+        self.members: list[Slot] = []
+        self.joining: list[tuple[Slot, object]] = []
+        self.event = None
+        self.ensembles: dict[tuple[int, ...], object] = {}
+        self.chunk_steps = 0  # steps of all launched chunks (each step: one operator launch group per stage)
+
+    def join(self, slot: Slot) -> None:
+        """Take an admitted slot (its admission is on the slot's stream)."""
+        slot.in_cohort = True
+        self.joining.append((slot, self._record(slot.stream)))
+
+    def progress(self) -> bool:
+        """Once the running chunk has completed: hand finished members their
+        result copy, take in the joining slots and launch the next chunk.
+        True when anything was done."""
+        if self.event is not None and not self.event.query():
+            return False
+        if not self.members and not self.joining:
+            return False
+        for slot in [s for s in self.members if s.left == 0]:
+            self._wait(slot.stream, self.event)
+            slot.in_cohort = False
+            slot.issue()  # the copy of the result, on the slot's own stream
+        self.members = [s for s in self.members if s.left > 0]
+        for slot, admitted in self.joining:
+            self._wait(self.stream, admitted)
+            self.members.append(slot)
+        self.joining = []
+        self.event = None
+        if not self.members:
+            return True
+        steps = min(self.chunk, min(s.left for s in self.members))
+        key = tuple(id(s) for s in self.members)
+        ens = self.ensembles.get(key)
+        if ens is None:
+            ens = self.ensembles[key] = self._ensemble(self.members)
+        self._advance(ens, self.members, steps)
+        self.chunk_steps += steps
+        for s in self.members:
+            s.left -= steps
+        self.event = self._record(self.stream)
+        return True
+
+    def close(self) -> None:
+        for ens in self.ensembles.values():
+            ens.close()
+        self.ensembles.clear()
+
+    # device calls
+    def _new_stream(self):
+        return torch.cuda.Stream(device=self.device)
+
+    @staticmethod
+    def _record(stream):
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        return ev
+
+    @staticmethod
+    def _wait(stream, event) -> None:
+        stream.wait_event(event)
+
+    @staticmethod
+    def _ensemble(slots: list[Slot]):
+        return Ensemble([s.shell for s in slots])
+
+    def _advance(self, ens, slots: list[Slot], steps: int) -> None:
+        with torch.cuda.stream(self.stream):
+            ens.advance([s.state for s in slots], steps, [s.time for s in slots])
 
 
 @dataclass
@@ -221,8 +318,9 @@ class EnsembleServer:
     """Continuous-batching server over pooled slots (see module docstring)."""
 
     def __init__(self, hbm_budget: float, max_inflight: int = 8, chunk: int = 10, device: int | None = None,
-                 keep_states: bool = True):
+                 keep_states: bool = True, cobatch: bool = True):
         self.keep_states = keep_states
+        self.cobatch = cobatch
         self.budget = hbm_budget
         self.max_inflight = max_inflight
         self.chunk = chunk
@@ -230,6 +328,7 @@ class EnsembleServer:
         self.pool: dict[tuple, list[Slot]] = {}
         self.slot_bytes: dict[tuple, int] = {}
         self.in_use = 0.0
+        self.cohort: Cohort | None = None  # built when the first fourth-order request joins
 
     @staticmethod
     def shape(req: Request) -> tuple[int, int, int]:
@@ -239,7 +338,7 @@ class EnsembleServer:
         """Build slots ahead of time (contexts, buffers, graphs)."""
         for shp in sorted({self.shape(r) for r in requests}):
             for _ in range(per_shape - len(self.pool.get(shp, []))):
-                s = Slot(shp, self.chunk, self.device)
+                s = self._new_slot(shp)
                 self.pool.setdefault(shp, []).append(s)
                 self.slot_bytes[shp] = s.bytes
 
@@ -260,13 +359,16 @@ class EnsembleServer:
         per_cell = [b / (6 * s[0] * s[1] * s[1]) for s, b in self.slot_bytes.items() if s[2] == order]
         return int(cells * (max(per_cell) if per_cell else self.BYTES_PER_CELL_GUESS.get(order, 64 * 40)))
 
+    def _new_slot(self, shp: tuple[int, int, int]) -> Slot:
+        return Slot(shp, self.chunk, self.device, graph=not (self.cobatch and shp[2] == 4))
+
     def _acquire(self, req: Request) -> Slot | None:
         shp = self.shape(req)
         need = self.estimate_bytes(shp)
         if self.in_use + need > self.budget:
             return None
         idle = self.pool.setdefault(shp, [])
-        slot = idle.pop() if idle else Slot(shp, self.chunk, self.device)
+        slot = idle.pop() if idle else self._new_slot(shp)
         self.slot_bytes[shp] = max(self.slot_bytes.get(shp, 0), slot.bytes)
         self.in_use += self.slot_bytes[shp]
         return slot
@@ -301,10 +403,17 @@ class EnsembleServer:
                 req = pending.pop(0)
                 slot.fingerprint = not self.keep_states
                 slot.start(req, now)
-                slot.issue()
+                if self.cobatch and req.order == 4 and req.steps > 0:
+                    if self.cohort is None:
+                        self.cohort = Cohort(self.chunk, self.device)
+                    self.cohort.join(slot)
+                else:
+                    slot.issue()
                 active.append(slot)
-            progressed = False
+            progressed = self.cohort.progress() if self.cohort is not None else False
             for slot in list(active):
+                if slot.in_cohort:
+                    continue
                 if slot.event is not None and not slot.event.query():
                     continue
                 progressed = True
@@ -326,7 +435,10 @@ class EnsembleServer:
 
 
     def close(self) -> None:
-        """Release every pooled slot (contexts, buffers, graphs)."""
+        """Release every pooled slot (contexts, buffers, graphs) and the
+        cohort's ensembles."""
+        if self.cohort is not None:
+            self.cohort.close()
         for slots in self.pool.values():
             for slot in slots:
                 slot.graph = None

@@ -169,6 +169,31 @@ int hc_o4_batch_rhs(hc_ctx* ctx, hc_o4_batch* batch, void* stream);
 
 int hc_o4_batch_destroy(hc_o4_batch* batch);
 
+/* An ensemble: several fourth-order levels (contexts of any sizes sharing
+ * the Riemann solver, Powell, gravity and WENO fallback settings) advanced
+ * together, one CFL step each per call step.  Each level keeps its own
+ * state, dt, model time, insertion schedule and seam register; the stage
+ * operator of all levels' panels is one batch, so every operator kernel is
+ * one launch for the ensemble.  The results equal those of
+ * hc_level_advance_cfl on each level alone, bit for bit.  The member
+ * contexts must outlive the ensemble and must not step on their own while
+ * it runs (they share their stage buffers with it).  Replaces running the
+ * reference's per-solve step loop (exec/main.cpp:369-497) once per served
+ * request; the reference has no ensemble batching. */
+typedef struct hc_ensemble hc_ensemble;
+
+int hc_ensemble_create(hc_ctx* const* members, int m, hc_ensemble** out);
+
+/* nsteps steps of every member: ju[q] is member q's state; time_dev[q] and
+ * dt_dev[q] as in hc_level_advance_cfl (time_dev and dt_dev may be NULL,
+ * or hold NULL entries).  No host synchronisation, no allocation: may be
+ * captured in a CUDA graph. */
+int hc_ensemble_advance_cfl(hc_ensemble* ens, double* const* ju, int nsteps,
+                            double* const* time_dev, double* const* dt_dev,
+                            void* stream);
+
+int hc_ensemble_destroy(hc_ensemble* ens);
+
 /* Solar gravity at fourth order on native averages, rhs[valid] += source
  * (fourth-order cell and face products of dr/dxi, <rho>, <rho V_r> and the
  * averaged metrics; context created with spatial_order 4).  usph lives on

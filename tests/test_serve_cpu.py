@@ -9,6 +9,7 @@ completes each issued chunk after a fixed wall time, so the scheduler runs
 exactly as it does over CUDA streams."""
 import threading
 import time
+import types
 
 import numpy as np
 import pytest
@@ -33,7 +34,7 @@ class FakeSlot:
     lock = threading.Lock()
     bytes_per_cell = 64.0
 
-    def __init__(self, shape, chunk, device):
+    def __init__(self, shape, chunk, device, graph=True):
         nr, na, _ = shape
         self.shape = shape
         self.chunk = chunk
@@ -44,6 +45,10 @@ class FakeSlot:
         self.t_start = 0.0
         self.host_out = None
         self.host_time = None
+        self.in_cohort = False
+        self.stream = None
+        self.graph = None
+        self.shell = types.SimpleNamespace(close=lambda: None)
         FakeSlot.built += 1
 
     def start(self, req, now):
@@ -180,3 +185,78 @@ def test_unseen_shape_admitted_by_estimate(fake_slots):
     # waits for one of them instead of being built past the budget
     assert res[2].t_start >= min(res[0].t_done, res[1].t_done) - 1e-3
     assert all(r.error is None for r in res.values())
+
+
+class FakeEnsemble:
+    def __init__(self, rids):
+        self.rids = rids
+        self.closed = False
+
+    def close(self):
+        self.closed = True
+
+
+class FakeCohort(serve.Cohort):
+    """serve.Cohort with its device calls simulated: a chunk completes
+    CHUNK_S after its launch, admissions at once."""
+    launches = []
+    built = []
+
+    def _new_stream(self):
+        return "cohort"
+
+    @staticmethod
+    def _record(stream):
+        return FakeEvent(time.perf_counter() + (CHUNK_S if stream == "cohort" else 0.0))
+
+    @staticmethod
+    def _wait(stream, event):
+        assert event.query()  # the scheduler waits only on completed work
+
+    @staticmethod
+    def _ensemble(slots):
+        ens = FakeEnsemble(tuple(s.req.rid for s in slots))
+        FakeCohort.built.append(ens)
+        return ens
+
+    def _advance(self, ens, slots, steps):
+        FakeCohort.launches.append(([s.req.rid for s in slots], steps, [s.left for s in slots]))
+
+
+def test_fourth_order_requests_step_as_one_cohort(fake_slots, monkeypatch):
+    """Fourth-order requests of different sizes step together in chunks of
+    min(chunk, fewest steps left); one that finishes leaves with its result,
+    a late arrival joins at a chunk boundary; second-order requests keep
+    their own slots; every request gets exactly its steps."""
+    FakeCohort.launches, FakeCohort.built = [], []
+    monkeypatch.setattr(serve, "Cohort", FakeCohort)
+    reqs = [serve.Request(0, 8, 8, 4, 45, 0.0), serve.Request(1, 16, 8, 4, 15, 0.0),
+            serve.Request(2, 8, 8, 2, 20, 0.0), serve.Request(3, 8, 8, 4, 10, 0.006)]
+    srv = serve.EnsembleServer(hbm_budget=1e18, max_inflight=8, chunk=10, device=0)
+    srv.warm(reqs, per_shape=2)
+    res = {r.rid: r for r in srv.run(reqs)}
+    assert sorted(res) == [0, 1, 2, 3]
+    assert all(r.state[0] == r.rid and r.model_time == r.steps for r in res.values())
+    stepped = {0: 0, 1: 0, 3: 0}
+    for rids, steps, left in FakeCohort.launches:
+        assert 2 not in rids                       # second order never joins
+        assert steps == min(10, min(left))         # lockstep chunk
+        for rid in rids:
+            stepped[rid] += steps
+    assert stepped == {0: 45, 1: 15, 3: 10}
+    assert FakeCohort.launches[0][0] == [0, 1]     # both arrivals at t = 0 start together
+    assert any(3 in rids and 0 in rids for rids, _, _ in FakeCohort.launches)  # the late one joined
+    assert len(FakeCohort.built) == len({tuple(r) for r, _, _ in FakeCohort.launches})
+    srv.close()
+    assert all(e.closed for e in FakeCohort.built)
+    assert srv.in_use == 0
+
+
+def test_cobatch_off_keeps_per_slot_chunks(fake_slots, monkeypatch):
+    FakeCohort.launches = []
+    monkeypatch.setattr(serve, "Cohort", FakeCohort)
+    reqs = [serve.Request(0, 8, 8, 4, 20, 0.0), serve.Request(1, 8, 8, 4, 20, 0.0)]
+    srv = serve.EnsembleServer(hbm_budget=1e18, max_inflight=8, chunk=10, device=0, cobatch=False)
+    srv.warm(reqs, per_shape=2)
+    res = srv.run(reqs)
+    assert len(res) == 2 and FakeCohort.launches == []

@@ -596,7 +596,7 @@ def run_serve(args, world, rank, local):
     # `chunk` steps), built before the timed runs as a long-running server has them
     chunk = max(1, min(10, args.steps))
     server = serve.EnsembleServer(hbm_budget=args.serve_budget_gb * 1e9, max_inflight=args.serve_inflight,
-                                  chunk=chunk, device=local, keep_states=False)
+                                  chunk=chunk, device=local, keep_states=False, cobatch=not args.no_cobatch)
     for shp in shapes:
         server.warm([r for r in reqs if (r.nr, r.na, r.order) == shp], per_shape=min(counts[shp], 3))
     torch.cuda.synchronize()
@@ -963,6 +963,8 @@ def main() -> int:
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-inflight", type=int, default=8)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
+    ap.add_argument("--no-cobatch", action="store_true",
+                    help="serve: fourth-order requests on their own streams instead of one cohort")
     args = ap.parse_args()
     # --order, --nr, --na or --init cone without --workload select the uniform workload
     uniform_opts = args.order is not None or args.nr is not None or args.na is not None or args.init != "default"

@@ -62,6 +62,11 @@ SIGNATURES = {
     "hc_amr_copy": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_amr_cf_mapped": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
     "hc_amr_cf_quotient": (C.c_int, [_VP, _VP, C.c_int, C.c_int, _VP]),
+    "hc_amr_plan_set_native": (C.c_int, [_VP, _VP, C.c_int]),
+    "hc_level_cartesian_size": (C.c_size_t, [_VP]),
+    "hc_level_prepare_cartesian": (C.c_int, [_VP, _VP, _VP, _VP, C.c_double, _VP]),
+    "hc_level_rhs_fluxes": (C.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "hc_amr_native": (C.c_int, [_VP, _VP, C.c_int, C.c_int, C.c_double, _VP]),
     "hc_ctx_set_o4_variants": (C.c_int, [_VP, _VP]),
     "hc_level_insert_cone": (C.c_int, [_VP, _VP, C.c_double, _VP, _VP, _VP]),
     "hc_cone_event": (C.c_int, [_VP, _VP]),
@@ -162,6 +167,12 @@ class HcCfFineBox(C.Structure):
                 ("mapped_lo", C.c_int * 3), ("mapped_n", C.c_int * 3), ("out_lo", C.c_int * 3),
                 ("out_n", C.c_int * 3), ("valid_lo", C.c_int * 3), ("valid_hi", C.c_int * 3),
                 ("block_lo", C.c_int * 3), ("block_hi", C.c_int * 3)]
+
+
+class HcNativeBox(C.Structure):
+    """Mirror of hc_native_box in include/hc_abi.h."""
+    _fields_ = [("cart", C.c_void_p), ("usph", C.c_void_p), ("cart_lo", C.c_int * 3), ("cart_n", C.c_int * 3),
+                ("usph_lo", C.c_int * 3), ("usph_n", C.c_int * 3), ("block", C.c_int)]
 
 
 class HcCmeEvent(C.Structure):

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/hc_abi.h"
+#include "hc_device.cuh"
 #include "hc_level.h"
 
 namespace {
@@ -354,6 +355,11 @@ static bool refluxInside(const hc_reflux_box& R) {
 }
 
 struct hc_amr_plan {
+  hc_native_box* natives = nullptr;     // fine boxes of the native conversion (device)
+  Chunk* nativeChunks = nullptr;
+  std::vector<hc_native_box> nativeHost;
+  std::vector<int> nativeStart;
+  mutable std::vector<std::pair<int, int>> nativeRangesChecked;  // ranges checked against a level
   hc_rk_box* boxes = nullptr;           // device copy
   hc_restrict_box* restricts = nullptr; // device copy
   hc_reflux_box* reflux = nullptr;      // device copy
@@ -458,6 +464,8 @@ extern "C" int hc_amr_plan_create(hc_ctx* ctx, const hc_rk_box* boxes, int nbox,
 
 extern "C" int hc_amr_plan_destroy(hc_amr_plan* P) {
   if (!P) return HC_OK;
+  cudaFree(P->natives);
+  cudaFree(P->nativeChunks);
   cudaFree(P->boxes);
   cudaFree(P->restricts);
   cudaFree(P->boxChunks);
@@ -868,6 +876,149 @@ extern "C" int hc_amr_cf_mapped(hc_ctx* ctx, const hc_amr_plan* P, int first, in
 
 extern "C" int hc_amr_cf_quotient(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, void* stream) {
   return cfFineLaunch(ctx, P, first, count, stream, false);
+}
+
+// ---------------------------------------------------------------------------
+// Native conversion and radial ghosts of fine boxes (the level's stage
+// preparation, step 3, on boxes).
+namespace {
+
+__device__ __forceinline__ long nbOff(const int lo[3], const int n[3], int i, int j, int k) {
+  return (long)(i - lo[0]) + (long)n[0] * ((long)(j - lo[1]) + (long)n[1] * (long)(k - lo[2]));
+}
+
+__global__ void __launch_bounds__(kThreads, 2) nativeBoxKernel(const hc::O4Level O, const hc_native_box* __restrict__ boxes,
+                                                            const Chunk* __restrict__ chunks, double t) {
+  const Chunk ch = chunks[blockIdx.x];
+  const hc_native_box B = boxes[ch.item];
+  const long NU = (long)B.usph_n[0] * B.usph_n[1] * B.usph_n[2];
+  const long NC = (long)B.cart_n[0] * B.cart_n[1] * B.cart_n[2];
+  const int b = B.block;
+  for (long long e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
+    long r = (long)e;
+    const int i = B.usph_lo[0] + (int)(r % B.usph_n[0]);
+    r /= B.usph_n[0];
+    const int j = B.usph_lo[1] + (int)(r % B.usph_n[1]);
+    const int k = B.usph_lo[2] + (int)(r / B.usph_n[1]);
+    double u[8];
+    auto native = [&](int ii, double out[8]) {
+      hc::o4NativeCore(B.cart + nbOff(B.cart_lo, B.cart_n, ii, j, k), B.cart_n[0], (long)B.cart_n[0] * B.cart_n[1], NC,
+                   O.coef + (((long)b * O.nA + (k + O.ga)) * O.nA + (j + O.ga)) * 27, 27, 27L * O.nA, out);
+    };
+    if (i < 0) {
+      const long cell = ((long)b * O.nG + (k + O.g)) * O.nG + (j + O.g);
+      if (O.inner) {
+        const double* w = O.inner + (cell * O.g + (i + O.g)) * 8;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) u[c] = w[c];
+      } else {
+        const double* xh = O.xhat + cell * 3;
+        const double radius = O.radial[i + O.g + 1].y;
+        const double X[3] = {radius * xh[0], radius * xh[1], radius * xh[2]};
+        hc::windConserved(O.gamma, O.r0, O.strength, X, t, u);
+      }
+    } else if (i < O.nr) {
+      native(i, u);
+    } else {
+      native(O.nr - 1, u);
+      const double rl = O.radial[O.nr - 1 + O.g + 1].y, rr = O.radial[i + O.g + 1].y;
+      const double s2 = pow(rl / rr, 2.0), s1 = pow(rl / rr, 1.0);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) u[c] *= c < 6 ? s2 : s1;
+    }
+    double* o = B.usph + nbOff(B.usph_lo, B.usph_n, i, j, k);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) o[c * NU] = u[c];
+  }
+}
+
+bool nativeShapeOk(const hc_native_box& B) {
+  if (!B.cart || !B.usph || B.block < 0 || B.block > 5) return false;
+  long long nu = 1, nc = 1;
+  for (int d = 0; d < 3; ++d) {
+    if (B.usph_n[d] < 1 || B.cart_n[d] < 1) return false;
+    nu *= B.usph_n[d];
+    nc *= B.cart_n[d];
+  }
+  return 8 * nu < 0x7fffffffLL && 8 * nc < 0x7fffffffLL;
+}
+
+// The box against the level: usph cells inside the tables' range, the cart
+// box holding every cell the conversion reads.
+bool nativeFits(const hc_native_box& B, const hc::O4Level& O) {
+  const int ulo0 = B.usph_lo[0], uhi0 = B.usph_lo[0] + B.usph_n[0] - 1;
+  for (int d = 1; d < 3; ++d)
+    if (B.usph_lo[d] < -O.g || B.usph_lo[d] + B.usph_n[d] > O.na + O.g) return false;
+  if (ulo0 < -O.g || uhi0 >= O.nr + O.g) return false;
+  const int i0 = ulo0 < 0 ? 0 : ulo0, i1 = uhi0 >= O.nr ? O.nr - 1 : uhi0;
+  if (uhi0 < 0) return true;  // inner ghosts only
+  const int need_lo[3] = {uhi0 >= O.nr && ulo0 >= O.nr ? O.nr - 1 : i0, B.usph_lo[1] - 1, B.usph_lo[2] - 1};
+  const int need_hi[3] = {i1, B.usph_lo[1] + B.usph_n[1], B.usph_lo[2] + B.usph_n[2]};
+  for (int d = 0; d < 3; ++d)
+    if (need_lo[d] < B.cart_lo[d] || need_hi[d] > B.cart_lo[d] + B.cart_n[d] - 1) return false;
+  return true;
+}
+
+}  // namespace
+
+extern "C" int hc_amr_plan_set_native(hc_amr_plan* P, const hc_native_box* boxes, int nbox) {
+  if (!P || nbox < 0 || (nbox && !boxes)) return argFail("hc_amr_plan_set_native: bad argument");
+  std::vector<Chunk> ch;
+  std::vector<int> st;
+  for (int b = 0; b < nbox; ++b) {
+    if (!nativeShapeOk(boxes[b]))
+      return argFail("hc_amr_plan_set_native: a box needs cart and usph arrays, a block 0..5 and non-empty boxes");
+    st.push_back((int)ch.size());
+    addChunks(ch, b, (long long)boxes[b].usph_n[0] * boxes[b].usph_n[1] * boxes[b].usph_n[2]);
+  }
+  st.push_back((int)ch.size());
+  hc_native_box* dev = nullptr;
+  Chunk* devC = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (nbox) {
+    e = cudaMalloc(&dev, sizeof(hc_native_box) * nbox);
+    if (e == cudaSuccess) e = cudaMemcpy(dev, boxes, sizeof(hc_native_box) * nbox, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&devC, sizeof(Chunk) * ch.size());
+    if (e == cudaSuccess) e = cudaMemcpy(devC, ch.data(), sizeof(Chunk) * ch.size(), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(dev);
+    cudaFree(devC);
+    return cudaFailed(e, "hc_amr_plan_set_native");
+  }
+  cudaFree(P->natives);
+  cudaFree(P->nativeChunks);
+  P->natives = dev;
+  P->nativeChunks = devC;
+  P->nativeHost.assign(boxes, boxes + nbox);
+  P->nativeStart = st;
+  P->nativeRangesChecked.clear();
+  return HC_OK;
+}
+
+extern "C" int hc_amr_native(hc_ctx* ctx, const hc_amr_plan* P, int first, int count, double t, void* stream) {
+  if (!ctx || !P) return argFail("hc_amr_native: null argument");
+  const hc::O4Level* O = hc::ctxO4Level(ctx);
+  if (!O) return hc::setLastError(HC_ERR_UNSUPPORTED, "hc_amr_native: the context is not fourth order");
+  const int n = (int)P->nativeHost.size();
+  if (first < 0 || count < 0 || first + count > n) return argFail("hc_amr_native: range outside the plan");
+  const std::pair<int, int> range{first, count};
+  if (std::find(P->nativeRangesChecked.begin(), P->nativeRangesChecked.end(), range) == P->nativeRangesChecked.end()) {
+    for (int a = first; a < first + count; ++a) {
+      if (!nativeFits(P->nativeHost[a], *O))
+        return argFail("hc_amr_native: a usph box leaves the level's tables or its cart box misses cells the "
+                       "conversion reads");
+      for (int b = a + 1; b < first + count; ++b)
+        if (P->nativeHost[a].usph == P->nativeHost[b].usph)
+          return argFail("hc_amr_native: two boxes of one launch write the same array");
+    }
+    P->nativeRangesChecked.push_back(range);
+  }
+  const int c0 = count ? P->nativeStart[first] : 0, c1 = count ? P->nativeStart[first + count] : 0;
+  if (c1 == c0) return HC_OK;
+  nativeBoxKernel<<<c1 - c0, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(*O, P->natives,
+                                                                                P->nativeChunks + c0, t);
+  return cudaFailed(cudaGetLastError(), "hc_amr_native");
 }
 
 // ---------------------------------------------------------------------------

@@ -1021,6 +1021,7 @@ namespace hc {
 const DevLevel* ctxLevel(const hc_ctx* c) { return &c->L; }
 const hc_params* ctxParams(const hc_ctx* c) { return &c->P; }
 int ctxDevice(const hc_ctx* c) { return c->device; }
+const O4Level* ctxO4Level(const hc_ctx* c) { return c->P.spatial_order == 4 ? &c->o4l : nullptr; }
 int setLastError(int code, const char* msg) { return fail(code, msg); }
 }  // namespace hc
 
@@ -1310,6 +1311,44 @@ int hc_level_prepare(hc_ctx* c, const double* ju, double* w, double t, void* str
   if (rc != HC_OK) return rc;
   StageTime st{t, nullptr, 0.0, nullptr, 0.0};
   return checkLaunch(launchGhosts(c->L, w, st, s), "ghosts");
+}
+
+size_t hc_level_cartesian_size(const hc_ctx* c) {
+  return c && c->P.spatial_order == 4 ? (size_t)6 * NC * c->o4l.Nc : 0;
+}
+
+int hc_level_prepare_cartesian(hc_ctx* c, const double* ju, double* w, double* cart, double t, void* stream) {
+  if (!c || !ju || !w || !cart) return fail(HC_ERR_ARG, "null argument");
+  if (c->P.spatial_order != 4) return fail(HC_ERR_UNSUPPORTED, "context was created with spatial_order != 4");
+  const int rc4 = ensureO4Buffers(c);
+  if (rc4 != HC_OK) return rc4;
+  O4StageIO io{c->o4l, ju, cart, w, c->o4pv, StageTime{t, nullptr, 0.0, nullptr, 0.0}};
+  return checkLaunch(launchO4Prepare(io, (cudaStream_t)stream), "O4 prepare");
+}
+
+int hc_level_rhs_fluxes(hc_ctx* c, const double* w, double* k, double* const* flux, void* stream) {
+  if (!c || !w || !k) return fail(HC_ERR_ARG, "null argument");
+  if (c->P.spatial_order != 4) return fail(HC_ERR_UNSUPPORTED, "context was created with spatial_order != 4");
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = ensureO4Buffers(c);
+  if (rc != HC_OK) return rc;
+  O4Args args = levelO4Args(c, w, k);
+  for (int d = 0; d < 3; ++d) args.flux[d] = flux ? flux[d] : nullptr;
+  O4Batch* B = cachedBatch(c, args, &rc);
+  if (!B) return rc;
+  const O4Level& O = c->o4l;
+  rc = checkLaunch(cudaMemsetAsync(k, 0, sizeof(double) * 6 * NC * O.Nv, s), "O4 k");
+  if (rc == HC_OK)
+    rc = checkLaunch(cudaMemsetAsync(c->o4reg, 0, sizeof(double) * 6 * 2 * 2 * 8 * O.na * O.nr, s), "register");
+  if (rc == HC_OK && c->P.sun_gravity) rc = checkLaunch(launchO4BatchGravity(B, s), "O4 gravity");
+  if (rc != HC_OK) return rc;
+  // this evaluation's seam fluxes (weight 1) into the register, then each
+  // seam face's rhs takes the mean of both panels' fluxes
+  const RegArgs rg{c->o4reg, 1.0, nullptr, c->P.cfl};
+  o4BatchSetVariants(B, c->o4var);
+  rc = checkLaunch(launchO4Batch(B, &rg, s), "O4 operator");
+  if (rc == HC_OK) rc = checkLaunch(launchO4Reflux(O, c->L, c->o4reg, k, s), "O4 seam reconciliation");
+  return rc;
 }
 
 int hc_level_rhs(hc_ctx* c, const double* w, double* k, void* stream) {

@@ -420,4 +420,65 @@ HC_DEV void windConserved(double gam, double r_BC, double strength, const double
   u[4] = p / (gam - 1.0) + 0.5 * u[0] * umag * umag + 0.0 / 8.0 / kPi;
 }
 
+// Native averages of one cell from fourth-order Cartesian averages
+// (src/MHD_CachedCartesianConversion.H:65-124): c0 points at the cell's
+// component 0 (neighbours j +- 1 at +-sj, k +- 1 at +-sk, components sc
+// apart); cf at the cell's 27 conversion coefficients (<A>^-1, D1 <A>,
+// D2 <A>), the neighbours' at +-cj, +-ck.
+HC_DEV void o4NativeCore(const double* c0, long sj, long sk, long sc, const double* cf,
+                         long cj, long ck, double out[8]) {
+  out[0] = c0[0];
+  out[4] = c0[4 * sc];
+  const long nOff[4] = {sj, -sj, sk, -sk};
+  const long cOff[4] = {cj, -cj, ck, -ck};
+#pragma unroll
+  for (int grp = 0; grp < 2; ++grp) {
+    const int st = grp == 0 ? 1 : 5;
+    const double* cs = c0 + st * sc;
+    double q[4][3];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const double* I = cf + cOff[e];
+      const double* x = cs + nOff[e];
+      const double x0 = x[0];
+      const double x1 = x[sc];
+      const double x2 = x[2 * sc];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        double v = 0.0;
+        v += I[3 * r] * x0 * 1.0;
+        v += I[3 * r + 1] * x1 * 1.0;
+        v += I[3 * r + 2] * x2 * 1.0;
+        q[e][r] = v;
+      }
+    }
+    double d1[3], d2[3], corrected[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      d1[r] = 0.5 * (q[0][r] - q[1][r]);
+      d2[r] = 0.5 * (q[2][r] - q[3][r]);
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      double first = 0.0, second = 0.0;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        first += cf[9 + 3 * r + s] * d1[s] * (-1.0 / 12.0);
+        second += cf[18 + 3 * r + s] * d2[s] * (-1.0 / 12.0);
+      }
+      double correction = 0.0;
+      correction += first;
+      correction += second;
+      corrected[r] = cs[r * sc] + correction;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      double v = 0.0;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) v += cf[3 * r + s] * corrected[s] * 1.0;
+      out[st + r] = v;
+    }
+  }
+}
+
 }  // namespace hc

@@ -338,5 +338,7 @@ namespace hc {
 const DevLevel* ctxLevel(const hc_ctx* c);
 const hc_params* ctxParams(const hc_ctx* c);
 int ctxDevice(const hc_ctx* c);
+// The fourth-order level tables of an order-4 context (null otherwise).
+const O4Level* ctxO4Level(const hc_ctx* c);
 int setLastError(int code, const char* msg);
 }  // namespace hc

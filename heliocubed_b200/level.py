@@ -399,6 +399,24 @@ class Shell:
         N.check(self._lib.hc_level_rhs(self._ctx, _ptr(w), _ptr(k), _stream()), "hc_level_rhs")
         return k
 
+    def prepare_cartesian(self, ju: torch.Tensor, t: float = 0.0, w: torch.Tensor | None = None,
+                          cart: torch.Tensor | None = None) -> tuple[torch.Tensor, torch.Tensor]:
+        """Fourth order: hc_level_prepare keeping the Cartesian averages
+        (hc_level_prepare_cartesian); returns (w, cart)."""
+        w = self.new_primitive() if w is None else w
+        if cart is None:
+            cart = torch.empty(int(self._lib.hc_level_cartesian_size(self._ctx)), dtype=torch.float64,
+                               device=self._dev)
+        N.check(self._lib.hc_level_prepare_cartesian(self._ctx, _ptr(ju), _ptr(w), _ptr(cart), t, _stream()),
+                "hc_level_prepare_cartesian")
+        return w, cart
+
+    def rhs_fluxes(self, w: torch.Tensor, k: torch.Tensor, fluxes=None) -> None:
+        """Fourth order: the AMR level evaluation (hc_level_rhs_fluxes): k
+        with the panel seams reconciled, fluxes[d] each panel's face fluxes."""
+        arr = (C.c_void_p * 3)(*[_ptr(f) if f is not None else None for f in fluxes]) if fluxes is not None else None
+        N.check(self._lib.hc_level_rhs_fluxes(self._ctx, _ptr(w), _ptr(k), arr, _stream()), "hc_level_rhs_fluxes")
+
     def rk4_step(self, ju: torch.Tensor, dt: float, t: float = 0.0) -> None:
         N.check(self._lib.hc_level_rk4_step(self._ctx, _ptr(ju), dt, t, _stream()), "hc_level_rk4_step")
 
@@ -701,6 +719,24 @@ class AmrPlan:
     def cf_quotient(self, first: int, count: int) -> None:
         N.check(self._lib.hc_amr_cf_quotient(self._shell._ctx, self._h, first, count, _stream()),
                 "hc_amr_cf_quotient")
+
+    def set_native(self, boxes) -> None:
+        """boxes: dicts with cart and usph (device tensors), cart_lo, cart_n,
+        usph_lo, usph_n (3 ints each) and block (hc_native_box)."""
+        n = len(boxes)
+        arr = (N.HcNativeBox * max(n, 1))()
+        for b, d in enumerate(boxes):
+            arr[b].cart = d["cart"].data_ptr()
+            arr[b].usph = d["usph"].data_ptr()
+            for k in ("cart_lo", "cart_n", "usph_lo", "usph_n"):
+                getattr(arr[b], k)[:] = list(d[k])
+            arr[b].block = d["block"]
+        N.check(self._lib.hc_amr_plan_set_native(self._h, arr, n), "hc_amr_plan_set_native")
+
+    def native(self, first: int, count: int, t: float) -> None:
+        """Native averages and radial ghosts of boxes first .. first+count-1
+        at time t, with the geometry of this plan's shell (hc_amr_native)."""
+        N.check(self._lib.hc_amr_native(self._shell._ctx, self._h, first, count, t, _stream()), "hc_amr_native")
 
     def close(self) -> None:
         if self._h:

@@ -221,6 +221,27 @@ int hc_level_prepare(hc_ctx* ctx, const double* ju, double* w, double t,
  * preStageLevel plus StageLevel (src/BoxOp_EulerCubedSphereImplem.H:961-1012). */
 int hc_level_rhs(hc_ctx* ctx, const double* w, double* k, void* stream);
 
+/* The AMR form of a fourth-order level's stage preparation and evaluation
+ * (CubedSphereAMR::prepare and evaluate on a level that covers the shell,
+ * src/MHD_AMR.H:1417-1499):
+ *
+ * hc_level_prepare_cartesian is hc_level_prepare that also keeps the
+ * level's fourth-order Cartesian averages (with their panel-seam ghosts) in
+ * the caller's cart, hc_level_cartesian_size doubles: [6][8][na+12][na+12]
+ * [nr], panel b's box (0, -6, -6) .. (nr-1, na+5, na+5), the coarse data a
+ * finer level interpolates its ghosts from.
+ *
+ * hc_level_rhs_fluxes is hc_level_rhs evaluated as the AMR level
+ * evaluation does it: every panel-seam face of k takes the mean of both
+ * panels' fluxes at once (the per-stage panel flux register reflux), and
+ * flux[d] (each may be NULL), [6][8][faces of valid.extrude(d)], receives
+ * every panel's own face fluxes for the coarse-fine registers. */
+size_t hc_level_cartesian_size(const hc_ctx* ctx);
+int hc_level_prepare_cartesian(hc_ctx* ctx, const double* ju, double* w,
+                               double* cart, double t, void* stream);
+int hc_level_rhs_fluxes(hc_ctx* ctx, const double* w, double* k,
+                        double* const* flux, void* stream);
+
 /* One classical RK4 step of the level in place, with dt from host.
  * Replaces MBLevelRK::advance(order 4) (src/MHD_LevelRK.H:22-61, tableau
  * src/MHD_AMRRungeKutta.H:10-12).  At spatial order 4 the panel-seam
@@ -460,6 +481,35 @@ int hc_amr_copy(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void
 int hc_amr_plan_set_cf_fine(hc_amr_plan* plan, const hc_cf_fine_box* boxes, int nbox);
 int hc_amr_cf_mapped(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
 int hc_amr_cf_quotient(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, void* stream);
+
+/* The last step of a fine box's fourth-order preparation: its native
+ * averages USph on the operator's input box (usph_lo, usph_n; valid.grow(5)
+ * for the Berta operator) from its Cartesian averages U (after the
+ * exchanges and the coarse-fine fill), and its radial boundary ghosts.
+ * Replaces cachedNativeConversion + fillRadialBoundaries on the fine
+ * boxes (src/MHD_AMRFourthOrder.H:86-100; conversion
+ * src/MHD_CachedCartesianConversion.H:65-124, ghosts
+ * src/BoxOp_PreStage.H:57-228), with the same arithmetic as the level's
+ * stage preparation: cells with 0 <= i < nr take the fourth-order matrix
+ * quotient of U at (i, j, k) and its angular neighbours; i < 0 the analytic
+ * inner wind at time t; i >= nr the native value at nr - 1 scaled by
+ * (r_last / r)^2 (B_t by r_last / r).  The context is the level's (its
+ * geometry); the usph box's angular cells lie within [-5, na + 5), radial
+ * within [-5, nr + 5); the cart box (8 components SoA) holds every
+ * (i, j +- 1, k +- 1) the conversion reads; cart cells beyond the panel
+ * must already hold the seam-interpolated averages (this library fills
+ * those for whole levels only, so AMR boxes whose cart box crosses a panel
+ * edge are the caller's). */
+typedef struct hc_native_box {
+  const double* cart;
+  double* usph;
+  int cart_lo[3], cart_n[3];
+  int usph_lo[3], usph_n[3];
+  int block;
+} hc_native_box;
+
+int hc_amr_plan_set_native(hc_amr_plan* plan, const hc_native_box* boxes, int nbox);
+int hc_amr_native(hc_ctx* ctx, const hc_amr_plan* plan, int first, int count, double t, void* stream);
 
 /* ---------------------------------------------------------------------------
  * Autotuner (no reference counterpart: the reference runs its face loops on

@@ -1454,6 +1454,11 @@ int orc_o4_cartesian(void* O, const double* ju, double* cart) {
   return 0;
 }
 int orc_o4_seams(void* O, double* cart) { o4Seams(*static_cast<O4Level*>(O), cart); return 0; }
+int orc_o4_box_native(void* O, const double* cart, const int* cart_lo, const int* cart_n, int block, double* us,
+                      const int* us_lo, const int* us_n, double t) {
+  o4BoxNative(*static_cast<O4Level*>(O), cart, cart_lo, cart_n, block, us, us_lo, us_n, t);
+  return 0;
+}
 long orc_o4_sizes(void* O, long* out) {
   const O4Level& o = *static_cast<O4Level*>(O);
   out[0] = (long)o.Nv; out[1] = (long)o.Ng; out[2] = (long)o.Nc; out[3] = o.g; out[4] = o.ga;

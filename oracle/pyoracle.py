@@ -11,6 +11,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 _D = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int)
 _I = C.POINTER(C.c_int)
 
 
@@ -133,6 +134,7 @@ def lib() -> C.CDLL:
         L.orc_o4_prepare.argtypes = [C.c_void_p, _D, _D, C.c_double]
         L.orc_o4_cartesian.argtypes = [C.c_void_p, _D, _D]
         L.orc_o4_seams.argtypes = [C.c_void_p, _D]
+        L.orc_o4_box_native.argtypes = [C.c_void_p, _D, _IP, _IP, C.c_int, _D, _IP, _IP, C.c_double]
         L.orc_o4_rhs.argtypes = [C.c_void_p, _D, _D, _D, C.c_double]
         L.orc_o4_reflux.argtypes = [C.c_void_p, _D, _D]
         L.orc_o4_rk4_step.argtypes = [C.c_void_p, _D, C.c_double, C.c_double]
@@ -329,6 +331,14 @@ class OracleLevelO4:
         cart = np.zeros(6 * 8 * self.nc)
         self.L.orc_o4_cartesian(self.h, dptr(ju), dptr(cart))
         return cart
+
+    def box_native(self, cart: np.ndarray, cart_lo, block: int, us: np.ndarray, us_lo, t: float) -> None:
+        """Native averages of one box (o4BoxNative): cart [8][k][j][i] over
+        cart_lo .. (its shape), us likewise over us_lo."""
+        cn = (C.c_int * 3)(cart.shape[3], cart.shape[2], cart.shape[1])
+        un = (C.c_int * 3)(us.shape[3], us.shape[2], us.shape[1])
+        self.L.orc_o4_box_native(self.h, dptr(cart), (C.c_int * 3)(*cart_lo), cn, block, dptr(us),
+                                 (C.c_int * 3)(*us_lo), un, t)
 
     def seams(self, cart: np.ndarray) -> None:
         self.L.orc_o4_seams(self.h, dptr(cart))

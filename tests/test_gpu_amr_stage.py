@@ -291,3 +291,50 @@ def test_region_copies_match_oracle(oracle_lib):
     with pytest.raises(hc.HcError):
         plan.copy(0, 2)
     plan.close()
+
+
+def test_native_conversion_of_boxes_matches_oracle(oracle_lib):
+    """hc_amr_native: native averages and radial ghosts of three fine boxes
+    in one launch (one reaching into the inner radial ghosts, one into the
+    outer, one inside), from random Cartesian averages, against the
+    oracle's o4BoxNative.  Tolerance 1e-13 of each component's largest
+    magnitude: the device contracts a*b+c into FMA where the oracle does
+    not."""
+    _need_gpu()
+    po = oracle_lib
+    rng = np.random.default_rng(23)
+    params = hc.Params(nr=12, na=16, spatial_order=4, riemann_solver=2, berta_fallback_type=0)
+    sh = hc.Shell(params)
+    orc = po.OracleLevelO4(po.make_params(nr=12, na=16, spatial_order=4, riemann_solver=2, berta_fallback_type=0))
+    plan = AmrPlan(sh, [])
+    # (block, usph_lo, usph_hi): the operator's input boxes valid.grow(5)
+    cases = [(0, (-5, 1, 2), (6, 12, 9)), (3, (5, 3, 4), (16, 10, 11)), (5, (2, 5, 6), (9, 10, 13))]
+    host, boxes = [], []
+    for b, ulo, uhi in cases:
+        un = [uhi[d] - ulo[d] + 1 for d in range(3)]
+        clo = [max(ulo[0], 0), ulo[1] - 1, ulo[2] - 1]
+        chi = [min(uhi[0], 11), uhi[1] + 1, uhi[2] + 1]
+        cn = [chi[d] - clo[d] + 1 for d in range(3)]
+        cart = rng.normal(size=[8] + cn[::-1])
+        cart[0] = 1.0 + rng.random(cn[::-1])
+        want = np.zeros([8] + un[::-1])
+        orc.box_native(cart, clo, b, want, ulo, 0.0)
+        dc = torch.from_numpy(cart).cuda()
+        du = torch.zeros(want.size, dtype=torch.float64, device="cuda")
+        host.append((want, du))
+        boxes.append({"cart": dc, "usph": du, "cart_lo": clo, "cart_n": cn, "usph_lo": ulo, "usph_n": un,
+                      "block": b, "_keep": dc})
+    plan.set_native(boxes)
+    plan.native(0, len(boxes), 0.0)
+    torch.cuda.synchronize()
+    for want, du in host:
+        got = du.cpu().numpy().reshape(want.shape)
+        scale = np.abs(want).reshape(8, -1).max(axis=1)
+        err = np.abs(got - want).reshape(8, -1).max(axis=1) / np.maximum(scale, 1e-300)
+        assert np.isfinite(got).all() and (err <= 1e-13).all(), err
+    # a cart box that misses a neighbour the conversion reads is refused
+    bad = dict(boxes[2], cart_lo=[boxes[2]["cart_lo"][0], boxes[2]["cart_lo"][1] + 1, boxes[2]["cart_lo"][2]])
+    plan.set_native([bad])
+    with pytest.raises(hc.HcError):
+        plan.native(0, 1, 0.0)
+    plan.close()

@@ -761,6 +761,59 @@ def cpu_baseline_serve(args, reqs, budget_s: float = 20.0) -> dict:
                       f"{el:.1f} s; combined by the schemes' shares of the ensemble's cell-updates"}
 
 
+def amr_two_level_step(args, local, seed: int) -> dict:
+    """The whole two-level AMR RK4 step on the device (heliocubed_b200.amr):
+    a 48 x 48^2 x 6 coarse shell and 8^3 boxes of the 96 x 96^2 x 6 level
+    tiling the interiors of panels 0 and 3 (radial 16..79, angular 24..71),
+    on the perturbed wind.  Per stage: coarse preparation and operator, the
+    fine boxes' coarse-fine fill, exchanges, native conversion and batched
+    operator, reflux and restrictions; the state update and averageDown."""
+    import torch
+    from heliocubed_b200.amr import AmrStep
+    from heliocubed_b200.level import Params, Shell, perturbed_wind_state
+    kw = dict(spatial_order=4, riemann_solver=2, berta_fallback_type=0)
+    nc, nf = 48, 96
+    coarse = Shell(Params(nr=nc, na=nc, **kw), device=local)
+    fine = Shell(Params(nr=nf, na=nf, **kw), device=local)
+
+    def wind(sh, n):
+        det = sh.geometry(4).reshape(6, n, n)
+        vol = sh.geometry(0).reshape(n + 1, 4)[:n, 3]
+        return perturbed_wind_state(sh.params, det, vol, seed=seed)
+
+    boxes = [(b, (i, j, k), (i + 7, j + 7, k + 7)) for b in (0, 3) for i in range(16, 80, 8)
+             for j in range(24, 72, 8) for k in range(24, 72, 8)]
+    ju_c = torch.from_numpy(np.ascontiguousarray(wind(coarse, nc).reshape(-1))).to(coarse._dev)
+    wf = wind(fine, nf)
+    states = [torch.from_numpy(np.ascontiguousarray(wf[b][:, lo[2]:hi[2] + 1, lo[1]:hi[1] + 1, lo[0]:hi[0] + 1]))
+              .to(fine._dev) for b, lo, hi in boxes]
+    del wf
+    step = AmrStep(coarse, fine, boxes)
+    step.load(ju_c, states)
+    dt = 0.5 * coarse.params.cfl / float(coarse.inv_dt_max(ju_c).item())
+    step.step(dt, 0.0)
+    torch.cuda.synchronize()
+    reps = 3
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for r in range(reps):
+        step.step(dt, (r + 1) * dt)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    valid = bool(torch.isfinite(step.state_c).all().item() and torch.isfinite(step.f["state"][0]).all().item())
+    cells_c, cells_f = 6 * nc ** 3, 512 * len(boxes)
+    step.close()
+    coarse.close()
+    fine.close()
+    return {"ms_per_step": ms, "cell_updates_per_s": (cells_c + cells_f) / (ms * 1e-3), "coarse_cells": cells_c,
+            "fine_boxes": len(boxes), "fine_cells": cells_f, "steps_timed": reps, "finite": valid,
+            "what": "coarse 48x48^2x6 shell + 8^3 fine boxes (ratio 2) tiling panels 0 and 3 (radial 16..79, "
+                    "angular 24..71 of 96): per stage the coarse preparation and operator with seam "
+                    "reconciliation, the fine boxes' coarse-fine fill, <JU>/<U> recovery, exchanges, native "
+                    "conversion and batched operator, reflux and restrictions; then the update and averageDown"}
+
+
 def run_amr(args, world, rank, local):
     """Batched AMR-style operator evaluation (config-3 style, scaled): boxes
     of 8^3-32^3 on three refinement levels (48^3, 96^3 and 192^3 per panel,
@@ -918,12 +971,17 @@ def run_amr(args, world, rank, local):
                                                      "every box of the two refined levels from coarse averages, "
                                                      "8 components, one launch"},
                "clocks": clocks}
-        print(json.dumps(out), flush=True)
     for _, sh, _, batch, singles in levels:
         batch.close()
         for one in singles:
             one.close()
         sh.close()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    two = amr_two_level_step(args, local, args.seed)
+    if rank == 0:
+        out["two_level_rk4_step"] = two
+        print(json.dumps(out), flush=True)
 
 
 def main() -> int:

@@ -151,7 +151,11 @@ constexpr int kCfMaxRatio = 8, kCfMaxComp = 16;
 struct CfItem {
   hc_cf_box box;
   double w[3][kCfMaxRatio][5];  // direction, child, coarse offset -2..2
+  long long scratch;            // offset of the box's separable-pass results in the plan's scratch
 };
+// Shared memory of the separable passes: a plane of first-pass sums and a
+// ring of five planes of second-pass sums (doubles), at most this many.
+constexpr long long kCfPassMaxDoubles = 200 * 1024 / 8;
 
 __device__ __forceinline__ int floorDiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
@@ -205,6 +209,116 @@ __global__ void __launch_bounds__(kThreads) cfInterpKernel(const CfItem* __restr
     const long long fo = t;
     for (int c = 0; c < B.ncomp; ++c) B.fine[(long long)c * fineN + fo] = out[c];
   }
+}
+
+// The same interpolation as separable passes over whole planes (one CTA per
+// box and component): for each coarse plane k of the box's footprint, the
+// first-pass sums along i for every fine i and coarse j, then the
+// second-pass sums along j for every fine (i, j), kept in a ring of five
+// planes; each fine plane k takes its third-pass sums from the ring as soon
+// as its five parents' planes are there.  Every sum is the per-cell
+// kernel's, formed from the same terms in the same order (zero weights
+// skipped, a first-pass point outside the coarse box making its sum NaN);
+// the results go to scratch, and cfCommitKernel writes the ghost cells
+// whose components are all finite.
+__global__ void __launch_bounds__(kThreads) cfPassKernel(const CfItem* __restrict__ items,
+                                                         const int2* __restrict__ pass, double* __restrict__ scratch) {
+  extern __shared__ double sm[];
+  const int2 pc = pass[blockIdx.x];
+  const CfItem& it = items[pc.x];
+  const hc_cf_box& B = it.box;
+  const int comp = pc.y, tid = threadIdx.x;
+  const int fn0 = B.fine_n[0], fn1 = B.fine_n[1], fn2 = B.fine_n[2];
+  int c0[3], c1[3];
+  for (int d = 0; d < 3; ++d) {
+    c0[d] = floorDiv(B.fine_lo[d], B.ratio[d]) - 2;
+    c1[d] = floorDiv(B.fine_lo[d] + B.fine_n[d] - 1, B.ratio[d]) + 2;
+  }
+  const int nc1 = c1[1] - c0[1] + 1, plane = fn0 * fn1;
+  double* v0 = sm;              // [nc1][fn0]
+  double* ring = sm + fn0 * nc1;  // [5][fn1][fn0]
+  const long long coarseN = (long long)B.coarse_n[0] * B.coarse_n[1] * B.coarse_n[2];
+  const long long fineN = (long long)plane * fn2;
+  const double* src = B.coarse + (long long)comp * coarseN;
+  double* out = scratch + it.scratch + (long long)comp * fineN;
+  for (int ck = c0[2]; ck <= c1[2]; ++ck) {
+    const int e2 = ck - B.coarse_lo[2];
+    for (int e = tid; e < fn0 * nc1; e += kThreads) {
+      const int fi = e % fn0, cj = c0[1] + e / fn0;
+      const int p0 = B.fine_lo[0] + fi, q0 = floorDiv(p0, B.ratio[0]);
+      const double* w = it.w[0][p0 - q0 * B.ratio[0]];
+      const int b = cj - B.coarse_lo[1];
+      double v = 0.0;
+      for (int k0 = -2; k0 <= 2; ++k0) {
+        if (w[k0 + 2] == 0.0) continue;
+        const int a = q0 + k0 - B.coarse_lo[0];
+        if (a < 0 || a >= B.coarse_n[0] || b < 0 || b >= B.coarse_n[1] || e2 < 0 || e2 >= B.coarse_n[2]) {
+          v = CUDART_NAN;
+          break;
+        }
+        v = __dadd_rn(v, __dmul_rn(w[k0 + 2], src[a + (long long)B.coarse_n[0] * (b + (long long)B.coarse_n[1] * e2)]));
+      }
+      v0[e] = v;
+    }
+    __syncthreads();
+    double* slot = ring + ((ck - c0[2]) % 5) * plane;
+    for (int e = tid; e < plane; e += kThreads) {
+      const int fi = e % fn0, fj = e / fn0;
+      const int p1 = B.fine_lo[1] + fj, q1 = floorDiv(p1, B.ratio[1]);
+      const double* w = it.w[1][p1 - q1 * B.ratio[1]];
+      double v = 0.0;
+      for (int k1 = -2; k1 <= 2; ++k1) {
+        if (w[k1 + 2] == 0.0) continue;
+        v = __dadd_rn(v, __dmul_rn(w[k1 + 2], v0[fi + fn0 * (q1 + k1 - c0[1])]));
+      }
+      slot[e] = v;
+    }
+    __syncthreads();
+    // fine planes whose parent is ck - 2 (their five coarse planes are in)
+    const int qk = ck - 2;
+    const int plo = max(qk * B.ratio[2], B.fine_lo[2]), phi = min(qk * B.ratio[2] + B.ratio[2] - 1, B.fine_lo[2] + fn2 - 1);
+    for (int p2 = plo; p2 <= phi; ++p2) {
+      const double* w = it.w[2][p2 - qk * B.ratio[2]];
+      double* o = out + (long long)plane * (p2 - B.fine_lo[2]);
+      for (int e = tid; e < plane; e += kThreads) {
+        double v = 0.0;
+        for (int k2 = -2; k2 <= 2; ++k2) {
+          if (w[k2 + 2] == 0.0) continue;
+          v = __dadd_rn(v, __dmul_rn(w[k2 + 2], ring[((qk + k2 - c0[2]) % 5) * plane + e]));
+        }
+        o[e] = v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) cfCommitKernel(const CfItem* __restrict__ items,
+                                                           const Chunk* __restrict__ chunks,
+                                                           const double* __restrict__ scratch) {
+  const Chunk ch = chunks[blockIdx.x];
+  const CfItem& it = items[ch.item];
+  const hc_cf_box& B = it.box;
+  const long long fineN = (long long)B.fine_n[0] * B.fine_n[1] * B.fine_n[2];
+  const double* res = scratch + it.scratch;
+  for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
+    const int p[3] = {B.fine_lo[0] + (int)(t % B.fine_n[0]), B.fine_lo[1] + (int)((t / B.fine_n[0]) % B.fine_n[1]),
+                      B.fine_lo[2] + (int)(t / ((long long)B.fine_n[0] * B.fine_n[1]))};
+    bool inside = true;
+    for (int d = 0; d < 3; ++d) inside = inside && p[d] >= B.valid_lo[d] && p[d] <= B.valid_hi[d];
+    if (inside) continue;
+    bool finite = true;
+    for (int c = 0; c < B.ncomp; ++c) finite = finite && isfinite(res[(long long)c * fineN + t]);
+    if (!finite) continue;
+    for (int c = 0; c < B.ncomp; ++c) B.fine[(long long)c * fineN + t] = res[(long long)c * fineN + t];
+  }
+}
+
+// The separable passes' shared memory of a box (doubles).
+long long cfPassDoubles(const hc_cf_box& B) {
+  auto fdiv = [](int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); };
+  const long long nc1 = (fdiv(B.fine_lo[1] + B.fine_n[1] - 1, B.ratio[1]) + 2) - (fdiv(B.fine_lo[1], B.ratio[1]) - 2) + 1;
+  return (long long)B.fine_n[0] * nc1 + 5LL * B.fine_n[0] * B.fine_n[1];
 }
 
 // Fourth-order <JU> of the ghost cells and <U> of the valid cells of a fine
@@ -384,6 +498,11 @@ struct hc_amr_plan {
   Chunk* cfChunks = nullptr;
   std::vector<hc_cf_box> cfHost;
   std::vector<int> cfChunkStart;
+  double* cfScratch = nullptr;          // separable-pass results of every box (device)
+  int2* cfPass = nullptr;               // (box, component) of each pass CTA (device)
+  std::vector<int> cfPassStart;
+  std::vector<char> cfSeparable;        // per box: its planes fit the pass kernel's shared memory
+  long long cfPassMax = 0;              // largest shared memory of a separable box (doubles)
   mutable std::vector<std::pair<int, int>> cfRangesChecked, cfFineRangesChecked[2];
 };
 
@@ -474,6 +593,8 @@ extern "C" int hc_amr_plan_destroy(hc_amr_plan* P) {
   cudaFree(P->refluxChunks);
   cudaFree(P->cf);
   cudaFree(P->cfChunks);
+  cudaFree(P->cfScratch);
+  cudaFree(P->cfPass);
   cudaFree(P->cfFine);
   cudaFree(P->cfMappedChunks);
   cudaFree(P->cfQuotientChunks);
@@ -717,10 +838,48 @@ extern "C" int hc_amr_plan_set_cf_interp(hc_amr_plan* P, const hc_cf_box* boxes,
     cudaFree(devChunks);
     return cudaFailed(e, "hc_amr_plan_set_cf_interp");
   }
+  // the separable passes: scratch for every box that fits, a CTA per box
+  // and component
+  std::vector<int2> pass;
+  std::vector<int> passStart;
+  std::vector<char> separable(nbox, 0);
+  long long scratchTotal = 0, passMax = 0;
+  for (int b = 0; b < nbox; ++b) {
+    passStart.push_back((int)pass.size());
+    const long long need = cfPassDoubles(boxes[b]);
+    if (need > kCfPassMaxDoubles) continue;
+    separable[b] = 1;
+    passMax = std::max(passMax, need);
+    items[b].scratch = scratchTotal;
+    scratchTotal += (long long)boxes[b].ncomp * boxes[b].fine_n[0] * boxes[b].fine_n[1] * boxes[b].fine_n[2];
+    for (int c = 0; c < boxes[b].ncomp; ++c) pass.push_back(make_int2(b, c));
+  }
+  passStart.push_back((int)pass.size());
+  double* scr = nullptr;
+  int2* devPass = nullptr;
+  if (e == cudaSuccess && nbox) e = cudaMemcpy(dev, items.data(), sizeof(CfItem) * nbox, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && scratchTotal) e = cudaMalloc(&scr, sizeof(double) * scratchTotal);
+  if (e == cudaSuccess && !pass.empty()) e = cudaMalloc(&devPass, sizeof(int2) * pass.size());
+  if (e == cudaSuccess && !pass.empty())
+    e = cudaMemcpy(devPass, pass.data(), sizeof(int2) * pass.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(dev);
+    cudaFree(devChunks);
+    cudaFree(scr);
+    cudaFree(devPass);
+    return cudaFailed(e, "hc_amr_plan_set_cf_interp");
+  }
   cudaFree(P->cf);
   cudaFree(P->cfChunks);
+  cudaFree(P->cfScratch);
+  cudaFree(P->cfPass);
   P->cf = dev;
   P->cfChunks = devChunks;
+  P->cfScratch = scr;
+  P->cfPass = devPass;
+  P->cfPassStart = passStart;
+  P->cfSeparable = separable;
+  P->cfPassMax = passMax;
   P->cfHost.assign(boxes, boxes + nbox);
   P->cfChunkStart = start;
   P->cfRangesChecked.clear();
@@ -748,7 +907,21 @@ extern "C" int hc_amr_cf_interpolate(hc_ctx* ctx, const hc_amr_plan* P, int firs
   }
   const int c0 = count ? P->cfChunkStart[first] : 0, c1 = count ? P->cfChunkStart[first + count] : 0;
   if (c1 == c0) return HC_OK;
-  cfInterpKernel<<<c1 - c0, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(P->cf, P->cfChunks + c0);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  bool separable = true;
+  for (int a = first; a < first + count && separable; ++a) separable = P->cfSeparable[a] != 0;
+  if (separable) {
+    // separable passes into scratch, then the commit of the finite ghosts
+    const size_t smem = sizeof(double) * (size_t)P->cfPassMax;
+    cudaError_t e = cudaFuncSetAttribute(cfPassKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cudaFailed(e, "hc_amr_cf_interpolate");
+    const int p0 = P->cfPassStart[first], p1 = P->cfPassStart[first + count];
+    cfPassKernel<<<p1 - p0, kThreads, smem, s>>>(P->cf, P->cfPass + p0, P->cfScratch);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cudaFailed(e, "hc_amr_cf_interpolate");
+    cfCommitKernel<<<c1 - c0, kThreads, 0, s>>>(P->cf, P->cfChunks + c0, P->cfScratch);
+    return cudaFailed(cudaGetLastError(), "hc_amr_cf_interpolate");
+  }
+  cfInterpKernel<<<c1 - c0, kThreads, 0, s>>>(P->cf, P->cfChunks + c0);
   return cudaFailed(cudaGetLastError(), "hc_amr_cf_interpolate");
 }
 

@@ -155,9 +155,19 @@ struct CfItem {
 };
 // Shared memory of the separable passes: a plane of first-pass sums and a
 // ring of five planes of second-pass sums (doubles), at most this many.
-constexpr long long kCfPassMaxDoubles = 200 * 1024 / 8;
+constexpr long long kCfPassMaxDoubles = 192 * 1024 / 8;
+constexpr int kCfPassMaxFine = 256;  // fine extent per direction of a separable box
 
 __device__ __forceinline__ int floorDiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+// Flat index t (below 2^31: every box of a plan is checked to be) of a box
+// of extents n0 x n1 x .. -> its three offsets, in 32-bit arithmetic.
+__device__ __forceinline__ void split3(long long t, int n0, int n1, int& x, int& y, int& z) {
+  const unsigned u = (unsigned)t, a = u / (unsigned)n0, b = a / (unsigned)n1;
+  x = (int)(u - a * (unsigned)n0);
+  y = (int)(a - b * (unsigned)n1);
+  z = (int)b;
+}
 
 __global__ void __launch_bounds__(kThreads) cfInterpKernel(const CfItem* __restrict__ items,
                                                            const Chunk* __restrict__ chunks) {
@@ -167,8 +177,9 @@ __global__ void __launch_bounds__(kThreads) cfInterpKernel(const CfItem* __restr
   const long long fineN = (long long)B.fine_n[0] * B.fine_n[1] * B.fine_n[2];
   const long long coarseN = (long long)B.coarse_n[0] * B.coarse_n[1] * B.coarse_n[2];
   for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
-    const int p[3] = {B.fine_lo[0] + (int)(t % B.fine_n[0]), B.fine_lo[1] + (int)((t / B.fine_n[0]) % B.fine_n[1]),
-                      B.fine_lo[2] + (int)(t / ((long long)B.fine_n[0] * B.fine_n[1]))};
+    int p[3];
+    split3(t, B.fine_n[0], B.fine_n[1], p[0], p[1], p[2]);
+    for (int d = 0; d < 3; ++d) p[d] += B.fine_lo[d];
     bool inside = true;
     for (int d = 0; d < 3; ++d) inside = inside && p[d] >= B.valid_lo[d] && p[d] <= B.valid_hi[d];
     if (inside) continue;  // valid cells keep their own data
@@ -224,61 +235,79 @@ __global__ void __launch_bounds__(kThreads) cfInterpKernel(const CfItem* __restr
 __global__ void __launch_bounds__(kThreads) cfPassKernel(const CfItem* __restrict__ items,
                                                          const int2* __restrict__ pass, double* __restrict__ scratch) {
   extern __shared__ double sm[];
+  // fine index -> parent offset and child of each direction (no division
+  // in the passes' loops)
+  __shared__ int sq[3][kCfPassMaxFine], sc[3][kCfPassMaxFine];
+  __shared__ double sw[3][kCfMaxRatio][5];
   const int2 pc = pass[blockIdx.x];
   const CfItem& it = items[pc.x];
-  const hc_cf_box& B = it.box;
-  const int comp = pc.y, tid = threadIdx.x;
+  const hc_cf_box B = it.box;
+  const int comp = pc.y, tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+  for (int e = tid; e < 3 * kCfMaxRatio * 5; e += kThreads) (&sw[0][0][0])[e] = (&it.w[0][0][0])[e];
+  constexpr int TY = kThreads / 32;
   const int fn0 = B.fine_n[0], fn1 = B.fine_n[1], fn2 = B.fine_n[2];
   int c0[3], c1[3];
   for (int d = 0; d < 3; ++d) {
     c0[d] = floorDiv(B.fine_lo[d], B.ratio[d]) - 2;
     c1[d] = floorDiv(B.fine_lo[d] + B.fine_n[d] - 1, B.ratio[d]) + 2;
   }
+  for (int d = 0; d < 3; ++d)
+    for (int f = tid; f < B.fine_n[d]; f += kThreads) {
+      const int p = B.fine_lo[d] + f, q = floorDiv(p, B.ratio[d]);
+      sq[d][f] = q;
+      sc[d][f] = p - q * B.ratio[d];
+    }
   const int nc1 = c1[1] - c0[1] + 1, plane = fn0 * fn1;
-  double* v0 = sm;              // [nc1][fn0]
+  double* v0 = sm;                // [nc1][fn0]
   double* ring = sm + fn0 * nc1;  // [5][fn1][fn0]
   const long long coarseN = (long long)B.coarse_n[0] * B.coarse_n[1] * B.coarse_n[2];
   const long long fineN = (long long)plane * fn2;
   const double* src = B.coarse + (long long)comp * coarseN;
   double* out = scratch + it.scratch + (long long)comp * fineN;
+  __syncthreads();
   for (int ck = c0[2]; ck <= c1[2]; ++ck) {
     const int e2 = ck - B.coarse_lo[2];
-    for (int e = tid; e < fn0 * nc1; e += kThreads) {
-      const int fi = e % fn0, cj = c0[1] + e / fn0;
-      const int p0 = B.fine_lo[0] + fi, q0 = floorDiv(p0, B.ratio[0]);
-      const double* w = it.w[0][p0 - q0 * B.ratio[0]];
-      const int b = cj - B.coarse_lo[1];
-      double v = 0.0;
-      for (int k0 = -2; k0 <= 2; ++k0) {
-        if (w[k0 + 2] == 0.0) continue;
-        const int a = q0 + k0 - B.coarse_lo[0];
-        if (a < 0 || a >= B.coarse_n[0] || b < 0 || b >= B.coarse_n[1] || e2 < 0 || e2 >= B.coarse_n[2]) {
-          v = CUDART_NAN;
-          break;
+    const bool kIn = e2 >= 0 && e2 < B.coarse_n[2];
+    for (int r = ty; r < nc1; r += TY) {
+      const int b = c0[1] + r - B.coarse_lo[1];
+      const bool rowIn = kIn && b >= 0 && b < B.coarse_n[1];
+      const double* row = src + (long long)B.coarse_n[0] * (b + (long long)B.coarse_n[1] * e2);
+      for (int fi = tx; fi < fn0; fi += 32) {
+        const double* w = sw[0][sc[0][fi]];
+        const int q0 = sq[0][fi];
+        double v = 0.0;
+        for (int k0 = -2; k0 <= 2; ++k0) {
+          if (w[k0 + 2] == 0.0) continue;
+          const int a = q0 + k0 - B.coarse_lo[0];
+          if (!rowIn || a < 0 || a >= B.coarse_n[0]) {
+            v = CUDART_NAN;
+            break;
+          }
+          v = __dadd_rn(v, __dmul_rn(w[k0 + 2], row[a]));
         }
-        v = __dadd_rn(v, __dmul_rn(w[k0 + 2], src[a + (long long)B.coarse_n[0] * (b + (long long)B.coarse_n[1] * e2)]));
+        v0[r * fn0 + fi] = v;
       }
-      v0[e] = v;
     }
     __syncthreads();
     double* slot = ring + ((ck - c0[2]) % 5) * plane;
-    for (int e = tid; e < plane; e += kThreads) {
-      const int fi = e % fn0, fj = e / fn0;
-      const int p1 = B.fine_lo[1] + fj, q1 = floorDiv(p1, B.ratio[1]);
-      const double* w = it.w[1][p1 - q1 * B.ratio[1]];
-      double v = 0.0;
-      for (int k1 = -2; k1 <= 2; ++k1) {
-        if (w[k1 + 2] == 0.0) continue;
-        v = __dadd_rn(v, __dmul_rn(w[k1 + 2], v0[fi + fn0 * (q1 + k1 - c0[1])]));
+    for (int fj = ty; fj < fn1; fj += TY) {
+      const double* w = sw[1][sc[1][fj]];
+      const int base = sq[1][fj] - c0[1];
+      for (int fi = tx; fi < fn0; fi += 32) {
+        double v = 0.0;
+        for (int k1 = -2; k1 <= 2; ++k1) {
+          if (w[k1 + 2] == 0.0) continue;
+          v = __dadd_rn(v, __dmul_rn(w[k1 + 2], v0[(base + k1) * fn0 + fi]));
+        }
+        slot[fj * fn0 + fi] = v;
       }
-      slot[e] = v;
     }
     __syncthreads();
     // fine planes whose parent is ck - 2 (their five coarse planes are in)
     const int qk = ck - 2;
     const int plo = max(qk * B.ratio[2], B.fine_lo[2]), phi = min(qk * B.ratio[2] + B.ratio[2] - 1, B.fine_lo[2] + fn2 - 1);
     for (int p2 = plo; p2 <= phi; ++p2) {
-      const double* w = it.w[2][p2 - qk * B.ratio[2]];
+      const double* w = sw[2][p2 - qk * B.ratio[2]];
       double* o = out + (long long)plane * (p2 - B.fine_lo[2]);
       for (int e = tid; e < plane; e += kThreads) {
         double v = 0.0;
@@ -298,12 +327,13 @@ __global__ void __launch_bounds__(kThreads) cfCommitKernel(const CfItem* __restr
                                                            const double* __restrict__ scratch) {
   const Chunk ch = chunks[blockIdx.x];
   const CfItem& it = items[ch.item];
-  const hc_cf_box& B = it.box;
+  const hc_cf_box B = it.box;
   const long long fineN = (long long)B.fine_n[0] * B.fine_n[1] * B.fine_n[2];
   const double* res = scratch + it.scratch;
   for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
-    const int p[3] = {B.fine_lo[0] + (int)(t % B.fine_n[0]), B.fine_lo[1] + (int)((t / B.fine_n[0]) % B.fine_n[1]),
-                      B.fine_lo[2] + (int)(t / ((long long)B.fine_n[0] * B.fine_n[1]))};
+    int p[3];
+    split3(t, B.fine_n[0], B.fine_n[1], p[0], p[1], p[2]);
+    for (int d = 0; d < 3; ++d) p[d] += B.fine_lo[d];
     bool inside = true;
     for (int d = 0; d < 3; ++d) inside = inside && p[d] >= B.valid_lo[d] && p[d] <= B.valid_hi[d];
     if (inside) continue;
@@ -335,11 +365,12 @@ __device__ __forceinline__ bool inValid(const hc_cf_fine_box& B, const int p[3])
 __global__ void __launch_bounds__(kThreads) cfMappedKernel(const hc_cf_fine_box* __restrict__ items,
                                                            const Chunk* __restrict__ chunks) {
   const Chunk ch = chunks[blockIdx.x];
-  const hc_cf_fine_box& B = items[ch.item];
+  const hc_cf_fine_box B = items[ch.item];
   const long long mN = boxSize(B.mapped_n), dN = boxSize(B.donor_n), sN = boxSize(B.state_n);
   for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
-    const int p[3] = {B.mapped_lo[0] + (int)(t % B.mapped_n[0]), B.mapped_lo[1] + (int)((t / B.mapped_n[0]) % B.mapped_n[1]),
-                      B.mapped_lo[2] + (int)(t / ((long long)B.mapped_n[0] * B.mapped_n[1]))};
+    int p[3];
+    split3(t, B.mapped_n[0], B.mapped_n[1], p[0], p[1], p[2]);
+    for (int d = 0; d < 3; ++d) p[d] += B.mapped_lo[d];
     if (inValid(B, p)) {
       const long long so = boxOff(B.state_lo, B.state_n, p[0], p[1], p[2]);
       for (int c = 0; c < 8; ++c) B.mapped[c * mN + t] = B.state[c * sN + so];
@@ -370,12 +401,13 @@ __global__ void __launch_bounds__(kThreads) cfMappedKernel(const hc_cf_fine_box*
 __global__ void __launch_bounds__(kThreads) cfQuotientKernel(const hc_cf_fine_box* __restrict__ items,
                                                              const Chunk* __restrict__ chunks) {
   const Chunk ch = chunks[blockIdx.x];
-  const hc_cf_fine_box& B = items[ch.item];
+  const hc_cf_fine_box B = items[ch.item];
   const long long mN = boxSize(B.mapped_n), oN = boxSize(B.out_n);
   const int vn[3] = {B.valid_hi[0] - B.valid_lo[0] + 1, B.valid_hi[1] - B.valid_lo[1] + 1, B.valid_hi[2] - B.valid_lo[2] + 1};
   for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
-    const int p[3] = {B.valid_lo[0] + (int)(t % vn[0]), B.valid_lo[1] + (int)((t / vn[0]) % vn[1]),
-                      B.valid_lo[2] + (int)(t / ((long long)vn[0] * vn[1]))};
+    int p[3];
+    split3(t, vn[0], vn[1], p[0], p[1], p[2]);
+    for (int d = 0; d < 3; ++d) p[d] += B.valid_lo[d];
     auto jacAt = [&](const int x[3]) { return B.jac[boxOff(B.jac_lo, B.jac_n, x[0], x[1], x[2])]; };
     const double Jp = jacAt(p);
     // per direction: the derivative's three cells and weights, and dJ
@@ -420,11 +452,13 @@ __global__ void __launch_bounds__(kThreads) cfQuotientKernel(const hc_cf_fine_bo
 __global__ void __launch_bounds__(kThreads) copyKernel(const hc_copy_box* __restrict__ items,
                                                        const Chunk* __restrict__ chunks) {
   const Chunk ch = chunks[blockIdx.x];
-  const hc_copy_box& B = items[ch.item];
+  const hc_copy_box B = items[ch.item];
   const int n0 = B.hi[0] - B.lo[0] + 1, n1 = B.hi[1] - B.lo[1] + 1;
   const long long sN = boxSize(B.src_n), dN = boxSize(B.dst_n);
   for (long long t = ch.begin + threadIdx.x; t < ch.end; t += blockDim.x) {
-    const int x[3] = {B.lo[0] + (int)(t % n0), B.lo[1] + (int)((t / n0) % n1), B.lo[2] + (int)(t / ((long long)n0 * n1))};
+    int x[3];
+    split3(t, n0, n1, x[0], x[1], x[2]);
+    for (int d = 0; d < 3; ++d) x[d] += B.lo[d];
     const int y[3] = {B.sign[0] * x[B.perm[0]] + B.shift[0], B.sign[1] * x[B.perm[1]] + B.shift[1],
                       B.sign[2] * x[B.perm[2]] + B.shift[2]};
     const long long so = boxOff(B.src_lo, B.src_n, x[0], x[1], x[2]);
@@ -847,7 +881,10 @@ extern "C" int hc_amr_plan_set_cf_interp(hc_amr_plan* P, const hc_cf_box* boxes,
   for (int b = 0; b < nbox; ++b) {
     passStart.push_back((int)pass.size());
     const long long need = cfPassDoubles(boxes[b]);
-    if (need > kCfPassMaxDoubles) continue;
+    const hc_cf_box& Bb = boxes[b];
+    if (need > kCfPassMaxDoubles || Bb.fine_n[0] > kCfPassMaxFine || Bb.fine_n[1] > kCfPassMaxFine ||
+        Bb.fine_n[2] > kCfPassMaxFine)
+      continue;
     separable[b] = 1;
     passMax = std::max(passMax, need);
     items[b].scratch = scratchTotal;
@@ -1068,11 +1105,11 @@ __global__ void __launch_bounds__(kThreads, 2) nativeBoxKernel(const hc::O4Level
   const long NC = (long)B.cart_n[0] * B.cart_n[1] * B.cart_n[2];
   const int b = B.block;
   for (long long e = ch.begin + threadIdx.x; e < ch.end; e += kThreads) {
-    long r = (long)e;
-    const int i = B.usph_lo[0] + (int)(r % B.usph_n[0]);
-    r /= B.usph_n[0];
-    const int j = B.usph_lo[1] + (int)(r % B.usph_n[1]);
-    const int k = B.usph_lo[2] + (int)(r / B.usph_n[1]);
+    int i, j, k;
+    split3(e, B.usph_n[0], B.usph_n[1], i, j, k);
+    i += B.usph_lo[0];
+    j += B.usph_lo[1];
+    k += B.usph_lo[2];
     double u[8];
     auto native = [&](int ii, double out[8]) {
       hc::o4NativeCore(B.cart + nbOff(B.cart_lo, B.cart_n, ii, j, k), B.cart_n[0], (long)B.cart_n[0] * B.cart_n[1], NC,

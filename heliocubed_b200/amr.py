@@ -32,8 +32,8 @@ disjoint, inside one panel with the six donor ghost layers inside it (no
 fine panel-seam interpolation is needed), and at least 10 fine cells from
 both radial boundaries (every ghost's coarse interpolation stencil inside
 the coarse level).  The coarse level is prepared by the uniform level's
-Cartesian conversion.  Every launch reads and writes only device memory the
-step owns: a step can be captured in a CUDA graph once it has run once.
+Cartesian conversion.  All arrays are allocated when the step is built; the
+first step also builds the coarse level's operator batch.
 """
 from __future__ import annotations
 

@@ -35,6 +35,7 @@ from __future__ import annotations
 
 import hashlib
 import time
+from collections import OrderedDict
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -213,9 +214,13 @@ class Slot:
 class Cohort:
     """The fourth-order slots in flight, stepped together as an ensemble on
     one stream (see the module docstring).  Ensembles are kept by their
-    member slots (slots are pooled, so a membership can recur) until
-    close(): freeing device memory mid-run would synchronise the GPU.  The
-    device calls go through the methods at the end of the class."""
+    member slots (slots are pooled, so a membership can recur), the
+    `max_kept` most recently used ones: releasing one frees device memory,
+    which synchronises the GPU, so it happens only between chunks and only
+    past that count.  The device calls go through the methods at the end of
+    the class."""
+
+    max_kept = 64
 
     def __init__(self, chunk: int, device: int):
         self.chunk = chunk
@@ -224,7 +229,7 @@ class Cohort:
         self.members: list[Slot] = []
         self.joining: list[tuple[Slot, object]] = []
         self.event = None
-        self.ensembles: dict[tuple[int, ...], object] = {}
+        self.ensembles: "OrderedDict[tuple[int, ...], object]" = OrderedDict()
         self.chunk_steps = 0  # steps of all launched chunks (each step: one operator launch group per stage)
 
     def join(self, slot: Slot) -> None:
@@ -257,6 +262,10 @@ class Cohort:
         ens = self.ensembles.get(key)
         if ens is None:
             ens = self.ensembles[key] = self._ensemble(self.members)
+            while len(self.ensembles) > self.max_kept:
+                self.ensembles.popitem(last=False)[1].close()
+        else:
+            self.ensembles.move_to_end(key)
         self._advance(ens, self.members, steps)
         self.chunk_steps += steps
         for s in self.members:

@@ -111,3 +111,29 @@ def test_ensemble_refuses_mixed_schemes_and_repeats():
     for members in ([o4, o2], [o4, o4], [o4, rus]):
         with pytest.raises(N.HcError):
             hl.Ensemble(members)
+
+
+@pytest.mark.parametrize("riemann,gravity", [(2, 1), (1, 0)])
+def test_ensemble_other_schemes_equal_levels_alone(riemann, gravity):
+    """Gravity (batched over the ensemble's panels) and the Rusanov solver:
+    the ensemble equals each level alone, bit for bit."""
+    _need_gpu()
+    kw = dict(spatial_order=4, riemann_solver=riemann, sun_gravity=gravity, berta_fallback_type=0)
+    sizes = [(16, 16), (20, 16)]
+    alone, together = [], []
+    for q, (nr, na) in enumerate(sizes):
+        for group in (alone, together):
+            sh = hl.Shell(hl.Params(nr=nr, na=na, **kw))
+            ju = sh.init_perturbed_wind(7 + q)
+            t = torch.zeros(1, dtype=torch.float64, device=ju.device)
+            group.append((sh, ju, t))
+    for sh, ju, t in alone:
+        sh.advance(ju, 3, t)
+    ens = hl.Ensemble([sh for sh, _, _ in together])
+    ens.advance([ju for _, ju, _ in together], 3, [t for _, _, t in together])
+    torch.cuda.synchronize()
+    for (sha, a, ta), (_, b, tb) in zip(alone, together):
+        assert torch.isfinite(a).all() and sha.valid(a)
+        assert torch.equal(ta, tb)
+        assert torch.equal(a, b)
+    ens.close()

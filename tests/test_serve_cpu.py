@@ -260,3 +260,21 @@ def test_cobatch_off_keeps_per_slot_chunks(fake_slots, monkeypatch):
     srv.warm(reqs, per_shape=2)
     res = srv.run(reqs)
     assert len(res) == 2 and FakeCohort.launches == []
+
+
+def test_cohort_keeps_a_bounded_number_of_ensembles(fake_slots, monkeypatch):
+    """Past max_kept memberships the least recently used ensemble is
+    released (between chunks, never the running one)."""
+    FakeCohort.launches, FakeCohort.built = [], []
+    monkeypatch.setattr(serve, "Cohort", FakeCohort)
+    monkeypatch.setattr(FakeCohort, "max_kept", 2)
+    reqs = [serve.Request(i, 8, 8, 4, 10 + 5 * (i % 3), 0.003 * i) for i in range(8)]
+    srv = serve.EnsembleServer(hbm_budget=1e18, max_inflight=3, chunk=5, device=0)
+    srv.warm(reqs, per_shape=4)
+    res = srv.run(reqs)
+    assert len(res) == 8 and all(r.state[0] == r.rid for r in res)
+    assert len(FakeCohort.built) > 2                  # memberships changed past the bound
+    assert len(srv.cohort.ensembles) <= 2
+    closed = [e for e in FakeCohort.built if e.closed]
+    assert len(closed) == len(FakeCohort.built) - len(srv.cohort.ensembles)
+    srv.close()

@@ -285,6 +285,12 @@ struct hc_ensemble {
   O4Batch* batch = nullptr;
   int gravity = 0;
   int device = 0;
+  // member q's own kernels (CFL, schedule, preparation, update, seam
+  // reconciliation, time) run on lane q % lanes.size(), forked from and
+  // joined to the caller's stream around the batched operator
+  std::vector<cudaStream_t> lanes;
+  cudaEvent_t forkEv = nullptr;
+  std::vector<cudaEvent_t> joinEv;
 };
 
 namespace {
@@ -1550,48 +1556,71 @@ int maybeAutotune(hc_ctx* c, const double* ju, cudaStream_t s) {
 // One CFL step of every member of an ensemble: the per-level sequence of
 // hc_level_advance_cfl (dtCFL, insertion schedule, four stages, seam
 // reconciliation, time) with the operator of each stage batched.
+int ensembleFork(hc_ensemble* E, cudaStream_t s) {
+  cudaError_t e = cudaEventRecord(E->forkEv, s);
+  for (size_t l = 0; l < E->lanes.size() && e == cudaSuccess; ++l) e = cudaStreamWaitEvent(E->lanes[l], E->forkEv, 0);
+  return checkLaunch(e, "ensemble fork");
+}
+
+int ensembleJoin(hc_ensemble* E, cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
+  for (size_t l = 0; l < E->lanes.size() && e == cudaSuccess; ++l) {
+    e = cudaEventRecord(E->joinEv[l], E->lanes[l]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, E->joinEv[l], 0);
+  }
+  return checkLaunch(e, "ensemble join");
+}
+
 int ensembleStep(hc_ensemble* E, double* const* ju, double* const* time, double* const* dtOut, cudaStream_t s) {
   static const double c4[4] = {0, 0.5, 0.5, 1}, b4[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
   const int m = (int)E->members.size();
   auto invMaxOf = [](const hc_ctx* c) { return reinterpret_cast<const double*>(c->invMax); };
-  int rc = HC_OK;
+  auto lane = [E](int q) { return E->lanes[q % E->lanes.size()]; };
+  int rc = ensembleFork(E, s);
   for (int q = 0; q < m && rc == HC_OK; ++q) {
     hc_ctx* c = E->members[q];
     double* tq = time ? time[q] : nullptr;
-    rc = checkLaunch(launchCfl(c->L, ju[q], c->invMax, s), "cfl");
+    rc = checkLaunch(launchCfl(c->L, ju[q], c->invMax, lane(q)), "cfl");
     if (rc == HC_OK && c->sched && tq)
-      rc = checkLaunch(launchCmeSchedule(c->sched, c->invMax, tq, c->rusanovFlag, s), "CME schedule");
+      rc = checkLaunch(launchCmeSchedule(c->sched, c->invMax, tq, c->rusanovFlag, lane(q)), "CME schedule");
     if (rc == HC_OK)
-      rc = checkLaunch(cudaMemsetAsync(c->o4reg, 0, sizeof(double) * 6 * 2 * 2 * 8 * c->o4l.na * c->o4l.nr, s),
-                       "register");
+      rc = checkLaunch(
+          cudaMemsetAsync(c->o4reg, 0, sizeof(double) * 6 * 2 * 2 * 8 * c->o4l.na * c->o4l.nr, lane(q)), "register");
   }
   for (int stage = 0; stage < 4 && rc == HC_OK; ++stage) {
     for (int q = 0; q < m && rc == HC_OK; ++q) {
       hc_ctx* c = E->members[q];
       const O4StageIO io{c->o4l, stage == 0 ? ju[q] : c->o4next, c->o4cart, c->o4us, c->o4pv,
                          StageTime{0.0, time ? time[q] : nullptr, c4[stage], invMaxOf(c), 0.0}};
-      rc = checkLaunch(launchO4Prepare(io, s), "O4 prepare");
-      if (rc == HC_OK) rc = checkLaunch(cudaMemsetAsync(c->o4k, 0, sizeof(double) * 6 * 8 * c->o4l.Nv, s), "O4 k");
+      rc = checkLaunch(launchO4Prepare(io, lane(q)), "O4 prepare");
+      if (rc == HC_OK)
+        rc = checkLaunch(cudaMemsetAsync(c->o4k, 0, sizeof(double) * 6 * 8 * c->o4l.Nv, lane(q)), "O4 k");
     }
+    if (rc == HC_OK) rc = ensembleJoin(E, s);
     if (rc == HC_OK && E->gravity) rc = checkLaunch(launchO4BatchGravity(E->batch, s), "O4 gravity");
     if (rc != HC_OK) break;
     const RegArgs rg{nullptr, b4[stage], nullptr, 0.0};  // each box carries its level's register
     o4BatchSetVariants(E->batch, E->members[0]->o4var);
     rc = checkLaunch(launchO4Batch(E->batch, &rg, s), "O4 operator");
+    if (rc == HC_OK) rc = ensembleFork(E, s);
     for (int q = 0; q < m && rc == HC_OK; ++q) {
       hc_ctx* c = E->members[q];
-      rc = checkLaunch(launchO4Update(c->o4l, stage, c->o4k, ju[q], c->acc, c->o4next, invMaxOf(c), c->P.cfl, 0.0, s),
-                       "O4 update");
+      rc = checkLaunch(
+          launchO4Update(c->o4l, stage, c->o4k, ju[q], c->acc, c->o4next, invMaxOf(c), c->P.cfl, 0.0, lane(q)),
+          "O4 update");
     }
   }
   for (int q = 0; q < m && rc == HC_OK; ++q) {
     hc_ctx* c = E->members[q];
-    rc = checkLaunch(launchO4Reflux(c->o4l, c->L, c->o4reg, ju[q], s), "O4 reflux");
+    rc = checkLaunch(launchO4Reflux(c->o4l, c->L, c->o4reg, ju[q], lane(q)), "O4 reflux");
     if (rc == HC_OK)
-      rc = checkLaunch(launchAdvanceTime(time ? time[q] : nullptr, invMaxOf(c), c->P.cfl, dtOut ? dtOut[q] : nullptr, s),
-                       "time");
+      rc = checkLaunch(
+          launchAdvanceTime(time ? time[q] : nullptr, invMaxOf(c), c->P.cfl, dtOut ? dtOut[q] : nullptr, lane(q)),
+          "time");
   }
-  return rc;
+  // the lanes always end joined to the caller's stream (a capture must end so)
+  const int rj = ensembleJoin(E, s);
+  return rc != HC_OK ? rc : rj;
 }
 
 }  // namespace
@@ -1636,8 +1665,18 @@ int hc_ensemble_create(hc_ctx* const* members, int m, hc_ensemble** out) {
   E->device = c0->device;
   cudaError_t e = cudaSuccess;
   E->batch = o4BatchCreate(boxes.data(), (int)boxes.size(), &e);
-  if (!E->batch) {
-    delete E;
+  const int nl = m < 4 ? m : 4;
+  if (E->batch) e = cudaEventCreateWithFlags(&E->forkEv, cudaEventDisableTiming);
+  for (int l = 0; l < nl && e == cudaSuccess; ++l) {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) E->lanes.push_back(st);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) E->joinEv.push_back(ev);
+  }
+  if (!E->batch || e != cudaSuccess) {
+    hc_ensemble_destroy(E);
     return cudaFail(e, "ensemble batch");
   }
   *out = E;
@@ -1658,7 +1697,11 @@ int hc_ensemble_advance_cfl(hc_ensemble* E, double* const* ju, int nsteps, doubl
 int hc_ensemble_destroy(hc_ensemble* E) {
   if (!E) return HC_OK;
   cudaSetDevice(E->device);
-  o4BatchDestroy(E->batch);
+  for (cudaStream_t st : E->lanes) cudaStreamSynchronize(st);
+  if (E->batch) o4BatchDestroy(E->batch);
+  for (cudaStream_t st : E->lanes) cudaStreamDestroy(st);
+  for (cudaEvent_t ev : E->joinEv) cudaEventDestroy(ev);
+  if (E->forkEv) cudaEventDestroy(E->forkEv);
   delete E;
   return HC_OK;
 }

@@ -220,7 +220,7 @@ class Cohort:
     past that count.  The device calls go through the methods at the end of
     the class."""
 
-    max_kept = 64
+    max_kept = 512
 
     def __init__(self, chunk: int, device: int):
         self.chunk = chunk

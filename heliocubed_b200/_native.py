@@ -37,6 +37,9 @@ SIGNATURES = {
     "hc_level_prepare": (C.c_int, [_VP, _VP, _VP, C.c_double, _VP]),
     "hc_level_rhs": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hc_level_rk4_step": (C.c_int, [_VP, _VP, C.c_double, C.c_double, _VP]),
+    "hc_level_rk4_stage": (C.c_int, [_VP, _VP, C.c_int, C.c_double, C.c_double, _VP, _VP, _VP]),
+    "hc_level_stage_state": (C.c_int, [_VP, _VP, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_long),
+                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "hc_level_rk4_step_noalloc": (C.c_int, [_VP, _VP, C.c_double, C.c_double, _VP]),
     "hc_level_advance_cfl": (C.c_int, [_VP, _VP, C.c_int, _VP, _VP, _VP]),
     "hc_level_dt_cfl": (C.c_int, [_VP, _VP, _VP, _VP]),
@@ -82,7 +85,8 @@ class HcParams(C.Structure):
         ("divergence_cleaning", C.c_int), ("sun_gravity", C.c_int),
         ("init_condition_type", C.c_int), ("temporal_order", C.c_int),
         ("nr", C.c_int), ("na", C.c_int), ("spatial_operator", C.c_int), ("berta_detector_type", C.c_int),
-        ("berta_fallback_type", C.c_int), ("autotune", C.c_int), ("reserved_i", C.c_int * 3),
+        ("berta_fallback_type", C.c_int), ("autotune", C.c_int),
+        ("radial_offset", C.c_int), ("radial_cells", C.c_int), ("reserved_i", C.c_int * 1),
         ("gamma", C.c_double), ("entropy_fix_coeff", C.c_double), ("cfl", C.c_double),
         ("inner_radius", C.c_double), ("outer_radius", C.c_double),
         ("radial_stretch", C.c_double), ("strength", C.c_double), ("berta_eta_d", C.c_double),

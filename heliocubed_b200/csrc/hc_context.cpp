@@ -163,10 +163,16 @@ FaceGeom makeFrame(const double normal[3]) {
   return r;
 }
 
-// Radial metrics, src/BoxOp_Utilities.H:36-59.
+// Radial cells of the whole shell (a slab level holds part of them).
+int shellCells(const hc_params& P) { return P.radial_cells > 0 ? P.radial_cells : P.nr; }
+bool isSlab(const hc_params& P) { return P.nr < shellCells(P); }
+
+// Radial metrics, src/BoxOp_Utilities.H:36-59, of the level's radial cell
+// iLocal (the shell's cell iLocal + radial_offset).
 struct RadialRow { double rlow, rhigh, rhalf, vol, Dr0, area0, areaT; };
-RadialRow radialRow(const hc_params& P, int i) {
-  const double r0 = P.inner_radius, r1 = P.outer_radius, C = P.radial_stretch, dxi0 = 1.0 / P.nr;
+RadialRow radialRow(const hc_params& P, int iLocal) {
+  const int i = iLocal + P.radial_offset;
+  const double r0 = P.inner_radius, r1 = P.outer_radius, C = P.radial_stretch, dxi0 = 1.0 / shellCells(P);
   const double R_t = C == 0.0 ? (r1 - r0) : (r1 - r0) / std::expm1(C);
   const double etalow = i * dxi0;
   const double rlow = r0 + R_t * (C == 0.0 ? etalow : std::expm1(C * etalow));
@@ -305,7 +311,7 @@ int buildLevel(hc_ctx* c) {
   L.n0 = nr + 2 * g; L.n1 = na + 2 * g;
   L.Nv = (long)nr * na * na;
   L.Ng = (long)L.n0 * L.n1 * L.n1;
-  L.h = h; L.dxi0 = 1.0 / nr;
+  L.h = h; L.dxi0 = 1.0 / shellCells(P);
   L.gamma = P.gamma; L.invGm1 = 1.0 / (P.gamma - 1.0); L.entropy = P.entropy_fix_coeff; L.cfl_number = P.cfl; L.strength = P.strength;
   L.r0 = P.inner_radius; L.innerBCType = P.init_condition_type;
 
@@ -642,7 +648,7 @@ int buildO4Geometry(hc_ctx* c) {
   g.frames = upload(roe, c->owned, err);
   g.radial = upload(radial, c->owned, err);
   g.gamma = P.gamma; g.invGm1 = 1.0 / (P.gamma - 1.0); g.entropy = P.entropy_fix_coeff; g.eta_d = P.berta_eta_d;
-  g.dx[0] = 1.0 / nr; g.dx[1] = 1.0 / na; g.dx[2] = 1.0 / na;
+  g.dx[0] = 1.0 / shellCells(P); g.dx[1] = 1.0 / na; g.dx[2] = 1.0 / na;
   g.roe = P.riemann_solver == 2; g.powell = P.divergence_cleaning == 1; g.fallback = P.berta_fallback_type;
   // the CME insertion window's Rusanov flag (0 until a schedule sets it)
   {
@@ -872,10 +878,10 @@ int checkLaunch(cudaError_t e, const char* what) { return e == cudaSuccess ? HC_
 // ghosts of W[s % 2], then the fused operator + update writes the next
 // stage's primitives into W[(s + 1) % 2]; stage 3 leaves the new state's
 // primitives in W[0] and, with invMaxOut, its CFL rate.
-int rkStep(hc_ctx* c, double* ju, double dtv, const double* invMax, unsigned long long* invMaxOut, double tbase,
-           const double* tdev, cudaStream_t s) {
+int rkStage(hc_ctx* c, double* ju, int stage, double dtv, const double* invMax, unsigned long long* invMaxOut,
+            double tbase, const double* tdev, cudaStream_t s) {
   static const double c4[4] = {0, 0.5, 0.5, 1};
-  for (int stage = 0; stage < 4; ++stage) {
+  {
     double* win = c->W[stage % 2];
     StageTime st{tbase, tdev, c4[stage], invMax, dtv};
     int rc = checkLaunch(launchGhosts(c->L, win, st, s), "ghosts");
@@ -909,6 +915,15 @@ int rkStep(hc_ctx* c, double* ju, double dtv, const double* invMax, unsigned lon
                                    c->P.sun_gravity == 1, s, c->tileRK),
                        "stage");
     }
+    if (rc != HC_OK) return rc;
+  }
+  return HC_OK;
+}
+
+int rkStep(hc_ctx* c, double* ju, double dtv, const double* invMax, unsigned long long* invMaxOut, double tbase,
+           const double* tdev, cudaStream_t s) {
+  for (int stage = 0; stage < 4; ++stage) {
+    const int rc = rkStage(c, ju, stage, dtv, invMax, invMaxOut, tbase, tdev, s);
     if (rc != HC_OK) return rc;
   }
   return HC_OK;
@@ -997,27 +1012,35 @@ int ensureO4Buffers(hc_ctx* c) {
 // One fourth-order RK4 step: per stage, prepare USph from the stage state,
 // evaluate the operator into k (seam fluxes into the register), update the
 // accumulator and the next stage; then reconcile the seam fluxes.
-int o4Step(hc_ctx* c, double* ju, double dtv, const double* invMax, double tbase, const double* tdev, cudaStream_t s) {
+int o4Stage(hc_ctx* c, double* ju, int stage, double dtv, const double* invMax, double tbase, const double* tdev,
+            cudaStream_t s) {
   static const double c4[4] = {0, 0.5, 0.5, 1}, b4[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
   const O4Level& O = c->o4l;
-  int rc = checkLaunch(cudaMemsetAsync(c->o4reg, 0, sizeof(double) * 6 * 2 * 2 * 8 * O.na * O.nr, s), "register");
-  for (int stage = 0; stage < 4 && rc == HC_OK; ++stage) {
-    O4StageIO io{O, stage == 0 ? ju : c->o4next, c->o4cart, c->o4us, c->o4pv,
-                 StageTime{tbase, tdev, c4[stage], invMax, dtv}};
-    rc = checkLaunch(launchO4Prepare(io, s), "O4 prepare");
-    if (rc == HC_OK) rc = checkLaunch(cudaMemsetAsync(c->o4k, 0, sizeof(double) * 6 * 8 * O.Nv, s), "O4 k");
-    if (rc != HC_OK) break;
-    if (c->P.sun_gravity) {
-      rc = checkLaunch(launchO4BatchGravity(c->o4levelBatch, s), "O4 gravity");
-      if (rc != HC_OK) break;
-    }
-    const RegArgs rg{c->o4reg, invMax ? b4[stage] : dtv * b4[stage], invMax, c->P.cfl};
-    o4BatchSetVariants(c->o4levelBatch, c->o4var);
-    rc = checkLaunch(launchO4Batch(c->o4levelBatch, &rg, s), "O4 operator");
-    if (rc == HC_OK)
-      rc = checkLaunch(launchO4Update(O, stage, c->o4k, ju, c->acc, c->o4next, invMax, c->P.cfl, dtv, s), "O4 update");
+  int rc = HC_OK;
+  if (stage == 0)
+    rc = checkLaunch(cudaMemsetAsync(c->o4reg, 0, sizeof(double) * 6 * 2 * 2 * 8 * O.na * O.nr, s), "register");
+  if (rc != HC_OK) return rc;
+  O4StageIO io{O, stage == 0 ? ju : c->o4next, c->o4cart, c->o4us, c->o4pv,
+               StageTime{tbase, tdev, c4[stage], invMax, dtv}};
+  rc = checkLaunch(launchO4Prepare(io, s), "O4 prepare");
+  if (rc == HC_OK) rc = checkLaunch(cudaMemsetAsync(c->o4k, 0, sizeof(double) * 6 * 8 * O.Nv, s), "O4 k");
+  if (rc != HC_OK) return rc;
+  if (c->P.sun_gravity) {
+    rc = checkLaunch(launchO4BatchGravity(c->o4levelBatch, s), "O4 gravity");
+    if (rc != HC_OK) return rc;
   }
-  if (rc == HC_OK) rc = checkLaunch(launchO4Reflux(O, c->L, c->o4reg, ju, s), "O4 reflux");
+  const RegArgs rg{c->o4reg, invMax ? b4[stage] : dtv * b4[stage], invMax, c->P.cfl};
+  o4BatchSetVariants(c->o4levelBatch, c->o4var);
+  rc = checkLaunch(launchO4Batch(c->o4levelBatch, &rg, s), "O4 operator");
+  if (rc == HC_OK)
+    rc = checkLaunch(launchO4Update(O, stage, c->o4k, ju, c->acc, c->o4next, invMax, c->P.cfl, dtv, s), "O4 update");
+  if (rc == HC_OK && stage == 3) rc = checkLaunch(launchO4Reflux(O, c->L, c->o4reg, ju, s), "O4 reflux");
+  return rc;
+}
+
+int o4Step(hc_ctx* c, double* ju, double dtv, const double* invMax, double tbase, const double* tdev, cudaStream_t s) {
+  int rc = HC_OK;
+  for (int stage = 0; stage < 4 && rc == HC_OK; ++stage) rc = o4Stage(c, ju, stage, dtv, invMax, tbase, tdev, s);
   return rc;
 }
 
@@ -1051,6 +1074,9 @@ int hc_ctx_create(const hc_params* p, int device, hc_ctx** out) {
   if (p->riemann_solver != 1 && p->riemann_solver != 2) return fail(HC_ERR_ARG, "Riemann_solver_type must be 1 or 2");
   if (p->temporal_order != 4) return fail(HC_ERR_UNSUPPORTED, "temporal_order must be 4 (classical RK4)");
   if (p->nr < 4 || p->na < 4) return fail(HC_ERR_ARG, "need nr >= 4 and na >= 4");
+  if (p->radial_offset < 0 || p->radial_cells < 0) return fail(HC_ERR_ARG, "radial_offset and radial_cells must be >= 0");
+  if (p->radial_cells == 0 ? p->radial_offset != 0 : p->radial_offset + p->nr > p->radial_cells)
+    return fail(HC_ERR_ARG, "a radial slab must lie inside its shell: radial_offset + nr <= radial_cells");
   // The level kernels index cells and components in 32 bits: every ghosted
   // component array of the level (ghost layers of either order) must stay
   // below 2^31 entries.
@@ -1720,6 +1746,8 @@ int hc_cone_event(const hc_cone* cone, hc_cme_event* out) {
 int hc_level_set_cme_schedule(hc_ctx* c, const hc_cme_event* events, int n, void* stream) {
   if (!c || (n && !events)) return fail(HC_ERR_ARG, "null argument");
   if (n < 0 || n > kCmeEvents) return fail(HC_ERR_ARG, "at most 8 CME events");
+  if (n && isSlab(c->P))
+    return fail(HC_ERR_UNSUPPORTED, "CME schedules steer the whole shell's dt: not on a radial slab");
   for (int i = 1; i < n; ++i)
     if (events[i].insertion_time < events[i - 1].insertion_time)
       return fail(HC_ERR_ARG, "CME events must be ordered by insertion time");
@@ -1759,6 +1787,8 @@ int hc_level_set_cme_schedule(hc_ctx* c, const hc_cme_event* events, int n, void
 int hc_level_set_inlet(hc_ctx* c, const hc_cone* cones, int n, void* stream) {
   if (!c || (n && !cones)) return fail(HC_ERR_ARG, "null argument");
   if (n < 0 || n > kInletCones) return fail(HC_ERR_ARG, "at most 8 inlet cones");
+  if (n && isSlab(c->P))
+    return fail(HC_ERR_UNSUPPORTED, "the boundary inlet enters the shell's CFL rate: not on a radial slab");
   if (n && c->P.spatial_order != 2) return fail(HC_ERR_UNSUPPORTED, "the boundary inlet is built for order-2 contexts");
   if (n && c->P.init_condition_type != 1) return fail(HC_ERR_UNSUPPORTED, "the inlet needs the analytic-wind inner boundary");
   InletCone h[kInletCones] = {};
@@ -1802,7 +1832,8 @@ int hc_level_set_inlet(hc_ctx* c, const hc_cone* cones, int n, void* stream) {
     S.inletTemp[i] = cones[i].temperature;
   }
   const double C = c->P.radial_stretch, span = c->P.outer_radius - c->P.inner_radius;
-  S.width = span * (C == 0 ? 1. / c->P.nr : std::expm1(C / c->P.nr) / std::expm1(C));
+  const int cells = shellCells(c->P);
+  S.width = span * (C == 0 ? 1. / cells : std::expm1(C / cells) / std::expm1(C));
   S.gamma = c->P.gamma;
   if (err == cudaSuccess) err = cudaMemcpyAsync(c->sched, &S, sizeof S, cudaMemcpyHostToDevice, s);
   if (err != cudaSuccess) return cudaFail(err, "inlet");
@@ -1868,6 +1899,47 @@ int hc_level_rk4_step(hc_ctx* c, double* ju, double dt, double t, void* stream) 
   if (rc == HC_OK) rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
   if (rc != HC_OK) return rc;
   return rkStep(c, ju, dt, nullptr, nullptr, t, nullptr, s);
+}
+
+int hc_level_rk4_stage(hc_ctx* c, double* ju, int stage, double dt, double t, const double* inv_dt_max,
+                       const double* time_dev, void* stream) {
+  if (!c || !ju) return fail(HC_ERR_ARG, "null argument");
+  if (stage < 0 || stage > 3) return fail(HC_ERR_ARG, "stage must be 0..3");
+  if (!inv_dt_max && !(dt > 0)) return fail(HC_ERR_ARG, "dt must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  const double dtv = inv_dt_max ? 0.0 : dt;
+  int rc = c->P.spatial_order == 4 ? ensureO4Buffers(c) : HC_OK;
+  if (rc == HC_OK && stage == 0) {
+    if (c->sched && c->rusanovFlag)
+      rc = checkLaunch(cudaMemsetAsync(c->rusanovFlag, 0, sizeof(int), s), "CME window flag");
+    if (rc == HC_OK) rc = maybeAutotune(c, ju, s);
+    if (rc == HC_OK && c->P.spatial_order == 2) rc = checkLaunch(launchPrimValid(c->L, ju, c->W[0], s), "prim");
+  }
+  if (rc != HC_OK) return rc;
+  if (c->P.spatial_order == 4) return o4Stage(c, ju, stage, dtv, inv_dt_max, t, time_dev, s);
+  return rkStage(c, ju, stage, dtv, inv_dt_max, nullptr, t, time_dev, s);
+}
+
+int hc_level_stage_state(hc_ctx* c, double* ju, int stage, double** data, long* rows, int* row_length, int* first) {
+  if (!c || !ju || !data || !rows || !row_length || !first) return fail(HC_ERR_ARG, "null argument");
+  if (stage < 0 || stage > 3) return fail(HC_ERR_ARG, "stage must be 0..3");
+  const int nr = c->P.nr, na = c->P.na;
+  if (stage == 0 || c->P.spatial_order == 4) {
+    if (stage > 0) {
+      const int rc = ensureO4Buffers(c);
+      if (rc != HC_OK) return rc;
+    }
+    *data = stage == 0 ? ju : c->o4next;
+    *rows = 6L * 8 * na * na;
+    *row_length = nr;
+    *first = 0;
+    return HC_OK;
+  }
+  *data = c->W[stage % 2];
+  *rows = 6L * 8 * c->L.n1 * c->L.n1;
+  *row_length = c->L.n0;
+  *first = c->L.g;
+  return HC_OK;
 }
 
 int hc_level_advance_cfl(hc_ctx* c, double* ju, int nsteps, double* time_dev, double* dt_dev, void* stream) {

@@ -56,13 +56,16 @@ class Params:
     berta_fallback_type: int = 0   # 0 WENO3, 1 PLM
     berta_eta_d: float = 0.02
     autotune: int = 0              # order 2: time the stage tiles on the first step
+    radial_offset: int = 0         # a radial slab: first radial cell within its shell
+    radial_cells: int = 0          # radial cells of that shell (0: the level is the whole shell)
 
     def to_c(self) -> N.HcParams:
         p = N.HcParams()
         for k in ("nr", "na", "spatial_order", "limiter", "riemann_solver", "divergence_cleaning",
                   "sun_gravity", "init_condition_type", "temporal_order", "gamma", "entropy_fix_coeff",
                   "cfl", "inner_radius", "outer_radius", "radial_stretch", "strength", "spatial_operator",
-                  "berta_detector_type", "berta_fallback_type", "berta_eta_d", "autotune"):
+                  "berta_detector_type", "berta_fallback_type", "berta_eta_d", "autotune", "radial_offset",
+                  "radial_cells"):
             setattr(p, k, getattr(self, k))
         return p
 
@@ -275,6 +278,14 @@ def _stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+class _DeviceArray:
+    """A float64 device buffer owned by the library, for a torch view."""
+
+    def __init__(self, ptr: int, shape: tuple[int, ...]):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
 class Shell:
     """One cubed-sphere level (six panels, one box each) on one GPU."""
 
@@ -419,6 +430,24 @@ class Shell:
 
     def rk4_step(self, ju: torch.Tensor, dt: float, t: float = 0.0) -> None:
         N.check(self._lib.hc_level_rk4_step(self._ctx, _ptr(ju), dt, t, _stream()), "hc_level_rk4_step")
+
+    def rk4_stage(self, ju: torch.Tensor, stage: int, dt: float = 0.0, t: float = 0.0,
+                  inv_dt: torch.Tensor | None = None, time: torch.Tensor | None = None) -> None:
+        """Stage `stage` of rk4_step (stages 0..3 in order make one step);
+        with inv_dt (device) dt = cfl / inv_dt, with time (device) the stage
+        time is t + time + c_s dt."""
+        N.check(self._lib.hc_level_rk4_stage(self._ctx, _ptr(ju), stage, dt, t, _ptr(inv_dt), _ptr(time),
+                                             _stream()), "hc_level_rk4_stage")
+
+    def stage_state(self, ju: torch.Tensor, stage: int) -> tuple[torch.Tensor, int]:
+        """The buffer stage `stage` reads, as a (rows, radial) view sharing
+        its memory, and the column of the level's first radial cell."""
+        data, rows, n, first = C.c_void_p(), C.c_long(), C.c_int(), C.c_int()
+        N.check(self._lib.hc_level_stage_state(self._ctx, _ptr(ju), stage, C.byref(data), C.byref(rows), C.byref(n),
+                                               C.byref(first)), "hc_level_stage_state")
+        if data.value == ju.data_ptr():
+            return ju.view(rows.value, n.value), first.value
+        return torch.as_tensor(_DeviceArray(data.value, (rows.value, n.value)), device=self._dev), first.value
 
     def advance(self, ju: torch.Tensor, nsteps: int, time: torch.Tensor | None = None,
                 dt_out: torch.Tensor | None = None) -> None:

@@ -1,0 +1,244 @@
+"""One shell split into radial slabs, one per rank (one process per GPU).
+
+The reference spreads each panel's boxes over MPI ranks (Proto's
+DisjointBoxLayout), exchanges the ghost cells of the stage primitives between
+boxes and ranks in every stage's preparation
+(src/BoxOp_SecondOrderPreStage.H:55) and takes dt from the maximum over ranks
+of the CFL rate (src/BoxOp_SecondOrderCFL.H:207-209).
+
+Here rank r owns the radial cells [lo, hi) of all six panels, so panel seams
+and their flux register never cross ranks, and its level holds `halo` more
+radial layers on each side that has a neighbour.  Before each RK4 stage the
+rank receives those layers of the stage state from its neighbours (the
+layers they own next to the boundary) and then runs the stage on its whole
+level.  The owned cells come out bit-identical to the single-level step:
+
+* every value an owned cell's update reads lies within `halo` radial layers
+  of it (order 2: the stage primitives, 2 layers; order 4: the operator
+  reads 5 ghost layers of native averages, each made from the stage state
+  within 1 radial cell, so 6);
+* the slab's metric tables use the shell's radial index and spacing
+  (`Params.radial_offset`, `Params.radial_cells`);
+* the CFL rate is a maximum, taken after the exchange, so the maximum over
+  ranks is the shell's exactly.
+
+The halo layers' own updates read the slab's radial ends and are replaced at
+the next exchange; `owned()` returns the layers a rank is responsible for.
+The exchange is point-to-point between radial neighbours (NCCL between
+GPUs, gloo between host processes); the dt reduction is one all-reduce.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, replace
+
+import torch
+
+from .level import Params
+
+HALO = {2: 2, 4: 6}
+
+
+def slab_range(nr: int, world: int, rank: int) -> tuple[int, int]:
+    """Radial cells [lo, hi) rank `rank` owns: sizes differ by at most one."""
+    return rank * nr // world, (rank + 1) * nr // world
+
+
+@dataclass(frozen=True)
+class SlabPlan:
+    """Which radial layers rank `rank` of `world` owns, holds and swaps."""
+    nr: int
+    world: int
+    rank: int
+    halo: int
+
+    def __post_init__(self):
+        if not 0 <= self.rank < self.world:
+            raise ValueError(f"rank {self.rank} outside a world of {self.world}")
+        if self.nr // self.world < max(self.halo, 4):
+            raise ValueError(f"{self.world} slabs of a {self.nr}-cell shell own fewer than "
+                             f"max(halo {self.halo}, 4) radial cells each")
+
+    @property
+    def lo(self) -> int:
+        return slab_range(self.nr, self.world, self.rank)[0]
+
+    @property
+    def hi(self) -> int:
+        return slab_range(self.nr, self.world, self.rank)[1]
+
+    @property
+    def below(self) -> int:
+        return self.halo if self.rank > 0 else 0
+
+    @property
+    def above(self) -> int:
+        return self.halo if self.rank < self.world - 1 else 0
+
+    @property
+    def local_nr(self) -> int:
+        return self.hi - self.lo + self.below + self.above
+
+    @property
+    def offset(self) -> int:
+        return self.lo - self.below
+
+    def params(self, shell: Params) -> Params:
+        if shell.radial_cells or shell.radial_offset:
+            raise ValueError("the shell to split must be a whole shell")
+        return replace(shell, nr=self.local_nr, radial_offset=self.offset, radial_cells=self.nr)
+
+    def links(self, first: int) -> list[tuple[int, slice, slice]]:
+        """(neighbour rank, columns sent to it, columns received from it) of a
+        (rows, radial) view whose first level cell is at column `first`."""
+        own, b, h = self.hi - self.lo, self.below, self.halo
+        out = []
+        if self.rank > 0:
+            out.append((self.rank - 1, slice(first + b, first + b + h), slice(first, first + b)))
+        if self.rank < self.world - 1:
+            out.append((self.rank + 1, slice(first + b + own - h, first + b + own),
+                        slice(first + b + own, first + b + own + self.above)))
+        return out
+
+
+class LocalTransport:
+    """All slabs in this process (one GPU, or the host): halo layers move by
+    copies between their buffers."""
+
+    def exchange(self, plans: list[SlabPlan], bufs: list[tuple[torch.Tensor, int]]) -> None:
+        at = {p.rank: q for q, p in enumerate(plans)}
+        for q, plan in enumerate(plans):
+            buf, first = bufs[q]
+            for peer, send, _ in plan.links(first):
+                dst, dfirst = bufs[at[peer]]
+                recv = next(r for p, _, r in plans[at[peer]].links(dfirst) if p == plan.rank)
+                dst[:, recv].copy_(buf[:, send])
+
+    def max(self, values: list[torch.Tensor]) -> torch.Tensor:
+        out = values[0].clone()
+        for v in values[1:]:
+            torch.maximum(out, v, out=out)
+        return out
+
+
+class DistTransport:
+    """One slab per process: halo layers swap with the radial neighbours by
+    torch.distributed point-to-point operations (NCCL between GPUs, gloo on
+    the host), the CFL rate by an all-reduce of its maximum."""
+
+    def __init__(self, group=None):
+        self.group = group
+
+    def exchange(self, plans: list[SlabPlan], bufs: list[tuple[torch.Tensor, int]]) -> None:
+        import torch.distributed as dist
+        (plan,), ((buf, first),) = plans, bufs
+        ops, landing = [], []
+        for peer, send, recv in plan.links(first):
+            ops.append(dist.P2POp(dist.isend, buf[:, send].contiguous(), peer, self.group))
+            tmp = torch.empty((buf.shape[0], recv.stop - recv.start), dtype=buf.dtype, device=buf.device)
+            ops.append(dist.P2POp(dist.irecv, tmp, peer, self.group))
+            landing.append((recv, tmp))
+        if ops:
+            for work in dist.batch_isend_irecv(ops):
+                work.wait()
+        for recv, tmp in landing:
+            buf[:, recv].copy_(tmp)
+
+    def max(self, values: list[torch.Tensor]) -> torch.Tensor:
+        import torch.distributed as dist
+        (v,) = values
+        out = v.clone()
+        dist.all_reduce(out, op=dist.ReduceOp.MAX, group=self.group)
+        return out
+
+
+class ShardedShell:
+    """The slabs of one shell that this process drives: its own under
+    torch.distributed (`ShardedShell(params, rank, world)`), or every slab on
+    one device (`ShardedShell.emulated(params, world)`).
+
+    Methods take and return one state per local slab, each a level state of
+    the slab (level layout, `local_nr` radial cells)."""
+
+    def __init__(self, params: Params, rank: int, world: int, transport=None, device: int | None = None,
+                 level=None, halo: int | None = None, ranks: list[int] | None = None):
+        from .level import Shell
+        halo = HALO[params.spatial_order] if halo is None else halo
+        self.params = params
+        self.world = world
+        self.plans = [SlabPlan(params.nr, world, r, halo) for r in (ranks if ranks is not None else [rank])]
+        make = level if level is not None else (lambda p: Shell(p, device))
+        self.levels = [make(plan.params(params)) for plan in self.plans]
+        if transport is None:
+            transport = DistTransport() if world > 1 and len(self.plans) == 1 else LocalTransport()
+        self.transport = transport
+
+    @classmethod
+    def emulated(cls, params: Params, world: int, device: int | None = None, level=None,
+                 halo: int | None = None) -> "ShardedShell":
+        return cls(params, 0, world, LocalTransport(), device, level, halo, ranks=list(range(world)))
+
+    def close(self) -> None:
+        for lvl in self.levels:
+            if hasattr(lvl, "close"):
+                lvl.close()
+        self.levels = []
+
+    def new_states(self) -> list[torch.Tensor]:
+        return [lvl.new_state() for lvl in self.levels]
+
+    def _shape(self, plan: SlabPlan) -> tuple[int, ...]:
+        na = self.params.na
+        return 6, 8, na, na, plan.local_nr
+
+    def scatter(self, full: torch.Tensor) -> list[torch.Tensor]:
+        """Each local slab's state (halo layers included) from a whole-shell
+        state (level layout of the whole shell, on any device)."""
+        na, nr = self.params.na, self.params.nr
+        f = full.reshape(6, 8, na, na, nr)
+        out = []
+        for plan, lvl in zip(self.plans, self.levels):
+            st = lvl.new_state()
+            st.view(self._shape(plan)).copy_(f[..., plan.offset:plan.offset + plan.local_nr])
+            out.append(st)
+        return out
+
+    def owned(self, states: list[torch.Tensor]) -> list[torch.Tensor]:
+        """Views of the radial cells each local slab owns, (6, 8, na, na, hi - lo)."""
+        return [st.view(self._shape(p))[..., p.below:p.below + p.hi - p.lo] for p, st in zip(self.plans, states)]
+
+    def gather(self, states: list[torch.Tensor]) -> torch.Tensor:
+        """The whole-shell state from the local slabs (emulated slabs only)."""
+        if len(self.plans) != self.world:
+            raise ValueError("gather needs every slab in this process")
+        return torch.cat(self.owned(states), dim=-1)
+
+    def exchange(self, states: list[torch.Tensor], stage: int) -> None:
+        """Halo layers of the buffer stage `stage` reads, from the neighbours."""
+        if self.world > 1:
+            self.transport.exchange(self.plans, [lvl.stage_state(st, stage) for lvl, st in zip(self.levels, states)])
+
+    def inv_dt_max(self, states: list[torch.Tensor]) -> torch.Tensor:
+        """The shell's maximum CFL rate (one element, on the slabs' device);
+        refreshes the halo layers of the states first."""
+        self.exchange(states, 0)
+        return self.transport.max([lvl.inv_dt_max(st) for lvl, st in zip(self.levels, states)])
+
+    def rk4_step(self, states: list[torch.Tensor], dt: float, t: float = 0.0) -> None:
+        """One RK4 step of the shell with dt from the host."""
+        for stage in range(4):
+            self.exchange(states, stage)
+            for lvl, st in zip(self.levels, states):
+                lvl.rk4_stage(st, stage, dt, t)
+
+    def advance(self, states: list[torch.Tensor], nsteps: int, time: torch.Tensor) -> None:
+        """nsteps RK4 steps with dt = cfl / (the shell's maximum CFL rate),
+        kept on the device: no host synchronisation between steps.  `time`
+        (one element, device) advances by each step's dt."""
+        for _ in range(nsteps):
+            inv = self.inv_dt_max(states)
+            for stage in range(4):
+                if stage:
+                    self.exchange(states, stage)
+                for lvl, st in zip(self.levels, states):
+                    lvl.rk4_stage(st, stage, inv_dt=inv, time=time)
+            time += self.params.cfl / inv

@@ -53,7 +53,15 @@ typedef struct hc_params {
   int berta_detector_type;  /* 0 Jameson (Inputs_Parsing.H:82-84) */
   int berta_fallback_type;  /* 0 WENO3, 1 PLM (theta = 1.5 minmod3) */
   int autotune;             /* 1: time the order-2 stage tiles on the first level step (hc_ctx_autotune) */
-  int reserved_i[3];
+  /* A radial slab of a larger shell: the level holds global radial cells
+   * [radial_offset, radial_offset + nr) of a shell of radial_cells cells;
+   * radial metrics and spacing are the shell's (0 = the level is the whole
+   * shell).  The reference spreads its boxes over ranks (Proto's
+   * DisjointBoxLayout); here a rank owns a radial range of all six panels
+   * and receives its halo layers from its neighbours every stage. */
+  int radial_offset;
+  int radial_cells;
+  int reserved_i[1];
   double gamma;             /* ratio of specific heats */
   double entropy_fix_coeff; /* Roe entropy fix, default 0.3 */
   double cfl;               /* dt = cfl / max(inverse dt) */
@@ -249,6 +257,27 @@ int hc_level_rhs_fluxes(hc_ctx* ctx, const double* w, double* k,
  * register: each side takes the mean of both sides (src/MHD_AMR.H:1478-1497). */
 int hc_level_rk4_step(hc_ctx* ctx, double* ju, double dt, double t,
                       void* stream);
+
+/* Stage `stage` (0..3) of hc_level_rk4_step, for callers that act between
+ * stages: a radial slab receives its halo layers from the ranks next to it
+ * there, where each stage's preparation exchanges the ghost cells of the
+ * stage primitives between boxes and ranks (src/BoxOp_SecondOrderPreStage.H:55).
+ * Stages 0, 1, 2, 3 called in order with the same
+ * ju, dt and t launch exactly the kernels of hc_level_rk4_step; stage 3
+ * writes the new state into ju (and at order 4 reconciles the panel seams).
+ * With inv_dt_max (device) dt = cfl / *inv_dt_max; with time_dev (device)
+ * the stage time is t + *time_dev + c_s dt.
+ * hc_level_stage_state returns the buffer that stage `stage` reads and may
+ * be overwritten between stages: `rows` rows of `row_length` doubles, radial
+ * index fastest, the level's radial cell i at row offset first + i.  Stage
+ * 0 reads ju itself; later stages read the context's stage state (order 4,
+ * level layout) or stage primitives (order 2, ghosted layout; their ghosts
+ * are refilled by the stage). */
+int hc_level_rk4_stage(hc_ctx* ctx, double* ju, int stage, double dt, double t,
+                       const double* inv_dt_max, const double* time_dev,
+                       void* stream);
+int hc_level_stage_state(hc_ctx* ctx, double* ju, int stage, double** data,
+                         long* rows, int* row_length, int* first);
 
 /* hc_level_rk4_step without any device allocation by the library: for
  * callers that cannot call cudaMalloc while they step (inside a stream

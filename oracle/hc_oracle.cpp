@@ -204,11 +204,17 @@ void inverse3(const double A[3][3], double inv[3][3]) {
   inv[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id;
 }
 
-// Radial metrics, restated from src/BoxOp_Utilities.H:36-59 (double, libm).
+// Radial cells of the whole shell; a level with radial_cells > 0 is the slab
+// [radial_offset, radial_offset + nr) of that shell.
+int shellCells(const hc_params& P) { return P.radial_cells > 0 ? P.radial_cells : P.nr; }
+
+// Radial metrics, restated from src/BoxOp_Utilities.H:36-59 (double, libm),
+// of the level's radial cell iLocal (the shell's cell iLocal + radial_offset).
 struct Radial { double rad, vol, Dr0, area0, areaT, rlow, rhigh; };
-Radial radialMetric(const hc_params& P, int i) {
+Radial radialMetric(const hc_params& P, int iLocal) {
   const double r0 = P.inner_radius, r1 = P.outer_radius, C = P.radial_stretch;
-  const double dxi0 = 1.0 / P.nr;
+  const int i = iLocal + P.radial_offset;
+  const double dxi0 = 1.0 / shellCells(P);
   double R_t = C == 0.0 ? (r1 - r0) : (r1 - r0) / std::expm1(C);
   double etalow = i * dxi0;
   double rlow = r0 + R_t * (C == 0.0 ? etalow : std::expm1(C * etalow));
@@ -719,7 +725,7 @@ void boxOperator(const Level& L, const int lo[3], const int hi[3], int ghost, in
   int glo[3], ghi[3];
   for (int d = 0; d < 3; ++d) { glo[d] = lo[d] - ghost; ghi[d] = hi[d] + ghost; }
   BoxIdx W(glo, ghi), V(lo, hi);
-  const double dx[3] = {1.0 / P.nr, 1.0 / P.na, 1.0 / P.na};
+  const double dx[3] = {1.0 / shellCells(P), 1.0 / P.na, 1.0 / P.na};
   std::vector<double> minusDiv(V.N, 0.0);
   for (int dir = 0; dir < 3; ++dir) {
     int flo[3] = {lo[0], lo[1], lo[2]}, fhi[3] = {hi[0], hi[1], hi[2]};
@@ -1150,7 +1156,7 @@ double levelInvDt(const Level& L, const double* ju, double coneDensity = 0) {
         }
         for (int i = 0; i < nr; ++i) {
           const Radial& r = L.rad(i);
-          const double inverseVolume = 1.0 / r.vol, width0 = r.Dr0 * (1.0 / nr);
+          const double inverseVolume = 1.0 / r.vol, width0 = r.Dr0 * (1.0 / shellCells(L.P));
           const double area[3] = {r.area0, r.areaT, r.areaT};
           double u[8];
           for (int c = 0; c < NC; ++c) u[c] = ju[I.v(b, c, i, j, k)];
@@ -1372,7 +1378,7 @@ void levelInsertCone(const Level& L, const hc_cone& c, double time, double* ju, 
   LevelArrays I(L);
   const int nr = L.nr, na = L.na;
   const double shift = c.entry_shift + c.speed * 1e5 * (time - c.entry_time);
-  const double dx0 = 1.0 / nr, dx1 = L.h;
+  const double dx0 = 1.0 / shellCells(L.P), dx1 = L.h;
   long long affected = 0;
   double added = 0;
   for (int b = 0; b < 6; ++b)

@@ -22,7 +22,8 @@ class HcParams(C.Structure):
         ("divergence_cleaning", C.c_int), ("sun_gravity", C.c_int),
         ("init_condition_type", C.c_int), ("temporal_order", C.c_int),
         ("nr", C.c_int), ("na", C.c_int), ("spatial_operator", C.c_int), ("berta_detector_type", C.c_int),
-        ("berta_fallback_type", C.c_int), ("autotune", C.c_int), ("reserved_i", C.c_int * 3),
+        ("berta_fallback_type", C.c_int), ("autotune", C.c_int),
+        ("radial_offset", C.c_int), ("radial_cells", C.c_int), ("reserved_i", C.c_int * 1),
         ("gamma", C.c_double), ("entropy_fix_coeff", C.c_double), ("cfl", C.c_double),
         ("inner_radius", C.c_double), ("outer_radius", C.c_double),
         ("radial_stretch", C.c_double), ("strength", C.c_double), ("berta_eta_d", C.c_double),

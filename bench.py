@@ -28,12 +28,17 @@ Workloads (synthetic input; the reference ships no data for them), gamma
       cone for other sizes).
   --workload amr: the AMR-style box batch (boxes of 8^3-32^3 on three
       levels), batched vs per-box launches.
+  --workload slabs: one shell (default 256 x 192^2 x 6, WENOZ + Roe + solar
+      gravity) split into radial slabs over the N ranks (strong scaling):
+      halo layers swapped with the radial neighbours before every RK4 stage,
+      dt from an all-reduce of the CFL rate.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ...]
 
 N > 1 (torchrun): every rank runs an independent replica of the workload
 (weak scaling; the path has no exchange between replicas), timed on the
-device and reduced as the max over ranks.  --impl reference times the CPU
+device and reduced as the max over ranks; --workload slabs shares one shell
+among the ranks instead.  --impl reference times the CPU
 restatement of the reference's algorithm (the reference itself cannot be
 built: its Proto dependency is absent) on the host cores, on a bounded
 sample of the same workload.
@@ -324,7 +329,8 @@ def run_reference(args, world, rank):
         config = {k: cfg[k] for k in ("workload", "cells", "scheme", "init")}
         config["dt"] = "host CFL reduction every step"
     out = {"impl": "reference", "metric": metric, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+           "scaling": "strong" if args.workload == "slabs" else "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": config, "cpu_baseline": cb,
            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -567,6 +573,108 @@ def measure_uniform(args, world, rank, local, e2e_min_steps: int = 4) -> dict:
     del lanes, scratch, bufs
     torch.cuda.empty_cache()
     return out
+
+
+def dist_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t)
+    return float(t.item())
+
+
+def run_slabs(args, world, rank, local):
+    """One shell split into radial slabs over the ranks (strong scaling): each
+    rank owns nr / N radial cells of all six panels plus halo layers, swaps
+    them with its neighbours before every RK4 stage (NCCL point-to-point)
+    and takes dt from an all-reduce of the CFL rate; dt stays on the device."""
+    import torch
+    from heliocubed_b200.shard import ShardedShell
+    torch.cuda.set_device(local)
+    params = workload_params(args)
+    sh = ShardedShell(params, rank, world, device=local)
+    lvl, plan = sh.levels[0], sh.plans[0]
+    st0 = lvl.init_perturbed_wind(args.seed)
+    states = [st0.clone()]
+    time_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    state_bytes = st0.numel() * 8
+    flush = 3 * state_bytes < 2 * L2_BYTES
+    scratch = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda") if flush else None
+    for _ in range(args.warmup):
+        sh.advance(states, 1, time_dev)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for s in range(args.steps):
+        if flush:
+            scratch.zero_()
+        ev[s][0].record(stream)
+        sh.advance(states, 1, time_dev)
+        ev[s][1].record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = dist_max(sum(a.elapsed_time(b) for a, b in ev), world)
+    sh.exchange(states, 0)
+    ok = dist_sum(float(lvl.valid(states[0])), world) == world
+
+    # End to end: each step takes the slab's state from pinned host memory
+    # and returns the cells the rank owns.
+    host_in = st0.cpu().pin_memory()
+    owned = sh.owned([st0])[0]
+    host_out = torch.empty(owned.shape, dtype=torch.float64).pin_memory()
+    dev = torch.empty_like(st0)
+    t_e2e = torch.zeros(1, dtype=torch.float64, device="cuda")
+    e2e_steps = max(2, args.steps // 2)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        dev.copy_(host_in, non_blocking=True)
+        sh.advance([dev], 1, t_e2e)
+        host_out.copy_(sh.owned([dev])[0], non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = dist_max(e0.elapsed_time(e1) / e2e_steps, world)
+    h2d = dist_sum(state_bytes, world)
+    d2h = dist_sum(owned.numel() * 8, world)
+
+    cells = 6 * args.nr * args.na * args.na
+    rows = 48 * args.na * args.na if args.order == 4 else 48 * (args.na + 4) ** 2
+    halo_bytes = 4 * (world - 1) * 2 * plan.halo * rows * 8
+    out = {
+        "metric": METRIC_UNIFORM, "value": cells * args.steps / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(workload_config(args, flush), parallelism=f"radial slabs x{world}",
+                       init="Parker-like wind + seeded 5% tangential v and B (stream-function curl)",
+                       launch="eager: per stage the halo swap, then hc_level_rk4_stage",
+                       slabs={"owned_radial_cells": [list(x) for x in
+                                                     (lambda w: [(r * args.nr // w, (r + 1) * args.nr // w)
+                                                                 for r in range(w)])(world)],
+                              "halo_layers": plan.halo, "halo_bytes_per_step": halo_bytes,
+                              "exchange": "before every RK4 stage, point-to-point with the radial neighbours "
+                                          "(NCCL); dt from an all-reduce (max) of the CFL rate"}),
+        "e2e": {"value": cells / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "pipeline": "each rank: its slab's state in from pinned host memory, one RK4 step, the cells it "
+                            "owns back, on one stream"},
+        "gpu_launches": (launches_per_step(args) - 1) * args.steps,
+        "clocks": clocks,
+        "valid_state": ok,
+    }
+    if rank == 0:
+        if not args.no_cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_baseline(args)
+        print(json.dumps(out), flush=True)
+    sh.close()
 
 
 SERVE_GRIDS = {"radial": (32, 48, 64, 96), "angular": (32, 48, 64)}
@@ -1034,7 +1142,7 @@ def main() -> int:
     ap.add_argument("--na", type=int, default=None)
     ap.add_argument("--limiter", type=int, default=3)
     ap.add_argument("--riemann", type=int, default=None)
-    ap.add_argument("--gravity", type=int, default=0)
+    ap.add_argument("--gravity", type=int, default=None, help="solar gravity (default: 1 for slabs, else 0)")
     ap.add_argument("--init", choices=["default", "cone"], default="default",
                     help="cone: the wind with a 1500 km/s, 45 deg cone-CME cloud (the large-solve workload)")
     ap.add_argument("--seed", type=int, default=20261204)
@@ -1046,9 +1154,9 @@ def main() -> int:
                          "kernels instead of timing them (for profiler runs)")
     ap.add_argument("--cpu-max-steps", type=int, default=60)
     ap.add_argument("--ref-budget", type=float, default=20.0)
-    ap.add_argument("--workload", choices=["serve", "uniform", "amr"], default=None,
+    ap.add_argument("--workload", choices=["serve", "uniform", "amr", "slabs"], default=None,
                     help="serve (default): the served CME ensemble with the large solve; uniform: one solve; "
-                         "amr: the AMR-style box batch")
+                         "amr: the AMR-style box batch; slabs: one shell split into radial slabs over the ranks")
     ap.add_argument("--serve", action="store_true", help="same as --workload serve")
     ap.add_argument("--amr", action="store_true", help="same as --workload amr")
     ap.add_argument("--no-large", action="store_true", help="serve: leave out the large single solve")
@@ -1068,10 +1176,12 @@ def main() -> int:
                                       else "uniform")
     args.order = args.order or 4
     o4 = args.order == 4
-    args.nr = args.nr or (64 if o4 else 32)
-    args.na = args.na or (64 if o4 else 32)
+    slabs = args.workload == "slabs"
+    args.nr = args.nr or (256 if slabs and o4 else 64 if o4 else 32)
+    args.na = args.na or (192 if slabs and o4 else 64 if o4 else 32)
     args.riemann = args.riemann or (2 if o4 else 1)
-    args.steps = args.steps or (20 if args.workload == "serve" else 100 if o4 else 2000)
+    args.gravity = (1 if slabs else 0) if args.gravity is None else args.gravity
+    args.steps = args.steps or (20 if args.workload == "serve" else 10 if slabs else 100 if o4 else 2000)
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
@@ -1087,6 +1197,8 @@ def main() -> int:
             run_serve(args, world, rank, local)
         elif args.workload == "amr":
             run_amr(args, world, rank, local)
+        elif args.workload == "slabs":
+            run_slabs(args, world, rank, local)
         else:
             run_b200(args, world, rank, local)
     finally:

@@ -132,13 +132,14 @@ def perturbed_wind_state(params: Params, det: np.ndarray, dvolr: np.ndarray, see
     relative size `amp` in v and B.  The tangential field is the surface
     curl of a seeded stream function times (r_ref / r)^2, so div B = 0 for
     the continuous field.  Cell averages are taken as J x point values at
-    the cell centre (J = <det A> dVolr); det [6][k][j], dvolr [nr]."""
+    the cell centre (J = <det A> dVolr); det [6][k][j], dvolr [nr].  A
+    radial slab (params.radial_cells > 0) gets its part of its shell's state."""
     spec = spec or InitSpec()
     nr, na, gam = params.nr, params.na, params.gamma
     rng = np.random.default_rng(seed)
     r0, r1, C = params.inner_radius, params.outer_radius, params.radial_stretch
     Rt = (r1 - r0) / np.expm1(C)
-    r = r0 + Rt * np.expm1(C * (np.arange(nr) + 0.5) / nr)
+    r = r0 + Rt * np.expm1(C * (params.radial_offset + np.arange(nr) + 0.5) / (params.radial_cells or nr))
     s = spec.r_ref / r
     X = cell_directions(na)                                    # [6][3][k][j]
 

@@ -38,6 +38,7 @@ SIGNATURES = {
     "hc_level_rhs": (C.c_int, [_VP, _VP, _VP, _VP]),
     "hc_level_rk4_step": (C.c_int, [_VP, _VP, C.c_double, C.c_double, _VP]),
     "hc_level_rk4_stage": (C.c_int, [_VP, _VP, C.c_int, C.c_double, C.c_double, _VP, _VP, _VP]),
+    "hc_level_set_radial_window": (C.c_int, [_VP, C.c_int, C.c_int]),
     "hc_level_stage_state": (C.c_int, [_VP, _VP, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_long),
                                        C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "hc_level_rk4_step_noalloc": (C.c_int, [_VP, _VP, C.c_double, C.c_double, _VP]),

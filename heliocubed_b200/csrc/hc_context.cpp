@@ -277,6 +277,7 @@ struct hc_ctx {
   double* o4lvlScratch = nullptr;
   double* o4pv = nullptr;      // seam interpolation point values [6][8][npts][nr]
   O4Batch* o4levelBatch = nullptr;  // the six panels on o4us -> o4k
+  int winLo = 0, winHi = 0;          // radial window of the level step's operator (winHi 0: all cells)
   // operator batches of recent argument sets (hc_box_rhs_o4, hc_level_rhs on
   // caller arrays), oldest first
   std::vector<std::pair<std::string, O4Batch*>> o4cache;
@@ -964,6 +965,7 @@ O4Batch* cachedBatch(hc_ctx* c, const O4Args& a, int* rc) {
   put(a.ur.n, sizeof a.ur.n); put(&a.uStride, sizeof a.uStride); put(&a.scale, sizeof a.scale);
   put(&a.rhs, sizeof a.rhs); put(&a.rhsStride, sizeof a.rhsStride); put(a.flux, sizeof a.flux);
   put(&a.WA, sizeof a.WA); put(&a.face, sizeof a.face); put(&a.face2, sizeof a.face2); put(&a.kp, sizeof a.kp);
+  put(&a.rr, sizeof a.rr);
   for (auto& e : c->o4cache)
     if (e.first == key) return e.second;
   std::vector<O4Args> boxes;
@@ -982,12 +984,34 @@ O4Batch* cachedBatch(hc_ctx* c, const O4Args& a, int* rc) {
   return B;
 }
 
+// The operator batch of the level step: the six panels, or their radial
+// window [winLo, winHi) writing into the level-layout k (the cells outside
+// keep rhs 0).
+int buildO4LevelBatch(hc_ctx* c) {
+  O4Args a = levelO4Args(c, c->o4us, c->o4k);
+  if (c->winHi > 0) {
+    a.vlo[0] = c->winLo;
+    a.vhi[0] = c->winHi - 1;
+    a.rr.lo[0] = a.rr.lo[1] = a.rr.lo[2] = 0;
+    a.rr.n[0] = c->o4l.nr;
+    a.rr.n[1] = a.rr.n[2] = c->o4l.na;
+    a.rr.N = c->o4l.Nv;
+    carveO4Scratch(a, c->o4lvlScratch);
+  }
+  std::vector<O4Args> boxes;
+  o4SplitArgs(a, boxes);
+  cudaError_t err;
+  c->o4levelBatch = o4BatchCreate(boxes.data(), (int)boxes.size(), &err);
+  return c->o4levelBatch ? HC_OK : cudaFail(err, "O4 level batch");
+}
+
 // Level-sized buffers of the fourth-order level step and the operator batch
 // over them, allocated on the first level call (so a context used only for
 // box and batch evaluations holds none): make that first call outside any
 // stream capture.
 int ensureO4Buffers(hc_ctx* c) {
   if (c->o4levelBatch) return HC_OK;
+  if (c->o4us) return buildO4LevelBatch(c);
   const O4Level& O = c->o4l;
   const int nr = O.nr, na = O.na;
   const int vlo[3] = {0, 0, 0}, vhi[3] = {nr - 1, na - 1, na - 1};
@@ -1003,10 +1027,7 @@ int ensureO4Buffers(hc_ctx* c) {
     *dst[q] = static_cast<double*>(p);
     if ((err = cudaMemset(p, 0, sizes[q] * sizeof(double))) != cudaSuccess) return cudaFail(err, "O4 level buffers");
   }
-  std::vector<O4Args> boxes;
-  o4SplitArgs(levelO4Args(c, c->o4us, c->o4k), boxes);
-  c->o4levelBatch = o4BatchCreate(boxes.data(), (int)boxes.size(), &err);
-  return c->o4levelBatch ? HC_OK : cudaFail(err, "O4 level batch");
+  return buildO4LevelBatch(c);
 }
 
 // One fourth-order RK4 step: per stage, prepare USph from the stage state,
@@ -1389,7 +1410,8 @@ int hc_level_rhs(hc_ctx* c, const double* w, double* k, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
     int rc = ensureO4Buffers(c);
     if (rc != HC_OK) return rc;
-    O4Batch* B = (w == c->o4us && k == c->o4k) ? c->o4levelBatch : cachedBatch(c, levelO4Args(c, w, k), &rc);
+    O4Batch* B = (w == c->o4us && k == c->o4k && c->winHi == 0) ? c->o4levelBatch
+                                                                 : cachedBatch(c, levelO4Args(c, w, k), &rc);
     if (!B) return rc;
     rc = checkLaunch(cudaMemsetAsync(k, 0, sizeof(double) * 6 * NC * c->o4l.Nv, s), "O4 k");
     if (rc == HC_OK && c->P.sun_gravity) rc = checkLaunch(launchO4BatchGravity(B, s), "O4 gravity");
@@ -1918,6 +1940,26 @@ int hc_level_rk4_stage(hc_ctx* c, double* ju, int stage, double dt, double t, co
   if (rc != HC_OK) return rc;
   if (c->P.spatial_order == 4) return o4Stage(c, ju, stage, dtv, inv_dt_max, t, time_dev, s);
   return rkStage(c, ju, stage, dtv, inv_dt_max, nullptr, t, time_dev, s);
+}
+
+int hc_level_set_radial_window(hc_ctx* c, int lo, int hi) {
+  if (!c) return fail(HC_ERR_ARG, "null argument");
+  if (c->P.spatial_order != 4) return fail(HC_ERR_UNSUPPORTED, "the radial window is built for order-4 contexts");
+  if (!(lo == 0 && hi == 0) && !(0 <= lo && lo < hi && hi <= c->P.nr))
+    return fail(HC_ERR_ARG, "the radial window needs 0 <= lo < hi <= nr (or 0, 0 for every cell)");
+  if (lo == 0 && hi == c->P.nr) hi = 0;
+  if (c->winLo == lo && c->winHi == hi) return HC_OK;
+  c->winLo = lo;
+  c->winHi = hi;
+  if (c->o4levelBatch) {
+    // the batch's device tables are freed after the device has finished
+    // the work already queued on them
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cudaFail(e, "radial window");
+    o4BatchDestroy(c->o4levelBatch);
+    c->o4levelBatch = nullptr;
+  }
+  return HC_OK;
 }
 
 int hc_level_stage_state(hc_ctx* c, double* ju, int stage, double** data, long* rows, int* row_length, int* first) {

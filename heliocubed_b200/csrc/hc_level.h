@@ -241,6 +241,10 @@ struct O4Args {
   double* seamReg;
   const double* seamInvMax;
   double seamCfl;
+  // Storage region of rhs when it is larger than the valid box (a level
+  // array of which the box evaluates a radial window); rr.N == 0: the
+  // valid box itself.
+  Reg rr;
 };
 constexpr int kO4FaceArrays = 8 * 4 + 5 + 9;  // WL, WR, FS, QD/DP (8 each) + thF, PS, BP, Bflux, Bprod + averages (8 + 1)
 

@@ -131,7 +131,7 @@ Ctx makeCtx(const O4Args& a, int d) {
   c.fr = regOf(faceBox(c.G));
   c.v1r = regOf(c.V1);
   c.v2r = regOf(c.V2);
-  c.vr = regOf(c.V);
+  c.vr = a.rr.N ? a.rr : regOf(c.V);
   return c;
 }
 

@@ -440,6 +440,11 @@ class Shell:
         N.check(self._lib.hc_level_rk4_stage(self._ctx, _ptr(ju), stage, dt, t, _ptr(inv_dt), _ptr(time),
                                              _stream()), "hc_level_rk4_stage")
 
+    def set_radial_window(self, lo: int, hi: int) -> None:
+        """Order 4: the RK4 stages evaluate the operator on radial cells
+        [lo, hi) only (0, 0: every cell); the others get rhs 0."""
+        N.check(self._lib.hc_level_set_radial_window(self._ctx, lo, hi), "hc_level_set_radial_window")
+
     def stage_state(self, ju: torch.Tensor, stage: int) -> tuple[torch.Tensor, int]:
         """The buffer stage `stage` reads, as a (rows, radial) view sharing
         its memory, and the column of the level's first radial cell."""

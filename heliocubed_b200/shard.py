@@ -22,8 +22,10 @@ level.  The owned cells come out bit-identical to the single-level step:
 * the CFL rate is a maximum, taken after the exchange, so the maximum over
   ranks is the shell's exactly.
 
-The halo layers' own updates read the slab's radial ends and are replaced at
-the next exchange; `owned()` returns the layers a rank is responsible for.
+The halo layers' own updates are replaced at the next exchange, so at order
+4 the operator runs on the owned layers only (`Shell.set_radial_window`) and
+the halo costs only its share of the stage preparation; `owned()` returns
+the layers a rank is responsible for.
 The exchange is point-to-point between radial neighbours (NCCL between
 GPUs, gloo between host processes); the dt reduction is one all-reduce.
 """
@@ -168,6 +170,12 @@ class ShardedShell:
         self.plans = [SlabPlan(params.nr, world, r, halo) for r in (ranks if ranks is not None else [rank])]
         make = level if level is not None else (lambda p: Shell(p, device))
         self.levels = [make(plan.params(params)) for plan in self.plans]
+        if params.spatial_order == 4 and world > 1:
+            # the halo layers' rhs is never used: the operator runs on the
+            # owned layers only (the stage preparation still covers the slab)
+            for plan, lvl in zip(self.plans, self.levels):
+                if hasattr(lvl, "set_radial_window"):
+                    lvl.set_radial_window(plan.below, plan.below + plan.hi - plan.lo)
         if transport is None:
             transport = DistTransport() if world > 1 and len(self.plans) == 1 else LocalTransport()
         self.transport = transport

@@ -279,6 +279,16 @@ int hc_level_rk4_stage(hc_ctx* ctx, double* ju, int stage, double dt, double t,
 int hc_level_stage_state(hc_ctx* ctx, double* ju, int stage, double** data,
                          long* rows, int* row_length, int* first);
 
+/* Order 4: the RK4 stages of this context (hc_level_rk4_step,
+ * hc_level_rk4_stage, hc_level_advance_cfl) evaluate the operator on the
+ * radial cells [lo, hi) only; every other cell's stage rhs is zero.  The
+ * stage preparation still covers the whole level, so a slab whose halo
+ * layers hold its neighbours' cells computes its own cells exactly and
+ * spends no operator work on the halo.  (0, 0) restores the whole level.
+ * Changing the window waits for the device (it rebuilds the operator's
+ * work lists): not inside a stream capture. */
+int hc_level_set_radial_window(hc_ctx* ctx, int lo, int hi);
+
 /* hc_level_rk4_step without any device allocation by the library: for
  * callers that cannot call cudaMalloc while they step (inside a stream
  * capture, under a host framework that owns all device memory, in a serving

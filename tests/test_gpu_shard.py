@@ -126,3 +126,37 @@ def test_slab_refusals():
     with pytest.raises(N.HcError):
         slab.set_cme_schedule([ev])
     slab.close()
+
+
+def test_radial_window_limits_the_operator():
+    """After stage 0 the next stage state is ju + (dt/2) k: with the window
+    [lo, hi) it equals the whole level's inside the window and ju outside."""
+    _need_gpu()
+    p = hl.Params(**CASES["o4_roe_gravity"])
+    full, win = hc.Shell(p), hc.Shell(p)
+    lo, hi = 7, 23
+    win.set_radial_window(lo, hi)
+    ju = _state(full, p)
+    dt = p.cfl / float(full.inv_dt_max(ju)[0])
+    a, b = ju.clone(), ju.clone()
+    full.rk4_stage(a, 0, dt, 0.0)
+    win.rk4_stage(b, 0, dt, 0.0)
+    sa = full.stage_state(a, 1)[0].view(6, 8, p.na, p.na, p.nr)
+    sb = win.stage_state(b, 1)[0].view(6, 8, p.na, p.na, p.nr)
+    u = ju.view(6, 8, p.na, p.na, p.nr)
+    torch.cuda.synchronize()
+    assert torch.equal(sb[..., lo:hi], sa[..., lo:hi])
+    assert torch.equal(sb[..., :lo], u[..., :lo]) and torch.equal(sb[..., hi:], u[..., hi:])
+    assert not torch.equal(sa[..., :lo], u[..., :lo])
+    win.set_radial_window(0, 0)                               # the whole level again
+    c = ju.clone()
+    win.rk4_stage(c, 0, dt, 0.0)
+    torch.cuda.synchronize()
+    assert torch.equal(win.stage_state(c, 1)[0], full.stage_state(a, 1)[0])
+    with pytest.raises(N.HcError):
+        win.set_radial_window(5, 40)
+    o2 = hc.Shell(hl.Params(**CASES["o2_roe"]))
+    with pytest.raises(N.HcError):
+        o2.set_radial_window(2, 10)
+    for s in (full, win, o2):
+        s.close()

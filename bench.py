@@ -594,11 +594,15 @@ def run_slabs(args, world, rank, local):
     from heliocubed_b200.shard import ShardedShell
     torch.cuda.set_device(local)
     params = workload_params(args)
+    from heliocubed_b200 import serve
     sh = ShardedShell(params, rank, world, device=local)
     lvl, plan = sh.levels[0], sh.plans[0]
-    st0 = lvl.init_perturbed_wind(args.seed)
-    states = [st0.clone()]
+    # the large-solve input: the wind with the cone cloud inserted, each rank
+    # building its own slab (the insertion is pointwise in the shell's radii)
+    st0 = lvl.new_state()
     time_dev = torch.zeros(1, dtype=torch.float64, device="cuda")
+    serve.admit(lvl, cone_request(args), st0, time_dev, schedule=False)
+    states = [st0.clone()]
     stream = torch.cuda.current_stream()
     state_bytes = st0.numel() * 8
     flush = 3 * state_bytes < 2 * L2_BYTES
@@ -630,7 +634,7 @@ def run_slabs(args, world, rank, local):
     owned = sh.owned([st0])[0]
     host_out = torch.empty(owned.shape, dtype=torch.float64).pin_memory()
     dev = torch.empty_like(st0)
-    t_e2e = torch.zeros(1, dtype=torch.float64, device="cuda")
+    t_e2e = torch.zeros(1, dtype=torch.float64, device="cuda") + time_dev
     e2e_steps = max(2, args.steps // 2)
     barrier(world)
     torch.cuda.synchronize()
@@ -654,7 +658,8 @@ def run_slabs(args, world, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": dict(workload_config(args, flush), parallelism=f"radial slabs x{world}",
-                       init="Parker-like wind + seeded 5% tangential v and B (stream-function curl)",
+                       init="Parker-like wind + finite cone-CME cloud (field model 4) 1500 km/s, 45 deg, 4x "
+                            "density, seeded axis, inserted on the device (each rank into its own slab)",
                        launch="eager: per stage the halo swap, then hc_level_rk4_stage",
                        slabs={"owned_radial_cells": [list(x) for x in
                                                      (lambda w: [(r * args.nr // w, (r + 1) * args.nr // w)

@@ -160,3 +160,36 @@ def test_radial_window_limits_the_operator():
         o2.set_radial_window(2, 10)
     for s in (full, win, o2):
         s.close()
+
+
+def test_slab_admission_is_the_shells():
+    """The served input (the wind with a cone cloud inserted on the device)
+    built on each slab is that slab's part of the whole shell's, bit for
+    bit, and the slabs then step like the shell."""
+    _need_gpu()
+    from heliocubed_b200 import serve
+    p = hl.Params(**CASES["o4_roe_gravity"])
+    shell = hc.Shell(p)
+    cone = serve.Cone(speed_kms=1500.0, half_width_deg=45.0, lat_deg=10.0, lon_deg=-20.0, density_ratio=4.0)
+    req = serve.Request(0, p.nr, p.na, 4, 1, 0.0, cone)
+    ju = shell.new_state()
+    t = torch.zeros(1, dtype=torch.float64, device="cuda")
+    serve.admit(shell, req, ju, t, schedule=False)
+    sh = ShardedShell.emulated(p, 3)
+    states = []
+    for lvl in sh.levels:
+        st = lvl.new_state()
+        serve.admit(lvl, req, st, torch.zeros(1, dtype=torch.float64, device="cuda"), schedule=False)
+        states.append(st)
+    torch.cuda.synchronize()
+    full = ju.view(6, 8, p.na, p.na, p.nr)
+    for plan, st in zip(sh.plans, states):
+        assert torch.equal(st.view(6, 8, p.na, p.na, plan.local_nr), full[..., plan.offset:plan.offset + plan.local_nr])
+    assert not torch.equal(ju, shell.init(serve.wind_spec()))       # the cloud is in
+    dt = p.cfl / float(shell.inv_dt_max(ju)[0])
+    shell.rk4_step(ju, dt, float(t[0]))
+    sh.rk4_step(states, dt, float(t[0]))
+    torch.cuda.synchronize()
+    assert torch.equal(sh.gather(states), ju.view(6, 8, p.na, p.na, p.nr))
+    sh.close()
+    shell.close()

@@ -249,4 +249,6 @@ class ShardedShell:
                     self.exchange(states, stage)
                 for lvl, st in zip(self.levels, states):
                     lvl.rk4_stage(st, stage, inv_dt=inv, time=time)
-            time += self.params.cfl / inv
+            # cfl / inv as one division (a float over a tensor would take
+            # its reciprocal and multiply, one rounding more than the stages')
+            time += torch.full_like(inv, self.params.cfl) / inv

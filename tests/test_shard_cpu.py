@@ -2,11 +2,12 @@
 
 * The slab plan: owned ranges, halo layers, the columns each rank sends and
   receives, and the refusals.
-* World size 2 over gloo: the sharded stepping code (ShardedShell with its
+* World sizes 2 and 3 over gloo: the sharded stepping code (ShardedShell with its
   point-to-point halo exchange and max all-reduce of the CFL rate) drives
   the oracle's level on each rank's slab; three RK4 steps with the shell's
   CFL dt equal the oracle's whole-shell steps bit for bit, at order 2
-  (PLM-MC + Rusanov, Powell) and order 4 (Berta WENOZ + Roe, Powell).  The
+  (PLM-MC + Rusanov, Powell; 2 and 3 ranks, the middle one swapping with
+  both neighbours) and order 4 (Berta WENOZ + Roe, Powell).  The
   reference exchanges ghost cells in each stage's preparation
   (src/BoxOp_SecondOrderPreStage.H:55) and reduces the CFL rate over ranks
   (src/BoxOp_SecondOrderCFL.H:207-209)."""
@@ -153,36 +154,47 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _worker(rank, port, order, ju0, q):
+def _worker(rank, world, port, order, ju0, q, advance=False):
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     sys.path.insert(0, ROOT)
-    dist.init_process_group("gloo", rank=rank, world_size=2)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         p = _params(order)
-        sh = ShardedShell(p, rank, 2, level=OracleSlab)
+        sh = ShardedShell(p, rank, world, level=OracleSlab)
         states = sh.scatter(torch.from_numpy(ju0))
         invs = []
-        for _ in range(STEPS):
-            inv = sh.inv_dt_max(states)
-            invs.append(float(inv[0]))
-            sh.rk4_step(states, p.cfl / invs[-1], 0.0)
+        if advance:
+            # dt kept as a tensor: the all-reduce feeds the stages directly
+            time = torch.zeros(1, dtype=torch.float64)
+            sh.advance(states, STEPS, time)
+            invs = [float(time[0])]
+        else:
+            for _ in range(STEPS):
+                inv = sh.inv_dt_max(states)
+                invs.append(float(inv[0]))
+                sh.rk4_step(states, p.cfl / invs[-1], 0.0)
         q.put((rank, sh.plans[0].lo, sh.owned(states)[0].numpy().copy(), invs))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("order", [2, 4])
-def test_two_rank_slabs_step_like_the_whole_shell(order, oracle_lib):
+@pytest.mark.parametrize("order,world,advance", [(2, 2, False), (2, 3, False), (2, 2, True), (4, 2, False)])
+def test_rank_slabs_step_like_the_whole_shell(order, world, advance, oracle_lib):
     ju0, invs_want, want = _whole_shell(order)
+    if advance:
+        t = 0.0
+        for inv in invs_want:
+            t += _params(order).cfl / inv
+        invs_want = [t]
     p = _params(order)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, port, order, ju0, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, order, ju0, q, advance)) for r in range(world)]
     for pr in procs:
         pr.start()
-    got = sorted((q.get(timeout=600) for _ in range(2)), key=lambda x: x[0])
+    got = sorted((q.get(timeout=600) for _ in range(world)), key=lambda x: x[0])
     for pr in procs:
         pr.join(timeout=120)
         assert pr.exitcode == 0

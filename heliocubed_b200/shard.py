@@ -145,12 +145,35 @@ class DistTransport:
         for recv, tmp in landing:
             buf[:, recv].copy_(tmp)
 
+    def agree(self, key: list[int]) -> None:
+        """Raise ValueError on every rank unless every rank passes the same
+        key (one all-gather): ranks that split different shells would swap
+        halo buffers of different shapes."""
+        import torch.distributed as dist
+        dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(self.group) == "nccl" else "cpu"
+        mine = torch.tensor(key, dtype=torch.int64, device=dev)
+        every = [torch.empty_like(mine) for _ in range(dist.get_world_size(self.group))]
+        dist.all_gather(every, mine, group=self.group)
+        bad = [r for r, k in enumerate(every) if not torch.equal(k, mine)]
+        if bad:
+            raise ValueError(f"ranks {bad} split a different shell (parameters or world size differ)")
+
     def max(self, values: list[torch.Tensor]) -> torch.Tensor:
         import torch.distributed as dist
         (v,) = values
         out = v.clone()
         dist.all_reduce(out, op=dist.ReduceOp.MAX, group=self.group)
         return out
+
+
+def _fingerprint(params: Params, world: int, halo: int) -> list[int]:
+    """Integers that differ when two ranks would split different shells:
+    the options, the bit patterns of the real parameters, world and halo."""
+    import struct
+    key = [world, halo]
+    for name, v in sorted(vars(params).items()):
+        key.append(struct.unpack("<q", struct.pack("<d", float(v)))[0] if isinstance(v, float) else int(v))
+    return key
 
 
 class ShardedShell:
@@ -168,6 +191,11 @@ class ShardedShell:
         self.params = params
         self.world = world
         self.plans = [SlabPlan(params.nr, world, r, halo) for r in (ranks if ranks is not None else [rank])]
+        if transport is None:
+            transport = DistTransport() if world > 1 and len(self.plans) == 1 else LocalTransport()
+        self.transport = transport
+        if hasattr(transport, "agree"):
+            transport.agree(_fingerprint(params, world, halo))
         make = level if level is not None else (lambda p: Shell(p, device))
         self.levels = [make(plan.params(params)) for plan in self.plans]
         if params.spatial_order == 4 and world > 1:
@@ -176,9 +204,6 @@ class ShardedShell:
             for plan, lvl in zip(self.plans, self.levels):
                 if hasattr(lvl, "set_radial_window"):
                     lvl.set_radial_window(plan.below, plan.below + plan.hi - plan.lo)
-        if transport is None:
-            transport = DistTransport() if world > 1 and len(self.plans) == 1 else LocalTransport()
-        self.transport = transport
 
     @classmethod
     def emulated(cls, params: Params, world: int, device: int | None = None, level=None,

@@ -203,3 +203,38 @@ def test_rank_slabs_step_like_the_whole_shell(order, world, advance, oracle_lib)
         assert invs == invs_want, (rank, invs, invs_want)
         assert np.array_equal(owned, want[..., lo:lo + owned.shape[-1]]), rank
     assert sum(x[2].shape[-1] for x in got) == p.nr
+
+
+def _mismatch_worker(rank, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    try:
+        p = _params(2)
+        if rank == 1:
+            p = hl.Params(**{**vars(p), "cfl": 0.3})        # one rank with another CFL number
+        try:
+            ShardedShell(p, rank, 2, level=OracleSlab)
+            q.put((rank, "built"))
+        except ValueError as e:
+            q.put((rank, str(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_ranks_with_different_shells_refuse_to_start(oracle_lib):
+    """Every rank raises before any halo swap when one rank's parameters
+    differ (its buffers would not match its neighbours')."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_mismatch_worker, args=(r, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    got = sorted(q.get(timeout=120) for _ in range(2))
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    assert [r for r, _ in got] == [0, 1]
+    assert all("split a different shell" in msg for _, msg in got), got

@@ -171,7 +171,7 @@ def _fingerprint(params: Params, world: int, halo: int) -> list[int]:
     the options, the bit patterns of the real parameters, world and halo."""
     import struct
     key = [world, halo]
-    for name, v in sorted(vars(params).items()):
+    for _, v in sorted(vars(params).items()):
         key.append(struct.unpack("<q", struct.pack("<d", float(v)))[0] if isinstance(v, float) else int(v))
     return key
 
@@ -191,6 +191,8 @@ class ShardedShell:
         self.params = params
         self.world = world
         self.plans = [SlabPlan(params.nr, world, r, halo) for r in (ranks if ranks is not None else [rank])]
+        if len(self.plans) not in (1, world) or len({p.rank for p in self.plans}) != len(self.plans):
+            raise ValueError("a process drives its own slab or every slab of the shell once")
         if transport is None:
             transport = DistTransport() if world > 1 and len(self.plans) == 1 else LocalTransport()
         self.transport = transport

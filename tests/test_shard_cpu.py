@@ -128,6 +128,10 @@ def test_slab_plan():
         SlabPlan(20, 2, 2, 2)                      # no such rank
     with pytest.raises(ValueError):
         p1.params(sp)                              # a slab is not split again
+    with pytest.raises(ValueError):                # two of three slabs in one process
+        ShardedShell(hl.Params(nr=24, na=8), 0, 3, level=lambda p: None, ranks=[0, 1])
+    with pytest.raises(ValueError):                # a slab twice
+        ShardedShell(hl.Params(nr=24, na=8), 0, 2, level=lambda p: None, ranks=[0, 0])
 
 
 def test_local_exchange_moves_owned_layers_into_halos():

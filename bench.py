@@ -769,6 +769,10 @@ def run_serve(args, world, rank, local):
     barrier(world)
     batched = server.run(reqs)
     cohort_steps = server.cohort.chunk_steps if server.cohort is not None else None
+    # the host-staged run starts, as the batched one did, without cached
+    # ensembles: the same arrivals would otherwise find every membership built
+    server.forget_ensembles()
+    torch.cuda.synchronize()
     barrier(world)
     hosted = server.run(staged)
     barrier(world)

@@ -443,6 +443,13 @@ class EnsembleServer:
         return results
 
 
+    def forget_ensembles(self) -> None:
+        """Release the cohort's cached ensembles (between runs: the next run
+        builds its memberships anew, as the first one did).  Frees device
+        memory, which synchronises the GPU."""
+        if self.cohort is not None:
+            self.cohort.close()
+
     def close(self) -> None:
         """Release every pooled slot (contexts, buffers, graphs) and the
         cohort's ensembles."""

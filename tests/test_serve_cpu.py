@@ -278,3 +278,24 @@ def test_cohort_keeps_a_bounded_number_of_ensembles(fake_slots, monkeypatch):
     closed = [e for e in FakeCohort.built if e.closed]
     assert len(closed) == len(FakeCohort.built) - len(srv.cohort.ensembles)
     srv.close()
+
+
+def test_forget_ensembles_rebuilds_memberships(fake_slots, monkeypatch):
+    """A second run of the same stream finds every membership cached unless
+    the cohort's ensembles are released between the runs; after release it
+    builds them again, as the first run did."""
+    FakeCohort.launches, FakeCohort.built = [], []
+    monkeypatch.setattr(serve, "Cohort", FakeCohort)
+    reqs = [serve.Request(i, 8, 8, 4, 10, 0.002 * i) for i in range(4)]
+    srv = serve.EnsembleServer(hbm_budget=1e18, max_inflight=4, chunk=5, device=0)
+    srv.warm(reqs, per_shape=4)
+    srv.run(reqs)
+    first = len(FakeCohort.built)
+    srv.run(reqs)
+    cached = len(FakeCohort.built) - first
+    srv.forget_ensembles()
+    assert srv.cohort.ensembles == {} and all(e.closed for e in FakeCohort.built)
+    before = len(FakeCohort.built)
+    srv.run(reqs)
+    assert first > 0 and len(FakeCohort.built) - before > 0 and cached <= len(FakeCohort.built) - before
+    srv.close()

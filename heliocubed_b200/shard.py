@@ -121,6 +121,12 @@ class LocalTransport:
             torch.maximum(out, v, out=out)
         return out
 
+    def collect(self, plans: list[SlabPlan], owned: list[torch.Tensor]) -> torch.Tensor:
+        return torch.cat([owned[q] for q in sorted(range(len(plans)), key=lambda q: plans[q].rank)], dim=-1)
+
+    def barrier(self) -> None:
+        pass
+
 
 class DistTransport:
     """One slab per process: halo layers swap with the radial neighbours by
@@ -164,6 +170,27 @@ class DistTransport:
         out = v.clone()
         dist.all_reduce(out, op=dist.ReduceOp.MAX, group=self.group)
         return out
+
+    def collect(self, plans: list[SlabPlan], owned: list[torch.Tensor]) -> torch.Tensor | None:
+        """The whole shell's cells on rank 0 (None on the others): every
+        rank sends rank 0 the cells it owns."""
+        import torch.distributed as dist
+        (plan,), (mine,) = plans, owned
+        mine = mine.contiguous()
+        if plan.rank != 0:
+            dist.send(mine, 0, group=self.group)
+            return None
+        parts = [mine]
+        for r in range(1, plan.world):
+            lo, hi = slab_range(plan.nr, plan.world, r)
+            part = torch.empty(mine.shape[:-1] + (hi - lo,), dtype=mine.dtype, device=mine.device)
+            dist.recv(part, r, group=self.group)
+            parts.append(part)
+        return torch.cat(parts, dim=-1)
+
+    def barrier(self) -> None:
+        import torch.distributed as dist
+        dist.barrier(group=self.group)
 
 
 def _fingerprint(params: Params, world: int, halo: int) -> list[int]:
@@ -246,6 +273,27 @@ class ShardedShell:
         if len(self.plans) != self.world:
             raise ValueError("gather needs every slab in this process")
         return torch.cat(self.owned(states), dim=-1)
+
+    def save(self, path: str, states: list[torch.Tensor], time: float, step: int = 0,
+             attributes: dict | None = None) -> None:
+        """Write the shell as one whole-shell checkpoint
+        (heliocubed_b200.checkpoint, the format a single-GPU level reads):
+        rank 0 collects the cells every rank owns and writes the file; every
+        rank returns once it is written."""
+        from . import checkpoint
+        full = self.transport.collect(self.plans, self.owned(states))
+        if full is not None:
+            checkpoint.save(path, self.params, full, time, step, attributes)
+        self.transport.barrier()
+
+    def load(self, path: str) -> tuple[list[torch.Tensor], float, int, dict]:
+        """Each local slab's state (halo layers included) from a whole-shell
+        checkpoint of this shell: (states, time, step, attributes)."""
+        from . import checkpoint
+        params, state, time, step, attributes = checkpoint.load(path)
+        if params != self.params:
+            raise checkpoint.CheckpointError(f"{path}: a checkpoint of another shell")
+        return self.scatter(torch.from_numpy(state)), time, step, attributes
 
     def exchange(self, states: list[torch.Tensor], stage: int) -> None:
         """Halo layers of the buffer stage `stage` reads, from the neighbours."""

@@ -242,3 +242,78 @@ def test_ranks_with_different_shells_refuse_to_start(oracle_lib):
         assert pr.exitcode == 0
     assert [r for r, _ in got] == [0, 1]
     assert all("split a different shell" in msg for _, msg in got), got
+
+
+def _resume_worker(rank, port, ju0, path, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    dist.init_process_group("gloo", rank=rank, world_size=2)
+    try:
+        p = _params(2)
+        sh = ShardedShell(p, rank, 2, level=OracleSlab)
+        states = sh.scatter(torch.from_numpy(ju0))
+        for _ in range(STEPS - 1):
+            sh.rk4_step(states, p.cfl / float(sh.inv_dt_max(states)[0]), 0.0)
+        sh.save(path, states, time=1.5, step=STEPS - 1, attributes={"cme_inserted_count": 0})
+        fresh = ShardedShell(p, rank, 2, level=OracleSlab)           # a restarted job
+        states, time, step, attrs = fresh.load(path)
+        fresh.rk4_step(states, p.cfl / float(fresh.inv_dt_max(states)[0]), 0.0)
+        q.put((rank, fresh.plans[0].lo, fresh.owned(states)[0].numpy().copy(), (time, step, attrs)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_checkpoint_resumes_exactly(oracle_lib, tmp_path):
+    """Two ranks step, write one whole-shell checkpoint (rank 0 collects the
+    owned cells), restart from it and step again: the same cells as the
+    oracle's uninterrupted whole-shell run, bit for bit, and the file is
+    the whole shell's state after the first steps."""
+    from heliocubed_b200 import checkpoint
+    ju0, invs, want = _whole_shell(2)
+    p = _params(2)
+    path = str(tmp_path / "slabs.ck")
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_resume_worker, args=(r, port, ju0, path, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    got = sorted((q.get(timeout=300) for _ in range(2)), key=lambda x: x[0])
+    for pr in procs:
+        pr.join(timeout=60)
+        assert pr.exitcode == 0
+    want = want.reshape(6, 8, p.na, p.na, p.nr)
+    for rank, lo, owned, meta in got:
+        assert meta == (1.5, STEPS - 1, {"cme_inserted_count": 0})
+        assert np.array_equal(owned, want[..., lo:lo + owned.shape[-1]]), rank
+    from oracle import pyoracle as po
+    o = po.OracleLevel(po.make_params(**{f: getattr(p, f) for f in FIELDS}))
+    mid = ju0.copy()
+    for inv in invs[:STEPS - 1]:
+        o.rk4_step(mid, p.cfl / inv, 0.0)
+    params, state, _, _, _ = checkpoint.load(path)
+    assert params == p and np.array_equal(state, mid)
+
+
+def test_emulated_slabs_checkpoint_round_trip(oracle_lib, tmp_path):
+    """A checkpoint written by three slabs in one process is the whole
+    shell's state; two slabs load it back with their halo layers; another
+    shell's checkpoint is refused."""
+    from heliocubed_b200 import checkpoint
+    ju0, _, _ = _whole_shell(2)
+    p = _params(2)
+    path = str(tmp_path / "three.ck")
+    three = ShardedShell.emulated(p, 3, level=OracleSlab)
+    three.save(path, three.scatter(torch.from_numpy(ju0)), time=2.0, step=7)
+    _, state, time, step, _ = checkpoint.load(path)
+    assert np.array_equal(state, ju0) and (time, step) == (2.0, 7)
+    two = ShardedShell.emulated(p, 2, level=OracleSlab)
+    states, _, _, _ = two.load(path)
+    full = ju0.reshape(6, 8, p.na, p.na, p.nr)
+    for plan, st in zip(two.plans, states):
+        assert np.array_equal(st.numpy().reshape(6, 8, p.na, p.na, plan.local_nr),
+                              full[..., plan.offset:plan.offset + plan.local_nr])
+    other = ShardedShell.emulated(hl.Params(**{**vars(p), "cfl": 0.3}), 2, level=OracleSlab)
+    with pytest.raises(checkpoint.CheckpointError):
+        other.load(path)

@@ -128,6 +128,11 @@ class LocalTransport:
         pass
 
 
+class SlabExchangeError(RuntimeError):
+    """A halo swap with a neighbouring rank failed (the rank left, or the
+    process group's timeout ran out)."""
+
+
 class DistTransport:
     """One slab per process: halo layers swap with the radial neighbours by
     torch.distributed point-to-point operations (NCCL between GPUs, gloo on
@@ -146,8 +151,14 @@ class DistTransport:
             ops.append(dist.P2POp(dist.irecv, tmp, peer, self.group))
             landing.append((recv, tmp))
         if ops:
-            for work in dist.batch_isend_irecv(ops):
-                work.wait()
+            try:
+                for work in dist.batch_isend_irecv(ops):
+                    work.wait()
+            except RuntimeError as e:
+                # a neighbour that left (or timed out) ends the swap with an
+                # error instead of a wait
+                peers = [p for p, _, _ in plan.links(first)]
+                raise SlabExchangeError(f"rank {plan.rank}: halo swap with ranks {peers} failed: {e}") from e
         for recv, tmp in landing:
             buf[:, recv].copy_(tmp)
 

@@ -16,6 +16,7 @@ from __future__ import annotations
 import os
 import socket
 import sys
+import time
 
 import numpy as np
 import pytest
@@ -317,3 +318,50 @@ def test_emulated_slabs_checkpoint_round_trip(oracle_lib, tmp_path):
     other = ShardedShell.emulated(hl.Params(**{**vars(p), "cfl": 0.3}), 2, level=OracleSlab)
     with pytest.raises(checkpoint.CheckpointError):
         other.load(path)
+
+
+def _leaving_worker(rank, port, ju0, q):
+    import datetime
+    import torch.distributed as dist
+    from heliocubed_b200.shard import SlabExchangeError
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    dist.init_process_group("gloo", rank=rank, world_size=2, timeout=datetime.timedelta(seconds=10))
+    p = _params(2)
+    sh = ShardedShell(p, rank, 2, level=OracleSlab)
+    states = sh.scatter(torch.from_numpy(ju0))
+    sh.rk4_step(states, 1.0e3, 0.0)
+    def report(msg):
+        q.put((rank, msg))
+        q.close()
+        q.join_thread()                               # flushed before the hard exit below
+
+    if rank == 1:
+        report("left")
+        os._exit(0)                                   # leaves between steps, with nothing in flight
+    t0 = time.monotonic()
+    try:
+        sh.rk4_step(states, 1.0e3, 0.0)
+        report("stepped")
+    except SlabExchangeError as e:
+        report(f"error after {time.monotonic() - t0:.1f} s: {e}")
+    os._exit(0)
+
+
+def test_a_rank_that_leaves_fails_the_next_swap(oracle_lib):
+    """Failure detection on the host: rank 1 exits between steps; rank 0's
+    next halo swap raises SlabExchangeError within the process group's
+    timeout instead of waiting for ever."""
+    ju0, _, _ = _whole_shell(2)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_leaving_worker, args=(r, port, ju0, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    got = dict(q.get(timeout=120) for _ in range(2))
+    for pr in procs:
+        pr.join(timeout=60)
+    assert got[1] == "left"
+    assert got[0].startswith("error after") and "halo swap with ranks [1]" in got[0], got[0]
+    assert float(got[0].split()[2]) < 30.0

@@ -53,6 +53,9 @@ def test_struct_layouts_match_header(product_lib_path):
     ({"spatial_order": 4, "berta_fallback_type": 2}, -1), ({"spatial_order": 4}, -1),  # na = 8 < 16
     # 48 (nr + 12)(na + 12)^2 >= 2^31: the level kernels index in 32 bits
     ({"nr": 4096, "na": 1024}, -1),
+    # radial slabs: an offset needs a shell, and the slab must lie inside it
+    ({"radial_offset": 2}, -1), ({"radial_offset": 30, "radial_cells": 36}, -1),
+    ({"radial_offset": -1, "radial_cells": 36}, -1), ({"radial_cells": -4}, -1),
 ])
 def test_bad_options_rejected(product_lib_path, fields, code):
     from heliocubed_b200 import _native

@@ -111,3 +111,15 @@ def test_every_struct_layout_matches_the_compiler(tmp_path):
     subprocess.run(["gcc", "-std=c11", str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
     assert got == expect
+
+
+def test_stage_entries_refuse_bad_arguments_on_the_host(product_lib_path):
+    """The per-stage step, its stage buffer and the radial window refuse a
+    null context or arguments with HC_ERR_ARG before touching a device."""
+    from heliocubed_b200 import _native
+    lib = _native.lib()
+    data, rows, n, first = C.c_void_p(), C.c_long(), C.c_int(), C.c_int()
+    assert lib.hc_level_rk4_stage(None, None, 0, 1.0, 0.0, None, None, None) == -1
+    assert lib.hc_level_stage_state(None, None, 0, C.byref(data), C.byref(rows), C.byref(n), C.byref(first)) == -1
+    assert lib.hc_level_set_radial_window(None, 0, 0) == -1
+    assert lib.hc_last_error()

@@ -46,3 +46,18 @@ def test_reference_arm_serving_workload_line():
     assert d["config"]["requests"] == 256 and d["config"]["steps_per_request"] == 1
     assert "PLM-MC+Rusanov" in d["cpu_baseline"]["sample"] and "WENOZ+Roe" in d["cpu_baseline"]["sample"]
     assert d["value"] > 0
+
+
+def test_reference_arm_slabs_workload_line():
+    """The sharded-shell workload's CPU arm: config 5's scheme and size in
+    `config`, strong scaling (one shell however many GPUs)."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", "slabs",
+                          "--steps", "1", "--warmup", "3", "--ref-budget", "1"],
+                         cwd=ROOT, capture_output=True, text=True, timeout=600, check=True).stdout
+    lines = [ln for ln in out.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert REQUIRED <= set(d), REQUIRED - set(d)
+    assert d["scaling"] == "strong" and d["config"]["cells"] == 6 * 256 * 192 * 192
+    assert d["config"]["scheme"]["spatial_order"] == 4 and d["config"]["scheme"]["gravity"] == 1
+    assert d["value"] > 0

@@ -875,8 +875,8 @@ StageArgs levelArgs(hc_ctx* c, const double* w) {
 
 int checkLaunch(cudaError_t e, const char* what) { return e == cudaSuccess ? HC_OK : cudaFail(e, what); }
 
-// One RK4 step on W[0] = primitives of ju (valid cells).  Stage s fills the
-// ghosts of W[s % 2], then the fused operator + update writes the next
+// Stage s of one RK4 step on W[0] = primitives of ju (valid cells): fill
+// the ghosts of W[s % 2], then the fused operator + update writes the next
 // stage's primitives into W[(s + 1) % 2]; stage 3 leaves the new state's
 // primitives in W[0] and, with invMaxOut, its CFL rate.
 int rkStage(hc_ctx* c, double* ju, int stage, double dtv, const double* invMax, unsigned long long* invMaxOut,
@@ -1030,9 +1030,10 @@ int ensureO4Buffers(hc_ctx* c) {
   return buildO4LevelBatch(c);
 }
 
-// One fourth-order RK4 step: per stage, prepare USph from the stage state,
-// evaluate the operator into k (seam fluxes into the register), update the
-// accumulator and the next stage; then reconcile the seam fluxes.
+// Stage `stage` of one fourth-order RK4 step: prepare USph from the stage
+// state, evaluate the operator into k (seam fluxes into the register, which
+// stage 0 clears), update the accumulator and the next stage; stage 3 then
+// reconciles the seam fluxes.
 int o4Stage(hc_ctx* c, double* ju, int stage, double dtv, const double* invMax, double tbase, const double* tdev,
             cudaStream_t s) {
   static const double c4[4] = {0, 0.5, 0.5, 1}, b4[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
